@@ -1,0 +1,228 @@
+"""Test infrastructure: ctypes binding of the CPU restatement in
+oracle/pforacle.c (built as oracle/liboracle.so).  Used only by tests/, the
+package smoke check and bench.py's CPU-baseline leg, as the checker.
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "liboracle.so")
+
+_dp = C.POINTER(C.c_double)
+
+
+class Problem(C.Structure):
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dx", C.c_double), ("dy", C.c_double), ("dz", C.c_double),
+                ("gravity", C.c_double), ("viscosity", C.c_double), ("density", C.c_double),
+                ("kx", _dp), ("ky", _dp), ("kz", _dp),
+                ("porosity", C.c_double), ("sstorage", C.c_double),
+                ("alpha", _dp), ("n", _dp), ("s_res", _dp), ("s_sat", _dp),
+                ("vg_from_file", C.c_int),
+                ("z_mult", _dp),
+                ("bc_type", C.c_int * 6),
+                ("bc_val", _dp * 6)]
+
+
+class Settings(C.Structure):
+    _fields_ = [("residual_tol", C.c_double), ("step_tol", C.c_double),
+                ("max_iter", C.c_int), ("krylov_dim", C.c_int), ("max_restarts", C.c_int),
+                ("eta_choice", C.c_int),
+                ("eta_value", C.c_double), ("eta_alpha", C.c_double), ("eta_gamma", C.c_double),
+                ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
+                ("wjacobi_weight", C.c_double)]
+
+
+class Stats(C.Structure):
+    _fields_ = [("status", C.c_int), ("nni", C.c_int), ("nli", C.c_int), ("nfe", C.c_int),
+                ("nps", C.c_int), ("npe", C.c_int), ("nbcf", C.c_int), ("nbktrk", C.c_int),
+                ("ncfl", C.c_int), ("fnorm", C.c_double)]
+
+
+def build(force: bool = False) -> str:
+    src = os.path.join(HERE, "pforacle.c")
+    if force or not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(src):
+        subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-o", LIB, src, "-lm"])
+    return LIB
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        L = C.CDLL(LIB)
+        L.pfo_residual.argtypes = [C.POINTER(Problem), C.c_double, _dp, _dp, _dp, _dp]
+        L.pfo_jacobian.argtypes = [C.POINTER(Problem), C.c_double, _dp, C.c_int, C.POINTER(_dp)]
+        L.pfo_matvec7.argtypes = [C.POINTER(Problem), C.POINTER(_dp), _dp, _dp]
+        L.pfo_saturation.argtypes = [C.POINTER(Problem), _dp, _dp, C.c_int]
+        L.pfo_relperm.argtypes = [C.POINTER(Problem), _dp, _dp, C.c_int]
+        L.pfo_mg_create.argtypes = [C.POINTER(Problem), C.POINTER(Settings)]
+        L.pfo_mg_create.restype = C.c_void_p
+        L.pfo_mg_setup.argtypes = [C.c_void_p, C.POINTER(_dp)]
+        L.pfo_mg_apply.argtypes = [C.c_void_p, _dp, _dp]
+        L.pfo_mg_num_levels.argtypes = [C.c_void_p]
+        L.pfo_mg_level_info.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_int)] * 4
+        L.pfo_mg_destroy.argtypes = [C.c_void_p]
+        L.pfo_newton_solve.argtypes = [C.POINTER(Problem), C.POINTER(Settings), C.c_double,
+                                       _dp, _dp, _dp, C.POINTER(Stats)]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+ETA = {"EtaConstant": 0, "Walker1": 1, "Walker2": 2}
+
+
+class Oracle:
+    """Oracle view of a :class:`parflow_b200.problem.RichardsProblem`."""
+
+    def __init__(self, prob, t: float = None):
+        self.prob = prob
+        self._keep = []
+        nz, ny, nx = prob.shape
+        k = np.ascontiguousarray(prob.field3d(prob.perm))
+        a = np.ascontiguousarray(prob.field3d(prob.vg_alpha))
+        n = np.ascontiguousarray(prob.field3d(prob.vg_n))
+        sr = np.ascontiguousarray(prob.field3d(prob.s_res))
+        ss = np.ascontiguousarray(prob.field3d(prob.s_sat))
+        zm = np.ascontiguousarray(prob.zmult())
+        self._keep += [k, a, n, sr, ss, zm]
+        P = Problem()
+        P.nx, P.ny, P.nz = nx, ny, nz
+        P.dx, P.dy, P.dz = prob.dx, prob.dy, prob.dz
+        P.gravity, P.viscosity, P.density = prob.gravity, prob.viscosity, prob.density
+        P.kx = P.ky = P.kz = _ptr(k)
+        P.porosity, P.sstorage = prob.porosity, prob.specific_storage
+        P.alpha, P.n, P.s_res, P.s_sat = _ptr(a), _ptr(n), _ptr(sr), _ptr(ss)
+        P.vg_from_file = 1 if prob.vg_from_file() else 0
+        P.z_mult = _ptr(zm)
+        self.P = P
+        self.set_time(prob.start_time + prob.dt if t is None else t)
+        s = prob.solver
+        S = Settings()
+        S.residual_tol, S.step_tol = s.residual_tol, s.step_tol
+        S.max_iter, S.krylov_dim, S.max_restarts = s.max_iter, s.krylov_dim, s.max_restarts
+        S.eta_choice = ETA[s.eta_choice]
+        S.eta_value, S.eta_alpha, S.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
+        S.mg_max_levels = s.mg_max_levels
+        S.mg_smoother = 0 if s.mg_smoother == "RedBlackGSPoint" else 1
+        S.wjacobi_weight = 1.0
+        self.S = S
+
+    def set_time(self, t: float):
+        self.t = t
+        self._bc = []
+        for f, (typ, vals) in enumerate(self.prob.bc_values(t)):
+            v = np.ascontiguousarray(vals, dtype=np.float64)
+            self._bc.append(v)
+            self.P.bc_type[f] = typ
+            self.P.bc_val[f] = _ptr(v)
+
+    # ---- functions --------------------------------------------------------
+    def residual(self, p, p_old, s_old, dt):
+        p, p_old, s_old = (np.ascontiguousarray(x, dtype=np.float64) for x in (p, p_old, s_old))
+        f = np.empty_like(p)
+        lib().pfo_residual(C.byref(self.P), dt, _ptr(p), _ptr(p_old), _ptr(s_old), _ptr(f))
+        return f
+
+    def saturation(self, p, der=0):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        s = np.empty_like(p)
+        lib().pfo_saturation(C.byref(self.P), _ptr(p), _ptr(s), der)
+        return s
+
+    def relperm(self, p, der=0):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        s = np.empty_like(p)
+        lib().pfo_relperm(C.byref(self.P), _ptr(p), _ptr(s), der)
+        return s
+
+    def jacobian(self, p, dt, symm=0):
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        ns = 4 if symm else 7
+        J = [np.empty_like(p) for _ in range(ns)]
+        arr = (_dp * ns)(*[_ptr(x) for x in J])
+        lib().pfo_jacobian(C.byref(self.P), dt, _ptr(p), symm, arr)
+        return J
+
+    def matvec(self, J, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        arr = (_dp * 7)(*[_ptr(np.ascontiguousarray(a)) for a in J])
+        lib().pfo_matvec7(C.byref(self.P), arr, _ptr(x), _ptr(y))
+        return y
+
+    def mg(self):
+        return MG(self)
+
+    def newton_solve(self, p_init, p_old, s_old, dt):
+        p = np.ascontiguousarray(p_init, dtype=np.float64).copy()
+        p_old, s_old = (np.ascontiguousarray(x, dtype=np.float64) for x in (p_old, s_old))
+        st = Stats()
+        lib().pfo_newton_solve(C.byref(self.P), C.byref(self.S), dt, _ptr(p_old), _ptr(s_old),
+                               _ptr(p), C.byref(st))
+        return p, st
+
+    def run(self, nsteps=None, callback=None):
+        """Advance the problem ``nsteps`` timesteps (AdvanceRichards semantics
+        without dt halving).  Returns (pressures per step, stats per step)."""
+        prob = self.prob
+        nsteps = prob.nsteps if nsteps is None else nsteps
+        p = prob.initial_pressure().copy()
+        t = prob.start_time
+        out_p, out_s = [], []
+        for _ in range(nsteps):
+            t += prob.dt
+            self.set_time(t)
+            s_old = self.saturation(p)
+            p_new, st = self.newton_solve(p, p, s_old, prob.dt)
+            p = p_new
+            out_p.append(p.copy())
+            out_s.append(st)
+            if callback:
+                callback(p, st)
+        return out_p, out_s
+
+
+class MG:
+    def __init__(self, orc: Oracle):
+        self.orc = orc
+        self.h = lib().pfo_mg_create(C.byref(orc.P), C.byref(orc.S))
+
+    def __del__(self):
+        try:
+            lib().pfo_mg_destroy(self.h)
+        except Exception:
+            pass
+
+    def levels(self):
+        out = []
+        for l in range(lib().pfo_mg_num_levels(self.h)):
+            v = [C.c_int() for _ in range(4)]
+            lib().pfo_mg_level_info(self.h, l, *[C.byref(x) for x in v])
+            out.append(tuple(x.value for x in v))
+        return out
+
+    def setup(self, A4):
+        A4 = [np.ascontiguousarray(a, dtype=np.float64) for a in A4]
+        self._A = A4
+        arr = (_dp * 4)(*[_ptr(a) for a in A4])
+        lib().pfo_mg_setup(self.h, arr)
+
+    def apply(self, b):
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        lib().pfo_mg_apply(self.h, _ptr(b), _ptr(x))
+        return x

@@ -1,0 +1,84 @@
+/* Test infrastructure: CPU restatement ("oracle") of ParFlow's Richards
+ * Newton-Krylov inner loop for box domains.  Only tests/, the package's smoke
+ * check and bench.py's CPU-baseline leg use it, as the checker; the product
+ * path never calls it.
+ *
+ * Layout: interior-only, x fastest, idx = i + nx*(j + ny*k).  Boundary faces
+ * are handled through the per-face boundary-condition tables, which is the
+ * net effect of ParFlow's ghost-frame insertion / correction / reset sequence
+ * (pfsimulator/parflow_lib/nl_function_eval.c:574-610, 979-1233, 2269-2311)
+ * when the permeability ghost frame is zero, as it is for box domains.
+ */
+#ifndef PFORACLE_H
+#define PFORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1 };
+
+typedef struct {
+  int nx, ny, nz;
+  double dx, dy, dz;
+  double gravity, viscosity, density;
+  const double *kx, *ky, *kz;      /* per cell */
+  double porosity, sstorage;
+  const double *alpha, *n;         /* per cell */
+  const double *s_res, *s_sat;     /* per cell */
+  int vg_from_file;                /* Saturation(p>=0): s_sat (1) or s_dif+s_res (0) */
+  const double *z_mult;            /* per layer (nz) */
+  int bc_type[6];                  /* x_lower x_upper y_lower y_upper z_lower z_upper */
+  const double *bc_val[6];         /* face arrays: x:(nz,ny) y:(nz,nx) z:(ny,nx) */
+} pfo_problem;
+
+typedef struct {
+  double residual_tol, step_tol;
+  int max_iter, krylov_dim, max_restarts;
+  int eta_choice;                  /* 0 = constant, 1 = Walker1, 2 = Walker2 */
+  double eta_value, eta_alpha, eta_gamma;
+  int mg_max_levels;
+  int mg_smoother;                 /* 0 = RBGS (symmetric), 1 = WJacobi */
+  double wjacobi_weight;
+} pfo_settings;
+
+typedef struct {
+  int status;                      /* KINSOL return: 1 ok, 0 initial guess ok, else failure */
+  int nni, nli, nfe, nps, npe, nbcf, nbktrk, ncfl;
+  double fnorm;
+} pfo_stats;
+
+/* van Genuchten (problem_saturation.c:221-415, problem_phase_rel_perm.c:567-1361) */
+void pfo_saturation(const pfo_problem *pb, const double *p, double *s, int der);
+void pfo_relperm(const pfo_problem *pb, const double *p, double *kr, int der);
+
+/* residual F(p) at (dt, time-fixed BC tables) (nl_function_eval.c:167-2323) */
+void pfo_residual(const pfo_problem *pb, double dt, const double *p,
+                  const double *p_old, const double *s_old, double *f);
+
+/* Jacobian: full 7 arrays C,W,E,S,N,L,U (symm=0) or the symmetric PC part
+ * stored as C,E,N,U (symm=1) (richards_jacobian_eval.c:217-1420) */
+void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
+                  double *const *J);
+
+/* y = J x for a full 7-array stencil matrix (matvec.c:35-330) */
+void pfo_matvec7(const pfo_problem *pb, double *const *J, const double *x, double *y);
+
+/* MGSemi preconditioner on a symmetric C,E,N,U level-0 matrix */
+typedef struct pfo_mg pfo_mg;
+pfo_mg *pfo_mg_create(const pfo_problem *pb, const pfo_settings *st);
+void pfo_mg_setup(pfo_mg *mg, double *const *A4);
+void pfo_mg_apply(pfo_mg *mg, const double *b, double *x);
+int pfo_mg_num_levels(const pfo_mg *mg);
+void pfo_mg_level_info(const pfo_mg *mg, int l, int *nx, int *ny, int *nz, int *dir);
+void pfo_mg_destroy(pfo_mg *mg);
+
+/* One KINSOL solve (kinsol.c:690-910): p in = initial guess, p out = result. */
+void pfo_newton_solve(const pfo_problem *pb, const pfo_settings *st, double dt,
+                      const double *p_old, const double *s_old, double *p,
+                      pfo_stats *stats);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
