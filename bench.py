@@ -1,0 +1,375 @@
+"""Richards timesteps/s at 13.1M cells (512x512x50 heterogeneous box):
+mixed-precision GPU solver against the plain FP64 GPU form, with the HBM
+roofline of the dominant kernel and the reference CPU build beside it.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+A step is one implicit timestep (a full KINSOL Newton-Krylov solve) of the
+workload, dt = 0.05 h.  Under torchrun (N > 1) every rank solves its own
+replica of the workload (the path does not shard on this build: "replicas
+only"); value = timesteps of all ranks / max wall time over ranks.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Richards steps/s @13M cells: mixed vs FP64 on B200 at ≤1e-8 rel err; HBM %"
+NX, NY, NZ = 512, 512, 50
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+             "--format=csv,noheader,nounits", "-lms", "200"],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# reference CPU arm
+# ---------------------------------------------------------------------------
+REF_SAMPLE = (128, 128, 50)   # 1/16 of the workload's cells, same depth and physics
+
+
+def _ref_binary():
+    for name in ("parflow_omp", "parflow"):
+        p = os.path.join(ROOT, "oracle", "_ref", "bin", name)
+        if os.path.exists(p):
+            return p, name
+    return None, None
+
+
+def run_reference_cpu(nsteps: int, threads: int):
+    """Time the unmodified reference (oracle/_ref) on a bounded sample of the
+    workload; returns (steps/s scaled to the full workload, info dict)."""
+    from parflow_b200 import configs
+
+    exe, name = _ref_binary()
+    sx, sy, sz = REF_SAMPLE
+    prob = configs.hetero(nx=sx, ny=sy, nz=sz, nsteps=nsteps)
+    if exe is None:
+        # the oracle port, one core
+        from oracle.oracle import Oracle
+
+        orc = Oracle(prob)
+        t0 = time.perf_counter()
+        orc.run(nsteps)
+        secs = time.perf_counter() - t0
+        kind, cores = "port", 1
+    else:
+        wd = tempfile.mkdtemp(prefix="pfref_")
+        run = prob.to_reference(wd, "bench", dump_interval=-1)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+        t0 = time.perf_counter()
+        subprocess.run([exe, run], cwd=wd, env=env, check=True,
+                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        wall = time.perf_counter() - t0
+        secs = wall
+        try:
+            txt = open(os.path.join(wd, run + ".out.timing.csv")).read()
+            m = re.search(r"^KINSol,\s*([0-9.eE+-]+)", txt, re.M)
+            if m:
+                secs = float(m.group(1))
+        except OSError:
+            pass
+        shutil.rmtree(wd, ignore_errors=True)
+        kind, cores = "reference", threads if name == "parflow_omp" else 1
+    scale = (sx * sy * sz) / float(NX * NY * NZ)
+    steps_per_s = nsteps / secs * scale
+    info = {"kind": kind, "cores": cores,
+            "sample": f"{sx}x{sy}x{sz} heterogeneous box (1/{int(round(1 / scale))} of the "
+                      f"workload's cells), {nsteps} steps dt=0.05 h, KINSol time "
+                      f"{secs:.2f} s, scaled by cell count to 512x512x50",
+            "binary": name or "oracle port"}
+    return steps_per_s, info
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    total = 0.0
+    per = []
+    k = max(1, args.steps)
+    # each step: one bounded reference sample of 2 timesteps
+    for _ in range(k):
+        v, info = run_reference_cpu(2, threads)
+        per.append(v)
+    value = float(np.median(per))
+    out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "timesteps/s",
+           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "hetero 512x512x50 (13.1M cells), sampled", "dt_h": 0.05},
+           "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": info["cores"],
+                            "kind": info["kind"], "sample": info["sample"]},
+           "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
+                   "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+def gpu_arm(args, rank, world, local_rank):
+    import torch
+
+    from parflow_b200 import configs
+    from parflow_b200.solver import RichardsGPU, pad
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+
+    prob = configs.hetero(nx=NX, ny=NY, nz=NZ, nsteps=args.warmup + args.steps + 2)
+    plan = prob.time_plan()
+    ic = prob.initial_pressure()
+
+    def timed_run(precision):
+        s = RichardsGPU(prob, precision=precision, device=local_rank)
+        s.set_pressure(ic)
+        stream = torch.cuda.ExternalStream(s.stream())
+        stats = []
+        pressures = []
+        for i in range(args.warmup):
+            t, dt = plan[i]
+            s.set_time(t)
+            stats.extend(s.advance(1, dt))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        launches0 = s.kernel_launches()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        clocks = ClockSampler(local_rank)
+        clocks.start()
+        e0.record(stream)
+        for i in range(args.warmup, args.warmup + args.steps):
+            t, dt = plan[i]
+            s.set_time(t)
+            stats.extend(s.advance(1, dt))
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ck = clocks.stop()
+        ms = e0.elapsed_time(e1)
+        launches = s.kernel_launches() - launches0
+        if dist:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+        p_final = s.get_pressure()
+        return s, ms, stats[args.warmup:], launches, ck, p_final
+
+    # plain FP64 form first, then the mixed form on the same steps
+    s64, ms64, st64, _, _, p64 = timed_run("fp64")
+    s64.close()
+    smx, msmx, stmx, launches, clocks, pmx = timed_run("mixed")
+    rel_err = float(np.abs(pmx - p64).max() / np.abs(p64).max())
+
+    # roofline of the dominant kernel (one red/black colour sweep of the
+    # finest multigrid level: the smoother carries the bulk of the V-cycle)
+    kern = {}
+    for name in ("rb_sweep", "matvec", "residual", "jacobian", "vcycle", "mg_setup"):
+        kms, kbytes = smx.time_kernel(name, reps=20)
+        kern[name] = (kms, kbytes)
+    dom = "rb_sweep"
+    dms, dbytes = kern[dom]
+    peak, peak_kind = peaks()
+    achieved = dbytes / (dms * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers: one pfgpu_newton_solve
+    # (p_old, s_old, p in; p out) and one pfgpu_saturation per step
+    e2e_steps = max(3, min(args.steps, 10))
+    shape_p = tuple(n + 2 for n in prob.shape)
+    p_host = torch.from_numpy(pad(ic)).pin_memory()
+    pold_host = torch.empty(shape_p, dtype=torch.float64).pin_memory()
+    s_host = torch.from_numpy(pad(smx.saturation(ic))).pin_memory()
+    import ctypes as C
+
+    from parflow_b200 import lib as L
+
+    lib = smx.lib
+    st = L.Stats()
+    # warm
+    t, dt = plan[0]
+    smx.set_time(t)
+    pold_host.copy_(p_host)
+    rc = lib.pfgpu_newton_solve(smx.h, C.c_void_p(pold_host.data_ptr()),
+                                C.c_void_p(s_host.data_ptr()), dt,
+                                C.c_void_p(p_host.data_ptr()), C.byref(st))
+    L.check(rc, "newton_solve")
+    L.check(lib.pfgpu_saturation(smx.h, C.c_void_p(p_host.data_ptr()), C.c_void_p(s_host.data_ptr())),
+            "saturation")
+    stream = torch.cuda.ExternalStream(smx.stream())
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(1, 1 + e2e_steps):
+        t, dt = plan[i]
+        smx.set_time(t)
+        pold_host.copy_(p_host)
+        rc = lib.pfgpu_newton_solve(smx.h, C.c_void_p(pold_host.data_ptr()),
+                                    C.c_void_p(s_host.data_ptr()), dt,
+                                    C.c_void_p(p_host.data_ptr()), C.byref(st))
+        L.check(rc, "newton_solve")
+        L.check(lib.pfgpu_saturation(smx.h, C.c_void_p(p_host.data_ptr()),
+                                     C.c_void_p(s_host.data_ptr())), "saturation")
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / e2e_steps
+    nbytes = int(np.prod(shape_p)) * 8
+    h2d = 4 * nbytes   # newton: p_old, s_old, p; saturation: p
+    d2h = 2 * nbytes   # newton: p; saturation: s
+    if dist:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        try:
+            v, info = run_reference_cpu(2, os.cpu_count() or 1)
+            cpu = {"value": v, "unit": "timesteps/s", "cores": info["cores"],
+                   "kind": info["kind"], "sample": info["sample"]}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "unit": "timesteps/s", "cores": 0, "kind": "reference",
+                   "sample": f"failed: {e}"}
+
+    if rank == 0:
+        steps_mx = args.steps * world / (msmx * 1e-3)
+        steps_64 = args.steps * world / (ms64 * 1e-3)
+        newton = sum(x.nonlin_iters for x in stmx)
+        out = {
+            "metric": METRIC, "value": steps_mx, "unit": "timesteps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": msmx / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 Newton/Arnoldi, f32 preconditioner + Jacobian storage",
+            "data": "synthetic",
+            "config": {"workload": "hetero 512x512x50 (13.1M cells) mixed precision",
+                       "dt_h": 0.05, "sigma_lnK": 1.5, "corr_cells": [32, 32, 4],
+                       "solver": "KINSOL line search, EtaConstant 1e-5, GMRES(25), MGSemi V(1,1)",
+                       "l2": "inputs larger than L2 (every vector 105 MB, working set > 3 GB)",
+                       "parallelism": f"replicas x{world}"},
+            "fp64_steps_per_s": steps_64,
+            "mixed_speedup_vs_fp64": steps_mx / steps_64,
+            "mixed_vs_fp64_max_rel_pressure_err": rel_err,
+            "newton_iters_per_step": newton / max(1, len(stmx)),
+            "gmres_iters_per_step": sum(x.lin_iters for x in stmx) / max(1, len(stmx)),
+            "cell_newton_updates_per_s": NX * NY * NZ * newton * world / (msmx * 1e-3),
+            "roofline": {"bound": "hbm", "kernel": "red/black smoother colour sweep, finest level (f32)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": peak_kind,
+                         "bytes_per_launch": dbytes, "ms_per_launch": dms},
+            "kernels": {k: {"ms": v[0], "alg_bytes": v[1],
+                            "gbs": (v[1] / (v[0] * 1e-3) / 1e9) if v[1] else None}
+                        for k, v in kern.items()},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "timesteps/s",
+                    "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "api": "pfgpu_newton_solve + pfgpu_saturation with pinned host buffers"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+        }
+        print(json.dumps(out), flush=True)
+    smx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    gpu_arm(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

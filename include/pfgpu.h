@@ -1,0 +1,210 @@
+/*
+ * pfgpu.h -- C ABI of the B200 Richards Newton-Krylov library (libpfgpu.so).
+ *
+ * One handle owns one Richards problem resident in GPU memory: the grid, the
+ * cell fields, the boundary-condition tables and the nonlinear-solver state.
+ * Every function is plain C: pointers, sizes and status codes; no CUDA or
+ * torch type appears in a signature.  All functions return 0 on success,
+ * a positive code for a recoverable condition (e.g. a nonlinear solve that
+ * did not converge, which ParFlow answers by halving dt) and a negative code
+ * for an error; pfgpu_last_error() describes the last failure.
+ *
+ * Cell vectors crossing this ABI use ParFlow's Subvector layout with a
+ * one-cell ghost frame: element (i,j,k), -1 <= i <= nx etc., lives at
+ *   (i+1) + ((j+1) + (k+1)*(ny+2))*(nx+2)
+ * which is SubvectorEltIndex (pfsimulator/parflow_lib/vector.h:133-138) for
+ * a subvector with ix = iy = iz = -1, so ParFlow can pass SubvectorData()
+ * pointers unchanged.  Ghost values are ignored on input and written as 0 on
+ * output.  Pointers may be host or device (including managed) memory; the
+ * library detects which.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths relative to the ParFlow source tree).
+ */
+#ifndef PFGPU_H
+#define PFGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PFGPU_ABI_VERSION 1
+
+/* status codes */
+#define PFGPU_OK 0
+#define PFGPU_NOT_CONVERGED 1      /* recoverable: retry the step with dt/2 */
+#define PFGPU_ERR_ARG (-1)
+#define PFGPU_ERR_CUDA (-2)
+#define PFGPU_ERR_STATE (-3)
+#define PFGPU_ERR_NOMEM (-4)
+
+/* precision of the preconditioner and of the Jacobian matvec inside GMRES;
+ * the residual, Newton update, Arnoldi process and all norms stay FP64 */
+#define PFGPU_PREC_FP64 0
+#define PFGPU_PREC_MIXED 1
+
+/* boundary-condition types, one per box face
+ * (pfsimulator/parflow_lib/bc_pressure.h:97 BC_TYPE_TABLE) */
+#define PFGPU_BC_FLUX 0        /* FluxConst: volume flux per area, + = out of upper faces */
+#define PFGPU_BC_DIRICHLET 1   /* DirEquilRefPatch: pressure head values on the face */
+
+/* faces, ParFlow box patch order */
+#define PFGPU_X_LOWER 0
+#define PFGPU_X_UPPER 1
+#define PFGPU_Y_LOWER 2
+#define PFGPU_Y_UPPER 3
+#define PFGPU_Z_LOWER 4
+#define PFGPU_Z_UPPER 5
+
+/* cell fields for pfgpu_set_field */
+#define PFGPU_FIELD_PERM_X 0
+#define PFGPU_FIELD_PERM_Y 1
+#define PFGPU_FIELD_PERM_Z 2
+#define PFGPU_FIELD_VG_ALPHA 3
+#define PFGPU_FIELD_VG_N 4
+#define PFGPU_FIELD_S_RES 5
+#define PFGPU_FIELD_S_SAT 6
+
+/* eta choice (pfsimulator/parflow_lib/kinsol_nonlin_solver.c:804-850) */
+#define PFGPU_ETA_CONSTANT 0
+#define PFGPU_ETA_WALKER1 1
+#define PFGPU_ETA_WALKER2 2
+
+/* smoothers (pfsimulator/parflow_lib/mg_semi.c:1251) */
+#define PFGPU_SMOOTH_RBGS 0
+#define PFGPU_SMOOTH_WJACOBI 1
+
+typedef struct pfgpu_handle pfgpu_handle;
+
+/* Grid, constant physics and solver keys of one problem.  Scalar fields
+ * (uniform porosity, storage, van Genuchten parameters) live here; spatially
+ * varying ones are uploaded with pfgpu_set_field. */
+typedef struct {
+  int abi_version;                  /* PFGPU_ABI_VERSION */
+  int nx, ny, nz;
+  double dx, dy, dz;
+  double gravity, viscosity, density;
+  double porosity, specific_storage;
+  double vg_alpha, vg_n, s_res, s_sat; /* used where no per-cell field is set */
+  int vg_from_file;                 /* Phase.Saturation.VanGenuchten.File */
+  const double *z_mult;             /* nz dz multipliers, NULL = 1 */
+  int precision;                    /* PFGPU_PREC_* */
+  /* Solver.Nonlinear.* / Solver.Linear.* keys */
+  double residual_tol, step_tol;
+  int max_iter, krylov_dim, max_restarts;
+  int eta_choice;
+  double eta_value, eta_alpha, eta_gamma;
+  int mg_max_levels, mg_smoother;
+  double wjacobi_weight;
+} pfgpu_desc;
+
+/* Counters of one nonlinear solve (the kinsol.log fields,
+ * pfsimulator/parflow_lib/kinsol_nonlin_solver.c:239-264). */
+typedef struct {
+  int kinsol_status;   /* KINSOL return value (1 success, 2 initial guess ok, ...) */
+  int nonlin_iters, lin_iters, fevals, pc_setups, pc_solves;
+  int lin_conv_fails, beta_cond_fails, backtracks;
+  double fnorm;
+} pfgpu_stats;
+
+/* Creates the problem on CUDA device `device`; replaces the instance setup of
+ * KinsolNonlinSolverInitInstanceXtra (pfsimulator/parflow_lib/kinsol_nonlin_solver.c:456-680).
+ * Returns NULL on error (see pfgpu_last_error). */
+pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device);
+
+/* Frees every device allocation of the handle
+ * (KinsolNonlinSolverFreeInstanceXtra, kinsol_nonlin_solver.c:690). */
+void pfgpu_destroy(pfgpu_handle *h);
+
+/* Message for the last failing call on this thread. */
+const char *pfgpu_last_error(void);
+
+/* Uploads a spatially varying cell field (ParFlow layout).  Replaces the
+ * ProblemData fields read by the modules: permeability (subsrf_sim.c:684-810),
+ * per-cell van Genuchten parameters (problem_saturation.c:943-950,
+ * problem_phase_rel_perm.c:1930-1932). */
+int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
+
+/* Sets the boundary condition of one face at the current time: `values`
+ * holds one value per boundary cell, x faces (nz, ny), y faces (nz, nx),
+ * z faces (ny, nx), first index slowest.  Replaces the BCStruct built by
+ * BCPressure (pfsimulator/parflow_lib/problem_bc_pressure.c:60). */
+int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values);
+
+/* Residual F(p) of one implicit step (NlFunctionEval,
+ * pfsimulator/parflow_lib/nl_function_eval.c:167).  p, p_old, s_old, f in
+ * ParFlow layout. */
+int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old,
+                           const double *s_old, double dt, double *f);
+
+/* y = J(p) x with the analytic 7-point Jacobian assembled at p
+ * (KINSolMatVec + RichardsJacobianEval with symm_part = 0,
+ * pfsimulator/parflow_lib/richards_jacobian_eval.c:165, :217; Matvec,
+ * matvec.c:35).  Uses the handle's matvec precision. */
+int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt,
+                          const double *x, double *y);
+
+/* Assembles the preconditioner matrix (PCMatrixType PFSymmetric) at p and
+ * builds the semicoarsening multigrid hierarchy
+ * (KinsolPCInitInstanceXtra, kinsol_pc.c:85; MGSemiInitInstanceXtra,
+ * mg_semi.c:766). */
+int pfgpu_pc_setup(pfgpu_handle *h, const double *p, double dt);
+
+/* z = M^{-1} r: one V-cycle with zero initial guess (KinsolPC,
+ * kinsol_pc.c:58 -> MGSemi, mg_semi.c:93).  r and z may alias. */
+int pfgpu_pc_apply(pfgpu_handle *h, const double *r, double *z);
+
+/* Saturation S(p) (Saturation with CALCFCN, problem_saturation.c:108). */
+int pfgpu_saturation(pfgpu_handle *h, const double *p, double *s);
+
+/* One implicit step: solves F(p) = 0 by inexact Newton-Krylov with line
+ * search, entirely on the GPU (KinsolNonlinSolver -> KINSol,
+ * kinsol_nonlin_solver.c:297, pfsimulator/kinsol/kinsol.c:690).
+ * p: in = initial guess (normally p_old), out = solution.  Returns
+ * PFGPU_OK, or PFGPU_NOT_CONVERGED when KINSOL would fail. */
+int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old,
+                       double dt, double *p, pfgpu_stats *stats);
+
+/* Device-resident time stepping: advances the handle's own pressure state by
+ * nsteps steps of dt with the boundary tables already set, keeping every
+ * vector on the GPU (the step body of AdvanceRichards,
+ * pfsimulator/parflow_lib/solver_richards.c:2965-3406, without output).
+ * stats (may be NULL) receives the per-step counters, nsteps entries. */
+int pfgpu_set_pressure(pfgpu_handle *h, const double *p);
+int pfgpu_get_pressure(pfgpu_handle *h, double *p);
+int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats);
+
+/* Number of multigrid levels and their sizes/coarsening directions
+ * (mg_semi.c:858-923); dims has 4*levels ints (nx, ny, nz, dir). */
+int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);
+
+/* Times one of the library's kernels on its own stream with CUDA events:
+ * `reps` back-to-back launches on the handle's current state (after a solve
+ * or pfgpu_pc_setup), average duration per launch in *ms, and the kernel's
+ * algorithmic HBM bytes per launch (each distinct per-cell array it needs
+ * counted once; uniform fields count zero) in *bytes.
+ * kernel: 0 residual (with its van Genuchten pass), 1 Jacobian + PC matrix
+ * assembly, 2 Jacobian matvec, 3 the fused red/black/red smoother on the
+ * finest level, 4 one multigrid V-cycle (all levels), 5 multigrid setup.
+ * Benchmark support; no counterpart in the reference. */
+#define PFGPU_KERNEL_RESIDUAL 0
+#define PFGPU_KERNEL_JACOBIAN 1
+#define PFGPU_KERNEL_MATVEC 2
+#define PFGPU_KERNEL_RB_SWEEP 3
+#define PFGPU_KERNEL_VCYCLE 4
+#define PFGPU_KERNEL_MG_SETUP 5
+int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double *bytes);
+
+/* CUDA stream the handle launches on (a cudaStream_t as an opaque pointer),
+ * so callers can order their own work. */
+void *pfgpu_stream(pfgpu_handle *h);
+
+/* Number of kernels this handle has launched so far. */
+long long pfgpu_kernel_launches(pfgpu_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PFGPU_H */

@@ -179,15 +179,14 @@ class Oracle:
         """Advance the problem ``nsteps`` timesteps (AdvanceRichards semantics
         without dt halving).  Returns (pressures per step, stats per step)."""
         prob = self.prob
-        nsteps = prob.nsteps if nsteps is None else nsteps
+        plan = prob.time_plan()
+        nsteps = len(plan) if nsteps is None else nsteps
         p = prob.initial_pressure().copy()
-        t = prob.start_time
         out_p, out_s = [], []
-        for _ in range(nsteps):
-            t += prob.dt
+        for t, dt in plan[:nsteps]:
             self.set_time(t)
             s_old = self.saturation(p)
-            p_new, st = self.newton_solve(p, p, s_old, prob.dt)
+            p_new, st = self.newton_solve(p, p, s_old, dt)
             p = p_new
             out_p.append(p.copy())
             out_s.append(st)

@@ -1196,6 +1196,9 @@ void pfo_newton_solve(const pfo_problem *pb, const pfo_settings *st, double dt,
   feval(&kc, uu, fval);
   if (maxabs(fval, N) <= 0.01 * fnormtol)
   {
+    /* KINSol returns before loading its optional outputs, so the reported
+     * counters stay at zero (KS/kinsol.c:726-731, 851-862) */
+    stats->nfe = 0;
     stats->status = 2;
     stats->fnorm = sqrt(dot(fval, fval, N));
     goto out;

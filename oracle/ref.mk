@@ -29,6 +29,9 @@ EXE     := $(REF)/pfsimulator/parflow_exe
 
 CC      ?= gcc
 CXX     ?= g++
+# the OpenMP build needs a toolchain that ships libgomp's spec file
+OMPCC   ?= $(if $(wildcard /usr/bin/gcc),/usr/bin/gcc,$(CC))
+OMPCXX  ?= $(if $(wildcard /usr/bin/g++),/usr/bin/g++,$(CXX))
 OPT     ?= -O2
 INC     := -I$(OUT)/include -I$(AM)/seq -I$(AM)/common -I$(PL) -I$(KS) -I$(CJ)
 CFLAGS  := $(OPT) -fcommon -w $(INC)
@@ -148,31 +151,31 @@ $(OUT)/bin/parflow_hook: $(SEQ_OBJ) $(OUT)/seq/main.o $(OUT)/seq/hooks.o
 OMPDEF := -DPARFLOW_HAVE_OMP -fopenmp
 $(OUT)/omp/pl_%.o: $(PL)/%.c $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) $(OMPDEF) -c $< -o $@
+	$(OMPCC) $(CFLAGS) $(OMPDEF) -c $< -o $@
 $(OUT)/omp/a0_%.o: $(PL)/%.cpp $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=0 -c $< -o $@
+	$(OMPCXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=0 -c $< -o $@
 $(OUT)/omp/a1_%.o: $(PL)/%.cpp $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=1 -c $< -o $@
+	$(OMPCXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=1 -c $< -o $@
 $(OUT)/omp/a2_%.o: $(PL)/%.cpp $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=2 -c $< -o $@
+	$(OMPCXX) $(CFLAGS) $(OMPDEF) -DPF_COMP_UNIT_TYPE=2 -c $< -o $@
 $(OUT)/omp/ks_%.o: $(KS)/%.c $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) $(OMPDEF) -c $< -o $@
+	$(OMPCC) $(CFLAGS) $(OMPDEF) -c $< -o $@
 $(OUT)/omp/am_%.o: $(AM)/common/%.c $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) $(OMPDEF) -c $< -o $@
+	$(OMPCC) $(CFLAGS) $(OMPDEF) -c $< -o $@
 $(OUT)/omp/cjson.o: $(CJ)/cJSON.c $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) -c $< -o $@
+	$(OMPCC) $(CFLAGS) -c $< -o $@
 $(OUT)/omp/main.o: $(EXE)/main.c $(HDRS)
 	@mkdir -p $(dir $@)
-	$(CC) $(CFLAGS) $(OMPDEF) -c $< -o $@
+	$(OMPCC) $(CFLAGS) $(OMPDEF) -c $< -o $@
 
 $(OUT)/bin/parflow_omp: $(OMP_OBJ) $(OUT)/omp/main.o
 	@mkdir -p $(dir $@)
-	$(CXX) -fopenmp -o $@ $^ -lm
+	$(OMPCXX) -fopenmp -o $@ $^ -lm
 
 .PHONY: all seq

@@ -1,0 +1,52 @@
+"""Named small problems used as parity cases (and their golden fixtures).
+
+Each is a scaled-down, seeded instance of a benchmark workload so that the
+reference CPU build and the oracle finish in seconds.
+"""
+
+from __future__ import annotations
+
+from . import configs
+from .problem import BC, BC_DIRICHLET, BC_FLUX, RichardsProblem, SolverSettings
+
+
+def box_small() -> RichardsProblem:
+    """Config-0 physics on 12x10x8, 2 steps."""
+    return configs.box(nx=12, ny=10, nz=8, nsteps=2)
+
+
+def box_odd() -> RichardsProblem:
+    """Odd sizes (ragged multigrid levels), 3 steps, another seed."""
+    return configs.box(nx=17, ny=9, nz=11, nsteps=3, seed=7)
+
+
+def hetero_small() -> RichardsProblem:
+    """Config-2 physics (per-cell van Genuchten files) on 16x16x10, 2 steps."""
+    return configs.hetero(nx=16, ny=16, nz=10, nsteps=2)
+
+
+def walker2_small() -> RichardsProblem:
+    """Default Walker2 forcing term and side Dirichlet faces."""
+    p = configs.box(nx=14, ny=12, nz=9, nsteps=2, seed=11,
+                    solver=SolverSettings(eta_choice="Walker2"))
+    p.bc["x_lower"] = BC(BC_DIRICHLET, (1.5,), ref_patch="z_lower")
+    p.bc["y_upper"] = BC(BC_DIRICHLET, (2.5,), ref_patch="z_lower")
+    return p
+
+
+def hydrostatic() -> RichardsProblem:
+    """Known answer: a box in hydrostatic equilibrium with no-flow faces and a
+    Dirichlet bottom needs zero Newton iterations and keeps its pressure."""
+    p = configs.box(nx=10, ny=8, nz=12, nsteps=2, seed=3)
+    p.bc["z_upper"] = BC(BC_FLUX, (0.0,))
+    return p
+
+
+GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"]
+
+
+def get(name: str) -> RichardsProblem:
+    return globals()[name]()
+
+
+__all__ = ["get", "GOLDEN"] + GOLDEN

@@ -1,0 +1,399 @@
+// Grid vectors, deterministic reductions and the scalar side of GMRES.
+//
+// Reductions: a fixed grid of blocks writes one partial per block; the last
+// block to finish (ticket counter) sums the partials in index order, so every
+// result is bitwise reproducible run to run.  Results stay in device memory.
+// The scalar GMRES steps (modified Gram-Schmidt bookkeeping, Givens QR,
+// back substitution) run in one thread on device-resident scalars and follow
+// pfsimulator/kinsol/iterativ.c:30-286 and spgmr.c:168-450.
+#include "pfgpu_kernels.h"
+
+namespace pfgpu {
+
+static const int RED_THREADS = 256;
+static const int RED_BLOCKS = 592;  // 4 x 148 SMs
+
+int reduce_blocks() { return RED_BLOCKS; }
+
+
+struct OpDot {
+  const double *a, *b;
+  __device__ double operator()(long long i) const { return a[i] * b[i]; }
+  __device__ static double comb(double x, double y) { return x + y; }
+  __device__ static double init() { return 0.0; }
+};
+struct OpMaxAbs {
+  const double *a;
+  __device__ double operator()(long long i) const { return fabs(a[i]); }
+  __device__ static double comb(double x, double y) { return x > y ? x : y; }
+  __device__ static double init() { return 0.0; }
+};
+struct OpStep {  // |s| / (1/1 + |u|)  (KINScSteplength, kinsol.c:1490-1505)
+  const double *s, *u;
+  __device__ double operator()(long long i) const { return fabs(s[i] / (1.0 / 1.0 + fabs(u[i]))); }
+  __device__ static double comb(double x, double y) { return x > y ? x : y; }
+  __device__ static double init() { return 0.0; }
+};
+struct OpStepDiff {  // |a - b| / (1 + |a|)  (KINStop, kinsol.c:1541-1544)
+  const double *a, *b;
+  __device__ double operator()(long long i) const {
+    return fabs((a[i] - b[i]) / (1.0 / 1.0 + fabs(a[i])));
+  }
+  __device__ static double comb(double x, double y) { return x > y ? x : y; }
+  __device__ static double init() { return 0.0; }
+};
+
+template <typename Op>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce(Op op, long long n, double *partial,
+                                                        double *dst, unsigned int *ticket,
+                                                        const double *gate) {
+  __shared__ double sh[RED_THREADS / 32];
+  __shared__ bool last;
+  if (gate && *gate == 0.0) return;  // reduction not needed this time
+  double acc = Op::init();
+  for (long long i = blockIdx.x * (long long)RED_THREADS + threadIdx.x; i < n;
+       i += (long long)gridDim.x * RED_THREADS)
+    acc = Op::comb(acc, op(i));
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc = Op::comb(acc, __shfl_down_sync(0xffffffffu, acc, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double b = sh[0];
+    for (int w = 1; w < RED_THREADS / 32; w++) b = Op::comb(b, sh[w]);
+    partial[blockIdx.x] = b;
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  // last block: ordered final sum
+  __threadfence();
+  double v = Op::init();
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += RED_THREADS) {
+    double pv = ((volatile double *)partial)[i];
+    v = (i == (int)threadIdx.x) ? pv : Op::comb(v, pv);
+  }
+  // fixed-order tree over threads
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = Op::comb(v, __shfl_down_sync(0xffffffffu, v, o));
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double r = sh[0];
+    for (int w = 1; w < RED_THREADS / 32; w++) r = Op::comb(r, sh[w]);
+    *dst = r;
+    *ticket = 0u;
+  }
+}
+
+template <typename Op>
+static void reduce(Op op, long long n, double *dst, ReduceBuf rb, cudaStream_t st,
+                   const double *gate = nullptr) {
+  long long need = (n + RED_THREADS - 1) / RED_THREADS;
+  int blocks = (int)(need < rb.blocks ? need : rb.blocks);
+  if (blocks < 1) blocks = 1;
+  k_reduce<Op><<<blocks, RED_THREADS, 0, st>>>(op, n, rb.partial, dst, rb.ticket, gate);
+}
+
+void launch_dot(const double *a, const double *b, long long n, double *dst, ReduceBuf rb,
+                cudaStream_t st) {
+  OpDot op{a, b};
+  reduce(op, n, dst, rb, st);
+}
+void launch_dot_gated(const double *a, const double *b, long long n, double *dst,
+                      const double *gate, ReduceBuf rb, cudaStream_t st) {
+  OpDot op{a, b};
+  reduce(op, n, dst, rb, st, gate);
+}
+void launch_maxabs(const double *a, long long n, double *dst, ReduceBuf rb, cudaStream_t st) {
+  OpMaxAbs op{a};
+  reduce(op, n, dst, rb, st);
+}
+void launch_steplen(const double *s, const double *u, long long n, double *dst, ReduceBuf rb,
+                    cudaStream_t st) {
+  OpStep op{s, u};
+  reduce(op, n, dst, rb, st);
+}
+void launch_steplen_diff(const double *a, const double *b, long long n, double *dst,
+                         ReduceBuf rb, cudaStream_t st) {
+  OpStepDiff op{a, b};
+  reduce(op, n, dst, rb, st);
+}
+
+// ---- element-wise ---------------------------------------------------------
+__global__ void k_axpy_dev(double *__restrict__ y, const double *__restrict__ x,
+                           const double *__restrict__ s, double sign, long long n) {
+  double a = sign * (*s);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = y[i] + a * x[i];
+}
+__global__ void k_axpby(double *__restrict__ y, const double *__restrict__ x, double a, double b,
+                        long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = (b == 0.0) ? a * x[i] : a * x[i] + b * y[i];
+}
+__global__ void k_xpay(double *__restrict__ z, const double *__restrict__ x, double a,
+                       const double *__restrict__ y, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    z[i] = x[i] + a * y[i];
+}
+__global__ void k_scale_inv_dev(double *__restrict__ x, const double *__restrict__ s,
+                                long long n) {
+  double a = 1.0 / (*s);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void k_scale(double *__restrict__ x, double a, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void k_fill(double *__restrict__ x, double v, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+struct VecList {
+  const double *v[32];
+};
+// xcor = yg[0] V0 + 0, then xcor = yg[k] Vk + xcor (sequential N_VLinearSum order)
+__global__ void k_combine(double *__restrict__ xcor, VecList V, const double *__restrict__ yg,
+                          int kdim, long long n) {
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int k = 0; k < kdim; k++) acc = yg[k] * V.v[k][i] + 1.0 * acc;
+    xcor[i] = acc;
+  }
+}
+
+static inline int grid_for(long long n) {
+  long long b = (n + 255) / 256;
+  return (int)(b < 148 * 16 ? (b < 1 ? 1 : b) : 148 * 16);
+}
+
+void launch_axpy_dev(double *y, const double *x, const double *s, double sign, long long n,
+                     cudaStream_t st) {
+  k_axpy_dev<<<grid_for(n), 256, 0, st>>>(y, x, s, sign, n);
+}
+void launch_axpby(double *y, const double *x, double a, double b, long long n, cudaStream_t st) {
+  k_axpby<<<grid_for(n), 256, 0, st>>>(y, x, a, b, n);
+}
+void launch_xpay(double *z, const double *x, double a, const double *y, long long n,
+                 cudaStream_t st) {
+  k_xpay<<<grid_for(n), 256, 0, st>>>(z, x, a, y, n);
+}
+void launch_scale_inv_dev(double *x, const double *s, long long n, cudaStream_t st) {
+  k_scale_inv_dev<<<grid_for(n), 256, 0, st>>>(x, s, n);
+}
+void launch_scale(double *x, double a, long long n, cudaStream_t st) {
+  k_scale<<<grid_for(n), 256, 0, st>>>(x, a, n);
+}
+void launch_fill(double *x, double v, long long n, cudaStream_t st) {
+  k_fill<<<grid_for(n), 256, 0, st>>>(x, v, n);
+}
+void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
+                    cudaStream_t st) {
+  VecList L;
+  for (int k = 0; k < kdim && k < 32; k++) L.v[k] = V[k];
+  k_combine<<<grid_for(n), 256, 0, st>>>(xcor, L, yg, kdim, n);
+}
+
+// ---- GMRES scalars ----------------------------------------------------------
+// S layout: [0, (lmax+1)*lmax) Hessenberg H(i,j) at i*lmax+j; then givens
+// (2*lmax), yg (lmax+1), then named scalars.
+struct GS {
+  double *H, *giv, *yg, *sc;
+  int lmax;
+  __device__ double &h(int i, int j) { return H[i * lmax + j]; }
+};
+enum { SC_RNORM = 0, SC_ROT, SC_RHO, SC_VKNORM2, SC_NEWNORM2, SC_FLAG, SC_NN2, SC_NP, SC_GATE,
+       SC_COEF, SC_HLL, SC_BETA, SC_QRFAIL };
+
+__device__ GS gs_view(double *S, int lmax) {
+  GS g;
+  g.lmax = lmax;
+  g.H = S;
+  g.giv = S + (lmax + 1) * lmax;
+  g.yg = g.giv + 2 * lmax;
+  g.sc = g.yg + lmax + 1;
+  return g;
+}
+
+__device__ void givens(double t1, double t2, double &c, double &s) {
+  if (t2 == 0.0) {
+    c = 1.0;
+    s = 0.0;
+  } else if (fabs(t2) >= fabs(t1)) {
+    double t3 = t1 / t2;
+    s = -1.0 / sqrt(1.0 + t3 * t3);
+    c = -s * t3;
+  } else {
+    double t3 = t2 / t1;
+    c = 1.0 / sqrt(1.0 + t3 * t3);
+    s = -c * t3;
+  }
+}
+
+__global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
+  GS g = gs_view(S, lmax);
+  double *sc = g.sc;
+  switch (op) {
+    case 0: {  // start: r_norm = sqrt(<V0,V0>) already in SC_RNORM as squared
+      double r = sqrt(sc[SC_RNORM]);
+      sc[SC_RNORM] = r;
+      sc[SC_BETA] = r;
+      sc[SC_ROT] = 1.0;
+      sc[SC_RHO] = r;
+      for (int i = 0; i < (lmax + 1) * lmax; i++) g.H[i] = 0.0;
+      break;
+    }
+    case 1: {  // after GS: H(i, k-1) stored by dots; compute new norm & reorth flag
+      int k = l + 1;
+      double vk_norm = sqrt(sc[SC_VKNORM2]);
+      double new_norm = sqrt(sc[SC_NEWNORM2]);
+      double temp = 1000.0 * vk_norm;
+      sc[SC_FLAG] = ((temp + new_norm) != temp) ? 0.0 : 1.0;
+      sc[SC_NN2] = 0.0;
+      g.h(k, k - 1) = new_norm;
+      break;
+    }
+    case 3: {  // QR update for column l and residual estimate (iterativ.c:205-250)
+      int n = l + 1;
+      if (l == 0) {
+        double t1 = g.h(0, 0), t2 = g.h(1, 0), c, s;
+        givens(t1, t2, c, s);
+        g.giv[0] = c;
+        g.giv[1] = s;
+        g.h(0, 0) = c * t1 - s * t2;
+      } else {
+        int nm1 = n - 1;
+        for (int k = 0; k < nm1; k++) {
+          double t1 = g.h(k, nm1), t2 = g.h(k + 1, nm1);
+          double c = g.giv[2 * k], s = g.giv[2 * k + 1];
+          g.h(k, nm1) = c * t1 - s * t2;
+          g.h(k + 1, nm1) = s * t1 + c * t2;
+        }
+        double t1 = g.h(nm1, nm1), t2 = g.h(n, nm1), c, s;
+        givens(t1, t2, c, s);
+        g.giv[2 * nm1] = c;
+        g.giv[2 * nm1 + 1] = s;
+        g.h(nm1, nm1) = c * t1 - s * t2;
+      }
+      sc[SC_ROT] *= g.giv[2 * l + 1];
+      sc[SC_RHO] = fabs(sc[SC_ROT] * sc[SC_RNORM]);
+      sc[SC_HLL] = g.h(l + 1, l);
+      break;
+    }
+    case 4: {  // QRsol with krydim = l (iterativ.c:253-286)
+      int kd = l;
+      g.yg[0] = sc[SC_RNORM];
+      for (int i = 1; i <= kd; i++) g.yg[i] = 0.0;
+      for (int k = 0; k < kd; k++) {
+        double c = g.giv[2 * k], s = g.giv[2 * k + 1];
+        double t1 = g.yg[k], t2 = g.yg[k + 1];
+        g.yg[k] = c * t1 - s * t2;
+        g.yg[k + 1] = s * t1 + c * t2;
+      }
+      sc[SC_QRFAIL] = 0.0;
+      for (int k = kd - 1; k >= 0; k--) {
+        if (g.h(k, k) == 0.0) {
+          sc[SC_QRFAIL] = 1.0;
+          break;
+        }
+        g.yg[k] /= g.h(k, k);
+        for (int i = 0; i < k; i++) g.yg[i] -= g.yg[k] * g.h(i, k);
+      }
+      break;
+    }
+    case 5: {  // finish reorthogonalisation: corrected new norm (iterativ.c:79-84)
+      int k = l + 1;
+      if (sc[SC_FLAG] != 0.0 && sc[SC_NN2] != 0.0) {
+        double nn = g.h(k, k - 1);
+        double np2 = nn * nn - sc[SC_NN2];
+        g.h(k, k - 1) = (np2 > 0.0) ? sqrt(np2) : 0.0;
+      }
+      sc[SC_HLL] = g.h(k, k - 1);
+      break;
+    }
+  }
+}
+
+// Reorthogonalisation decision for basis vector i against V_k
+// (iterativ.c:68-77): dot result in SC_NP; sets SC_GATE (apply?) and SC_COEF.
+__global__ void k_reorth_decide(double *S, int i, int l, int lmax) {
+  GS g = gs_view(S, lmax);
+  double *sc = g.sc;
+  int k = l + 1;
+  sc[SC_GATE] = 0.0;
+  if (sc[SC_FLAG] == 0.0) return;
+  double new_product = sc[SC_NP];
+  double temp = 1000.0 * g.h(i, k - 1);
+  if ((temp + new_product) == temp) return;
+  g.h(i, k - 1) += new_product;
+  sc[SC_COEF] = -new_product;
+  sc[SC_NN2] += new_product * new_product;
+  sc[SC_GATE] = 1.0;
+}
+
+// y = y + (*coef) * x when *gate != 0
+__global__ void k_axpy_gated(double *__restrict__ y, const double *__restrict__ x,
+                             const double *__restrict__ coef, const double *__restrict__ gate,
+                             long long n) {
+  if (*gate == 0.0) return;
+  double a = *coef;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    y[i] = y[i] + a * x[i];
+}
+
+void launch_gmres_scalar(int op, double *S, int l, int lmax, cudaStream_t st) {
+  k_gmres_scalar<<<1, 1, 0, st>>>(op, S, l, lmax);
+}
+void launch_reorth_decide(double *S, int i, int l, int lmax, cudaStream_t st) {
+  k_reorth_decide<<<1, 1, 0, st>>>(S, i, l, lmax);
+}
+void launch_axpy_gated(double *y, const double *x, const double *coef, const double *gate,
+                       long long n, cudaStream_t st) {
+  k_axpy_gated<<<grid_for(n), 256, 0, st>>>(y, x, coef, gate, n);
+}
+
+// ---- ParFlow layout <-> dense ------------------------------------------------
+__global__ void k_unpad(const double *__restrict__ pad, double *__restrict__ dense, int nx,
+                        int ny, int nz) {
+  long long n = (long long)nx * ny * nz;
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c % nx);
+    long long r = c / nx;
+    int j = (int)(r % ny), k = (int)(r / ny);
+    dense[c] = pad[(i + 1) + (long long)(nx + 2) * ((j + 1) + (long long)(ny + 2) * (k + 1))];
+  }
+}
+__global__ void k_pad(const double *__restrict__ dense, double *__restrict__ pad, int nx, int ny,
+                      int nz) {
+  long long n = (long long)(nx + 2) * (ny + 2) * (nz + 2);
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c % (nx + 2)) - 1;
+    long long r = c / (nx + 2);
+    int j = (int)(r % (ny + 2)) - 1, k = (int)(r / (ny + 2)) - 1;
+    bool in = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
+    pad[c] = in ? dense[i + (long long)nx * (j + (long long)ny * k)] : 0.0;
+  }
+}
+void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st) {
+  k_unpad<<<grid_for((long long)nx * ny * nz), 256, 0, st>>>(pad, dense, nx, ny, nz);
+}
+void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st) {
+  k_pad<<<grid_for((long long)(nx + 2) * (ny + 2) * (nz + 2)), 256, 0, st>>>(dense, pad, nx, ny,
+                                                                             nz);
+}
+
+}  // namespace pfgpu

@@ -1,0 +1,1172 @@
+// libpfgpu: handle, C ABI entry points and the device-resident KINSOL /
+// SPGMR / MGSemi driver.
+//
+// Control flow mirrors the embedded KINSOL of ParFlow (pfsimulator/kinsol/
+// kinsol.c:690-910, kinspgmr.c:344-440, spgmr.c:168-450, iterativ.c:30-286)
+// with every vector and every GMRES scalar in device memory; the host reads
+// back only the few scalars that steer control flow (one small copy per
+// GMRES iteration and per line-search evaluation).  The multigrid V-cycle is
+// a fixed kernel sequence and is replayed from a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "../../include/pfgpu.h"
+#include "pfgpu_kernels.h"
+
+using namespace pfgpu;
+
+static thread_local char g_err[512] = "";
+
+static void set_err(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof(g_err), fmt, ap);
+  va_end(ap);
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess) {                                                            \
+      set_err("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+      return PFGPU_ERR_CUDA;                                                            \
+    }                                                                                   \
+  } while (0)
+
+namespace {
+
+// device scalar slots
+enum {
+  D_F2 = 0,      // <f, f>
+  D_FMAX,        // max |f|
+  D_STEP,        // max |unew - u| / (1 + |unew|)
+  D_P2,          // <p, p>
+  D_PLEN,        // max |p| / (1 + |u|)
+  D_JP2,         // <Jp, Jp>
+  D_FJP,         // <f, Jp>
+  D_U2,          // <u, u>
+  D_COUNT
+};
+
+struct Handle;
+
+template <typename T>
+struct MG {
+  std::vector<MGLevel<T>> L;
+  MGLevel<T> *Ldev = nullptr;  // device copy of the level table (tail kernels)
+  int tail = 0;                // first level run by the single-block tail kernels
+  T *wtmp = nullptr;           // Jacobi temp (finest size)
+  bool fused = false;          // fused red/black/red smoother on grid levels
+};
+
+// Tuning (read once per handle from the environment; all variants compute
+// the same V-cycle):
+//   PFGPU_TAIL_CELLS  levels at or below this many cells run inside the
+//                     single-block tail kernels (default 1024)
+//   PFGPU_FUSED_RBR   1: fused red/black/red smoother kernel, 0: one kernel
+//                     per colour sweep (default 0)
+static long long env_ll(const char *name, long long dflt) {
+  const char *v = getenv(name);
+  return v && *v ? atoll(v) : dflt;
+}
+
+}  // namespace
+
+struct pfgpu_handle {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  pfgpu_desc d;
+  DevProblem P;
+  int nx, ny, nz;
+  long long N, NP;  // interior cells, ParFlow-layout cells
+  bool mixed = false;
+  // fields
+  double *kx = nullptr, *ky = nullptr, *kz = nullptr;
+  double *alpha = nullptr, *vgn = nullptr, *sres = nullptr, *ssat = nullptr, *zmult = nullptr;
+  double *bcv[6] = {nullptr};
+  // state and work vectors (dense interior layout)
+  double *u = nullptr;      // current iterate / handle pressure state
+  double *unew = nullptr, *fval = nullptr, *pp = nullptr, *bb = nullptr;
+  double *p_old = nullptr, *s_old = nullptr;
+  double *kr = nullptr, *dkr = nullptr, *sat = nullptr, *dsat = nullptr;
+  const double *vg_for = nullptr;  // iterate the cached kr/dkr/S/dS belong to
+  double *zface = nullptr;
+  double *xcor = nullptr, *vtemp = nullptr;
+  std::vector<double *> V;
+  double *gs = nullptr;   // GMRES scalars
+  double *dsc = nullptr;  // named device scalars
+  double *hsc = nullptr;  // pinned host mirror of dsc / rho
+  ReduceBuf rb{};
+  double *stage = nullptr;  // ParFlow-layout staging (device)
+  double *stage2 = nullptr;
+  // Jacobian
+  JacOut<double> Jd{};
+  JacOut<float> Jf{};
+  // multigrid
+  MG<double> mgd;
+  MG<float> mgf;
+  int nlev = 0;
+  double *pc_in = nullptr, *pc_out = nullptr;  // FP64 level-0 staging when mixed
+  cudaGraphExec_t vgraph = nullptr;
+  long long graph_nodes = 0;
+  bool pc_ready = false;
+  long long launches = 0;
+  int jac_valid = 0;
+};
+
+// ---------------------------------------------------------------------------
+// helpers
+// ---------------------------------------------------------------------------
+static bool is_device_ptr(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+template <typename T>
+static int dalloc(T **p, long long n) {
+  if (cudaMalloc((void **)p, (size_t)(n > 0 ? n : 1) * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    set_err("cudaMalloc of %lld bytes failed", (long long)(n * sizeof(T)));
+    return PFGPU_ERR_NOMEM;
+  }
+  return 0;
+}
+
+// ParFlow-layout input (host or device) -> dense device array
+static int in_vec(pfgpu_handle *h, const double *src, double *dense) {
+  if (h->vg_for == dense) h->vg_for = nullptr;
+  if (is_device_ptr(src)) {
+    launch_unpad(src, dense, h->nx, h->ny, h->nz, h->st);
+  } else {
+    CK(cudaMemcpyAsync(h->stage, src, h->NP * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_unpad(h->stage, dense, h->nx, h->ny, h->nz, h->st);
+  }
+  h->launches++;
+  return 0;
+}
+
+static int out_vec(pfgpu_handle *h, const double *dense, double *dst) {
+  if (is_device_ptr(dst)) {
+    launch_pad(dense, dst, h->nx, h->ny, h->nz, h->st);
+    h->launches++;
+  } else {
+    launch_pad(dense, h->stage, h->nx, h->ny, h->nz, h->st);
+    h->launches++;
+    CK(cudaMemcpyAsync(dst, h->stage, h->NP * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+  }
+  return 0;
+}
+
+static int read_scalars(pfgpu_handle *h, int first, int count) {
+  CK(cudaMemcpyAsync(h->hsc + first, h->dsc + first, count * sizeof(double),
+                     cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// physics building blocks
+// ---------------------------------------------------------------------------
+// van Genuchten state at u (kr, dkr, S, dS), unless already cached for u
+static void vg_state(pfgpu_handle *h, const double *u, bool reuse) {
+  if (reuse && h->vg_for == u) return;
+  launch_vg_all(h->P, u, h->kr, h->dkr, h->sat, h->dsat, h->st);
+  h->launches++;
+  h->vg_for = u;
+}
+
+static void feval(pfgpu_handle *h, const double *u, double dt, double *f) {
+  vg_state(h, u, false);
+  launch_residual(h->P, u, h->p_old, h->s_old, h->kr, h->sat, dt, f, h->st);
+  h->launches++;
+}
+
+// assemble J (full) and the preconditioner matrix at u (one pass); the VG
+// state of the last residual evaluation is reused when it was taken at u
+static void assemble(pfgpu_handle *h, const double *u, double dt, bool want_J, bool want_M,
+                     bool reuse_vg = false) {
+  vg_state(h, u, reuse_vg);
+  if (h->mixed) {
+    PCOut<float> M{};
+    if (want_M) M = {h->mgf.L[0].a[0], h->mgf.L[0].a[1], h->mgf.L[0].a[2], h->mgf.L[0].a[3]};
+    JacOut<float> J{};
+    if (want_J) J = h->Jf;
+    launch_jacobian<float, float>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
+  } else {
+    PCOut<double> M{};
+    if (want_M) M = {h->mgd.L[0].a[0], h->mgd.L[0].a[1], h->mgd.L[0].a[2], h->mgd.L[0].a[3]};
+    JacOut<double> J{};
+    if (want_J) J = h->Jd;
+    launch_jacobian<double, double>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
+  }
+  h->launches++;
+}
+
+static void matvec(pfgpu_handle *h, const double *x, double *y) {
+  if (h->mixed) {
+    JacIn<float> J{h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
+    launch_matvec7<float>(h->nx, h->ny, h->nz, J, x, y, h->st);
+  } else {
+    JacIn<double> J{h->Jd.c, h->Jd.w, h->Jd.e, h->Jd.s, h->Jd.n, h->Jd.l, h->Jd.u};
+    launch_matvec7<double>(h->nx, h->ny, h->nz, J, x, y, h->st);
+  }
+  h->launches++;
+}
+
+template <typename T>
+static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
+  long long k = 0;
+  const int nl = (int)mg.L.size();
+  for (int l = 0; l < mg.tail && l + 1 < nl; l++) {
+    launch_mg_prolong_weights<T>(mg.L[l], st);
+    launch_mg_coarse_op<T>(mg.L[l], mg.L[l + 1], st);
+    k += 2;
+  }
+  if (mg.tail < nl - 1) {
+    launch_setup_tail<T>(mg.Ldev, mg.tail, nl, st);
+    k++;
+  }
+  return k;
+}
+
+// One V-cycle with zero initial guess on level-0 (b -> x)
+// (pfsimulator/parflow_lib/mg_semi.c:93-432 with MaxIter 1)
+// Levels below mg.tail use one grid-wide kernel per phase; levels mg.tail ..
+// nl-1 (a few thousand cells each) run inside one single-block kernel.
+template <typename T>
+static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
+  long long k = 0;
+  const int nl = (int)mg.L.size();
+  const int sk = smoother == 1 ? 2 : 3;
+  const int first = mg.tail;
+  const bool fused = smoother == 0 && mg.fused;
+  for (int l = 0; l < first; l++) {
+    MGLevel<T> &Ll = mg.L[l];
+    if (fused) {
+      launch_rbr_fused<T>(Ll, Ll.x, Ll.x, Ll.b, 1, st);  // zero guess: xin unused
+      k++;
+    } else {
+      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st);
+      k += sk;
+    }
+    launch_mg_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st);
+    launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st);
+    k += 2;
+  }
+  // levels first .. nl-1, coarse solve (RedBlackGSPoint, mg_semi.c:1276) included
+  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, st);
+  k++;
+  for (int l = first - 1; l >= 0; l--) {
+    MGLevel<T> &Ll = mg.L[l];
+    const MGLevel<T> &C = mg.L[l + 1];
+    const T *ec = (fused && l + 1 < first) ? C.x2 : C.x;  // where level l+1's result lives
+    launch_mg_prolong_add<T>(Ll, C, ec, Ll.x, st);
+    if (fused) {
+      launch_rbr_fused<T>(Ll, Ll.x, Ll.x2, Ll.b, 0, st);
+      k += 2;
+    } else {
+      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st);
+      k += 1 + sk;
+    }
+  }
+  return k;
+}
+
+// buffer holding the level-0 result of a V-cycle
+template <typename T>
+static T *vcycle_out(MG<T> &mg, int smoother) {
+  return (smoother == 0 && mg.fused && mg.tail > 0) ? mg.L[0].x2 : mg.L[0].x;
+}
+
+static long long vcycle_launch(pfgpu_handle *h) {
+  if (h->mixed) return vcycle_T<float>(h->mgf, h->d.mg_smoother, h->d.wjacobi_weight, h->st);
+  return vcycle_T<double>(h->mgd, h->d.mg_smoother, h->d.wjacobi_weight, h->st);
+}
+
+static int build_vgraph(pfgpu_handle *h) {
+  cudaGraph_t g;
+  CK(cudaStreamBeginCapture(h->st, cudaStreamCaptureModeThreadLocal));
+  long long k = vcycle_launch(h);
+  CK(cudaStreamEndCapture(h->st, &g));
+  CK(cudaGraphInstantiate(&h->vgraph, g, 0));
+  CK(cudaGraphDestroy(g));
+  h->graph_nodes = k;
+  return 0;
+}
+
+// z = M^{-1} r (dense FP64 device vectors; r and z may alias)
+static int pc_apply_dense(pfgpu_handle *h, const double *r, double *z) {
+  if (h->mixed) {
+    launch_convert<double, float>(r, h->mgf.L[0].b, h->N, h->st);
+  } else {
+    CK(cudaMemcpyAsync(h->mgd.L[0].b, r, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  }
+  CK(cudaGraphLaunch(h->vgraph, h->st));
+  h->launches += h->graph_nodes + (h->mixed ? 2 : 0);
+  if (h->mixed) {
+    launch_convert<float, double>(vcycle_out(h->mgf, h->d.mg_smoother), z, h->N, h->st);
+  } else {
+    CK(cudaMemcpyAsync(z, vcycle_out(h->mgd, h->d.mg_smoother), h->N * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->st));
+  }
+  return 0;
+}
+
+static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool also_J,
+                           bool reuse_vg = false) {
+  assemble(h, u, dt, also_J, true, reuse_vg);
+  if (h->mixed)
+    h->launches += mg_setup_T<float>(h->mgf, h->st);
+  else
+    h->launches += mg_setup_T<double>(h->mgd, h->st);
+  if (also_J) h->jac_valid = 1;
+  h->pc_ready = true;
+}
+
+// ---------------------------------------------------------------------------
+// SPGMR (pfsimulator/kinsol/spgmr.c:168-450), x0 = 0, right preconditioning,
+// modified Gram-Schmidt.  Returns 0 success, 1 residual reduced, 2 failure,
+// 6 QR failure; J is assembled at the first matvec if not current.
+// ---------------------------------------------------------------------------
+static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, const double *u,
+                 double dt, pfgpu_stats *stats, int *status) {
+  const long long N = h->N;
+  const int lmax = h->d.krylov_dim;
+  double *S = h->gs;
+  double *sc = S + gs_sc_offset(lmax);
+  double *H = S;
+  auto Hp = [&](int i, int j) { return H + (long long)i * lmax + j; };
+  int krydim = 0, converged = 0;
+  double rho = 0.0, r_norm;
+
+  *status = 0;
+  launch_fill(x, 0.0, N, h->st);
+  CK(cudaMemcpyAsync(h->V[0], b, N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  launch_dot(h->V[0], h->V[0], N, sc + SCI_RNORM, h->rb, h->st);
+  launch_gmres_scalar(GM_START, S, 0, lmax, h->st);
+  h->launches += 3;
+  CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_RNORM, sizeof(double), cudaMemcpyDeviceToHost,
+                     h->st));
+  CK(cudaStreamSynchronize(h->st));
+  r_norm = h->hsc[D_COUNT];
+  const double beta = r_norm;
+  if (r_norm <= delta) return 0;
+
+  for (int ntries = 0; ntries <= h->d.max_restarts; ntries++) {
+    if (ntries > 0) {
+      launch_gmres_scalar(GM_START, S, 0, lmax, h->st);  // re-zero H, keep r_norm squared?
+      h->launches++;
+    }
+    // V0 *= 1 / r_norm
+    launch_scale(h->V[0], 1.0 / r_norm, N, h->st);
+    h->launches++;
+    int l;
+    for (l = 0; l < lmax; l++) {
+      stats->lin_iters++;
+      krydim = l + 1;
+      CK(cudaMemcpyAsync(h->vtemp, h->V[l], N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+      if (pc_apply_dense(h, h->vtemp, h->vtemp)) return PFGPU_ERR_CUDA;
+      stats->pc_solves++;
+      if (!h->jac_valid) {
+        assemble(h, u, dt, true, false, true);
+        h->jac_valid = 1;
+      }
+      matvec(h, h->vtemp, h->V[l + 1]);
+      // ModifiedGS (iterativ.c:30-86)
+      const int k = l + 1;
+      launch_dot(h->V[k], h->V[k], N, sc + SCI_VKNORM2, h->rb, h->st);
+      h->launches++;
+      for (int i = 0; i < k; i++) {
+        launch_dot(h->V[i], h->V[k], N, Hp(i, k - 1), h->rb, h->st);
+        launch_axpy_dev(h->V[k], h->V[i], Hp(i, k - 1), -1.0, N, h->st);
+        h->launches += 2;
+      }
+      launch_dot(h->V[k], h->V[k], N, sc + SCI_NEWNORM2, h->rb, h->st);
+      launch_gmres_scalar(GM_AFTER_GS, S, l, lmax, h->st);
+      h->launches += 2;
+      for (int i = 0; i < k; i++) {
+        launch_dot_gated(h->V[i], h->V[k], N, sc + SCI_NP, sc + SCI_FLAG, h->rb, h->st);
+        launch_reorth_decide(S, i, l, lmax, h->st);
+        launch_axpy_gated(h->V[k], h->V[i], sc + SCI_COEF, sc + SCI_GATE, N, h->st);
+        h->launches += 3;
+      }
+      launch_gmres_scalar(GM_REORTH_DONE, S, l, lmax, h->st);
+      launch_gmres_scalar(GM_QR, S, l, lmax, h->st);
+      h->launches += 2;
+      CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_RHO, sizeof(double), cudaMemcpyDeviceToHost,
+                         h->st));
+      CK(cudaStreamSynchronize(h->st));
+      rho = h->hsc[D_COUNT];
+      if (rho <= delta) {
+        converged = 1;
+        break;
+      }
+      launch_scale_inv_dev(h->V[l + 1], Hp(l + 1, l), N, h->st);
+      h->launches++;
+    }
+    // QRsol and xcor = V y
+    launch_gmres_scalar(GM_QRSOL, S, krydim, lmax, h->st);
+    launch_combine(h->xcor, h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st);
+    h->launches += 2;
+    CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_QRFAIL, sizeof(double),
+                       cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    if (h->hsc[D_COUNT] != 0.0) {
+      *status = 6;
+      return 0;
+    }
+    if (converged) {
+      if (pc_apply_dense(h, h->xcor, h->xcor)) return PFGPU_ERR_CUDA;
+      stats->pc_solves++;
+      launch_xpay(x, x, 1.0, h->xcor, N, h->st);
+      h->launches++;
+      *status = 0;
+      return 0;
+    }
+    if (ntries == h->d.max_restarts) break;
+    // restart: not used by the configurations here (MaxRestarts 0)
+    set_err("GMRES restarts are not supported by this build");
+    return PFGPU_ERR_ARG;
+  }
+  if (rho < beta) {
+    if (pc_apply_dense(h, h->xcor, h->xcor)) return PFGPU_ERR_CUDA;
+    stats->pc_solves++;
+    launch_xpay(x, x, 1.0, h->xcor, N, h->st);
+    h->launches++;
+    *status = 1;
+  } else {
+    *status = 2;
+  }
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// KINSol with LineSearch (pfsimulator/kinsol/kinsol.c:363-910, 1054-1589).
+// u (dense, device) holds the initial guess on entry and the result on exit.
+// ---------------------------------------------------------------------------
+static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
+  const long long N = h->N;
+  const pfgpu_desc &d = h->d;
+  const double uround = DBL_EPSILON;
+  double fnormtol = d.residual_tol, scsteptol = d.step_tol;
+  if (scsteptol <= 0.0) scsteptol = pow(uround, 2.0 / 3.0);
+  if (fnormtol <= 0.0) fnormtol = pow(uround, 1.0 / 3.0);
+  const int mxiter = d.max_iter > 0 ? d.max_iter : 200;
+  int etaflag = d.eta_choice;
+  double ealpha = 0.0, egamma = 0.0;
+  if (etaflag == 1) ealpha = (1.0 + sqrt(5.0)) / 2.0;
+  if (etaflag == 2) {
+    ealpha = d.eta_alpha;
+    egamma = d.eta_gamma;
+    if (ealpha <= 1.0 || ealpha > 2.0) ealpha = 2.0;
+    if (egamma <= 0.0 || egamma > 1.0) egamma = 0.9;
+  }
+  double eta = (etaflag == 0) ? d.eta_value : 0.5;
+  if (eta <= 0.0 || eta > 1.0) eta = 0.1;
+  const bool callForcingTerm = (etaflag != 0);
+  const double epsmin = 0.01 * fnormtol;
+  memset(stats, 0, sizeof(*stats));
+  double *u = h->u;
+  double *unew = h->unew;
+  double *dsc = h->dsc, *hsc = h->hsc;
+  h->vg_for = nullptr;
+
+  // mxnewtstep = 1000 ||u|| (KINSolInit, kinsol.c:540-545)
+  launch_dot(u, u, N, dsc + D_U2, h->rb, h->st);
+  // KINInitialStop
+  feval(h, u, dt, h->fval);
+  stats->fevals++;
+  launch_maxabs(h->fval, N, dsc + D_FMAX, h->rb, h->st);
+  launch_dot(h->fval, h->fval, N, dsc + D_F2, h->rb, h->st);
+  h->launches += 3;
+  if (read_scalars(h, 0, D_COUNT)) return PFGPU_ERR_CUDA;
+  double mxnewtstep = 1000.0 * sqrt(hsc[D_U2]);
+  if (mxnewtstep < 1.0) mxnewtstep = 1.0;
+  if (hsc[D_FMAX] <= 0.01 * fnormtol) {
+    // KINSol returns before loading its optional outputs: counters stay zero
+    // (pfsimulator/kinsol/kinsol.c:726-731, 851-862)
+    stats->fevals = 0;
+    stats->kinsol_status = 2;
+    stats->fnorm = sqrt(hsc[D_F2]);
+    return PFGPU_OK;
+  }
+  double fnorm = sqrt(hsc[D_F2]);
+  double f1norm = 0.5 * fnorm * fnorm;
+  int ret = 0, ncscmx = 0;
+
+  for (int guard = 0; guard < 100000; guard++) {
+    stats->nonlin_iters++;
+    double eps = (eta + uround) * fnorm;
+    if (eps < epsmin) eps = epsmin;
+    // preconditioner setup every iteration (msbpre = 1); J at the same u
+    h->jac_valid = 0;
+    pc_setup_dense(h, u, dt, true, true);
+    stats->pc_setups++;
+    launch_axpby(h->bb, h->fval, -1.0, 0.0, N, h->st);
+    h->launches++;
+    int sstat = 0;
+    int rc = spgmr(h, h->pp, h->bb, eps, u, dt, stats, &sstat);
+    if (rc) return rc;
+    if (sstat != 0 && sstat != 1) {
+      stats->lin_conv_fails++;
+      ret = 8;
+      break;
+    }
+    if (!h->jac_valid) {
+      assemble(h, u, dt, true, false, true);
+      h->jac_valid = 1;
+    }
+    // sJpnorm, sfdotJp (kinspgmr.c:422-431) and line-search inputs
+    matvec(h, h->pp, h->bb);
+    launch_dot(h->bb, h->bb, N, dsc + D_JP2, h->rb, h->st);
+    launch_dot(h->fval, h->bb, N, dsc + D_FJP, h->rb, h->st);
+    launch_dot(h->pp, h->pp, N, dsc + D_P2, h->rb, h->st);
+    launch_steplen(h->pp, u, N, dsc + D_PLEN, h->rb, h->st);
+    h->launches += 4;
+    if (read_scalars(h, 0, D_COUNT)) return PFGPU_ERR_CUDA;
+    double sJpnorm = sqrt(hsc[D_JP2]);
+    double sfdotJp = hsc[D_FJP];
+
+    // KINLineSearch (kinsol.c:1228-1420)
+    int globalret = 0, maxStepTaken = 0;
+    double fnormp = 0.0, f1normp = 0.0, fmax = 0.0, steplen_new = 0.0;
+    double pnorm = sqrt(hsc[D_P2]);
+    double ratio = 1.0;
+    const double alpha = 0.0001, beta = 0.9;
+    if (pnorm > mxnewtstep) {
+      ratio = mxnewtstep / pnorm;
+      launch_scale(h->pp, ratio, N, h->st);
+      launch_steplen(h->pp, u, N, dsc + D_PLEN, h->rb, h->st);
+      h->launches += 2;
+      if (read_scalars(h, D_PLEN, 1)) return PFGPU_ERR_CUDA;
+      pnorm = mxnewtstep;
+    }
+    const double stepl = pnorm;
+    const double slpi = sfdotJp * ratio;
+    const double rlength = hsc[D_PLEN];
+    const double rlmin = scsteptol / rlength;
+    double rl = 1.0, rlprev = 0.0, alpha_cond, beta_cond;
+    const int nfesav = stats->fevals;
+    auto try_step = [&](double lam) -> int {
+      if (lam == 0.0) {  // N_VScale(ONE, uu, unew)
+        if (cudaMemcpyAsync(unew, u, N * sizeof(double), cudaMemcpyDeviceToDevice, h->st) !=
+            cudaSuccess)
+          return PFGPU_ERR_CUDA;
+      } else {
+        launch_xpay(unew, u, lam, h->pp, N, h->st);
+      }
+      feval(h, unew, dt, h->fval);
+      stats->fevals++;
+      launch_dot(h->fval, h->fval, N, dsc + D_F2, h->rb, h->st);
+      launch_maxabs(h->fval, N, dsc + D_FMAX, h->rb, h->st);
+      launch_steplen_diff(unew, u, N, dsc + D_STEP, h->rb, h->st);
+      h->launches += 4;
+      if (read_scalars(h, 0, 3)) return PFGPU_ERR_CUDA;
+      fnormp = sqrt(hsc[D_F2]);
+      f1normp = 0.5 * fnormp * fnormp;
+      fmax = hsc[D_FMAX];
+      steplen_new = hsc[D_STEP];
+      return 0;
+    };
+    for (int it = 0;; it++) {
+      if (it > 1000) {
+        set_err("line search exceeded its iteration bound");
+        return PFGPU_ERR_STATE;
+      }
+      if (try_step(rl)) return PFGPU_ERR_CUDA;
+      alpha_cond = f1norm + alpha * slpi * rl;
+      if (f1normp <= alpha_cond) break;
+      if (rl < rlmin) {
+        // unew = u, re-evaluate and return 1
+        if (try_step(0.0)) return PFGPU_ERR_CUDA;
+        stats->backtracks = stats->fevals - nfesav - 1;
+        globalret = 1;
+        goto ls_done;
+      }
+      {
+        double rltmp = -slpi / (2.0 * (f1normp - f1norm - slpi));
+        if (rltmp > 0.5 * rl) rltmp = 0.5 * rl;
+        rlprev = rl;
+        double pt1trl = 0.1 * rl;
+        rl = (pt1trl > rltmp) ? pt1trl : rltmp;
+      }
+    }
+    beta_cond = f1norm + beta * slpi * rl;
+    if (f1normp < beta_cond) {
+      // (rl == 1 && pnorm < stepl) never holds without constraints
+      if (rl < 1.0 || ((rl > 1.0) && (f1normp > alpha_cond))) {
+        double rllo = (rl < rlprev) ? rl : rlprev;
+        double rldiff = fabs(rlprev - rl);
+        int it = 0;
+        do {
+          if (++it > 1000) {
+            set_err("line search refinement exceeded its iteration bound");
+            return PFGPU_ERR_STATE;
+          }
+          double rlincr = 0.5 * rldiff;
+          rl = rllo + rlincr;
+          if (try_step(rl)) return PFGPU_ERR_CUDA;
+          alpha_cond = f1norm + alpha * slpi * rl;
+          beta_cond = f1norm + beta * slpi * rl;
+          if (f1normp > alpha_cond)
+            rldiff = rlincr;
+          else if (f1normp < beta_cond) {
+            rllo = rl;
+            rldiff = rldiff - rlincr;
+          }
+        } while (f1normp > alpha_cond || ((f1normp < beta_cond) && (rldiff > rlmin)));
+        if (f1normp < beta_cond) {
+          if (try_step(rllo)) return PFGPU_ERR_CUDA;
+          stats->beta_cond_fails++;
+        }
+      }
+    }
+    stats->backtracks = stats->fevals - nfesav - 1;
+    sfdotJp = sfdotJp * rl * ratio;
+    sJpnorm = sJpnorm * rl * ratio;
+    if (rl * pnorm > 0.99 * mxnewtstep) maxStepTaken = 1;
+    (void)stepl;
+  ls_done:
+    if (stats->beta_cond_fails > 10) {
+      ret = 7;
+      break;
+    }
+    // KINForcingTerm (kinsol.c:1054-1090)
+    if (callForcingTerm) {
+      double eta_max = 0.9, eta_min = 0.0001, eta_safe = 0.5;
+      if (etaflag == 1) {
+        double linmodel_norm = sqrt(fnorm * fnorm + 2.0 * sfdotJp + sJpnorm * sJpnorm);
+        eta_safe = pow(eta, ealpha);
+        eta = fabs(fnormp - linmodel_norm) / fnorm;
+      }
+      if (etaflag == 2) {
+        eta_safe = egamma * pow(eta, ealpha);
+        eta = egamma * pow(fnormp / fnorm, ealpha);
+      }
+      if (eta_safe < 0.1) eta_safe = 0.0;
+      if (eta < eta_safe) eta = eta_safe;
+      if (eta < eta_min) eta = eta_min;
+      if (eta > eta_max) eta = eta_max;
+    }
+    fnorm = fnormp;
+    // KINStop (kinsol.c:1507-1589); the preconditioner is always current
+    int sret = 0;
+    if (globalret == 1)
+      sret = 3;
+    else if (fmax <= fnormtol)
+      sret = 1;
+    else if (steplen_new <= scsteptol)
+      sret = 2;
+    else if (stats->nonlin_iters >= mxiter)
+      sret = 4;
+    else {
+      ncscmx = maxStepTaken ? ncscmx + 1 : 0;
+      if (ncscmx == 5) sret = 5;
+    }
+    // u <- unew (swap)
+    double *t = h->u;
+    h->u = h->unew;
+    h->unew = t;
+    u = h->u;
+    unew = h->unew;
+    f1norm = f1normp;
+    if (sret != 0) {
+      ret = sret;
+      break;
+    }
+  }
+  stats->kinsol_status = ret;
+  stats->fnorm = fnorm;
+  return (ret == 1 || ret == 2) ? PFGPU_OK : PFGPU_NOT_CONVERGED;
+}
+
+// ---------------------------------------------------------------------------
+// allocation
+// ---------------------------------------------------------------------------
+template <typename T>
+static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
+  double DX = h->d.dx, DY = h->d.dy, DZ = h->d.dz;
+  int NX = h->nx, NY = h->ny, NZ = h->nz;
+  const int minN = 2;
+  int max_levels = h->d.mg_max_levels > 0 ? h->d.mg_max_levels : 100;
+  std::vector<int> dirs;
+  // coarsening directions (mg_semi.c:858-923)
+  for (int l = 0; l < max_levels - 1; l++) {
+    double ms = DX + DY + DZ;
+    int dd = -1;
+    if ((NX >= minN) && (DX < ms)) { ms = DX; dd = 0; }
+    if ((NY >= minN) && (DY < ms)) { ms = DY; dd = 1; }
+    if ((NZ >= minN) && (DZ < ms)) { ms = DZ; dd = 2; }
+    if (dd == -1) break;
+    if (dd == 0) { DX *= 2; NX = (NX + 1) / 2; }
+    if (dd == 1) { DY *= 2; NY = (NY + 1) / 2; }
+    if (dd == 2) { DZ *= 2; NZ = (NZ + 1) / 2; }
+    dirs.push_back(dd);
+  }
+  int nl = (int)dirs.size() + 1;
+  mg.L.resize(nl);
+  int nx = h->nx, ny = h->ny, nz = h->nz;
+  for (int l = 0; l < nl; l++) {
+    MGLevel<T> &L = mg.L[l];
+    L.nx = nx; L.ny = ny; L.nz = nz;
+    L.n = (long long)nx * ny * nz;
+    L.dir = l < nl - 1 ? dirs[l] : -1;
+    for (int s = 0; s < 4; s++)
+      if (dalloc(&L.a[s], L.n)) return PFGPU_ERR_NOMEM;
+    if (dalloc(&L.x, L.n) || dalloc(&L.b, L.n) || dalloc(&L.t, L.n)) return PFGPU_ERR_NOMEM;
+    if (l < nl - 1) {
+      if (dalloc(&L.p1, L.n) || dalloc(&L.p2, L.n)) return PFGPU_ERR_NOMEM;
+      CK(cudaMemset(L.p1, 0, L.n * sizeof(T)));
+      CK(cudaMemset(L.p2, 0, L.n * sizeof(T)));
+    }
+    CK(cudaMemset(L.x, 0, L.n * sizeof(T)));
+    if (L.dir == 0) nx = (nx + 1) / 2;
+    if (L.dir == 1) ny = (ny + 1) / 2;
+    if (L.dir == 2) nz = (nz + 1) / 2;
+  }
+  if (dalloc(&mg.wtmp, mg.L[0].n)) return PFGPU_ERR_NOMEM;
+  // first level small enough for the single-block tail kernels
+  mg.tail = nl - 1;
+  mg.fused = env_ll("PFGPU_FUSED_RBR", 0) != 0;
+  const long long tail_cells = env_ll("PFGPU_TAIL_CELLS", 1024);
+  for (int l = 0; l < nl; l++)
+    if (mg.L[l].n <= tail_cells) {
+      mg.tail = l;
+      break;
+    }
+  for (int l = 0; l < mg.tail; l++) {
+    if (dalloc(&mg.L[l].x2, mg.L[l].n)) return PFGPU_ERR_NOMEM;
+    CK(cudaMemset(mg.L[l].x2, 0, mg.L[l].n * sizeof(T)));
+  }
+  CK(cudaMalloc((void **)&mg.Ldev, nl * sizeof(MGLevel<T>)));
+  CK(cudaMemcpy(mg.Ldev, mg.L.data(), nl * sizeof(MGLevel<T>), cudaMemcpyHostToDevice));
+  h->nlev = nl;
+  return 0;
+}
+
+template <typename T>
+static void free_mg(MG<T> &mg) {
+  for (auto &L : mg.L) {
+    for (int s = 0; s < 4; s++) cudaFree(L.a[s]);
+    cudaFree(L.x); cudaFree(L.b); cudaFree(L.t); cudaFree(L.p1); cudaFree(L.p2);
+    cudaFree(L.x2);
+  }
+  cudaFree(mg.wtmp);
+  cudaFree(mg.Ldev);
+  mg.L.clear();
+}
+
+static int create_impl(pfgpu_handle *h) {
+  const pfgpu_desc &d = h->d;
+  const long long N = h->N;
+  CK(cudaSetDevice(h->device));
+  CK(mg_prepare_kernels());
+  CK(cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking));
+  double **vecs[] = {&h->kx, &h->u, &h->unew, &h->fval, &h->pp, &h->bb, &h->p_old,
+                     &h->s_old, &h->kr, &h->dkr, &h->sat, &h->dsat, &h->xcor, &h->vtemp};
+  for (double **v : vecs)
+    if (dalloc(v, N)) return PFGPU_ERR_NOMEM;
+  h->ky = h->kx;
+  h->kz = h->kx;
+  if (dalloc(&h->zmult, h->nz)) return PFGPU_ERR_NOMEM;
+  std::vector<double> zm(h->nz, 1.0);
+  if (d.z_mult)
+    for (int k = 0; k < h->nz; k++) zm[k] = d.z_mult[k];
+  CK(cudaMemcpy(h->zmult, zm.data(), h->nz * sizeof(double), cudaMemcpyHostToDevice));
+  // per z face constants: 1/(dz mean(z_k, z_k+1)), z_k/(z_k+z_k+1), z_k+1/(z_k+z_k+1)
+  std::vector<double> zf(3 * (size_t)h->nz, 0.0);
+  for (int k = 0; k + 1 < h->nz; k++) {
+    double za = zm[k], zb = zm[k + 1];
+    zf[3 * k] = 1.0 / (d.dz * (0.5 * (za + zb)));
+    zf[3 * k + 1] = za / (za + zb);
+    zf[3 * k + 2] = zb / (za + zb);
+  }
+  if (dalloc(&h->zface, 3 * h->nz)) return PFGPU_ERR_NOMEM;
+  CK(cudaMemcpy(h->zface, zf.data(), zf.size() * sizeof(double), cudaMemcpyHostToDevice));
+  for (int f = 0; f < 6; f++) {
+    long long fs = f < 2 ? (long long)h->nz * h->ny : f < 4 ? (long long)h->nz * h->nx
+                                                           : (long long)h->ny * h->nx;
+    if (dalloc(&h->bcv[f], fs)) return PFGPU_ERR_NOMEM;
+    CK(cudaMemset(h->bcv[f], 0, fs * sizeof(double)));
+  }
+  h->V.resize(d.krylov_dim + 1);
+  for (auto &v : h->V)
+    if (dalloc(&v, N)) return PFGPU_ERR_NOMEM;
+  if (dalloc(&h->gs, gs_size(d.krylov_dim)) || dalloc(&h->dsc, 64) ||
+      dalloc(&h->stage, h->NP) || dalloc(&h->rb.partial, reduce_blocks()))
+    return PFGPU_ERR_NOMEM;
+  CK(cudaMemset(h->gs, 0, gs_size(d.krylov_dim) * sizeof(double)));
+  CK(cudaMalloc((void **)&h->rb.ticket, sizeof(unsigned int)));
+  CK(cudaMemset(h->rb.ticket, 0, sizeof(unsigned int)));
+  h->rb.blocks = reduce_blocks();
+  CK(cudaMallocHost((void **)&h->hsc, 64 * sizeof(double)));
+  // Jacobian storage
+  if (h->mixed) {
+    float **J[] = {&h->Jf.c, &h->Jf.w, &h->Jf.e, &h->Jf.s, &h->Jf.n, &h->Jf.l, &h->Jf.u};
+    for (float **a : J)
+      if (dalloc(a, N)) return PFGPU_ERR_NOMEM;
+    if (alloc_mg<float>(h, h->mgf)) return PFGPU_ERR_NOMEM;
+  } else {
+    double **J[] = {&h->Jd.c, &h->Jd.w, &h->Jd.e, &h->Jd.s, &h->Jd.n, &h->Jd.l, &h->Jd.u};
+    for (double **a : J)
+      if (dalloc(a, N)) return PFGPU_ERR_NOMEM;
+    if (alloc_mg<double>(h, h->mgd)) return PFGPU_ERR_NOMEM;
+  }
+  CK(cudaMemsetAsync(h->u, 0, N * sizeof(double), h->st));
+  // device problem
+  DevProblem &P = h->P;
+  memset(&P, 0, sizeof(P));
+  P.nx = h->nx; P.ny = h->ny; P.nz = h->nz; P.n = N;
+  P.dx = d.dx; P.dy = d.dy; P.dz = d.dz;
+  P.gravity = d.gravity; P.viscosity = d.viscosity; P.density = d.density;
+  P.porosity = d.porosity; P.sstorage = d.specific_storage;
+  P.alpha0 = d.vg_alpha; P.vgn0 = d.vg_n; P.sres0 = d.s_res; P.ssat0 = d.s_sat;
+  P.vg_from_file = d.vg_from_file;
+  P.kx = h->kx; P.ky = h->ky; P.kz = h->kz;
+  P.zmult = h->zmult;
+  P.zface = h->zface;
+  P.inv_dx = 1.0 / d.dx;
+  P.inv_dy = 1.0 / d.dy;
+  P.inv_visc = 1.0 / d.viscosity;
+  for (int f = 0; f < 6; f++) {
+    P.bc_type[f] = PFGPU_BC_FLUX;
+    P.bc_val[f] = h->bcv[f];
+  }
+  if (build_vgraph(h)) return PFGPU_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  return 0;
+}
+
+static void destroy_impl(pfgpu_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->st) cudaStreamSynchronize(h->st);
+  if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
+  double *vecs[] = {h->u, h->unew, h->fval, h->pp, h->bb, h->p_old, h->s_old, h->kr,
+                    h->dkr, h->sat, h->dsat, h->xcor, h->vtemp, h->gs, h->dsc, h->stage,
+                    h->rb.partial, h->zmult, h->zface, h->alpha, h->vgn, h->sres, h->ssat};
+  for (double *v : vecs) cudaFree(v);
+  if (h->kx) cudaFree(h->kx);
+  if (h->ky && h->ky != h->kx) cudaFree(h->ky);
+  if (h->kz && h->kz != h->kx && h->kz != h->ky) cudaFree(h->kz);
+  for (int f = 0; f < 6; f++) cudaFree(h->bcv[f]);
+  for (auto v : h->V) cudaFree(v);
+  cudaFree(h->rb.ticket);
+  double *jd[] = {h->Jd.c, h->Jd.w, h->Jd.e, h->Jd.s, h->Jd.n, h->Jd.l, h->Jd.u};
+  for (double *a : jd) cudaFree(a);
+  float *jf[] = {h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
+  for (float *a : jf) cudaFree(a);
+  free_mg(h->mgd);
+  free_mg(h->mgf);
+  if (h->hsc) cudaFreeHost(h->hsc);
+  if (h->st) cudaStreamDestroy(h->st);
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *pfgpu_last_error(void) { return g_err; }
+
+pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
+  if (!desc || desc->abi_version != PFGPU_ABI_VERSION) {
+    set_err("pfgpu_create: null descriptor or ABI version mismatch");
+    return nullptr;
+  }
+  if (desc->nx < 1 || desc->ny < 1 || desc->nz < 1 ||
+      (long long)desc->nx * desc->ny * desc->nz < 2) {
+    set_err("pfgpu_create: grid must hold at least two cells");
+    return nullptr;
+  }
+  if (desc->krylov_dim < 1 || desc->krylov_dim > 30) {
+    set_err("pfgpu_create: krylov_dim must be in [1, 30]");
+    return nullptr;
+  }
+  if (desc->max_restarts != 0) {
+    set_err("pfgpu_create: only MaxRestarts 0 is supported");
+    return nullptr;
+  }
+  if (!(desc->dx > 0 && desc->dy > 0 && desc->dz > 0 && desc->density > 0 &&
+        desc->gravity > 0 && desc->viscosity > 0)) {
+    set_err("pfgpu_create: spacings, density, gravity and viscosity must be positive");
+    return nullptr;
+  }
+  pfgpu_handle *h = new pfgpu_handle();
+  h->d = *desc;
+  h->d.z_mult = nullptr;
+  h->device = device;
+  h->nx = desc->nx; h->ny = desc->ny; h->nz = desc->nz;
+  h->N = (long long)h->nx * h->ny * h->nz;
+  h->NP = (long long)(h->nx + 2) * (h->ny + 2) * (h->nz + 2);
+  h->mixed = desc->precision == PFGPU_PREC_MIXED;
+  if (create_impl(h) != 0) {
+    destroy_impl(h);
+    delete h;
+    return nullptr;
+  }
+  return h;
+}
+
+void pfgpu_destroy(pfgpu_handle *h) {
+  destroy_impl(h);
+  delete h;
+}
+
+int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
+  if (!h || !values) { set_err("pfgpu_set_field: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  double **dst = nullptr;
+  switch (field) {
+    case PFGPU_FIELD_PERM_X: dst = &h->kx; break;
+    case PFGPU_FIELD_PERM_Y:
+      if (h->ky == h->kx && dalloc(&h->ky, h->N)) return PFGPU_ERR_NOMEM;
+      dst = &h->ky;
+      break;
+    case PFGPU_FIELD_PERM_Z:
+      if ((h->kz == h->kx || h->kz == h->ky) && dalloc(&h->kz, h->N)) return PFGPU_ERR_NOMEM;
+      dst = &h->kz;
+      break;
+    case PFGPU_FIELD_VG_ALPHA: dst = &h->alpha; break;
+    case PFGPU_FIELD_VG_N: dst = &h->vgn; break;
+    case PFGPU_FIELD_S_RES: dst = &h->sres; break;
+    case PFGPU_FIELD_S_SAT: dst = &h->ssat; break;
+    default: set_err("pfgpu_set_field: unknown field %d", field); return PFGPU_ERR_ARG;
+  }
+  if (!*dst && dalloc(dst, h->N)) return PFGPU_ERR_NOMEM;
+  if (in_vec(h, values, *dst)) return PFGPU_ERR_CUDA;
+  // a permeability set only in x serves all three directions
+  if (field == PFGPU_FIELD_PERM_X) {
+    if (h->ky == h->kx) h->ky = h->kx;
+    if (h->kz == h->kx) h->kz = h->kx;
+  }
+  DevProblem &P = h->P;
+  P.kx = h->kx; P.ky = h->ky; P.kz = h->kz;
+  P.alpha = h->alpha; P.vgn = h->vgn; P.sres = h->sres; P.ssat = h->ssat;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values) {
+  if (!h || !values || face < 0 || face > 5 || (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET)) {
+    set_err("pfgpu_set_bc: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  long long fs = face < 2 ? (long long)h->nz * h->ny : face < 4 ? (long long)h->nz * h->nx
+                                                               : (long long)h->ny * h->nx;
+  CK(cudaMemcpyAsync(h->bcv[face], values, fs * sizeof(double), cudaMemcpyDefault, h->st));
+  h->P.bc_type[face] = type;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_saturation(pfgpu_handle *h, const double *p, double *s) {
+  if (!h || !p || !s) { set_err("pfgpu_saturation: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p, h->unew)) return PFGPU_ERR_CUDA;
+  launch_saturation(h->P, h->unew, h->fval, h->st);
+  h->launches++;
+  return out_vec(h, h->fval, s);
+}
+
+int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old,
+                           const double *s_old, double dt, double *f) {
+  if (!h || !p || !p_old || !s_old || !f) {
+    set_err("pfgpu_nl_function_eval: null argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p, h->unew) || in_vec(h, p_old, h->p_old) || in_vec(h, s_old, h->s_old))
+    return PFGPU_ERR_CUDA;
+  feval(h, h->unew, dt, h->fval);
+  return out_vec(h, h->fval, f);
+}
+
+int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt, const double *x,
+                          double *y) {
+  if (!h || !p || !x || !y) { set_err("pfgpu_jacobian_matvec: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p, h->unew) || in_vec(h, x, h->vtemp)) return PFGPU_ERR_CUDA;
+  assemble(h, h->unew, dt, true, false);
+  h->jac_valid = 0;
+  matvec(h, h->vtemp, h->bb);
+  return out_vec(h, h->bb, y);
+}
+
+int pfgpu_pc_setup(pfgpu_handle *h, const double *p, double dt) {
+  if (!h || !p) { set_err("pfgpu_pc_setup: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p, h->unew)) return PFGPU_ERR_CUDA;
+  pc_setup_dense(h, h->unew, dt, false);
+  h->jac_valid = 0;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_pc_apply(pfgpu_handle *h, const double *r, double *z) {
+  if (!h || !r || !z) { set_err("pfgpu_pc_apply: null argument"); return PFGPU_ERR_ARG; }
+  if (!h->pc_ready) { set_err("pfgpu_pc_apply: call pfgpu_pc_setup first"); return PFGPU_ERR_STATE; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, r, h->vtemp)) return PFGPU_ERR_CUDA;
+  if (pc_apply_dense(h, h->vtemp, h->vtemp)) return PFGPU_ERR_CUDA;
+  return out_vec(h, h->vtemp, z);
+}
+
+int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old, double dt,
+                       double *p, pfgpu_stats *stats) {
+  if (!h || !p_old || !s_old || !p) { set_err("pfgpu_newton_solve: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p_old, h->p_old) || in_vec(h, s_old, h->s_old) || in_vec(h, p, h->u))
+    return PFGPU_ERR_CUDA;
+  pfgpu_stats local;
+  int rc = newton(h, dt, stats ? stats : &local);
+  if (rc < 0) return rc;
+  int rc2 = out_vec(h, h->u, p);
+  return rc2 ? rc2 : rc;
+}
+
+int pfgpu_set_pressure(pfgpu_handle *h, const double *p) {
+  if (!h || !p) { set_err("pfgpu_set_pressure: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p, h->u)) return PFGPU_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_get_pressure(pfgpu_handle *h, double *p) {
+  if (!h || !p) { set_err("pfgpu_get_pressure: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  return out_vec(h, h->u, p);
+}
+
+// AdvanceRichards step body (solver_richards.c:2965-3406): old state copies,
+// nonlinear solve, dt halving on failure (Solver.MaxConvergenceFailures 3).
+int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats) {
+  if (!h || nsteps < 0 || !(dt > 0)) { set_err("pfgpu_advance: bad argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  for (int s = 0; s < nsteps; s++) {
+    CK(cudaMemcpyAsync(h->p_old, h->u, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    launch_saturation(h->P, h->u, h->s_old, h->st);
+    h->launches++;
+    double dts = dt;
+    int rc = PFGPU_NOT_CONVERGED;
+    pfgpu_stats st{};
+    for (int fail = 0; fail < 3; fail++) {
+      rc = newton(h, dts, &st);
+      if (rc < 0) return rc;
+      if (rc == PFGPU_OK) break;
+      CK(cudaMemcpyAsync(h->u, h->p_old, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+      h->vg_for = nullptr;
+      dts *= 0.5;
+    }
+    if (stats) stats[s] = st;
+    if (rc != PFGPU_OK) {
+      set_err("pfgpu_advance: time step %d failed after 3 convergence failures", s);
+      return PFGPU_NOT_CONVERGED;
+    }
+  }
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels) {
+  if (!h || !levels) { set_err("pfgpu_mg_levels: null argument"); return PFGPU_ERR_ARG; }
+  *levels = h->nlev;
+  if (dims) {
+    for (int l = 0; l < h->nlev && l < max_levels; l++) {
+      if (h->mixed) {
+        const MGLevel<float> &L = h->mgf.L[l];
+        dims[4 * l] = L.nx; dims[4 * l + 1] = L.ny; dims[4 * l + 2] = L.nz; dims[4 * l + 3] = L.dir;
+      } else {
+        const MGLevel<double> &L = h->mgd.L[l];
+        dims[4 * l] = L.nx; dims[4 * l + 1] = L.ny; dims[4 * l + 2] = L.nz; dims[4 * l + 3] = L.dir;
+      }
+    }
+  }
+  return PFGPU_OK;
+}
+
+// Algorithmic HBM bytes per launch (every per-cell array the operation needs,
+// counted once; uniform fields count zero).
+static double kernel_bytes(pfgpu_handle *h, int kernel) {
+  const double N = (double)h->N;
+  const double wJ = h->mixed ? 4.0 : 8.0;
+  const double vg = (h->alpha ? 8.0 : 0.0) + (h->vgn ? 8.0 : 0.0) + (h->sres ? 8.0 : 0.0) +
+                    (h->ssat ? 8.0 : 0.0);
+  const double kf = 8.0 * (1 + (h->ky != h->kx) + (h->kz != h->kx && h->kz != h->ky));
+  switch (kernel) {
+    case PFGPU_KERNEL_RESIDUAL: return N * (8.0 * 4 + kf + vg);         // p p_old s_old f
+    case PFGPU_KERNEL_JACOBIAN: return N * (8.0 + kf + vg + 7 * wJ + 4 * wJ);
+    case PFGPU_KERNEL_MATVEC: return N * (7 * wJ + 8.0 + 8.0);
+    case PFGPU_KERNEL_RB_SWEEP: return N * (4 * wJ + wJ + 2 * wJ);      // C E N U, b, x in + out
+    default: return 0.0;
+  }
+}
+
+int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double *bytes) {
+  if (!h || reps < 1 || !ms) { set_err("pfgpu_time_kernel: bad argument"); return PFGPU_ERR_ARG; }
+  if (!h->pc_ready) { set_err("pfgpu_time_kernel: no assembled state yet"); return PFGPU_ERR_STATE; }
+  CK(cudaSetDevice(h->device));
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const double dt = 0.05;
+  auto one = [&]() {
+    switch (kernel) {
+      case PFGPU_KERNEL_RESIDUAL: feval(h, h->u, dt, h->fval); break;
+      case PFGPU_KERNEL_JACOBIAN: assemble(h, h->u, dt, true, true); break;
+      case PFGPU_KERNEL_MATVEC: matvec(h, h->pp, h->bb); break;
+      case PFGPU_KERNEL_RB_SWEEP:  // the finest level's post-smoother as the V-cycle runs it
+        if (h->mixed) {
+          MGLevel<float> &L = h->mgf.L[0];
+          if (h->mgf.fused && L.x2) launch_rbr_fused<float>(L, L.x, L.x2, L.b, 0, h->st);
+          else launch_mg_smooth<float>(L, L.x, L.b, 0, 0, 1.0, h->mgf.wtmp, h->st);
+        } else {
+          MGLevel<double> &L = h->mgd.L[0];
+          if (h->mgd.fused && L.x2) launch_rbr_fused<double>(L, L.x, L.x2, L.b, 0, h->st);
+          else launch_mg_smooth<double>(L, L.x, L.b, 0, 0, 1.0, h->mgd.wtmp, h->st);
+        }
+        h->launches++;
+        break;
+      case PFGPU_KERNEL_VCYCLE:
+        cudaGraphLaunch(h->vgraph, h->st);
+        h->launches += h->graph_nodes;
+        break;
+      case PFGPU_KERNEL_MG_SETUP:
+        h->launches += h->mixed ? mg_setup_T<float>(h->mgf, h->st) : mg_setup_T<double>(h->mgd, h->st);
+        break;
+    }
+  };
+  one();  // warm
+  CK(cudaEventRecord(e0, h->st));
+  for (int r = 0; r < reps; r++) one();
+  CK(cudaEventRecord(e1, h->st));
+  CK(cudaEventSynchronize(e1));
+  float t = 0.f;
+  CK(cudaEventElapsedTime(&t, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  *ms = (double)t / reps;
+  if (bytes) *bytes = kernel_bytes(h, kernel);
+  h->jac_valid = 0;
+  return PFGPU_OK;
+}
+
+void *pfgpu_stream(pfgpu_handle *h) { return h ? (void *)h->st : nullptr; }
+
+long long pfgpu_kernel_launches(pfgpu_handle *h) { return h ? h->launches : 0; }
+
+}  // extern "C"

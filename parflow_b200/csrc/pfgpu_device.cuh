@@ -1,0 +1,200 @@
+// Device-side problem description and per-cell physics shared by the
+// residual, Jacobian and saturation kernels.
+//
+// Internal layout: interior cells only, x fastest, c = i + nx*(j + ny*k).
+// Boundary faces never read a neighbour: their contribution comes from the
+// per-face BC tables, which is the net effect of ParFlow's ghost-cell
+// insertion / correction / reset sequence for box domains
+// (pfsimulator/parflow_lib/nl_function_eval.c:574-610, 979-1233, 2269-2311).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pfgpu {
+
+struct DevProblem {
+  int nx, ny, nz;
+  long long n;
+  double dx, dy, dz;
+  double gravity, viscosity, density;
+  double porosity, sstorage;
+  // van Genuchten: per-cell arrays or (when the pointer is null) scalars
+  const double *alpha, *vgn, *sres, *ssat;
+  double alpha0, vgn0, sres0, ssat0;
+  int vg_from_file;
+  const double *kx, *ky, *kz;   // per cell
+  const double *zmult;          // per layer
+  // per z face between layers k and k+1: 1/sep, z_k/(z_k+z_k+1), z_k+1/(z_k+z_k+1)
+  const double *zface;          // 3*nz
+  double inv_dx, inv_dy, inv_visc;
+  int bc_type[6];
+  const double *bc_val[6];
+};
+
+// ParFlow's mean macros (pfsimulator/parflow_lib/solver.h:42-47)
+__device__ __forceinline__ double harmonic(double a, double b) {
+  return (a + b) ? (2.0 * a * b) / (a + b) : 0.0;
+}
+__device__ __forceinline__ double harmonic_dz(double a, double b, double c, double d) {
+  return ((c * b) + (a * d)) ? (((c + d) * a * b) / ((b * c) + (a * d))) : 0.0;
+}
+__device__ __forceinline__ double upstream(double a, double b, double c, double d) {
+  return ((a - b) >= 0) ? c : d;
+}
+__device__ __forceinline__ double amean(double a, double b) { return 0.5 * (a + b); }
+
+struct VG {
+  double alpha, n, sres, ssat;
+};
+
+__device__ __forceinline__ VG vg_at(const DevProblem &P, long long c) {
+  VG v;
+  v.alpha = P.alpha ? __ldg(P.alpha + c) : P.alpha0;
+  v.n = P.vgn ? __ldg(P.vgn + c) : P.vgn0;
+  v.sres = P.sres ? __ldg(P.sres + c) : P.sres0;
+  v.ssat = P.ssat ? __ldg(P.ssat + c) : P.ssat0;
+  return v;
+}
+
+// Saturation (pfsimulator/parflow_lib/problem_saturation.c:221-415)
+__device__ __forceinline__ double vg_sat(const DevProblem &P, double p, const VG &v) {
+  double m = 1.0 - (1.0 / v.n);
+  double s_dif = v.ssat - v.sres;
+  if (p >= 0.0) return P.vg_from_file ? v.ssat : s_dif + v.sres;
+  double head = fabs(p) / (P.density * P.gravity);
+  return s_dif / pow(1.0 + pow(v.alpha * head, v.n), m) + v.sres;
+}
+
+__device__ __forceinline__ double vg_dsat(const DevProblem &P, double p, const VG &v) {
+  double m = 1.0 - (1.0 / v.n);
+  double s_dif = v.ssat - v.sres;
+  if (p >= 0.0) return 0.0;
+  double head = fabs(p) / (P.density * P.gravity);
+  return (m * v.n * v.alpha * pow(v.alpha * head, (v.n - 1))) * s_dif /
+         (pow(1.0 + pow(v.alpha * head, v.n), m + 1));
+}
+
+// Relative permeability (pfsimulator/parflow_lib/problem_phase_rel_perm.c:788, :981)
+__device__ __forceinline__ double vg_kr(const DevProblem &P, double p, double alpha, double n) {
+  if (p >= 0.0) return 1.0;
+  double m = 1.0 - (1.0 / n);
+  double head = fabs(p) / (P.density * P.gravity);
+  double opahn = 1.0 + pow(alpha * head, n);
+  double ahnm1 = pow(alpha * head, n - 1);
+  double t = 1.0 - ahnm1 / pow(opahn, m);
+  return (t * t) / pow(opahn, m / 2);
+}
+
+__device__ __forceinline__ double vg_dkr(const DevProblem &P, double p, double alpha, double n) {
+  if (p >= 0.0) return 0.0;
+  double m = 1.0 - (1.0 / n);
+  double head = fabs(p) / (P.density * P.gravity);
+  double opahn = 1.0 + pow(alpha * head, n);
+  double ahnm1 = pow(alpha * head, n - 1);
+  double coeff = 1.0 - ahnm1 * pow(opahn, -m);
+  return 2.0 * (coeff / (pow(opahn, (m / 2)))) *
+             ((n - 1) * pow(alpha * head, n - 2) * alpha * pow(opahn, -m) -
+              ahnm1 * m * pow(opahn, -(m + 1)) * n * alpha * ahnm1) +
+         (coeff * coeff) * (m / 2) * pow(opahn, (-(m + 2) / 2)) * n * alpha * ahnm1;
+}
+
+// All four van Genuchten quantities of one cell from one log(alpha h) and one
+// log1p((alpha h)^n): every power of the reference formulas
+// (problem_saturation.c:221-415, problem_phase_rel_perm.c:788, :981) is
+// rewritten as exp(y * log x) over these two logarithms.
+struct VGAll {
+  double kr, dkr, s, ds;
+};
+
+__device__ __forceinline__ VGAll vg_all(const DevProblem &P, double p, const VG &v) {
+  VGAll r;
+  const double s_dif = v.ssat - v.sres;
+  if (p >= 0.0) {
+    r.kr = 1.0;
+    r.dkr = 0.0;
+    r.s = P.vg_from_file ? v.ssat : s_dif + v.sres;
+    r.ds = 0.0;
+    return r;
+  }
+  const double n = v.n, alpha = v.alpha;
+  const double m = 1.0 - (1.0 / n);
+  const double head = fabs(p) / (P.density * P.gravity);
+  const double L = log(alpha * head);
+  const double ahn = exp(n * L);           // (alpha h)^n
+  const double ahnm1 = exp((n - 1) * L);   // (alpha h)^(n-1)
+  const double ahnm2 = exp((n - 2) * L);   // (alpha h)^(n-2)
+  const double lop = log1p(ahn);           // log(1 + (alpha h)^n)
+  const double opahn = 1.0 + ahn;
+  const double opm = exp(m * lop);         // opahn^m
+  const double opm2 = exp(0.5 * m * lop);  // opahn^(m/2)
+  const double inv_opm = 1.0 / opm;
+  const double t = 1.0 - ahnm1 * inv_opm;
+  const double inv_opm2 = 1.0 / opm2;
+  const double inv_op = 1.0 / opahn;
+  r.kr = (t * t) * inv_opm2;
+  r.dkr = 2.0 * (t * inv_opm2) *
+              ((n - 1) * ahnm2 * alpha * inv_opm - ahnm1 * m * (inv_opm * inv_op) * n * alpha * ahnm1) +
+          (t * t) * (m / 2) * (inv_opm2 * inv_op) * n * alpha * ahnm1;
+  r.s = s_dif * inv_opm + v.sres;
+  r.ds = (m * n * alpha * ahnm1) * s_dif * (inv_opm * inv_op);
+  return r;
+}
+
+// ---------------------------------------------------------------------------
+// Face fluxes of the residual (nl_function_eval.c:696-854); slopes are zero
+// on this path: x_dir_g = 0, x_dir_g_c = gravity.
+// a = lower/left cell, b = upper/right cell.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double flux_x(const DevProblem &P, double pa, double pb, double ka,
+                                         double kb, double kra, double krb, double zm) {
+  const double g = P.gravity;
+  const double x_dir_g = amean(g * 0.0, g * 0.0);
+  const double x_dir_g_c = amean(g * 1.0, g * 1.0);
+  double diff_l = pa - pb;
+  double updir = (diff_l * P.inv_dx) * x_dir_g_c - x_dir_g;
+  double km = harmonic(ka, kb);
+  double up = upstream(updir, 0.0, kra * P.density, krb * P.density);
+  double ffx = P.dy * P.dz;
+  double u = zm * ffx * 1.0 * km * (diff_l * P.inv_dx) * x_dir_g_c * up * P.inv_visc;
+  u += zm * ffx * 1.0 * km * (-x_dir_g) * up * P.inv_visc;
+  return u;
+}
+
+__device__ __forceinline__ double flux_y(const DevProblem &P, double pa, double pb, double ka,
+                                         double kb, double kra, double krb, double zm) {
+  const double g = P.gravity;
+  const double y_dir_g = amean(g * 0.0, g * 0.0);
+  const double y_dir_g_c = amean(g * 1.0, g * 1.0);
+  double diff_l = pa - pb;
+  double updir = (diff_l * P.inv_dy) * y_dir_g_c - y_dir_g;
+  double km = harmonic(ka, kb);
+  double up = upstream(updir, 0.0, kra * P.density, krb * P.density);
+  double ffy = P.dx * P.dz;
+  double u = zm * ffy * 1.0 * km * (diff_l * P.inv_dy) * y_dir_g_c * up * P.inv_visc;
+  u += zm * ffy * 1.0 * km * (-y_dir_g) * up * P.inv_visc;
+  return u;
+}
+
+// z face between layer k (a, below) and k+1 (b, above)
+__device__ __forceinline__ double flux_z(const DevProblem &P, double pa, double pb, double ka,
+                                         double kb, double kra, double krb, double za,
+                                         double zb, int k) {
+  const double g = P.gravity, rho = P.density;
+  const double inv_sep = __ldg(P.zface + 3 * k);
+  double lower = pa * inv_sep - __ldg(P.zface + 3 * k + 1) * rho * g * 1.0;
+  double upper = pb * inv_sep + __ldg(P.zface + 3 * k + 2) * rho * g * 1.0;
+  double diff_l = lower - upper;
+  double ffz = P.dx * P.dy;
+  return ffz * 1.0 * 1.0 * harmonic_dz(ka, kb, za, zb) * diff_l *
+         upstream(lower, upper, kra * rho, krb * rho) * P.inv_visc;
+}
+
+// Index of a boundary cell in its face table.
+__device__ __forceinline__ int face_slot(const DevProblem &P, int face, int i, int j, int k) {
+  if (face < 2) return j + P.ny * k;
+  if (face < 4) return i + P.nx * k;
+  return i + P.nx * j;
+}
+
+}  // namespace pfgpu

@@ -1,0 +1,138 @@
+// Kernel launch interfaces shared between the library's translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "pfgpu_device.cuh"
+
+namespace pfgpu {
+
+// Full 7-point Jacobian, stencil order of jacobian_stencil_shape
+// (pfsimulator/parflow_lib/richards_jacobian_eval.c:126-132): C W E S N L U.
+template <typename T>
+struct JacOut {
+  T *c, *w, *e, *s, *n, *l, *u;
+};
+template <typename T>
+struct JacIn {
+  const T *c, *w, *e, *s, *n, *l, *u;
+};
+// Symmetric operator: C and the upper entries E N U; W(i) = E(i-1),
+// S(i) = N(i-nx), L(i) = U(i-nx*ny) (pfsimulator/parflow_lib/matrix.c:258-310).
+template <typename T>
+struct PCOut {
+  T *c, *e, *n, *u;
+};
+
+void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
+                   double *dsat, cudaStream_t st);
+void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStream_t st);
+void launch_residual(const DevProblem &P, const double *p, const double *p_old,
+                     const double *s_old, const double *kr, const double *sat, double dt,
+                     double *f, cudaStream_t st);
+template <typename TJ, typename TP>
+void launch_jacobian(const DevProblem &P, const double *p, const double *kr, const double *dkr,
+                     const double *sat, const double *dsat, double dt, JacOut<TJ> J,
+                     PCOut<TP> M, cudaStream_t st);
+template <typename TJ>
+void launch_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double *y,
+                    cudaStream_t st);
+
+// ---- multigrid (mg_kernels.cu) --------------------------------------------
+template <typename T>
+struct MGLevel {
+  int nx, ny, nz;
+  long long n;
+  int dir;          // coarsening direction to the next level (-1 on the coarsest)
+  T *a[4];          // C E N U
+  T *x, *b, *t;
+  T *x2;            // output of the fused post-smoother (levels run by grid kernels)
+  T *p1, *p2;       // prolongation weights (fine points of this level)
+};
+
+template <typename T>
+void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st);
+template <typename T>
+void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
+template <typename T>
+void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
+                      double weight, T *tmp, cudaStream_t st);
+cudaError_t mg_prepare_kernels();
+// symmetric red/black Gauss-Seidel (red, black, red) in one fused pass,
+// x read from xin (ignored when zero) and written to xout (xin != xout)
+template <typename T>
+void launch_rbr_fused(const MGLevel<T> &L, const T *xin, T *xout, const T *b, int zero,
+                      cudaStream_t st);
+template <typename T>
+void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st);
+template <typename T>
+void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
+                        cudaStream_t st);
+template <typename T>
+void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
+                           cudaStream_t st);
+// levels `first` .. nl-1 of a V-cycle / of the setup in one single-block
+// kernel; levels_dev is a device copy of the level table
+template <typename T>
+void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
+                        double weight, T *tmp, cudaStream_t st);
+template <typename T>
+void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
+template <typename TI, typename TO>
+void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st);
+
+// ---- vectors and reductions (krylov_kernels.cu) ----------------------------
+struct ReduceBuf {
+  double *partial;        // >= reduce_blocks() doubles
+  unsigned int *ticket;   // one counter, zero between reductions
+  int blocks;
+};
+int reduce_blocks();
+// dst = sum(a .* b); deterministic (fixed grid, fixed order)
+void launch_dot(const double *a, const double *b, long long n, double *dst, ReduceBuf rb,
+                cudaStream_t st);
+// as launch_dot, skipped entirely when *gate == 0
+void launch_dot_gated(const double *a, const double *b, long long n, double *dst,
+                      const double *gate, ReduceBuf rb, cudaStream_t st);
+// dst = max |a|
+void launch_maxabs(const double *a, long long n, double *dst, ReduceBuf rb, cudaStream_t st);
+// dst = max |s| / (1 + |u|)
+void launch_steplen(const double *s, const double *u, long long n, double *dst, ReduceBuf rb,
+                    cudaStream_t st);
+// dst = max |a - b| / (1 + |a|)
+void launch_steplen_diff(const double *a, const double *b, long long n, double *dst,
+                         ReduceBuf rb, cudaStream_t st);
+// y = y + (sign * (*s)) * x
+void launch_axpy_dev(double *y, const double *x, const double *s, double sign, long long n,
+                     cudaStream_t st);
+// y = a*x + b*y (host scalars)
+void launch_axpby(double *y, const double *x, double a, double b, long long n, cudaStream_t st);
+// z = x + a*y
+void launch_xpay(double *z, const double *x, double a, const double *y, long long n,
+                 cudaStream_t st);
+// x *= 1 / (*s)
+void launch_scale_inv_dev(double *x, const double *s, long long n, cudaStream_t st);
+// x *= a
+void launch_scale(double *x, double a, long long n, cudaStream_t st);
+// xcor = sum_k yg[k] * V[k] (sequential axpy order)
+void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
+                    cudaStream_t st);
+void launch_fill(double *x, double v, long long n, cudaStream_t st);
+
+// GMRES scalar kernels (single thread); S layout and ops in krylov_kernels.cu
+enum { GM_START = 0, GM_AFTER_GS = 1, GM_QR = 3, GM_QRSOL = 4, GM_REORTH_DONE = 5 };
+enum { SCI_RNORM = 0, SCI_ROT, SCI_RHO, SCI_VKNORM2, SCI_NEWNORM2, SCI_FLAG, SCI_NN2, SCI_NP,
+       SCI_GATE, SCI_COEF, SCI_HLL, SCI_BETA, SCI_QRFAIL, SCI_COUNT };
+inline long long gs_size(int lmax) { return (long long)(lmax + 1) * lmax + 2 * lmax + lmax + 1 + SCI_COUNT; }
+inline long long gs_sc_offset(int lmax) { return (long long)(lmax + 1) * lmax + 2 * lmax + lmax + 1; }
+inline long long gs_yg_offset(int lmax) { return (long long)(lmax + 1) * lmax + 2 * lmax; }
+void launch_gmres_scalar(int op, double *S, int l, int lmax, cudaStream_t st);
+void launch_reorth_decide(double *S, int i, int l, int lmax, cudaStream_t st);
+void launch_axpy_gated(double *y, const double *x, const double *coef, const double *gate,
+                       long long n, cudaStream_t st);
+
+// ParFlow layout (ghost frame 1) <-> dense interior
+void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st);
+void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st);
+
+}  // namespace pfgpu

@@ -1,0 +1,432 @@
+// Richards residual, analytic Jacobian assembly and stencil matvec.
+//
+// Gather form: every cell computes the fluxes (or flux derivatives) of its
+// own six faces; a face shared by two cells is evaluated by both with the
+// same operands in the same order, so both see identical bits and no atomics
+// are needed.  Per-cell relative permeabilities are produced by a first pass
+// (k_vg_all) so that each cell's van Genuchten state is evaluated once per
+// iterate and shared by the residual and the Jacobian.
+#include "pfgpu_device.cuh"
+#include "pfgpu_kernels.h"
+
+namespace pfgpu {
+
+// (i, j, k) of a thread in a 3-D launch (x across the block's threads,
+// rows in y, one plane per blockIdx.z): no integer division
+__device__ __forceinline__ bool launch_ijk(int nx, int ny, int nz, int &i, int &j, int &k) {
+  i = blockIdx.x * blockDim.x + threadIdx.x;
+  j = blockIdx.y * blockDim.y + threadIdx.y;
+  k = blockIdx.z;
+  return i < nx && j < ny && k < nz;
+}
+
+// Van Genuchten state of every cell at one pressure iterate: kr, dkr/dp, S,
+// dS/dp (problem_phase_rel_perm.c:1312-1361, problem_saturation.c:342-412).
+// The residual uses kr and S; the Jacobian at the same iterate reuses all four.
+__global__ void k_vg_all(DevProblem P, const double *__restrict__ p, double *__restrict__ kr,
+                         double *__restrict__ dkr, double *__restrict__ sat,
+                         double *__restrict__ dsat) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= P.n) return;
+  VGAll v = vg_all(P, p[c], vg_at(P, c));
+  kr[c] = v.kr;
+  dkr[c] = v.dkr;
+  sat[c] = v.s;
+  dsat[c] = v.ds;
+}
+
+__global__ void k_saturation(DevProblem P, const double *__restrict__ p, double *__restrict__ s) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= P.n) return;
+  s[c] = vg_all(P, p[c], vg_at(P, c)).s;
+}
+
+// Residual (nl_function_eval.c:167-2323).  Accumulation order per cell
+// follows the reference: accumulation, storage, sources, then the face
+// fluxes scattered from the k-1, j-1, i-1 neighbours, the cell's own three
+// upper faces, and finally the boundary patches in patch order.
+__global__ void k_residual(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ p_old, const double *__restrict__ s_old,
+                           const double *__restrict__ kr, const double *__restrict__ satv,
+                           double dt, double *__restrict__ f) {
+  int i, j, k;
+  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
+  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double rho = P.density, g = P.gravity;
+  const double vol = P.dx * P.dy * P.dz;
+  const double zm = __ldg(P.zmult + k);
+  const double pc = p[c];
+  const double sat = satv[c];
+  const double so = s_old[c];
+  double fc = (sat * rho - so * rho) * P.porosity * vol * 1.0 * 1.0 * zm;
+  fc += P.sstorage * vol * 1.0 * 1.0 * zm * (pc * sat * rho - p_old[c] * so * rho);
+  fc -= vol * 1.0 * 1.0 * zm * dt * (0.0 + 0.0);
+
+  const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+  const double krc = kr[c];
+  // neighbours' scatter (reference loop order: plane k-1, row j-1, cell i-1)
+  if (k > 0) {
+    long long l = c - sz;
+    double zl = __ldg(P.zmult + k - 1);
+    fc += -dt * flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
+  }
+  if (j > 0) {
+    long long s = c - sy;
+    fc += -dt * flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm);
+  }
+  if (i > 0) {
+    long long w = c - 1;
+    fc += -dt * flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm);
+  }
+  double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
+  if (i + 1 < P.nx) {
+    long long e = c + 1;
+    u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm);
+  }
+  if (j + 1 < P.ny) {
+    long long nn = c + sy;
+    u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm);
+  }
+  if (k + 1 < P.nz) {
+    long long u = c + sz;
+    u_upper = flux_z(P, pc, p[u], kzc, __ldg(P.kz + u), krc, kr[u], zm,
+                     __ldg(P.zmult + k + 1), k);
+  }
+  fc += dt * (u_right + u_front + u_upper);
+
+  // boundary patches (nl_function_eval.c:979-1435)
+  const double ffx = P.dy * P.dz, ffy = P.dx * P.dz, ffz = P.dx * P.dy;
+  const bool onf[6] = {i == 0, i == P.nx - 1, j == 0, j == P.ny - 1, k == 0, k == P.nz - 1};
+#pragma unroll
+  for (int face = 0; face < 6; face++) {
+    if (!onf[face]) continue;
+    const double value = __ldg(P.bc_val[face] + face_slot(P, face, i, j, k));
+    const double dir = (face & 1) ? 1.0 : -1.0;
+    double u_new;
+    if (P.bc_type[face] == 0) {
+      double h = (face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz;
+      u_new = h * value;
+    } else {
+      const VG v = vg_at(P, c);
+      double krg = vg_kr(P, value, v.alpha, v.n);
+      if (face < 4) {
+        double h = (face < 2) ? ffx * zm : ffy * zm;
+        double kk = (face < 2) ? kxc : kyc;
+        double dd = (face < 2) ? P.dx : P.dy;
+        if (dir < 0) {
+          double diff = value - pc;
+          u_new = upstream(value, pc, krg * rho, krc * rho);
+          u_new = u_new * h * (kk * P.inv_visc) * 2.0 * (diff / dd);
+        } else {
+          double diff = pc - value;
+          u_new = upstream(pc, value, krc * rho, krg * rho);
+          u_new = u_new * h * (kk * P.inv_visc) * 2.0 * (diff / dd);
+        }
+      } else {
+        double sep = P.dz * zm;
+        double lower, upper;
+        if (dir < 0) {
+          lower = value / sep - 0.25 * rho * g;
+          upper = pc / sep + 0.25 * rho * g;
+          u_new = upstream(lower, upper, krg * rho, krc * rho);
+        } else {
+          lower = (pc / sep) - 0.25 * rho * g * 1.0;
+          upper = (value / sep) + 0.25 * rho * g * 1.0;
+          u_new = upstream(lower, upper, krc * rho, krg * rho);
+        }
+        u_new = u_new * ffz * (kzc * P.inv_visc) * 2.0 * (lower - upper);
+      }
+    }
+    fc += dt * dir * u_new;
+  }
+  f[c] = fc;
+}
+
+// Flux derivatives of one x (or y) face between a (left) and b (right)
+// (richards_jacobian_eval.c:618-660): returns west/east and symmetric parts.
+struct FaceDer {
+  double lo, hi, sym;  // d/dp of the face flux w.r.t. lower cell (negated), upper cell; sym part
+};
+
+__device__ __forceinline__ FaceDer face_der_xy(const DevProblem &P, double dt, double h_ff,
+                                               double dd, double pa, double pb, double ka,
+                                               double kb, double prod, double prod_der,
+                                               double prod_rt, double prod_rt_der, double zm) {
+  const double g = P.gravity;
+  const double dir_g = amean(g * 0.0, g * 0.0);
+  const double dir_g_c = amean(g * 1.0, g * 1.0);
+  double diff = pa - pb;
+  const double inv_dd = 1.0 / dd;
+  double updir = (diff * inv_dd) * dir_g_c - dir_g;
+  double coeff = 1.0 * dt * h_ff * inv_dd * zm * harmonic(ka, kb) * P.inv_visc;
+  FaceDer r;
+  double sym_lo = (-coeff * upstream(updir, 0.0, prod, prod_rt)) * dir_g_c;
+  r.lo = (-coeff * diff * upstream(updir, 0.0, prod_der, 0.0)) * dir_g_c + sym_lo;
+  r.lo += (coeff * dd * upstream(updir, 0.0, prod_der, 0.0)) * dir_g;
+  r.sym = (-coeff * upstream(updir, 0.0, prod, prod_rt)) * dir_g_c;
+  r.hi = (coeff * diff * upstream(updir, 0.0, 0.0, prod_rt_der)) * dir_g_c + r.sym;
+  r.hi += -(coeff * dd * upstream(updir, 0.0, 0.0, prod_rt_der)) * dir_g;
+  return r;
+}
+
+// z face between a (lower) and b (upper) (richards_jacobian_eval.c:697-745)
+__device__ __forceinline__ FaceDer face_der_z(const DevProblem &P, double dt, double pa,
+                                              double pb, double ka, double kb, double prod,
+                                              double prod_der, double prod_up,
+                                              double prod_up_der, double za, double zb, int k) {
+  const double g = P.gravity, rho = P.density, drho = 0.0;
+  const double dz = P.dz;
+  const double inv_sep = __ldg(P.zface + 3 * k);
+  double lower_cond = pa * inv_sep - __ldg(P.zface + 3 * k + 1) * rho * g;
+  double upper_cond = pb * inv_sep + __ldg(P.zface + 3 * k + 2) * rho * g;
+  double diff = lower_cond - upper_cond;
+  double z_coeff = 1.0 * dt * (P.dx * P.dy) * harmonic_dz(ka, kb, za, zb) * P.inv_visc;
+  double up = upstream(lower_cond, upper_cond, prod, prod_up);
+  double sym_lower = -z_coeff * inv_sep * up;
+  FaceDer r;
+  r.lo = -z_coeff * (diff * upstream(lower_cond, upper_cond, prod_der, 0.0) +
+                     (-g * 0.5 * dz * (amean(za, zb)) * drho * up)) +
+         sym_lower;
+  r.sym = z_coeff * inv_sep * -up;
+  r.hi = z_coeff * (diff * upstream(lower_cond, upper_cond, 0.0, prod_up_der) +
+                    (-g * 0.5 * dz * (amean(za, zb)) * drho * up)) +
+         r.sym;
+  return r;
+}
+
+// Jacobian assembly (richards_jacobian_eval.c:217-1420).  Writes the full
+// 7-point J (C W E S N L U, FP64 or FP32) and the symmetric preconditioner
+// matrix (C E N U: full diagonal, symmetric off-diagonal parts; PCMatrixType
+// PFSymmetric), in the preconditioner's precision.
+template <typename TJ, typename TP>
+__global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ kr, const double *__restrict__ dkr,
+                           const double *__restrict__ satv, const double *__restrict__ dsatv,
+                           double dt, JacOut<TJ> J, PCOut<TP> M) {
+  int i, j, k;
+  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
+  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double rho = P.density, g = P.gravity, drho = 0.0;
+  const double vol = P.dx * P.dy * P.dz;
+  const double ffx = P.dy * P.dz, ffy = P.dx * P.dz, ffz = P.dx * P.dy;
+  const double zm = __ldg(P.zmult + k);
+  const double pc = p[c];
+  const double sat = satv[c], dsat = dsatv[c];
+  const double prod = kr[c] * rho, prod_der = dkr[c] * rho + kr[c] * drho;
+  const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+
+  double vol2 = vol * zm;
+  double cp = 0.0;
+  cp += (dsat * rho + sat * drho) * P.porosity * vol2 +
+        P.sstorage * vol2 * (dsat * rho * pc + sat * drho * pc + sat * rho);
+
+  double w = 0.0, s = 0.0, l = 0.0, e = 0.0, nn = 0.0, u = 0.0;
+  double es = 0.0, ns = 0.0, us = 0.0;
+  if (k > 0) {
+    long long q = c - sz;
+    FaceDer d = face_der_z(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
+                           dkr[q] * rho + kr[q] * drho, prod, prod_der, __ldg(P.zmult + k - 1),
+                           zm, k - 1);
+    cp += -d.hi;
+    l = d.lo;
+  }
+  if (j > 0) {
+    long long q = c - sy;
+    FaceDer d = face_der_xy(P, dt, ffy, P.dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm);
+    cp += -d.hi;
+    s = d.lo;
+  }
+  if (i > 0) {
+    long long q = c - 1;
+    FaceDer d = face_der_xy(P, dt, ffx, P.dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm);
+    cp += -d.hi;
+    w = d.lo;
+  }
+  double west_t = 0.0, south_t = 0.0, lower_t = 0.0;
+  if (i + 1 < P.nx) {
+    long long q = c + 1;
+    FaceDer d = face_der_xy(P, dt, ffx, P.dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm);
+    west_t = d.lo;
+    e = d.hi;
+    es = d.sym;
+  }
+  if (j + 1 < P.ny) {
+    long long q = c + sy;
+    FaceDer d = face_der_xy(P, dt, ffy, P.dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm);
+    south_t = d.lo;
+    nn = d.hi;
+    ns = d.sym;
+  }
+  if (k + 1 < P.nz) {
+    long long q = c + sz;
+    FaceDer d = face_der_z(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
+                           dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
+    lower_t = d.lo;
+    u = d.hi;
+    us = d.sym;
+  }
+  cp += -(west_t + south_t + lower_t);
+
+  // Dirichlet patches (richards_jacobian_eval.c:1049-1200); flux patches
+  // leave the row as is (their boundary entries are zero)
+  const bool onf[6] = {i == 0, i == P.nx - 1, j == 0, j == P.ny - 1, k == 0, k == P.nz - 1};
+#pragma unroll
+  for (int face = 0; face < 6; face++) {
+    if (!onf[face] || P.bc_type[face] != 1) continue;
+    const double value = __ldg(P.bc_val[face] + face_slot(P, face, i, j, k));
+    const double den_d = rho;
+    const VG v = vg_at(P, c);
+    const double prod_val = vg_kr(P, value, v.alpha, v.n) * den_d;
+    const double zu = (k + 1 < P.nz) ? __ldg(P.zmult + k + 1) : 0.0;
+    double coeff, diff, o_temp;
+    switch (face) {
+      case 0:
+        coeff = dt * ffx * zm * (2.0 / P.dx) * kxc * P.inv_visc;
+        diff = value - pc;
+        o_temp = coeff * (diff * upstream(value, pc, 0.0, prod_der) -
+                          upstream(value, pc, prod_val, prod));
+        break;
+      case 1:
+        coeff = dt * ffx * zm * (2.0 / P.dx) * kxc * P.inv_visc;
+        diff = pc - value;
+        o_temp = -coeff * (diff * upstream(pc, value, prod_der, 0.0) +
+                           upstream(pc, value, prod, prod_val));
+        break;
+      case 2:
+        coeff = dt * ffy * zm * (2.0 / P.dy) * kyc * P.inv_visc;
+        diff = value - pc;
+        o_temp = coeff * (diff * upstream(value, pc, 0.0, prod_der) -
+                          upstream(value, pc, prod_val, prod));
+        break;
+      case 3:
+        coeff = dt * ffy * zm * (2.0 / P.dy) * kyc * P.inv_visc;
+        diff = pc - value;
+        o_temp = -coeff * (diff * upstream(pc, value, prod_der, 0.0) +
+                           upstream(pc, value, prod, prod_val));
+        break;
+      case 4: {
+        coeff = dt * ffz * (2.0 / (P.dz * amean(zm, zu))) * kzc * P.inv_visc;
+        double lc = (value)-0.5 * P.dz * zm * den_d * g;
+        double uc = (pc) + 0.5 * P.dz * zm * rho * g;
+        diff = lc - uc;
+        o_temp = coeff * (diff * upstream(lc, uc, 0.0, prod_der) +
+                          ((-1.0 - g * 0.5 * P.dz * zm * drho) * upstream(lc, uc, prod_val, prod)));
+        break;
+      }
+      default: {
+        coeff = dt * ffz * (2.0 / (P.dz * amean(zm, zu))) * kzc * P.inv_visc;
+        double lc = (pc)-0.5 * P.dz * zm * rho * g;
+        double uc = (value) + 0.5 * P.dz * zm * den_d * g;
+        diff = lc - uc;
+        o_temp = -coeff * (diff * upstream(lc, uc, prod_der, 0.0) +
+                           ((1.0 - g * 0.5 * P.dz * zm * drho) * upstream(lc, uc, prod, prod_val)));
+        break;
+      }
+    }
+    cp -= o_temp;
+  }
+  if (J.c) {
+    J.c[c] = (TJ)cp;
+    J.w[c] = (TJ)w;
+    J.e[c] = (TJ)e;
+    J.s[c] = (TJ)s;
+    J.n[c] = (TJ)nn;
+    J.l[c] = (TJ)l;
+    J.u[c] = (TJ)u;
+  }
+  if (M.c) {
+    M.c[c] = (TP)cp;
+    M.e[c] = (TP)es;
+    M.n[c] = (TP)ns;
+    M.u[c] = (TP)us;
+  }
+}
+
+// y = J x (matvec.c:35-330 order: y = 0, then C W E S N L U), FP64 accumulate
+template <typename TJ>
+__global__ void k_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *__restrict__ x,
+                          double *__restrict__ y) {
+  int i, j, k;
+  if (!launch_ijk(nx, ny, nz, i, j, k)) return;
+  const long long c = i + (long long)nx * (j + (long long)ny * k);
+  const long long sy = nx, sz = (long long)nx * ny;
+  double acc = 0.0;
+  acc += (double)J.c[c] * x[c];
+  acc += (double)J.w[c] * (i > 0 ? x[c - 1] : 0.0);
+  acc += (double)J.e[c] * (i + 1 < nx ? x[c + 1] : 0.0);
+  acc += (double)J.s[c] * (j > 0 ? x[c - sy] : 0.0);
+  acc += (double)J.n[c] * (j + 1 < ny ? x[c + sy] : 0.0);
+  acc += (double)J.l[c] * (k > 0 ? x[c - sz] : 0.0);
+  acc += (double)J.u[c] * (k + 1 < nz ? x[c + sz] : 0.0);
+  y[c] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// 3-D launch covering (nx, ny, nz) with `threads` threads per block
+static inline void shape(int nx, int ny, int nz, int threads, dim3 &grid, dim3 &block) {
+  int bx = 32;
+  while (bx < nx && bx < 128) bx *= 2;
+  if (bx > threads) bx = threads;
+  int by = threads / bx;
+  if (by > ny) by = ny;
+  block = dim3(bx, by, 1);
+  grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
+}
+
+void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
+                   double *dsat, cudaStream_t st) {
+  k_vg_all<<<blocks_for(P.n, 256), 256, 0, st>>>(P, p, kr, dkr, sat, dsat);
+}
+
+void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStream_t st) {
+  k_saturation<<<blocks_for(P.n, 256), 256, 0, st>>>(P, p, s);
+}
+
+void launch_residual(const DevProblem &P, const double *p, const double *p_old,
+                     const double *s_old, const double *kr, const double *sat, double dt,
+                     double *f, cudaStream_t st) {
+  dim3 g, b;
+  shape(P.nx, P.ny, P.nz, 256, g, b);
+  k_residual<<<g, b, 0, st>>>(P, p, p_old, s_old, kr, sat, dt, f);
+}
+
+template <typename TJ, typename TP>
+void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
+                     const double *dkr, const double *sat, const double *dsat, double dt,
+                     JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
+  dim3 g, b;
+  shape(P.nx, P.ny, P.nz, 128, g, b);
+  k_jacobian<TJ, TP><<<g, b, 0, st>>>(P, p, kr, dkr, sat, dsat, dt, J, M);
+}
+
+template <typename TJ>
+void launch_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double *y,
+                    cudaStream_t st) {
+  dim3 g, b;
+  shape(nx, ny, nz, 256, g, b);
+  k_matvec7<TJ><<<g, b, 0, st>>>(nx, ny, nz, J, x, y);
+}
+
+template void launch_jacobian<double, double>(const DevProblem &, const double *,
+                                              const double *, const double *, const double *,
+                                              const double *, double, JacOut<double>,
+                                              PCOut<double>, cudaStream_t);
+template void launch_jacobian<float, float>(const DevProblem &, const double *, const double *,
+                                            const double *, const double *, const double *,
+                                            double, JacOut<float>, PCOut<float>, cudaStream_t);
+template void launch_matvec7<double>(int, int, int, JacIn<double>, const double *, double *,
+                                     cudaStream_t);
+template void launch_matvec7<float>(int, int, int, JacIn<float>, const double *, double *,
+                                    cudaStream_t);
+
+}  // namespace pfgpu

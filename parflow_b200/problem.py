@@ -259,6 +259,35 @@ class RichardsProblem:
                 out.append((bc.kind, np.full(self.face_shape(face), v)))
         return out
 
+    def stop_time(self) -> float:
+        return float(self.start_time + self.nsteps * self.dt)
+
+    def time_plan(self, dump_interval: int = 1):
+        """[(t_new, dt)] per timestep, as AdvanceRichards chooses them
+        (pfsimulator/parflow_lib/solver_richards.c:3139-3230): constant dt,
+        snapped to the next dump time when within TIME_EPSILON
+        (general.h:257, FLT_EPSILON * 10) and cut to the stop time on the
+        last step; stepping continues while t < stop_time (:4616-4618)."""
+        time_eps = float(np.finfo(np.float32).eps) * 10.0
+        stop = self.stop_time()
+        dump = float(dump_interval * self.dt) if dump_interval > 0 else 0.0
+        t = float(self.start_time)
+        dump_index = 1.0
+        out = []
+        while t < stop and len(out) < 10 * self.nsteps + 10:
+            dt = float(self.dt)
+            if dump > 0:
+                print_dt = self.start_time + dump_index * dump - t
+                if (dt + time_eps) > print_dt:
+                    if abs(dt - print_dt) > time_eps:
+                        dt = print_dt
+                    dump_index += 1.0
+            if (t + dt) >= stop:
+                dt = stop - t
+            t += dt
+            out.append((t, dt))
+        return out
+
     def initial_pressure(self) -> np.ndarray:
         if self.ic is None:
             raise ValueError("problem has no initial pressure")
@@ -323,7 +352,7 @@ class RichardsProblem:
         k["TimingInfo.BaseUnit"] = float(base)
         k["TimingInfo.StartCount"] = 0
         k["TimingInfo.StartTime"] = float(self.start_time)
-        k["TimingInfo.StopTime"] = float(self.start_time + self.nsteps * self.dt)
+        k["TimingInfo.StopTime"] = self.stop_time()
         k["TimingInfo.DumpInterval"] = -1 if dump_interval < 0 else float(dump_interval * self.dt)
         k["TimeStep.Type"] = "Constant"
         k["TimeStep.Value"] = float(self.dt)

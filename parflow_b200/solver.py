@@ -1,0 +1,213 @@
+"""Host-side mirror of ParFlow's Richards nonlinear-solver interface over the
+C ABI of libpfgpu.
+
+:class:`RichardsGPU` plays the role of the PFModules on this path, with the
+same argument meaning: ``nl_function_eval`` (NlFunctionEval,
+pfsimulator/parflow_lib/nl_function_eval.c:167), ``jacobian_matvec``
+(KINSolMatVec, richards_jacobian_eval.c:165), ``pc_setup`` / ``pc_apply``
+(KinsolPC, kinsol_pc.c:58-149), ``saturation`` (Saturation,
+problem_saturation.c:108), ``newton_solve`` (KinsolNonlinSolver,
+kinsol_nonlin_solver.c:297, returning nonzero when KINSOL fails so the caller
+halves dt) and ``advance`` (the AdvanceRichards step body,
+solver_richards.c:2965-3406).
+
+Arrays are accepted as numpy arrays of shape (nz, ny, nx) (interior cells;
+converted to ParFlow's ghost-framed layout at the boundary) or as torch CUDA
+tensors already in the ghost-framed layout (passed by device pointer, no copy).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import lib as L
+from .problem import FACES, RichardsProblem
+
+_ETA = {"EtaConstant": 0, "Walker1": 1, "Walker2": 2}
+
+
+def pad(a: np.ndarray) -> np.ndarray:
+    """(nz, ny, nx) interior -> (nz+2, ny+2, nx+2) ParFlow Subvector layout."""
+    a = np.asarray(a, dtype=np.float64)
+    out = np.zeros((a.shape[0] + 2, a.shape[1] + 2, a.shape[2] + 2))
+    out[1:-1, 1:-1, 1:-1] = a
+    return out
+
+
+def unpad(a: np.ndarray) -> np.ndarray:
+    return np.ascontiguousarray(a[1:-1, 1:-1, 1:-1])
+
+
+def _ptr(a):
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr())
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class RichardsGPU:
+    """One Richards problem resident on a GPU."""
+
+    def __init__(self, prob: RichardsProblem, precision: str = "fp64", device: int = 0):
+        self.prob = prob
+        self.lib = L.load()
+        s = prob.solver
+        d = L.Desc()
+        d.abi_version = L.ABI_VERSION
+        d.nx, d.ny, d.nz = prob.nx, prob.ny, prob.nz
+        d.dx, d.dy, d.dz = prob.dx, prob.dy, prob.dz
+        d.gravity, d.viscosity, d.density = prob.gravity, prob.viscosity, prob.density
+        d.porosity, d.specific_storage = prob.porosity, prob.specific_storage
+        file_mode = prob.vg_from_file()
+        d.vg_alpha = float(prob.field3d(prob.vg_alpha).flat[0])
+        d.vg_n = float(prob.field3d(prob.vg_n).flat[0])
+        d.s_res = float(prob.field3d(prob.s_res).flat[0])
+        d.s_sat = float(prob.field3d(prob.s_sat).flat[0])
+        d.vg_from_file = 1 if file_mode else 0
+        self._zm = np.ascontiguousarray(prob.zmult())
+        d.z_mult = self._zm.ctypes.data_as(C.POINTER(C.c_double))
+        d.precision = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
+        d.residual_tol, d.step_tol = s.residual_tol, s.step_tol
+        d.max_iter, d.krylov_dim, d.max_restarts = s.max_iter, s.krylov_dim, s.max_restarts
+        d.eta_choice = _ETA[s.eta_choice]
+        d.eta_value, d.eta_alpha, d.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
+        d.mg_max_levels = s.mg_max_levels
+        d.mg_smoother = 0 if s.mg_smoother == "RedBlackGSPoint" else 1
+        d.wjacobi_weight = 1.0
+        self.desc = d
+        self.precision = precision
+        h = self.lib.pfgpu_create(C.byref(d), device)
+        if not h:
+            raise L.PfgpuError("pfgpu_create failed: " + L.last_error())
+        self.h = C.c_void_p(h)
+        self._upload_fields()
+        self.set_time(prob.start_time + prob.dt)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.pfgpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ---- setup ---------------------------------------------------------------
+    def _upload_fields(self):
+        p = self.prob
+        L.check(self.lib.pfgpu_set_field(self.h, L.FIELD_PERM_X, _ptr(pad(p.field3d(p.perm)))),
+                "set_field perm")
+        if p.vg_from_file():
+            for fid, v in ((L.FIELD_VG_ALPHA, p.vg_alpha), (L.FIELD_VG_N, p.vg_n),
+                           (L.FIELD_S_RES, p.s_res), (L.FIELD_S_SAT, p.s_sat)):
+                a = p.field3d(v)
+                if np.all(a == a.flat[0]):
+                    continue  # uniform: the descriptor scalar serves every cell
+                L.check(self.lib.pfgpu_set_field(self.h, fid, _ptr(pad(a))), "set_field vg")
+
+    def set_time(self, t: float):
+        """Upload the boundary tables BCPressure would build at time t."""
+        self.t = t
+        for f, (typ, vals) in enumerate(self.prob.bc_values(t)):
+            v = np.ascontiguousarray(vals, dtype=np.float64)
+            L.check(self.lib.pfgpu_set_bc(self.h, f, typ, _ptr(v)), f"set_bc {FACES[f]}")
+
+    # ---- function-level operators (ParFlow layout in/out) -------------------
+    def _io(self, a):
+        return a if hasattr(a, "data_ptr") else pad(a)
+
+    def nl_function_eval(self, p, p_old, s_old, dt):
+        f = np.zeros(tuple(x + 2 for x in self.prob.shape))
+        L.check(self.lib.pfgpu_nl_function_eval(self.h, _ptr(self._io(p)), _ptr(self._io(p_old)),
+                                                _ptr(self._io(s_old)), dt, _ptr(f)),
+                "nl_function_eval")
+        return unpad(f)
+
+    def saturation(self, p):
+        s = np.zeros(tuple(x + 2 for x in self.prob.shape))
+        L.check(self.lib.pfgpu_saturation(self.h, _ptr(self._io(p)), _ptr(s)), "saturation")
+        return unpad(s)
+
+    def jacobian_matvec(self, p, dt, x):
+        y = np.zeros(tuple(n + 2 for n in self.prob.shape))
+        L.check(self.lib.pfgpu_jacobian_matvec(self.h, _ptr(self._io(p)), dt, _ptr(self._io(x)),
+                                               _ptr(y)), "jacobian_matvec")
+        return unpad(y)
+
+    def pc_setup(self, p, dt):
+        L.check(self.lib.pfgpu_pc_setup(self.h, _ptr(self._io(p)), dt), "pc_setup")
+
+    def pc_apply(self, r):
+        z = np.zeros(tuple(n + 2 for n in self.prob.shape))
+        L.check(self.lib.pfgpu_pc_apply(self.h, _ptr(self._io(r)), _ptr(z)), "pc_apply")
+        return unpad(z)
+
+    def mg_levels(self):
+        n = C.c_int()
+        dims = (C.c_int * 512)()
+        L.check(self.lib.pfgpu_mg_levels(self.h, C.byref(n), dims, 128), "mg_levels")
+        return [tuple(dims[4 * l: 4 * l + 4]) for l in range(n.value)]
+
+    def newton_solve(self, p_init, p_old, s_old, dt):
+        """KinsolNonlinSolver: returns (p, status, stats); status 0 = converged."""
+        p = pad(p_init)
+        st = L.Stats()
+        rc = L.check(self.lib.pfgpu_newton_solve(self.h, _ptr(self._io(p_old)),
+                                                 _ptr(self._io(s_old)), dt, _ptr(p),
+                                                 C.byref(st)), "newton_solve")
+        return unpad(p), rc, st
+
+    # ---- device-resident stepping ---------------------------------------------
+    def set_pressure(self, p):
+        L.check(self.lib.pfgpu_set_pressure(self.h, _ptr(self._io(p))), "set_pressure")
+
+    def get_pressure(self, out=None):
+        if out is not None and hasattr(out, "data_ptr"):
+            L.check(self.lib.pfgpu_get_pressure(self.h, _ptr(out)), "get_pressure")
+            return out
+        p = np.zeros(tuple(n + 2 for n in self.prob.shape))
+        L.check(self.lib.pfgpu_get_pressure(self.h, _ptr(p)), "get_pressure")
+        return unpad(p)
+
+    def advance(self, nsteps: int = 1, dt: Optional[float] = None):
+        """Advance the device state nsteps steps; returns per-step stats."""
+        dt = self.prob.dt if dt is None else dt
+        stats = (L.Stats * max(1, nsteps))()
+        rc = L.check(self.lib.pfgpu_advance(self.h, dt, nsteps, stats), "advance")
+        if rc != L.OK:
+            raise L.PfgpuError("advance: " + L.last_error())
+        return [stats[i] for i in range(nsteps)]
+
+    def run(self, nsteps: Optional[int] = None):
+        """Solve the problem's time loop step by step (BCs re-evaluated per
+        step); returns (pressures after each step, stats per step)."""
+        prob = self.prob
+        plan = prob.time_plan()
+        nsteps = len(plan) if nsteps is None else nsteps
+        self.set_pressure(prob.initial_pressure())
+        ps, sts = [], []
+        for t, dt in plan[:nsteps]:
+            self.set_time(t)
+            sts.extend(self.advance(1, dt))
+            ps.append(self.get_pressure())
+        return ps, sts
+
+    def time_kernel(self, name: str, reps: int = 10):
+        """(ms per launch, algorithmic bytes per launch) of one library kernel."""
+        ms, by = C.c_double(), C.c_double()
+        L.check(self.lib.pfgpu_time_kernel(self.h, L.KERNELS[name], reps, C.byref(ms), C.byref(by)),
+                "time_kernel")
+        return ms.value, by.value
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.pfgpu_kernel_launches(self.h))
+
+    def stream(self) -> int:
+        return int(self.lib.pfgpu_stream(self.h) or 0)
+
+
+__all__ = ["RichardsGPU", "pad", "unpad"]
