@@ -3,6 +3,11 @@ mixed-precision GPU solver against the plain FP64 GPU form, with the HBM
 roofline of the dominant kernel and the reference CPU build beside it.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+    python bench.py --profile [--size NX,NY,NZ] --steps 1 --warmup 3
+
+--profile runs only the mixed solve and brackets its timed steps with
+cudaProfilerStart/Stop, for `ncu --profile-from-start off`; its line is a
+profiling run, not a bench value.
 
 A step is one implicit timestep (a full KINSOL Newton-Krylov solve) of the
 workload, dt = 0.05 h.  Under torchrun (N > 1) every rank solves its own
@@ -195,7 +200,8 @@ def gpu_arm(args, rank, world, local_rank):
         dist = dist_mod
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
-    prob = configs.hetero(nx=NX, ny=NY, nz=NZ, nsteps=args.warmup + args.steps + 2)
+    nx, ny, nz = args.size
+    prob = configs.hetero(nx=nx, ny=ny, nz=nz, nsteps=args.warmup + args.steps + 2)
     plan = prob.time_plan()
     ic = prob.initial_pressure()
 
@@ -217,6 +223,8 @@ def gpu_arm(args, rank, world, local_rank):
         e1 = torch.cuda.Event(enable_timing=True)
         clocks = ClockSampler(local_rank)
         clocks.start()
+        if args.profile:
+            torch.cuda.profiler.start()
         e0.record(stream)
         for i in range(args.warmup, args.warmup + args.steps):
             t, dt = plan[i]
@@ -225,6 +233,8 @@ def gpu_arm(args, rank, world, local_rank):
         e1.record(stream)
         e1.synchronize()
         torch.cuda.synchronize()
+        if args.profile:
+            torch.cuda.profiler.stop()
         ck = clocks.stop()
         ms = e0.elapsed_time(e1)
         launches = s.kernel_launches() - launches0
@@ -234,6 +244,19 @@ def gpu_arm(args, rank, world, local_rank):
             ms = float(tt.item())
         p_final = s.get_pressure()
         return s, ms, stats[args.warmup:], launches, ck, p_final
+
+    if args.profile:
+        smx, msmx, stmx, launches, clocks, _ = timed_run("mixed")
+        smx.close()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "size": [nx, ny, nz], "steps": args.steps,
+                              "ms_per_step": msmx / args.steps, "gpu_launches": int(launches),
+                              "newton_iters": sum(x.nonlin_iters for x in stmx),
+                              "gmres_iters": sum(x.lin_iters for x in stmx)}), flush=True)
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     # plain FP64 form first, then the mixed form on the same steps
     s64, ms64, st64, _, _, p64 = timed_run("fp64")
@@ -361,7 +384,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile", action="store_true",
+                    help="mixed solve only, timed steps bracketed by cudaProfilerStart/Stop")
+    ap.add_argument("--size", default=f"{NX},{NY},{NZ}",
+                    help="grid NX,NY,NZ (profiling runs only; the bench line is 512,512,50)")
     args = ap.parse_args()
+    args.size = tuple(int(v) for v in args.size.split(","))
+    if not args.profile and args.size != (NX, NY, NZ):
+        ap.error("--size is for --profile runs; the bench workload is 512x512x50")
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
