@@ -197,6 +197,30 @@ int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);
 #define PFGPU_KERNEL_MG_SETUP 5
 int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double *bytes);
 
+/* Residual F(p) without any device allocation, for callers that may not call
+ * the CUDA allocator (a host framework with a fixed device-memory budget
+ * reserved at start-up, or a latency-critical loop where cudaMalloc/cudaFree
+ * would synchronise the device).  No handle: the per-cell van Genuchten
+ * scratch lives in a static device array of the library (2^18 cells and 1024
+ * layers at most; larger grids return PFGPU_ERR_ARG).  All vectors are DEVICE
+ * pointers in dense interior layout (no ghost frame, x fastest,
+ * c = i + nx*(j + ny*k)); perm is the one permeability array used for x, y
+ * and z; vg_alpha, vg_n, s_res, s_sat are per-cell arrays or NULL for desc's
+ * scalars; bc_type[6] lives on the host and bc_values[6] are device tables
+ * laid out as for pfgpu_set_bc.  Runs on the current device and is ordered on
+ * `stream` (a cudaStream_t, NULL = legacy default stream): f is ready when the
+ * stream reaches this point.  The first call on a device resolves the scratch
+ * address (cudaGetSymbolAddress) and should come before any stream capture.
+ * Calls on one device share the scratch, so calls that may overlap on the GPU
+ * race.  Same arithmetic as pfgpu_nl_function_eval (nl_function_eval.c:167).
+ * No counterpart in the reference. */
+int pfgpu_residual_noalloc(const pfgpu_desc *desc, const double *perm,
+                           const double *vg_alpha, const double *vg_n,
+                           const double *s_res, const double *s_sat,
+                           const int *bc_type, const double *const *bc_values,
+                           const double *p, const double *p_old, const double *s_old,
+                           double dt, double *f, void *stream);
+
 /* CUDA stream the handle launches on (a cudaStream_t as an opaque pointer),
  * so callers can order their own work. */
 void *pfgpu_stream(pfgpu_handle *h);

@@ -31,6 +31,9 @@ static void set_err(const char *fmt, ...) {
   va_end(ap);
 }
 
+// lets other translation units of the library report through pfgpu_last_error
+void pfgpu::record_error(const char *msg) { set_err("%s", msg); }
+
 #define CK(call)                                                                        \
   do {                                                                                  \
     cudaError_t e_ = (call);                                                            \

@@ -135,4 +135,7 @@ void launch_axpy_gated(double *y, const double *x, const double *coef, const dou
 void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st);
 void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st);
 
+// sets the message pfgpu_last_error returns on this thread
+void record_error(const char *msg);
+
 }  // namespace pfgpu
