@@ -174,13 +174,12 @@ __device__ __forceinline__ void rb_cell(const MGLevel<T> &Lv, T *__restrict__ x,
     return;
   }
   const long long sy = nx, sz = (long long)nx * ny;
-  T s = coef(L, 1, i, j, k) * (i > 0 ? x[c - 1] : T(0)) +
-        coef(L, 2, i, j, k) * (i + 1 < nx ? x[c + 1] : T(0)) +
-        coef(L, 3, i, j, k) * (j > 0 ? x[c - sy] : T(0)) +
-        coef(L, 4, i, j, k) * (j + 1 < ny ? x[c + sy] : T(0)) +
-        coef(L, 5, i, j, k) * (k > 0 ? x[c - sz] : T(0)) +
-        coef(L, 6, i, j, k) * (k + 1 < Lv.nz ? x[c + sz] : T(0));
-  x[c] = (b[c] - s) / L.a0[c];
+  x[c] = rb_update<T>(L.a0[c], b[c], coef(L, 1, i, j, k), i > 0 ? x[c - 1] : T(0),
+                      coef(L, 2, i, j, k), i + 1 < nx ? x[c + 1] : T(0),
+                      coef(L, 3, i, j, k), j > 0 ? x[c - sy] : T(0),
+                      coef(L, 4, i, j, k), j + 1 < ny ? x[c + sy] : T(0),
+                      coef(L, 5, i, j, k), k > 0 ? x[c - sz] : T(0),
+                      coef(L, 6, i, j, k), k + 1 < Lv.nz ? x[c + sz] : T(0));
 }
 
 template <typename T>
@@ -189,121 +188,6 @@ __global__ void k_rb_sweep(MGLevel<T> Lv, T *__restrict__ x, const T *__restrict
   int q, j, k;
   thread_ijk(q, j, k);
   rb_cell(Lv, x, b, colour, init, q, j, k);
-}
-
-// ---------------------------------------------------------------------------
-// Fused symmetric red/black Gauss-Seidel (red, black, red) in one pass.
-//
-// A block owns a TX x TY column of the level and marches its z planes.  The
-// three colour sweeps run as a software pipeline lagged by one plane:
-// red sweep 1 on plane s, the black sweep on plane s-1, red sweep 2 on plane
-// s-2, each on the data staged in shared memory for the tile plus a halo
-// (3 cells for sweep 1, 2 for the black sweep, 1 for sweep 2, so each stage
-// has the neighbours it reads).  Halo cells are recomputed by every block that
-// stages them, from the same inputs, so the values agree bit for bit with the
-// unfused sweeps (k_rb_sweep) and between blocks.  x is read from `xin` and
-// written to `xout` (distinct buffers): no block ever reads a value another
-// block has already updated.  Each cell's arithmetic is exactly rb_cell's.
-// ---------------------------------------------------------------------------
-template <typename T, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY) k_rbr_fused(MGLevel<T> Lv, const T *__restrict__ xin,
-                                                       T *__restrict__ xout,
-                                                       const T *__restrict__ b, int zero) {
-  constexpr int H = 3;
-  constexpr int RX = TX + 2 * H, RY = TY + 2 * H, RP = RX * RY;
-  constexpr int NTH = TX * TY;
-  constexpr int NS = 6;                      // ring: planes s-3 .. s+2
-  constexpr int NL = (RP + NTH - 1) / NTH;   // staged positions per thread
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  T *sm = reinterpret_cast<T *>(smem_raw);
-  // slot record: C E N U b x, RP each
-  auto slot = [&](int k) { return sm + (size_t)(((k % NS) + NS) % NS) * 6 * RP; };
-  const int nx = Lv.nx, ny = Lv.ny, nz = Lv.nz;
-  const int x0 = blockIdx.x * TX - H, y0 = blockIdx.y * TY - H;
-  const long long sz = (long long)nx * ny;
-  const T *A0 = Lv.a[0], *AE = Lv.a[1], *AN = Lv.a[2], *AU = Lv.a[3];
-
-  // staged positions of this thread (fixed for the whole column)
-  int lq[NL];
-  long long lg[NL];
-  bool lin[NL];
-#pragma unroll
-  for (int r = 0; r < NL; r++) {
-    const int q = threadIdx.x + r * NTH;
-    lq[r] = q;
-    const int ix = x0 + q % RX, iy = y0 + q / RX;
-    lin[r] = q < RP && ix >= 0 && iy >= 0 && ix < nx && iy < ny;
-    lg[r] = lin[r] ? ix + (long long)nx * iy : 0;
-  }
-  T pf[NL][6];
-  auto fetch = [&](int k) {  // global -> registers
-    const bool kin = k >= 0 && k < nz;
-#pragma unroll
-    for (int r = 0; r < NL; r++) {
-      const bool in = kin && lin[r];
-      const long long g = lg[r] + sz * k;
-      pf[r][0] = in ? A0[g] : T(0);
-      pf[r][1] = in ? AE[g] : T(0);
-      pf[r][2] = in ? AN[g] : T(0);
-      pf[r][3] = in ? AU[g] : T(0);
-      pf[r][4] = in ? b[g] : T(0);
-      pf[r][5] = (in && !zero) ? xin[g] : T(0);
-    }
-  };
-  auto stash = [&](int k) {  // registers -> ring slot of plane k
-    T *rec = slot(k);
-#pragma unroll
-    for (int r = 0; r < NL; r++)
-      if (lq[r] < RP) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) rec[a * RP + lq[r]] = pf[r][a];
-      }
-  };
-  // one colour on plane k over the region tile+h
-  auto stage = [&](int k, int colour, int h, int init, bool store) {
-    const int w = TX + 2 * h, cnt = w * (TY + 2 * h);
-    const T *rec = slot(k), *recl = slot(k - 1), *recu = slot(k + 1);
-    const T *c = rec, *e = rec + RP, *n = rec + 2 * RP, *u = rec + 3 * RP, *bb = rec + 4 * RP;
-    T *xx = const_cast<T *>(rec) + 5 * RP;
-    const T *ul = recl + 3 * RP, *xl = recl + 5 * RP, *xu = recu + 5 * RP;
-    const int want = colour == 0 ? 1 : 0;
-    for (int t = threadIdx.x; t < cnt; t += NTH) {
-      const int lx = t % w + (H - h), ly = t / w + (H - h);
-      const int i = x0 + lx, j = y0 + ly;
-      if (i < 0 || j < 0 || i >= nx || j >= ny || ((i + j + k) & 1) != want) continue;
-      const int q = lx + RX * ly;
-      T v;
-      if (init) {
-        v = bb[q] / c[q];
-      } else {
-        const T s = e[q - 1] * xx[q - 1] + e[q] * xx[q + 1] + n[q - RX] * xx[q - RX] +
-                    n[q] * xx[q + RX] + ul[q] * xl[q] + u[q] * xu[q];
-        v = (bb[q] - s) / c[q];
-      }
-      xx[q] = v;
-      if (store && lx >= H && ly >= H && lx < H + TX && ly < H + TY)
-        xout[i + (long long)nx * j + sz * k] = v;
-    }
-  };
-
-  // prologue: planes -3 .. 1 resident, plane 2 in flight
-  for (int k = -3; k <= 1; k++) {
-    fetch(k);
-    stash(k);
-  }
-  fetch(2);
-  __syncthreads();
-  for (int s = 0; s < nz + 2; s++) {
-    if (s < nz) stage(s, 0, 2, zero, false);                  // red, sweep 1
-    __syncthreads();
-    if (s - 1 >= 0 && s - 1 < nz) stage(s - 1, 1, 1, 0, true);  // black
-    __syncthreads();
-    if (s - 2 >= 0) stage(s - 2, 0, 0, 0, true);             // red, sweep 2
-    // plane s+2 lands in the slot of plane s-4 (no longer read); fetch s+3
-    stash(s + 2);
-    if (s + 3 <= nz + 1) fetch(s + 3);
-    __syncthreads();
-  }
 }
 
 // weighted Jacobi (pfsimulator/parflow_lib/w_jacobi.c:120-290)
@@ -601,33 +485,12 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
   rb_sweep(L, x, b, 1, 0, st);
   rb_sweep(L, x, b, 0, 0, st);
 }
-template <typename T>
-constexpr int rbr_tx() { return 32; }
-template <typename T>
-constexpr int rbr_ty() { return 8; }
-template <typename T>
-size_t rbr_smem() {
-  constexpr int RX = rbr_tx<T>() + 6, RY = rbr_ty<T>() + 6;
-  return (size_t)6 * 6 * RX * RY * sizeof(T);
-}
 // opt the fused smoother into its dynamic shared memory (> 48 KB); called
 // once per device before any launch or graph capture
 cudaError_t mg_prepare_kernels() {
-  cudaError_t e = cudaFuncSetAttribute(k_rbr_fused<float, rbr_tx<float>(), rbr_ty<float>()>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)rbr_smem<float>());
+  cudaError_t e = rbr_fused_prepare<float>();
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_rbr_fused<double, rbr_tx<double>(), rbr_ty<double>()>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize,
-                              (int)rbr_smem<double>());
-}
-
-template <typename T>
-void launch_rbr_fused(const MGLevel<T> &L, const T *xin, T *xout, const T *b, int zero,
-                      cudaStream_t st) {
-  constexpr int TX = rbr_tx<T>(), TY = rbr_ty<T>();
-  dim3 grid((L.nx + TX - 1) / TX, (L.ny + TY - 1) / TY);
-  k_rbr_fused<T, TX, TY><<<grid, TX * TY, rbr_smem<T>(), st>>>(L, xin, xout, b, zero);
+  return rbr_fused_prepare<double>();
 }
 
 template <typename T>
@@ -675,8 +538,6 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
                                          T *, cudaStream_t);                                  \
   template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *,         \
                                       cudaStream_t);                                          \
-  template void launch_rbr_fused<T>(const MGLevel<T> &, const T *, T *, const T *, int,       \
-                                    cudaStream_t);                                            \
   template void launch_setup_tail<T>(const MGLevel<T> *, int, int, cudaStream_t);
 INST(double)
 INST(float)

@@ -11,6 +11,7 @@
 
 #include <cfloat>
 #include <cmath>
+#include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -66,15 +67,21 @@ struct MG {
   MGLevel<T> *Ldev = nullptr;  // device copy of the level table (tail kernels)
   int tail = 0;                // first level run by the single-block tail kernels
   T *wtmp = nullptr;           // Jacobi temp (finest size)
-  bool fused = false;          // fused red/black/red smoother on grid levels
+  std::vector<char> fused;     // level smoothed by the fused red/black/red kernel
+  std::vector<RbrMaps> maps;   // its tensor maps (input iterate = x)
+  int *kerr = nullptr;         // pipeline-wait error word of the fused kernel
+  // buffer holding the smoothed result of level l (post-smoother output)
+  T *res(int l) const { return (l < (int)fused.size() && fused[l]) ? L[l].x2 : L[l].x; }
 };
 
 // Tuning (read once per handle from the environment; all variants compute
 // the same V-cycle):
 //   PFGPU_TAIL_CELLS  levels at or below this many cells run inside the
 //                     single-block tail kernels (default 1024)
-//   PFGPU_FUSED_RBR   1: fused red/black/red smoother kernel, 0: one kernel
-//                     per colour sweep (default 0)
+//   PFGPU_RBR_FUSED_CELLS  grid levels with at least this many cells (and a
+//                     row pitch TMA can address) use the TMA-pipelined fused
+//                     red/black/red smoother; the rest one kernel per colour
+//                     sweep (default: no level; the fused kernel is slower)
 static long long env_ll(const char *name, long long dflt) {
   const char *v = getenv(name);
   return v && *v ? atoll(v) : dflt;
@@ -122,11 +129,27 @@ struct pfgpu_handle {
   bool pc_ready = false;
   long long launches = 0;
   int jac_valid = 0;
+  int *kerr = nullptr;   // device error word of the pipelined kernels
+  int *hkerr = nullptr;  // pinned host mirror
 };
 
 // ---------------------------------------------------------------------------
 // helpers
 // ---------------------------------------------------------------------------
+// Error word of the pipelined kernels: nonzero once a bounded pipeline wait
+// expired (the results of that launch are then invalid).  Cleared when read.
+static int check_kernel_error(pfgpu_handle *h) {
+  CK(cudaMemcpyAsync(h->hkerr, h->kerr, sizeof(int), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  if (*h->hkerr) {
+    *h->hkerr = 0;
+    CK(cudaMemsetAsync(h->kerr, 0, sizeof(int), h->st));
+    set_err("a pipelined smoother kernel gave up waiting for its TMA copies");
+    return PFGPU_ERR_CUDA;
+  }
+  return 0;
+}
+
 static bool is_device_ptr(const void *p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
@@ -254,11 +277,10 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   const int nl = (int)mg.L.size();
   const int sk = smoother == 1 ? 2 : 3;
   const int first = mg.tail;
-  const bool fused = smoother == 0 && mg.fused;
   for (int l = 0; l < first; l++) {
     MGLevel<T> &Ll = mg.L[l];
-    if (fused) {
-      launch_rbr_fused<T>(Ll, Ll.x, Ll.x, Ll.b, 1, st);  // zero guess: xin unused
+    if (mg.fused[l]) {
+      launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x, 1, mg.kerr, st);  // zero guess: x not read
       k++;
     } else {
       launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st);
@@ -274,10 +296,9 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
     const MGLevel<T> &C = mg.L[l + 1];
-    const T *ec = (fused && l + 1 < first) ? C.x2 : C.x;  // where level l+1's result lives
-    launch_mg_prolong_add<T>(Ll, C, ec, Ll.x, st);
-    if (fused) {
-      launch_rbr_fused<T>(Ll, Ll.x, Ll.x2, Ll.b, 0, st);
+    launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st);
+    if (mg.fused[l]) {
+      launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x2, 0, mg.kerr, st);
       k += 2;
     } else {
       launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st);
@@ -289,8 +310,8 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
 
 // buffer holding the level-0 result of a V-cycle
 template <typename T>
-static T *vcycle_out(MG<T> &mg, int smoother) {
-  return (smoother == 0 && mg.fused && mg.tail > 0) ? mg.L[0].x2 : mg.L[0].x;
+static T *vcycle_out(MG<T> &mg, int) {
+  return mg.res(0);
 }
 
 static long long vcycle_launch(pfgpu_handle *h) {
@@ -742,17 +763,30 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   if (dalloc(&mg.wtmp, mg.L[0].n)) return PFGPU_ERR_NOMEM;
   // first level small enough for the single-block tail kernels
   mg.tail = nl - 1;
-  mg.fused = env_ll("PFGPU_FUSED_RBR", 0) != 0;
   const long long tail_cells = env_ll("PFGPU_TAIL_CELLS", 1024);
   for (int l = 0; l < nl; l++)
     if (mg.L[l].n <= tail_cells) {
       mg.tail = l;
       break;
     }
+  // grid levels large enough for the fused smoother get an output buffer
+  // distinct from the input iterate
+  const long long fused_cells = env_ll("PFGPU_RBR_FUSED_CELLS", LLONG_MAX);
+  mg.fused.assign(nl, 0);
+  mg.maps.resize(nl);
   for (int l = 0; l < mg.tail; l++) {
-    if (dalloc(&mg.L[l].x2, mg.L[l].n)) return PFGPU_ERR_NOMEM;
-    CK(cudaMemset(mg.L[l].x2, 0, mg.L[l].n * sizeof(T)));
+    MGLevel<T> &L = mg.L[l];
+    if (h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells || !rbr_fused_eligible(L))
+      continue;
+    if (dalloc(&L.x2, L.n)) return PFGPU_ERR_NOMEM;
+    CK(cudaMemset(L.x2, 0, L.n * sizeof(T)));
+    if (make_rbr_maps<T>(L, L.x, &mg.maps[l]) != 0) {
+      set_err("tensor map creation failed for multigrid level %d", l);
+      return PFGPU_ERR_CUDA;
+    }
+    mg.fused[l] = 1;
   }
+  mg.kerr = h->kerr;
   CK(cudaMalloc((void **)&mg.Ldev, nl * sizeof(MGLevel<T>)));
   CK(cudaMemcpy(mg.Ldev, mg.L.data(), nl * sizeof(MGLevel<T>), cudaMemcpyHostToDevice));
   h->nlev = nl;
@@ -815,6 +849,11 @@ static int create_impl(pfgpu_handle *h) {
   CK(cudaMemset(h->rb.ticket, 0, sizeof(unsigned int)));
   h->rb.blocks = reduce_blocks();
   CK(cudaMallocHost((void **)&h->hsc, 64 * sizeof(double)));
+  CK(cudaMalloc((void **)&h->kerr, sizeof(int)));
+  CK(cudaMemset(h->kerr, 0, sizeof(int)));
+  CK(cudaMallocHost((void **)&h->hkerr, sizeof(int)));
+  *h->hkerr = 0;
+
   // Jacobian storage
   if (h->mixed) {
     float **J[] = {&h->Jf.c, &h->Jf.w, &h->Jf.e, &h->Jf.s, &h->Jf.n, &h->Jf.l, &h->Jf.u};
@@ -867,6 +906,9 @@ static void destroy_impl(pfgpu_handle *h) {
   for (int f = 0; f < 6; f++) cudaFree(h->bcv[f]);
   for (auto v : h->V) cudaFree(v);
   cudaFree(h->rb.ticket);
+  cudaFree(h->kerr);
+  if (h->hkerr) cudaFreeHost(h->hkerr);
+
   double *jd[] = {h->Jd.c, h->Jd.w, h->Jd.e, h->Jd.s, h->Jd.n, h->Jd.l, h->Jd.u};
   for (double *a : jd) cudaFree(a);
   float *jf[] = {h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
@@ -1025,6 +1067,7 @@ int pfgpu_pc_apply(pfgpu_handle *h, const double *r, double *z) {
   CK(cudaSetDevice(h->device));
   if (in_vec(h, r, h->vtemp)) return PFGPU_ERR_CUDA;
   if (pc_apply_dense(h, h->vtemp, h->vtemp)) return PFGPU_ERR_CUDA;
+  if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
   return out_vec(h, h->vtemp, z);
 }
 
@@ -1037,6 +1080,7 @@ int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old
   pfgpu_stats local;
   int rc = newton(h, dt, stats ? stats : &local);
   if (rc < 0) return rc;
+  if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
   int rc2 = out_vec(h, h->u, p);
   return rc2 ? rc2 : rc;
 }
@@ -1070,7 +1114,8 @@ int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats) {
     for (int fail = 0; fail < 3; fail++) {
       rc = newton(h, dts, &st);
       if (rc < 0) return rc;
-      if (rc == PFGPU_OK) break;
+      if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
+          if (rc == PFGPU_OK) break;
       CK(cudaMemcpyAsync(h->u, h->p_old, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
       h->vg_for = nullptr;
       dts *= 0.5;
@@ -1134,13 +1179,15 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
       case PFGPU_KERNEL_MATVEC: matvec(h, h->pp, h->bb); break;
       case PFGPU_KERNEL_RB_SWEEP:  // the finest level's post-smoother as the V-cycle runs it
         if (h->mixed) {
-          MGLevel<float> &L = h->mgf.L[0];
-          if (h->mgf.fused && L.x2) launch_rbr_fused<float>(L, L.x, L.x2, L.b, 0, h->st);
-          else launch_mg_smooth<float>(L, L.x, L.b, 0, 0, 1.0, h->mgf.wtmp, h->st);
+          MG<float> &mg = h->mgf;
+          MGLevel<float> &L = mg.L[0];
+          if (!mg.fused.empty() && mg.fused[0]) launch_rbr_fused<float>(L, mg.maps[0], L.x2, 0, mg.kerr, h->st);
+          else launch_mg_smooth<float>(L, L.x, L.b, 0, 0, 1.0, mg.wtmp, h->st);
         } else {
-          MGLevel<double> &L = h->mgd.L[0];
-          if (h->mgd.fused && L.x2) launch_rbr_fused<double>(L, L.x, L.x2, L.b, 0, h->st);
-          else launch_mg_smooth<double>(L, L.x, L.b, 0, 0, 1.0, h->mgd.wtmp, h->st);
+          MG<double> &mg = h->mgd;
+          MGLevel<double> &L = mg.L[0];
+          if (!mg.fused.empty() && mg.fused[0]) launch_rbr_fused<double>(L, mg.maps[0], L.x2, 0, mg.kerr, h->st);
+          else launch_mg_smooth<double>(L, L.x, L.b, 0, 0, 1.0, mg.wtmp, h->st);
         }
         h->launches++;
         break;
@@ -1164,6 +1211,7 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
   cudaEventDestroy(e1);
   *ms = (double)t / reps;
   if (bytes) *bytes = kernel_bytes(h, kernel);
+  if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
   h->jac_valid = 0;
   return PFGPU_OK;
 }

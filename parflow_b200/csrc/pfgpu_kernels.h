@@ -1,6 +1,7 @@
 // Kernel launch interfaces shared between the library's translation units.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "pfgpu_device.cuh"
@@ -46,9 +47,63 @@ struct MGLevel {
   int dir;          // coarsening direction to the next level (-1 on the coarsest)
   T *a[4];          // C E N U
   T *x, *b, *t;
-  T *x2;            // output of the fused post-smoother (levels run by grid kernels)
+  T *x2;            // output of the fused post-smoother (levels it runs on)
   T *p1, *p2;       // prolongation weights (fine points of this level)
 };
+
+// One Gauss-Seidel point update x = (b - sum_nb a_nb x_nb) / a0, the six
+// neighbour products accumulated in the order W E S N L U with explicit fused
+// multiply-adds, so that every smoother kernel rounds identically.
+template <typename T>
+__device__ __forceinline__ T rb_update(T c, T b, T w, T xw, T e, T xe, T s, T xs, T n, T xn,
+                                       T l, T xl, T u, T xu) {
+  T acc = w * xw;
+  acc = fma(e, xe, acc);
+  acc = fma(s, xs, acc);
+  acc = fma(n, xn, acc);
+  acc = fma(l, xl, acc);
+  acc = fma(u, xu, acc);
+  return (b - acc) / c;
+}
+
+// Fused red/black/red smoother (mg_rbr.cu, TMA pipeline): tile, ring size
+// and threads per storage type, box halo (x rounded up to the 16-byte rule)
+// and the six tensor maps C E N U b x of one level.  The float tile is a
+// compile-time tuning knob (PFGPU_RBR_F32_TY / _NS / _NTH).
+template <typename T>
+struct RbrTile;
+#ifndef PFGPU_RBR_F32_TY
+#define PFGPU_RBR_F32_TY 16
+#define PFGPU_RBR_F32_NS 10
+#define PFGPU_RBR_F32_NTH 1024
+#endif
+template <>
+struct RbrTile<float> {
+  static constexpr int TX = 32, TY = PFGPU_RBR_F32_TY, NS = PFGPU_RBR_F32_NS,
+                       NTH = PFGPU_RBR_F32_NTH;
+};
+template <>
+struct RbrTile<double> {
+  static constexpr int TX = 32, TY = 8, NS = 8, NTH = 512;
+};
+constexpr int RBR_HX = 4, RBR_HY = 3;
+struct RbrMaps {
+  CUtensorMap m[6];
+};
+// level storage the TMA smoother can address (row pitch a multiple of 16 B)
+template <typename T>
+bool rbr_fused_eligible(const MGLevel<T> &L);
+// tensor maps of level L with input iterate xin; 0 on success
+template <typename T>
+int make_rbr_maps(const MGLevel<T> &L, const T *xin, RbrMaps *out);
+template <typename T>
+cudaError_t rbr_fused_prepare();
+// red, black, red on level L: b and the coefficients from the maps, the input
+// iterate from maps.m[5] (not read when zero != 0), the result to xout, which
+// must not be the input iterate; *err is set if a pipeline wait expires
+template <typename T>
+void launch_rbr_fused(const MGLevel<T> &L, const RbrMaps &maps, T *xout, int zero, int *err,
+                      cudaStream_t st);
 
 template <typename T>
 void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st);
@@ -58,11 +113,6 @@ template <typename T>
 void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st);
 cudaError_t mg_prepare_kernels();
-// symmetric red/black Gauss-Seidel (red, black, red) in one fused pass,
-// x read from xin (ignored when zero) and written to xout (xin != xout)
-template <typename T>
-void launch_rbr_fused(const MGLevel<T> &L, const T *xin, T *xout, const T *b, int zero,
-                      cudaStream_t st);
 template <typename T>
 void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st);
 template <typename T>
