@@ -35,6 +35,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "Richards steps/s @13M cells: mixed vs FP64 on B200 at ≤1e-8 rel err; HBM %"
 NX, NY, NZ = 512, 512, 50
+# DRAM bytes (read + write) per cell of one k_rb_sweep launch, from the ncu
+# capture summarised in profiles/k_rb_sweep_hetero_256x256x50_mixed.md
+RB_SWEEP_DRAM_BYTES_PER_CELL = 24.78
 
 
 def peaks():
@@ -264,16 +267,20 @@ def gpu_arm(args, rank, world, local_rank):
     smx, msmx, stmx, launches, clocks, pmx = timed_run("mixed")
     rel_err = float(np.abs(pmx - p64).max() / np.abs(p64).max())
 
-    # roofline of the dominant kernel (one red/black colour sweep of the
-    # finest multigrid level: the smoother carries the bulk of the V-cycle)
+    # roofline of the dominant kernel: k_rb_sweep, one red/black colour sweep
+    # (37% of a timestep's GPU time in the launch list); timed on the finest
+    # level, 13.1M cells, 28 algorithmic bytes per cell in f32
     kern = {}
-    for name in ("rb_sweep", "matvec", "residual", "jacobian", "vcycle", "mg_setup"):
+    for name in ("colour_sweep", "rb_smooth", "matvec", "residual", "jacobian", "vcycle",
+                 "mg_setup"):
         kms, kbytes = smx.time_kernel(name, reps=20)
         kern[name] = (kms, kbytes)
-    dom = "rb_sweep"
+    dom = "colour_sweep"
     dms, dbytes = kern[dom]
     peak, peak_kind = peaks()
     achieved = dbytes / (dms * 1e-3) / 1e9
+    traffic = None if RB_SWEEP_DRAM_BYTES_PER_CELL is None else \
+        RB_SWEEP_DRAM_BYTES_PER_CELL * NX * NY * NZ
 
     # end to end through the C ABI with host buffers: one pfgpu_newton_solve
     # (p_old, s_old, p in; p out) and one pfgpu_saturation per step
@@ -355,9 +362,10 @@ def gpu_arm(args, rank, world, local_rank):
             "newton_iters_per_step": newton / max(1, len(stmx)),
             "gmres_iters_per_step": sum(x.lin_iters for x in stmx) / max(1, len(stmx)),
             "cell_newton_updates_per_s": NX * NY * NZ * newton * world / (msmx * 1e-3),
-            "roofline": {"bound": "hbm", "kernel": "red/black smoother colour sweep, finest level (f32)",
+            "roofline": {"bound": "hbm",
+                         "kernel": "k_rb_sweep: one red/black colour sweep, finest level (f32)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None,
+                         "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
                          "bytes_per_launch": dbytes, "ms_per_launch": dms},
             "kernels": {k: {"ms": v[0], "alg_bytes": v[1],

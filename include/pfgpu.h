@@ -186,8 +186,10 @@ int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);
  * algorithmic HBM bytes per launch (each distinct per-cell array it needs
  * counted once; uniform fields count zero) in *bytes.
  * kernel: 0 residual (with its van Genuchten pass), 1 Jacobian + PC matrix
- * assembly, 2 Jacobian matvec, 3 the fused red/black/red smoother on the
- * finest level, 4 one multigrid V-cycle (all levels), 5 multigrid setup.
+ * assembly, 2 Jacobian matvec, 3 the symmetric red/black/red smoother on the
+ * finest level as the V-cycle runs it (bytes: each array once, the one-pass
+ * ideal), 4 one multigrid V-cycle (all levels), 5 multigrid setup, 6 one red
+ * colour sweep on the finest level (a single k_rb_sweep launch).
  * Benchmark support; no counterpart in the reference. */
 #define PFGPU_KERNEL_RESIDUAL 0
 #define PFGPU_KERNEL_JACOBIAN 1
@@ -195,6 +197,7 @@ int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);
 #define PFGPU_KERNEL_RB_SWEEP 3
 #define PFGPU_KERNEL_VCYCLE 4
 #define PFGPU_KERNEL_MG_SETUP 5
+#define PFGPU_KERNEL_COLOUR_SWEEP 6
 int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double *bytes);
 
 /* Residual F(p) without any device allocation, for callers that may not call

@@ -1159,7 +1159,8 @@ static double kernel_bytes(pfgpu_handle *h, int kernel) {
     case PFGPU_KERNEL_RESIDUAL: return N * (8.0 * 4 + kf + vg);         // p p_old s_old f
     case PFGPU_KERNEL_JACOBIAN: return N * (8.0 + kf + vg + 7 * wJ + 4 * wJ);
     case PFGPU_KERNEL_MATVEC: return N * (7 * wJ + 8.0 + 8.0);
-    case PFGPU_KERNEL_RB_SWEEP: return N * (4 * wJ + wJ + 2 * wJ);      // C E N U, b, x in + out
+    case PFGPU_KERNEL_RB_SWEEP:                                          // C E N U, b, x in + out
+    case PFGPU_KERNEL_COLOUR_SWEEP: return N * (4 * wJ + wJ + 2 * wJ);
     default: return 0.0;
   }
 }
@@ -1194,6 +1195,16 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
       case PFGPU_KERNEL_VCYCLE:
         cudaGraphLaunch(h->vgraph, h->st);
         h->launches += h->graph_nodes;
+        break;
+      case PFGPU_KERNEL_COLOUR_SWEEP:  // one red sweep of the finest level
+        if (h->mixed) {
+          MGLevel<float> &L = h->mgf.L[0];
+          launch_mg_smooth<float>(L, L.x, L.b, 0, 2, 1.0, h->mgf.wtmp, h->st);
+        } else {
+          MGLevel<double> &L = h->mgd.L[0];
+          launch_mg_smooth<double>(L, L.x, L.b, 0, 2, 1.0, h->mgd.wtmp, h->st);
+        }
+        h->launches++;
         break;
       case PFGPU_KERNEL_MG_SETUP:
         h->launches += h->mixed ? mg_setup_T<float>(h->mgf, h->st) : mg_setup_T<double>(h->mgd, h->st);

@@ -59,7 +59,8 @@ EXPORTS = ["pfgpu_create", "pfgpu_destroy", "pfgpu_last_error", "pfgpu_set_field
            "pfgpu_set_pressure", "pfgpu_get_pressure", "pfgpu_advance", "pfgpu_mg_levels",
            "pfgpu_stream", "pfgpu_kernel_launches", "pfgpu_time_kernel",
            "pfgpu_residual_noalloc"]
-KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_sweep": 3, "vcycle": 4, "mg_setup": 5}
+KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_smooth": 3, "vcycle": 4, "mg_setup": 5,
+           "colour_sweep": 6}
 
 _lib = None
 
