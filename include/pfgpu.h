@@ -176,6 +176,18 @@ int pfgpu_set_pressure(pfgpu_handle *h, const double *p);
 int pfgpu_get_pressure(pfgpu_handle *h, double *p);
 int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats);
 
+/* Ensemble stepping: advances n independent problems (one handle each, same
+ * semantics as pfgpu_advance, members[m] by dt[m]) concurrently, their
+ * kernels overlapping on the GPU through the handles' own streams, driven by
+ * nthreads host threads (0 = one per member).  stats (may be NULL) receives
+ * n * nsteps entries, member-major; status[m] receives each member's
+ * pfgpu_advance result.  Returns PFGPU_OK when every member succeeded,
+ * otherwise the first error (or PFGPU_NOT_CONVERGED).  The members must be
+ * distinct handles.  The reference runs ensemble members as separate runs;
+ * no counterpart in its API. */
+int pfgpu_ensemble_advance(pfgpu_handle *const *members, int n, const double *dt, int nsteps,
+                           int nthreads, pfgpu_stats *stats, int *status);
+
 /* Number of multigrid levels and their sizes/coarsening directions
  * (mg_semi.c:858-923); dims has 4*levels ints (nx, ny, nz, dir). */
 int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);

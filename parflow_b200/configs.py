@@ -8,6 +8,10 @@
 * ``hetero`` (config 2): 512x512x50 heterogeneous box, sigma_lnK 1.5,
   correlation 32x32x4 cells, alpha perturbed +-20 % per cell (per-cell VG
   files), 20 steps of 0.05 h.
+* ``ensemble_member`` / ``ensemble`` (config 3): 48 members of uneven size,
+  per member nx = ny from {64, 96, 128, 192}, nz from {16, 24, 32, 40},
+  sigma_lnK ~ U[0.5, 2], alpha ~ U[0.5, 4], n ~ U[1.4, 3], top flux ~
+  U[-0.1, -0.02] m/h, config-0 physics otherwise, 10 steps of 0.1 h.
 * ``adjoint_box`` (config 4): 128x128x32 with config-0 physics, 20 steps.
 
 Every size can be scaled down (``nx``, ``ny``, ``nz`` overrides) for parity
@@ -65,8 +69,36 @@ def hetero(nx=512, ny=512, nz=50, nsteps=20, dt=0.05, seed=2,
     return p
 
 
+ENSEMBLE_NXY = (64, 96, 128, 192)
+ENSEMBLE_NZ = (16, 24, 32, 40)
+
+
+def ensemble_member(m: int, seed: int = 3, nxy=ENSEMBLE_NXY, nz=ENSEMBLE_NZ,
+                    nsteps: int = 10, solver: SolverSettings = None) -> RichardsProblem:
+    """Member m of the ensemble: size and parameters drawn from its own seeded
+    stream (``nxy`` / ``nz`` choose the size sets, smaller ones for tests)."""
+    rng = np.random.default_rng(seed * 100003 + m)
+    n_xy = int(rng.choice(np.asarray(nxy)))
+    n_z = int(rng.choice(np.asarray(nz)))
+    sigma = float(rng.uniform(0.5, 2.0))
+    alpha = float(rng.uniform(0.5, 4.0))
+    vg_n = float(rng.uniform(1.4, 3.0))
+    top = float(rng.uniform(-0.1, -0.02))
+    p = box(nx=n_xy, ny=n_xy, nz=n_z, nsteps=nsteps, dt=0.1, seed=seed * 1009 + m,
+            sigma=sigma, solver=solver)
+    p.vg_alpha = alpha
+    p.vg_n = vg_n
+    p.bc["z_upper"] = BC(BC_FLUX, (top,))
+    p.name = f"member{m}"
+    return p
+
+
+def ensemble(n: int = 48, seed: int = 3, **kw):
+    return [ensemble_member(m, seed=seed, **kw) for m in range(n)]
+
+
 def adjoint_box(nx=128, ny=128, nz=32, nsteps=20, seed=4) -> RichardsProblem:
     return box(nx=nx, ny=ny, nz=nz, nsteps=nsteps, dt=0.1, seed=seed)
 
 
-__all__ = ["box", "hetero", "adjoint_box"]
+__all__ = ["box", "hetero", "ensemble_member", "ensemble", "adjoint_box"]

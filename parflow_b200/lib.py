@@ -58,7 +58,7 @@ EXPORTS = ["pfgpu_create", "pfgpu_destroy", "pfgpu_last_error", "pfgpu_set_field
            "pfgpu_pc_setup", "pfgpu_pc_apply", "pfgpu_saturation", "pfgpu_newton_solve",
            "pfgpu_set_pressure", "pfgpu_get_pressure", "pfgpu_advance", "pfgpu_mg_levels",
            "pfgpu_stream", "pfgpu_kernel_launches", "pfgpu_time_kernel",
-           "pfgpu_residual_noalloc"]
+           "pfgpu_residual_noalloc", "pfgpu_ensemble_advance"]
 KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_smooth": 3, "vcycle": 4, "mg_setup": 5,
            "colour_sweep": 6}
 
@@ -99,6 +99,8 @@ def load(path: str = LIB_PATH):
     L.pfgpu_kernel_launches.restype = C.c_longlong
     L.pfgpu_time_kernel.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_double),
                                     C.POINTER(C.c_double)]
+    L.pfgpu_ensemble_advance.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(C.c_double), C.c_int,
+                                         C.c_int, C.POINTER(Stats), C.POINTER(C.c_int)]
     L.pfgpu_residual_noalloc.argtypes = [C.POINTER(Desc)] + [vp] * 5 + \
         [C.POINTER(C.c_int), C.POINTER(C.c_void_p)] + [vp] * 3 + [C.c_double, vp, vp]
     _lib = L

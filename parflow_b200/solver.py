@@ -211,3 +211,25 @@ class RichardsGPU:
 
 
 __all__ = ["RichardsGPU", "pad", "unpad"]
+
+
+def ensemble_advance(members, nsteps: int = 1, dts=None, threads: int = 0):
+    """Advance several :class:`RichardsGPU` problems concurrently by nsteps
+    steps each (pfgpu_ensemble_advance): every member on its own stream,
+    ``threads`` host threads driving their Newton loops (0 = one per member).
+    Boundary tables and pressures must already be set.  Returns the per-member
+    lists of per-step stats; raises on an error or a step that fails."""
+    n = len(members)
+    if n == 0:
+        return []
+    lib = members[0].lib
+    dts = [m.prob.dt for m in members] if dts is None else list(dts)
+    handles = (C.c_void_p * n)(*[m.h.value for m in members])
+    dt_arr = (C.c_double * n)(*dts)
+    per = max(1, nsteps)
+    stats = (L.Stats * (n * per))()
+    status = (C.c_int * n)()
+    rc = lib.pfgpu_ensemble_advance(handles, n, dt_arr, nsteps, threads, stats, status)
+    if rc != L.OK:
+        raise L.PfgpuError(f"ensemble_advance failed ({rc}): {L.last_error()}")
+    return [[stats[m * per + s] for s in range(nsteps)] for m in range(n)]

@@ -137,3 +137,19 @@ def test_create_rejects_bad_descriptor():
     d.nx = d.ny = d.nz = 1
     assert not L.pfgpu_create(ctypes.byref(d), 0)
     assert "two cells" in lib.last_error()
+
+
+def test_ensemble_members_seeded_and_in_range():
+    """Config-3 members: sizes from the stated sets, parameters in their
+    ranges, the same member twice is the same problem."""
+    from parflow_b200 import configs
+
+    ms = configs.ensemble(48)
+    assert len(ms) == 48
+    for m in ms:
+        assert m.nx == m.ny and m.nx in configs.ENSEMBLE_NXY and m.nz in configs.ENSEMBLE_NZ
+        assert 0.5 <= m.vg_alpha <= 4.0 and 1.4 <= m.vg_n <= 3.0
+        assert -0.1 <= m.bc["z_upper"].values[0] <= -0.02
+    a, b = configs.ensemble_member(7), configs.ensemble_member(7)
+    assert np.array_equal(a.perm, b.perm) and a.vg_alpha == b.vg_alpha
+    assert len({(m.nx, m.nz) for m in ms}) > 4  # uneven sizes
