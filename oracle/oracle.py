@@ -27,7 +27,11 @@ class Problem(C.Structure):
                 ("vg_from_file", C.c_int),
                 ("z_mult", _dp),
                 ("bc_type", C.c_int * 6),
-                ("bc_val", _dp * 6)]
+                ("bc_val", _dp * 6),
+                ("sslope_x", _dp), ("sslope_y", _dp),
+                ("tslope_x", _dp), ("tslope_y", _dp),
+                ("mannings", _dp),
+                ("ov_epsilon", C.c_double)]
 
 
 class Settings(C.Structure):
@@ -108,6 +112,16 @@ class Oracle:
         P.alpha, P.n, P.s_res, P.s_sat = _ptr(a), _ptr(n), _ptr(sr), _ptr(ss)
         P.vg_from_file = 1 if prob.vg_from_file() else 0
         P.z_mult = _ptr(zm)
+        # slopes and Manning's n (2-D, (ny, nx)); subsurface slopes only under
+        # the terrain-following grid (solver_richards.c:562-572)
+        sx = np.ascontiguousarray(prob.field2d(prob.slope_x))
+        sy = np.ascontiguousarray(prob.field2d(prob.slope_y))
+        man = np.ascontiguousarray(prob.field2d(prob.mannings))
+        self._keep += [sx, sy, man]
+        P.tslope_x, P.tslope_y, P.mannings = _ptr(sx), _ptr(sy), _ptr(man)
+        if prob.terrain_following:
+            P.sslope_x, P.sslope_y = _ptr(sx), _ptr(sy)
+        P.ov_epsilon = 1.0e-5
         self.P = P
         self.set_time(prob.start_time + prob.dt if t is None else t)
         s = prob.solver

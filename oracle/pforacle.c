@@ -123,6 +123,136 @@ static int on_face(const pfo_problem *pb, int f, int i, int j, int k)
 }
 
 /* -------------------------------------------------------------------------
+ * Terrain-following face gravity terms (PL/nl_function_eval.c:725-733,
+ * SlopeUpwindFormulation "Original"): the mean over the two columns of
+ * g sin(atan S) and g cos(atan S); zero slopes give 0 and g.
+ * ------------------------------------------------------------------------- */
+static double slope_at(const double *s, int nx, int ny, int i, int j)
+{
+  /* beyond the last column or row: the slope vector's zero ghost frame */
+  if (!s || i >= nx || j >= ny) return 0.0;
+  return s[i + nx * j];
+}
+
+static void tfg_x(const pfo_problem *pb, int i, int j, double *g_s, double *g_c)
+{
+  const double g = pb->gravity;
+  double a = slope_at(pb->sslope_x, pb->nx, pb->ny, i, j);
+  double b = slope_at(pb->sslope_x, pb->nx, pb->ny, i + 1, j);
+  *g_s = AMEAN(g * sin(atan(a)), g * sin(atan(b)));
+  *g_c = AMEAN(g * cos(atan(a)), g * cos(atan(b)));
+}
+
+static void tfg_y(const pfo_problem *pb, int i, int j, double *g_s, double *g_c)
+{
+  const double g = pb->gravity;
+  double a = slope_at(pb->sslope_y, pb->nx, pb->ny, i, j);
+  double b = slope_at(pb->sslope_y, pb->nx, pb->ny, i, j + 1);
+  *g_s = AMEAN(g * sin(atan(a)), g * sin(atan(b)));
+  *g_c = AMEAN(g * cos(atan(a)), g * cos(atan(b)));
+}
+
+/* -------------------------------------------------------------------------
+ * Kinematic overland flow on the top layer (PL/overlandflow_eval_Kin.c).
+ * 2-D arrays carry ParFlow's one-cell ghost frame: io = (i+1) + (j+1)*(nx+2).
+ * The domain top index is nz-1 in every column and -1 in the ghost frame
+ * (compute_top_and_bottom.c:69); the patch-index vector is all zero, so the
+ * internal patch-edge fixes never apply; the pressure beyond the upper x / y
+ * edge is a ghost value that is never positive, so it enters as 0.
+ * ------------------------------------------------------------------------- */
+#define PFMAX(a, b) (((a) < (b)) ? (b) : (a))
+
+static void ovl_common(const pfo_problem *pb, const double *p, int i, int j,
+                       double *sfx, double *sfy, double *sqm, double *px, double *py)
+{
+  const int nx = pb->nx, ny = pb->ny, nz = pb->nz;
+  const long top = (long)nx * ny * (nz - 1);
+  double Sf_x = pb->tslope_x[i + nx * j], Sf_y = pb->tslope_y[i + nx * j];
+  double Sf_mag = pow(Sf_x * Sf_x + Sf_y * Sf_y, 0.5);
+  if (Sf_mag < pb->ov_epsilon) Sf_mag = pb->ov_epsilon;
+  double pp_ip = p[top + i + nx * j];
+  double pp_e = (i + 1 < nx) ? p[top + i + 1 + nx * j] : 0.0;
+  double pp_n = (j + 1 < ny) ? p[top + i + nx * (j + 1)] : 0.0;
+  *sfx = Sf_x;
+  *sfy = Sf_y;
+  *sqm = pow(fabs(Sf_mag), 0.5);
+  *px = UPSTREAM(-Sf_x, 0.0, PFMAX(pp_ip, 0.0), PFMAX(pp_e, 0.0));
+  *py = UPSTREAM(-Sf_y, 0.0, PFMAX(pp_ip, 0.0), PFMAX(pp_n, 0.0));
+}
+
+/* CALCFCN (:120-290): ke, kw, kn, ks per top cell, ghost-framed */
+static void ovl_fcn(const pfo_problem *pb, const double *p, double *ke, double *kw,
+                    double *kn, double *ks)
+{
+  const int nx = pb->nx, ny = pb->ny, nz = pb->nz, sy = nx + 2;
+  const long n2 = (long)(nx + 2) * (ny + 2);
+  const long top = (long)nx * ny * (nz - 1);
+  double *qx = (double*)calloc(n2, sizeof(double));
+  double *qy = (double*)calloc(n2, sizeof(double));
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      double n_man = pb->mannings[i + nx * j];
+      double Sf_x, Sf_y, sq, Px, Py;
+      ovl_common(pb, p, i, j, &Sf_x, &Sf_y, &sq, &Px, &Py);
+      qx[io] = -(Sf_x / (sq * n_man)) * pow(Px, (5.0 / 3.0));
+      qy[io] = -(Sf_y / (sq * n_man)) * pow(Py, (5.0 / 3.0));
+      double pown = PFMAX(p[top + i + nx * j], 0.0);
+      if (i == 0 && Sf_x > 0.0)   /* lower x boundary */
+        qx[io - 1] = -(Sf_x / (sq * n_man)) * pow(pown, (5.0 / 3.0));
+      if (j == 0 && Sf_y > 0.0)   /* lower y boundary */
+        qy[io - sy] = -(Sf_y / (sq * n_man)) * pow(pown, (5.0 / 3.0));
+    }
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      ke[io] = qx[io];
+      kw[io] = qx[io - 1];
+      kn[io] = qy[io];
+      ks[io] = qy[io - sy];
+    }
+  free(qx);
+  free(qy);
+}
+
+/* CALCDER (:293-460): derivative terms, written into neighbouring entries */
+static void ovl_der(const pfo_problem *pb, const double *p, double *ke, double *kw,
+                    double *kn, double *ks)
+{
+  const int nx = pb->nx, ny = pb->ny, nz = pb->nz, sy = nx + 2;
+  const long top = (long)nx * ny * (nz - 1);
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      double n_man = pb->mannings[i + nx * j];
+      double Sf_x, Sf_y, sq, Px, Py;
+      ovl_common(pb, p, i, j, &Sf_x, &Sf_y, &sq, &Px, &Py);
+      double qx_temp = -(5.0 / 3.0) * (Sf_x / (sq * n_man)) * pow(Px, (2.0 / 3.0));
+      double qy_temp = -(5.0 / 3.0) * (Sf_y / (sq * n_man)) * pow(Py, (2.0 / 3.0));
+      ke[io] = PFMAX(qx_temp, 0);
+      kw[io + 1] = -PFMAX(-qx_temp, 0);
+      kn[io] = PFMAX(qy_temp, 0);
+      ks[io + sy] = -PFMAX(-qy_temp, 0);
+      double pown = PFMAX(p[top + i + nx * j], 0.0);
+      if (i == 0 && Sf_x > 0.0)
+      {
+        qx_temp = -(5.0 / 3.0) * (Sf_x / (sq * n_man)) * pow(pown, (2.0 / 3.0));
+        kw[io] = -PFMAX(-qx_temp, 0);
+        ke[io - 1] = PFMAX(qx_temp, 0);
+      }
+      if (j == 0 && Sf_y > 0.0)
+      {
+        qy_temp = -(5.0 / 3.0) * (Sf_y / (sq * n_man)) * pow(pown, (2.0 / 3.0));
+        ks[io] = -PFMAX(-qy_temp, 0);
+        kn[io - sy] = PFMAX(qy_temp, 0);
+      }
+    }
+}
+
+/* -------------------------------------------------------------------------
  * Residual  (PL/nl_function_eval.c:167-2323)
  * ------------------------------------------------------------------------- */
 void pfo_residual(const pfo_problem *pb, double dt, const double *p,
@@ -153,16 +283,16 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
         f[c] -= vol * 1.0 * 1.0 * zm[k] * dt * (0.0 + 0.0);
       }
 
-  /* interior faces :696-854 (slopes zero: x_dir_g = 0, x_dir_g_c = g) */
-  const double x_dir_g = AMEAN(g * sin(atan(0.0)), g * sin(atan(0.0)));
-  const double x_dir_g_c = AMEAN(g * cos(atan(0.0)), g * cos(atan(0.0)));
-  const double y_dir_g = x_dir_g, y_dir_g_c = x_dir_g_c;
+  /* interior faces :696-854, gravity terms from the subsurface slopes */
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++)
       {
         long c = IDX(i, j, k);
         double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
+        double x_dir_g, x_dir_g_c, y_dir_g, y_dir_g_c;
+        tfg_x(pb, i, j, &x_dir_g, &x_dir_g_c);
+        tfg_y(pb, i, j, &y_dir_g, &y_dir_g_c);
         if (i + 1 < nx)
         {
           long e = c + 1;
@@ -200,11 +330,33 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
         if (k + 1 < nz) f[c + (long)nx * ny] += -dt * u_upper;
       }
 
-  /* boundary patches :979-1435, in patch order */
+  /* boundary patches :979-2060, in patch order */
+  double *ke = NULL, *kw = NULL, *kn = NULL, *ks = NULL;
   for (int face = 0; face < 6; face++)
   {
     const double *vals = pb->bc_val[face];
     int type = pb->bc_type[face];
+    if (type == PFO_BC_OVERLAND_KIN)
+    {
+      /* OverlandKinematicBC :1786-2000, z_upper only */
+      long n2 = (long)(nx + 2) * (ny + 2);
+      ke = (double*)calloc(n2, sizeof(double));
+      kw = (double*)calloc(n2, sizeof(double));
+      kn = (double*)calloc(n2, sizeof(double));
+      ks = (double*)calloc(n2, sizeof(double));
+      ovl_fcn(pb, p, ke, kw, kn, ks);
+      for (int j = 0; j < ny; j++)
+        for (int i = 0; i < nx; i++)
+        {
+          long c = IDX(i, j, nz - 1);
+          long io = (i + 1) + (long)(nx + 2) * (j + 1);
+          double q_overlnd = vol * (PFMAX(p[c], 0.0) - PFMAX(p_old[c], 0.0)) / dz +
+                             dt * vol * ((ke[io] - kw[io]) / dx + (kn[io] - ks[io]) / dy) / dz;
+          f[c] += q_overlnd;
+          f[c] += dt * 1.0 * (ffz * vals[i + nx * j]);
+        }
+      continue;
+    }
     for (int k = 0; k < nz; k++)
       for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++)
@@ -266,6 +418,10 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           f[c] += dt * dir * u_new;
         }
   }
+  free(ke);
+  free(kw);
+  free(kn);
+  free(ks);
   free(sat);
   free(kr);
 }
@@ -312,16 +468,15 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
                + pb->sstorage * vol2 * (dsat[c] * rho * p[c] + sat[c] * drho * p[c] + sat[c] * rho);
     }
 
-  const double x_dir_g = AMEAN(g * sin(atan(0.0)), g * sin(atan(0.0)));
-  const double x_dir_g_c = AMEAN(g * cos(atan(0.0)), g * cos(atan(0.0)));
-  const double y_dir_g = x_dir_g, y_dir_g_c = x_dir_g_c;
-
-  /* face terms :594-780 */
+  /* face terms :594-780, gravity terms from the subsurface slopes */
   for (int k = 0; k < nz; k++)
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++)
       {
         long c = IDX(i, j, k);
+        double x_dir_g, x_dir_g_c, y_dir_g, y_dir_g_c;
+        tfg_x(pb, i, j, &x_dir_g, &x_dir_g_c);
+        tfg_y(pb, i, j, &y_dir_g, &y_dir_g_c);
         double prod = kr[c] * rho;
         double prod_der = dkr[c] * rho + kr[c] * drho;
         double west_temp = 0.0, east_temp = 0.0, sym_east_temp = 0.0;
@@ -470,6 +625,51 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           }
           cp[c] -= o_temp;
         }
+  }
+
+  /* kinematic overland terms on the top layer, MGSemi form (:1863-1990),
+   * after every other term.  In the symmetric storage a lower coefficient is
+   * the neighbour's upper one (matrix.c:484-490): W(i) = E(i-1), S(j) = N(j-1). */
+  if (pb->bc_type[5] == PFO_BC_OVERLAND_KIN)
+  {
+    const int sy2 = nx + 2;
+    long n2 = (long)(nx + 2) * (ny + 2);
+    double *ke = (double*)calloc(n2, sizeof(double));
+    double *kw = (double*)calloc(n2, sizeof(double));
+    double *kn = (double*)calloc(n2, sizeof(double));
+    double *ks = (double*)calloc(n2, sizeof(double));
+    ovl_der(pb, p, ke, kw, kn, ks);
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        long io = (i + 1) + (long)sy2 * (j + 1);
+        if (p[c] > 0.0)
+          cp[c] += (vol / dz) + (vol / ffy) * dt * (ke[io] - kw[io])
+                   + (vol / ffx) * dt * (kn[io] - ks[io]);
+        double tw = (vol / ffy) * dt * (ke[io - 1]);
+        double te = (vol / ffy) * dt * (kw[io + 1]);
+        double ts = (vol / ffx) * dt * (kn[io - sy2]);
+        double tn = (vol / ffx) * dt * (ks[io + sy2]);
+        if (!symm)
+        {
+          wp[c] -= tw;
+          ep[c] += te;
+          sop[c] -= ts;
+          np[c] += tn;
+        }
+        else
+        {
+          if (i > 0) ep[c - 1] -= tw;
+          ep[c] += te;
+          if (j > 0) np[c - sy] -= ts;
+          np[c] += tn;
+        }
+      }
+    free(ke);
+    free(kw);
+    free(kn);
+    free(ks);
   }
   free(sat);
   free(dsat);

@@ -16,7 +16,7 @@
 extern "C" {
 #endif
 
-enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1 };
+enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2 };
 
 typedef struct {
   int nx, ny, nz;
@@ -30,6 +30,15 @@ typedef struct {
   const double *z_mult;            /* per layer (nz) */
   int bc_type[6];                  /* x_lower x_upper y_lower y_upper z_lower z_upper */
   const double *bc_val[6];         /* face arrays: x:(nz,ny) y:(nz,nx) z:(ny,nx) */
+  /* slopes (ny, nx): subsurface ones enter the x/y face gravity terms
+   * (nl_function_eval.c:696-741; equal to the topographic ones under
+   * Solver.TerrainFollowingGrid, solver_richards.c:562-572, else NULL = 0);
+   * topographic ones and Manning's n drive the kinematic overland flow on an
+   * OverlandKinematic z_upper patch (overlandflow_eval_Kin.c) */
+  const double *sslope_x, *sslope_y;
+  const double *tslope_x, *tslope_y;
+  const double *mannings;
+  double ov_epsilon;               /* Solver.OverlandKinematic.Epsilon */
 } pfo_problem;
 
 typedef struct {

@@ -42,7 +42,25 @@ def hydrostatic() -> RichardsProblem:
     return p
 
 
-GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"]
+def overland_small() -> RichardsProblem:
+    """Config-1 physics on 12x10x6 with the surface ponded from the start, so
+    that kinematic overland flow and its boundary outflow are active; rain for
+    2 steps, then none."""
+    return configs.overland(nx=12, ny=10, nz=6, nsteps=4, seed=13, wt_depth=-0.02,
+                            mannings=1e-3, rain_steps=2, dry_steps=2)
+
+
+def tfg_small() -> RichardsProblem:
+    """Terrain-following slopes in the subsurface fluxes without overland
+    flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""
+    p = configs.overland(nx=13, ny=11, nz=7, nsteps=2, seed=17, wt_depth=0.5)
+    p.bc["z_upper"] = BC(BC_FLUX, (-0.01,))
+    p.bc["z_lower"] = BC(BC_DIRICHLET, (0.3,), ref_patch="z_lower")
+    return p
+
+
+GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
+          "overland_small", "tfg_small"]
 
 
 def get(name: str) -> RichardsProblem:

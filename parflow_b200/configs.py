@@ -12,6 +12,12 @@
   per member nx = ny from {64, 96, 128, 192}, nz from {16, 24, 32, 40},
   sigma_lnK ~ U[0.5, 2], alpha ~ U[0.5, 4], n ~ U[1.4, 3], top flux ~
   U[-0.1, -0.02] m/h, config-0 physics otherwise, 10 steps of 0.1 h.
+* ``overland`` (config 1): 256x256x20 hillslope, dx = dy = 10 m, dz = 0.2 m,
+  terrain-following grid with smoothed random slopes |S| in [1e-4, 5e-2],
+  Manning's n 5.5e-5, kinematic overland flow on the top face with rain
+  0.01 m/h for 2 h then none until 4 h, two layers (K 0.1 / 0.005 m/h,
+  alpha 3.5 / 1.0, n 2.0 / 1.8), water table 1 m below the surface,
+  16 steps of 0.25 h.
 * ``adjoint_box`` (config 4): 128x128x32 with config-0 physics, 20 steps.
 
 Every size can be scaled down (``nx``, ``ny``, ``nz`` overrides) for parity
@@ -22,8 +28,8 @@ from __future__ import annotations
 
 import numpy as np
 
-from .problem import BC, BC_DIRICHLET, BC_FLUX, RichardsProblem, SolverSettings
-from .synth import lognormal_field
+from .problem import BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND_KIN, RichardsProblem, SolverSettings
+from .synth import lognormal_field, smoothed_slopes
 
 
 def box(nx=64, ny=64, nz=32, nsteps=10, dt=0.1, seed=0, sigma=1.0, corr=8.0,
@@ -69,6 +75,31 @@ def hetero(nx=512, ny=512, nz=50, nsteps=20, dt=0.05, seed=2,
     return p
 
 
+def overland(nx=256, ny=256, nz=20, nsteps=16, dt=0.25, seed=1, wt_depth=1.0,
+             mannings=5.5e-5, rain=-0.01, rain_steps=8, dry_steps=8,
+             solver: SolverSettings = None) -> RichardsProblem:
+    """Config 1.  ``wt_depth`` is the water-table depth below the surface
+    (negative: ponded start)."""
+    shape = (nz, ny, nx)
+    top = np.arange(nz)[:, None, None] >= nz // 2
+    perm = np.where(top, 0.1, 0.005) * np.ones(shape)
+    alpha = np.where(top, 3.5, 1.0) * np.ones(shape)
+    vg_n = np.where(top, 2.0, 1.8) * np.ones(shape)
+    p = RichardsProblem(nx=nx, ny=ny, nz=nz, dx=10.0, dy=10.0, dz=0.2, perm=perm,
+                        porosity=0.4, specific_storage=1e-4, vg_alpha=alpha, vg_n=vg_n,
+                        s_res=0.1, s_sat=1.0, dt=dt, nsteps=nsteps,
+                        solver=solver or SolverSettings(), name="overland")
+    p.terrain_following = True
+    p.slope_x = smoothed_slopes((ny, nx), seed, 1e-4, 5e-2)
+    p.slope_y = smoothed_slopes((ny, nx), seed + 1, 1e-4, 5e-2)
+    p.mannings = mannings
+    p.bc = {face: BC(BC_FLUX, (0.0,)) for face in
+            ("x_lower", "x_upper", "y_lower", "y_upper", "z_lower")}
+    p.bc["z_upper"] = BC(BC_OVERLAND_KIN, (rain, 0.0), lengths=(rain_steps, dry_steps))
+    p.ic = p.hydrostatic_ic(-wt_depth, "z_upper")
+    return p
+
+
 ENSEMBLE_NXY = (64, 96, 128, 192)
 ENSEMBLE_NZ = (16, 24, 32, 40)
 
@@ -101,4 +132,4 @@ def adjoint_box(nx=128, ny=128, nz=32, nsteps=20, seed=4) -> RichardsProblem:
     return box(nx=nx, ny=ny, nz=nz, nsteps=nsteps, dt=0.1, seed=seed)
 
 
-__all__ = ["box", "hetero", "ensemble_member", "ensemble", "adjoint_box"]
+__all__ = ["box", "hetero", "overland", "ensemble_member", "ensemble", "adjoint_box"]
