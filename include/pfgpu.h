@@ -49,6 +49,8 @@ extern "C" {
  * (pfsimulator/parflow_lib/bc_pressure.h:97 BC_TYPE_TABLE) */
 #define PFGPU_BC_FLUX 0        /* FluxConst: volume flux per area, + = out of upper faces */
 #define PFGPU_BC_DIRICHLET 1   /* DirEquilRefPatch: pressure head values on the face */
+#define PFGPU_BC_OVERLAND_KIN 2 /* OverlandKinematic (z_upper only): rain flux values as
+                                  * FluxConst plus kinematic-wave ponding and routing */
 
 /* faces, ParFlow box patch order */
 #define PFGPU_X_LOWER 0
@@ -127,10 +129,24 @@ const char *pfgpu_last_error(void);
  * problem_phase_rel_perm.c:1930-1932). */
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
 
+/* Surface data of the top layer (ProblemData TSlopeX / TSlopeY / Mannings,
+ * problem_toposlopes.c, problem_mannings.c): host arrays in ParFlow's 2-D
+ * subvector layout, element (i,j) at (i+1) + (j+1)*(nx+2), ghosts ignored.
+ * terrain_following (Solver.TerrainFollowingGrid, solver_richards.c:562-572)
+ * puts the slopes into the subsurface x / y face gravity terms
+ * (nl_function_eval.c:725-733, richards_jacobian_eval.c:620-660);
+ * ov_epsilon is Solver.OverlandKinematic.Epsilon (1e-5 by default).  Needed
+ * before a PFGPU_BC_OVERLAND_KIN face is set. */
+int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
+                      const double *mannings, int terrain_following, double ov_epsilon);
+
 /* Sets the boundary condition of one face at the current time: `values`
  * holds one value per boundary cell, x faces (nz, ny), y faces (nz, nx),
  * z faces (ny, nx), first index slowest.  Replaces the BCStruct built by
- * BCPressure (pfsimulator/parflow_lib/problem_bc_pressure.c:60). */
+ * BCPressure (pfsimulator/parflow_lib/problem_bc_pressure.c:60).  An
+ * OverlandKinematic face (z_upper) adds the kinematic-wave overland flow of
+ * overlandflow_eval_Kin.c to the top layer (nl_function_eval.c:1786-2000,
+ * richards_jacobian_eval.c:1863-1990). */
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values);
 
 /* Residual F(p) of one implicit step (NlFunctionEval,

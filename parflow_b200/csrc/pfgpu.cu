@@ -100,6 +100,9 @@ struct pfgpu_handle {
   // fields
   double *kx = nullptr, *ky = nullptr, *kz = nullptr;
   double *alpha = nullptr, *vgn = nullptr, *sres = nullptr, *ssat = nullptr, *zmult = nullptr;
+  // surface: 7 column arrays of ny*nx (TFG g sin / g cos of x and y slopes,
+  // overland slopes x / y, Manning's n) in one allocation
+  double *surf = nullptr;
   double *bcv[6] = {nullptr};
   // state and work vectors (dense interior layout)
   double *u = nullptr;      // current iterate / handle pressure state
@@ -898,7 +901,8 @@ static void destroy_impl(pfgpu_handle *h) {
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   double *vecs[] = {h->u, h->unew, h->fval, h->pp, h->bb, h->p_old, h->s_old, h->kr,
                     h->dkr, h->sat, h->dsat, h->xcor, h->vtemp, h->gs, h->dsc, h->stage,
-                    h->rb.partial, h->zmult, h->zface, h->alpha, h->vgn, h->sres, h->ssat};
+                    h->rb.partial, h->zmult, h->zface, h->alpha, h->vgn, h->sres, h->ssat,
+                    h->surf};
   for (double *v : vecs) cudaFree(v);
   if (h->kx) cudaFree(h->kx);
   if (h->ky && h->ky != h->kx) cudaFree(h->ky);
@@ -1004,9 +1008,57 @@ int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
   return PFGPU_OK;
 }
 
+int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
+                      const double *mannings, int terrain_following, double ov_epsilon) {
+  if (!h || !slope_x || !slope_y || !mannings || !(ov_epsilon > 0)) {
+    set_err("pfgpu_set_surface: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  const int nx = h->nx, ny = h->ny;
+  const size_t n2 = (size_t)nx * ny;
+  // interior of ParFlow's 2-D subvector layout: (i+1) + (j+1)*(nx+2)
+  std::vector<double> col(7 * n2);
+  const double g = h->d.gravity;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++) {
+      const size_t a = i + (size_t)nx * j, q = (i + 1) + (size_t)(nx + 2) * (j + 1);
+      const double sx = slope_x[q], sy = slope_y[q];
+      col[a] = g * sin(atan(sx));
+      col[n2 + a] = g * cos(atan(sx));
+      col[2 * n2 + a] = g * sin(atan(sy));
+      col[3 * n2 + a] = g * cos(atan(sy));
+      col[4 * n2 + a] = sx;
+      col[5 * n2 + a] = sy;
+      col[6 * n2 + a] = mannings[q];
+    }
+  if (!h->surf && dalloc(&h->surf, 7 * n2)) return PFGPU_ERR_NOMEM;
+  CK(cudaMemcpy(h->surf, col.data(), col.size() * sizeof(double), cudaMemcpyHostToDevice));
+  DevProblem &P = h->P;
+  if (terrain_following) {
+    P.tfg_xs = h->surf;
+    P.tfg_xc = h->surf + n2;
+    P.tfg_ys = h->surf + 2 * n2;
+    P.tfg_yc = h->surf + 3 * n2;
+  } else {
+    P.tfg_xs = P.tfg_xc = P.tfg_ys = P.tfg_yc = nullptr;
+  }
+  P.ov_sx = h->surf + 4 * n2;
+  P.ov_sy = h->surf + 5 * n2;
+  P.ov_n = h->surf + 6 * n2;
+  P.ov_eps = ov_epsilon;
+  h->vg_for = nullptr;
+  return PFGPU_OK;
+}
+
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values) {
-  if (!h || !values || face < 0 || face > 5 || (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET)) {
+  if (!h || !values || face < 0 || face > 5 ||
+      (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET && type != PFGPU_BC_OVERLAND_KIN)) {
     set_err("pfgpu_set_bc: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  if (type == PFGPU_BC_OVERLAND_KIN && (face != PFGPU_Z_UPPER || !h->P.ov_sx)) {
+    set_err("pfgpu_set_bc: OverlandKinematic needs face z_upper and pfgpu_set_surface first");
     return PFGPU_ERR_ARG;
   }
   CK(cudaSetDevice(h->device));

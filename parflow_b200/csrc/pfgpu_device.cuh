@@ -30,7 +30,44 @@ struct DevProblem {
   double inv_dx, inv_dy, inv_visc;
   int bc_type[6];
   const double *bc_val[6];
+  // terrain-following grid: per column (ny*nx) g sin(atan S) and g cos(atan S)
+  // of the subsurface slopes; null = flat (0 and g)
+  const double *tfg_xs, *tfg_xc, *tfg_ys, *tfg_yc;
+  // kinematic overland flow on a z_upper patch of type 2: topographic slopes
+  // and Manning's n per column (ny*nx), Solver.OverlandKinematic.Epsilon
+  const double *ov_sx, *ov_sy, *ov_n;
+  double ov_eps;
 };
+
+// Gravity terms of the x face between columns i and i+1 (and of the y face
+// between rows j and j+1): mean over the two columns of g sin(atan S) and
+// g cos(atan S) (nl_function_eval.c:725-733, SlopeUpwindFormulation 0).
+__device__ __forceinline__ void tfg_face_x(const DevProblem &P, int i, int j, double &gs,
+                                           double &gc) {
+  const double g = P.gravity;
+  if (!P.tfg_xs) {
+    gs = 0.5 * (g * 0.0 + g * 0.0);
+    gc = 0.5 * (g * 1.0 + g * 1.0);
+    return;
+  }
+  const long long a = i + (long long)P.nx * j;
+  const bool in = i + 1 < P.nx;
+  gs = 0.5 * (__ldg(P.tfg_xs + a) + (in ? __ldg(P.tfg_xs + a + 1) : g * 0.0));
+  gc = 0.5 * (__ldg(P.tfg_xc + a) + (in ? __ldg(P.tfg_xc + a + 1) : g * 1.0));
+}
+__device__ __forceinline__ void tfg_face_y(const DevProblem &P, int i, int j, double &gs,
+                                           double &gc) {
+  const double g = P.gravity;
+  if (!P.tfg_ys) {
+    gs = 0.5 * (g * 0.0 + g * 0.0);
+    gc = 0.5 * (g * 1.0 + g * 1.0);
+    return;
+  }
+  const long long a = i + (long long)P.nx * j;
+  const bool in = j + 1 < P.ny;
+  gs = 0.5 * (__ldg(P.tfg_ys + a) + (in ? __ldg(P.tfg_ys + a + P.nx) : g * 0.0));
+  gc = 0.5 * (__ldg(P.tfg_yc + a) + (in ? __ldg(P.tfg_yc + a + P.nx) : g * 1.0));
+}
 
 // ParFlow's mean macros (pfsimulator/parflow_lib/solver.h:42-47)
 __device__ __forceinline__ double harmonic(double a, double b) {
@@ -142,15 +179,13 @@ __device__ __forceinline__ VGAll vg_all(const DevProblem &P, double p, const VG 
 }
 
 // ---------------------------------------------------------------------------
-// Face fluxes of the residual (nl_function_eval.c:696-854); slopes are zero
-// on this path: x_dir_g = 0, x_dir_g_c = gravity.
+// Face fluxes of the residual (nl_function_eval.c:696-854) with the face's
+// gravity terms x_dir_g / x_dir_g_c (tfg_face_x).
 // a = lower/left cell, b = upper/right cell.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ double flux_x(const DevProblem &P, double pa, double pb, double ka,
-                                         double kb, double kra, double krb, double zm) {
-  const double g = P.gravity;
-  const double x_dir_g = amean(g * 0.0, g * 0.0);
-  const double x_dir_g_c = amean(g * 1.0, g * 1.0);
+                                         double kb, double kra, double krb, double zm,
+                                         double x_dir_g, double x_dir_g_c) {
   double diff_l = pa - pb;
   double updir = (diff_l * P.inv_dx) * x_dir_g_c - x_dir_g;
   double km = harmonic(ka, kb);
@@ -162,10 +197,8 @@ __device__ __forceinline__ double flux_x(const DevProblem &P, double pa, double 
 }
 
 __device__ __forceinline__ double flux_y(const DevProblem &P, double pa, double pb, double ka,
-                                         double kb, double kra, double krb, double zm) {
-  const double g = P.gravity;
-  const double y_dir_g = amean(g * 0.0, g * 0.0);
-  const double y_dir_g_c = amean(g * 1.0, g * 1.0);
+                                         double kb, double kra, double krb, double zm,
+                                         double y_dir_g, double y_dir_g_c) {
   double diff_l = pa - pb;
   double updir = (diff_l * P.inv_dy) * y_dir_g_c - y_dir_g;
   double km = harmonic(ka, kb);
@@ -188,6 +221,44 @@ __device__ __forceinline__ double flux_z(const DevProblem &P, double pa, double 
   double ffz = P.dx * P.dy;
   return ffz * 1.0 * 1.0 * harmonic_dz(ka, kb, za, zb) * diff_l *
          upstream(lower, upper, kra * rho, krb * rho) * P.inv_visc;
+}
+
+// ---------------------------------------------------------------------------
+// Kinematic overland flow on the top layer (overlandflow_eval_Kin.c).  The
+// domain top is layer nz-1 in every column and -1 outside the domain, the
+// patch index is uniform (no internal patch edges), and the pressure beyond
+// the upper x / y edge is a ghost value that never exceeds zero, so it
+// enters as 0.  PFMAX(a, 0) as in the reference: (a < 0) ? 0 : a.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double pmax0(double a) { return (a < 0.0) ? 0.0 : a; }
+
+struct OvCell {
+  double sfx, sfy, sq, n;  // slopes, |S_f|^(1/2) (floored magnitude), Manning's n
+};
+__device__ __forceinline__ OvCell ov_cell(const DevProblem &P, int i, int j) {
+  const long long a = i + (long long)P.nx * j;
+  OvCell o;
+  o.sfx = __ldg(P.ov_sx + a);
+  o.sfy = __ldg(P.ov_sy + a);
+  o.n = __ldg(P.ov_n + a);
+  double mag = pow(o.sfx * o.sfx + o.sfy * o.sfy, 0.5);
+  if (mag < P.ov_eps) mag = P.ov_eps;
+  o.sq = pow(fabs(mag), 0.5);
+  return o;
+}
+// pressure of the top cell of column (i, j); 0 beyond the upper edges
+__device__ __forceinline__ double p_top(const DevProblem &P, const double *p, int i, int j) {
+  if (i >= P.nx || j >= P.ny) return 0.0;
+  return p[i + (long long)P.nx * (j + (long long)P.ny * (P.nz - 1))];
+}
+// upwinded ponded depth of the x face (i | i+1) and the y face (j | j+1)
+__device__ __forceinline__ double ov_press_x(const DevProblem &P, const double *p, int i, int j,
+                                             const OvCell &o) {
+  return upstream(-o.sfx, 0.0, pmax0(p_top(P, p, i, j)), pmax0(p_top(P, p, i + 1, j)));
+}
+__device__ __forceinline__ double ov_press_y(const DevProblem &P, const double *p, int i, int j,
+                                             const OvCell &o) {
+  return upstream(-o.sfy, 0.0, pmax0(p_top(P, p, i, j)), pmax0(p_top(P, p, i, j + 1)));
 }
 
 // Index of a boundary cell in its face table.

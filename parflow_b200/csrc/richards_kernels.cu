@@ -71,22 +71,27 @@ __global__ void k_residual(DevProblem P, const double *__restrict__ p,
     double zl = __ldg(P.zmult + k - 1);
     fc += -dt * flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
   }
+  double gs, gc;
   if (j > 0) {
     long long s = c - sy;
-    fc += -dt * flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm);
+    tfg_face_y(P, i, j - 1, gs, gc);
+    fc += -dt * flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm, gs, gc);
   }
   if (i > 0) {
     long long w = c - 1;
-    fc += -dt * flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm);
+    tfg_face_x(P, i - 1, j, gs, gc);
+    fc += -dt * flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm, gs, gc);
   }
   double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
   if (i + 1 < P.nx) {
     long long e = c + 1;
-    u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm);
+    tfg_face_x(P, i, j, gs, gc);
+    u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm, gs, gc);
   }
   if (j + 1 < P.ny) {
     long long nn = c + sy;
-    u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm);
+    tfg_face_y(P, i, j, gs, gc);
+    u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm, gs, gc);
   }
   if (k + 1 < P.nz) {
     long long u = c + sz;
@@ -107,6 +112,28 @@ __global__ void k_residual(DevProblem P, const double *__restrict__ p,
     if (P.bc_type[face] == 0) {
       double h = (face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz;
       u_new = h * value;
+    } else if (P.bc_type[face] == 2) {
+      // OverlandKinematic top face (nl_function_eval.c:1786-2000): ponding and
+      // routing term, then the rain flux like FluxConst
+      const OvCell o = ov_cell(P, i, j);
+      double ke = -(o.sfx / (o.sq * o.n)) * pow(ov_press_x(P, p, i, j, o), (5.0 / 3.0));
+      double kn = -(o.sfy / (o.sq * o.n)) * pow(ov_press_y(P, p, i, j, o), (5.0 / 3.0));
+      double kw = 0.0, ks = 0.0;
+      if (i > 0) {
+        const OvCell ow = ov_cell(P, i - 1, j);
+        kw = -(ow.sfx / (ow.sq * ow.n)) * pow(ov_press_x(P, p, i - 1, j, ow), (5.0 / 3.0));
+      } else if (o.sfx > 0.0) {  // outflow through the lower x edge
+        kw = -(o.sfx / (o.sq * o.n)) * pow(pmax0(pc), (5.0 / 3.0));
+      }
+      if (j > 0) {
+        const OvCell os = ov_cell(P, i, j - 1);
+        ks = -(os.sfy / (os.sq * os.n)) * pow(ov_press_y(P, p, i, j - 1, os), (5.0 / 3.0));
+      } else if (o.sfy > 0.0) {  // outflow through the lower y edge
+        ks = -(o.sfy / (o.sq * o.n)) * pow(pmax0(pc), (5.0 / 3.0));
+      }
+      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      u_new = ffz * value;
     } else {
       const VG v = vg_at(P, c);
       double krg = vg_kr(P, value, v.alpha, v.n);
@@ -152,10 +179,8 @@ struct FaceDer {
 __device__ __forceinline__ FaceDer face_der_xy(const DevProblem &P, double dt, double h_ff,
                                                double dd, double pa, double pb, double ka,
                                                double kb, double prod, double prod_der,
-                                               double prod_rt, double prod_rt_der, double zm) {
-  const double g = P.gravity;
-  const double dir_g = amean(g * 0.0, g * 0.0);
-  const double dir_g_c = amean(g * 1.0, g * 1.0);
+                                               double prod_rt, double prod_rt_der, double zm,
+                                               double dir_g, double dir_g_c) {
   double diff = pa - pb;
   const double inv_dd = 1.0 / dd;
   double updir = (diff * inv_dd) * dir_g_c - dir_g;
@@ -232,33 +257,38 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
     cp += -d.hi;
     l = d.lo;
   }
+  double gs, gc;
   if (j > 0) {
     long long q = c - sy;
+    tfg_face_y(P, i, j - 1, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffy, P.dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm);
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
     s = d.lo;
   }
   if (i > 0) {
     long long q = c - 1;
+    tfg_face_x(P, i - 1, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffx, P.dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm);
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
     w = d.lo;
   }
   double west_t = 0.0, south_t = 0.0, lower_t = 0.0;
   if (i + 1 < P.nx) {
     long long q = c + 1;
+    tfg_face_x(P, i, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffx, P.dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm);
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     west_t = d.lo;
     e = d.hi;
     es = d.sym;
   }
   if (j + 1 < P.ny) {
     long long q = c + sy;
+    tfg_face_y(P, i, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffy, P.dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm);
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     south_t = d.lo;
     nn = d.hi;
     ns = d.sym;
@@ -330,6 +360,56 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
       }
     }
     cp -= o_temp;
+  }
+
+  // kinematic overland terms of a top cell, MGSemi form
+  // (richards_jacobian_eval.c:1863-1990, CALCDER of overlandflow_eval_Kin.c),
+  // added after every other term.  In the symmetric storage the west / south
+  // terms belong to the neighbour's E / N entry (lower coefficient aliasing,
+  // matrix.c:484-490): E(i) gets this cell's east term, then the east
+  // neighbour's west term, in the reference's loop order.
+  if (k == P.nz - 1 && P.bc_type[5] == 2) {
+    const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
+    const double two3 = 2.0 / 3.0;
+    const OvCell o = ov_cell(P, i, j);
+    const double qxt = -(5.0 / 3.0) * (o.sfx / (o.sq * o.n)) * pow(ov_press_x(P, p, i, j, o), two3);
+    const double qyt = -(5.0 / 3.0) * (o.sfy / (o.sq * o.n)) * pow(ov_press_y(P, p, i, j, o), two3);
+    const double ke_d = pmax0(qxt), kn_d = pmax0(qyt);
+    double kw_d = 0.0, ks_d = 0.0, ke_w = 0.0, kn_s = 0.0;
+    if (i > 0) {
+      const OvCell ow = ov_cell(P, i - 1, j);
+      const double q = -(5.0 / 3.0) * (ow.sfx / (ow.sq * ow.n)) *
+                       pow(ov_press_x(P, p, i - 1, j, ow), two3);
+      kw_d = -pmax0(-q);
+      ke_w = pmax0(q);
+    } else if (o.sfx > 0.0) {
+      const double q = -(5.0 / 3.0) * (o.sfx / (o.sq * o.n)) * pow(pmax0(pc), two3);
+      kw_d = -pmax0(-q);
+      ke_w = pmax0(q);
+    }
+    if (j > 0) {
+      const OvCell os = ov_cell(P, i, j - 1);
+      const double q = -(5.0 / 3.0) * (os.sfy / (os.sq * os.n)) *
+                       pow(ov_press_y(P, p, i, j - 1, os), two3);
+      ks_d = -pmax0(-q);
+      kn_s = pmax0(q);
+    } else if (o.sfy > 0.0) {
+      const double q = -(5.0 / 3.0) * (o.sfy / (o.sq * o.n)) * pow(pmax0(pc), two3);
+      ks_d = -pmax0(-q);
+      kn_s = pmax0(q);
+    }
+    if (pc > 0.0)
+      cp += (vol / P.dz) + cx * (ke_d - kw_d) + cy * (kn_d - ks_d);
+    const double tw = cx * (ke_w), te = cx * (-pmax0(-qxt));
+    const double ts = cy * (kn_s), tn = cy * (-pmax0(-qyt));
+    w -= tw;
+    e += te;
+    s -= ts;
+    nn += tn;
+    es += te;
+    if (i + 1 < P.nx) es -= cx * (ke_d);  // the east neighbour's west term
+    ns += tn;
+    if (j + 1 < P.ny) ns -= cy * (kn_d);  // the north neighbour's south term
   }
   if (J.c) {
     J.c[c] = (TJ)cp;

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(HERE, "libpfgpu.so")
 
 ABI_VERSION = 1
 PREC_FP64, PREC_MIXED = 0, 1
-BC_FLUX, BC_DIRICHLET = 0, 1
+BC_FLUX, BC_DIRICHLET, BC_OVERLAND_KIN = 0, 1, 2
 FIELD_PERM_X, FIELD_PERM_Y, FIELD_PERM_Z = 0, 1, 2
 FIELD_VG_ALPHA, FIELD_VG_N, FIELD_S_RES, FIELD_S_SAT = 3, 4, 5, 6
 OK, NOT_CONVERGED = 0, 1
@@ -58,7 +58,7 @@ EXPORTS = ["pfgpu_create", "pfgpu_destroy", "pfgpu_last_error", "pfgpu_set_field
            "pfgpu_pc_setup", "pfgpu_pc_apply", "pfgpu_saturation", "pfgpu_newton_solve",
            "pfgpu_set_pressure", "pfgpu_get_pressure", "pfgpu_advance", "pfgpu_mg_levels",
            "pfgpu_stream", "pfgpu_kernel_launches", "pfgpu_time_kernel",
-           "pfgpu_residual_noalloc", "pfgpu_ensemble_advance"]
+           "pfgpu_residual_noalloc", "pfgpu_ensemble_advance", "pfgpu_set_surface"]
 KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_smooth": 3, "vcycle": 4, "mg_setup": 5,
            "colour_sweep": 6}
 
@@ -81,6 +81,7 @@ def load(path: str = LIB_PATH):
     L.pfgpu_last_error.restype = C.c_char_p
     L.pfgpu_set_field.argtypes = [vp, C.c_int, C.c_void_p]
     L.pfgpu_set_bc.argtypes = [vp, C.c_int, C.c_int, C.c_void_p]
+    L.pfgpu_set_surface.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double]
     L.pfgpu_nl_function_eval.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                          C.c_void_p]
     L.pfgpu_jacobian_matvec.argtypes = [vp, C.c_void_p, C.c_double, C.c_void_p, C.c_void_p]

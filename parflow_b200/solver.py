@@ -99,6 +99,8 @@ class RichardsGPU:
     # ---- setup ---------------------------------------------------------------
     def _upload_fields(self):
         p = self.prob
+        if p.terrain_following or any(bc.kind == L.BC_OVERLAND_KIN for bc in p.bc.values()):
+            self._upload_surface()
         L.check(self.lib.pfgpu_set_field(self.h, L.FIELD_PERM_X, _ptr(pad(p.field3d(p.perm)))),
                 "set_field perm")
         if p.vg_from_file():
@@ -108,6 +110,16 @@ class RichardsGPU:
                 if np.all(a == a.flat[0]):
                     continue  # uniform: the descriptor scalar serves every cell
                 L.check(self.lib.pfgpu_set_field(self.h, fid, _ptr(pad(a))), "set_field vg")
+
+    def _upload_surface(self):
+        """Slopes and Manning's n in ParFlow's 2-D layout (pfgpu_set_surface)."""
+        p = self.prob
+        pad2 = lambda a: np.pad(np.asarray(a, dtype=np.float64), 1)
+        self._surf = [pad2(p.field2d(p.slope_x)), pad2(p.field2d(p.slope_y)),
+                      pad2(p.field2d(p.mannings))]
+        L.check(self.lib.pfgpu_set_surface(self.h, *[_ptr(a) for a in self._surf],
+                                           1 if p.terrain_following else 0, 1.0e-5),
+                "set_surface")
 
     def set_time(self, t: float):
         """Upload the boundary tables BCPressure would build at time t."""
