@@ -106,7 +106,24 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # reference CPU arm
 # ---------------------------------------------------------------------------
-REF_SAMPLE = (128, 128, 50)   # 1/16 of the workload's cells, same depth and physics
+def _workloads():
+    from parflow_b200 import configs
+
+    return {
+        # the bench line: heterogeneous box, 13.1M cells
+        "hetero": {
+            "build": lambda nx, ny, nz, nsteps: configs.hetero(nx=nx, ny=ny, nz=nz, nsteps=nsteps),
+            "dims": (NX, NY, NZ), "sample": (128, 128, 50),
+            "label": "hetero 512x512x50 (13.1M cells)",
+            "config": {"dt_h": 0.05, "sigma_lnK": 1.5, "corr_cells": [32, 32, 4]}},
+        # config 1: hillslope with kinematic overland flow, terrain-following grid
+        "overland": {
+            "build": lambda nx, ny, nz, nsteps: configs.overland(nx=nx, ny=ny, nz=nz, nsteps=nsteps),
+            "dims": (256, 256, 20), "sample": (64, 64, 20),
+            "label": "overland hillslope 256x256x20 (1.31M cells), kinematic overland flow, "
+                     "terrain-following grid, rain 2 h on / 2 h off",
+            "config": {"dt_h": 0.25, "dx_m": 10.0, "dz_m": 0.2, "mannings": 5.5e-5}},
+    }
 
 
 def _ref_binary():
@@ -117,14 +134,15 @@ def _ref_binary():
     return None, None
 
 
-def run_reference_cpu(nsteps: int, threads: int):
+def run_reference_cpu(nsteps: int, threads: int, workload: str = "hetero"):
     """Time the unmodified reference (oracle/_ref) on a bounded sample of the
-    workload; returns (steps/s scaled to the full workload, info dict)."""
-    from parflow_b200 import configs
-
+    workload (same physics, fewer cells); returns (steps/s scaled by cells to
+    the full workload, info dict)."""
+    wl = _workloads()[workload]
     exe, name = _ref_binary()
-    sx, sy, sz = REF_SAMPLE
-    prob = configs.hetero(nx=sx, ny=sy, nz=sz, nsteps=nsteps)
+    sx, sy, sz = wl["sample"]
+    fx, fy, fz = wl["dims"]
+    prob = wl["build"](sx, sy, sz, nsteps)
     if exe is None:
         # the oracle port, one core
         from oracle.oracle import Oracle
@@ -152,12 +170,12 @@ def run_reference_cpu(nsteps: int, threads: int):
             pass
         shutil.rmtree(wd, ignore_errors=True)
         kind, cores = "reference", threads if name == "parflow_omp" else 1
-    scale = (sx * sy * sz) / float(NX * NY * NZ)
+    scale = (sx * sy * sz) / float(fx * fy * fz)
     steps_per_s = nsteps / secs * scale
     info = {"kind": kind, "cores": cores,
-            "sample": f"{sx}x{sy}x{sz} heterogeneous box (1/{int(round(1 / scale))} of the "
-                      f"workload's cells), {nsteps} steps dt=0.05 h, KINSol time "
-                      f"{secs:.2f} s, scaled by cell count to 512x512x50",
+            "sample": f"{sx}x{sy}x{sz} sample of the {workload} workload "
+                      f"(1/{int(round(1 / scale))} of its cells), {nsteps} steps, KINSol time "
+                      f"{secs:.2f} s, scaled by cell count to {fx}x{fy}x{fz}",
             "binary": name or "oracle port"}
     return steps_per_s, info
 
@@ -171,14 +189,16 @@ def reference_arm(args, rank, world):
     k = max(1, args.steps)
     # each step: one bounded reference sample of 2 timesteps
     for _ in range(k):
-        v, info = run_reference_cpu(2, threads)
+        v, info = run_reference_cpu(2, threads, args.workload if args.workload != "ensemble"
+                                    else "hetero")
         per.append(v)
     value = float(np.median(per))
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "timesteps/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": "hetero 512x512x50 (13.1M cells), sampled", "dt_h": 0.05},
+           "config": {"workload": _workloads()[args.workload if args.workload != "ensemble"
+                                                else "hetero"]["label"] + ", sampled"},
            "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": info["cores"],
                             "kind": info["kind"], "sample": info["sample"]},
            "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
@@ -203,8 +223,10 @@ def gpu_arm(args, rank, world, local_rank):
         dist = dist_mod
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
 
-    nx, ny, nz = args.size
-    prob = configs.hetero(nx=nx, ny=ny, nz=nz, nsteps=args.warmup + args.steps + 2)
+    wl = _workloads()[args.workload]
+    nx, ny, nz = args.size if args.profile else wl["dims"]
+    prob = wl["build"](nx, ny, nz, args.warmup + args.steps + 2)
+    cells = prob.ncells
     plan = prob.time_plan()
     ic = prob.initial_pressure()
 
@@ -280,7 +302,7 @@ def gpu_arm(args, rank, world, local_rank):
     peak, peak_kind = peaks()
     achieved = dbytes / (dms * 1e-3) / 1e9
     traffic = None if RB_SWEEP_DRAM_BYTES_PER_CELL is None else \
-        RB_SWEEP_DRAM_BYTES_PER_CELL * NX * NY * NZ
+        RB_SWEEP_DRAM_BYTES_PER_CELL * cells
 
     # end to end through the C ABI with host buffers: one pfgpu_newton_solve
     # (p_old, s_old, p in; p out) and one pfgpu_saturation per step
@@ -334,7 +356,7 @@ def gpu_arm(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            v, info = run_reference_cpu(2, os.cpu_count() or 1)
+            v, info = run_reference_cpu(2, os.cpu_count() or 1, args.workload)
             cpu = {"value": v, "unit": "timesteps/s", "cores": info["cores"],
                    "kind": info["kind"], "sample": info["sample"]}
         except Exception as e:  # reported, not fatal
@@ -351,17 +373,17 @@ def gpu_arm(args, rank, world, local_rank):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f64 Newton/Arnoldi, f32 preconditioner + Jacobian storage",
             "data": "synthetic",
-            "config": {"workload": "hetero 512x512x50 (13.1M cells) mixed precision",
-                       "dt_h": 0.05, "sigma_lnK": 1.5, "corr_cells": [32, 32, 4],
-                       "solver": "KINSOL line search, EtaConstant 1e-5, GMRES(25), MGSemi V(1,1)",
-                       "l2": "inputs larger than L2 (every vector 105 MB, working set > 3 GB)",
-                       "parallelism": f"replicas x{world}"},
+            "config": dict({"workload": wl["label"] + " mixed precision"}, **wl["config"],
+                           solver="KINSOL line search, EtaConstant 1e-5, GMRES(25), MGSemi V(1,1)",
+                           l2=f"inputs larger than L2 (every vector {cells * 8 / 1e6:.0f} MB, "
+                              "working set several GB)",
+                           parallelism=f"replicas x{world}"),
             "fp64_steps_per_s": steps_64,
             "mixed_speedup_vs_fp64": steps_mx / steps_64,
             "mixed_vs_fp64_max_rel_pressure_err": rel_err,
             "newton_iters_per_step": newton / max(1, len(stmx)),
             "gmres_iters_per_step": sum(x.lin_iters for x in stmx) / max(1, len(stmx)),
-            "cell_newton_updates_per_s": NX * NY * NZ * newton * world / (msmx * 1e-3),
+            "cell_newton_updates_per_s": cells * newton * world / (msmx * 1e-3),
             "roofline": {"bound": "hbm",
                          "kernel": "k_rb_sweep: one red/black colour sweep, finest level (f32)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
@@ -468,8 +490,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="hetero", choices=["hetero", "ensemble"],
-                    help="hetero: the 512x512x50 bench line; ensemble: the 48-member set")
+    ap.add_argument("--workload", default="hetero", choices=["hetero", "overland", "ensemble"],
+                    help="hetero: the 512x512x50 bench line; overland: the 256x256x20 "
+                         "overland hillslope; ensemble: the 48-member set")
     ap.add_argument("--profile", action="store_true",
                     help="mixed solve only, timed steps bracketed by cudaProfilerStart/Stop")
     ap.add_argument("--size", default=f"{NX},{NY},{NZ}",
@@ -477,7 +500,7 @@ def main():
     args = ap.parse_args()
     args.size = tuple(int(v) for v in args.size.split(","))
     if not args.profile and args.size != (NX, NY, NZ):
-        ap.error("--size is for --profile runs; the bench workload is 512x512x50")
+        ap.error("--size is for --profile runs; the bench workloads have fixed sizes")
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
