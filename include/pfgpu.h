@@ -204,6 +204,29 @@ int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats);
 int pfgpu_ensemble_advance(pfgpu_handle *const *members, int n, const double *dt, int nsteps,
                            int nthreads, pfgpu_stats *stats, int *status);
 
+/* Discrete adjoint of the implicit timesteps (no counterpart in the
+ * reference).  pfgpu_adjoint_record starts a trajectory at the handle's
+ * current pressure (p_0) with room for max_steps steps; every successful step
+ * of pfgpu_advance after it appends p_n and the dt it used.
+ * pfgpu_adjoint_gradient then returns, for the objective
+ *   g = sum over observed steps n and observed cells c of (p_n[c] - obs)^2,
+ * its value (*misfit) and its gradient with respect to the per-cell ln K
+ * (every direction's permeability scaled together), van Genuchten alpha and
+ * n (ParFlow layout, host or device; NULL skips one), by solving
+ * J_n^T lambda_n = -dg/dp_n - (dF_{n+1}/dp_n)^T lambda_{n+1} backwards in n
+ * with GMRES on the transposed analytic Jacobian (multigrid preconditioned)
+ * to relative residual tol, and summing lambda_n^T dF_n/dtheta.
+ * obs_steps (nobs_steps values in 1..recorded steps), obs_cells (nobs dense
+ * interior indices i + nx*(j + ny*k)) and obs_values (nobs_steps x nobs,
+ * step-major) are host arrays.  The boundary tables in effect are used for
+ * every step (constant boundary conditions over the window).  Use an FP64
+ * handle: the mixed form stores J in FP32. */
+int pfgpu_adjoint_record(pfgpu_handle *h, int max_steps);
+int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps, int nobs,
+                           const long long *obs_cells, const double *obs_values, double tol,
+                           double *misfit, double *grad_lnk, double *grad_alpha,
+                           double *grad_n);
+
 /* Number of multigrid levels and their sizes/coarsening directions
  * (mg_semi.c:858-923); dims has 4*levels ints (nx, ny, nz, dir). */
 int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);

@@ -134,6 +134,14 @@ struct pfgpu_handle {
   int jac_valid = 0;
   int *kerr = nullptr;   // device error word of the pipelined kernels
   int *hkerr = nullptr;  // pinned host mirror
+  // discrete adjoint: recorded trajectory p_0 .. p_len (dense, device) and
+  // the dt of each recorded step; work vectors of the backward sweep
+  double *hist = nullptr;
+  int hist_cap = 0, hist_len = 0;
+  bool recording = false, hist_overflow = false;
+  std::vector<double> hist_dt;
+  double *adj = nullptr;  // 8 vectors: lam, lam_next, rhs, r, dx, g_lnk, g_a, g_n
+  bool adj_transpose = false;  // matvec applies J^T (adjoint solves)
 };
 
 // ---------------------------------------------------------------------------
@@ -244,6 +252,17 @@ static void assemble(pfgpu_handle *h, const double *u, double dt, bool want_J, b
 }
 
 static void matvec(pfgpu_handle *h, const double *x, double *y) {
+  if (h->adj_transpose) {
+    if (h->mixed) {
+      JacIn<float> J{h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
+      launch_matvec7_t<float>(h->nx, h->ny, h->nz, J, x, y, h->st);
+    } else {
+      JacIn<double> J{h->Jd.c, h->Jd.w, h->Jd.e, h->Jd.s, h->Jd.n, h->Jd.l, h->Jd.u};
+      launch_matvec7_t<double>(h->nx, h->ny, h->nz, J, x, y, h->st);
+    }
+    h->launches++;
+    return;
+  }
   if (h->mixed) {
     JacIn<float> J{h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
     launch_matvec7<float>(h->nx, h->ny, h->nz, J, x, y, h->st);
@@ -899,6 +918,8 @@ static void destroy_impl(pfgpu_handle *h) {
   cudaSetDevice(h->device);
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
+  cudaFree(h->hist);
+  cudaFree(h->adj);
   double *vecs[] = {h->u, h->unew, h->fval, h->pp, h->bb, h->p_old, h->s_old, h->kr,
                     h->dkr, h->sat, h->dsat, h->xcor, h->vtemp, h->gs, h->dsc, h->stage,
                     h->rb.partial, h->zmult, h->zface, h->alpha, h->vgn, h->sres, h->ssat,
@@ -1173,11 +1194,170 @@ int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats) {
       dts *= 0.5;
     }
     if (stats) stats[s] = st;
+    if (rc == PFGPU_OK && h->recording) {
+      if (h->hist_len < h->hist_cap) {
+        CK(cudaMemcpyAsync(h->hist + (size_t)(h->hist_len + 1) * h->N, h->u,
+                           h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+        h->hist_dt.push_back(dts);
+        h->hist_len++;
+      } else {
+        h->hist_overflow = true;
+      }
+    }
     if (rc != PFGPU_OK) {
       set_err("pfgpu_advance: time step %d failed after 3 convergence failures", s);
       return PFGPU_NOT_CONVERGED;
     }
   }
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Discrete adjoint (no counterpart in the reference)
+// ---------------------------------------------------------------------------
+int pfgpu_adjoint_record(pfgpu_handle *h, int max_steps) {
+  if (!h || max_steps < 1) { set_err("pfgpu_adjoint_record: bad argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->st));
+  cudaFree(h->hist);
+  h->hist = nullptr;
+  if (dalloc(&h->hist, (long long)(max_steps + 1) * h->N)) return PFGPU_ERR_NOMEM;
+  CK(cudaMemcpyAsync(h->hist, h->u, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  h->hist_cap = max_steps;
+  h->hist_len = 0;
+  h->hist_dt.clear();
+  h->hist_overflow = false;
+  h->recording = true;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+// J^T lam = rhs by right-preconditioned GMRES (the forward SPGMR on the
+// transposed operator, same multigrid preconditioner), restarted on the true
+// residual until ||rhs - J^T lam|| <= tol ||rhs||
+static int adjoint_solve(pfgpu_handle *h, double *lam, const double *rhs, double *r, double *dx,
+                         double tol, const double *u, double dt, int *iters) {
+  const long long N = h->N;
+  double *sc = h->dsc;
+  launch_dot(rhs, rhs, N, sc + D_COUNT, h->rb, h->st);
+  if (read_scalars(h, D_COUNT, 1)) return PFGPU_ERR_CUDA;
+  const double bnorm = sqrt(h->hsc[D_COUNT]);
+  launch_fill(lam, 0.0, N, h->st);
+  if (bnorm == 0.0) return 0;
+  CK(cudaMemcpyAsync(r, rhs, N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+  h->adj_transpose = true;
+  int rc = 0;
+  for (int outer = 0; outer < 100; outer++) {
+    pfgpu_stats st{};
+    int status = 0;
+    rc = spgmr(h, dx, r, 0.5 * tol * bnorm, u, dt, &st, &status);
+    *iters += st.lin_iters;
+    if (rc) break;
+    launch_xpay(lam, lam, 1.0, dx, N, h->st);
+    matvec(h, lam, dx);
+    launch_axpby(r, rhs, 1.0, 0.0, N, h->st);
+    launch_xpay(r, r, -1.0, dx, N, h->st);
+    launch_dot(r, r, N, sc + D_COUNT, h->rb, h->st);
+    h->launches += 4;
+    if (read_scalars(h, D_COUNT, 1)) { rc = PFGPU_ERR_CUDA; break; }
+    if (sqrt(h->hsc[D_COUNT]) <= tol * bnorm) break;
+    if (status == 2 || status == 6) {
+      set_err("adjoint GMRES made no progress (status %d)", status);
+      rc = PFGPU_NOT_CONVERGED;
+      break;
+    }
+  }
+  h->adj_transpose = false;
+  return rc;
+}
+
+int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps, int nobs,
+                           const long long *obs_cells, const double *obs_values, double tol,
+                           double *misfit, double *grad_lnk, double *grad_alpha,
+                           double *grad_n) {
+  if (!h || nobs_steps < 0 || nobs < 0 || (nobs > 0 && (!obs_cells || !obs_values)) ||
+      (nobs_steps > 0 && !obs_steps) || !(tol > 0)) {
+    set_err("pfgpu_adjoint_gradient: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  if (!h->recording || h->hist_len < 1) {
+    set_err("pfgpu_adjoint_gradient: no recorded steps (pfgpu_adjoint_record, then pfgpu_advance)");
+    return PFGPU_ERR_STATE;
+  }
+  if (h->hist_overflow) {
+    set_err("pfgpu_adjoint_gradient: more steps were advanced than recorded");
+    return PFGPU_ERR_STATE;
+  }
+  for (int k = 0; k < nobs_steps; k++)
+    if (obs_steps[k] < 1 || obs_steps[k] > h->hist_len) {
+      set_err("pfgpu_adjoint_gradient: observation step %d outside 1..%d", obs_steps[k], h->hist_len);
+      return PFGPU_ERR_ARG;
+    }
+  for (int m = 0; m < nobs; m++)
+    if (obs_cells[m] < 0 || obs_cells[m] >= h->N) {
+      set_err("pfgpu_adjoint_gradient: observation cell out of range");
+      return PFGPU_ERR_ARG;
+    }
+  CK(cudaSetDevice(h->device));
+  const long long N = h->N;
+  if (!h->adj && dalloc(&h->adj, 8 * N)) return PFGPU_ERR_NOMEM;
+  double *lam = h->adj, *lam_next = h->adj + N, *rhs = h->adj + 2 * N, *r = h->adj + 3 * N,
+         *dx = h->adj + 4 * N, *g_lnk = h->adj + 5 * N, *g_a = h->adj + 6 * N,
+         *g_n = h->adj + 7 * N;
+  // observations on the device
+  long long *d_cells = nullptr;
+  double *d_obs = nullptr, *d_pick = nullptr;
+  const size_t nov = (size_t)nobs_steps * nobs;
+  if (nobs > 0) {
+    CK(cudaMalloc((void **)&d_cells, nobs * sizeof(long long)));
+    CK(cudaMalloc((void **)&d_obs, (nov + nobs) * sizeof(double)));
+    d_pick = d_obs + nov;
+    CK(cudaMemcpy(d_cells, obs_cells, nobs * sizeof(long long), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(d_obs, obs_values, nov * sizeof(double), cudaMemcpyHostToDevice));
+  }
+  launch_fill(lam_next, 0.0, N, h->st);
+  launch_fill(g_lnk, 0.0, N, h->st);
+  launch_fill(g_a, 0.0, N, h->st);
+  launch_fill(g_n, 0.0, N, h->st);
+  double J = 0.0;
+  int rc = 0, iters = 0;
+  std::vector<double> pick(nobs);
+  for (int n = h->hist_len; n >= 1 && rc == 0; n--) {
+    const double *pn = h->hist + (size_t)n * N, *pprev = h->hist + (size_t)(n - 1) * N;
+    const double dt = h->hist_dt[n - 1];
+    h->vg_for = nullptr;
+    pc_setup_dense(h, pn, dt, true);  // VG state, J and the multigrid at p_n
+    launch_adj_rhs(h->P, pn, h->sat, h->dsat, lam_next, rhs, h->st);
+    h->launches++;
+    for (int k = 0; k < nobs_steps; k++)
+      if (obs_steps[k] == n) {
+        launch_adj_obs(nobs, d_cells, d_obs + (size_t)k * nobs, pn, rhs, h->st);
+        launch_gather(nobs, d_cells, pn, d_pick, h->st);
+        h->launches += 2;
+        CK(cudaMemcpyAsync(pick.data(), d_pick, nobs * sizeof(double), cudaMemcpyDeviceToHost,
+                           h->st));
+        CK(cudaStreamSynchronize(h->st));
+        for (int m = 0; m < nobs; m++) {
+          const double e = pick[m] - obs_values[(size_t)k * nobs + m];
+          J += e * e;
+        }
+      }
+    rc = adjoint_solve(h, lam, rhs, r, dx, tol, pn, dt, &iters);
+    if (rc) break;
+    launch_adj_grad(h->P, pn, pprev, lam, h->kr, dt, g_lnk, g_a, g_n, h->st);
+    h->launches++;
+    std::swap(lam, lam_next);
+  }
+  cudaFree(d_cells);
+  cudaFree(d_obs);
+  h->vg_for = nullptr;
+  h->jac_valid = 0;
+  if (rc) return rc < 0 ? rc : PFGPU_NOT_CONVERGED;
+  if (misfit) *misfit = J;
+  if (grad_lnk && out_vec(h, g_lnk, grad_lnk)) return PFGPU_ERR_CUDA;
+  if (grad_alpha && out_vec(h, g_a, grad_alpha)) return PFGPU_ERR_CUDA;
+  if (grad_n && out_vec(h, g_n, grad_n)) return PFGPU_ERR_CUDA;
   CK(cudaStreamSynchronize(h->st));
   return PFGPU_OK;
 }

@@ -185,6 +185,19 @@ void launch_axpy_gated(double *y, const double *x, const double *coef, const dou
 void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st);
 void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st);
 
+// ---- discrete adjoint (adjoint.cu) ------------------------------------------
+template <typename TJ>
+void launch_matvec7_t(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double *y,
+                      cudaStream_t st);
+void launch_adj_rhs(const DevProblem &P, const double *p, const double *sat, const double *dsat,
+                    const double *lam_next, double *rhs, cudaStream_t st);
+void launch_gather(int n, const long long *idx, const double *src, double *dst, cudaStream_t st);
+void launch_adj_obs(int nobs, const long long *cells, const double *obs, const double *p,
+                    double *rhs, cudaStream_t st);
+void launch_adj_grad(const DevProblem &P, const double *p, const double *p_prev,
+                     const double *lam, const double *kr, double dt, double *g_lnk, double *g_a,
+                     double *g_n, cudaStream_t st);
+
 // sets the message pfgpu_last_error returns on this thread
 void record_error(const char *msg);
 

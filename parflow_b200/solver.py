@@ -208,6 +208,32 @@ class RichardsGPU:
             ps.append(self.get_pressure())
         return ps, sts
 
+    # ---- discrete adjoint ------------------------------------------------------
+    def adjoint_record(self, max_steps: int):
+        """Start recording the trajectory at the current pressure."""
+        L.check(self.lib.pfgpu_adjoint_record(self.h, max_steps), "adjoint_record")
+
+    def adjoint_gradient(self, obs_steps, obs_cells, obs_values, tol: float = 1e-10):
+        """Misfit sum (p_n[c] - obs)^2 over the observed steps/cells of the
+        recorded trajectory and its gradient w.r.t. per-cell ln K, alpha, n
+        (each (nz, ny, nx)).  obs_cells are dense indices i + nx*(j + ny*k);
+        obs_values has shape (len(obs_steps), len(obs_cells))."""
+        steps = np.ascontiguousarray(obs_steps, dtype=np.int32)
+        cells = np.ascontiguousarray(obs_cells, dtype=np.int64)
+        vals = np.ascontiguousarray(obs_values, dtype=np.float64).reshape(len(steps), len(cells))
+        shape_p = tuple(n + 2 for n in self.prob.shape)
+        g = [np.zeros(shape_p) for _ in range(3)]
+        misfit = C.c_double()
+        rc = self.lib.pfgpu_adjoint_gradient(
+            self.h, len(steps), steps.ctypes.data_as(C.POINTER(C.c_int)), len(cells),
+            cells.ctypes.data_as(C.POINTER(C.c_longlong)),
+            vals.ctypes.data_as(C.POINTER(C.c_double)), tol, C.byref(misfit),
+            *[_ptr(a) for a in g])
+        L.check(rc, "adjoint_gradient")
+        if rc != L.OK:
+            raise L.PfgpuError("adjoint_gradient: " + L.last_error())
+        return misfit.value, unpad(g[0]), unpad(g[1]), unpad(g[2])
+
     def time_kernel(self, name: str, reps: int = 10):
         """(ms per launch, algorithmic bytes per launch) of one library kernel."""
         ms, by = C.c_double(), C.c_double()
