@@ -183,22 +183,23 @@ def run_reference_cpu(nsteps: int, threads: int, workload: str = "hetero"):
 def reference_arm(args, rank, world):
     if rank != 0:
         return
+    # the reference has no ensemble driver or adjoint: those fall back to the
+    # headline workload's sample
+    wl_name = args.workload if args.workload in ("hetero", "overland") else "hetero"
     threads = os.cpu_count() or 1
     total = 0.0
     per = []
     k = max(1, args.steps)
     # each step: one bounded reference sample of 2 timesteps
     for _ in range(k):
-        v, info = run_reference_cpu(2, threads, args.workload if args.workload != "ensemble"
-                                    else "hetero")
+        v, info = run_reference_cpu(2, threads, wl_name)
         per.append(v)
     value = float(np.median(per))
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "timesteps/s",
            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
            "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": _workloads()[args.workload if args.workload != "ensemble"
-                                                else "hetero"]["label"] + ", sampled"},
+           "config": {"workload": _workloads()[wl_name]["label"] + ", sampled"},
            "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": info["cores"],
                             "kind": info["kind"], "sample": info["sample"]},
            "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
@@ -483,6 +484,108 @@ def ensemble_arm(args, rank, world, local_rank):
         }), flush=True)
 
 
+# ---------------------------------------------------------------------------
+# Adjoint workload (config 4): gradient of a misfit w.r.t. ln K, alpha, n
+# ---------------------------------------------------------------------------
+def adjoint_arm(args, rank, world, local_rank):
+    """Forward run (20 FP64 steps, 128x128x32, trajectory recorded) plus the
+    discrete-adjoint gradient of sum (p - p_obs)^2 over 256 observation cells
+    at steps 5/10/15/20, timed on the device; then a central-difference check
+    of the gradient with the same forward model (ResidualTol 1e-13)."""
+    import torch
+
+    from parflow_b200 import configs
+    from parflow_b200.problem import SolverSettings
+    from parflow_b200.solver import RichardsGPU
+
+    torch.cuda.set_device(local_rank)
+    nsteps, obs_steps = 20, [5, 10, 15, 20]
+    solver = SolverSettings(residual_tol=1e-13, step_tol=1e-30)
+    prob = configs.box(nx=128, ny=128, nz=32, nsteps=nsteps, dt=0.1, seed=4, solver=solver)
+    shape = prob.shape
+    lnk0 = np.log(prob.perm)
+    prob.vg_alpha = np.full(shape, 2.0)
+    prob.vg_n = np.full(shape, 3.0)
+    rng = np.random.default_rng(40)
+    cells = rng.choice(prob.ncells, size=256, replace=False)
+    plan = prob.time_plan()[:nsteps]
+    g = RichardsGPU(prob, precision="fp64", device=local_rank)
+    stream = torch.cuda.ExternalStream(g.stream())
+
+    def forward(lnk, alpha, vg_n, record=False):
+        prob.perm = np.exp(lnk)
+        prob.vg_alpha, prob.vg_n = alpha, vg_n
+        g._upload_fields()
+        g.set_pressure(prob.initial_pressure())
+        if record:
+            g.adjoint_record(nsteps)
+        ps = {}
+        for n, (t, dt) in enumerate(plan, start=1):
+            g.set_time(t)
+            g.advance(1, dt)
+            if n in obs_steps:
+                ps[n] = g.get_pressure().ravel()[cells]
+        return ps
+
+    alpha0, n0 = prob.vg_alpha.copy(), prob.vg_n.copy()
+    truth = forward(lnk0 + 0.3 * rng.standard_normal(shape), alpha0, n0)
+    obs = np.stack([truth[n] + 0.01 * rng.standard_normal(len(cells)) for n in obs_steps])
+
+    def misfit(ps):
+        return sum(float(np.sum((ps[n] - obs[k]) ** 2)) for k, n in enumerate(obs_steps))
+
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    forward(lnk0, alpha0, n0, record=True)
+    e1.record(stream)
+    m, g_lnk, g_a, g_n = g.adjoint_gradient(obs_steps, cells, obs, tol=1e-12)
+    e2.record(stream)
+    e2.synchronize()
+    t_fwd, t_adj = e0.elapsed_time(e1), e1.elapsed_time(e2)
+    grads = {"lnk": g_lnk, "alpha": g_a, "n": g_n}
+
+    # central differences with the same forward model: the largest-gradient
+    # cells and random cells of each field, and random directions
+    h = 1e-5
+    errs = []
+    for which in ("lnk", "alpha", "n"):
+        ga = np.abs(grads[which]).ravel()
+        floor = 1e-6 * float(ga.max())  # relative error floor for near-zero entries
+        order = np.argsort(-ga)
+        nz = order[:max(4, int(np.count_nonzero(ga > floor)) // 20)]
+        picks = list(order[:4]) + list(rng.choice(nz, 4, replace=False))
+        for c in picks:
+            fields = {"lnk": lnk0.copy(), "alpha": alpha0.copy(), "n": n0.copy()}
+            fields[which].ravel()[c] += h
+            jp = misfit(forward(fields["lnk"], fields["alpha"], fields["n"]))
+            fields[which].ravel()[c] -= 2 * h
+            jm = misfit(forward(fields["lnk"], fields["alpha"], fields["n"]))
+            fd = (jp - jm) / (2 * h)
+            errs.append(abs(grads[which].ravel()[c] - fd) / max(abs(fd), floor))
+    for _ in range(2):
+        d = {k: rng.standard_normal(shape) for k in grads}
+        ad = sum(float(np.sum(grads[k] * d[k])) for k in grads)
+        jp = misfit(forward(lnk0 + h * d["lnk"], alpha0 + h * d["alpha"], n0 + h * d["n"]))
+        jm = misfit(forward(lnk0 - h * d["lnk"], alpha0 - h * d["alpha"], n0 - h * d["n"]))
+        fd = (jp - jm) / (2 * h)
+        errs.append(abs(ad - fd) / abs(fd))
+    g.close()
+    if rank == 0:
+        print(json.dumps({
+            "metric": "adjoint gradient (ln K, alpha, n) of a 20-step misfit, 128x128x32",
+            "value": 1e3 / (t_fwd + t_adj), "unit": "gradients/s", "n_gpus": world,
+            "steps": nsteps, "warmup": 0, "ms_per_step": (t_fwd + t_adj) / nsteps,
+            "higher_is_better": True, "scaling": "weak", "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "box 128x128x32 (524k cells), config-0 physics, 20 steps "
+                                   "dt 0.1 h, 256 observation cells at steps 5/10/15/20",
+                       "residual_tol": 1e-13, "adjoint_gmres_tol": 1e-12},
+            "forward_ms": t_fwd, "adjoint_ms": t_adj, "adjoint_over_forward": t_adj / t_fwd,
+            "misfit": m, "fd_checks": len(errs), "fd_max_rel_err": max(errs),
+            "fd_median_rel_err": float(np.median(errs)), "fd_step": h,
+        }), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -490,7 +593,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
-    ap.add_argument("--workload", default="hetero", choices=["hetero", "overland", "ensemble"],
+    ap.add_argument("--workload", default="hetero",
+                    choices=["hetero", "overland", "ensemble", "adjoint"],
                     help="hetero: the 512x512x50 bench line; overland: the 256x256x20 "
                          "overland hillslope; ensemble: the 48-member set")
     ap.add_argument("--profile", action="store_true",
@@ -509,6 +613,9 @@ def main():
         return
     if args.workload == "ensemble":
         ensemble_arm(args, rank, world, local_rank)
+        return
+    if args.workload == "adjoint":
+        adjoint_arm(args, rank, world, local_rank)
         return
     gpu_arm(args, rank, world, local_rank)
 
