@@ -5,9 +5,23 @@
 // pfsimulator/parflow_lib/matrix.c:258-310, 477-490).  Coarse grids take the
 // even fine indices in the coarsening direction; fine points are the odd ones
 // (pfsimulator/parflow_lib/mg_semi.c:960-1058).
+#include <cstdlib>
+
 #include "pfgpu_kernels.h"
 
 namespace pfgpu {
+
+// Programmatic dependent launch: every multigrid kernel is launched so that
+// its blocks may be scheduled while the previous kernel in the stream drains;
+// it waits here, before touching memory, until that kernel has completed and
+// its writes are visible.  The early trigger lets the next kernel's launch
+// start as soon as this one is running.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#ifndef PFGPU_PDL_LATE_TRIGGER
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
 
 template <typename T>
 struct LV {
@@ -97,6 +111,7 @@ __device__ __forceinline__ void prolong_weights_cell(const MGLevel<T> &F, int i,
 
 template <typename T>
 __global__ void k_prolong_weights(MGLevel<T> F) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   prolong_weights_cell(F, i, j, k);
@@ -150,6 +165,7 @@ __device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLeve
 
 template <typename T>
 __global__ void k_coarse_op(MGLevel<T> F, MGLevel<T> C) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   coarse_op_cell(F, C, i, j, k);
@@ -185,6 +201,7 @@ __device__ __forceinline__ void rb_cell(const MGLevel<T> &Lv, T *__restrict__ x,
 template <typename T>
 __global__ void k_rb_sweep(MGLevel<T> Lv, T *__restrict__ x, const T *__restrict__ b,
                            int colour, int init) {
+  pdl_enter();
   int q, j, k;
   thread_ijk(q, j, k);
   rb_cell(Lv, x, b, colour, init, q, j, k);
@@ -216,6 +233,7 @@ __device__ __forceinline__ void wjacobi_cell(const MGLevel<T> &Lv, const T *__re
 template <typename T>
 __global__ void k_wjacobi(MGLevel<T> Lv, const T *__restrict__ x, const T *__restrict__ b,
                           T *__restrict__ t, int zero) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   wjacobi_cell(Lv, x, b, t, zero, i, j, k);
@@ -234,6 +252,7 @@ __device__ __forceinline__ void wjacobi_update_cell(T *__restrict__ x, const T *
 template <typename T>
 __global__ void k_wjacobi_update(T *__restrict__ x, const T *__restrict__ t, long long n,
                                  T w, int zero) {
+  pdl_enter();
   wjacobi_update_cell(x, t, n, w, zero, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
@@ -260,6 +279,7 @@ __device__ __forceinline__ void mg_residual_cell(const MGLevel<T> &Lv, const T *
 template <typename T>
 __global__ void k_mg_residual(MGLevel<T> Lv, const T *__restrict__ x, const T *__restrict__ b,
                               T *__restrict__ r) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   mg_residual_cell(Lv, x, b, r, i, j, k);
@@ -286,6 +306,7 @@ __device__ __forceinline__ void restrict_cell(const MGLevel<T> &F, const MGLevel
 template <typename T>
 __global__ void k_restrict(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ rf,
                            T *__restrict__ rc) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   restrict_cell(F, C, rf, rc, i, j, k);
@@ -320,6 +341,7 @@ __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLe
 template <typename T>
 __global__ void k_prolong_add(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ ec,
                               T *__restrict__ xf) {
+  pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
   prolong_add_cell(F, C, ec, xf, i, j, k);
@@ -366,6 +388,7 @@ template <typename T>
 __global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restrict__ Ls,
                                                       int first, int nl, int smoother, T w,
                                                       T *tmp) {
+  pdl_enter();
   // down: levels first .. nl-2
   for (int l = first; l <= nl - 2; l++) {
     const MGLevel<T> L = Ls[l];
@@ -407,6 +430,7 @@ __global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restric
 template <typename T>
 __global__ void __launch_bounds__(512) k_setup_tail(const MGLevel<T> *__restrict__ Ls,
                                                      int first, int nl) {
+  pdl_enter();
   for (int l = first; l <= nl - 2; l++) {
     const MGLevel<T> F = Ls[l];
     const MGLevel<T> C = Ls[l + 1];
@@ -427,12 +451,38 @@ __global__ void __launch_bounds__(512) k_setup_tail(const MGLevel<T> *__restrict
 
 template <typename TI, typename TO>
 __global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, long long n) {
+  pdl_enter();
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c < n) out[c] = (TO)in[c];
 }
 
 // ---------------------------------------------------------------------------
 static inline unsigned nb(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+// PFGPU_PDL=0 turns programmatic dependent launch off (plain stream order)
+static bool pdl_on() {
+  static const bool on = [] {
+    const char *v = getenv("PFGPU_PDL");
+    return !(v && *v == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl_on() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
 
 // 3-D launch shape covering (nx, ny, nz): x in warps, rows stacked in y
 struct Shape3 {
@@ -453,18 +503,18 @@ static inline Shape3 shape3(int nx, int ny, int nz) {
 template <typename T>
 void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st) {
   Shape3 g = shape3(F.nx, F.ny, F.nz);
-  k_prolong_weights<T><<<g.grid, g.block, 0, st>>>(F);
+  launch_pdl(k_prolong_weights<T>, dim3(g.grid), dim3(g.block), st, F);
 }
 template <typename T>
 void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st) {
   Shape3 g = shape3(C.nx, C.ny, C.nz);
-  k_coarse_op<T><<<g.grid, g.block, 0, st>>>(F, C);
+  launch_pdl(k_coarse_op<T>, dim3(g.grid), dim3(g.block), st, F, C);
 }
 template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
                      cudaStream_t st) {
   Shape3 g = shape3((L.nx + 1) / 2, L.ny, L.nz);
-  k_rb_sweep<T><<<g.grid, g.block, 0, st>>>(L, x, b, colour, init);
+  launch_pdl(k_rb_sweep<T>, dim3(g.grid), dim3(g.block), st, L, x, b, colour, init);
 }
 // RedBlackGSPoint, MaxIter 1, Symmetric: red, black, red; a zero initial
 // guess turns the first red sweep into x = b / a0 (rb_GS_point.c:107-240)
@@ -473,8 +523,9 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
                       double weight, T *tmp, cudaStream_t st) {
   if (smoother == 1) {
     Shape3 g = shape3(L.nx, L.ny, L.nz);
-    k_wjacobi<T><<<g.grid, g.block, 0, st>>>(L, x, b, tmp, zero);
-    k_wjacobi_update<T><<<nb(L.n, 256), 256, 0, st>>>(x, tmp, L.n, (T)weight, zero);
+    launch_pdl(k_wjacobi<T>, dim3(g.grid), dim3(g.block), st, L, x, b, tmp, zero);
+    launch_pdl(k_wjacobi_update<T>, dim3(nb(L.n, 256)), dim3(256), st, x, tmp, L.n, (T)weight,
+               zero);
     return;
   }
   if (smoother == 2) {  // a single red sweep (kernel timing)
@@ -496,33 +547,34 @@ cudaError_t mg_prepare_kernels() {
 template <typename T>
 void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st) {
   Shape3 g = shape3(L.nx, L.ny, L.nz);
-  k_mg_residual<T><<<g.grid, g.block, 0, st>>>(L, x, b, r);
+  launch_pdl(k_mg_residual<T>, dim3(g.grid), dim3(g.block), st, L, x, b, r);
 }
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
                         cudaStream_t st) {
   Shape3 g = shape3(C.nx, C.ny, C.nz);
-  k_restrict<T><<<g.grid, g.block, 0, st>>>(F, C, rf, rc);
+  launch_pdl(k_restrict<T>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc);
 }
 template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
                            cudaStream_t st) {
   Shape3 g = shape3(F.nx, F.ny, F.nz);
-  k_prolong_add<T><<<g.grid, g.block, 0, st>>>(F, C, ec, xf);
+  launch_pdl(k_prolong_add<T>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf);
 }
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
                         double weight, T *tmp, cudaStream_t st) {
-  k_vcycle_tail<T><<<1, 512, 0, st>>>(levels_dev, first, nl, smoother, (T)weight, tmp);
+  launch_pdl(k_vcycle_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
+             (T)weight, tmp);
 }
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st) {
-  k_setup_tail<T><<<1, 512, 0, st>>>(levels_dev, first, nl);
+  launch_pdl(k_setup_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl);
 }
 
 template <typename TI, typename TO>
 void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
-  k_convert<TI, TO><<<nb(n, 256), 256, 0, st>>>(in, out, n);
+  launch_pdl(k_convert<TI, TO>, dim3(nb(n, 256)), dim3(256), st, in, out, n);
 }
 
 #define INST(T)                                                                              \
