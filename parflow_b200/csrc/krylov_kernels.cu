@@ -6,6 +6,7 @@
 // The scalar GMRES steps (modified Gram-Schmidt bookkeeping, Givens QR,
 // back substitution) run in one thread on device-resident scalars and follow
 // pfsimulator/kinsol/iterativ.c:30-286 and spgmr.c:168-450.
+#include "pdl.cuh"
 #include "pfgpu_kernels.h"
 
 namespace pfgpu {
@@ -47,6 +48,7 @@ template <typename Op>
 __global__ void __launch_bounds__(RED_THREADS) k_reduce(Op op, long long n, double *partial,
                                                         double *dst, unsigned int *ticket,
                                                         const double *gate) {
+  pdl_enter();
   __shared__ double sh[RED_THREADS / 32];
   __shared__ bool last;
   if (gate && *gate == 0.0) return;  // reduction not needed this time
@@ -94,7 +96,7 @@ static void reduce(Op op, long long n, double *dst, ReduceBuf rb, cudaStream_t s
   long long need = (n + RED_THREADS - 1) / RED_THREADS;
   int blocks = (int)(need < rb.blocks ? need : rb.blocks);
   if (blocks < 1) blocks = 1;
-  k_reduce<Op><<<blocks, RED_THREADS, 0, st>>>(op, n, rb.partial, dst, rb.ticket, gate);
+  launch_pdl(k_reduce<Op>, dim3(blocks), dim3(RED_THREADS), st, op, n, rb.partial, dst, rb.ticket, gate);
 }
 
 void launch_dot(const double *a, const double *b, long long n, double *dst, ReduceBuf rb,
@@ -125,6 +127,7 @@ void launch_steplen_diff(const double *a, const double *b, long long n, double *
 // ---- element-wise ---------------------------------------------------------
 __global__ void k_axpy_dev(double *__restrict__ y, const double *__restrict__ x,
                            const double *__restrict__ s, double sign, long long n) {
+  pdl_enter();
   double a = sign * (*s);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
@@ -132,29 +135,34 @@ __global__ void k_axpy_dev(double *__restrict__ y, const double *__restrict__ x,
 }
 __global__ void k_axpby(double *__restrict__ y, const double *__restrict__ x, double a, double b,
                         long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     y[i] = (b == 0.0) ? a * x[i] : a * x[i] + b * y[i];
 }
 __global__ void k_xpay(double *__restrict__ z, const double *__restrict__ x, double a,
                        const double *__restrict__ y, long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     z[i] = x[i] + a * y[i];
 }
 __global__ void k_scale_inv_dev(double *__restrict__ x, const double *__restrict__ s,
                                 long long n) {
+  pdl_enter();
   double a = 1.0 / (*s);
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x[i] *= a;
 }
 __global__ void k_scale(double *__restrict__ x, double a, long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x[i] *= a;
 }
 __global__ void k_fill(double *__restrict__ x, double v, long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x)
     x[i] = v;
@@ -165,6 +173,7 @@ struct VecList {
 // xcor = yg[0] V0 + 0, then xcor = yg[k] Vk + xcor (sequential N_VLinearSum order)
 __global__ void k_combine(double *__restrict__ xcor, VecList V, const double *__restrict__ yg,
                           int kdim, long long n) {
+  pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
     double acc = 0.0;
@@ -180,29 +189,29 @@ static inline int grid_for(long long n) {
 
 void launch_axpy_dev(double *y, const double *x, const double *s, double sign, long long n,
                      cudaStream_t st) {
-  k_axpy_dev<<<grid_for(n), 256, 0, st>>>(y, x, s, sign, n);
+  launch_pdl(k_axpy_dev, dim3(grid_for(n)), dim3(256), st, y, x, s, sign, n);
 }
 void launch_axpby(double *y, const double *x, double a, double b, long long n, cudaStream_t st) {
-  k_axpby<<<grid_for(n), 256, 0, st>>>(y, x, a, b, n);
+  launch_pdl(k_axpby, dim3(grid_for(n)), dim3(256), st, y, x, a, b, n);
 }
 void launch_xpay(double *z, const double *x, double a, const double *y, long long n,
                  cudaStream_t st) {
-  k_xpay<<<grid_for(n), 256, 0, st>>>(z, x, a, y, n);
+  launch_pdl(k_xpay, dim3(grid_for(n)), dim3(256), st, z, x, a, y, n);
 }
 void launch_scale_inv_dev(double *x, const double *s, long long n, cudaStream_t st) {
-  k_scale_inv_dev<<<grid_for(n), 256, 0, st>>>(x, s, n);
+  launch_pdl(k_scale_inv_dev, dim3(grid_for(n)), dim3(256), st, x, s, n);
 }
 void launch_scale(double *x, double a, long long n, cudaStream_t st) {
-  k_scale<<<grid_for(n), 256, 0, st>>>(x, a, n);
+  launch_pdl(k_scale, dim3(grid_for(n)), dim3(256), st, x, a, n);
 }
 void launch_fill(double *x, double v, long long n, cudaStream_t st) {
-  k_fill<<<grid_for(n), 256, 0, st>>>(x, v, n);
+  launch_pdl(k_fill, dim3(grid_for(n)), dim3(256), st, x, v, n);
 }
 void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
                     cudaStream_t st) {
   VecList L;
   for (int k = 0; k < kdim && k < 32; k++) L.v[k] = V[k];
-  k_combine<<<grid_for(n), 256, 0, st>>>(xcor, L, yg, kdim, n);
+  launch_pdl(k_combine, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, n);
 }
 
 // ---- GMRES scalars ----------------------------------------------------------
@@ -242,6 +251,7 @@ __device__ void givens(double t1, double t2, double &c, double &s) {
 }
 
 __global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
+  pdl_enter();
   GS g = gs_view(S, lmax);
   double *sc = g.sc;
   switch (op) {
@@ -328,6 +338,7 @@ __global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
 // Reorthogonalisation decision for basis vector i against V_k
 // (iterativ.c:68-77): dot result in SC_NP; sets SC_GATE (apply?) and SC_COEF.
 __global__ void k_reorth_decide(double *S, int i, int l, int lmax) {
+  pdl_enter();
   GS g = gs_view(S, lmax);
   double *sc = g.sc;
   int k = l + 1;
@@ -346,6 +357,7 @@ __global__ void k_reorth_decide(double *S, int i, int l, int lmax) {
 __global__ void k_axpy_gated(double *__restrict__ y, const double *__restrict__ x,
                              const double *__restrict__ coef, const double *__restrict__ gate,
                              long long n) {
+  pdl_enter();
   if (*gate == 0.0) return;
   double a = *coef;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
@@ -354,19 +366,20 @@ __global__ void k_axpy_gated(double *__restrict__ y, const double *__restrict__ 
 }
 
 void launch_gmres_scalar(int op, double *S, int l, int lmax, cudaStream_t st) {
-  k_gmres_scalar<<<1, 1, 0, st>>>(op, S, l, lmax);
+  launch_pdl(k_gmres_scalar, dim3(1), dim3(1), st, op, S, l, lmax);
 }
 void launch_reorth_decide(double *S, int i, int l, int lmax, cudaStream_t st) {
-  k_reorth_decide<<<1, 1, 0, st>>>(S, i, l, lmax);
+  launch_pdl(k_reorth_decide, dim3(1), dim3(1), st, S, i, l, lmax);
 }
 void launch_axpy_gated(double *y, const double *x, const double *coef, const double *gate,
                        long long n, cudaStream_t st) {
-  k_axpy_gated<<<grid_for(n), 256, 0, st>>>(y, x, coef, gate, n);
+  launch_pdl(k_axpy_gated, dim3(grid_for(n)), dim3(256), st, y, x, coef, gate, n);
 }
 
 // ---- ParFlow layout <-> dense ------------------------------------------------
 __global__ void k_unpad(const double *__restrict__ pad, double *__restrict__ dense, int nx,
                         int ny, int nz) {
+  pdl_enter();
   long long n = (long long)nx * ny * nz;
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
        c += (long long)gridDim.x * blockDim.x) {
@@ -378,6 +391,7 @@ __global__ void k_unpad(const double *__restrict__ pad, double *__restrict__ den
 }
 __global__ void k_pad(const double *__restrict__ dense, double *__restrict__ pad, int nx, int ny,
                       int nz) {
+  pdl_enter();
   long long n = (long long)(nx + 2) * (ny + 2) * (nz + 2);
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
        c += (long long)gridDim.x * blockDim.x) {
@@ -389,10 +403,10 @@ __global__ void k_pad(const double *__restrict__ dense, double *__restrict__ pad
   }
 }
 void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st) {
-  k_unpad<<<grid_for((long long)nx * ny * nz), 256, 0, st>>>(pad, dense, nx, ny, nz);
+  launch_pdl(k_unpad, dim3(grid_for((long long)nx * ny * nz)), dim3(256), st, pad, dense, nx, ny, nz);
 }
 void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st) {
-  k_pad<<<grid_for((long long)(nx + 2) * (ny + 2) * (nz + 2)), 256, 0, st>>>(dense, pad, nx, ny,
+  launch_pdl(k_pad, dim3(grid_for((long long)(nx + 2) * (ny + 2) * (nz + 2))), dim3(256), st, dense, pad, nx, ny,
                                                                              nz);
 }
 

@@ -5,23 +5,10 @@
 // pfsimulator/parflow_lib/matrix.c:258-310, 477-490).  Coarse grids take the
 // even fine indices in the coarsening direction; fine points are the odd ones
 // (pfsimulator/parflow_lib/mg_semi.c:960-1058).
-#include <cstdlib>
-
+#include "pdl.cuh"
 #include "pfgpu_kernels.h"
 
 namespace pfgpu {
-
-// Programmatic dependent launch: every multigrid kernel is launched so that
-// its blocks may be scheduled while the previous kernel in the stream drains;
-// it waits here, before touching memory, until that kernel has completed and
-// its writes are visible.  The early trigger lets the next kernel's launch
-// start as soon as this one is running.
-__device__ __forceinline__ void pdl_enter() {
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-#ifndef PFGPU_PDL_LATE_TRIGGER
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-#endif
-}
 
 template <typename T>
 struct LV {
@@ -458,31 +445,6 @@ __global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, long 
 
 // ---------------------------------------------------------------------------
 static inline unsigned nb(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
-
-// PFGPU_PDL=0 turns programmatic dependent launch off (plain stream order)
-static bool pdl_on() {
-  static const bool on = [] {
-    const char *v = getenv("PFGPU_PDL");
-    return !(v && *v == '0');
-  }();
-  return on;
-}
-
-template <typename... KArgs, typename... Args>
-static void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
-                       Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = st;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = pdl_on() ? 1 : 0;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
-}
 
 // 3-D launch shape covering (nx, ny, nz): x in warps, rows stacked in y
 struct Shape3 {

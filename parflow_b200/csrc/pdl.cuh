@@ -1,0 +1,48 @@
+// Programmatic dependent launch (PDL) helpers shared by the kernel files.
+//
+// A kernel launched with launch_pdl may have its blocks scheduled while the
+// previous kernel in the stream is still draining; it calls pdl_enter()
+// first, which waits until that kernel has completed and its writes are
+// visible, then lets the next kernel's launch begin.  Kernels launched this
+// way keep exact stream order for memory; only launch latency overlaps.
+// PFGPU_PDL=0 in the environment turns the attribute off.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+
+namespace pfgpu {
+
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+#ifndef PFGPU_PDL_LATE_TRIGGER
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+#endif
+}
+
+inline bool pdl_on() {
+  static const bool on = [] {
+    const char *v = getenv("PFGPU_PDL");
+    return !(v && *v == '0');
+  }();
+  return on;
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl_on() ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+}  // namespace pfgpu

@@ -7,6 +7,7 @@
 // (k_vg_all) so that each cell's van Genuchten state is evaluated once per
 // iterate and shared by the residual and the Jacobian.
 #include "pfgpu_device.cuh"
+#include "pdl.cuh"
 #include "pfgpu_kernels.h"
 
 namespace pfgpu {
@@ -26,6 +27,7 @@ __device__ __forceinline__ bool launch_ijk(int nx, int ny, int nz, int &i, int &
 __global__ void k_vg_all(DevProblem P, const double *__restrict__ p, double *__restrict__ kr,
                          double *__restrict__ dkr, double *__restrict__ sat,
                          double *__restrict__ dsat) {
+  pdl_enter();
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= P.n) return;
   VGAll v = vg_all(P, p[c], vg_at(P, c));
@@ -36,6 +38,7 @@ __global__ void k_vg_all(DevProblem P, const double *__restrict__ p, double *__r
 }
 
 __global__ void k_saturation(DevProblem P, const double *__restrict__ p, double *__restrict__ s) {
+  pdl_enter();
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= P.n) return;
   s[c] = vg_all(P, p[c], vg_at(P, c)).s;
@@ -45,10 +48,13 @@ __global__ void k_saturation(DevProblem P, const double *__restrict__ p, double 
 // follows the reference: accumulation, storage, sources, then the face
 // fluxes scattered from the k-1, j-1, i-1 neighbours, the cell's own three
 // upper faces, and finally the boundary patches in patch order.
+// SURF: slopes and/or overland flow present (false: flat box, the lean path)
+template <bool SURF>
 __global__ void k_residual(DevProblem P, const double *__restrict__ p,
                            const double *__restrict__ p_old, const double *__restrict__ s_old,
                            const double *__restrict__ kr, const double *__restrict__ satv,
                            double dt, double *__restrict__ f) {
+  pdl_enter();
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
   const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
@@ -71,26 +77,26 @@ __global__ void k_residual(DevProblem P, const double *__restrict__ p,
     double zl = __ldg(P.zmult + k - 1);
     fc += -dt * flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
   }
-  double gs, gc;
+  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
   if (j > 0) {
     long long s = c - sy;
-    tfg_face_y(P, i, j - 1, gs, gc);
+    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
     fc += -dt * flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm, gs, gc);
   }
   if (i > 0) {
     long long w = c - 1;
-    tfg_face_x(P, i - 1, j, gs, gc);
+    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
     fc += -dt * flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm, gs, gc);
   }
   double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
   if (i + 1 < P.nx) {
     long long e = c + 1;
-    tfg_face_x(P, i, j, gs, gc);
+    if (SURF) tfg_face_x(P, i, j, gs, gc);
     u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm, gs, gc);
   }
   if (j + 1 < P.ny) {
     long long nn = c + sy;
-    tfg_face_y(P, i, j, gs, gc);
+    if (SURF) tfg_face_y(P, i, j, gs, gc);
     u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm, gs, gc);
   }
   if (k + 1 < P.nz) {
@@ -112,7 +118,7 @@ __global__ void k_residual(DevProblem P, const double *__restrict__ p,
     if (P.bc_type[face] == 0) {
       double h = (face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz;
       u_new = h * value;
-    } else if (P.bc_type[face] == 2) {
+    } else if (SURF && P.bc_type[face] == 2) {
       // OverlandKinematic top face (nl_function_eval.c:1786-2000): ponding and
       // routing term, then the rain flux like FluxConst
       const OvCell o = ov_cell(P, i, j);
@@ -224,11 +230,12 @@ __device__ __forceinline__ FaceDer face_der_z(const DevProblem &P, double dt, do
 // 7-point J (C W E S N L U, FP64 or FP32) and the symmetric preconditioner
 // matrix (C E N U: full diagonal, symmetric off-diagonal parts; PCMatrixType
 // PFSymmetric), in the preconditioner's precision.
-template <typename TJ, typename TP>
+template <typename TJ, typename TP, bool SURF>
 __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
                            const double *__restrict__ kr, const double *__restrict__ dkr,
                            const double *__restrict__ satv, const double *__restrict__ dsatv,
                            double dt, JacOut<TJ> J, PCOut<TP> M) {
+  pdl_enter();
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
   const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
@@ -257,10 +264,10 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
     cp += -d.hi;
     l = d.lo;
   }
-  double gs, gc;
+  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
   if (j > 0) {
     long long q = c - sy;
-    tfg_face_y(P, i, j - 1, gs, gc);
+    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffy, P.dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
                             dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
@@ -268,7 +275,7 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
   }
   if (i > 0) {
     long long q = c - 1;
-    tfg_face_x(P, i - 1, j, gs, gc);
+    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffx, P.dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
                             dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
@@ -277,7 +284,7 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
   double west_t = 0.0, south_t = 0.0, lower_t = 0.0;
   if (i + 1 < P.nx) {
     long long q = c + 1;
-    tfg_face_x(P, i, j, gs, gc);
+    if (SURF) tfg_face_x(P, i, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffx, P.dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
                             kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     west_t = d.lo;
@@ -286,7 +293,7 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
   }
   if (j + 1 < P.ny) {
     long long q = c + sy;
-    tfg_face_y(P, i, j, gs, gc);
+    if (SURF) tfg_face_y(P, i, j, gs, gc);
     FaceDer d = face_der_xy(P, dt, ffy, P.dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
                             kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     south_t = d.lo;
@@ -368,7 +375,7 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
   // terms belong to the neighbour's E / N entry (lower coefficient aliasing,
   // matrix.c:484-490): E(i) gets this cell's east term, then the east
   // neighbour's west term, in the reference's loop order.
-  if (k == P.nz - 1 && P.bc_type[5] == 2) {
+  if (SURF && k == P.nz - 1 && P.bc_type[5] == 2) {
     const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
     const double two3 = 2.0 / 3.0;
     const OvCell o = ov_cell(P, i, j);
@@ -432,6 +439,7 @@ __global__ void k_jacobian(DevProblem P, const double *__restrict__ p,
 template <typename TJ>
 __global__ void k_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *__restrict__ x,
                           double *__restrict__ y) {
+  pdl_enter();
   int i, j, k;
   if (!launch_ijk(nx, ny, nz, i, j, k)) return;
   const long long c = i + (long long)nx * (j + (long long)ny * k);
@@ -465,11 +473,11 @@ static inline void shape(int nx, int ny, int nz, int threads, dim3 &grid, dim3 &
 
 void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
                    double *dsat, cudaStream_t st) {
-  k_vg_all<<<blocks_for(P.n, 256), 256, 0, st>>>(P, p, kr, dkr, sat, dsat);
+  launch_pdl(k_vg_all, dim3(blocks_for(P.n, 256)), dim3(256), st, P, p, kr, dkr, sat, dsat);
 }
 
 void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStream_t st) {
-  k_saturation<<<blocks_for(P.n, 256), 256, 0, st>>>(P, p, s);
+  launch_pdl(k_saturation, dim3(blocks_for(P.n, 256)), dim3(256), st, P, p, s);
 }
 
 void launch_residual(const DevProblem &P, const double *p, const double *p_old,
@@ -477,7 +485,10 @@ void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      double *f, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 256, g, b);
-  k_residual<<<g, b, 0, st>>>(P, p, p_old, s_old, kr, sat, dt, f);
+  if (P.tfg_xs || P.bc_type[5] == 2)
+    launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
+  else
+    launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
 }
 
 template <typename TJ, typename TP>
@@ -486,7 +497,11 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
                      JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 128, g, b);
-  k_jacobian<TJ, TP><<<g, b, 0, st>>>(P, p, kr, dkr, sat, dsat, dt, J, M);
+  if (P.tfg_xs || P.bc_type[5] == 2)
+    launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J, M);
+  else
+    launch_pdl(k_jacobian<TJ, TP, false>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J,
+               M);
 }
 
 template <typename TJ>
@@ -494,7 +509,7 @@ void launch_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double
                     cudaStream_t st) {
   dim3 g, b;
   shape(nx, ny, nz, 256, g, b);
-  k_matvec7<TJ><<<g, b, 0, st>>>(nx, ny, nz, J, x, y);
+  launch_pdl(k_matvec7<TJ>, dim3(g), dim3(b), st, nx, ny, nz, J, x, y);
 }
 
 template void launch_jacobian<double, double>(const DevProblem &, const double *,
