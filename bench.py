@@ -208,6 +208,26 @@ def reference_arm(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+# replicas: every rank solves its own copy; the job's time is the slowest rank
+# ---------------------------------------------------------------------------
+def max_over_ranks(ms: float, dist=None, device: str = "cuda") -> float:
+    """Device-timed milliseconds of this rank -> the maximum over all ranks
+    (one all-reduce of a scalar; NCCL on the GPU box, gloo in the tests)."""
+    if dist is None:
+        return ms
+    import torch
+
+    tt = torch.tensor([ms], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def job_throughput(steps: int, world: int, ms_max: float) -> float:
+    """Whole-job timesteps/s: every rank's steps over the slowest rank's time."""
+    return steps * world / (ms_max * 1e-3)
+
+
+# ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
 def gpu_arm(args, rank, world, local_rank):
@@ -264,10 +284,7 @@ def gpu_arm(args, rank, world, local_rank):
         ck = clocks.stop()
         ms = e0.elapsed_time(e1)
         launches = s.kernel_launches() - launches0
-        if dist:
-            tt = torch.tensor([ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            ms = float(tt.item())
+        ms = max_over_ranks(ms, dist)
         p_final = s.get_pressure()
         return s, ms, stats[args.warmup:], launches, ck, p_final
 
@@ -349,10 +366,7 @@ def gpu_arm(args, rank, world, local_rank):
     nbytes = int(np.prod(shape_p)) * 8
     h2d = 4 * nbytes   # newton: p_old, s_old, p; saturation: p
     d2h = 2 * nbytes   # newton: p; saturation: s
-    if dist:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+    e2e_ms = max_over_ranks(e2e_ms, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -365,8 +379,8 @@ def gpu_arm(args, rank, world, local_rank):
                    "sample": f"failed: {e}"}
 
     if rank == 0:
-        steps_mx = args.steps * world / (msmx * 1e-3)
-        steps_64 = args.steps * world / (ms64 * 1e-3)
+        steps_mx = job_throughput(args.steps, world, msmx)
+        steps_64 = job_throughput(args.steps, world, ms64)
         newton = sum(x.nonlin_iters for x in stmx)
         out = {
             "metric": METRIC, "value": steps_mx, "unit": "timesteps/s", "n_gpus": world,
