@@ -138,8 +138,10 @@ __device__ __forceinline__ double vg_dkr(const DevProblem &P, double p, double a
 
 // All four van Genuchten quantities of one cell from one log(alpha h) and one
 // log1p((alpha h)^n): every power of the reference formulas
-// (problem_saturation.c:221-415, problem_phase_rel_perm.c:788, :981) is
-// rewritten as exp(y * log x) over these two logarithms.
+// (problem_saturation.c:221-415, problem_phase_rel_perm.c:788, :981) comes
+// from two exponentials of these logarithms, one reciprocal of alpha h (for
+// the (alpha h)^(n-1), (alpha h)^(n-2) factors), one reciprocal of
+// 1 + (alpha h)^n and one square root ((1+A)^(-m/2) = sqrt((1+A)^(-m))).
 struct VGAll {
   double kr, dkr, s, ds;
 };
@@ -157,18 +159,16 @@ __device__ __forceinline__ VGAll vg_all(const DevProblem &P, double p, const VG 
   const double n = v.n, alpha = v.alpha;
   const double m = 1.0 - (1.0 / n);
   const double head = fabs(p) / (P.density * P.gravity);
-  const double L = log(alpha * head);
-  const double ahn = exp(n * L);           // (alpha h)^n
-  const double ahnm1 = exp((n - 1) * L);   // (alpha h)^(n-1)
-  const double ahnm2 = exp((n - 2) * L);   // (alpha h)^(n-2)
+  const double ah = alpha * head;
+  const double ahn = exp(n * log(ah));     // (alpha h)^n
+  const double inv_ah = 1.0 / ah;
+  const double ahnm1 = ahn * inv_ah;       // (alpha h)^(n-1)
+  const double ahnm2 = ahnm1 * inv_ah;     // (alpha h)^(n-2)
   const double lop = log1p(ahn);           // log(1 + (alpha h)^n)
-  const double opahn = 1.0 + ahn;
-  const double opm = exp(m * lop);         // opahn^m
-  const double opm2 = exp(0.5 * m * lop);  // opahn^(m/2)
-  const double inv_opm = 1.0 / opm;
+  const double inv_opm = exp(-m * lop);    // opahn^-m
+  const double inv_opm2 = sqrt(inv_opm);   // opahn^(-m/2)
+  const double inv_op = 1.0 / (1.0 + ahn);
   const double t = 1.0 - ahnm1 * inv_opm;
-  const double inv_opm2 = 1.0 / opm2;
-  const double inv_op = 1.0 / opahn;
   r.kr = (t * t) * inv_opm2;
   r.dkr = 2.0 * (t * inv_opm2) *
               ((n - 1) * ahnm2 * alpha * inv_opm - ahnm1 * m * (inv_opm * inv_op) * n * alpha * ahnm1) +
