@@ -124,6 +124,198 @@ void launch_steplen_diff(const double *a, const double *b, long long n, double *
   reduce(op, n, dst, rb, st);
 }
 
+// ---- fused multi-value reductions ------------------------------------------
+// One pass over the vectors for several sums / maxima that the solver needs
+// together; each value is reduced exactly like k_reduce (per-thread grid-
+// stride accumulation, fixed-order block and final combination).  An op
+// may also update a vector element-wise in the same pass (MGS axpy).
+static const int RED_MAX_K = 4;
+
+template <typename Op>
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_multi(Op op, long long n,
+                                                              double *partial,
+                                                              unsigned int *ticket) {
+  constexpr int K = Op::K;
+  pdl_enter();
+  __shared__ double sh[K][RED_THREADS / 32];
+  __shared__ bool last;
+  Op o = op;
+  o.setup();
+  double acc[K];
+#pragma unroll
+  for (int q = 0; q < K; q++) acc[q] = 0.0;
+  for (long long i = blockIdx.x * (long long)RED_THREADS + threadIdx.x; i < n;
+       i += (long long)gridDim.x * RED_THREADS)
+    o.acc(i, acc);
+#pragma unroll
+  for (int q = 0; q < K; q++) {
+    double a = acc[q];
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) a = Op::comb(q, a, __shfl_down_sync(0xffffffffu, a, w));
+    if ((threadIdx.x & 31) == 0) sh[q][threadIdx.x >> 5] = a;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      double b = sh[q][0];
+      for (int w = 1; w < RED_THREADS / 32; w++) b = Op::comb(q, b, sh[q][w]);
+      partial[q * gridDim.x + blockIdx.x] = b;
+    }
+    __threadfence();
+    unsigned int t = atomicAdd(ticket, 1u);
+    last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+#pragma unroll
+  for (int q = 0; q < K; q++) {
+    double v = 0.0;
+    for (int i = threadIdx.x; i < (int)gridDim.x; i += RED_THREADS) {
+      double pv = ((volatile double *)partial)[q * gridDim.x + i];
+      v = (i == (int)threadIdx.x) ? pv : Op::comb(q, v, pv);
+    }
+#pragma unroll
+    for (int w = 16; w > 0; w >>= 1) v = Op::comb(q, v, __shfl_down_sync(0xffffffffu, v, w));
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) sh[q][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < K; q++) {
+      double r = sh[q][0];
+      for (int w = 1; w < RED_THREADS / 32; w++) r = Op::comb(q, r, sh[q][w]);
+      *o.dst[q] = r;
+    }
+    *ticket = 0u;
+  }
+}
+
+__device__ __forceinline__ double comb_sum(double x, double y) { return x + y; }
+__device__ __forceinline__ double comb_max(double x, double y) { return x > y ? x : y; }
+
+// <vk, vk> and <v0, vk> (the first two dot products of ModifiedGS)
+struct OpMgsFirst {
+  static constexpr int K = 2;
+  const double *vk, *v0;
+  double *dst[K];
+  __device__ void setup() {}
+  __device__ void acc(long long i, double *v) const {
+    const double a = vk[i];
+    v[0] = v[0] + a * a;
+    v[1] = v[1] + v0[i] * a;
+  }
+  __device__ static double comb(int, double x, double y) { return comb_sum(x, y); }
+};
+// y = y + sign * (*s) x, then <z, y> with the updated y (z = y when null):
+// one ModifiedGS projection fused with the next dot product
+struct OpAxpyDot {
+  static constexpr int K = 1;
+  double *y;
+  const double *x, *s, *z;
+  double sign, a;
+  double *dst[K];
+  __device__ void setup() { a = sign * (*s); }
+  __device__ void acc(long long i, double *v) {
+    const double yn = y[i] + a * x[i];
+    y[i] = yn;
+    const double zi = z ? z[i] : yn;
+    v[0] = v[0] + zi * yn;
+  }
+  __device__ static double comb(int, double x, double y) { return comb_sum(x, y); }
+};
+// line-search inputs after the Newton direction p: <Jp, Jp>, <f, Jp>, <p, p>
+// and max |p| / (1 + |u|)
+struct OpLineSearchIn {
+  static constexpr int K = 4;
+  const double *jp, *f, *p, *u;
+  double *dst[K];
+  __device__ void setup() {}
+  __device__ void acc(long long i, double *v) const {
+    const double j = jp[i], pi = p[i];
+    v[0] = v[0] + j * j;
+    v[1] = v[1] + f[i] * j;
+    v[2] = v[2] + pi * pi;
+    v[3] = comb_max(v[3], fabs(pi / (1.0 / 1.0 + fabs(u[i]))));
+  }
+  __device__ static double comb(int q, double x, double y) {
+    return q == 3 ? comb_max(x, y) : comb_sum(x, y);
+  }
+};
+// after a trial step: <f, f>, max |f| and max |unew - u| / (1 + |unew|)
+struct OpStepNorms {
+  static constexpr int K = 3;
+  const double *f, *unew, *u;
+  double *dst[K];
+  __device__ void setup() {}
+  __device__ void acc(long long i, double *v) const {
+    const double fi = f[i], a = unew[i];
+    v[0] = v[0] + fi * fi;
+    v[1] = comb_max(v[1], fabs(fi));
+    v[2] = comb_max(v[2], fabs((a - u[i]) / (1.0 / 1.0 + fabs(a))));
+  }
+  __device__ static double comb(int q, double x, double y) {
+    return q == 0 ? comb_sum(x, y) : comb_max(x, y);
+  }
+};
+// at KINSol's start: <u, u>, max |f|, <f, f>
+struct OpInitNorms {
+  static constexpr int K = 3;
+  const double *u, *f;
+  double *dst[K];
+  __device__ void setup() {}
+  __device__ void acc(long long i, double *v) const {
+    const double ui = u[i], fi = f[i];
+    v[0] = v[0] + ui * ui;
+    v[1] = comb_max(v[1], fabs(fi));
+    v[2] = v[2] + fi * fi;
+  }
+  __device__ static double comb(int q, double x, double y) {
+    return q == 1 ? comb_max(x, y) : comb_sum(x, y);
+  }
+};
+
+template <typename Op>
+static void reduce_multi(Op op, long long n, ReduceBuf rb, cudaStream_t st) {
+  long long need = (n + RED_THREADS - 1) / RED_THREADS;
+  int blocks = (int)(need < rb.blocks ? need : rb.blocks);
+  if (blocks < 1) blocks = 1;
+  launch_pdl(k_reduce_multi<Op>, dim3(blocks), dim3(RED_THREADS), st, op, n, rb.partial,
+             rb.ticket);
+}
+
+int reduce_partials() { return RED_BLOCKS * RED_MAX_K; }
+
+void launch_mgs_first(const double *vk, const double *v0, long long n, double *d_vk2,
+                      double *d_h0, ReduceBuf rb, cudaStream_t st) {
+  OpMgsFirst op{vk, v0, {d_vk2, d_h0}};
+  reduce_multi(op, n, rb, st);
+}
+void launch_axpy_dot(double *y, const double *x, const double *s, double sign, const double *z,
+                     long long n, double *dst, ReduceBuf rb, cudaStream_t st) {
+  OpAxpyDot op{y, x, s, z, sign, 0.0, {dst}};
+  reduce_multi(op, n, rb, st);
+}
+void launch_linesearch_inputs(const double *jp, const double *f, const double *p,
+                              const double *u, long long n, double *d_jp2, double *d_fjp,
+                              double *d_p2, double *d_plen, ReduceBuf rb, cudaStream_t st) {
+  OpLineSearchIn op{jp, f, p, u, {d_jp2, d_fjp, d_p2, d_plen}};
+  reduce_multi(op, n, rb, st);
+}
+void launch_step_norms(const double *f, const double *unew, const double *u, long long n,
+                       double *d_f2, double *d_fmax, double *d_step, ReduceBuf rb,
+                       cudaStream_t st) {
+  OpStepNorms op{f, unew, u, {d_f2, d_fmax, d_step}};
+  reduce_multi(op, n, rb, st);
+}
+void launch_init_norms(const double *u, const double *f, long long n, double *d_u2,
+                       double *d_fmax, double *d_f2, ReduceBuf rb, cudaStream_t st) {
+  OpInitNorms op{u, f, {d_u2, d_fmax, d_f2}};
+  reduce_multi(op, n, rb, st);
+}
+
 // ---- element-wise ---------------------------------------------------------
 __global__ void k_axpy_dev(double *__restrict__ y, const double *__restrict__ x,
                            const double *__restrict__ s, double sign, long long n) {

@@ -75,6 +75,23 @@ __device__ __forceinline__ void split_ijk(int t, int nx, int ny, int &i, int &j,
   k = r / ny;
 }
 
+// prolongation weights of one fine point (mg_semi.c:534-575): the
+// along-direction entries over the collapsed diagonal
+template <typename T>
+__device__ __forceinline__ void weights_at(const LV<T> &L, int d, int i, int j, int k, T &w1,
+                                           T &w2) {
+  T ap0 = coef(L, snum(d, 0), i, j, k) + coef(L, snum(d, 3), i, j, k) +
+          coef(L, snum(d, 4), i, j, k) + coef(L, snum(d, 5), i, j, k) +
+          coef(L, snum(d, 6), i, j, k);
+  if (ap0 != T(0)) {
+    w1 = -coef(L, snum(d, 1), i, j, k) / ap0;
+    w2 = -coef(L, snum(d, 2), i, j, k) / ap0;
+  } else {
+    w1 = T(0);
+    w2 = T(0);
+  }
+}
+
 // prolongation weights at fine points (mg_semi.c:534-575)
 template <typename T>
 __device__ __forceinline__ void prolong_weights_cell(const MGLevel<T> &F, int i, int j, int k) {
@@ -83,17 +100,10 @@ __device__ __forceinline__ void prolong_weights_cell(const MGLevel<T> &F, int i,
   int ci = F.dir == 0 ? i : F.dir == 1 ? j : k;
   if (!(ci & 1)) return;
   LV<T> L = lv(F);
-  const int d = F.dir;
-  T ap0 = coef(L, snum(d, 0), i, j, k) + coef(L, snum(d, 3), i, j, k) +
-          coef(L, snum(d, 4), i, j, k) + coef(L, snum(d, 5), i, j, k) +
-          coef(L, snum(d, 6), i, j, k);
-  if (ap0 != T(0)) {
-    F.p1[c] = -coef(L, snum(d, 1), i, j, k) / ap0;
-    F.p2[c] = -coef(L, snum(d, 2), i, j, k) / ap0;
-  } else {
-    F.p1[c] = T(0);
-    F.p2[c] = T(0);
-  }
+  T w1, w2;
+  weights_at(L, F.dir, i, j, k, w1, w2);
+  F.p1[c] = w1;
+  F.p2[c] = w2;
 }
 
 template <typename T>
@@ -107,10 +117,10 @@ __global__ void k_prolong_weights(MGLevel<T> F) {
 // collapsed-stencil coarse operator (mg_semi.c:577-740), stored symmetric:
 // the along-direction upper entry of coarse point c is the value ParFlow
 // leaves there last, i.e. the lower entry written for c+1 when it exists.
+// p2_1 = p2 at fine 2c-1, p1_2 / p2_2 = p1 / p2 at fine 2c+1 (zero outside).
 template <typename T>
-__device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLevel<T> &C, int ic,
-                                               int jc, int kc) {
-  if (ic >= C.nx || jc >= C.ny || kc >= C.nz) return;
+__device__ __forceinline__ void coarse_op_core(const MGLevel<T> &F, const MGLevel<T> &C, int ic,
+                                               int jc, int kc, T p2_1, T p1_2, T p2_2) {
   const long long cc = ic + (long long)C.nx * (jc + (long long)C.ny * kc);
   const int d = F.dir;
   const int ox = d == 0, oy = d == 1, oz = d == 2;
@@ -118,9 +128,6 @@ __device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLeve
   const int i1 = i - ox, j1 = j - oy, k1 = k - oz;
   const int i2 = i + ox, j2 = j + oy, k2 = k + oz;
   LV<T> L = lv(F);
-  const T p2_1 = vget(F.nx, F.ny, F.nz, (const T *)F.p2, i1, j1, k1);
-  const T p1_2 = vget(F.nx, F.ny, F.nz, (const T *)F.p1, i2, j2, k2);
-  const T p2_2 = vget(F.nx, F.ny, F.nz, (const T *)F.p2, i2, j2, k2);
   T ac[7];
 #pragma unroll
   for (int q = 3; q <= 6; q++)
@@ -137,8 +144,7 @@ __device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLeve
     along_up = ac[2];
   } else {
     // lower entry of coarse point c+1: a1(fine 2c+2) * p1(fine 2c+1)
-    along_up = coef(L, snum(d, 1), i + 2 * ox, j + 2 * oy, k + 2 * oz) *
-               vget(F.nx, F.ny, F.nz, (const T *)F.p1, i2, j2, k2);
+    along_up = coef(L, snum(d, 1), i + 2 * ox, j + 2 * oy, k + 2 * oz) * p1_2;
   }
   T E, N, U;
   if (d == 0) { E = along_up; N = ac[4]; U = ac[6]; }
@@ -148,6 +154,53 @@ __device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLeve
   C.a[2][cc] = N;
   C.a[3][cc] = U;
   C.a[0][cc] = ac[0] - (ac[3] + ac[4] + ac[5] + ac[6]);
+}
+
+// coarse operator from stored weights (single-block setup tail)
+template <typename T>
+__device__ __forceinline__ void coarse_op_cell(const MGLevel<T> &F, const MGLevel<T> &C, int ic,
+                                               int jc, int kc) {
+  if (ic >= C.nx || jc >= C.ny || kc >= C.nz) return;
+  const int d = F.dir;
+  const int ox = d == 0, oy = d == 1, oz = d == 2;
+  const int i = ox ? 2 * ic : ic, j = oy ? 2 * jc : jc, k = oz ? 2 * kc : kc;
+  const T p2_1 = vget(F.nx, F.ny, F.nz, (const T *)F.p2, i - ox, j - oy, k - oz);
+  const T p1_2 = vget(F.nx, F.ny, F.nz, (const T *)F.p1, i + ox, j + oy, k + oz);
+  const T p2_2 = vget(F.nx, F.ny, F.nz, (const T *)F.p2, i + ox, j + oy, k + oz);
+  coarse_op_core(F, C, ic, jc, kc, p2_1, p1_2, p2_2);
+}
+
+// weights and coarse operator of one level in one pass: the thread of
+// coarse point c computes the weights of fine points 2c-1 and 2c+1 itself
+// (the same arithmetic as prolong_weights_cell) and stores those of 2c+1,
+// so every fine point's weights are written once and the fine operator is
+// read in a single sweep
+template <typename T>
+__device__ __forceinline__ void setup_level_cell(const MGLevel<T> &F, const MGLevel<T> &C,
+                                                 int ic, int jc, int kc) {
+  if (ic >= C.nx || jc >= C.ny || kc >= C.nz) return;
+  const int d = F.dir;
+  const int ox = d == 0, oy = d == 1, oz = d == 2;
+  const int i = ox ? 2 * ic : ic, j = oy ? 2 * jc : jc, k = oz ? 2 * kc : kc;
+  LV<T> L = lv(F);
+  T p2_1 = T(0), p1_2 = T(0), p2_2 = T(0), w1;
+  if (inside(F.nx, F.ny, F.nz, i - ox, j - oy, k - oz))
+    weights_at(L, d, i - ox, j - oy, k - oz, w1, p2_1);
+  if (inside(F.nx, F.ny, F.nz, i + ox, j + oy, k + oz)) {
+    weights_at(L, d, i + ox, j + oy, k + oz, p1_2, p2_2);
+    const long long f = (i + ox) + (long long)F.nx * ((j + oy) + (long long)F.ny * (k + oz));
+    F.p1[f] = p1_2;
+    F.p2[f] = p2_2;
+  }
+  coarse_op_core(F, C, ic, jc, kc, p2_1, p1_2, p2_2);
+}
+
+template <typename T>
+__global__ void k_setup_level(MGLevel<T> F, MGLevel<T> C) {
+  pdl_enter();
+  int i, j, k;
+  thread_ijk(i, j, k);
+  setup_level_cell(F, C, i, j, k);
 }
 
 template <typename T>
@@ -371,11 +424,10 @@ __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b
   }
 }
 
+// the tail cycle over levels first .. nl-1 of the table Ls (global or shared)
 template <typename T>
-__global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restrict__ Ls,
-                                                      int first, int nl, int smoother, T w,
-                                                      T *tmp) {
-  pdl_enter();
+__device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int nl,
+                                           int smoother, T w, T *tmp) {
   // down: levels first .. nl-2
   for (int l = first; l <= nl - 2; l++) {
     const MGLevel<T> L = Ls[l];
@@ -413,6 +465,115 @@ __global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restric
   }
 }
 
+// Tail levels in global memory (used when they do not fit in shared memory).
+template <typename T>
+__global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restrict__ Ls,
+                                                      int first, int nl, int smoother, T w,
+                                                      T *tmp) {
+  pdl_enter();
+  tail_cycle(Ls, first, nl, smoother, w, tmp);
+}
+
+// Tail levels in shared memory: the block copies every tail level's C E N U,
+// prolongation weights and the first tail level's right-hand side into
+// shared memory (x and b of the coarser levels live there too, plus one
+// scratch vector for residuals and Jacobi updates), runs the cycle with each
+// phase waiting on shared-memory rather than L2 latency, and writes the first
+// tail level's x back.  The copy-in is one flattened loop over all arrays
+// with eight loads in flight per thread.
+template <typename T>
+struct TailSeg {
+  T *dst;
+  const T *src;
+  int start;  // first flattened element of this array
+};
+
+template <typename T>
+__host__ __device__ inline long long tail_pad(long long n) {
+  const long long q = 16 / (long long)sizeof(T);
+  return (n + q - 1) / q * q;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
+    const MGLevel<T> *__restrict__ Ls, int first, int nl, int smoother, T w) {
+  extern __shared__ __align__(16) unsigned char tail_raw[];
+  __shared__ MGLevel<T> S[TAIL_MAX_LEVELS];
+  __shared__ TailSeg<T> seg[7 * TAIL_MAX_LEVELS + 1];
+  __shared__ int nseg;
+  pdl_enter();
+  const int nt = nl - first;
+  if ((int)threadIdx.x < nt) S[threadIdx.x] = Ls[first + threadIdx.x];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    T *p = reinterpret_cast<T *>(tail_raw);
+    int ns = 0, e = 0, maxn = 0;
+    auto place = [&](T *&ptr, int n, bool load) {
+      if (load) {
+        seg[ns].dst = p;
+        seg[ns].src = ptr;
+        seg[ns].start = e;
+        ns++;
+        e += n;
+      }
+      ptr = p;
+      p += tail_pad<T>(n);
+    };
+    for (int q = 0; q < nt; q++) {
+      MGLevel<T> &L = S[q];
+      const int n = (int)L.n;
+      for (int s = 0; s < 4; s++) place(L.a[s], n, true);
+      place(L.x, n, false);
+      place(L.b, n, q == 0);
+      if (q < nt - 1) {
+        place(L.p1, n, true);
+        place(L.p2, n, true);
+      }
+      maxn = n > maxn ? n : maxn;
+    }
+    for (int q = 0; q < nt; q++) S[q].t = p;
+    seg[ns].start = e;  // sentinel
+    nseg = ns;
+  }
+  __syncthreads();
+  const int E = seg[nseg].start;
+  int sg = 0;
+  for (int e0 = threadIdx.x; e0 < E; e0 += 8 * blockDim.x) {
+    T v[8];
+    T *d[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * (int)blockDim.x;
+      d[u] = nullptr;
+      if (e < E) {
+        while (seg[sg + 1].start <= e) sg++;
+        const int o = e - seg[sg].start;
+        v[u] = seg[sg].src[o];
+        d[u] = seg[sg].dst + o;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++)
+      if (d[u]) *d[u] = v[u];
+  }
+  __syncthreads();
+  tail_cycle(S, 0, nt, smoother, w, S[0].t);
+  T *xo = Ls[first].x;
+  for (int c = threadIdx.x; c < (int)S[0].n; c += blockDim.x) xo[c] = S[0].x[c];
+}
+
+template <typename T>
+size_t tail_smem_bytes(const MGLevel<T> *L, int first, int nl) {
+  if (nl - first > TAIL_MAX_LEVELS) return ~(size_t)0;
+  long long elems = 0, maxn = 0;
+  for (int q = first; q < nl; q++) {
+    elems += tail_pad<T>(L[q].n) * (q < nl - 1 ? 8 : 6);
+    maxn = L[q].n > maxn ? L[q].n : maxn;
+  }
+  elems += tail_pad<T>(maxn);
+  return (size_t)elems * sizeof(T);
+}
+
 // multigrid setup of the tail levels in one block (mg_semi.c:534-740)
 template <typename T>
 __global__ void __launch_bounds__(512) k_setup_tail(const MGLevel<T> *__restrict__ Ls,
@@ -436,11 +597,43 @@ __global__ void __launch_bounds__(512) k_setup_tail(const MGLevel<T> *__restrict
   }
 }
 
+// four consecutive elements per vector access (16-byte aligned pointers)
+__device__ __forceinline__ void ld4(const double *p, double v[4]) {
+  const double2 a = reinterpret_cast<const double2 *>(p)[0];
+  const double2 b = reinterpret_cast<const double2 *>(p)[1];
+  v[0] = a.x; v[1] = a.y; v[2] = b.x; v[3] = b.y;
+}
+__device__ __forceinline__ void ld4(const float *p, float v[4]) {
+  const float4 a = reinterpret_cast<const float4 *>(p)[0];
+  v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+}
+__device__ __forceinline__ void st4(double *p, const double v[4]) {
+  reinterpret_cast<double2 *>(p)[0] = make_double2(v[0], v[1]);
+  reinterpret_cast<double2 *>(p)[1] = make_double2(v[2], v[3]);
+}
+__device__ __forceinline__ void st4(float *p, const float v[4]) {
+  reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// out = (TO) in; with vec set (both pointers 16-byte aligned) each thread
+// moves four elements per vector access, which keeps enough bytes in flight
+// for a streaming conversion to run at HBM bandwidth
 template <typename TI, typename TO>
-__global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, long long n) {
+__global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, long long n,
+                          int vec) {
   pdl_enter();
-  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (c < n) out[c] = (TO)in[c];
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n4 = vec ? n / 4 : 0;
+  if (t < n4) {
+    TI a[4];
+    TO b[4];
+    ld4(in + 4 * t, a);
+#pragma unroll
+    for (int u = 0; u < 4; u++) b[u] = (TO)a[u];
+    st4(out + 4 * t, b);
+  }
+  const long long c = 4 * n4 + t;
+  if (c < n && t < (vec ? 4 : n)) out[c] = (TO)in[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -473,6 +666,11 @@ void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t 
   launch_pdl(k_coarse_op<T>, dim3(g.grid), dim3(g.block), st, F, C);
 }
 template <typename T>
+void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st) {
+  Shape3 g = shape3(C.nx, C.ny, C.nz);
+  launch_pdl(k_setup_level<T>, dim3(g.grid), dim3(g.block), st, F, C);
+}
+template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
                      cudaStream_t st) {
   Shape3 g = shape3((L.nx + 1) / 2, L.ny, L.nz);
@@ -503,7 +701,13 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
 cudaError_t mg_prepare_kernels() {
   cudaError_t e = rbr_fused_prepare<float>();
   if (e != cudaSuccess) return e;
-  return rbr_fused_prepare<double>();
+  e = rbr_fused_prepare<double>();
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_vcycle_tail_smem<float>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_vcycle_tail_smem<double>,
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
 }
 
 template <typename T>
@@ -525,9 +729,13 @@ void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec
 }
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
-                        double weight, T *tmp, cudaStream_t st) {
-  launch_pdl(k_vcycle_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
-             (T)weight, tmp);
+                        double weight, T *tmp, size_t smem, cudaStream_t st) {
+  if (smem > 0)
+    launch_pdl_smem(k_vcycle_tail_smem<T>, dim3(1), dim3(TAIL_THREADS), smem, st, levels_dev,
+                    first, nl, smoother, (T)weight);
+  else
+    launch_pdl(k_vcycle_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
+               (T)weight, tmp);
 }
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st) {
@@ -536,12 +744,15 @@ void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStre
 
 template <typename TI, typename TO>
 void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
-  launch_pdl(k_convert<TI, TO>, dim3(nb(n, 256)), dim3(256), st, in, out, n);
+  const int vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
+  const long long threads = vec ? (n / 4 > 4 ? n / 4 : 4) : (n > 1 ? n : 1);
+  launch_pdl(k_convert<TI, TO>, dim3(nb(threads, 256)), dim3(256), st, in, out, n, vec);
 }
 
 #define INST(T)                                                                              \
   template void launch_mg_prolong_weights<T>(const MGLevel<T> &, cudaStream_t);               \
   template void launch_mg_coarse_op<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
+  template void launch_mg_setup_level<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
   template void launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *, \
                                     cudaStream_t);                                            \
   template void launch_mg_residual<T>(const MGLevel<T> &, const T *, const T *, T *,          \
@@ -550,8 +761,9 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
                                       cudaStream_t);                                          \
   template void launch_mg_prolong_add<T>(const MGLevel<T> &, const MGLevel<T> &, const T *,   \
                                          T *, cudaStream_t);                                  \
-  template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *,         \
+  template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *, size_t, \
                                       cudaStream_t);                                          \
+  template size_t tail_smem_bytes<T>(const MGLevel<T> *, int, int);                          \
   template void launch_setup_tail<T>(const MGLevel<T> *, int, int, cudaStream_t);
 INST(double)
 INST(float)

@@ -30,12 +30,12 @@ inline bool pdl_on() {
 }
 
 template <typename... KArgs, typename... Args>
-inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
-                       Args... args) {
+inline void launch_pdl_smem(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                            cudaStream_t st, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = grid;
   cfg.blockDim = block;
-  cfg.dynamicSmemBytes = 0;
+  cfg.dynamicSmemBytes = smem;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
   attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
@@ -43,6 +43,12 @@ inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream
   cfg.attrs = attr;
   cfg.numAttrs = 1;
   cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
+template <typename... KArgs, typename... Args>
+inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                       Args... args) {
+  launch_pdl_smem(kern, grid, block, 0, st, args...);
 }
 
 }  // namespace pfgpu

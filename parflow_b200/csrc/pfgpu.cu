@@ -66,6 +66,7 @@ struct MG {
   std::vector<MGLevel<T>> L;
   MGLevel<T> *Ldev = nullptr;  // device copy of the level table (tail kernels)
   int tail = 0;                // first level run by the single-block tail kernels
+  size_t tail_smem = 0;        // shared-memory bytes of the V-cycle tail (0: global)
   T *wtmp = nullptr;           // Jacobi temp (finest size)
   std::vector<char> fused;     // level smoothed by the fused red/black/red kernel
   std::vector<RbrMaps> maps;   // its tensor maps (input iterate = x)
@@ -76,8 +77,10 @@ struct MG {
 
 // Tuning (read once per handle from the environment; all variants compute
 // the same V-cycle):
-//   PFGPU_TAIL_CELLS  levels at or below this many cells run inside the
-//                     single-block tail kernels (default 1024)
+//   PFGPU_TAIL_CELLS  levels at or below this many cells may run inside the
+//                     single-block tail kernels, as far as the tail fits in
+//                     shared memory (default 1024)
+//   PFGPU_TAIL_SMEM   0 runs the V-cycle tail from global memory
 //   PFGPU_RBR_FUSED_CELLS  grid levels with at least this many cells (and a
 //                     row pitch TMA can address) use the TMA-pipelined fused
 //                     red/black/red smoother; the rest one kernel per colour
@@ -278,9 +281,8 @@ static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
   for (int l = 0; l < mg.tail && l + 1 < nl; l++) {
-    launch_mg_prolong_weights<T>(mg.L[l], st);
-    launch_mg_coarse_op<T>(mg.L[l], mg.L[l + 1], st);
-    k += 2;
+    launch_mg_setup_level<T>(mg.L[l], mg.L[l + 1], st);
+    k++;
   }
   if (mg.tail < nl - 1) {
     launch_setup_tail<T>(mg.Ldev, mg.tail, nl, st);
@@ -313,7 +315,7 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
     k += 2;
   }
   // levels first .. nl-1, coarse solve (RedBlackGSPoint, mg_semi.c:1276) included
-  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, st);
+  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st);
   k++;
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
@@ -422,26 +424,28 @@ static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, cons
     for (l = 0; l < lmax; l++) {
       stats->lin_iters++;
       krydim = l + 1;
-      CK(cudaMemcpyAsync(h->vtemp, h->V[l], N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
-      if (pc_apply_dense(h, h->vtemp, h->vtemp)) return PFGPU_ERR_CUDA;
+      // vtemp = M^{-1} V[l] (the preconditioner reads V[l], writes vtemp)
+      if (pc_apply_dense(h, h->V[l], h->vtemp)) return PFGPU_ERR_CUDA;
       stats->pc_solves++;
       if (!h->jac_valid) {
         assemble(h, u, dt, true, false, true);
         h->jac_valid = 1;
       }
       matvec(h, h->vtemp, h->V[l + 1]);
-      // ModifiedGS (iterativ.c:30-86)
+      // ModifiedGS (iterativ.c:30-86): <vk,vk> and h(0) in one pass, then each
+      // projection vk -= h(i) v_i fused with the next dot (h(i+1), or the
+      // new <vk,vk> after the last); same per-element arithmetic
       const int k = l + 1;
-      launch_dot(h->V[k], h->V[k], N, sc + SCI_VKNORM2, h->rb, h->st);
+      launch_mgs_first(h->V[k], h->V[0], N, sc + SCI_VKNORM2, Hp(0, k - 1), h->rb, h->st);
       h->launches++;
       for (int i = 0; i < k; i++) {
-        launch_dot(h->V[i], h->V[k], N, Hp(i, k - 1), h->rb, h->st);
-        launch_axpy_dev(h->V[k], h->V[i], Hp(i, k - 1), -1.0, N, h->st);
-        h->launches += 2;
+        const bool more = i + 1 < k;
+        launch_axpy_dot(h->V[k], h->V[i], Hp(i, k - 1), -1.0, more ? h->V[i + 1] : nullptr, N,
+                        more ? Hp(i + 1, k - 1) : sc + SCI_NEWNORM2, h->rb, h->st);
+        h->launches++;
       }
-      launch_dot(h->V[k], h->V[k], N, sc + SCI_NEWNORM2, h->rb, h->st);
       launch_gmres_scalar(GM_AFTER_GS, S, l, lmax, h->st);
-      h->launches += 2;
+      h->launches++;
       for (int i = 0; i < k; i++) {
         launch_dot_gated(h->V[i], h->V[k], N, sc + SCI_NP, sc + SCI_FLAG, h->rb, h->st);
         launch_reorth_decide(S, i, l, lmax, h->st);
@@ -530,13 +534,11 @@ static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   h->vg_for = nullptr;
 
   // mxnewtstep = 1000 ||u|| (KINSolInit, kinsol.c:540-545)
-  launch_dot(u, u, N, dsc + D_U2, h->rb, h->st);
-  // KINInitialStop
+  // KINInitialStop; <u,u>, max|f| and <f,f> in one pass
   feval(h, u, dt, h->fval);
   stats->fevals++;
-  launch_maxabs(h->fval, N, dsc + D_FMAX, h->rb, h->st);
-  launch_dot(h->fval, h->fval, N, dsc + D_F2, h->rb, h->st);
-  h->launches += 3;
+  launch_init_norms(u, h->fval, N, dsc + D_U2, dsc + D_FMAX, dsc + D_F2, h->rb, h->st);
+  h->launches++;
   if (read_scalars(h, 0, D_COUNT)) return PFGPU_ERR_CUDA;
   double mxnewtstep = 1000.0 * sqrt(hsc[D_U2]);
   if (mxnewtstep < 1.0) mxnewtstep = 1.0;
@@ -576,11 +578,9 @@ static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
     }
     // sJpnorm, sfdotJp (kinspgmr.c:422-431) and line-search inputs
     matvec(h, h->pp, h->bb);
-    launch_dot(h->bb, h->bb, N, dsc + D_JP2, h->rb, h->st);
-    launch_dot(h->fval, h->bb, N, dsc + D_FJP, h->rb, h->st);
-    launch_dot(h->pp, h->pp, N, dsc + D_P2, h->rb, h->st);
-    launch_steplen(h->pp, u, N, dsc + D_PLEN, h->rb, h->st);
-    h->launches += 4;
+    launch_linesearch_inputs(h->bb, h->fval, h->pp, u, N, dsc + D_JP2, dsc + D_FJP, dsc + D_P2,
+                             dsc + D_PLEN, h->rb, h->st);
+    h->launches++;
     if (read_scalars(h, 0, D_COUNT)) return PFGPU_ERR_CUDA;
     double sJpnorm = sqrt(hsc[D_JP2]);
     double sfdotJp = hsc[D_FJP];
@@ -615,10 +615,9 @@ static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
       }
       feval(h, unew, dt, h->fval);
       stats->fevals++;
-      launch_dot(h->fval, h->fval, N, dsc + D_F2, h->rb, h->st);
-      launch_maxabs(h->fval, N, dsc + D_FMAX, h->rb, h->st);
-      launch_steplen_diff(unew, u, N, dsc + D_STEP, h->rb, h->st);
-      h->launches += 4;
+      launch_step_norms(h->fval, unew, u, N, dsc + D_F2, dsc + D_FMAX, dsc + D_STEP, h->rb,
+                        h->st);
+      h->launches += 2;
       if (read_scalars(h, 0, 3)) return PFGPU_ERR_CUDA;
       fnormp = sqrt(hsc[D_F2]);
       f1normp = 0.5 * fnormp * fnormp;
@@ -783,14 +782,19 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
     if (L.dir == 2) nz = (nz + 1) / 2;
   }
   if (dalloc(&mg.wtmp, mg.L[0].n)) return PFGPU_ERR_NOMEM;
-  // first level small enough for the single-block tail kernels
+  // first level of the single-block tail: the largest whose tail fits in
+  // shared memory (else the coarsest level alone, run from global memory)
   mg.tail = nl - 1;
   const long long tail_cells = env_ll("PFGPU_TAIL_CELLS", 1024);
   for (int l = 0; l < nl; l++)
-    if (mg.L[l].n <= tail_cells) {
+    if (mg.L[l].n <= tail_cells && tail_smem_bytes<T>(mg.L.data(), l, nl) <= TAIL_SMEM_MAX) {
       mg.tail = l;
       break;
     }
+  {
+    const size_t b = tail_smem_bytes<T>(mg.L.data(), mg.tail, nl);
+    mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
+  }
   // grid levels large enough for the fused smoother get an output buffer
   // distinct from the input iterate
   const long long fused_cells = env_ll("PFGPU_RBR_FUSED_CELLS", LLONG_MAX);
@@ -864,7 +868,7 @@ static int create_impl(pfgpu_handle *h) {
   for (auto &v : h->V)
     if (dalloc(&v, N)) return PFGPU_ERR_NOMEM;
   if (dalloc(&h->gs, gs_size(d.krylov_dim)) || dalloc(&h->dsc, 64) ||
-      dalloc(&h->stage, h->NP) || dalloc(&h->rb.partial, reduce_blocks()))
+      dalloc(&h->stage, h->NP) || dalloc(&h->rb.partial, reduce_partials()))
     return PFGPU_ERR_NOMEM;
   CK(cudaMemset(h->gs, 0, gs_size(d.krylov_dim) * sizeof(double)));
   CK(cudaMalloc((void **)&h->rb.ticket, sizeof(unsigned int)));

@@ -109,6 +109,9 @@ template <typename T>
 void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st);
 template <typename T>
 void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
+// prolongation weights of F and the coarse operator C in one launch
+template <typename T>
+void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
 template <typename T>
 void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st);
@@ -122,10 +125,17 @@ template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
                            cudaStream_t st);
 // levels `first` .. nl-1 of a V-cycle / of the setup in one single-block
-// kernel; levels_dev is a device copy of the level table
+// kernel; levels_dev is a device copy of the level table.  With smem > 0
+// (tail_smem_bytes of those levels, at most TAIL_SMEM_MAX) the V-cycle tail
+// runs out of shared memory, otherwise in global memory with tmp as scratch.
+constexpr int TAIL_MAX_LEVELS = 32;
+constexpr int TAIL_THREADS = 1024;
+constexpr size_t TAIL_SMEM_MAX = 200 * 1024;
+template <typename T>
+size_t tail_smem_bytes(const MGLevel<T> *levels_host, int first, int nl);
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
-                        double weight, T *tmp, cudaStream_t st);
+                        double weight, T *tmp, size_t smem, cudaStream_t st);
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
 template <typename TI, typename TO>
@@ -138,6 +148,7 @@ struct ReduceBuf {
   int blocks;
 };
 int reduce_blocks();
+int reduce_partials();  // doubles the partial buffer must hold (multi-value reductions)
 // dst = sum(a .* b); deterministic (fixed grid, fixed order)
 void launch_dot(const double *a, const double *b, long long n, double *dst, ReduceBuf rb,
                 cudaStream_t st);
@@ -152,6 +163,20 @@ void launch_steplen(const double *s, const double *u, long long n, double *dst, 
 // dst = max |a - b| / (1 + |a|)
 void launch_steplen_diff(const double *a, const double *b, long long n, double *dst,
                          ReduceBuf rb, cudaStream_t st);
+// fused reductions (one pass each)
+void launch_mgs_first(const double *vk, const double *v0, long long n, double *d_vk2,
+                      double *d_h0, ReduceBuf rb, cudaStream_t st);
+// y += sign * (*s) x, then dst = <z, y> (z null: <y, y>)
+void launch_axpy_dot(double *y, const double *x, const double *s, double sign, const double *z,
+                     long long n, double *dst, ReduceBuf rb, cudaStream_t st);
+void launch_linesearch_inputs(const double *jp, const double *f, const double *p,
+                              const double *u, long long n, double *d_jp2, double *d_fjp,
+                              double *d_p2, double *d_plen, ReduceBuf rb, cudaStream_t st);
+void launch_step_norms(const double *f, const double *unew, const double *u, long long n,
+                       double *d_f2, double *d_fmax, double *d_step, ReduceBuf rb,
+                       cudaStream_t st);
+void launch_init_norms(const double *u, const double *f, long long n, double *d_u2,
+                       double *d_fmax, double *d_f2, ReduceBuf rb, cudaStream_t st);
 // y = y + (sign * (*s)) * x
 void launch_axpy_dev(double *y, const double *x, const double *s, double sign, long long n,
                      cudaStream_t st);
