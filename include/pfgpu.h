@@ -44,6 +44,15 @@ extern "C" {
  * the residual, Newton update, Arnoldi process and all norms stay FP64 */
 #define PFGPU_PREC_FP64 0
 #define PFGPU_PREC_MIXED 1
+/* as MIXED, with each multigrid level's operator stored symmetrically
+ * diagonal-scaled in FP16: with S = sqrt(diag A) the V-cycle runs on S x,
+ * S^-1 b and S^-1 A S^-1 (unit diagonal, off-diagonals A_ij / (S_i S_j) in
+ * FP16), the scaling folded into the transfer weights.  In exact arithmetic
+ * this is the same MGSemi V-cycle; it moves 6 instead of 16 operator bytes
+ * per cell (8 on hierarchies where some diagonal is not positive, e.g. with
+ * kinematic overland terms: S = sqrt(|diag A|) and the +-1 diagonal is then
+ * read too).  No counterpart in the reference. */
+#define PFGPU_PREC_MIXED_H16 2
 
 /* boundary-condition types, one per box face
  * (pfsimulator/parflow_lib/bc_pressure.h:97 BC_TYPE_TABLE) */

@@ -5,6 +5,9 @@
 // pfsimulator/parflow_lib/matrix.c:258-310, 477-490).  Coarse grids take the
 // even fine indices in the coarsening direction; fine points are the odd ones
 // (pfsimulator/parflow_lib/mg_semi.c:960-1058).
+#include <cstdint>
+#include <type_traits>
+
 #include "pdl.cuh"
 #include "pfgpu_kernels.h"
 
@@ -15,6 +18,8 @@ struct LV {
   int nx, ny, nz;
   long long n;
   const T *a0, *ae, *an, *au;
+  const __half *he, *hn, *hu, *hd;  // scaled FP16 operator (H mode)
+  const int *hflag;                  // nonzero: read the scaled diagonal hd
 };
 
 template <typename T>
@@ -22,7 +27,26 @@ __device__ __forceinline__ LV<T> lv(const MGLevel<T> &L) {
   LV<T> v;
   v.nx = L.nx; v.ny = L.ny; v.nz = L.nz; v.n = L.n;
   v.a0 = L.a[0]; v.ae = L.a[1]; v.an = L.a[2]; v.au = L.a[3];
+  v.he = L.h[0]; v.hn = L.h[1]; v.hu = L.h[2]; v.hd = L.h[3];
+  v.hflag = L.hflag;
   return v;
+}
+
+// Template flag H selects the scaled FP16 operator (unit diagonal, E^ N^ U^
+// in h, transfer weights q1/q2); H = false is the plain operator C E N U.
+template <typename T, bool H>
+__device__ __forceinline__ T ld_off(const T *a, const __half *h, long long c) {
+  if constexpr (H)
+    return (T)__half2float(h[c]);
+  else
+    return a[c];
+}
+template <typename T, bool H>
+__device__ __forceinline__ T diag(const LV<T> &L, long long c) {
+  if constexpr (H)
+    return *L.hflag ? (T)__half2float(L.hd[c]) : T(1);
+  else
+    return L.a0[c];
 }
 
 __device__ __forceinline__ bool inside(int nx, int ny, int nz, int i, int j, int k) {
@@ -30,18 +54,18 @@ __device__ __forceinline__ bool inside(int nx, int ny, int nz, int i, int j, int
 }
 
 // coefficient s (0..6 = C W E S N L U) of cell (i,j,k), zero outside
-template <typename T>
+template <typename T, bool H = false>
 __device__ __forceinline__ T coef(const LV<T> &L, int s, int i, int j, int k) {
   if (!inside(L.nx, L.ny, L.nz, i, j, k)) return T(0);
   long long c = i + (long long)L.nx * (j + (long long)L.ny * k);
   switch (s) {
-    case 0: return L.a0[c];
-    case 1: return i > 0 ? L.ae[c - 1] : T(0);
-    case 2: return L.ae[c];
-    case 3: return j > 0 ? L.an[c - L.nx] : T(0);
-    case 4: return L.an[c];
-    case 5: return k > 0 ? L.au[c - (long long)L.nx * L.ny] : T(0);
-    default: return L.au[c];
+    case 0: return diag<T, H>(L, c);
+    case 1: return i > 0 ? ld_off<T, H>(L.ae, L.he, c - 1) : T(0);
+    case 2: return ld_off<T, H>(L.ae, L.he, c);
+    case 3: return j > 0 ? ld_off<T, H>(L.an, L.hn, c - L.nx) : T(0);
+    case 4: return ld_off<T, H>(L.an, L.hn, c);
+    case 5: return k > 0 ? ld_off<T, H>(L.au, L.hu, c - (long long)L.nx * L.ny) : T(0);
+    default: return ld_off<T, H>(L.au, L.hu, c);
   }
 }
 
@@ -66,6 +90,15 @@ __device__ __forceinline__ void thread_ijk(int &i, int &j, int &k) {
   i = blockIdx.x * blockDim.x + threadIdx.x;
   j = blockIdx.y * blockDim.y + threadIdx.y;
   k = blockIdx.z;
+}
+// the same with the block order along y and z reversed when flip is set:
+// consecutive sweeps over a level that alternate direction begin on the
+// planes the previous launch touched last, which are still in L2
+__device__ __forceinline__ void thread_ijk_flip(int &i, int &j, int &k, int flip) {
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  i = blockIdx.x * blockDim.x + threadIdx.x;
+  j = by * blockDim.y + threadIdx.y;
+  k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
 }
 // (i, j, k) of linear index t inside a level (32-bit; single-block loops)
 __device__ __forceinline__ void split_ijk(int t, int nx, int ny, int &i, int &j, int &k) {
@@ -195,12 +228,86 @@ __device__ __forceinline__ void setup_level_cell(const MGLevel<T> &F, const MGLe
   coarse_op_core(F, C, ic, jc, kc, p2_1, p1_2, p2_2);
 }
 
+// The seven entries C W E S N L U of fine cell (i,j,k), zero outside the
+// level: the values coef() returns, gathered with predicated loads so that
+// a thread issues all its loads at once.
 template <typename T>
-__global__ void k_setup_level(MGLevel<T> F, MGLevel<T> C) {
+__device__ __forceinline__ void gather7(const LV<T> &L, int i, int j, int k, T st[7]) {
+  const bool in = i >= 0 && j >= 0 && k >= 0 && i < L.nx && j < L.ny && k < L.nz;
+  const int sy = L.nx, sz = L.nx * L.ny;
+  const int c = in ? i + sy * j + sz * k : 0;
+  st[0] = in ? L.a0[c] : T(0);
+  st[1] = in && i > 0 ? L.ae[c - 1] : T(0);
+  st[2] = in ? L.ae[c] : T(0);
+  st[3] = in && j > 0 ? L.an[c - sy] : T(0);
+  st[4] = in ? L.an[c] : T(0);
+  st[5] = in && k > 0 ? L.au[c - sz] : T(0);
+  st[6] = in ? L.au[c] : T(0);
+}
+
+// setup_level_cell with the coarsening direction D fixed at compile time and
+// every fine operand gathered up front (fine points 2c-1, 2c, 2c+1 along D;
+// the lower entry of 2c+2 is the upper entry of 2c+1 in symmetric storage).
+// Same operations in the same order as weights_at + coarse_op_core, so the
+// result is bitwise that of setup_level_cell.
+template <typename T, int D>
+__global__ void __launch_bounds__(256) k_setup_level(MGLevel<T> F, MGLevel<T> C) {
   pdl_enter();
-  int i, j, k;
-  thread_ijk(i, j, k);
-  setup_level_cell(F, C, i, j, k);
+  int ic, jc, kc;
+  thread_ijk(ic, jc, kc);
+  if (ic >= C.nx || jc >= C.ny || kc >= C.nz) return;
+  constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
+  constexpr int s0 = D == 0 ? 0 : D == 1 ? 0 : 0;
+  constexpr int s1 = D == 0 ? 1 : D == 1 ? 3 : 5;  // along-D lower
+  constexpr int s2 = D == 0 ? 2 : D == 1 ? 4 : 6;  // along-D upper
+  constexpr int s3 = D == 0 ? 3 : D == 1 ? 1 : 3;
+  constexpr int s4 = D == 0 ? 4 : D == 1 ? 2 : 4;
+  constexpr int s5 = D == 0 ? 5 : D == 1 ? 5 : 1;
+  constexpr int s6 = D == 0 ? 6 : D == 1 ? 6 : 2;
+  const int i = ox ? 2 * ic : ic, j = oy ? 2 * jc : jc, k = oz ? 2 * kc : kc;
+  LV<T> L = lv(F);
+  T sm[7], sc[7], sp[7];  // fine cells f-1, f, f+1 along D
+  gather7(L, i - ox, j - oy, k - oz, sm);
+  gather7(L, i, j, k, sc);
+  gather7(L, i + ox, j + oy, k + oz, sp);
+  // prolongation weights of f-1 (its p2) and f+1 (p1, p2): weights_at
+  T p2_1 = T(0), p1_2 = T(0), p2_2 = T(0);
+  {
+    const T ap0 = sm[s0] + sm[s3] + sm[s4] + sm[s5] + sm[s6];
+    if (ap0 != T(0)) p2_1 = -sm[s2] / ap0;
+  }
+  {
+    const T ap0 = sp[s0] + sp[s3] + sp[s4] + sp[s5] + sp[s6];
+    if (ap0 != T(0)) {
+      p1_2 = -sp[s1] / ap0;
+      p2_2 = -sp[s2] / ap0;
+    }
+  }
+  const int ip = i + ox, jp = j + oy, kp = k + oz;
+  if (ip < F.nx && jp < F.ny && kp < F.nz) {
+    const long long f = ip + (long long)F.nx * (jp + (long long)F.ny * kp);
+    F.p1[f] = p1_2;
+    F.p2[f] = p2_2;
+  }
+  // coarse operator: coarse_op_core
+  const long long cc = ic + (long long)C.nx * (jc + (long long)C.ny * kc);
+  const T ac3 = sc[s3] + T(0.5) * sm[s3] + T(0.5) * sp[s3];
+  const T ac4 = sc[s4] + T(0.5) * sm[s4] + T(0.5) * sp[s4];
+  const T ac5 = sc[s5] + T(0.5) * sm[s5] + T(0.5) * sp[s5];
+  const T ac6 = sc[s6] + T(0.5) * sm[s6] + T(0.5) * sp[s6];
+  const T ac2 = sc[s2] * p2_2;
+  const T ac0 = sc[s0] + sc[s3] + sc[s4] + sc[s5] + sc[s6] + sc[s1] * p2_1 + sc[s2] * p1_2;
+  const int last = D == 0 ? (ic + 1 >= C.nx) : D == 1 ? (jc + 1 >= C.ny) : (kc + 1 >= C.nz);
+  // not last: fine 2c+2 exists, and its lower entry is the upper entry of 2c+1
+  const T along_up = last ? ac2 : sp[s2] * p1_2;
+  T E, N, U;
+  if (D == 0) { E = along_up; N = ac4; U = ac6; }
+  else if (D == 1) { E = ac4; N = along_up; U = ac6; }
+  else { E = ac6; N = ac4; U = along_up; }
+  C.a[1][cc] = E;
+  C.a[2][cc] = N;
+  C.a[3][cc] = U;
+  C.a[0][cc] = ac0 - (ac3 + ac4 + ac5 + ac6);
 }
 
 template <typename T>
@@ -213,7 +320,7 @@ __global__ void k_coarse_op(MGLevel<T> F, MGLevel<T> C) {
 
 // one colour of red/black Gauss-Seidel; colour 0 = red = (i+j+k) odd
 // (pfsimulator/parflow_lib/comm_pkg.c:132-139, rb_GS_point.c:342-370)
-template <typename T>
+template <typename T, bool H = false>
 __device__ __forceinline__ void rb_cell(const MGLevel<T> &Lv, T *__restrict__ x,
                                         const T *__restrict__ b, int colour, int init, int q,
                                         int j, int k) {
@@ -226,29 +333,79 @@ __device__ __forceinline__ void rb_cell(const MGLevel<T> &Lv, T *__restrict__ x,
   const long long c = i + (long long)nx * (j + (long long)ny * k);
   LV<T> L = lv(Lv);
   if (init) {
-    x[c] = b[c] / L.a0[c];
+    x[c] = b[c] / diag<T, H>(L, c);
     return;
   }
   const long long sy = nx, sz = (long long)nx * ny;
-  x[c] = rb_update<T>(L.a0[c], b[c], coef(L, 1, i, j, k), i > 0 ? x[c - 1] : T(0),
-                      coef(L, 2, i, j, k), i + 1 < nx ? x[c + 1] : T(0),
-                      coef(L, 3, i, j, k), j > 0 ? x[c - sy] : T(0),
-                      coef(L, 4, i, j, k), j + 1 < ny ? x[c + sy] : T(0),
-                      coef(L, 5, i, j, k), k > 0 ? x[c - sz] : T(0),
-                      coef(L, 6, i, j, k), k + 1 < Lv.nz ? x[c + sz] : T(0));
+  x[c] = rb_update<T>(diag<T, H>(L, c), b[c], coef<T, H>(L, 1, i, j, k), i > 0 ? x[c - 1] : T(0),
+                      coef<T, H>(L, 2, i, j, k), i + 1 < nx ? x[c + 1] : T(0),
+                      coef<T, H>(L, 3, i, j, k), j > 0 ? x[c - sy] : T(0),
+                      coef<T, H>(L, 4, i, j, k), j + 1 < ny ? x[c + sy] : T(0),
+                      coef<T, H>(L, 5, i, j, k), k > 0 ? x[c - sz] : T(0),
+                      coef<T, H>(L, 6, i, j, k), k + 1 < Lv.nz ? x[c + sz] : T(0));
 }
 
-template <typename T>
-__global__ void k_rb_sweep(MGLevel<T> Lv, T *__restrict__ x, const T *__restrict__ b,
-                           int colour, int init) {
+// Grid form of rb_cell with lean index arithmetic: 32-bit cell indices (a
+// level that fits in device memory has fewer than 2^31 cells), the grid's z
+// extent equal to nz, predicated neighbour loads, no neighbour loads on the
+// zero-guess sweep and, for the scaled operator with unit diagonal, no
+// division.  Bitwise the same result as rb_cell.
+template <typename T, bool H>
+__global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ x,
+                                                  const T *__restrict__ b, int colour, int init,
+                                                  int flip) {
   pdl_enter();
-  int q, j, k;
-  thread_ijk(q, j, k);
-  rb_cell(Lv, x, b, colour, init, q, j, k);
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (j >= ny) return;
+  const int i = 2 * q + ((colour ^ 1 ^ j ^ k) & 1);  // red: (i+j+k) odd
+  if (i >= nx) return;
+  const int sy = nx, sz = nx * ny;
+  const int c = i + sy * j + sz * k;
+  bool unit = false;  // scaled operator with unit diagonal everywhere
+  T d = T(1);
+  if constexpr (H) {
+    unit = *L.hflag == 0;
+    if (!unit) d = (T)__half2float(L.h[3][c]);
+  } else {
+    d = L.a[0][c];
+  }
+  if (init) {
+    x[c] = unit ? b[c] : b[c] / d;
+    return;
+  }
+  const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
+             hu = k + 1 < nz;
+  T cw, ce, cs, cn, cl, cu;
+  if constexpr (H) {
+    cw = hw ? (T)__half2float(L.h[0][c - 1]) : T(0);
+    ce = (T)__half2float(L.h[0][c]);
+    cs = hs ? (T)__half2float(L.h[1][c - sy]) : T(0);
+    cn = (T)__half2float(L.h[1][c]);
+    cl = hl ? (T)__half2float(L.h[2][c - sz]) : T(0);
+    cu = (T)__half2float(L.h[2][c]);
+  } else {
+    cw = hw ? L.a[1][c - 1] : T(0);
+    ce = L.a[1][c];
+    cs = hs ? L.a[2][c - sy] : T(0);
+    cn = L.a[2][c];
+    cl = hl ? L.a[3][c - sz] : T(0);
+    cu = L.a[3][c];
+  }
+  T acc = cw * (hw ? x[c - 1] : T(0));
+  acc = fma(ce, he ? x[c + 1] : T(0), acc);
+  acc = fma(cs, hs ? x[c - sy] : T(0), acc);
+  acc = fma(cn, hn ? x[c + sy] : T(0), acc);
+  acc = fma(cl, hl ? x[c - sz] : T(0), acc);
+  acc = fma(cu, hu ? x[c + sz] : T(0), acc);
+  x[c] = unit ? b[c] - acc : (b[c] - acc) / d;
 }
 
 // weighted Jacobi (pfsimulator/parflow_lib/w_jacobi.c:120-290)
-template <typename T>
+template <typename T, bool H = false>
 __device__ __forceinline__ void wjacobi_cell(const MGLevel<T> &Lv, const T *__restrict__ x,
                                              const T *__restrict__ b, T *__restrict__ t,
                                              int zero, int i, int j, int k) {
@@ -256,27 +413,27 @@ __device__ __forceinline__ void wjacobi_cell(const MGLevel<T> &Lv, const T *__re
   const long long c = i + (long long)Lv.nx * (j + (long long)Lv.ny * k);
   LV<T> L = lv(Lv);
   if (zero) {
-    t[c] = b[c] / L.a0[c];
+    t[c] = b[c] / diag<T, H>(L, c);
     return;
   }
   const int nx = Lv.nx, ny = Lv.ny, nz = Lv.nz;
   T v = b[c];
-  v -= coef(L, 1, i, j, k) * vget(nx, ny, nz, x, i - 1, j, k);
-  v -= coef(L, 2, i, j, k) * vget(nx, ny, nz, x, i + 1, j, k);
-  v -= coef(L, 3, i, j, k) * vget(nx, ny, nz, x, i, j - 1, k);
-  v -= coef(L, 4, i, j, k) * vget(nx, ny, nz, x, i, j + 1, k);
-  v -= coef(L, 5, i, j, k) * vget(nx, ny, nz, x, i, j, k - 1);
-  v -= coef(L, 6, i, j, k) * vget(nx, ny, nz, x, i, j, k + 1);
-  t[c] = v / L.a0[c];
+  v -= coef<T, H>(L, 1, i, j, k) * vget(nx, ny, nz, x, i - 1, j, k);
+  v -= coef<T, H>(L, 2, i, j, k) * vget(nx, ny, nz, x, i + 1, j, k);
+  v -= coef<T, H>(L, 3, i, j, k) * vget(nx, ny, nz, x, i, j - 1, k);
+  v -= coef<T, H>(L, 4, i, j, k) * vget(nx, ny, nz, x, i, j + 1, k);
+  v -= coef<T, H>(L, 5, i, j, k) * vget(nx, ny, nz, x, i, j, k - 1);
+  v -= coef<T, H>(L, 6, i, j, k) * vget(nx, ny, nz, x, i, j, k + 1);
+  t[c] = v / diag<T, H>(L, c);
 }
 
-template <typename T>
+template <typename T, bool H>
 __global__ void k_wjacobi(MGLevel<T> Lv, const T *__restrict__ x, const T *__restrict__ b,
                           T *__restrict__ t, int zero) {
   pdl_enter();
   int i, j, k;
   thread_ijk(i, j, k);
-  wjacobi_cell(Lv, x, b, t, zero, i, j, k);
+  wjacobi_cell<T, H>(Lv, x, b, t, zero, i, j, k);
 }
 
 template <typename T>
@@ -297,7 +454,7 @@ __global__ void k_wjacobi_update(T *__restrict__ x, const T *__restrict__ t, lon
 }
 
 // r = b - A x in ParFlow's Matvec order (alpha = -1, beta = 1)
-template <typename T>
+template <typename T, bool H = false>
 __device__ __forceinline__ void mg_residual_cell(const MGLevel<T> &Lv, const T *__restrict__ x,
                                                  const T *__restrict__ b, T *__restrict__ r,
                                                  int i, int j, int k) {
@@ -306,27 +463,65 @@ __device__ __forceinline__ void mg_residual_cell(const MGLevel<T> &Lv, const T *
   const int nx = Lv.nx, ny = Lv.ny, nz = Lv.nz;
   LV<T> L = lv(Lv);
   T y = -b[c];
-  y += L.a0[c] * x[c];
-  y += coef(L, 1, i, j, k) * vget(nx, ny, nz, x, i - 1, j, k);
-  y += coef(L, 2, i, j, k) * vget(nx, ny, nz, x, i + 1, j, k);
-  y += coef(L, 3, i, j, k) * vget(nx, ny, nz, x, i, j - 1, k);
-  y += coef(L, 4, i, j, k) * vget(nx, ny, nz, x, i, j + 1, k);
-  y += coef(L, 5, i, j, k) * vget(nx, ny, nz, x, i, j, k - 1);
-  y += coef(L, 6, i, j, k) * vget(nx, ny, nz, x, i, j, k + 1);
+  y += diag<T, H>(L, c) * x[c];
+  y += coef<T, H>(L, 1, i, j, k) * vget(nx, ny, nz, x, i - 1, j, k);
+  y += coef<T, H>(L, 2, i, j, k) * vget(nx, ny, nz, x, i + 1, j, k);
+  y += coef<T, H>(L, 3, i, j, k) * vget(nx, ny, nz, x, i, j - 1, k);
+  y += coef<T, H>(L, 4, i, j, k) * vget(nx, ny, nz, x, i, j + 1, k);
+  y += coef<T, H>(L, 5, i, j, k) * vget(nx, ny, nz, x, i, j, k - 1);
+  y += coef<T, H>(L, 6, i, j, k) * vget(nx, ny, nz, x, i, j, k + 1);
   r[c] = -y;
 }
 
-template <typename T>
-__global__ void k_mg_residual(MGLevel<T> Lv, const T *__restrict__ x, const T *__restrict__ b,
-                              T *__restrict__ r) {
+// grid form of mg_residual_cell (same operation order, lean indices)
+template <typename T, bool H>
+__global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__restrict__ x,
+                                                     const T *__restrict__ b,
+                                                     T *__restrict__ r, int flip) {
   pdl_enter();
-  int i, j, k;
-  thread_ijk(i, j, k);
-  mg_residual_cell(Lv, x, b, r, i, j, k);
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (i >= nx || j >= ny) return;
+  const int sy = nx, sz = nx * ny;
+  const int c = i + sy * j + sz * k;
+  const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
+             hu = k + 1 < nz;
+  T d, cw, ce, cs, cn, cl, cu;
+  if constexpr (H) {
+    d = *L.hflag ? (T)__half2float(L.h[3][c]) : T(1);
+    cw = hw ? (T)__half2float(L.h[0][c - 1]) : T(0);
+    ce = (T)__half2float(L.h[0][c]);
+    cs = hs ? (T)__half2float(L.h[1][c - sy]) : T(0);
+    cn = (T)__half2float(L.h[1][c]);
+    cl = hl ? (T)__half2float(L.h[2][c - sz]) : T(0);
+    cu = (T)__half2float(L.h[2][c]);
+  } else {
+    d = L.a[0][c];
+    cw = hw ? L.a[1][c - 1] : T(0);
+    ce = L.a[1][c];
+    cs = hs ? L.a[2][c - sy] : T(0);
+    cn = L.a[2][c];
+    cl = hl ? L.a[3][c - sz] : T(0);
+    cu = L.a[3][c];
+  }
+  T y = -b[c];
+  y += d * x[c];
+  y += cw * (hw ? x[c - 1] : T(0));
+  y += ce * (he ? x[c + 1] : T(0));
+  y += cs * (hs ? x[c - sy] : T(0));
+  y += cn * (hn ? x[c + sy] : T(0));
+  y += cl * (hl ? x[c - sz] : T(0));
+  y += cu * (hu ? x[c + sz] : T(0));
+  r[c] = -y;
 }
 
 // r_c = r_f(c) + (p2(f-1) r_f(f-1) + p1(f+1) r_f(f+1)) (mg_semi_restrict.c:161-169)
-template <typename T>
+// (H: r^_c = s_c r^_f(c) + (q2(f-1) r^_f(f-1) + q1(f+1) r^_f(f+1)), the
+// scaled form of the same operator, s_c = q1 at the coarse point)
+template <typename T, bool H = false>
 __device__ __forceinline__ void restrict_cell(const MGLevel<T> &F, const MGLevel<T> &C,
                                               const T *__restrict__ rf, T *__restrict__ rc,
                                               int ic, int jc, int kc) {
@@ -336,25 +531,30 @@ __device__ __forceinline__ void restrict_cell(const MGLevel<T> &F, const MGLevel
   const int ox = d == 0, oy = d == 1, oz = d == 2;
   const int i = ox ? 2 * ic : ic, j = oy ? 2 * jc : jc, k = oz ? 2 * kc : kc;
   const int nx = F.nx, ny = F.ny, nz = F.nz;
-  rc[cc] = rf[i + (long long)nx * (j + (long long)ny * k)] +
-           (vget(nx, ny, nz, (const T *)F.p2, i - ox, j - oy, k - oz) *
-                vget(nx, ny, nz, rf, i - ox, j - oy, k - oz) +
-            vget(nx, ny, nz, (const T *)F.p1, i + ox, j + oy, k + oz) *
-                vget(nx, ny, nz, rf, i + ox, j + oy, k + oz));
+  const T *w1 = H ? F.q1 : F.p1;
+  const T *w2 = H ? F.q2 : F.p2;
+  const long long f = i + (long long)nx * (j + (long long)ny * k);
+  T centre = rf[f];
+  if constexpr (H) centre = w1[f] * centre;
+  rc[cc] = centre + (vget(nx, ny, nz, w2, i - ox, j - oy, k - oz) *
+                         vget(nx, ny, nz, rf, i - ox, j - oy, k - oz) +
+                     vget(nx, ny, nz, w1, i + ox, j + oy, k + oz) *
+                         vget(nx, ny, nz, rf, i + ox, j + oy, k + oz));
 }
 
-template <typename T>
+template <typename T, bool H>
 __global__ void k_restrict(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ rf,
-                           T *__restrict__ rc) {
+                           T *__restrict__ rc, int flip) {
   pdl_enter();
   int i, j, k;
-  thread_ijk(i, j, k);
-  restrict_cell(F, C, rf, rc, i, j, k);
+  thread_ijk_flip(i, j, k, flip);
+  restrict_cell<T, H>(F, C, rf, rc, i, j, k);
 }
 
 // x_f += P e_c: injection at coarse points, p1 e(f-1) + p2 e(f+1) at fine
 // points (mg_semi_prolong.c:119-124, 191-197), followed by Axpy(1, e, x)
-template <typename T>
+// (H: s_c e at coarse points, q1 e(f-1) + q2 e(f+1) at fine points)
+template <typename T, bool H = false>
 __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLevel<T> &C,
                                                  const T *__restrict__ ec, T *__restrict__ xf,
                                                  int i, int j, int k) {
@@ -363,9 +563,12 @@ __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLe
   const int d = F.dir;
   const int ci = d == 0 ? i : d == 1 ? j : k;
   const int ox = d == 0, oy = d == 1, oz = d == 2;
+  const T *w1 = H ? F.q1 : F.p1;
+  const T *w2 = H ? F.q2 : F.p2;
   T e;
   if (!(ci & 1)) {
     e = ec[(ox ? i / 2 : i) + (long long)C.nx * ((oy ? j / 2 : j) + (long long)C.ny * (oz ? k / 2 : k))];
+    if constexpr (H) e = w1[c] * e;
   } else {
     int il = i - ox, jl = j - oy, kl = k - oz;  // coarse point below (even)
     int ih = i + ox, jh = j + oy, kh = k + oz;  // coarse point above (even), may be outside
@@ -373,18 +576,18 @@ __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLe
     T eh = inside(F.nx, F.ny, F.nz, ih, jh, kh)
                ? ec[(ox ? ih / 2 : ih) + (long long)C.nx * ((oy ? jh / 2 : jh) + (long long)C.ny * (oz ? kh / 2 : kh))]
                : T(0);
-    e = (F.p1[c] * el + F.p2[c] * eh);
+    e = (w1[c] * el + w2[c] * eh);
   }
   xf[c] = xf[c] + e;
 }
 
-template <typename T>
+template <typename T, bool H>
 __global__ void k_prolong_add(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ ec,
-                              T *__restrict__ xf) {
+                              T *__restrict__ xf, int flip) {
   pdl_enter();
   int i, j, k;
-  thread_ijk(i, j, k);
-  prolong_add_cell(F, C, ec, xf, i, j, k);
+  thread_ijk_flip(i, j, k, flip);
+  prolong_add_cell<T, H>(F, C, ec, xf, i, j, k);
 }
 
 // ---------------------------------------------------------------------------
@@ -395,14 +598,14 @@ __global__ void k_prolong_add(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ 
 // (smooth, residual, restrict, ..., coarse solve, prolong + correct, smooth),
 // separated by __syncthreads(); the arithmetic per cell is identical.
 // ---------------------------------------------------------------------------
-template <typename T>
+template <typename T, bool H>
 __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b, int zero,
                                            int smoother, T w, T *tmp) {
   if (smoother == 1) {
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
       split_ijk(t, L.nx, L.ny, i, j, k);
-      wjacobi_cell(L, x, b, tmp, zero, i, j, k);
+      wjacobi_cell<T, H>(L, x, b, tmp, zero, i, j, k);
     }
     __syncthreads();
     for (long long c = threadIdx.x; c < L.n; c += blockDim.x)
@@ -418,38 +621,38 @@ __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b
     for (int t = threadIdx.x; t < half; t += blockDim.x) {
       int q, j, k;
       split_ijk(t, hx, L.ny, q, j, k);
-      rb_cell(L, x, b, colour, init, q, j, k);
+      rb_cell<T, H>(L, x, b, colour, init, q, j, k);
     }
     __syncthreads();
   }
 }
 
 // the tail cycle over levels first .. nl-1 of the table Ls (global or shared)
-template <typename T>
+template <typename T, bool H>
 __device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int nl,
                                            int smoother, T w, T *tmp) {
   // down: levels first .. nl-2
   for (int l = first; l <= nl - 2; l++) {
     const MGLevel<T> L = Ls[l];
     const MGLevel<T> C = Ls[l + 1];
-    blk_smooth(L, L.x, (const T *)L.b, 1, smoother, w, tmp);
+    blk_smooth<T, H>(L, L.x, (const T *)L.b, 1, smoother, w, tmp);
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
       split_ijk(t, L.nx, L.ny, i, j, k);
-      mg_residual_cell(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
+      mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
     }
     __syncthreads();
     for (int t = threadIdx.x; t < (int)C.n; t += blockDim.x) {
       int i, j, k;
       split_ijk(t, C.nx, C.ny, i, j, k);
-      restrict_cell(L, C, (const T *)L.t, C.b, i, j, k);
+      restrict_cell<T, H>(L, C, (const T *)L.t, C.b, i, j, k);
     }
     __syncthreads();
   }
   // coarse solve: red/black Gauss-Seidel
   {
     const MGLevel<T> L = Ls[nl - 1];
-    blk_smooth(L, L.x, (const T *)L.b, 1, 0, T(1), tmp);
+    blk_smooth<T, H>(L, L.x, (const T *)L.b, 1, 0, T(1), tmp);
   }
   // up: levels nl-2 .. first
   for (int l = nl - 2; l >= first; l--) {
@@ -458,80 +661,88 @@ __device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int 
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
       split_ijk(t, L.nx, L.ny, i, j, k);
-      prolong_add_cell(L, C, (const T *)C.x, L.x, i, j, k);
+      prolong_add_cell<T, H>(L, C, (const T *)C.x, L.x, i, j, k);
     }
     __syncthreads();
-    blk_smooth(L, L.x, (const T *)L.b, 0, smoother, w, tmp);
+    blk_smooth<T, H>(L, L.x, (const T *)L.b, 0, smoother, w, tmp);
   }
 }
 
 // Tail levels in global memory (used when they do not fit in shared memory).
-template <typename T>
+template <typename T, bool H>
 __global__ void __launch_bounds__(512) k_vcycle_tail(const MGLevel<T> *__restrict__ Ls,
                                                       int first, int nl, int smoother, T w,
                                                       T *tmp) {
   pdl_enter();
-  tail_cycle(Ls, first, nl, smoother, w, tmp);
+  tail_cycle<T, H>(Ls, first, nl, smoother, w, tmp);
 }
 
-// Tail levels in shared memory: the block copies every tail level's C E N U,
-// prolongation weights and the first tail level's right-hand side into
-// shared memory (x and b of the coarser levels live there too, plus one
-// scratch vector for residuals and Jacobi updates), runs the cycle with each
-// phase waiting on shared-memory rather than L2 latency, and writes the first
-// tail level's x back.  The copy-in is one flattened loop over all arrays
-// with eight loads in flight per thread.
-template <typename T>
+// Tail levels in shared memory: the block copies every tail level's operator
+// (C E N U, or the scaled FP16 off-diagonals in H mode), transfer weights and
+// the first tail level's right-hand side into shared memory (x and b of the
+// coarser levels live there too, plus one scratch vector for residuals and
+// Jacobi updates), runs the cycle with each phase waiting on shared-memory
+// rather than L2 latency, and writes the first tail level's x back.  The
+// copy-in is one flattened loop over all arrays in 32-bit words with eight
+// loads in flight per thread (FP16 arrays are allocated with padding, so the
+// last word of an odd-length one stays inside its allocation).
 struct TailSeg {
-  T *dst;
-  const T *src;
-  int start;  // first flattened element of this array
+  uint32_t *dst;
+  const uint32_t *src;
+  int start;  // first flattened word of this array
 };
 
-template <typename T>
-__host__ __device__ inline long long tail_pad(long long n) {
-  const long long q = 16 / (long long)sizeof(T);
-  return (n + q - 1) / q * q;
-}
+__host__ __device__ inline long long pad16(long long bytes) { return (bytes + 15) / 16 * 16; }
 
-template <typename T>
+template <typename T, bool H>
 __global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
     const MGLevel<T> *__restrict__ Ls, int first, int nl, int smoother, T w) {
   extern __shared__ __align__(16) unsigned char tail_raw[];
   __shared__ MGLevel<T> S[TAIL_MAX_LEVELS];
-  __shared__ TailSeg<T> seg[7 * TAIL_MAX_LEVELS + 1];
+  __shared__ TailSeg seg[7 * TAIL_MAX_LEVELS + 1];
   __shared__ int nseg;
   pdl_enter();
   const int nt = nl - first;
   if ((int)threadIdx.x < nt) S[threadIdx.x] = Ls[first + threadIdx.x];
   __syncthreads();
   if (threadIdx.x == 0) {
-    T *p = reinterpret_cast<T *>(tail_raw);
+    unsigned char *p = tail_raw;
     int ns = 0, e = 0, maxn = 0;
-    auto place = [&](T *&ptr, int n, bool load) {
+    auto place = [&](auto &ptr, int n, bool load) {
+      using E = typename std::remove_pointer<typename std::remove_reference<decltype(ptr)>::type>::type;
+      const long long bytes = (long long)n * (long long)sizeof(E);
       if (load) {
-        seg[ns].dst = p;
-        seg[ns].src = ptr;
+        seg[ns].dst = reinterpret_cast<uint32_t *>(p);
+        seg[ns].src = reinterpret_cast<const uint32_t *>(ptr);
         seg[ns].start = e;
         ns++;
-        e += n;
+        e += (int)((bytes + 3) / 4);
       }
-      ptr = p;
-      p += tail_pad<T>(n);
+      ptr = reinterpret_cast<E *>(p);
+      p += pad16(bytes);
     };
     for (int q = 0; q < nt; q++) {
       MGLevel<T> &L = S[q];
       const int n = (int)L.n;
-      for (int s = 0; s < 4; s++) place(L.a[s], n, true);
+      if constexpr (H) {
+        for (int s = 0; s < 4; s++) place(L.h[s], n, true);
+      } else {
+        for (int s = 0; s < 4; s++) place(L.a[s], n, true);
+      }
       place(L.x, n, false);
       place(L.b, n, q == 0);
       if (q < nt - 1) {
-        place(L.p1, n, true);
-        place(L.p2, n, true);
+        if constexpr (H) {
+          place(L.q1, n, true);
+          place(L.q2, n, true);
+        } else {
+          place(L.p1, n, true);
+          place(L.p2, n, true);
+        }
       }
       maxn = n > maxn ? n : maxn;
     }
-    for (int q = 0; q < nt; q++) S[q].t = p;
+    for (int q = 0; q < nt; q++) S[q].t = reinterpret_cast<T *>(p);
     seg[ns].start = e;  // sentinel
     nseg = ns;
   }
@@ -539,8 +750,8 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
   const int E = seg[nseg].start;
   int sg = 0;
   for (int e0 = threadIdx.x; e0 < E; e0 += 8 * blockDim.x) {
-    T v[8];
-    T *d[8];
+    uint32_t v[8];
+    uint32_t *d[8];
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       const int e = e0 + u * (int)blockDim.x;
@@ -557,21 +768,24 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
       if (d[u]) *d[u] = v[u];
   }
   __syncthreads();
-  tail_cycle(S, 0, nt, smoother, w, S[0].t);
+  tail_cycle<T, H>(S, 0, nt, smoother, w, S[0].t);
   T *xo = Ls[first].x;
   for (int c = threadIdx.x; c < (int)S[0].n; c += blockDim.x) xo[c] = S[0].x[c];
 }
 
 template <typename T>
-size_t tail_smem_bytes(const MGLevel<T> *L, int first, int nl) {
+size_t tail_smem_bytes(const MGLevel<T> *L, int first, int nl, bool h16) {
   if (nl - first > TAIL_MAX_LEVELS) return ~(size_t)0;
-  long long elems = 0, maxn = 0;
+  long long bytes = 0, maxn = 0;
   for (int q = first; q < nl; q++) {
-    elems += tail_pad<T>(L[q].n) * (q < nl - 1 ? 8 : 6);
-    maxn = L[q].n > maxn ? L[q].n : maxn;
+    const long long n = L[q].n;
+    bytes += h16 ? 4 * pad16(2 * n) : 4 * pad16((long long)sizeof(T) * n);  // operator
+    bytes += 2 * pad16((long long)sizeof(T) * n);                          // x, b
+    if (q < nl - 1) bytes += 2 * pad16((long long)sizeof(T) * n);          // weights
+    maxn = n > maxn ? n : maxn;
   }
-  elems += tail_pad<T>(maxn);
-  return (size_t)elems * sizeof(T);
+  bytes += pad16((long long)sizeof(T) * maxn);
+  return (size_t)bytes;
 }
 
 // multigrid setup of the tail levels in one block (mg_semi.c:534-740)
@@ -615,25 +829,41 @@ __device__ __forceinline__ void st4(float *p, const float v[4]) {
   reinterpret_cast<float4 *>(p)[0] = make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// out = (TO) in; with vec set (both pointers 16-byte aligned) each thread
-// moves four elements per vector access, which keeps enough bytes in flight
-// for a streaming conversion to run at HBM bandwidth
+// one converted element: (TO) v, or with a scale s (H mode) the FP32
+// product (float) v * s (into the V-cycle) / v * s widened (out of it)
+template <typename TI, typename TO>
+__device__ __forceinline__ TO cvt(TI v, const float *s, long long i) {
+  if (!s) return (TO)v;
+  return (TO)((float)v * s[i]);
+}
+
+// out = (TO) in (times scale when given); with vec set (all pointers 16-byte
+// aligned) each thread moves four elements per vector access, which keeps
+// enough bytes in flight for a streaming conversion to run at HBM bandwidth
 template <typename TI, typename TO>
 __global__ void k_convert(const TI *__restrict__ in, TO *__restrict__ out, long long n,
-                          int vec) {
+                          int vec, int flip, const float *__restrict__ scale) {
   pdl_enter();
-  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long bx = flip ? gridDim.x - 1 - blockIdx.x : blockIdx.x;
+  const long long t = bx * blockDim.x + threadIdx.x;
   const long long n4 = vec ? n / 4 : 0;
   if (t < n4) {
     TI a[4];
     TO b[4];
     ld4(in + 4 * t, a);
+    if (scale) {
+      float sv[4];
+      ld4(scale + 4 * t, sv);
 #pragma unroll
-    for (int u = 0; u < 4; u++) b[u] = (TO)a[u];
+      for (int u = 0; u < 4; u++) b[u] = (TO)((float)a[u] * sv[u]);
+    } else {
+#pragma unroll
+      for (int u = 0; u < 4; u++) b[u] = (TO)a[u];
+    }
     st4(out + 4 * t, b);
   }
   const long long c = 4 * n4 + t;
-  if (c < n && t < (vec ? 4 : n)) out[c] = (TO)in[c];
+  if (c < n && t < (vec ? 4 : n)) out[c] = cvt<TI, TO>(in[c], scale, c);
 }
 
 // ---------------------------------------------------------------------------
@@ -668,73 +898,133 @@ void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t 
 template <typename T>
 void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st) {
   Shape3 g = shape3(C.nx, C.ny, C.nz);
-  launch_pdl(k_setup_level<T>, dim3(g.grid), dim3(g.block), st, F, C);
+  if (F.dir == 0)
+    launch_pdl(k_setup_level<T, 0>, dim3(g.grid), dim3(g.block), st, F, C);
+  else if (F.dir == 1)
+    launch_pdl(k_setup_level<T, 1>, dim3(g.grid), dim3(g.block), st, F, C);
+  else
+    launch_pdl(k_setup_level<T, 2>, dim3(g.grid), dim3(g.block), st, F, C);
 }
+// H-mode kernels exist for float storage only
+template <typename T>
+constexpr bool kHasH16 = std::is_same<T, float>::value;
+
 template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
-                     cudaStream_t st) {
+                     cudaStream_t st, int flip, bool h16) {
   Shape3 g = shape3((L.nx + 1) / 2, L.ny, L.nz);
-  launch_pdl(k_rb_sweep<T>, dim3(g.grid), dim3(g.block), st, L, x, b, colour, init);
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      launch_pdl(k_rb_sweep<T, true>, dim3(g.grid), dim3(g.block), st, L, x, b, colour, init,
+                 flip);
+      return;
+    }
+  }
+  launch_pdl(k_rb_sweep<T, false>, dim3(g.grid), dim3(g.block), st, L, x, b, colour, init, flip);
 }
 // RedBlackGSPoint, MaxIter 1, Symmetric: red, black, red; a zero initial
 // guess turns the first red sweep into x = b / a0 (rb_GS_point.c:107-240)
 template <typename T>
 void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
-                      double weight, T *tmp, cudaStream_t st) {
+                      double weight, T *tmp, cudaStream_t st, int *flip, bool h16) {
+  const int f = flip ? *flip : 0, g = flip ? f ^ 1 : 0;
   if (smoother == 1) {
-    Shape3 g = shape3(L.nx, L.ny, L.nz);
-    launch_pdl(k_wjacobi<T>, dim3(g.grid), dim3(g.block), st, L, x, b, tmp, zero);
+    Shape3 sh = shape3(L.nx, L.ny, L.nz);
+    bool done = false;
+    if constexpr (kHasH16<T>) {
+      if (h16) {
+        launch_pdl(k_wjacobi<T, true>, dim3(sh.grid), dim3(sh.block), st, L, x, b, tmp, zero);
+        done = true;
+      }
+    }
+    if (!done)
+      launch_pdl(k_wjacobi<T, false>, dim3(sh.grid), dim3(sh.block), st, L, x, b, tmp, zero);
     launch_pdl(k_wjacobi_update<T>, dim3(nb(L.n, 256)), dim3(256), st, x, tmp, L.n, (T)weight,
                zero);
     return;
   }
   if (smoother == 2) {  // a single red sweep (kernel timing)
-    rb_sweep(L, x, b, 0, 0, st);
+    rb_sweep(L, x, b, 0, 0, st, 0, h16);
     return;
   }
-  rb_sweep(L, x, b, 0, zero, st);
-  rb_sweep(L, x, b, 1, 0, st);
-  rb_sweep(L, x, b, 0, 0, st);
+  rb_sweep(L, x, b, 0, zero, st, f, h16);
+  rb_sweep(L, x, b, 1, 0, st, g, h16);
+  rb_sweep(L, x, b, 0, 0, st, f, h16);
+  if (flip) *flip = g;
 }
-// opt the fused smoother into its dynamic shared memory (> 48 KB); called
-// once per device before any launch or graph capture
+// opt the fused smoother and the shared-memory tails into their dynamic
+// shared memory (> 48 KB); called once per device before any launch or
+// graph capture
 cudaError_t mg_prepare_kernels() {
   cudaError_t e = rbr_fused_prepare<float>();
   if (e != cudaSuccess) return e;
   e = rbr_fused_prepare<double>();
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(k_vcycle_tail_smem<float>,
+  e = cudaFuncSetAttribute(k_vcycle_tail_smem<float, false>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_vcycle_tail_smem<double>,
+  e = cudaFuncSetAttribute(k_vcycle_tail_smem<float, true>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_vcycle_tail_smem<double, false>,
                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
 }
 
 template <typename T>
-void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st) {
+void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st,
+                        int flip, bool h16) {
   Shape3 g = shape3(L.nx, L.ny, L.nz);
-  launch_pdl(k_mg_residual<T>, dim3(g.grid), dim3(g.block), st, L, x, b, r);
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      launch_pdl(k_mg_residual<T, true>, dim3(g.grid), dim3(g.block), st, L, x, b, r, flip);
+      return;
+    }
+  }
+  launch_pdl(k_mg_residual<T, false>, dim3(g.grid), dim3(g.block), st, L, x, b, r, flip);
 }
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
-                        cudaStream_t st) {
+                        cudaStream_t st, int flip, bool h16) {
   Shape3 g = shape3(C.nx, C.ny, C.nz);
-  launch_pdl(k_restrict<T>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc);
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      launch_pdl(k_restrict<T, true>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+      return;
+    }
+  }
+  launch_pdl(k_restrict<T, false>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
 }
 template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
-                           cudaStream_t st) {
+                           cudaStream_t st, int flip, bool h16) {
   Shape3 g = shape3(F.nx, F.ny, F.nz);
-  launch_pdl(k_prolong_add<T>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf);
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      launch_pdl(k_prolong_add<T, true>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+      return;
+    }
+  }
+  launch_pdl(k_prolong_add<T, false>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
 }
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
-                        double weight, T *tmp, size_t smem, cudaStream_t st) {
+                        double weight, T *tmp, size_t smem, cudaStream_t st, bool h16) {
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      if (smem > 0)
+        launch_pdl_smem(k_vcycle_tail_smem<T, true>, dim3(1), dim3(TAIL_THREADS), smem, st,
+                        levels_dev, first, nl, smoother, (T)weight);
+      else
+        launch_pdl(k_vcycle_tail<T, true>, dim3(1), dim3(512), st, levels_dev, first, nl,
+                   smoother, (T)weight, tmp);
+      return;
+    }
+  }
   if (smem > 0)
-    launch_pdl_smem(k_vcycle_tail_smem<T>, dim3(1), dim3(TAIL_THREADS), smem, st, levels_dev,
-                    first, nl, smoother, (T)weight);
+    launch_pdl_smem(k_vcycle_tail_smem<T, false>, dim3(1), dim3(TAIL_THREADS), smem, st,
+                    levels_dev, first, nl, smoother, (T)weight);
   else
-    launch_pdl(k_vcycle_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
+    launch_pdl(k_vcycle_tail<T, false>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
                (T)weight, tmp);
 }
 template <typename T>
@@ -742,11 +1032,112 @@ void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStre
   launch_pdl(k_setup_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl);
 }
 
+// ---------------------------------------------------------------------------
+// Scaled FP16 operator (H mode): from the plain FP32 operator of level F (and
+// the diagonal of the next coarser level C) build h = off-diagonals over
+// S_i S_j and the diagonal C / S^2, the scaled transfer weights q1/q2 and, on
+// level 0, sinv = 1/S, with S = sqrt(|C|) (1 where C is 0 or not finite).
+// 1/S comes from the hardware reciprocal square root (a few ulp): the
+// results are stored as 11-bit FP16 significands, the +-1 diagonal rounds
+// exactly, and sinv is used consistently on the way into and out of the cycle.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float inv_scale_of(float c) {
+  const float a = fabsf(c);
+  return (a > 0.0f && isfinite(a)) ? rsqrtf(a) : 1.0f;
+}
+
+__device__ __forceinline__ void h16_scale_cell(const MGLevel<float> &F, const MGLevel<float> &C,
+                                               int has_coarse, int i, int j, int k) {
+  if (i >= F.nx || j >= F.ny || k >= F.nz) return;
+  const int nx = F.nx, ny = F.ny, nz = F.nz;
+  const int sy = nx, sz = nx * ny;
+  const int c = i + sy * j + sz * k;
+  const float *a0 = F.a[0];
+  // every operand first (predicated loads, one round trip per thread)
+  const float cd = a0[c];
+  const float ce = i + 1 < nx ? a0[c + 1] : 0.0f;
+  const float cn = j + 1 < ny ? a0[c + sy] : 0.0f;
+  const float cu = k + 1 < nz ? a0[c + sz] : 0.0f;
+  const float e = F.a[1][c], n = F.a[2][c], u = F.a[3][c];
+  const int d = F.dir;
+  const int ci = d == 0 ? i : d == 1 ? j : k;
+  const int nd = d == 0 ? nx : d == 1 ? ny : nz;
+  const int ncd = d == 0 ? C.nx : d == 1 ? C.ny : C.nz;
+  float w1 = 0.0f, w2 = 0.0f, clo = 0.0f, chi = 0.0f;
+  if (has_coarse) {
+    // p1/p2 are zero at coarse points (written at fine points only)
+    w1 = F.p1[c];
+    w2 = F.p2[c];
+    const int lo = ci >> 1, hi = (ci + 1) >> 1;  // coarse point at/below, at/above
+    const int il = d == 0 ? lo : i, jl = d == 1 ? lo : j, kl = d == 2 ? lo : k;
+    clo = C.a[0][il + C.nx * (jl + C.ny * kl)];
+    if (hi < ncd) {
+      const int ih = d == 0 ? hi : i, jh = d == 1 ? hi : j, kh = d == 2 ? hi : k;
+      chi = C.a[0][ih + C.nx * (jh + C.ny * kh)];
+    }
+  }
+  const float ic = inv_scale_of(cd);
+  const float ie = i + 1 < nx ? inv_scale_of(ce) : 0.0f;
+  const float in = j + 1 < ny ? inv_scale_of(cn) : 0.0f;
+  const float iu = k + 1 < nz ? inv_scale_of(cu) : 0.0f;
+  F.h[0][c] = __float2half_rn(e * ic * ie);
+  F.h[1][c] = __float2half_rn(n * ic * in);
+  F.h[2][c] = __float2half_rn(u * ic * iu);
+  const __half hd = __float2half_rn(cd * ic * ic);
+  F.h[3][c] = hd;
+  if (__half2float(hd) != 1.0f && *(volatile const int *)F.hflag == 0)
+    atomicExch(const_cast<int *>(F.hflag), 1);
+  if (F.sinv) F.sinv[c] = ic;
+  if (!has_coarse) return;
+  // S_f = |C| / S_f (no division), 1 where C is 0 or not finite
+  const float acd = fabsf(cd);
+  const float sf = (acd > 0.0f && isfinite(acd)) ? acd * ic : 1.0f;
+  if (!(ci & 1)) {
+    F.q1[c] = sf * inv_scale_of(clo);
+    F.q2[c] = 0.0f;
+  } else {
+    F.q1[c] = w1 * sf * inv_scale_of(clo);
+    F.q2[c] = ci + 1 < nd ? w2 * sf * inv_scale_of(chi) : 0.0f;
+  }
+}
+
+__global__ void k_h16_scale(MGLevel<float> F, MGLevel<float> C, int has_coarse) {
+  pdl_enter();
+  int i, j, k;
+  thread_ijk(i, j, k);
+  h16_scale_cell(F, C, has_coarse, i, j, k);
+}
+
+__global__ void __launch_bounds__(512) k_h16_scale_tail(const MGLevel<float> *__restrict__ Ls,
+                                                        int first, int nl) {
+  pdl_enter();
+  for (int l = first; l < nl; l++) {
+    const MGLevel<float> F = Ls[l];
+    const MGLevel<float> C = Ls[l + 1 < nl ? l + 1 : l];
+    for (int t = threadIdx.x; t < (int)F.n; t += blockDim.x) {
+      int i, j, k;
+      split_ijk(t, F.nx, F.ny, i, j, k);
+      h16_scale_cell(F, C, l + 1 < nl, i, j, k);
+    }
+  }
+}
+
+void launch_h16_scale(const MGLevel<float> &F, const MGLevel<float> *C, cudaStream_t st) {
+  Shape3 g = shape3(F.nx, F.ny, F.nz);
+  launch_pdl(k_h16_scale, dim3(g.grid), dim3(g.block), st, F, C ? *C : F, C ? 1 : 0);
+}
+void launch_h16_scale_tail(const MGLevel<float> *levels_dev, int first, int nl,
+                           cudaStream_t st) {
+  launch_pdl(k_h16_scale_tail, dim3(1), dim3(512), st, levels_dev, first, nl);
+}
+
 template <typename TI, typename TO>
-void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
-  const int vec = (((uintptr_t)in | (uintptr_t)out) & 15) == 0;
+void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int flip,
+                    const float *scale) {
+  const int vec = (((uintptr_t)in | (uintptr_t)out | (uintptr_t)scale) & 15) == 0;
   const long long threads = vec ? (n / 4 > 4 ? n / 4 : 4) : (n > 1 ? n : 1);
-  launch_pdl(k_convert<TI, TO>, dim3(nb(threads, 256)), dim3(256), st, in, out, n, vec);
+  launch_pdl(k_convert<TI, TO>, dim3(nb(threads, 256)), dim3(256), st, in, out, n, vec, flip,
+             scale);
 }
 
 #define INST(T)                                                                              \
@@ -754,21 +1145,24 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st) {
   template void launch_mg_coarse_op<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
   template void launch_mg_setup_level<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
   template void launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *, \
-                                    cudaStream_t);                                            \
+                                    cudaStream_t, int *, bool);                               \
   template void launch_mg_residual<T>(const MGLevel<T> &, const T *, const T *, T *,          \
-                                      cudaStream_t);                                          \
+                                      cudaStream_t, int, bool);                               \
   template void launch_mg_restrict<T>(const MGLevel<T> &, const MGLevel<T> &, const T *, T *, \
-                                      cudaStream_t);                                          \
+                                      cudaStream_t, int, bool);                               \
   template void launch_mg_prolong_add<T>(const MGLevel<T> &, const MGLevel<T> &, const T *,   \
-                                         T *, cudaStream_t);                                  \
+                                         T *, cudaStream_t, int, bool);                       \
   template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *, size_t, \
-                                      cudaStream_t);                                          \
-  template size_t tail_smem_bytes<T>(const MGLevel<T> *, int, int);                          \
+                                      cudaStream_t, bool);                                    \
+  template size_t tail_smem_bytes<T>(const MGLevel<T> *, int, int, bool);                    \
   template void launch_setup_tail<T>(const MGLevel<T> *, int, int, cudaStream_t);
 INST(double)
 INST(float)
-template void launch_convert<double, float>(const double *, float *, long long, cudaStream_t);
-template void launch_convert<float, double>(const float *, double *, long long, cudaStream_t);
-template void launch_convert<double, double>(const double *, double *, long long, cudaStream_t);
+template void launch_convert<double, float>(const double *, float *, long long, cudaStream_t, int,
+                                            const float *);
+template void launch_convert<float, double>(const float *, double *, long long, cudaStream_t, int,
+                                            const float *);
+template void launch_convert<double, double>(const double *, double *, long long, cudaStream_t,
+                                             int, const float *);
 
 }  // namespace pfgpu

@@ -11,11 +11,13 @@
 
 #include <cfloat>
 #include <cmath>
+#include <array>
 #include <climits>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/pfgpu.h"
@@ -67,6 +69,12 @@ struct MG {
   MGLevel<T> *Ldev = nullptr;  // device copy of the level table (tail kernels)
   int tail = 0;                // first level run by the single-block tail kernels
   size_t tail_smem = 0;        // shared-memory bytes of the V-cycle tail (0: global)
+  std::vector<char> waved;     // level smoothed by the wavefront kernel
+  std::vector<WaveLevel> wave; // its control words
+  bool h16 = false;            // scaled FP16 operator storage (float levels only)
+  int *hflag = nullptr;        // some scaled diagonal is not +1 (set by the setup)
+  int flip = 1;                // alternate the block order of consecutive launches
+  int flip_out = 0;            // block order for the launch after a V-cycle
   T *wtmp = nullptr;           // Jacobi temp (finest size)
   std::vector<char> fused;     // level smoothed by the fused red/black/red kernel
   std::vector<RbrMaps> maps;   // its tensor maps (input iterate = x)
@@ -81,6 +89,17 @@ struct MG {
 //                     single-block tail kernels, as far as the tail fits in
 //                     shared memory (default 1024)
 //   PFGPU_TAIL_SMEM   0 runs the V-cycle tail from global memory
+//   PFGPU_FLIP        0 runs every V-cycle launch in forward block order
+//   PFGPU_PHASE_TIMES 1 times the solver phases with CUDA events and prints
+//                     the sums to stderr when the handle is destroyed
+//   PFGPU_WAVE_CELLS  grid levels with at least this many cells use the
+//                     wavefront red/black/red kernel (red/black Gauss-Seidel
+//                     smoother only; default: no level, the per-colour sweeps
+//                     are faster on B200)
+//   PFGPU_WAVE_CTAS   resident blocks per SM of the wavefront kernel (default:
+//                     as many as fit)
+//   PFGPU_WAVE_LAG    planes by which each wavefront sweep trails the previous
+//   PFGPU_WAVE_CHUNK  cells of one colour per wavefront work item
 //   PFGPU_RBR_FUSED_CELLS  grid levels with at least this many cells (and a
 //                     row pitch TMA can address) use the TMA-pipelined fused
 //                     red/black/red smoother; the rest one kernel per colour
@@ -99,7 +118,8 @@ struct pfgpu_handle {
   DevProblem P;
   int nx, ny, nz;
   long long N, NP;  // interior cells, ParFlow-layout cells
-  bool mixed = false;
+  bool mixed = false;  // FP32 multigrid and Jacobian storage
+  bool h16 = false;    // ... with the scaled FP16 multigrid operator
   // fields
   double *kx = nullptr, *ky = nullptr, *kz = nullptr;
   double *alpha = nullptr, *vgn = nullptr, *sres = nullptr, *ssat = nullptr, *zmult = nullptr;
@@ -145,6 +165,14 @@ struct pfgpu_handle {
   std::vector<double> hist_dt;
   double *adj = nullptr;  // 8 vectors: lam, lam_next, rhs, r, dx, g_lnk, g_a, g_n
   bool adj_transpose = false;  // matvec applies J^T (adjoint solves)
+  // optional per-phase device timing (PFGPU_PHASE_TIMES=1): events recorded
+  // around each phase on the solver stream, summed after every Newton solve
+  // and printed to stderr when the handle is destroyed
+  bool ptime = false;
+  std::vector<cudaEvent_t> pev;                  // event pool
+  std::vector<std::array<int, 3>> pmark;        // (phase, start event, end event)
+  double pacc[8] = {};
+  long long pcnt[8] = {};
 };
 
 // ---------------------------------------------------------------------------
@@ -156,9 +184,11 @@ static int check_kernel_error(pfgpu_handle *h) {
   CK(cudaMemcpyAsync(h->hkerr, h->kerr, sizeof(int), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
   if (*h->hkerr) {
+    const int code = *h->hkerr;
     *h->hkerr = 0;
     CK(cudaMemsetAsync(h->kerr, 0, sizeof(int), h->st));
-    set_err("a pipelined smoother kernel gave up waiting for its TMA copies");
+    set_err(code == 2 ? "the wavefront smoother gave up waiting for a neighbouring plane"
+                      : "a pipelined smoother kernel gave up waiting for its TMA copies");
     return PFGPU_ERR_CUDA;
   }
   return 0;
@@ -227,10 +257,53 @@ static void vg_state(pfgpu_handle *h, const double *u, bool reuse) {
   h->vg_for = u;
 }
 
+// ---- phase timing (diagnostics) -------------------------------------------
+enum { PH_FEVAL = 0, PH_PCSETUP, PH_PCAPPLY, PH_MATVEC, PH_NEWTON, PH_COUNT };
+static const char *const kPhaseName[PH_COUNT] = {"residual (with VG state)",
+                                                 "preconditioner setup (J + MG setup)",
+                                                 "preconditioner apply (V-cycle)",
+                                                 "Jacobian matvec", "Newton solve total"};
+static int ph_event(pfgpu_handle *h) {
+  const int i = (int)h->pmark.size() * 2 + 1;  // a fresh slot per mark
+  while ((int)h->pev.size() <= i) {
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return -1;
+    h->pev.push_back(e);
+  }
+  return i;
+}
+static int ph_begin(pfgpu_handle *h) {
+  if (!h->ptime) return -1;
+  const int i = ph_event(h);
+  if (i < 0) return -1;
+  h->pmark.push_back({-1, i - 1, i});
+  cudaEventRecord(h->pev[i - 1], h->st);
+  return (int)h->pmark.size() - 1;
+}
+static void ph_end(pfgpu_handle *h, int mark, int phase) {
+  if (!h->ptime || mark < 0) return;
+  h->pmark[mark][0] = phase;
+  cudaEventRecord(h->pev[h->pmark[mark][2]], h->st);
+}
+static void ph_collect(pfgpu_handle *h) {
+  if (!h->ptime || h->pmark.empty()) return;
+  cudaStreamSynchronize(h->st);
+  for (auto &m : h->pmark) {
+    float ms = 0.0f;
+    if (m[0] >= 0 && cudaEventElapsedTime(&ms, h->pev[m[1]], h->pev[m[2]]) == cudaSuccess) {
+      h->pacc[m[0]] += ms;
+      h->pcnt[m[0]]++;
+    }
+  }
+  h->pmark.clear();
+}
+
 static void feval(pfgpu_handle *h, const double *u, double dt, double *f) {
+  const int m = ph_begin(h);
   vg_state(h, u, false);
   launch_residual(h->P, u, h->p_old, h->s_old, h->kr, h->sat, dt, f, h->st);
   h->launches++;
+  ph_end(h, m, PH_FEVAL);
 }
 
 // assemble J (full) and the preconditioner matrix at u (one pass); the VG
@@ -254,7 +327,7 @@ static void assemble(pfgpu_handle *h, const double *u, double dt, bool want_J, b
   h->launches++;
 }
 
-static void matvec(pfgpu_handle *h, const double *x, double *y) {
+static void matvec_impl(pfgpu_handle *h, const double *x, double *y) {
   if (h->adj_transpose) {
     if (h->mixed) {
       JacIn<float> J{h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
@@ -275,6 +348,11 @@ static void matvec(pfgpu_handle *h, const double *x, double *y) {
   }
   h->launches++;
 }
+static void matvec(pfgpu_handle *h, const double *x, double *y) {
+  const int m = ph_begin(h);
+  matvec_impl(h, x, y);
+  ph_end(h, m, PH_MATVEC);
+}
 
 template <typename T>
 static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
@@ -287,6 +365,18 @@ static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
   if (mg.tail < nl - 1) {
     launch_setup_tail<T>(mg.Ldev, mg.tail, nl, st);
     k++;
+  }
+  if constexpr (std::is_same<T, float>::value) {
+    if (mg.h16) {
+      // scaled FP16 operators and weights, once every level's operator is final
+      cudaMemsetAsync(mg.hflag, 0, sizeof(int), st);
+      for (int l = 0; l < mg.tail; l++) {
+        launch_h16_scale(mg.L[l], l + 1 < nl ? &mg.L[l + 1] : nullptr, st);
+        k++;
+      }
+      launch_h16_scale_tail(mg.Ldev, mg.tail, nl, st);
+      k++;
+    }
   }
   return k;
 }
@@ -301,34 +391,53 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   const int nl = (int)mg.L.size();
   const int sk = smoother == 1 ? 2 : 3;
   const int first = mg.tail;
+  // block order of the next grid launch: with mg.flip every launch runs in
+  // the opposite order of the one before it (the input conversion runs
+  // forward), so it starts on the data still in L2
+  int f = mg.flip ? 1 : 0;
+  int *fp = mg.flip ? &f : nullptr;
+  auto next = [&]() {
+    const int r = f;
+    if (mg.flip) f ^= 1;
+    return r;
+  };
   for (int l = 0; l < first; l++) {
     MGLevel<T> &Ll = mg.L[l];
     if (mg.fused[l]) {
       launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x, 1, mg.kerr, st);  // zero guess: x not read
       k++;
+    } else if (mg.waved[l]) {
+      launch_rbr_wave<T>(Ll, mg.wave[l], Ll.x, Ll.b, 1, mg.kerr, st);
+      f = mg.flip ? 1 : 0;  // the wave ends on the top planes
+      k++;
     } else {
-      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st);
+      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st, fp, mg.h16);
       k += sk;
     }
-    launch_mg_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st);
-    launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st);
+    launch_mg_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st, next(), mg.h16);
+    launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st, next(), mg.h16);
     k += 2;
   }
   // levels first .. nl-1, coarse solve (RedBlackGSPoint, mg_semi.c:1276) included
-  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st);
+  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st, mg.h16);
   k++;
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
     const MGLevel<T> &C = mg.L[l + 1];
-    launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st);
+    launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st, next(), mg.h16);
     if (mg.fused[l]) {
       launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x2, 0, mg.kerr, st);
       k += 2;
+    } else if (mg.waved[l]) {
+      launch_rbr_wave<T>(Ll, mg.wave[l], Ll.x, Ll.b, 0, mg.kerr, st);
+      f = mg.flip ? 1 : 0;
+      k += 2;
     } else {
-      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st);
+      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st, fp, mg.h16);
       k += 1 + sk;
     }
   }
+  mg.flip_out = f;
   return k;
 }
 
@@ -355,25 +464,33 @@ static int build_vgraph(pfgpu_handle *h) {
 }
 
 // z = M^{-1} r (dense FP64 device vectors; r and z may alias)
-static int pc_apply_dense(pfgpu_handle *h, const double *r, double *z) {
+static int pc_apply_dense_impl(pfgpu_handle *h, const double *r, double *z) {
   if (h->mixed) {
-    launch_convert<double, float>(r, h->mgf.L[0].b, h->N, h->st);
+    launch_convert<double, float>(r, h->mgf.L[0].b, h->N, h->st, 0,
+                                  h->h16 ? h->mgf.L[0].sinv : nullptr);
   } else {
     CK(cudaMemcpyAsync(h->mgd.L[0].b, r, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
   }
   CK(cudaGraphLaunch(h->vgraph, h->st));
   h->launches += h->graph_nodes + (h->mixed ? 2 : 0);
   if (h->mixed) {
-    launch_convert<float, double>(vcycle_out(h->mgf, h->d.mg_smoother), z, h->N, h->st);
+    launch_convert<float, double>(vcycle_out(h->mgf, h->d.mg_smoother), z, h->N, h->st,
+                                  h->mgf.flip_out, h->h16 ? h->mgf.L[0].sinv : nullptr);
   } else {
     CK(cudaMemcpyAsync(z, vcycle_out(h->mgd, h->d.mg_smoother), h->N * sizeof(double),
                        cudaMemcpyDeviceToDevice, h->st));
   }
   return 0;
 }
+static int pc_apply_dense(pfgpu_handle *h, const double *r, double *z) {
+  const int m = ph_begin(h);
+  const int rc = pc_apply_dense_impl(h, r, z);
+  ph_end(h, m, PH_PCAPPLY);
+  return rc;
+}
 
-static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool also_J,
-                           bool reuse_vg = false) {
+static void pc_setup_dense_impl(pfgpu_handle *h, const double *u, double dt, bool also_J,
+                                bool reuse_vg) {
   assemble(h, u, dt, also_J, true, reuse_vg);
   if (h->mixed)
     h->launches += mg_setup_T<float>(h->mgf, h->st);
@@ -381,6 +498,12 @@ static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool als
     h->launches += mg_setup_T<double>(h->mgd, h->st);
   if (also_J) h->jac_valid = 1;
   h->pc_ready = true;
+}
+static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool also_J,
+                           bool reuse_vg = false) {
+  const int m = ph_begin(h);
+  pc_setup_dense_impl(h, u, dt, also_J, reuse_vg);
+  ph_end(h, m, PH_PCSETUP);
 }
 
 // ---------------------------------------------------------------------------
@@ -506,7 +629,7 @@ static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, cons
 // KINSol with LineSearch (pfsimulator/kinsol/kinsol.c:363-910, 1054-1589).
 // u (dense, device) holds the initial guess on entry and the result on exit.
 // ---------------------------------------------------------------------------
-static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
+static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   const long long N = h->N;
   const pfgpu_desc &d = h->d;
   const double uround = DBL_EPSILON;
@@ -736,6 +859,13 @@ static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   stats->fnorm = fnorm;
   return (ret == 1 || ret == 2) ? PFGPU_OK : PFGPU_NOT_CONVERGED;
 }
+static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
+  const int m = ph_begin(h);
+  const int rc = newton_impl(h, dt, stats);
+  ph_end(h, m, PH_NEWTON);
+  ph_collect(h);
+  return rc;
+}
 
 // ---------------------------------------------------------------------------
 // allocation
@@ -777,6 +907,20 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
       CK(cudaMemset(L.p2, 0, L.n * sizeof(T)));
     }
     CK(cudaMemset(L.x, 0, L.n * sizeof(T)));
+    if (mg.h16) {
+      // FP16 arrays padded so that whole 32-bit words can be copied
+      if (!mg.hflag) {
+        CK(cudaMalloc((void **)&mg.hflag, sizeof(int)));
+        CK(cudaMemset(mg.hflag, 0, sizeof(int)));
+      }
+      L.hflag = mg.hflag;
+      for (int s = 0; s < 4; s++) {
+        if (dalloc(&L.h[s], L.n + 8)) return PFGPU_ERR_NOMEM;
+        CK(cudaMemset(L.h[s], 0, (L.n + 8) * sizeof(__half)));
+      }
+      if (l < nl - 1 && (dalloc(&L.q1, L.n) || dalloc(&L.q2, L.n))) return PFGPU_ERR_NOMEM;
+      if (l == 0 && dalloc(&L.sinv, L.n)) return PFGPU_ERR_NOMEM;
+    }
     if (L.dir == 0) nx = (nx + 1) / 2;
     if (L.dir == 1) ny = (ny + 1) / 2;
     if (L.dir == 2) nz = (nz + 1) / 2;
@@ -787,14 +931,15 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   mg.tail = nl - 1;
   const long long tail_cells = env_ll("PFGPU_TAIL_CELLS", 1024);
   for (int l = 0; l < nl; l++)
-    if (mg.L[l].n <= tail_cells && tail_smem_bytes<T>(mg.L.data(), l, nl) <= TAIL_SMEM_MAX) {
+    if (mg.L[l].n <= tail_cells && tail_smem_bytes<T>(mg.L.data(), l, nl, mg.h16) <= TAIL_SMEM_MAX) {
       mg.tail = l;
       break;
     }
   {
-    const size_t b = tail_smem_bytes<T>(mg.L.data(), mg.tail, nl);
+    const size_t b = tail_smem_bytes<T>(mg.L.data(), mg.tail, nl, mg.h16);
     mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
   }
+  mg.flip = env_ll("PFGPU_FLIP", 1) != 0;
   // grid levels large enough for the fused smoother get an output buffer
   // distinct from the input iterate
   const long long fused_cells = env_ll("PFGPU_RBR_FUSED_CELLS", LLONG_MAX);
@@ -802,7 +947,8 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   mg.maps.resize(nl);
   for (int l = 0; l < mg.tail; l++) {
     MGLevel<T> &L = mg.L[l];
-    if (h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells || !rbr_fused_eligible(L))
+    if (mg.h16 || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells ||
+        !rbr_fused_eligible(L))
       continue;
     if (dalloc(&L.x2, L.n)) return PFGPU_ERR_NOMEM;
     CK(cudaMemset(L.x2, 0, L.n * sizeof(T)));
@@ -811,6 +957,23 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
       return PFGPU_ERR_CUDA;
     }
     mg.fused[l] = 1;
+  }
+  // grid levels large enough for the wavefront smoother (not the fused one)
+  const long long wave_cells = env_ll("PFGPU_WAVE_CELLS", LLONG_MAX);
+  const int wave_ctas = (int)env_ll("PFGPU_WAVE_CTAS", 0);
+  const int wave_lag = (int)env_ll("PFGPU_WAVE_LAG", 8);
+  const int wave_chunk = (int)env_ll("PFGPU_WAVE_CHUNK", 2048);
+  mg.waved.assign(nl, 0);
+  mg.wave.resize(nl);
+  for (int l = 0; l < mg.tail; l++) {
+    if (mg.h16 || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || mg.fused[l] ||
+        mg.L[l].n < wave_cells)
+      continue;
+    if (wave_setup<T>(mg.L[l], wave_ctas, wave_lag, wave_chunk, &mg.wave[l]) != 0) {
+      set_err("wavefront smoother setup failed for multigrid level %d", l);
+      return PFGPU_ERR_CUDA;
+    }
+    mg.waved[l] = 1;
   }
   mg.kerr = h->kerr;
   CK(cudaMalloc((void **)&mg.Ldev, nl * sizeof(MGLevel<T>)));
@@ -825,9 +988,15 @@ static void free_mg(MG<T> &mg) {
     for (int s = 0; s < 4; s++) cudaFree(L.a[s]);
     cudaFree(L.x); cudaFree(L.b); cudaFree(L.t); cudaFree(L.p1); cudaFree(L.p2);
     cudaFree(L.x2);
+    for (int s = 0; s < 4; s++) cudaFree(L.h[s]);
+    cudaFree(L.q1); cudaFree(L.q2); cudaFree(L.sinv);
   }
   cudaFree(mg.wtmp);
   cudaFree(mg.Ldev);
+  for (auto &w : mg.wave) wave_free(&w);
+  cudaFree(mg.hflag);
+  mg.hflag = nullptr;
+  mg.wave.clear();
   mg.L.clear();
 }
 
@@ -885,12 +1054,13 @@ static int create_impl(pfgpu_handle *h) {
     float **J[] = {&h->Jf.c, &h->Jf.w, &h->Jf.e, &h->Jf.s, &h->Jf.n, &h->Jf.l, &h->Jf.u};
     for (float **a : J)
       if (dalloc(a, N)) return PFGPU_ERR_NOMEM;
-    if (alloc_mg<float>(h, h->mgf)) return PFGPU_ERR_NOMEM;
+    h->mgf.h16 = h->h16;
+    if (int rc = alloc_mg<float>(h, h->mgf)) return rc;
   } else {
     double **J[] = {&h->Jd.c, &h->Jd.w, &h->Jd.e, &h->Jd.s, &h->Jd.n, &h->Jd.l, &h->Jd.u};
     for (double **a : J)
       if (dalloc(a, N)) return PFGPU_ERR_NOMEM;
-    if (alloc_mg<double>(h, h->mgd)) return PFGPU_ERR_NOMEM;
+    if (int rc = alloc_mg<double>(h, h->mgd)) return rc;
   }
   CK(cudaMemsetAsync(h->u, 0, N * sizeof(double), h->st));
   // device problem
@@ -921,6 +1091,15 @@ static void destroy_impl(pfgpu_handle *h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->st) cudaStreamSynchronize(h->st);
+  if (h->ptime && h->pcnt[PH_NEWTON] > 0) {
+    fprintf(stderr, "pfgpu phase times (%lldx%lldx%lld, %s): device ms summed over %lld solves\n",
+            (long long)h->nx, (long long)h->ny, (long long)h->nz, h->mixed ? "mixed" : "fp64",
+            h->pcnt[PH_NEWTON]);
+    for (int q = 0; q < PH_COUNT; q++)
+      fprintf(stderr, "  %-40s %10.3f ms  %6lld calls  %8.4f ms/call\n", kPhaseName[q],
+              h->pacc[q], h->pcnt[q], h->pcnt[q] ? h->pacc[q] / h->pcnt[q] : 0.0);
+  }
+  for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   cudaFree(h->hist);
   cudaFree(h->adj);
@@ -965,12 +1144,23 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
     set_err("pfgpu_create: grid must hold at least two cells");
     return nullptr;
   }
+  // the multigrid kernels index cells in 32 bits (a grid this large would
+  // need far more than one device's memory anyway)
+  if ((long long)desc->nx * desc->ny * desc->nz >= (1LL << 31)) {
+    set_err("pfgpu_create: grid must hold fewer than 2^31 cells");
+    return nullptr;
+  }
   if (desc->krylov_dim < 1 || desc->krylov_dim > 30) {
     set_err("pfgpu_create: krylov_dim must be in [1, 30]");
     return nullptr;
   }
   if (desc->max_restarts != 0) {
     set_err("pfgpu_create: only MaxRestarts 0 is supported");
+    return nullptr;
+  }
+  if (desc->precision != PFGPU_PREC_FP64 && desc->precision != PFGPU_PREC_MIXED &&
+      desc->precision != PFGPU_PREC_MIXED_H16) {
+    set_err("pfgpu_create: unknown precision %d", desc->precision);
     return nullptr;
   }
   if (!(desc->dx > 0 && desc->dy > 0 && desc->dz > 0 && desc->density > 0 &&
@@ -985,7 +1175,9 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
   h->nx = desc->nx; h->ny = desc->ny; h->nz = desc->nz;
   h->N = (long long)h->nx * h->ny * h->nz;
   h->NP = (long long)(h->nx + 2) * (h->ny + 2) * (h->nz + 2);
-  h->mixed = desc->precision == PFGPU_PREC_MIXED;
+  h->mixed = desc->precision == PFGPU_PREC_MIXED || desc->precision == PFGPU_PREC_MIXED_H16;
+  h->h16 = desc->precision == PFGPU_PREC_MIXED_H16;
+  h->ptime = env_ll("PFGPU_PHASE_TIMES", 0) != 0;
   if (create_impl(h) != 0) {
     destroy_impl(h);
     delete h;
@@ -1388,6 +1580,8 @@ int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels) {
 static double kernel_bytes(pfgpu_handle *h, int kernel) {
   const double N = (double)h->N;
   const double wJ = h->mixed ? 4.0 : 8.0;
+  // multigrid operator bytes per cell: C E N U, or three FP16 off-diagonals
+  const double wA = h->h16 ? 6.0 : 4 * wJ;
   const double vg = (h->alpha ? 8.0 : 0.0) + (h->vgn ? 8.0 : 0.0) + (h->sres ? 8.0 : 0.0) +
                     (h->ssat ? 8.0 : 0.0);
   const double kf = 8.0 * (1 + (h->ky != h->kx) + (h->kz != h->kx && h->kz != h->ky));
@@ -1396,7 +1590,7 @@ static double kernel_bytes(pfgpu_handle *h, int kernel) {
     case PFGPU_KERNEL_JACOBIAN: return N * (8.0 + kf + vg + 7 * wJ + 4 * wJ);
     case PFGPU_KERNEL_MATVEC: return N * (7 * wJ + 8.0 + 8.0);
     case PFGPU_KERNEL_RB_SWEEP:                                          // C E N U, b, x in + out
-    case PFGPU_KERNEL_COLOUR_SWEEP: return N * (4 * wJ + wJ + 2 * wJ);
+    case PFGPU_KERNEL_COLOUR_SWEEP: return N * (wA + wJ + 2 * wJ);
     default: return 0.0;
   }
 }
@@ -1419,7 +1613,7 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
           MG<float> &mg = h->mgf;
           MGLevel<float> &L = mg.L[0];
           if (!mg.fused.empty() && mg.fused[0]) launch_rbr_fused<float>(L, mg.maps[0], L.x2, 0, mg.kerr, h->st);
-          else launch_mg_smooth<float>(L, L.x, L.b, 0, 0, 1.0, mg.wtmp, h->st);
+          else launch_mg_smooth<float>(L, L.x, L.b, 0, 0, 1.0, mg.wtmp, h->st, nullptr, mg.h16);
         } else {
           MG<double> &mg = h->mgd;
           MGLevel<double> &L = mg.L[0];
@@ -1435,7 +1629,7 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
       case PFGPU_KERNEL_COLOUR_SWEEP:  // one red sweep of the finest level
         if (h->mixed) {
           MGLevel<float> &L = h->mgf.L[0];
-          launch_mg_smooth<float>(L, L.x, L.b, 0, 2, 1.0, h->mgf.wtmp, h->st);
+          launch_mg_smooth<float>(L, L.x, L.b, 0, 2, 1.0, h->mgf.wtmp, h->st, nullptr, h->mgf.h16);
         } else {
           MGLevel<double> &L = h->mgd.L[0];
           launch_mg_smooth<double>(L, L.x, L.b, 0, 2, 1.0, h->mgd.wtmp, h->st);

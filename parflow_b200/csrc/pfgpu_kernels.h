@@ -1,7 +1,10 @@
 // Kernel launch interfaces shared between the library's translation units.
 #pragma once
 
+#include <vector>
+
 #include <cuda.h>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "pfgpu_device.cuh"
@@ -49,6 +52,19 @@ struct MGLevel {
   T *x, *b, *t;
   T *x2;            // output of the fused post-smoother (levels it runs on)
   T *p1, *p2;       // prolongation weights (fine points of this level)
+  // scaled FP16 operator (PFGPU_PREC_MIXED_H16): with S = sqrt(|C|) (1 where
+  // C is 0 or not finite) the V-cycle runs on y = S x, b^ = b / S and
+  // A^ = S^-1 A S^-1, whose off-diagonals A_ij / (S_i S_j) are h[0..2] =
+  // E^ N^ U^ and whose diagonal C / S^2 is h[3]: +1 wherever C > 0, which
+  // the kernels assume unless *hflag (set by the scaling pass when some
+  // diagonal on some level is not +1) tells them to read h[3].  The transfer
+  // weights absorb the scaling: q1 holds S_f / S_c at coarse points (even
+  // indices along dir) and p1 S_f / S_c(below) at fine points, q2 holds
+  // p2 S_f / S_c(above); sinv = 1 / S on level 0 only.
+  __half *h[4];
+  T *q1, *q2;
+  T *sinv;
+  const int *hflag;
 };
 
 // One Gauss-Seidel point update x = (b - sum_nb a_nb x_nb) / a0, the six
@@ -105,6 +121,24 @@ template <typename T>
 void launch_rbr_fused(const MGLevel<T> &L, const RbrMaps &maps, T *xout, int zero, int *err,
                       cudaStream_t st);
 
+// Wavefront red/black/red smoother (mg_wave.cu): per-level control words,
+// the (sweep, plane) order and the launch shape
+struct WaveLevel {
+  int *ctl = nullptr;   // item counter, abort flag, exit counter, per-(sweep, plane) counts
+  int *plan = nullptr;  // (sweep, plane) tasks in wavefront order
+  int rows = 0, nchunks = 0, grid = 0;
+};
+// lag: planes by which each sweep trails the one before (>= 2); chunk_cells:
+// cells of one colour per work item
+template <typename T>
+int wave_setup(const MGLevel<T> &L, int ctas_per_sm, int lag, int chunk_cells, WaveLevel *w);
+void wave_free(WaveLevel *w);
+// red, black, red on level L in place (x not read when zero != 0); *err = 2
+// if a dependency wait expires
+template <typename T>
+void launch_rbr_wave(const MGLevel<T> &L, const WaveLevel &w, T *x, const T *b, int zero,
+                     int *err, cudaStream_t st);
+
 template <typename T>
 void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st);
 template <typename T>
@@ -112,17 +146,28 @@ void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t 
 // prolongation weights of F and the coarse operator C in one launch
 template <typename T>
 void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
+// flip (optional): block order of the first sweep (0 forward, 1 reversed);
+// sweeps alternate and *flip returns the order the next launch should use
 template <typename T>
 void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
-                      double weight, T *tmp, cudaStream_t st);
+                      double weight, T *tmp, cudaStream_t st, int *flip = nullptr,
+                      bool h16 = false);
 cudaError_t mg_prepare_kernels();
+// h16: the level's scaled FP16 operator and weights (float levels only)
 template <typename T>
-void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st);
+void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st,
+                        int flip = 0, bool h16 = false);
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
-                        cudaStream_t st);
+                        cudaStream_t st, int flip = 0, bool h16 = false);
 template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
+                           cudaStream_t st, int flip = 0, bool h16 = false);
+// scaled FP16 operator of level F from its FP32 operator and the diagonal of
+// the next coarser level C (null on the coarsest); sets *F.hflag when a
+// scaled diagonal is not +1 (the flag is cleared before the first level)
+void launch_h16_scale(const MGLevel<float> &F, const MGLevel<float> *C, cudaStream_t st);
+void launch_h16_scale_tail(const MGLevel<float> *levels_dev, int first, int nl,
                            cudaStream_t st);
 // levels `first` .. nl-1 of a V-cycle / of the setup in one single-block
 // kernel; levels_dev is a device copy of the level table.  With smem > 0
@@ -132,14 +177,16 @@ constexpr int TAIL_MAX_LEVELS = 32;
 constexpr int TAIL_THREADS = 1024;
 constexpr size_t TAIL_SMEM_MAX = 200 * 1024;
 template <typename T>
-size_t tail_smem_bytes(const MGLevel<T> *levels_host, int first, int nl);
+size_t tail_smem_bytes(const MGLevel<T> *levels_host, int first, int nl, bool h16 = false);
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
-                        double weight, T *tmp, size_t smem, cudaStream_t st);
+                        double weight, T *tmp, size_t smem, cudaStream_t st, bool h16 = false);
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
+// out = (TO) in, or (TO)((float) in * scale) when scale is given
 template <typename TI, typename TO>
-void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st);
+void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int flip = 0,
+                    const float *scale = nullptr);
 
 // ---- vectors and reductions (krylov_kernels.cu) ----------------------------
 struct ReduceBuf {

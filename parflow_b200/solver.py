@@ -68,7 +68,10 @@ class RichardsGPU:
         d.vg_from_file = 1 if file_mode else 0
         self._zm = np.ascontiguousarray(prob.zmult())
         d.z_mult = self._zm.ctypes.data_as(C.POINTER(C.c_double))
-        d.precision = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
+        precisions = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED, "mixed16": L.PREC_MIXED_H16}
+        if precision not in precisions:
+            raise ValueError(f"precision must be one of {sorted(precisions)}")
+        d.precision = precisions[precision]
         d.residual_tol, d.step_tol = s.residual_tol, s.step_tol
         d.max_iter, d.krylov_dim, d.max_restarts = s.max_iter, s.krylov_dim, s.max_restarts
         d.eta_choice = _ETA[s.eta_choice]

@@ -54,7 +54,7 @@ def _pc(solver, prob, precision, monkeypatch, env):
     return z, launches
 
 
-@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+@pytest.mark.parametrize("precision", ["fp64", "mixed", "mixed16"])
 @pytest.mark.parametrize("name", ["box_small", "box_64", "hetero_96"])
 def test_tail_variants_bitwise_equal(solver, monkeypatch, name, precision):
     prob = _problems()[name]
