@@ -228,6 +228,43 @@ __device__ __forceinline__ void setup_level_cell(const MGLevel<T> &F, const MGLe
   coarse_op_core(F, C, ic, jc, kc, p2_1, p1_2, p2_2);
 }
 
+// H-mode kernels exist for float storage only
+template <typename T>
+constexpr bool kHasH16 = std::is_same<T, float>::value;
+
+// ---- scaled FP16 operator helpers (H mode) --------------------------------
+// 1/S for S = sqrt(|c|), 1 where c is 0 or not finite (hardware reciprocal
+// square root: the scaled values are stored as 11-bit FP16 significands)
+__device__ __forceinline__ float inv_scale_of(float c) {
+  const float a = fabsf(c);
+  return (a > 0.0f && isfinite(a)) ? rsqrtf(a) : 1.0f;
+}
+// S from c and 1/S without a division
+__device__ __forceinline__ float scale_from(float c, float inv) {
+  const float a = fabsf(c);
+  return (a > 0.0f && isfinite(a)) ? a * inv : 1.0f;
+}
+// scaled operator of fine cell c: off-diagonals E N U over S_c S_nb (a0 of
+// the +x, +y, +z neighbours, ignored where has_* is false), the diagonal
+// C / S^2 (raising *hflag when it is not +1) and, on level 0, 1/S; returns 1/S
+__device__ __forceinline__ float h16_store(const MGLevel<float> &F, int c, float cd, float e,
+                                           float n, float u, bool has_e, float ae, bool has_n,
+                                           float an, bool has_u, float au) {
+  const float ic = inv_scale_of(cd);
+  const float ie = has_e ? inv_scale_of(ae) : 0.0f;
+  const float in = has_n ? inv_scale_of(an) : 0.0f;
+  const float iu = has_u ? inv_scale_of(au) : 0.0f;
+  F.h[0][c] = __float2half_rn(e * ic * ie);
+  F.h[1][c] = __float2half_rn(n * ic * in);
+  F.h[2][c] = __float2half_rn(u * ic * iu);
+  const __half hd = __float2half_rn(cd * ic * ic);
+  F.h[3][c] = hd;
+  if (__half2float(hd) != 1.0f && *(volatile const int *)F.hflag == 0)
+    atomicExch(const_cast<int *>(F.hflag), 1);
+  if (F.sinv) F.sinv[c] = ic;
+  return ic;
+}
+
 // The seven entries C W E S N L U of fine cell (i,j,k), zero outside the
 // level: the values coef() returns, gathered with predicated loads so that
 // a thread issues all its loads at once.
@@ -250,7 +287,13 @@ __device__ __forceinline__ void gather7(const LV<T> &L, int i, int j, int k, T s
 // the lower entry of 2c+2 is the upper entry of 2c+1 in symmetric storage).
 // Same operations in the same order as weights_at + coarse_op_core, so the
 // result is bitwise that of setup_level_cell.
-template <typename T, int D>
+//
+// H (float only): the same thread also writes the scaled FP16 operator of
+// its fine points 2c and 2c+1 and the scaled weights q1(2c) = s_c,
+// q1(2c+1), q2(2c-1) (all against its own coarse diagonal; q2(2c+1) comes
+// from the thread of c+1, or is 0 on the last coarse point), exactly as
+// h16_scale_cell computes them; the plain weights p1/p2 are not stored then.
+template <typename T, int D, bool H>
 __global__ void __launch_bounds__(256) k_setup_level(MGLevel<T> F, MGLevel<T> C) {
   pdl_enter();
   int ic, jc, kc;
@@ -284,7 +327,8 @@ __global__ void __launch_bounds__(256) k_setup_level(MGLevel<T> F, MGLevel<T> C)
     }
   }
   const int ip = i + ox, jp = j + oy, kp = k + oz;
-  if (ip < F.nx && jp < F.ny && kp < F.nz) {
+  const bool has_p = ip < F.nx && jp < F.ny && kp < F.nz;
+  if (!H && has_p) {
     const long long f = ip + (long long)F.nx * (jp + (long long)F.ny * kp);
     F.p1[f] = p1_2;
     F.p2[f] = p2_2;
@@ -307,7 +351,40 @@ __global__ void __launch_bounds__(256) k_setup_level(MGLevel<T> F, MGLevel<T> C)
   C.a[1][cc] = E;
   C.a[2][cc] = N;
   C.a[3][cc] = U;
-  C.a[0][cc] = ac0 - (ac3 + ac4 + ac5 + ac6);
+  const T cdiag = ac0 - (ac3 + ac4 + ac5 + ac6);
+  C.a[0][cc] = cdiag;
+  if constexpr (H) {
+    const int nx = F.nx, ny = F.ny, nz = F.nz;
+    const int sy = nx, sz = nx * ny;
+    const float *a0 = F.a[0];
+    const float ics = inv_scale_of(cdiag);
+    // fine point 2c
+    const int f0 = i + sy * j + sz * k;
+    const float ae0 = i + 1 < nx ? a0[f0 + 1] : 0.0f;
+    const float an0 = j + 1 < ny ? a0[f0 + sy] : 0.0f;
+    const float au0 = k + 1 < nz ? a0[f0 + sz] : 0.0f;
+    const float ic0 = h16_store(F, f0, sc[0], sc[2], sc[4], sc[6], i + 1 < nx, ae0, j + 1 < ny,
+                                an0, k + 1 < nz, au0);
+    F.q1[f0] = scale_from(sc[0], ic0) * ics;
+    F.q2[f0] = 0.0f;
+    // fine point 2c-1: its q2 pairs with this coarse point
+    const int im = i - ox, jm = j - oy, km = k - oz;
+    if (im >= 0 && jm >= 0 && km >= 0) {
+      const int fm = im + sy * jm + sz * km;
+      F.q2[fm] = p2_1 * scale_from(sm[0], inv_scale_of(sm[0])) * ics;
+    }
+    // fine point 2c+1
+    if (has_p) {
+      const int f1 = ip + sy * jp + sz * kp;
+      const float ae1 = ip + 1 < nx ? a0[f1 + 1] : 0.0f;
+      const float an1 = jp + 1 < ny ? a0[f1 + sy] : 0.0f;
+      const float au1 = kp + 1 < nz ? a0[f1 + sz] : 0.0f;
+      const float ic1 = h16_store(F, f1, sp[0], sp[2], sp[4], sp[6], ip + 1 < nx, ae1,
+                                  jp + 1 < ny, an1, kp + 1 < nz, au1);
+      F.q1[f1] = p1_2 * scale_from(sp[0], ic1) * ics;
+      if (last) F.q2[f1] = 0.0f;
+    }
+  }
 }
 
 template <typename T>
@@ -542,13 +619,33 @@ __device__ __forceinline__ void restrict_cell(const MGLevel<T> &F, const MGLevel
                          vget(nx, ny, nz, rf, i + ox, j + oy, k + oz));
 }
 
-template <typename T, bool H>
-__global__ void k_restrict(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ rf,
-                           T *__restrict__ rc, int flip) {
+// grid form of restrict_cell with the direction D fixed at compile time and
+// 32-bit indices (same operations, same order)
+template <typename T, bool H, int D>
+__global__ void __launch_bounds__(256) k_restrict(MGLevel<T> F, MGLevel<T> C,
+                                                  const T *__restrict__ rf, T *__restrict__ rc,
+                                                  int flip) {
   pdl_enter();
-  int i, j, k;
-  thread_ijk_flip(i, j, k, flip);
-  restrict_cell<T, H>(F, C, rf, rc, i, j, k);
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int ic = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jc = by * blockDim.y + threadIdx.y;
+  const int kc = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  if (ic >= C.nx || jc >= C.ny) return;
+  constexpr int ox = D == 0, oy = D == 1, oz = D == 2;
+  const int nx = F.nx, ny = F.ny;
+  const int i = ox ? 2 * ic : ic, j = oy ? 2 * jc : jc, k = oz ? 2 * kc : kc;
+  const int so = D == 0 ? 1 : D == 1 ? nx : nx * ny;  // fine stride along D
+  const int nd = D == 0 ? nx : D == 1 ? ny : F.nz;
+  const int cd = D == 0 ? i : D == 1 ? j : k;
+  const int f = i + nx * (j + ny * k);
+  const T *w1 = H ? F.q1 : F.p1;
+  const T *w2 = H ? F.q2 : F.p2;
+  const bool lo = cd > 0, hi = cd + 1 < nd;
+  T centre = rf[f];
+  if constexpr (H) centre = w1[f] * centre;
+  rc[ic + C.nx * (jc + C.ny * kc)] =
+      centre + ((lo ? w2[f - so] : T(0)) * (lo ? rf[f - so] : T(0)) +
+                (hi ? w1[f + so] : T(0)) * (hi ? rf[f + so] : T(0)));
 }
 
 // x_f += P e_c: injection at coarse points, p1 e(f-1) + p2 e(f+1) at fine
@@ -581,13 +678,41 @@ __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLe
   xf[c] = xf[c] + e;
 }
 
-template <typename T, bool H>
-__global__ void k_prolong_add(MGLevel<T> F, MGLevel<T> C, const T *__restrict__ ec,
-                              T *__restrict__ xf, int flip) {
+// grid form of prolong_add_cell with the direction D fixed at compile time:
+// one branch-free formula for both parities (at a coarse point the weights
+// are (1, 0), or (s_c, 0) in H mode, and both coarse neighbours coincide),
+// bitwise the same values as prolong_add_cell
+template <typename T, bool H, int D>
+__global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
+                                                     const T *__restrict__ ec,
+                                                     T *__restrict__ xf, int flip) {
   pdl_enter();
-  int i, j, k;
-  thread_ijk_flip(i, j, k, flip);
-  prolong_add_cell<T, H>(F, C, ec, xf, i, j, k);
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  const int nx = F.nx, ny = F.ny;
+  if (i >= nx || j >= ny) return;
+  const int c = i + nx * (j + ny * k);
+  const int cd = D == 0 ? i : D == 1 ? j : k;
+  const int nd = D == 0 ? nx : D == 1 ? ny : F.nz;
+  const int lo = cd >> 1, hi = (cd + 1) >> 1;  // coarse points at/below, at/above
+  const bool odd = cd & 1;
+  const bool has_hi = hi < (nd + 1) / 2;
+  const int base = D == 0 ? C.nx * (j + C.ny * k) : D == 1 ? i + C.nx * C.ny * k : i + C.nx * j;
+  const int cs = D == 0 ? 1 : D == 1 ? C.nx : C.nx * C.ny;  // coarse stride along D
+  const T el = ec[base + cs * lo];
+  const T eh = has_hi ? ec[base + cs * hi] : T(0);
+  const T *w1p = H ? F.q1 : F.p1;
+  const T *w2p = H ? F.q2 : F.p2;
+  T e;
+  if constexpr (H) {
+    // coarse points: q1 = s_c, q2 = 0
+    e = odd ? (w1p[c] * el + w2p[c] * eh) : w1p[c] * el;
+  } else {
+    e = odd ? (w1p[c] * el + w2p[c] * eh) : el;
+  }
+  xf[c] = xf[c] + e;
 }
 
 // ---------------------------------------------------------------------------
@@ -895,20 +1020,27 @@ void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t 
   Shape3 g = shape3(C.nx, C.ny, C.nz);
   launch_pdl(k_coarse_op<T>, dim3(g.grid), dim3(g.block), st, F, C);
 }
-template <typename T>
-void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st) {
+template <typename T, bool H>
+static void setup_level_d(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st) {
   Shape3 g = shape3(C.nx, C.ny, C.nz);
   if (F.dir == 0)
-    launch_pdl(k_setup_level<T, 0>, dim3(g.grid), dim3(g.block), st, F, C);
+    launch_pdl(k_setup_level<T, 0, H>, dim3(g.grid), dim3(g.block), st, F, C);
   else if (F.dir == 1)
-    launch_pdl(k_setup_level<T, 1>, dim3(g.grid), dim3(g.block), st, F, C);
+    launch_pdl(k_setup_level<T, 1, H>, dim3(g.grid), dim3(g.block), st, F, C);
   else
-    launch_pdl(k_setup_level<T, 2>, dim3(g.grid), dim3(g.block), st, F, C);
+    launch_pdl(k_setup_level<T, 2, H>, dim3(g.grid), dim3(g.block), st, F, C);
 }
-// H-mode kernels exist for float storage only
 template <typename T>
-constexpr bool kHasH16 = std::is_same<T, float>::value;
-
+void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st,
+                           bool h16) {
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      setup_level_d<T, true>(F, C, st);
+      return;
+    }
+  }
+  setup_level_d<T, false>(F, C, st);
+}
 template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
                      cudaStream_t st, int flip, bool h16) {
@@ -982,29 +1114,49 @@ void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaS
   }
   launch_pdl(k_mg_residual<T, false>, dim3(g.grid), dim3(g.block), st, L, x, b, r, flip);
 }
+template <typename T, bool H>
+static void restrict_d(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
+                       cudaStream_t st, int flip) {
+  Shape3 g = shape3(C.nx, C.ny, C.nz);
+  if (F.dir == 0)
+    launch_pdl(k_restrict<T, H, 0>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+  else if (F.dir == 1)
+    launch_pdl(k_restrict<T, H, 1>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+  else
+    launch_pdl(k_restrict<T, H, 2>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+}
+template <typename T, bool H>
+static void prolong_d(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
+                      cudaStream_t st, int flip) {
+  Shape3 g = shape3(F.nx, F.ny, F.nz);
+  if (F.dir == 0)
+    launch_pdl(k_prolong_add<T, H, 0>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+  else if (F.dir == 1)
+    launch_pdl(k_prolong_add<T, H, 1>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+  else
+    launch_pdl(k_prolong_add<T, H, 2>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+}
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
                         cudaStream_t st, int flip, bool h16) {
-  Shape3 g = shape3(C.nx, C.ny, C.nz);
   if constexpr (kHasH16<T>) {
     if (h16) {
-      launch_pdl(k_restrict<T, true>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+      restrict_d<T, true>(F, C, rf, rc, st, flip);
       return;
     }
   }
-  launch_pdl(k_restrict<T, false>, dim3(g.grid), dim3(g.block), st, F, C, rf, rc, flip);
+  restrict_d<T, false>(F, C, rf, rc, st, flip);
 }
 template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
                            cudaStream_t st, int flip, bool h16) {
-  Shape3 g = shape3(F.nx, F.ny, F.nz);
   if constexpr (kHasH16<T>) {
     if (h16) {
-      launch_pdl(k_prolong_add<T, true>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+      prolong_d<T, true>(F, C, ec, xf, st, flip);
       return;
     }
   }
-  launch_pdl(k_prolong_add<T, false>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+  prolong_d<T, false>(F, C, ec, xf, st, flip);
 }
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
@@ -1041,10 +1193,6 @@ void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStre
 // results are stored as 11-bit FP16 significands, the +-1 diagonal rounds
 // exactly, and sinv is used consistently on the way into and out of the cycle.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float inv_scale_of(float c) {
-  const float a = fabsf(c);
-  return (a > 0.0f && isfinite(a)) ? rsqrtf(a) : 1.0f;
-}
 
 __device__ __forceinline__ void h16_scale_cell(const MGLevel<float> &F, const MGLevel<float> &C,
                                                int has_coarse, int i, int j, int k) {
@@ -1076,22 +1224,9 @@ __device__ __forceinline__ void h16_scale_cell(const MGLevel<float> &F, const MG
       chi = C.a[0][ih + C.nx * (jh + C.ny * kh)];
     }
   }
-  const float ic = inv_scale_of(cd);
-  const float ie = i + 1 < nx ? inv_scale_of(ce) : 0.0f;
-  const float in = j + 1 < ny ? inv_scale_of(cn) : 0.0f;
-  const float iu = k + 1 < nz ? inv_scale_of(cu) : 0.0f;
-  F.h[0][c] = __float2half_rn(e * ic * ie);
-  F.h[1][c] = __float2half_rn(n * ic * in);
-  F.h[2][c] = __float2half_rn(u * ic * iu);
-  const __half hd = __float2half_rn(cd * ic * ic);
-  F.h[3][c] = hd;
-  if (__half2float(hd) != 1.0f && *(volatile const int *)F.hflag == 0)
-    atomicExch(const_cast<int *>(F.hflag), 1);
-  if (F.sinv) F.sinv[c] = ic;
+  const float ic = h16_store(F, c, cd, e, n, u, i + 1 < nx, ce, j + 1 < ny, cn, k + 1 < nz, cu);
   if (!has_coarse) return;
-  // S_f = |C| / S_f (no division), 1 where C is 0 or not finite
-  const float acd = fabsf(cd);
-  const float sf = (acd > 0.0f && isfinite(acd)) ? acd * ic : 1.0f;
+  const float sf = scale_from(cd, ic);
   if (!(ci & 1)) {
     F.q1[c] = sf * inv_scale_of(clo);
     F.q2[c] = 0.0f;
@@ -1143,7 +1278,8 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
 #define INST(T)                                                                              \
   template void launch_mg_prolong_weights<T>(const MGLevel<T> &, cudaStream_t);               \
   template void launch_mg_coarse_op<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
-  template void launch_mg_setup_level<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
+  template void launch_mg_setup_level<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t, \
+                                         bool);                                               \
   template void launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *, \
                                     cudaStream_t, int *, bool);                               \
   template void launch_mg_residual<T>(const MGLevel<T> &, const T *, const T *, T *,          \

@@ -358,8 +358,9 @@ template <typename T>
 static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
+  if (mg.h16) cudaMemsetAsync(mg.hflag, 0, sizeof(int), st);
   for (int l = 0; l < mg.tail && l + 1 < nl; l++) {
-    launch_mg_setup_level<T>(mg.L[l], mg.L[l + 1], st);
+    launch_mg_setup_level<T>(mg.L[l], mg.L[l + 1], st, mg.h16);
     k++;
   }
   if (mg.tail < nl - 1) {
@@ -368,12 +369,8 @@ static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
   }
   if constexpr (std::is_same<T, float>::value) {
     if (mg.h16) {
-      // scaled FP16 operators and weights, once every level's operator is final
-      cudaMemsetAsync(mg.hflag, 0, sizeof(int), st);
-      for (int l = 0; l < mg.tail; l++) {
-        launch_h16_scale(mg.L[l], l + 1 < nl ? &mg.L[l + 1] : nullptr, st);
-        k++;
-      }
+      // the grid levels were scaled by their setup kernels; the tail levels
+      // once their operators are final
       launch_h16_scale_tail(mg.Ldev, mg.tail, nl, st);
       k++;
     }

@@ -144,8 +144,10 @@ void launch_mg_prolong_weights(const MGLevel<T> &F, cudaStream_t st);
 template <typename T>
 void launch_mg_coarse_op(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
 // prolongation weights of F and the coarse operator C in one launch
+// (h16: also the scaled FP16 operator of F and its scaled transfer weights)
 template <typename T>
-void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st);
+void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st,
+                           bool h16 = false);
 // flip (optional): block order of the first sweep (0 forward, 1 reversed);
 // sweeps alternate and *flip returns the order the next launch should use
 template <typename T>
