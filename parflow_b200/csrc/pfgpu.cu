@@ -508,8 +508,14 @@ static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool als
 // modified Gram-Schmidt.  Returns 0 success, 1 residual reduced, 2 failure,
 // 6 QR failure; J is assembled at the first matvec if not current.
 // ---------------------------------------------------------------------------
-static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, const double *u,
-                 double dt, pfgpu_stats *stats, int *status) {
+// The right-hand side is b = bsign * src.  When its norm is already known
+// (bnorm >= 0, with bnorm^2 in device memory at *bn2_dev: the Newton step
+// reuses the norm of f from the line search) the start needs no reduction and
+// no host synchronisation; V0 = b / ||b|| is then formed in one pass.  The
+// solution x is written only on return, as M^{-1} (V y) (x0 = 0).
+static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
+                 const double *bn2_dev, double bnorm, double delta, const double *u, double dt,
+                 pfgpu_stats *stats, int *status) {
   const long long N = h->N;
   const int lmax = h->d.krylov_dim;
   double *S = h->gs;
@@ -520,25 +526,34 @@ static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, cons
   double rho = 0.0, r_norm;
 
   *status = 0;
-  launch_fill(x, 0.0, N, h->st);
-  CK(cudaMemcpyAsync(h->V[0], b, N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
-  launch_dot(h->V[0], h->V[0], N, sc + SCI_RNORM, h->rb, h->st);
-  launch_gmres_scalar(GM_START, S, 0, lmax, h->st);
-  h->launches += 3;
-  CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_RNORM, sizeof(double), cudaMemcpyDeviceToHost,
-                     h->st));
-  CK(cudaStreamSynchronize(h->st));
-  r_norm = h->hsc[D_COUNT];
+  if (bnorm >= 0.0) {
+    CK(cudaMemcpyAsync(sc + SCI_RNORM, bn2_dev, sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    launch_gmres_scalar(GM_START, S, 0, lmax, h->st);
+    h->launches++;
+    r_norm = bnorm;
+  } else {
+    launch_dot(src, src, N, sc + SCI_RNORM, h->rb, h->st);
+    launch_gmres_scalar(GM_START, S, 0, lmax, h->st);
+    h->launches += 2;
+    CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_RNORM, sizeof(double), cudaMemcpyDeviceToHost,
+                       h->st));
+    CK(cudaStreamSynchronize(h->st));
+    r_norm = h->hsc[D_COUNT];
+  }
   const double beta = r_norm;
-  if (r_norm <= delta) return 0;
+  if (r_norm <= delta) {
+    launch_fill(x, 0.0, N, h->st);
+    h->launches++;
+    return 0;
+  }
 
   for (int ntries = 0; ntries <= h->d.max_restarts; ntries++) {
     if (ntries > 0) {
       launch_gmres_scalar(GM_START, S, 0, lmax, h->st);  // re-zero H, keep r_norm squared?
       h->launches++;
     }
-    // V0 *= 1 / r_norm
-    launch_scale(h->V[0], 1.0 / r_norm, N, h->st);
+    // V0 = b / r_norm = src * (bsign / r_norm)
+    launch_axpby(h->V[0], src, bsign * (1.0 / r_norm), 0.0, N, h->st);
     h->launches++;
     int l;
     for (l = 0; l < lmax; l++) {
@@ -595,13 +610,13 @@ static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, cons
     CK(cudaStreamSynchronize(h->st));
     if (h->hsc[D_COUNT] != 0.0) {
       *status = 6;
+      launch_fill(x, 0.0, N, h->st);  // no solution: x stays x0 = 0
+      h->launches++;
       return 0;
     }
     if (converged) {
-      if (pc_apply_dense(h, h->xcor, h->xcor)) return PFGPU_ERR_CUDA;
+      if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;  // x = 0 + M^{-1} V y
       stats->pc_solves++;
-      launch_xpay(x, x, 1.0, h->xcor, N, h->st);
-      h->launches++;
       *status = 0;
       return 0;
     }
@@ -611,13 +626,13 @@ static int spgmr(pfgpu_handle *h, double *x, const double *b, double delta, cons
     return PFGPU_ERR_ARG;
   }
   if (rho < beta) {
-    if (pc_apply_dense(h, h->xcor, h->xcor)) return PFGPU_ERR_CUDA;
+    if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;
     stats->pc_solves++;
-    launch_xpay(x, x, 1.0, h->xcor, N, h->st);
-    h->launches++;
     *status = 1;
   } else {
     *status = 2;
+    launch_fill(x, 0.0, N, h->st);
+    h->launches++;
   }
   return 0;
 }
@@ -682,10 +697,9 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
     h->jac_valid = 0;
     pc_setup_dense(h, u, dt, true, true);
     stats->pc_setups++;
-    launch_axpby(h->bb, h->fval, -1.0, 0.0, N, h->st);
-    h->launches++;
+    // b = -f; its norm is the fnorm of the last residual evaluation
     int sstat = 0;
-    int rc = spgmr(h, h->pp, h->bb, eps, u, dt, stats, &sstat);
+    int rc = spgmr(h, h->pp, h->fval, -1.0, dsc + D_F2, fnorm, eps, u, dt, stats, &sstat);
     if (rc) return rc;
     if (sstat != 0 && sstat != 1) {
       stats->lin_conv_fails++;
@@ -1444,7 +1458,7 @@ static int adjoint_solve(pfgpu_handle *h, double *lam, const double *rhs, double
   for (int outer = 0; outer < 100; outer++) {
     pfgpu_stats st{};
     int status = 0;
-    rc = spgmr(h, dx, r, 0.5 * tol * bnorm, u, dt, &st, &status);
+    rc = spgmr(h, dx, r, 1.0, nullptr, -1.0, 0.5 * tol * bnorm, u, dt, &st, &status);
     *iters += st.lin_iters;
     if (rc) break;
     launch_xpay(lam, lam, 1.0, dx, N, h->st);
