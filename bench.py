@@ -42,7 +42,7 @@ HEADLINE = "mixed16"
 # DRAM bytes (read + write) per cell of one k_rb_sweep launch of the headline
 # form, from the ncu capture summarised in
 # profiles/k_rb_sweep_hetero_384x384x50_mixed16.md
-RB_SWEEP_DRAM_BYTES_PER_CELL = None
+RB_SWEEP_DRAM_BYTES_PER_CELL = 15.27
 
 
 def peaks():
@@ -317,8 +317,9 @@ def gpu_arm(args, rank, world, local_rank):
     rel_err32 = float(np.abs(p32 - p64).max() / np.abs(p64).max())
 
     # roofline of the dominant kernel: k_rb_sweep, one red/black colour sweep
-    # (37% of a timestep's GPU time in the launch list); timed on the finest
-    # level, 13.1M cells, 28 algorithmic bytes per cell in f32
+    # (35% of a timestep's GPU time in the launch list); timed on the finest
+    # level, 13.1M cells, 18 algorithmic bytes per cell (FP16 scaled operator
+    # 6 B, b 4 B, x read and written 4 + 4 B)
     kern = {}
     for name in ("colour_sweep", "rb_smooth", "matvec", "residual", "jacobian", "vcycle",
                  "mg_setup"):

@@ -427,6 +427,21 @@ __device__ __forceinline__ void rb_cell(const MGLevel<T> &Lv, T *__restrict__ x,
 // extent equal to nz, predicated neighbour loads, no neighbour loads on the
 // zero-guess sweep and, for the scaled operator with unit diagonal, no
 // division.  Bitwise the same result as rb_cell.
+template <typename T>
+__device__ __forceinline__ T ldro(const T *p) {
+  return __ldg(p);
+}
+__device__ __forceinline__ float ldro_h(const __half *p) {
+  return __half2float(__ldg(p));
+}
+
+// Grid form of rb_cell with lean index arithmetic: 32-bit cell indices (a
+// level that fits in device memory has fewer than 2^31 cells), the grid's z
+// extent equal to nz, predicated neighbour loads, no neighbour loads on the
+// zero-guess sweep and, for the scaled operator with unit diagonal, no
+// division.  Every array the sweep reads is read-only for the launch (it
+// writes one colour and reads only the other), so all loads take the
+// read-only data path.  Bitwise the same result as rb_cell.
 template <typename T, bool H>
 __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ x,
                                                   const T *__restrict__ b, int colour, int init,
@@ -445,40 +460,42 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
   bool unit = false;  // scaled operator with unit diagonal everywhere
   T d = T(1);
   if constexpr (H) {
-    unit = *L.hflag == 0;
-    if (!unit) d = (T)__half2float(L.h[3][c]);
+    unit = ldro(L.hflag) == 0;
+    if (!unit) d = (T)ldro_h(L.h[3] + c);
   } else {
-    d = L.a[0][c];
+    d = ldro(L.a[0] + c);
   }
   if (init) {
-    x[c] = unit ? b[c] : b[c] / d;
+    x[c] = unit ? ldro(b + c) : ldro(b + c) / d;
     return;
   }
   const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
              hu = k + 1 < nz;
   T cw, ce, cs, cn, cl, cu;
   if constexpr (H) {
-    cw = hw ? (T)__half2float(L.h[0][c - 1]) : T(0);
-    ce = (T)__half2float(L.h[0][c]);
-    cs = hs ? (T)__half2float(L.h[1][c - sy]) : T(0);
-    cn = (T)__half2float(L.h[1][c]);
-    cl = hl ? (T)__half2float(L.h[2][c - sz]) : T(0);
-    cu = (T)__half2float(L.h[2][c]);
+    cw = hw ? (T)ldro_h(L.h[0] + c - 1) : T(0);
+    ce = (T)ldro_h(L.h[0] + c);
+    cs = hs ? (T)ldro_h(L.h[1] + c - sy) : T(0);
+    cn = (T)ldro_h(L.h[1] + c);
+    cl = hl ? (T)ldro_h(L.h[2] + c - sz) : T(0);
+    cu = (T)ldro_h(L.h[2] + c);
   } else {
-    cw = hw ? L.a[1][c - 1] : T(0);
-    ce = L.a[1][c];
-    cs = hs ? L.a[2][c - sy] : T(0);
-    cn = L.a[2][c];
-    cl = hl ? L.a[3][c - sz] : T(0);
-    cu = L.a[3][c];
+    cw = hw ? ldro(L.a[1] + c - 1) : T(0);
+    ce = ldro(L.a[1] + c);
+    cs = hs ? ldro(L.a[2] + c - sy) : T(0);
+    cn = ldro(L.a[2] + c);
+    cl = hl ? ldro(L.a[3] + c - sz) : T(0);
+    cu = ldro(L.a[3] + c);
   }
-  T acc = cw * (hw ? x[c - 1] : T(0));
-  acc = fma(ce, he ? x[c + 1] : T(0), acc);
-  acc = fma(cs, hs ? x[c - sy] : T(0), acc);
-  acc = fma(cn, hn ? x[c + sy] : T(0), acc);
-  acc = fma(cl, hl ? x[c - sz] : T(0), acc);
-  acc = fma(cu, hu ? x[c + sz] : T(0), acc);
-  x[c] = unit ? b[c] - acc : (b[c] - acc) / d;
+  const T *xr = x;  // the other colour: not written by this launch
+  T acc = cw * (hw ? ldro(xr + c - 1) : T(0));
+  acc = fma(ce, he ? ldro(xr + c + 1) : T(0), acc);
+  acc = fma(cs, hs ? ldro(xr + c - sy) : T(0), acc);
+  acc = fma(cn, hn ? ldro(xr + c + sy) : T(0), acc);
+  acc = fma(cl, hl ? ldro(xr + c - sz) : T(0), acc);
+  acc = fma(cu, hu ? ldro(xr + c + sz) : T(0), acc);
+  const T bc = ldro(b + c);
+  x[c] = unit ? bc - acc : (bc - acc) / d;
 }
 
 // weighted Jacobi (pfsimulator/parflow_lib/w_jacobi.c:120-290)
@@ -568,30 +585,30 @@ __global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__re
              hu = k + 1 < nz;
   T d, cw, ce, cs, cn, cl, cu;
   if constexpr (H) {
-    d = *L.hflag ? (T)__half2float(L.h[3][c]) : T(1);
-    cw = hw ? (T)__half2float(L.h[0][c - 1]) : T(0);
-    ce = (T)__half2float(L.h[0][c]);
-    cs = hs ? (T)__half2float(L.h[1][c - sy]) : T(0);
-    cn = (T)__half2float(L.h[1][c]);
-    cl = hl ? (T)__half2float(L.h[2][c - sz]) : T(0);
-    cu = (T)__half2float(L.h[2][c]);
+    d = ldro(L.hflag) ? (T)ldro_h(L.h[3] + c) : T(1);
+    cw = hw ? (T)ldro_h(L.h[0] + c - 1) : T(0);
+    ce = (T)ldro_h(L.h[0] + c);
+    cs = hs ? (T)ldro_h(L.h[1] + c - sy) : T(0);
+    cn = (T)ldro_h(L.h[1] + c);
+    cl = hl ? (T)ldro_h(L.h[2] + c - sz) : T(0);
+    cu = (T)ldro_h(L.h[2] + c);
   } else {
-    d = L.a[0][c];
-    cw = hw ? L.a[1][c - 1] : T(0);
-    ce = L.a[1][c];
-    cs = hs ? L.a[2][c - sy] : T(0);
-    cn = L.a[2][c];
-    cl = hl ? L.a[3][c - sz] : T(0);
-    cu = L.a[3][c];
+    d = ldro(L.a[0] + c);
+    cw = hw ? ldro(L.a[1] + c - 1) : T(0);
+    ce = ldro(L.a[1] + c);
+    cs = hs ? ldro(L.a[2] + c - sy) : T(0);
+    cn = ldro(L.a[2] + c);
+    cl = hl ? ldro(L.a[3] + c - sz) : T(0);
+    cu = ldro(L.a[3] + c);
   }
-  T y = -b[c];
-  y += d * x[c];
-  y += cw * (hw ? x[c - 1] : T(0));
-  y += ce * (he ? x[c + 1] : T(0));
-  y += cs * (hs ? x[c - sy] : T(0));
-  y += cn * (hn ? x[c + sy] : T(0));
-  y += cl * (hl ? x[c - sz] : T(0));
-  y += cu * (hu ? x[c + sz] : T(0));
+  T y = -ldro(b + c);
+  y += d * ldro(x + c);
+  y += cw * (hw ? ldro(x + c - 1) : T(0));
+  y += ce * (he ? ldro(x + c + 1) : T(0));
+  y += cs * (hs ? ldro(x + c - sy) : T(0));
+  y += cn * (hn ? ldro(x + c + sy) : T(0));
+  y += cl * (hl ? ldro(x + c - sz) : T(0));
+  y += cu * (hu ? ldro(x + c + sz) : T(0));
   r[c] = -y;
 }
 
@@ -641,11 +658,11 @@ __global__ void __launch_bounds__(256) k_restrict(MGLevel<T> F, MGLevel<T> C,
   const T *w1 = H ? F.q1 : F.p1;
   const T *w2 = H ? F.q2 : F.p2;
   const bool lo = cd > 0, hi = cd + 1 < nd;
-  T centre = rf[f];
-  if constexpr (H) centre = w1[f] * centre;
+  T centre = ldro(rf + f);
+  if constexpr (H) centre = ldro(w1 + f) * centre;
   rc[ic + C.nx * (jc + C.ny * kc)] =
-      centre + ((lo ? w2[f - so] : T(0)) * (lo ? rf[f - so] : T(0)) +
-                (hi ? w1[f + so] : T(0)) * (hi ? rf[f + so] : T(0)));
+      centre + ((lo ? ldro(w2 + f - so) : T(0)) * (lo ? ldro(rf + f - so) : T(0)) +
+                (hi ? ldro(w1 + f + so) : T(0)) * (hi ? ldro(rf + f + so) : T(0)));
 }
 
 // x_f += P e_c: injection at coarse points, p1 e(f-1) + p2 e(f+1) at fine
@@ -701,16 +718,17 @@ __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
   const bool has_hi = hi < (nd + 1) / 2;
   const int base = D == 0 ? C.nx * (j + C.ny * k) : D == 1 ? i + C.nx * C.ny * k : i + C.nx * j;
   const int cs = D == 0 ? 1 : D == 1 ? C.nx : C.nx * C.ny;  // coarse stride along D
-  const T el = ec[base + cs * lo];
-  const T eh = has_hi ? ec[base + cs * hi] : T(0);
+  const T el = ldro(ec + base + cs * lo);
+  const T eh = has_hi ? ldro(ec + base + cs * hi) : T(0);
   const T *w1p = H ? F.q1 : F.p1;
   const T *w2p = H ? F.q2 : F.p2;
   T e;
   if constexpr (H) {
     // coarse points: q1 = s_c, q2 = 0
-    e = odd ? (w1p[c] * el + w2p[c] * eh) : w1p[c] * el;
+    const T w1 = ldro(w1p + c);
+    e = odd ? (w1 * el + ldro(w2p + c) * eh) : w1 * el;
   } else {
-    e = odd ? (w1p[c] * el + w2p[c] * eh) : el;
+    e = odd ? (ldro(w1p + c) * el + ldro(w2p + c) * eh) : el;
   }
   xf[c] = xf[c] + e;
 }
