@@ -135,7 +135,9 @@ const char *pfgpu_last_error(void);
 /* Uploads a spatially varying cell field (ParFlow layout).  Replaces the
  * ProblemData fields read by the modules: permeability (subsrf_sim.c:684-810),
  * per-cell van Genuchten parameters (problem_saturation.c:943-950,
- * problem_phase_rel_perm.c:1930-1932). */
+ * problem_phase_rel_perm.c:1930-1932).  values == NULL on a van Genuchten
+ * field (PFGPU_FIELD_VG_ALPHA .. S_SAT) drops its per-cell array, so that the
+ * descriptor's scalar serves every cell again; permeability needs values. */
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
 
 /* Surface data of the top layer (ProblemData TSlopeX / TSlopeY / Mannings,

@@ -1203,8 +1203,27 @@ void pfgpu_destroy(pfgpu_handle *h) {
 }
 
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
-  if (!h || !values) { set_err("pfgpu_set_field: null argument"); return PFGPU_ERR_ARG; }
+  if (!h) { set_err("pfgpu_set_field: null handle"); return PFGPU_ERR_ARG; }
   CK(cudaSetDevice(h->device));
+  if (!values) {
+    // drop a per-cell van Genuchten array: the descriptor scalar serves again
+    double **vg = field == PFGPU_FIELD_VG_ALPHA ? &h->alpha
+                  : field == PFGPU_FIELD_VG_N   ? &h->vgn
+                  : field == PFGPU_FIELD_S_RES  ? &h->sres
+                  : field == PFGPU_FIELD_S_SAT  ? &h->ssat
+                                                : nullptr;
+    if (!vg) {
+      set_err("pfgpu_set_field: values may be null only for van Genuchten fields");
+      return PFGPU_ERR_ARG;
+    }
+    CK(cudaStreamSynchronize(h->st));
+    cudaFree(*vg);
+    *vg = nullptr;
+    DevProblem &P = h->P;
+    P.alpha = h->alpha; P.vgn = h->vgn; P.sres = h->sres; P.ssat = h->ssat;
+    h->vg_for = nullptr;  // cached van Genuchten state is stale
+    return PFGPU_OK;
+  }
   double **dst = nullptr;
   switch (field) {
     case PFGPU_FIELD_PERM_X: dst = &h->kx; break;
@@ -1232,6 +1251,7 @@ int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
   DevProblem &P = h->P;
   P.kx = h->kx; P.ky = h->ky; P.kz = h->kz;
   P.alpha = h->alpha; P.vgn = h->vgn; P.sres = h->sres; P.ssat = h->ssat;
+  h->vg_for = nullptr;  // cached van Genuchten state is stale
   CK(cudaStreamSynchronize(h->st));
   return PFGPU_OK;
 }

@@ -85,6 +85,11 @@ class RichardsGPU:
         if not h:
             raise L.PfgpuError("pfgpu_create failed: " + L.last_error())
         self.h = C.c_void_p(h)
+        # descriptor scalars of the van Genuchten fields, and the fields that
+        # currently have a per-cell array on the device
+        self._vg_scalar = {L.FIELD_VG_ALPHA: d.vg_alpha, L.FIELD_VG_N: d.vg_n,
+                           L.FIELD_S_RES: d.s_res, L.FIELD_S_SAT: d.s_sat}
+        self._vg_cells = set()
         self._upload_fields()
         self.set_time(prob.start_time + prob.dt)
 
@@ -110,9 +115,20 @@ class RichardsGPU:
             for fid, v in ((L.FIELD_VG_ALPHA, p.vg_alpha), (L.FIELD_VG_N, p.vg_n),
                            (L.FIELD_S_RES, p.s_res), (L.FIELD_S_SAT, p.s_sat)):
                 a = p.field3d(v)
-                if np.all(a == a.flat[0]):
-                    continue  # uniform: the descriptor scalar serves every cell
+                if np.all(a == a.flat[0]) and a.flat[0] == self._vg_scalar[fid]:
+                    # the descriptor scalar serves every cell; drop a per-cell
+                    # array left by an earlier upload
+                    if fid in self._vg_cells:
+                        L.check(self.lib.pfgpu_set_field(self.h, fid, None), "clear field vg")
+                        self._vg_cells.discard(fid)
+                    continue
                 L.check(self.lib.pfgpu_set_field(self.h, fid, _ptr(pad(a))), "set_field vg")
+                self._vg_cells.add(fid)
+
+    def update_fields(self):
+        """Re-upload the problem's cell fields (permeability, van Genuchten,
+        surface) after they changed, e.g. between runs of a parameter study."""
+        self._upload_fields()
 
     def _upload_surface(self):
         """Slopes and Manning's n in ParFlow's 2-D layout (pfgpu_set_surface)."""
