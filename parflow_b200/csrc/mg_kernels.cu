@@ -453,10 +453,22 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
   const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
   const int nx = L.nx, ny = L.ny, nz = L.nz;
   if (j >= ny) return;
-  const int i = 2 * q + ((colour ^ 1 ^ j ^ k) & 1);  // red: (i+j+k) odd
+  const int r = (colour ^ 1 ^ j ^ k) & 1;
+  const int i = 2 * q + r;  // red: (i+j+k) odd
   if (i >= nx) return;
   const int sy = nx, sz = nx * ny;
   const int c = i + sy * j + sz * k;
+  // x / b storage of this cell and of its six (other-colour) neighbours
+  int xo, xw, xe, xs, xn, xl, xu;
+  if (L.split) {
+    const int hx = L.hx, hs = hx * ny, half = hs * nz;
+    const int base = q + hx * j + hs * k;
+    xo = (colour ^ 1) * half + base;  // this colour's parity block
+    const int ob = colour * half + base;
+    xw = ob - 1 + r; xe = ob + r; xs = ob - hx; xn = ob + hx; xl = ob - hs; xu = ob + hs;
+  } else {
+    xo = c; xw = c - 1; xe = c + 1; xs = c - sy; xn = c + sy; xl = c - sz; xu = c + sz;
+  }
   bool unit = false;  // scaled operator with unit diagonal everywhere
   T d = T(1);
   if constexpr (H) {
@@ -466,7 +478,7 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
     d = ldro(L.a[0] + c);
   }
   if (init) {
-    x[c] = unit ? ldro(b + c) : ldro(b + c) / d;
+    x[xo] = unit ? ldro(b + xo) : ldro(b + xo) / d;
     return;
   }
   const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
@@ -488,14 +500,14 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
     cu = ldro(L.a[3] + c);
   }
   const T *xr = x;  // the other colour: not written by this launch
-  T acc = cw * (hw ? ldro(xr + c - 1) : T(0));
-  acc = fma(ce, he ? ldro(xr + c + 1) : T(0), acc);
-  acc = fma(cs, hs ? ldro(xr + c - sy) : T(0), acc);
-  acc = fma(cn, hn ? ldro(xr + c + sy) : T(0), acc);
-  acc = fma(cl, hl ? ldro(xr + c - sz) : T(0), acc);
-  acc = fma(cu, hu ? ldro(xr + c + sz) : T(0), acc);
-  const T bc = ldro(b + c);
-  x[c] = unit ? bc - acc : (bc - acc) / d;
+  T acc = cw * (hw ? ldro(xr + xw) : T(0));
+  acc = fma(ce, he ? ldro(xr + xe) : T(0), acc);
+  acc = fma(cs, hs ? ldro(xr + xs) : T(0), acc);
+  acc = fma(cn, hn ? ldro(xr + xn) : T(0), acc);
+  acc = fma(cl, hl ? ldro(xr + xl) : T(0), acc);
+  acc = fma(cu, hu ? ldro(xr + xu) : T(0), acc);
+  const T bc = ldro(b + xo);
+  x[xo] = unit ? bc - acc : (bc - acc) / d;
 }
 
 // weighted Jacobi (pfsimulator/parflow_lib/w_jacobi.c:120-290)
@@ -583,6 +595,16 @@ __global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__re
   const int c = i + sy * j + sz * k;
   const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
              hu = k + 1 < nz;
+  int xo, xw, xe, xs, xn, xl, xu;  // x / b storage of the cell and its neighbours
+  if (L.split) {
+    const int hx = L.hx, hsl = hx * ny, half = hsl * nz;
+    const int p = (i + j + k) & 1, base = (i >> 1) + hx * j + hsl * k, r = i & 1;
+    xo = p * half + base;
+    const int ob = (p ^ 1) * half + base;
+    xw = ob - 1 + r; xe = ob + r; xs = ob - hx; xn = ob + hx; xl = ob - hsl; xu = ob + hsl;
+  } else {
+    xo = c; xw = c - 1; xe = c + 1; xs = c - sy; xn = c + sy; xl = c - sz; xu = c + sz;
+  }
   T d, cw, ce, cs, cn, cl, cu;
   if constexpr (H) {
     d = ldro(L.hflag) ? (T)ldro_h(L.h[3] + c) : T(1);
@@ -601,14 +623,14 @@ __global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__re
     cl = hl ? ldro(L.a[3] + c - sz) : T(0);
     cu = ldro(L.a[3] + c);
   }
-  T y = -ldro(b + c);
-  y += d * ldro(x + c);
-  y += cw * (hw ? ldro(x + c - 1) : T(0));
-  y += ce * (he ? ldro(x + c + 1) : T(0));
-  y += cs * (hs ? ldro(x + c - sy) : T(0));
-  y += cn * (hn ? ldro(x + c + sy) : T(0));
-  y += cl * (hl ? ldro(x + c - sz) : T(0));
-  y += cu * (hu ? ldro(x + c + sz) : T(0));
+  T y = -ldro(b + xo);
+  y += d * ldro(x + xo);
+  y += cw * (hw ? ldro(x + xw) : T(0));
+  y += ce * (he ? ldro(x + xe) : T(0));
+  y += cs * (hs ? ldro(x + xs) : T(0));
+  y += cn * (hn ? ldro(x + xn) : T(0));
+  y += cl * (hl ? ldro(x + xl) : T(0));
+  y += cu * (hu ? ldro(x + xu) : T(0));
   r[c] = -y;
 }
 
@@ -660,7 +682,7 @@ __global__ void __launch_bounds__(256) k_restrict(MGLevel<T> F, MGLevel<T> C,
   const bool lo = cd > 0, hi = cd + 1 < nd;
   T centre = ldro(rf + f);
   if constexpr (H) centre = ldro(w1 + f) * centre;
-  rc[ic + C.nx * (jc + C.ny * kc)] =
+  rc[xb_index(C, ic, jc, kc)] =
       centre + ((lo ? ldro(w2 + f - so) : T(0)) * (lo ? ldro(rf + f - so) : T(0)) +
                 (hi ? ldro(w1 + f + so) : T(0)) * (hi ? ldro(rf + f + so) : T(0)));
 }
@@ -716,10 +738,12 @@ __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
   const int lo = cd >> 1, hi = (cd + 1) >> 1;  // coarse points at/below, at/above
   const bool odd = cd & 1;
   const bool has_hi = hi < (nd + 1) / 2;
-  const int base = D == 0 ? C.nx * (j + C.ny * k) : D == 1 ? i + C.nx * C.ny * k : i + C.nx * j;
-  const int cs = D == 0 ? 1 : D == 1 ? C.nx : C.nx * C.ny;  // coarse stride along D
-  const T el = ldro(ec + base + cs * lo);
-  const T eh = has_hi ? ldro(ec + base + cs * hi) : T(0);
+  const int clo = D == 0 ? xb_index(C, lo, j, k) : D == 1 ? xb_index(C, i, lo, k)
+                                                         : xb_index(C, i, j, lo);
+  const int chi = D == 0 ? xb_index(C, hi, j, k) : D == 1 ? xb_index(C, i, hi, k)
+                                                         : xb_index(C, i, j, hi);
+  const T el = ldro(ec + clo);
+  const T eh = has_hi ? ldro(ec + chi) : T(0);
   const T *w1p = H ? F.q1 : F.p1;
   const T *w2p = H ? F.q2 : F.p2;
   T e;
@@ -730,7 +754,8 @@ __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
   } else {
     e = odd ? (ldro(w1p + c) * el + ldro(w2p + c) * eh) : el;
   }
-  xf[c] = xf[c] + e;
+  const int xc = xb_index(F, i, j, k);
+  xf[xc] = xf[xc] + e;
 }
 
 // ---------------------------------------------------------------------------
@@ -1283,6 +1308,87 @@ void launch_h16_scale_tail(const MGLevel<float> *levels_dev, int first, int nl,
                            cudaStream_t st) {
   launch_pdl(k_h16_scale_tail, dim3(1), dim3(512), st, levels_dev, first, nl);
 }
+
+// level-0 transfers of the preconditioner: a natural-layout FP64 vector into
+// b of level 0 (its storage type and layout, times the FP16 scaling when
+// given), and x of level 0 back out
+// Each thread moves one cell in each of four consecutive planes: accesses
+// stay contiguous across a warp (in the natural vector and within each
+// colour block) and four loads are in flight per thread.
+constexpr int LEVEL_PLANES = 4;
+
+template <typename TO>
+__global__ void k_level_in(MGLevel<TO> L, const double *__restrict__ in, TO *__restrict__ out,
+                           const float *__restrict__ scale) {
+  pdl_enter();
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y * blockDim.y + threadIdx.y, k0 = LEVEL_PLANES * blockIdx.z;
+  if (i >= L.nx || j >= L.ny) return;
+  const int sz = L.nx * L.ny, c0 = i + L.nx * j + sz * k0;
+  double v[LEVEL_PLANES];
+#pragma unroll
+  for (int u = 0; u < LEVEL_PLANES; u++) v[u] = k0 + u < L.nz ? in[c0 + u * sz] : 0.0;
+#pragma unroll
+  for (int u = 0; u < LEVEL_PLANES; u++)
+    if (k0 + u < L.nz)
+      out[xb_index(L, i, j, k0 + u)] = cvt<double, TO>(v[u], scale, c0 + u * sz);
+}
+template <typename TI>
+__global__ void k_level_out(MGLevel<TI> L, const TI *__restrict__ in, double *__restrict__ out,
+                            const float *__restrict__ scale, int flip) {
+  pdl_enter();
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k0 = LEVEL_PLANES * (flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z);
+  if (i >= L.nx || j >= L.ny) return;
+  const int sz = L.nx * L.ny, c0 = i + L.nx * j + sz * k0;
+  TI v[LEVEL_PLANES];
+#pragma unroll
+  for (int u = 0; u < LEVEL_PLANES; u++)
+    v[u] = k0 + u < L.nz ? in[xb_index(L, i, j, k0 + u)] : TI(0);
+#pragma unroll
+  for (int u = 0; u < LEVEL_PLANES; u++)
+    if (k0 + u < L.nz) out[c0 + u * sz] = cvt<TI, double>(v[u], scale, c0 + u * sz);
+}
+
+template <typename T>
+int launch_level_in(const MGLevel<T> &L, const double *r, const float *scale, cudaStream_t st) {
+  if (L.split) {
+    Shape3 g = shape3(L.nx, L.ny, (L.nz + LEVEL_PLANES - 1) / LEVEL_PLANES);
+    launch_pdl(k_level_in<T>, dim3(g.grid), dim3(g.block), st, L, r, L.b, scale);
+    return 1;
+  }
+  if (std::is_same<T, double>::value && !scale) {
+    cudaMemcpyAsync(L.b, r, L.n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    return 0;
+  }
+  launch_convert<double, T>(r, L.b, L.n, st, 0, scale);
+  return 1;
+}
+template <typename T>
+int launch_level_out(const MGLevel<T> &L, const T *x, double *z, const float *scale, int flip,
+                     cudaStream_t st) {
+  if (L.split) {
+    Shape3 g = shape3(L.nx, L.ny, (L.nz + LEVEL_PLANES - 1) / LEVEL_PLANES);
+    launch_pdl(k_level_out<T>, dim3(g.grid), dim3(g.block), st, L, x, z, scale, flip);
+    return 1;
+  }
+  if (std::is_same<T, double>::value && !scale) {
+    cudaMemcpyAsync(z, x, L.n * sizeof(double), cudaMemcpyDeviceToDevice, st);
+    return 0;
+  }
+  launch_convert<T, double>(x, z, L.n, st, flip, scale);
+  return 1;
+}
+template int launch_level_in<float>(const MGLevel<float> &, const double *, const float *,
+                                    cudaStream_t);
+template int launch_level_in<double>(const MGLevel<double> &, const double *, const float *,
+                                     cudaStream_t);
+template int launch_level_out<float>(const MGLevel<float> &, const float *, double *,
+                                     const float *, int, cudaStream_t);
+template int launch_level_out<double>(const MGLevel<double> &, const double *, double *,
+                                      const float *, int, cudaStream_t);
 
 template <typename TI, typename TO>
 void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int flip,

@@ -11,6 +11,7 @@
 
 #include <cfloat>
 #include <cmath>
+#include <algorithm>
 #include <array>
 #include <climits>
 #include <cstdarg>
@@ -90,6 +91,9 @@ struct MG {
 //                     shared memory (default 1024)
 //   PFGPU_TAIL_SMEM   0 runs the V-cycle tail from global memory
 //   PFGPU_FLIP        0 runs every V-cycle launch in forward block order
+//   PFGPU_SPLIT       0 keeps x and b of the grid levels in the natural
+//                     (interleaved-colour) layout; the TMA-fused and wavefront
+//                     smoothers need it
 //   PFGPU_PHASE_TIMES 1 times the solver phases with CUDA events and prints
 //                     the sums to stderr when the handle is destroyed
 //   PFGPU_WAVE_CELLS  grid levels with at least this many cells use the
@@ -462,21 +466,21 @@ static int build_vgraph(pfgpu_handle *h) {
 
 // z = M^{-1} r (dense FP64 device vectors; r and z may alias)
 static int pc_apply_dense_impl(pfgpu_handle *h, const double *r, double *z) {
-  if (h->mixed) {
-    launch_convert<double, float>(r, h->mgf.L[0].b, h->N, h->st, 0,
-                                  h->h16 ? h->mgf.L[0].sinv : nullptr);
-  } else {
-    CK(cudaMemcpyAsync(h->mgd.L[0].b, r, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
-  }
+  int k = 0;
+  if (h->mixed)
+    k += launch_level_in<float>(h->mgf.L[0], r, h->h16 ? h->mgf.L[0].sinv : nullptr, h->st);
+  else
+    k += launch_level_in<double>(h->mgd.L[0], r, nullptr, h->st);
+  CK(cudaGetLastError());
   CK(cudaGraphLaunch(h->vgraph, h->st));
-  h->launches += h->graph_nodes + (h->mixed ? 2 : 0);
-  if (h->mixed) {
-    launch_convert<float, double>(vcycle_out(h->mgf, h->d.mg_smoother), z, h->N, h->st,
-                                  h->mgf.flip_out, h->h16 ? h->mgf.L[0].sinv : nullptr);
-  } else {
-    CK(cudaMemcpyAsync(z, vcycle_out(h->mgd, h->d.mg_smoother), h->N * sizeof(double),
-                       cudaMemcpyDeviceToDevice, h->st));
-  }
+  if (h->mixed)
+    k += launch_level_out<float>(h->mgf.L[0], vcycle_out(h->mgf, h->d.mg_smoother), z,
+                                 h->h16 ? h->mgf.L[0].sinv : nullptr, h->mgf.flip_out, h->st);
+  else
+    k += launch_level_out<double>(h->mgd.L[0], vcycle_out(h->mgd, h->d.mg_smoother), z, nullptr,
+                                  h->mgd.flip_out, h->st);
+  CK(cudaGetLastError());
+  h->launches += h->graph_nodes + k;
   return 0;
 }
 static int pc_apply_dense(pfgpu_handle *h, const double *r, double *z) {
@@ -909,9 +913,13 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
     L.nx = nx; L.ny = ny; L.nz = nz;
     L.n = (long long)nx * ny * nz;
     L.dir = l < nl - 1 ? dirs[l] : -1;
+    L.hx = (nx + 1) / 2;
     for (int s = 0; s < 4; s++)
       if (dalloc(&L.a[s], L.n)) return PFGPU_ERR_NOMEM;
-    if (dalloc(&L.x, L.n) || dalloc(&L.b, L.n) || dalloc(&L.t, L.n)) return PFGPU_ERR_NOMEM;
+    // x and b sized for the colour-split layout too (one slot more per row of
+    // the shorter colour when nx is odd)
+    const long long nxb = std::max(L.n, 2LL * L.hx * ny * nz);
+    if (dalloc(&L.x, nxb) || dalloc(&L.b, nxb) || dalloc(&L.t, L.n)) return PFGPU_ERR_NOMEM;
     if (l < nl - 1) {
       if (dalloc(&L.p1, L.n) || dalloc(&L.p2, L.n)) return PFGPU_ERR_NOMEM;
       CK(cudaMemset(L.p1, 0, L.n * sizeof(T)));
@@ -951,6 +959,10 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
     mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
   }
   mg.flip = env_ll("PFGPU_FLIP", 1) != 0;
+  // colour-split x / b on the grid levels (red/black smoother); the tail
+  // levels keep the natural layout
+  const bool split = h->d.mg_smoother == PFGPU_SMOOTH_RBGS && env_ll("PFGPU_SPLIT", 1) != 0;
+  for (int l = 0; l < nl; l++) mg.L[l].split = split && l < mg.tail ? 1 : 0;
   // grid levels large enough for the fused smoother get an output buffer
   // distinct from the input iterate
   const long long fused_cells = env_ll("PFGPU_RBR_FUSED_CELLS", LLONG_MAX);
@@ -958,7 +970,7 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   mg.maps.resize(nl);
   for (int l = 0; l < mg.tail; l++) {
     MGLevel<T> &L = mg.L[l];
-    if (mg.h16 || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells ||
+    if (mg.h16 || L.split || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells ||
         !rbr_fused_eligible(L))
       continue;
     if (dalloc(&L.x2, L.n)) return PFGPU_ERR_NOMEM;
@@ -977,7 +989,7 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   mg.waved.assign(nl, 0);
   mg.wave.resize(nl);
   for (int l = 0; l < mg.tail; l++) {
-    if (mg.h16 || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || mg.fused[l] ||
+    if (mg.h16 || mg.L[l].split || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || mg.fused[l] ||
         mg.L[l].n < wave_cells)
       continue;
     if (wave_setup<T>(mg.L[l], wave_ctas, wave_lag, wave_chunk, &mg.wave[l]) != 0) {

@@ -65,7 +65,20 @@ struct MGLevel {
   T *q1, *q2;
   T *sinv;
   const int *hflag;
+  // colour-split storage of x and b (grid levels with the red/black smoother):
+  // cell (i,j,k) of parity p = (i+j+k) & 1 lives at
+  // p * hx*ny*nz + (i >> 1) + hx * (j + ny * k), hx = (nx + 1) / 2, so that a
+  // colour sweep reads and writes whole lines of one colour only
+  int split;
+  int hx;
 };
+
+// storage index of cell (i,j,k) in a level's x / b arrays
+template <typename T>
+__host__ __device__ __forceinline__ int xb_index(const MGLevel<T> &L, int i, int j, int k) {
+  if (!L.split) return i + L.nx * (j + L.ny * k);
+  return ((i + j + k) & 1) * (L.hx * L.ny * L.nz) + (i >> 1) + L.hx * (j + L.ny * k);
+}
 
 // One Gauss-Seidel point update x = (b - sum_nb a_nb x_nb) / a0, the six
 // neighbour products accumulated in the order W E S N L U with explicit fused
@@ -185,6 +198,14 @@ void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smo
                         double weight, T *tmp, size_t smem, cudaStream_t st, bool h16 = false);
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
+// a natural-layout FP64 vector r into b of level 0 / x of level 0 back into a
+// natural FP64 vector z, in the level's type and layout (times the FP16
+// scaling when scale is given); return the number of kernels launched
+template <typename T>
+int launch_level_in(const MGLevel<T> &L, const double *r, const float *scale, cudaStream_t st);
+template <typename T>
+int launch_level_out(const MGLevel<T> &L, const T *x, double *z, const float *scale, int flip,
+                     cudaStream_t st);
 // out = (TO) in, or (TO)((float) in * scale) when scale is given
 template <typename TI, typename TO>
 void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int flip = 0,

@@ -181,50 +181,78 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
 
 // Flux derivatives of one x (or y) face between a (left) and b (right)
 // (richards_jacobian_eval.c:618-660): returns west/east and symmetric parts.
+// TA is the arithmetic of the face terms: double for the FP64 Jacobian; for
+// a Jacobian stored in FP32 the face terms are formed in FP32 too (their
+// products round no worse than the storage), while the upwind decisions, the
+// pressure differences they come from and the row sums stay FP64.  With TA =
+// double the operations are those of the reference macros, in their order.
+template <typename TA>
 struct FaceDer {
-  double lo, hi, sym;  // d/dp of the face flux w.r.t. lower cell (negated), upper cell; sym part
+  TA lo, hi, sym;  // d/dp of the face flux w.r.t. lower cell (negated), upper cell; sym part
 };
 
-__device__ __forceinline__ FaceDer face_der_xy(const DevProblem &P, double dt, double h_ff,
-                                               double dd, double pa, double pb, double ka,
-                                               double kb, double prod, double prod_der,
-                                               double prod_rt, double prod_rt_der, double zm,
-                                               double dir_g, double dir_g_c) {
-  double diff = pa - pb;
-  const double inv_dd = 1.0 / dd;
-  double updir = (diff * inv_dd) * dir_g_c - dir_g;
-  double coeff = 1.0 * dt * h_ff * inv_dd * zm * harmonic(ka, kb) * P.inv_visc;
-  FaceDer r;
-  double sym_lo = (-coeff * upstream(updir, 0.0, prod, prod_rt)) * dir_g_c;
-  r.lo = (-coeff * diff * upstream(updir, 0.0, prod_der, 0.0)) * dir_g_c + sym_lo;
-  r.lo += (coeff * dd * upstream(updir, 0.0, prod_der, 0.0)) * dir_g;
-  r.sym = (-coeff * upstream(updir, 0.0, prod, prod_rt)) * dir_g_c;
-  r.hi = (coeff * diff * upstream(updir, 0.0, 0.0, prod_rt_der)) * dir_g_c + r.sym;
-  r.hi += -(coeff * dd * upstream(updir, 0.0, 0.0, prod_rt_der)) * dir_g;
+template <typename TA>
+__device__ __forceinline__ TA harmonic_t(TA a, TA b) {
+  return (a + b) ? (TA(2) * a * b) / (a + b) : TA(0);
+}
+template <typename TA>
+__device__ __forceinline__ TA harmonic_dz_t(TA a, TA b, TA c, TA d) {
+  return ((c * b) + (a * d)) ? (((c + d) * a * b) / ((b * c) + (a * d))) : TA(0);
+}
+// upstream() with the decision taken in FP64 and the values in TA
+template <typename TA>
+__device__ __forceinline__ TA pick(double a, double b, TA c, TA d) {
+  return ((a - b) >= 0) ? c : d;
+}
+
+template <typename TA>
+__device__ __forceinline__ FaceDer<TA> face_der_xy(const DevProblem &P, double dt, double h_ff,
+                                                   double dd, double inv_dd, double pa,
+                                                   double pb, double ka, double kb, double prod,
+                                                   double prod_der, double prod_rt,
+                                                   double prod_rt_der, double zm, double dir_g,
+                                                   double dir_g_c) {
+  const double diff64 = pa - pb;
+  const double updir = (diff64 * inv_dd) * dir_g_c - dir_g;
+  const TA diff = (TA)diff64;
+  const TA coeff = TA(1.0) * (TA)dt * (TA)h_ff * (TA)inv_dd * (TA)zm *
+                   harmonic_t<TA>((TA)ka, (TA)kb) * (TA)P.inv_visc;
+  const TA dgc = (TA)dir_g_c, dg = (TA)dir_g, tdd = (TA)dd;
+  FaceDer<TA> r;
+  TA sym_lo = (-coeff * pick<TA>(updir, 0.0, (TA)prod, (TA)prod_rt)) * dgc;
+  r.lo = (-coeff * diff * pick<TA>(updir, 0.0, (TA)prod_der, TA(0.0))) * dgc + sym_lo;
+  r.lo += (coeff * tdd * pick<TA>(updir, 0.0, (TA)prod_der, TA(0.0))) * dg;
+  r.sym = (-coeff * pick<TA>(updir, 0.0, (TA)prod, (TA)prod_rt)) * dgc;
+  r.hi = (coeff * diff * pick<TA>(updir, 0.0, TA(0.0), (TA)prod_rt_der)) * dgc + r.sym;
+  r.hi += -(coeff * tdd * pick<TA>(updir, 0.0, TA(0.0), (TA)prod_rt_der)) * dg;
   return r;
 }
 
 // z face between a (lower) and b (upper) (richards_jacobian_eval.c:697-745)
-__device__ __forceinline__ FaceDer face_der_z(const DevProblem &P, double dt, double pa,
-                                              double pb, double ka, double kb, double prod,
-                                              double prod_der, double prod_up,
-                                              double prod_up_der, double za, double zb, int k) {
+template <typename TA>
+__device__ __forceinline__ FaceDer<TA> face_der_z(const DevProblem &P, double dt, double pa,
+                                                  double pb, double ka, double kb, double prod,
+                                                  double prod_der, double prod_up,
+                                                  double prod_up_der, double za, double zb,
+                                                  int k) {
   const double g = P.gravity, rho = P.density, drho = 0.0;
   const double dz = P.dz;
   const double inv_sep = __ldg(P.zface + 3 * k);
   double lower_cond = pa * inv_sep - __ldg(P.zface + 3 * k + 1) * rho * g;
   double upper_cond = pb * inv_sep + __ldg(P.zface + 3 * k + 2) * rho * g;
-  double diff = lower_cond - upper_cond;
-  double z_coeff = 1.0 * dt * (P.dx * P.dy) * harmonic_dz(ka, kb, za, zb) * P.inv_visc;
-  double up = upstream(lower_cond, upper_cond, prod, prod_up);
-  double sym_lower = -z_coeff * inv_sep * up;
-  FaceDer r;
-  r.lo = -z_coeff * (diff * upstream(lower_cond, upper_cond, prod_der, 0.0) +
-                     (-g * 0.5 * dz * (amean(za, zb)) * drho * up)) +
+  const TA diff = (TA)(lower_cond - upper_cond);
+  const TA z_coeff = TA(1.0) * (TA)dt * ((TA)P.dx * (TA)P.dy) *
+                     harmonic_dz_t<TA>((TA)ka, (TA)kb, (TA)za, (TA)zb) * (TA)P.inv_visc;
+  const TA up = pick<TA>(lower_cond, upper_cond, (TA)prod, (TA)prod_up);
+  const TA grav = (TA)(-g * 0.5 * dz * (amean(za, zb)) * drho);
+  const TA sym_lower = -z_coeff * (TA)inv_sep * up;
+  FaceDer<TA> r;
+  r.lo = -z_coeff * (diff * pick<TA>(lower_cond, upper_cond, (TA)prod_der, TA(0.0)) +
+                     (grav * up)) +
          sym_lower;
-  r.sym = z_coeff * inv_sep * -up;
-  r.hi = z_coeff * (diff * upstream(lower_cond, upper_cond, 0.0, prod_up_der) +
-                    (-g * 0.5 * dz * (amean(za, zb)) * drho * up)) +
+  r.sym = z_coeff * (TA)inv_sep * -up;
+  r.hi = z_coeff * (diff * pick<TA>(lower_cond, upper_cond, TA(0.0), (TA)prod_up_der) +
+                    (grav * up)) +
          r.sym;
   return r;
 }
@@ -239,6 +267,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
                            const double *__restrict__ satv, const double *__restrict__ dsatv,
                            double dt, JacOut<TJ> J, PCOut<TP> M) {
   pdl_enter();
+  using TA = TJ;  // arithmetic of the face terms (see face_der_xy)
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
   const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
@@ -261,7 +290,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   double es = 0.0, ns = 0.0, us = 0.0;
   if (k > 0) {
     long long q = c - sz;
-    FaceDer d = face_der_z(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
+    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
                            dkr[q] * rho + kr[q] * drho, prod, prod_der, __ldg(P.zmult + k - 1),
                            zm, k - 1);
     cp += -d.hi;
@@ -271,7 +300,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   if (j > 0) {
     long long q = c - sy;
     if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
-    FaceDer d = face_der_xy(P, dt, ffy, P.dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
                             dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
     s = d.lo;
@@ -279,7 +308,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   if (i > 0) {
     long long q = c - 1;
     if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
-    FaceDer d = face_der_xy(P, dt, ffx, P.dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
                             dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     cp += -d.hi;
     w = d.lo;
@@ -288,7 +317,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   if (i + 1 < P.nx) {
     long long q = c + 1;
     if (SURF) tfg_face_x(P, i, j, gs, gc);
-    FaceDer d = face_der_xy(P, dt, ffx, P.dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
                             kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     west_t = d.lo;
     e = d.hi;
@@ -297,7 +326,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   if (j + 1 < P.ny) {
     long long q = c + sy;
     if (SURF) tfg_face_y(P, i, j, gs, gc);
-    FaceDer d = face_der_xy(P, dt, ffy, P.dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
                             kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
     south_t = d.lo;
     nn = d.hi;
@@ -305,7 +334,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   }
   if (k + 1 < P.nz) {
     long long q = c + sz;
-    FaceDer d = face_der_z(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
+    FaceDer<TA> d = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
                            dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
     lower_t = d.lo;
     u = d.hi;

@@ -3,7 +3,7 @@ per-colour sweep kernels and the reference.
 
 PFGPU_RBR_FUSED_CELLS selects, at handle creation, the grid levels the fused
 kernel smooths: 0 = every level whose row pitch TMA can address, a huge
-value = none (the default).  PFGPU_TAIL_CELLS = 16 keeps all but the last few levels on grid
+value = none (the default); it reads the natural (PFGPU_SPLIT=0) layout.  PFGPU_TAIL_CELLS = 16 keeps all but the last few levels on grid
 kernels, so that the small fixtures exercise the fused kernel too.  Both
 smoothers perform the same per-cell arithmetic, so the V-cycle output must be
 bitwise identical; against the reference's preconditioner output the usual
@@ -42,6 +42,7 @@ def _problems():
 def _pc(solver, prob, precision, monkeypatch, cells):
     monkeypatch.setenv("PFGPU_RBR_FUSED_CELLS", cells)
     monkeypatch.setenv("PFGPU_TAIL_CELLS", "16")
+    monkeypatch.setenv("PFGPU_SPLIT", "0")  # the fused kernel reads the natural layout
     s = solver.RichardsGPU(prob, precision=precision)
     rng = np.random.default_rng(3)
     p = prob.initial_pressure() + 0.1 * rng.standard_normal(prob.shape)
@@ -71,6 +72,7 @@ def test_fused_smoother_bitwise_equals_colour_sweeps(solver, monkeypatch, name, 
 def test_fused_preconditioner_vs_reference(solver, monkeypatch, golden, name):
     monkeypatch.setenv("PFGPU_RBR_FUSED_CELLS", ALL)
     monkeypatch.setenv("PFGPU_TAIL_CELLS", "16")
+    monkeypatch.setenv("PFGPU_SPLIT", "0")  # the fused kernel reads the natural layout
     g = golden(name)
     s = solver.RichardsGPU(cases.get(name))
     for i in range(len(g["pc_in"])):
@@ -87,6 +89,7 @@ def test_fused_timesteps_vs_oracle(solver, monkeypatch):
     from oracle.oracle import Oracle
 
     monkeypatch.setenv("PFGPU_RBR_FUSED_CELLS", ALL)
+    monkeypatch.setenv("PFGPU_SPLIT", "0")
     prob = configs.box(nsteps=2)
     ps_o, st_o = Oracle(prob).run()
     s = solver.RichardsGPU(prob)

@@ -43,6 +43,7 @@ def _problems():
 def _env(monkeypatch, cells):
     monkeypatch.setenv("PFGPU_WAVE_CELLS", cells)
     monkeypatch.setenv("PFGPU_TAIL_CELLS", "16")
+    monkeypatch.setenv("PFGPU_SPLIT", "0")  # the wavefront kernel reads the natural layout
 
 
 def _pc(solver, prob, precision, monkeypatch, cells):
