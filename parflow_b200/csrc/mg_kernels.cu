@@ -228,6 +228,15 @@ __device__ __forceinline__ void setup_level_cell(const MGLevel<T> &F, const MGLe
   coarse_op_core(F, C, ic, jc, kc, p2_1, p1_2, p2_2);
 }
 
+// PFGPU_SWEEP_ONE_CELL=1: one cell per thread in every colour sweep (A/B)
+static bool getenv_flag_one_cell() {
+  static const bool v = [] {
+    const char *e = getenv("PFGPU_SWEEP_ONE_CELL");
+    return e && *e == '1';
+  }();
+  return v;
+}
+
 // H-mode kernels exist for float storage only
 template <typename T>
 constexpr bool kHasH16 = std::is_same<T, float>::value;
@@ -508,6 +517,88 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
   acc = fma(cu, hu ? ldro(xr + xu) : T(0), acc);
   const T bc = ldro(b + xo);
   x[xo] = unit ? bc - acc : (bc - acc) / d;
+}
+
+// Colour sweep of a colour-split level with two cells per thread: cells q
+// and q+1 of one colour in a row (x indices i and i+2, adjacent in the colour
+// block) share the row's index arithmetic, the predicates, the diagonal flag
+// and the other-colour cell between them.  Same per-cell arithmetic, in the
+// same order, as k_rb_sweep.
+template <typename T, bool H>
+__global__ void __launch_bounds__(256) k_rb_sweep2(MGLevel<T> L, T *__restrict__ x,
+                                                   const T *__restrict__ b, int colour,
+                                                   int init, int flip) {
+  pdl_enter();
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int q0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  const int nx = L.nx, ny = L.ny, nz = L.nz;
+  if (j >= ny) return;
+  const int r = (colour ^ 1 ^ j ^ k) & 1;
+  const int i0 = 2 * q0 + r;  // red: (i+j+k) odd
+  if (i0 >= nx) return;
+  const bool two = i0 + 2 < nx;  // the second cell, i0 + 2, exists
+  const int sy = nx, sz = nx * ny;
+  const int c0 = i0 + sy * j + sz * k, c1 = c0 + 2;
+  const int hx = L.hx, hs = hx * ny, half = hs * nz;
+  const int base = q0 + hx * j + hs * k;
+  const int xo = (colour ^ 1) * half + base;  // own cells: xo, xo + 1
+  const int ob = colour * half + base;        // other colour, same (q, j, k)
+  bool unit = false;
+  T d0 = T(1), d1 = T(1);
+  if constexpr (H) {
+    unit = ldro(L.hflag) == 0;
+    if (!unit) {
+      d0 = (T)ldro_h(L.h[3] + c0);
+      if (two) d1 = (T)ldro_h(L.h[3] + c1);
+    }
+  } else {
+    d0 = ldro(L.a[0] + c0);
+    if (two) d1 = ldro(L.a[0] + c1);
+  }
+  if (init) {
+    x[xo] = unit ? ldro(b + xo) : ldro(b + xo) / d0;
+    if (two) x[xo + 1] = unit ? ldro(b + xo + 1) : ldro(b + xo + 1) / d1;
+    return;
+  }
+  const bool hw = i0 > 0, he0 = i0 + 1 < nx, he1 = i0 + 3 < nx, hsj = j > 0, hn = j + 1 < ny,
+             hl = k > 0, hu = k + 1 < nz;
+  auto coef = [&](int s, int c) -> T {  // E / N / U entry s of cell c
+    if constexpr (H)
+      return (T)ldro_h(L.h[s] + c);
+    else
+      return ldro(L.a[s + 1] + c);
+  };
+  const T *xr = x;  // the other colour: not written by this launch
+  const T xm = he0 ? ldro(xr + ob + r) : T(0);  // between the two cells
+  {
+    const T cw = hw ? coef(0, c0 - 1) : T(0), ce = coef(0, c0);
+    const T cs = hsj ? coef(1, c0 - sy) : T(0), cn = coef(1, c0);
+    const T cl = hl ? coef(2, c0 - sz) : T(0), cu = coef(2, c0);
+    T acc = cw * (hw ? ldro(xr + ob - 1 + r) : T(0));
+    acc = fma(ce, xm, acc);
+    acc = fma(cs, hsj ? ldro(xr + ob - hx) : T(0), acc);
+    acc = fma(cn, hn ? ldro(xr + ob + hx) : T(0), acc);
+    acc = fma(cl, hl ? ldro(xr + ob - hs) : T(0), acc);
+    acc = fma(cu, hu ? ldro(xr + ob + hs) : T(0), acc);
+    const T bc = ldro(b + xo);
+    x[xo] = unit ? bc - acc : (bc - acc) / d0;
+  }
+  if (two) {
+    const int o1 = ob + 1;
+    const T cw = coef(0, c1 - 1), ce = coef(0, c1);
+    const T cs = hsj ? coef(1, c1 - sy) : T(0), cn = coef(1, c1);
+    const T cl = hl ? coef(2, c1 - sz) : T(0), cu = coef(2, c1);
+    T acc = cw * xm;
+    acc = fma(ce, he1 ? ldro(xr + o1 + r) : T(0), acc);
+    acc = fma(cs, hsj ? ldro(xr + o1 - hx) : T(0), acc);
+    acc = fma(cn, hn ? ldro(xr + o1 + hx) : T(0), acc);
+    acc = fma(cl, hl ? ldro(xr + o1 - hs) : T(0), acc);
+    acc = fma(cu, hu ? ldro(xr + o1 + hs) : T(0), acc);
+    const T bc = ldro(b + xo + 1);
+    x[xo + 1] = unit ? bc - acc : (bc - acc) / d1;
+  }
 }
 
 // weighted Jacobi (pfsimulator/parflow_lib/w_jacobi.c:120-290)
@@ -1087,6 +1178,17 @@ void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_
 template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
                      cudaStream_t st, int flip, bool h16) {
+  // two cells per thread on colour-split levels of the FP16 operator (it is
+  // bound by instruction issue there; the FP32 and FP64 sweeps, bound by
+  // memory, are as fast or faster with one cell per thread and more threads)
+  if constexpr (kHasH16<T>) {
+    if (h16 && L.split && !getenv_flag_one_cell()) {
+      Shape3 g2 = shape3((L.hx + 1) / 2, L.ny, L.nz);
+      launch_pdl(k_rb_sweep2<T, true>, dim3(g2.grid), dim3(g2.block), st, L, x, b, colour,
+                 init, flip);
+      return;
+    }
+  }
   Shape3 g = shape3((L.nx + 1) / 2, L.ny, L.nz);
   if constexpr (kHasH16<T>) {
     if (h16) {

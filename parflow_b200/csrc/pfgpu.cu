@@ -1625,6 +1625,12 @@ static double kernel_bytes(pfgpu_handle *h, int kernel) {
   const double wJ = h->mixed ? 4.0 : 8.0;
   // multigrid operator bytes per cell: C E N U, or three FP16 off-diagonals
   const double wA = h->h16 ? 6.0 : 4 * wJ;
+  // x / b bytes per cell of one colour sweep: b of the swept colour, x of the
+  // other colour read and of the swept colour written; with the natural
+  // layout every line of b and x is read and x written back
+  const bool split0 = h->mixed ? (h->mgf.L.size() && h->mgf.L[0].split)
+                               : (h->mgd.L.size() && h->mgd.L[0].split);
+  const double wXB = split0 ? 1.5 * wJ : 3 * wJ;
   const double vg = (h->alpha ? 8.0 : 0.0) + (h->vgn ? 8.0 : 0.0) + (h->sres ? 8.0 : 0.0) +
                     (h->ssat ? 8.0 : 0.0);
   const double kf = 8.0 * (1 + (h->ky != h->kx) + (h->kz != h->kx && h->kz != h->ky));
@@ -1633,7 +1639,7 @@ static double kernel_bytes(pfgpu_handle *h, int kernel) {
     case PFGPU_KERNEL_JACOBIAN: return N * (8.0 + kf + vg + 7 * wJ + 4 * wJ);
     case PFGPU_KERNEL_MATVEC: return N * (7 * wJ + 8.0 + 8.0);
     case PFGPU_KERNEL_RB_SWEEP:                                          // C E N U, b, x in + out
-    case PFGPU_KERNEL_COLOUR_SWEEP: return N * (wA + wJ + 2 * wJ);
+    case PFGPU_KERNEL_COLOUR_SWEEP: return N * (wA + wXB);
     default: return 0.0;
   }
 }
