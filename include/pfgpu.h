@@ -140,6 +140,26 @@ const char *pfgpu_last_error(void);
  * descriptor's scalar serves every cell again; permeability needs values. */
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
 
+/* ParFlow binary (PFB) files of the device state.  The format
+ * (write_parflow_binary.c:74-205, read_parflow_binary.c:38-120): big-endian
+ * origin x y z and spacings, nx ny nz, the number of subgrids, then per
+ * subgrid its box and values, x fastest.
+ *
+ * pfgpu_write_pfb writes the current pressure (PFGPU_PFB_PRESSURE) or the
+ * saturation at it (PFGPU_PFB_SATURATION) as one subgrid with the
+ * descriptor's spacings and the given origin; the values are packed and
+ * byte-swapped on the device and copied to the host once.
+ * pfgpu_read_pfb reads a file of any subgrid layout for this grid and sets
+ * the current pressure (PFGPU_PFB_PRESSURE) or a cell field
+ * (PFGPU_FIELD_*, as pfgpu_set_field): each subgrid's raw values are copied
+ * to the device once and scattered and byte-swapped there.  A file for
+ * another grid size, or a subgrid outside the grid, is an argument error. */
+#define PFGPU_PFB_PRESSURE 100
+#define PFGPU_PFB_SATURATION 101
+int pfgpu_write_pfb(pfgpu_handle *h, int what, const char *path, double x0, double y0,
+                    double z0);
+int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path);
+
 /* Surface data of the top layer (ProblemData TSlopeX / TSlopeY / Mannings,
  * problem_toposlopes.c, problem_mannings.c): host arrays in ParFlow's 2-D
  * subvector layout, element (i,j) at (i+1) + (j+1)*(nx+2), ghosts ignored.

@@ -1268,6 +1268,136 @@ int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
   return PFGPU_OK;
 }
 
+// ---------------------------------------------------------------------------
+// PFB files (write_parflow_binary.c:74-205, read_parflow_binary.c:38-120)
+// ---------------------------------------------------------------------------
+namespace {
+void put_be64(FILE *f, double v) {
+  unsigned long long u;
+  memcpy(&u, &v, 8);
+  unsigned char b[8];
+  for (int q = 0; q < 8; q++) b[q] = (unsigned char)(u >> (56 - 8 * q));
+  fwrite(b, 1, 8, f);
+}
+void put_be32(FILE *f, int v) {
+  const unsigned u = (unsigned)v;
+  unsigned char b[4] = {(unsigned char)(u >> 24), (unsigned char)(u >> 16),
+                        (unsigned char)(u >> 8), (unsigned char)u};
+  fwrite(b, 1, 4, f);
+}
+bool get_be64(FILE *f, double *v) {
+  unsigned char b[8];
+  if (fread(b, 1, 8, f) != 8) return false;
+  unsigned long long u = 0;
+  for (int q = 0; q < 8; q++) u = (u << 8) | b[q];
+  memcpy(v, &u, 8);
+  return true;
+}
+bool get_be32(FILE *f, int *v) {
+  unsigned char b[4];
+  if (fread(b, 1, 4, f) != 4) return false;
+  *v = (int)(((unsigned)b[0] << 24) | ((unsigned)b[1] << 16) | ((unsigned)b[2] << 8) | b[3]);
+  return true;
+}
+}  // namespace
+
+int pfgpu_write_pfb(pfgpu_handle *h, int what, const char *path, double x0, double y0,
+                    double z0) {
+  if (!h || !path) { set_err("pfgpu_write_pfb: null argument"); return PFGPU_ERR_ARG; }
+  if (what != PFGPU_PFB_PRESSURE && what != PFGPU_PFB_SATURATION) {
+    set_err("pfgpu_write_pfb: unknown field %d", what);
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  const double *src = h->u;
+  if (what == PFGPU_PFB_SATURATION) {
+    launch_saturation(h->P, h->u, h->vtemp, h->st);
+    src = h->vtemp;
+    h->launches++;
+  }
+  // big-endian values in the staging buffer (NP >= N doubles), one copy out
+  unsigned long long *raw = reinterpret_cast<unsigned long long *>(h->stage);
+  launch_pfb_pack(src, raw, h->N, h->st);
+  h->launches++;
+  std::vector<unsigned long long> host((size_t)h->N);
+  CK(cudaMemcpyAsync(host.data(), raw, h->N * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  FILE *f = fopen(path, "wb");
+  if (!f) { set_err("pfgpu_write_pfb: cannot open %s", path); return PFGPU_ERR_ARG; }
+  put_be64(f, x0); put_be64(f, y0); put_be64(f, z0);
+  put_be32(f, h->nx); put_be32(f, h->ny); put_be32(f, h->nz);
+  put_be64(f, h->d.dx); put_be64(f, h->d.dy); put_be64(f, h->d.dz);
+  put_be32(f, 1);
+  const int box[9] = {0, 0, 0, h->nx, h->ny, h->nz, 0, 0, 0};
+  for (int v : box) put_be32(f, v);
+  const size_t w = fwrite(host.data(), sizeof(double), host.size(), f);
+  const bool ok = fclose(f) == 0 && w == host.size();
+  if (!ok) { set_err("pfgpu_write_pfb: short write to %s", path); return PFGPU_ERR_ARG; }
+  return PFGPU_OK;
+}
+
+int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path) {
+  if (!h || !path) { set_err("pfgpu_read_pfb: null argument"); return PFGPU_ERR_ARG; }
+  if (what != PFGPU_PFB_PRESSURE && (what < PFGPU_FIELD_PERM_X || what > PFGPU_FIELD_S_SAT)) {
+    set_err("pfgpu_read_pfb: unknown field %d", what);
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  FILE *f = fopen(path, "rb");
+  if (!f) { set_err("pfgpu_read_pfb: cannot open %s", path); return PFGPU_ERR_ARG; }
+  double hdr_d[6];
+  int nx = 0, ny = 0, nz = 0, nsg = 0;
+  bool ok = get_be64(f, hdr_d) && get_be64(f, hdr_d + 1) && get_be64(f, hdr_d + 2) &&
+            get_be32(f, &nx) && get_be32(f, &ny) && get_be32(f, &nz) &&
+            get_be64(f, hdr_d + 3) && get_be64(f, hdr_d + 4) && get_be64(f, hdr_d + 5) &&
+            get_be32(f, &nsg);
+  if (!ok || nx != h->nx || ny != h->ny || nz != h->nz || nsg < 1) {
+    fclose(f);
+    set_err("pfgpu_read_pfb: %s is not a PFB file of a %dx%dx%d grid", path, h->nx, h->ny,
+            h->nz);
+    return PFGPU_ERR_ARG;
+  }
+  // dense field assembled in vtemp (free outside a solve); raw bytes staged
+  // in the staging buffer (NP >= N doubles) one subgrid at a time
+  CK(cudaMemsetAsync(h->vtemp, 0, h->N * sizeof(double), h->st));
+  unsigned long long *raw = reinterpret_cast<unsigned long long *>(h->stage);
+  std::vector<unsigned long long> host;
+  for (int g = 0; g < nsg; g++) {
+    int box[9];
+    for (int q = 0; q < 9 && ok; q++) ok = get_be32(f, box + q);
+    const int ix = box[0], iy = box[1], iz = box[2], snx = box[3], sny = box[4], snz = box[5];
+    if (!ok || ix < 0 || iy < 0 || iz < 0 || snx < 0 || sny < 0 || snz < 0 ||
+        ix + snx > nx || iy + sny > ny || iz + snz > nz) {
+      fclose(f);
+      set_err("pfgpu_read_pfb: subgrid %d of %s lies outside the grid", g, path);
+      return PFGPU_ERR_ARG;
+    }
+    const size_t cnt = (size_t)snx * sny * snz;
+    if (cnt == 0) continue;
+    CK(cudaStreamSynchronize(h->st));  // the staging buffer is free again
+    host.resize(cnt);
+    if (fread(host.data(), sizeof(double), cnt, f) != cnt) {
+      fclose(f);
+      set_err("pfgpu_read_pfb: %s ends inside subgrid %d", path, g);
+      return PFGPU_ERR_ARG;
+    }
+    CK(cudaMemcpyAsync(raw, host.data(), cnt * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    launch_pfb_scatter(raw, h->vtemp, nx, ny, ix, iy, iz, snx, sny, snz, h->st);
+    h->launches++;
+  }
+  fclose(f);
+  if (what == PFGPU_PFB_PRESSURE) {
+    CK(cudaMemcpyAsync(h->u, h->vtemp, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    if (h->vg_for == h->u) h->vg_for = nullptr;
+    CK(cudaStreamSynchronize(h->st));
+    return PFGPU_OK;
+  }
+  // a cell field: through pfgpu_set_field in ParFlow layout (device pointer)
+  launch_pad(h->vtemp, h->stage, h->nx, h->ny, h->nz, h->st);
+  h->launches++;
+  return pfgpu_set_field(h, what, h->stage);
+}
+
 int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
                       const double *mannings, int terrain_following, double ov_epsilon) {
   if (!h || !slope_x || !slope_y || !mannings || !(ov_epsilon > 0)) {

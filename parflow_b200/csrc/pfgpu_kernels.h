@@ -211,6 +211,14 @@ template <typename TI, typename TO>
 void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int flip = 0,
                     const float *scale = nullptr);
 
+// ---- PFB values (pfb_kernels.cu) --------------------------------------------
+// out = big-endian bytes of dense[0..n)
+void launch_pfb_pack(const double *dense, unsigned long long *out, long long n, cudaStream_t st);
+// raw big-endian values of the subgrid box (ix..ix+snx) x (iy..) x (iz..) into
+// the dense nx x ny x nz field
+void launch_pfb_scatter(const unsigned long long *raw, double *dense, int nx, int ny, int ix,
+                        int iy, int iz, int snx, int sny, int snz, cudaStream_t st);
+
 // ---- vectors and reductions (krylov_kernels.cu) ----------------------------
 struct ReduceBuf {
   double *partial;        // >= reduce_blocks() doubles

@@ -19,6 +19,7 @@ tensors already in the ghost-framed layout (passed by device pointer, no copy).
 from __future__ import annotations
 
 import ctypes as C
+import os
 from typing import Optional
 
 import numpy as np
@@ -124,6 +125,23 @@ class RichardsGPU:
                     continue
                 L.check(self.lib.pfgpu_set_field(self.h, fid, _ptr(pad(a))), "set_field vg")
                 self._vg_cells.add(fid)
+
+    # ---- PFB files of the device state ------------------------------------------
+    _PFB = {"pressure": L.PFB_PRESSURE, "saturation": L.PFB_SATURATION,
+            "perm_x": L.FIELD_PERM_X, "perm_y": L.FIELD_PERM_Y, "perm_z": L.FIELD_PERM_Z,
+            "vg_alpha": L.FIELD_VG_ALPHA, "vg_n": L.FIELD_VG_N, "s_res": L.FIELD_S_RES,
+            "s_sat": L.FIELD_S_SAT}
+
+    def write_pfb(self, path: str, what: str = "pressure", origin=(0.0, 0.0, 0.0)):
+        """WritePFBinary of the device pressure or of the saturation at it."""
+        L.check(self.lib.pfgpu_write_pfb(self.h, self._PFB[what], os.fsencode(path),
+                                         *[float(v) for v in origin]), "write_pfb")
+
+    def read_pfb(self, path: str, what: str = "pressure"):
+        """ReadPFBinary into the device pressure or a cell field."""
+        L.check(self.lib.pfgpu_read_pfb(self.h, self._PFB[what], os.fsencode(path)), "read_pfb")
+        if what in ("vg_alpha", "vg_n", "s_res", "s_sat"):
+            self._vg_cells.add(self._PFB[what])
 
     def update_fields(self):
         """Re-upload the problem's cell fields (permeability, van Genuchten,
