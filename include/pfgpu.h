@@ -140,6 +140,37 @@ const char *pfgpu_last_error(void);
  * descriptor's scalar serves every cell again; permeability needs values. */
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
 
+/* Time-cycled boundary data (TimeCycleData, time_cycle_data.c, and the
+ * per-interval patch values BCPressure keeps): face `face` takes, during
+ * interval q of its cycle, type types[q] and the face table
+ * values + q * (face cells) (the layout of pfgpu_set_bc).  Interval q lasts
+ * lengths[q] base time units; the cycle repeats `repeat` times (-1: for
+ * ever), counted from start_time (ProblemBaseTimeUnit / ProblemStartTime).
+ * Every table is uploaded once; pfgpu_run selects the interval of each step
+ * on the device side.  pfgpu_set_bc on the face replaces the cycle. */
+int pfgpu_set_bc_cycle(pfgpu_handle *h, int face, int nint, const int *types,
+                       const double *values, const int *lengths, int repeat, double base_unit,
+                       double start_time);
+
+/* Time step selection (SelectTimeStep, select_time_step.c:58-155): type 0
+ * constant `step`; type 1 growth: `step` on the first step, then the last
+ * step times `factor`, clamped to [min_step, max_step]; either is then cut to
+ * the next boundary-cycle transition.  max_failures: convergence failures
+ * (each halves dt) before a step is given up (Solver.MaxConvergenceFailures). */
+int pfgpu_set_time_step(pfgpu_handle *h, int type, double step, double factor,
+                        double min_step, double max_step, int max_failures);
+
+/* AdvanceRichards's time loop on the device state (solver_richards.c:
+ * 2965-3406): from time t until stop_time (at most max_steps steps) select
+ * dt, snap it to the next dump time (dump_interval > 0) and cut it to the
+ * stop time, copy the old pressure and saturation on the device, evaluate the
+ * boundary cycles at the new time, solve, and on failure halve dt and retry
+ * from the old state.  times / dts / stats (each max_steps long, may be
+ * null) receive the new time, dt and counters of every step; *nsteps the
+ * number of steps taken.  No counterpart as one call in the reference. */
+int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval, int max_steps,
+              double *times, double *dts, pfgpu_stats *stats, int *nsteps);
+
 /* ParFlow binary (PFB) files of the device state.  The format
  * (write_parflow_binary.c:74-205, read_parflow_binary.c:38-120): big-endian
  * origin x y z and spacings, nx ny nz, the number of subgrids, then per

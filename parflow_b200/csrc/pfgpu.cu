@@ -172,6 +172,18 @@ struct pfgpu_handle {
   // optional per-phase device timing (PFGPU_PHASE_TIMES=1): events recorded
   // around each phase on the solver stream, summed after every Newton solve
   // and printed to stderr when the handle is destroyed
+  // time-cycled boundary tables (pfgpu_set_bc_cycle) and the time step
+  // selection of the native time loop (pfgpu_set_time_step, pfgpu_run)
+  struct BcCycle {
+    int nint = 0, repeat = -1, cycle_len = 0;
+    std::vector<int> lengths, types;
+    double *table = nullptr;  // device: nint face tables
+    long long face_cells = 0;
+    double base_unit = 1.0, start_time = 0.0;
+  } cyc[6];
+  int ts_type = 0;  // 0 constant, 1 growth (select_time_step.c:42-51)
+  double ts_step = 0.0, ts_factor = 1.0, ts_min = 0.0, ts_max = 0.0, ts_dt = 0.0;
+  int max_failures = 3;
   bool ptime = false;
   std::vector<cudaEvent_t> pev;                  // event pool
   std::vector<std::array<int, 3>> pmark;        // (phase, start event, end event)
@@ -1135,6 +1147,7 @@ static void destroy_impl(pfgpu_handle *h) {
   if (h->ky && h->ky != h->kx) cudaFree(h->ky);
   if (h->kz && h->kz != h->kx && h->kz != h->ky) cudaFree(h->kz);
   for (int f = 0; f < 6; f++) cudaFree(h->bcv[f]);
+  for (int f = 0; f < 6; f++) cudaFree(h->cyc[f].table);
   for (auto v : h->V) cudaFree(v);
   cudaFree(h->rb.ticket);
   cudaFree(h->kerr);
@@ -1456,6 +1469,222 @@ int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values) {
                                                                : (long long)h->ny * h->nx;
   CK(cudaMemcpyAsync(h->bcv[face], values, fs * sizeof(double), cudaMemcpyDefault, h->st));
   h->P.bc_type[face] = type;
+  h->P.bc_val[face] = h->bcv[face];
+  h->cyc[face].nint = 0;  // a fixed table replaces a time cycle
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Time cycles, time step selection and the native time loop
+// ---------------------------------------------------------------------------
+namespace {
+const int kTimeCycleSubdivisions = 1000;   // time_cycle_data.c:190
+const double kTimeEpsilon = FLT_EPSILON * 10.0;  // general.h:257
+int pf_round(double x) { return x < 0.0 ? (int)(x - 0.5) : (int)(x + 0.5); }  // general.h:176
+
+// interval of the cycle at time t (TimeCycleDataComputeIntervalNumber,
+// time_cycle_data.c:160-199)
+int cycle_interval(const pfgpu_handle::BcCycle &c, double t) {
+  if (c.repeat < 0 || t < (double)(c.repeat * c.cycle_len * c.base_unit)) {
+    const int dtime = pf_round(t / (c.base_unit / kTimeCycleSubdivisions)) / kTimeCycleSubdivisions;
+    const int dstart =
+        pf_round(c.start_time / (c.base_unit / kTimeCycleSubdivisions)) / kTimeCycleSubdivisions;
+    const int done = (dtime - dstart - 1) % c.cycle_len;
+    int n = 0, total = c.lengths[0];
+    while (done >= total && n + 1 < c.nint) total += c.lengths[++n];
+    return n;
+  }
+  return c.nint - 1;
+}
+
+// time to the next interval transition of any cycle, or -1
+// (TimeCycleDataComputeNextTransition, time_cycle_data.c:206-297)
+double next_transition(const pfgpu_handle *h, double t) {
+  double dt = -1.0;
+  bool assigned = false;
+  for (int f = 0; f < 6; f++) {
+    const auto &c = h->cyc[f];
+    if (c.nint <= 1) continue;
+    const double stop_defined =
+        c.repeat > 0 ? (double)(c.repeat * c.cycle_len * c.base_unit) : 1e300;
+    if (!(t < stop_defined)) continue;
+    const int dtime = pf_round(t / (c.base_unit / kTimeCycleSubdivisions)) / kTimeCycleSubdivisions;
+    const int dstart =
+        pf_round(c.start_time / (c.base_unit / kTimeCycleSubdivisions)) / kTimeCycleSubdivisions;
+    int n = (dtime - dstart) / c.cycle_len;
+    const int done = (dtime - dstart - 1) % c.cycle_len;
+    int q = 0, total = c.lengths[0];
+    while (done >= total && q + 1 < c.nint) total += c.lengths[++q];
+    double tt;
+    if ((q + 1) % c.nint == 0) {
+      n++;
+      tt = c.start_time + (double)(n * c.cycle_len) * c.base_unit;
+    } else {
+      tt = c.start_time + (double)(n * c.cycle_len + total) * c.base_unit;
+    }
+    if (tt < stop_defined) {
+      dt = assigned ? std::min(dt, tt - t) : tt - t;
+      assigned = true;
+    }
+  }
+  if (assigned && !((t + dt) - t > kTimeEpsilon)) dt = -1.0;
+  return dt;
+}
+}  // namespace
+
+int pfgpu_set_bc_cycle(pfgpu_handle *h, int face, int nint, const int *types,
+                       const double *values, const int *lengths, int repeat, double base_unit,
+                       double start_time) {
+  if (!h || face < 0 || face > 5 || nint < 1 || !types || !values || !lengths ||
+      !(base_unit > 0)) {
+    set_err("pfgpu_set_bc_cycle: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  int len = 0;
+  for (int q = 0; q < nint; q++) {
+    const int t = types[q];
+    if ((t != PFGPU_BC_FLUX && t != PFGPU_BC_DIRICHLET && t != PFGPU_BC_OVERLAND_KIN) ||
+        lengths[q] < 1 ||
+        (t == PFGPU_BC_OVERLAND_KIN && (face != PFGPU_Z_UPPER || !h->P.ov_sx))) {
+      set_err("pfgpu_set_bc_cycle: bad type or length in interval %d", q);
+      return PFGPU_ERR_ARG;
+    }
+    len += lengths[q];
+  }
+  CK(cudaSetDevice(h->device));
+  auto &c = h->cyc[face];
+  c.face_cells = face < 2 ? (long long)h->nz * h->ny : face < 4 ? (long long)h->nz * h->nx
+                                                                : (long long)h->ny * h->nx;
+  cudaFree(c.table);
+  c.table = nullptr;
+  if (dalloc(&c.table, c.face_cells * nint)) return PFGPU_ERR_NOMEM;
+  CK(cudaMemcpyAsync(c.table, values, c.face_cells * nint * sizeof(double), cudaMemcpyDefault,
+                     h->st));
+  c.nint = nint;
+  c.repeat = repeat;
+  c.cycle_len = len;
+  c.lengths.assign(lengths, lengths + nint);
+  c.types.assign(types, types + nint);
+  c.base_unit = base_unit;
+  c.start_time = start_time;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_set_time_step(pfgpu_handle *h, int type, double step, double factor,
+                        double min_step, double max_step, int max_failures) {
+  if (!h || (type != 0 && type != 1) || !(step > 0) || max_failures < 1 ||
+      (type == 1 && !(factor > 0 && min_step > 0 && max_step >= min_step))) {
+    set_err("pfgpu_set_time_step: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  h->ts_type = type;
+  h->ts_step = step;
+  h->ts_factor = factor;
+  h->ts_min = min_step;
+  h->ts_max = max_step;
+  h->ts_dt = 0.0;
+  h->max_failures = max_failures;
+  return PFGPU_OK;
+}
+
+// point every cycled face at its interval's table for time t
+static void bc_cycles_at(pfgpu_handle *h, double t) {
+  for (int f = 0; f < 6; f++) {
+    const auto &c = h->cyc[f];
+    if (c.nint < 1) continue;
+    const int q = cycle_interval(c, t);
+    h->P.bc_type[f] = c.types[q];
+    h->P.bc_val[f] = c.table + q * c.face_cells;
+  }
+}
+
+// SelectTimeStep (select_time_step.c:58-155): the step rule, then the next
+// boundary-cycle transition
+static double select_time_step(pfgpu_handle *h, double t) {
+  double dt;
+  if (h->ts_type == 0) {
+    dt = h->ts_step;
+  } else if (h->ts_dt == 0.0) {
+    dt = h->ts_step;
+  } else {
+    dt = h->ts_dt * h->ts_factor;
+    if (dt < h->ts_min) dt = h->ts_min;
+    if (dt > h->ts_max) dt = h->ts_max;
+  }
+  const double bc_dt = next_transition(h, t);
+  if (bc_dt > 0.0 && dt > bc_dt) dt = bc_dt;
+  return dt;
+}
+
+// AdvanceRichards's time loop on the device state (solver_richards.c:2965-3406
+// and the dump/stop adjustments of :3139-3230)
+int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval, int max_steps,
+              double *times, double *dts, pfgpu_stats *stats, int *nsteps) {
+  if (!h || !(stop_time > t) || max_steps < 1 || !nsteps || !(h->ts_step > 0)) {
+    set_err("pfgpu_run: bad argument (set the time step first)");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  const double start = t;
+  double dump_index = 1.0;
+  int n = 0;
+  *nsteps = 0;
+  while (t < stop_time && n < max_steps) {
+    bool converged = true;
+    int failures = 0;
+    double dt = 0.0;
+    pfgpu_stats st{};
+    int rc = PFGPU_NOT_CONVERGED;
+    do {
+      if (converged) {
+        dt = select_time_step(h, t);
+        if (dump_interval > 0) {
+          const double print_dt = start + dump_index * dump_interval - t;
+          if ((dt + kTimeEpsilon) > print_dt) {
+            if (fabs(dt - print_dt) > kTimeEpsilon) dt = print_dt;
+            dump_index += 1.0;
+          }
+        }
+        if (t + dt >= stop_time) dt = stop_time - t;
+        CK(cudaMemcpyAsync(h->p_old, h->u, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->st));
+        launch_saturation(h->P, h->u, h->s_old, h->st);
+        h->launches++;
+      } else {
+        t -= dt;
+        const double half = 0.5 * dt;
+        if (!((t + half) - t > kTimeEpsilon)) {
+          set_err("pfgpu_run: time increment too small at t = %g; the solver has failed", t);
+          *nsteps = n;
+          return PFGPU_NOT_CONVERGED;
+        }
+        dt = half;
+        CK(cudaMemcpyAsync(h->u, h->p_old, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->st));
+        h->vg_for = nullptr;
+      }
+      t += dt;
+      bc_cycles_at(h, t);
+      rc = newton(h, dt, &st);
+      if (rc < 0) { *nsteps = n; return rc; }
+      if (check_kernel_error(h)) { *nsteps = n; return PFGPU_ERR_CUDA; }
+      converged = rc == PFGPU_OK;
+      if (!converged) failures++;
+    } while (!converged && failures < h->max_failures);
+    if (!converged) {
+      set_err("pfgpu_run: time step at t = %g failed %d times", t, failures);
+      *nsteps = n;
+      return PFGPU_NOT_CONVERGED;
+    }
+    h->ts_dt = dt;
+    if (times) times[n] = t;
+    if (dts) dts[n] = dt;
+    if (stats) stats[n] = st;
+    n++;
+  }
+  *nsteps = n;
   CK(cudaStreamSynchronize(h->st));
   return PFGPU_OK;
 }

@@ -60,7 +60,7 @@ EXPORTS = ["pfgpu_create", "pfgpu_destroy", "pfgpu_last_error", "pfgpu_set_field
            "pfgpu_stream", "pfgpu_kernel_launches", "pfgpu_time_kernel",
            "pfgpu_residual_noalloc", "pfgpu_ensemble_advance", "pfgpu_set_surface",
            "pfgpu_adjoint_record", "pfgpu_adjoint_gradient", "pfgpu_write_pfb",
-           "pfgpu_read_pfb"]
+           "pfgpu_read_pfb", "pfgpu_set_bc_cycle", "pfgpu_set_time_step", "pfgpu_run"]
 PFB_PRESSURE, PFB_SATURATION = 100, 101
 KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_smooth": 3, "vcycle": 4, "mg_setup": 5,
            "colour_sweep": 6}
@@ -90,6 +90,14 @@ def load(path: str = LIB_PATH):
                                          C.c_double, C.POINTER(C.c_double), vp, vp, vp]
     L.pfgpu_set_surface.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double]
     L.pfgpu_write_pfb.argtypes = [vp, C.c_int, C.c_char_p, C.c_double, C.c_double, C.c_double]
+    L.pfgpu_set_bc_cycle.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_int), C.c_int,
+                                     C.c_double, C.c_double]
+    L.pfgpu_set_time_step.argtypes = [vp, C.c_int, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_int]
+    L.pfgpu_run.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_int,
+                            C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(Stats),
+                            C.POINTER(C.c_int)]
     L.pfgpu_read_pfb.argtypes = [vp, C.c_int, C.c_char_p]
     L.pfgpu_nl_function_eval.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double,
                                          C.c_void_p]

@@ -245,6 +245,61 @@ class RichardsGPU:
             ps.append(self.get_pressure())
         return ps, sts
 
+    def upload_bc_cycles(self):
+        """Every face's time cycle as device tables (pfgpu_set_bc_cycle): one
+        face table per interval, selected by the native time loop."""
+        p = self.prob
+        base = p.base_unit if p.base_unit is not None else p.dt
+        for f, face in enumerate(FACES):
+            bc = p.bc.get(face)
+            kind = bc.kind if bc is not None else L.BC_FLUX
+            values = tuple(bc.values) if bc is not None else (0.0,)
+            lengths = tuple(bc.lengths) if bc is not None else (1,)
+            repeat = bc.repeat if bc is not None else -1
+            tables = []
+            for v in values:
+                if kind == L.BC_DIRICHLET:
+                    tables.append(p._dir_equil_values(face, float(v), bc.ref_patch))
+                else:
+                    tables.append(np.full(p.face_shape(face), float(v)))
+            vals = np.ascontiguousarray(np.stack(tables), dtype=np.float64)
+            n = len(values)
+            types = (C.c_int * n)(*([kind] * n))
+            lens = (C.c_int * n)(*[int(x) for x in lengths])
+            L.check(self.lib.pfgpu_set_bc_cycle(
+                self.h, f, n, types, vals.ctypes.data_as(C.POINTER(C.c_double)), lens,
+                int(repeat), float(base), float(p.start_time)), f"set_bc_cycle {face}")
+
+    def run_device(self, max_steps: Optional[int] = None, dump_interval: Optional[float] = None,
+                   growth=None):
+        """The problem's time loop as one native call (pfgpu_run): time-cycled
+        boundary tables on the device, SelectTimeStep (constant dt, or
+        growth = (initial, factor, min, max)), dump-time snapping, the dt-halving
+        retry.  Returns (final pressure, times, dts, stats per step)."""
+        p = self.prob
+        self.upload_bc_cycles()
+        fails = int(p.solver.max_convergence_failures)
+        if growth is None:
+            L.check(self.lib.pfgpu_set_time_step(self.h, 0, float(p.dt), 1.0, 0.0, 0.0, fails),
+                    "set_time_step")
+        else:
+            init, factor, lo, hi = (float(v) for v in growth)
+            L.check(self.lib.pfgpu_set_time_step(self.h, 1, init, factor, lo, hi, fails),
+                    "set_time_step")
+        n_max = max_steps if max_steps is not None else 10 * p.nsteps + 10
+        times = (C.c_double * n_max)()
+        dts = (C.c_double * n_max)()
+        stats = (L.Stats * n_max)()
+        n = C.c_int()
+        dump = float(p.dt) if dump_interval is None else float(dump_interval)
+        self.set_pressure(p.initial_pressure())
+        rc = L.check(self.lib.pfgpu_run(self.h, float(p.start_time), float(p.stop_time()), dump,
+                                        n_max, times, dts, stats, C.byref(n)), "run")
+        if rc != L.OK:
+            raise L.PfgpuError("run: " + L.last_error())
+        k = n.value
+        return (self.get_pressure(), list(times[:k]), list(dts[:k]), [stats[i] for i in range(k)])
+
     # ---- discrete adjoint ------------------------------------------------------
     def adjoint_record(self, max_steps: int):
         """Start recording the trajectory at the current pressure."""
