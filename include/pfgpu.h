@@ -240,10 +240,19 @@ int pfgpu_saturation(pfgpu_handle *h, const double *p, double *s);
 /* One implicit step: solves F(p) = 0 by inexact Newton-Krylov with line
  * search, entirely on the GPU (KinsolNonlinSolver -> KINSol,
  * kinsol_nonlin_solver.c:297, pfsimulator/kinsol/kinsol.c:690).
- * p: in = initial guess (normally p_old), out = solution.  Returns
+ * p: in = initial guess (normally p_old), out = solution; p may be the
+ * p_old buffer itself (it is then copied in once).  Returns
  * PFGPU_OK, or PFGPU_NOT_CONVERGED when KINSOL would fail. */
 int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old,
                        double dt, double *p, pfgpu_stats *stats);
+
+/* pfgpu_newton_solve followed by the saturation at the new pressure
+ * (AdvanceRichards evaluates it right after the solve,
+ * solver_richards.c:3408-3420): both results leave the device in one call, so
+ * a host caller copies p in once and p and s out once.  s may be the s_old
+ * buffer and p the p_old buffer (both are read before anything is written). */
+int pfgpu_newton_solve_sat(pfgpu_handle *h, const double *p_old, const double *s_old,
+                           double dt, double *p, double *s, pfgpu_stats *stats);
 
 /* Device-resident time stepping: advances the handle's own pressure state by
  * nsteps steps of dt with the boundary tables already set, keeping every

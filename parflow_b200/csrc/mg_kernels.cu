@@ -107,6 +107,30 @@ __device__ __forceinline__ void split_ijk(int t, int nx, int ny, int &i, int &j,
   j = r % ny;
   k = r / ny;
 }
+// A divisor with its float reciprocal: t / d from one multiplication and a
+// one-step correction (exact while the float product errs by less than one,
+// i.e. for t < 2^22; larger t take the integer division).  The single-block
+// tail splits a linear index per cell and phase, where integer division
+// would dominate its instruction count.
+struct FastDiv {
+  int d;
+  float inv;
+};
+__device__ __forceinline__ FastDiv fast_div(int d) { return FastDiv{d, 1.0f / (float)d}; }
+__device__ __forceinline__ int quot(int t, FastDiv f) {
+  if (t >= (1 << 22)) return t / f.d;
+  int q = (int)((float)t * f.inv);
+  if ((q + 1) * f.d <= t) q++;
+  if (q * f.d > t) q--;
+  return q;
+}
+__device__ __forceinline__ void split_ijk(int t, FastDiv fx, FastDiv fy, int &i, int &j,
+                                          int &k) {
+  const int r = quot(t, fx);
+  i = t - r * fx.d;
+  k = quot(r, fy);
+  j = r - k * fy.d;
+}
 
 // prolongation weights of one fine point (mg_semi.c:534-575): the
 // along-direction entries over the collapsed diagonal
@@ -861,9 +885,10 @@ template <typename T, bool H>
 __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b, int zero,
                                            int smoother, T w, T *tmp) {
   if (smoother == 1) {
+    const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
-      split_ijk(t, L.nx, L.ny, i, j, k);
+      split_ijk(t, fx, fy, i, j, k);
       wjacobi_cell<T, H>(L, x, b, tmp, zero, i, j, k);
     }
     __syncthreads();
@@ -874,12 +899,13 @@ __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b
   }
   const int hx = (L.nx + 1) / 2;
   const int half = hx * L.ny * L.nz;
+  const FastDiv fx = fast_div(hx), fy = fast_div(L.ny);
   for (int sweep = 0; sweep < 3; sweep++) {
     const int colour = sweep == 1 ? 1 : 0;
     const int init = (sweep == 0) ? zero : 0;
     for (int t = threadIdx.x; t < half; t += blockDim.x) {
       int q, j, k;
-      split_ijk(t, hx, L.ny, q, j, k);
+      split_ijk(t, fx, fy, q, j, k);
       rb_cell<T, H>(L, x, b, colour, init, q, j, k);
     }
     __syncthreads();
@@ -895,15 +921,17 @@ __device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int 
     const MGLevel<T> L = Ls[l];
     const MGLevel<T> C = Ls[l + 1];
     blk_smooth<T, H>(L, L.x, (const T *)L.b, 1, smoother, w, tmp);
+    const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
-      split_ijk(t, L.nx, L.ny, i, j, k);
+      split_ijk(t, fx, fy, i, j, k);
       mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
     }
     __syncthreads();
+    const FastDiv cx = fast_div(C.nx), cy = fast_div(C.ny);
     for (int t = threadIdx.x; t < (int)C.n; t += blockDim.x) {
       int i, j, k;
-      split_ijk(t, C.nx, C.ny, i, j, k);
+      split_ijk(t, cx, cy, i, j, k);
       restrict_cell<T, H>(L, C, (const T *)L.t, C.b, i, j, k);
     }
     __syncthreads();
@@ -917,9 +945,10 @@ __device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int 
   for (int l = nl - 2; l >= first; l--) {
     const MGLevel<T> L = Ls[l];
     const MGLevel<T> C = Ls[l + 1];
+    const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
     for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
       int i, j, k;
-      split_ijk(t, L.nx, L.ny, i, j, k);
+      split_ijk(t, fx, fy, i, j, k);
       prolong_add_cell<T, H>(L, C, (const T *)C.x, L.x, i, j, k);
     }
     __syncthreads();

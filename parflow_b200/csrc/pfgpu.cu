@@ -1742,17 +1742,49 @@ int pfgpu_pc_apply(pfgpu_handle *h, const double *r, double *z) {
   return out_vec(h, h->vtemp, z);
 }
 
+// the three inputs of a step; an initial guess passed in the same buffer as
+// the old pressure (as at the start of every AdvanceRichards step) is copied
+// in once
+static int load_step_inputs(pfgpu_handle *h, const double *p_old, const double *s_old,
+                            const double *p) {
+  if (in_vec(h, p_old, h->p_old) || in_vec(h, s_old, h->s_old)) return PFGPU_ERR_CUDA;
+  if (p == p_old) {
+    CK(cudaMemcpyAsync(h->u, h->p_old, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    if (h->vg_for == h->u) h->vg_for = nullptr;
+    return 0;
+  }
+  return in_vec(h, p, h->u);
+}
+
 int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old, double dt,
                        double *p, pfgpu_stats *stats) {
   if (!h || !p_old || !s_old || !p) { set_err("pfgpu_newton_solve: null argument"); return PFGPU_ERR_ARG; }
   CK(cudaSetDevice(h->device));
-  if (in_vec(h, p_old, h->p_old) || in_vec(h, s_old, h->s_old) || in_vec(h, p, h->u))
-    return PFGPU_ERR_CUDA;
+  if (load_step_inputs(h, p_old, s_old, p)) return PFGPU_ERR_CUDA;
   pfgpu_stats local;
   int rc = newton(h, dt, stats ? stats : &local);
   if (rc < 0) return rc;
   if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
   int rc2 = out_vec(h, h->u, p);
+  return rc2 ? rc2 : rc;
+}
+
+int pfgpu_newton_solve_sat(pfgpu_handle *h, const double *p_old, const double *s_old,
+                           double dt, double *p, double *s, pfgpu_stats *stats) {
+  if (!h || !p_old || !s_old || !p || !s) {
+    set_err("pfgpu_newton_solve_sat: null argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  if (load_step_inputs(h, p_old, s_old, p)) return PFGPU_ERR_CUDA;
+  pfgpu_stats local;
+  int rc = newton(h, dt, stats ? stats : &local);
+  if (rc < 0) return rc;
+  if (check_kernel_error(h)) return PFGPU_ERR_CUDA;
+  launch_saturation(h->P, h->u, h->fval, h->st);
+  h->launches++;
+  int rc2 = out_vec(h, h->u, p);
+  if (!rc2) rc2 = out_vec(h, h->fval, s);
   return rc2 ? rc2 : rc;
 }
 

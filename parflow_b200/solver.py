@@ -210,6 +210,17 @@ class RichardsGPU:
                                                  C.byref(st)), "newton_solve")
         return unpad(p), rc, st
 
+    def newton_solve_sat(self, p_init, p_old, s_old, dt):
+        """newton_solve and the saturation at the solution in one call:
+        returns (p, s, status)."""
+        p = pad(p_init)
+        sat = np.zeros_like(p)
+        st = L.Stats()
+        rc = L.check(self.lib.pfgpu_newton_solve_sat(self.h, _ptr(self._io(p_old)),
+                                                     _ptr(self._io(s_old)), dt, _ptr(p),
+                                                     _ptr(sat), C.byref(st)), "newton_solve_sat")
+        return unpad(p), unpad(sat), rc
+
     # ---- device-resident stepping ---------------------------------------------
     def set_pressure(self, p):
         L.check(self.lib.pfgpu_set_pressure(self.h, _ptr(self._io(p))), "set_pressure")

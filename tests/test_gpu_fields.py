@@ -71,3 +71,42 @@ def test_uniform_field_different_from_descriptor(solver):
     # per-cell array on one handle, descriptor scalar on the other: the same
     # values through the same arithmetic
     np.testing.assert_allclose(p, ref, rtol=1e-13, atol=0)
+
+
+def test_newton_solve_sat_equals_solve_then_saturation(solver):
+    prob = _problem()
+    p0 = prob.initial_pressure()
+    a = solver.RichardsGPU(prob)
+    s_old = a.saturation(p0)
+    p_a, rc_a, _ = a.newton_solve(p0, p0, s_old, prob.dt)
+    s_a = a.saturation(p_a)
+    a.close()
+    b = solver.RichardsGPU(prob)
+    p_b, s_b, rc_b = b.newton_solve_sat(p0, p0, s_old, prob.dt)
+    b.close()
+    assert rc_a == rc_b == 0
+    assert np.array_equal(p_a, p_b) and np.array_equal(s_a, s_b)
+
+
+def test_newton_solve_sat_aliased_buffers(solver):
+    """p passed in the p_old buffer and s in the s_old buffer (the caller's
+    state at the start of a step): same result as separate buffers."""
+    import ctypes as C
+
+    from parflow_b200 import lib as L
+    from parflow_b200.solver import pad, unpad
+
+    prob = _problem()
+    p0 = prob.initial_pressure()
+    a = solver.RichardsGPU(prob)
+    s0 = a.saturation(p0)
+    p_ref, s_ref, _ = a.newton_solve_sat(p0, p0, s0, prob.dt)
+    a.close()
+    b = solver.RichardsGPU(prob)
+    pb, sb = pad(p0), pad(s0)
+    pp, sp = pb.ctypes.data_as(C.c_void_p), sb.ctypes.data_as(C.c_void_p)
+    st = L.Stats()
+    rc = b.lib.pfgpu_newton_solve_sat(b.h, pp, sp, prob.dt, pp, sp, C.byref(st))
+    b.close()
+    assert rc == 0
+    assert np.array_equal(unpad(pb), p_ref) and np.array_equal(unpad(sb), s_ref)
