@@ -39,10 +39,10 @@ NX, NY, NZ = 512, 512, 50
 # multigrid arithmetic on the symmetrically diagonal-scaled operator stored in
 # FP16 ("mixed16"); the all-FP32 multigrid ("mixed") is timed beside it.
 HEADLINE = "mixed16"
-# DRAM bytes (read + write) per cell of one k_rb_sweep launch of the headline
+# DRAM bytes (read + write) per cell of one k_rb_sweep2 launch of the headline
 # form, from the ncu capture summarised in
-# profiles/k_rb_sweep_hetero_384x384x50_mixed16.md
-RB_SWEEP_DRAM_BYTES_PER_CELL = 15.27
+# profiles/k_rb_sweep2_hetero_384x384x50_mixed16.md
+RB_SWEEP_DRAM_BYTES_PER_CELL = 10.51
 
 
 def peaks():
@@ -407,8 +407,8 @@ def gpu_arm(args, rank, world, local_rank):
             "gmres_iters_per_step": sum(x.lin_iters for x in stmx) / max(1, len(stmx)),
             "cell_newton_updates_per_s": cells * newton * world / (msmx * 1e-3),
             "roofline": {"bound": "hbm",
-                         "kernel": "k_rb_sweep: one red/black colour sweep, finest level "
-                                   "(scaled f16 operator, f32 b and x)",
+                         "kernel": "k_rb_sweep2: one red/black colour sweep, finest level "
+                                   "(scaled f16 operator, colour-split f32 b and x)",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_source": peak_kind,
