@@ -879,22 +879,51 @@ __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
 // cells, so launching a grid per smoothing sweep costs more than the sweep.
 // The block walks the same sequence of phases as the per-level kernels
 // (smooth, residual, restrict, ..., coarse solve, prolong + correct, smooth),
-// separated by __syncthreads(); the arithmetic per cell is identical.
+// separated by barriers; the arithmetic per cell is identical.
+//
+// A team is the set of threads that walks those phases together:
+// BlockTeam is one thread block (barrier __syncthreads); ClusterTeam is every
+// block of a thread-block cluster (barrier.cluster with release / acquire
+// semantics, which orders one phase's global-memory writes before the next
+// phase's reads on every SM of the cluster).
 // ---------------------------------------------------------------------------
-template <typename T, bool H>
-__device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b, int zero,
-                                           int smoother, T w, T *tmp) {
+__device__ __forceinline__ int cluster_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return (int)r;
+}
+__device__ __forceinline__ int cluster_blocks() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return (int)r;
+}
+struct BlockTeam {
+  __device__ static int rank() { return threadIdx.x; }
+  __device__ static int size() { return blockDim.x; }
+  __device__ static void sync() { __syncthreads(); }
+};
+struct ClusterTeam {
+  __device__ static int rank() { return cluster_rank() * blockDim.x + threadIdx.x; }
+  __device__ static int size() { return cluster_blocks() * blockDim.x; }
+  __device__ static void sync() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+  }
+};
+
+template <typename T, bool H, class Team>
+__device__ __forceinline__ void team_smooth(const MGLevel<T> &L, T *x, const T *b, int zero,
+                                            int smoother, T w, T *tmp) {
+  const int r0 = Team::rank(), rs = Team::size();
   if (smoother == 1) {
     const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
-    for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
+    for (int t = r0; t < (int)L.n; t += rs) {
       int i, j, k;
       split_ijk(t, fx, fy, i, j, k);
       wjacobi_cell<T, H>(L, x, b, tmp, zero, i, j, k);
     }
-    __syncthreads();
-    for (long long c = threadIdx.x; c < L.n; c += blockDim.x)
-      wjacobi_update_cell(x, (const T *)tmp, L.n, w, zero, c);
-    __syncthreads();
+    Team::sync();
+    for (long long c = r0; c < L.n; c += rs) wjacobi_update_cell(x, (const T *)tmp, L.n, w, zero, c);
+    Team::sync();
     return;
   }
   const int hx = (L.nx + 1) / 2;
@@ -903,56 +932,70 @@ __device__ __forceinline__ void blk_smooth(const MGLevel<T> &L, T *x, const T *b
   for (int sweep = 0; sweep < 3; sweep++) {
     const int colour = sweep == 1 ? 1 : 0;
     const int init = (sweep == 0) ? zero : 0;
-    for (int t = threadIdx.x; t < half; t += blockDim.x) {
+    for (int t = r0; t < half; t += rs) {
       int q, j, k;
       split_ijk(t, fx, fy, q, j, k);
       rb_cell<T, H>(L, x, b, colour, init, q, j, k);
     }
-    __syncthreads();
+    Team::sync();
   }
 }
 
+// down-leg of one level: pre-smooth (zero guess), residual, restriction to C
+template <typename T, bool H, class Team>
+__device__ __forceinline__ void team_down(const MGLevel<T> &L, const MGLevel<T> &C,
+                                          int smoother, T w, T *tmp) {
+  const int r0 = Team::rank(), rs = Team::size();
+  team_smooth<T, H, Team>(L, L.x, (const T *)L.b, 1, smoother, w, tmp);
+  const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
+  for (int t = r0; t < (int)L.n; t += rs) {
+    int i, j, k;
+    split_ijk(t, fx, fy, i, j, k);
+    mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
+  }
+  Team::sync();
+  const FastDiv cx = fast_div(C.nx), cy = fast_div(C.ny);
+  for (int t = r0; t < (int)C.n; t += rs) {
+    int i, j, k;
+    split_ijk(t, cx, cy, i, j, k);
+    restrict_cell<T, H>(L, C, (const T *)L.t, C.b, i, j, k);
+  }
+  Team::sync();
+}
+
+// up-leg of one level: prolong C's correction and add it, post-smooth
+template <typename T, bool H, class Team>
+__device__ __forceinline__ void team_up(const MGLevel<T> &L, const MGLevel<T> &C, int smoother,
+                                        T w, T *tmp) {
+  const int r0 = Team::rank(), rs = Team::size();
+  const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
+  for (int t = r0; t < (int)L.n; t += rs) {
+    int i, j, k;
+    split_ijk(t, fx, fy, i, j, k);
+    prolong_add_cell<T, H>(L, C, (const T *)C.x, L.x, i, j, k);
+  }
+  Team::sync();
+  team_smooth<T, H, Team>(L, L.x, (const T *)L.b, 0, smoother, w, tmp);
+}
+
 // the tail cycle over levels first .. nl-1 of the table Ls (global or shared)
-template <typename T, bool H>
+template <typename T, bool H, class Team = BlockTeam>
 __device__ __forceinline__ void tail_cycle(const MGLevel<T> *Ls, int first, int nl,
                                            int smoother, T w, T *tmp) {
   // down: levels first .. nl-2
   for (int l = first; l <= nl - 2; l++) {
-    const MGLevel<T> L = Ls[l];
-    const MGLevel<T> C = Ls[l + 1];
-    blk_smooth<T, H>(L, L.x, (const T *)L.b, 1, smoother, w, tmp);
-    const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
-    for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
-      int i, j, k;
-      split_ijk(t, fx, fy, i, j, k);
-      mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
-    }
-    __syncthreads();
-    const FastDiv cx = fast_div(C.nx), cy = fast_div(C.ny);
-    for (int t = threadIdx.x; t < (int)C.n; t += blockDim.x) {
-      int i, j, k;
-      split_ijk(t, cx, cy, i, j, k);
-      restrict_cell<T, H>(L, C, (const T *)L.t, C.b, i, j, k);
-    }
-    __syncthreads();
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_down<T, H, Team>(L, C, smoother, w, tmp);
   }
   // coarse solve: red/black Gauss-Seidel
   {
     const MGLevel<T> L = Ls[nl - 1];
-    blk_smooth<T, H>(L, L.x, (const T *)L.b, 1, 0, T(1), tmp);
+    team_smooth<T, H, Team>(L, L.x, (const T *)L.b, 1, 0, T(1), tmp);
   }
   // up: levels nl-2 .. first
   for (int l = nl - 2; l >= first; l--) {
-    const MGLevel<T> L = Ls[l];
-    const MGLevel<T> C = Ls[l + 1];
-    const FastDiv fx = fast_div(L.nx), fy = fast_div(L.ny);
-    for (int t = threadIdx.x; t < (int)L.n; t += blockDim.x) {
-      int i, j, k;
-      split_ijk(t, fx, fy, i, j, k);
-      prolong_add_cell<T, H>(L, C, (const T *)C.x, L.x, i, j, k);
-    }
-    __syncthreads();
-    blk_smooth<T, H>(L, L.x, (const T *)L.b, 0, smoother, w, tmp);
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_up<T, H, Team>(L, C, smoother, w, tmp);
   }
 }
 
@@ -983,13 +1026,12 @@ struct TailSeg {
 __host__ __device__ inline long long pad16(long long bytes) { return (bytes + 15) / 16 * 16; }
 
 template <typename T, bool H>
-__global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
-    const MGLevel<T> *__restrict__ Ls, int first, int nl, int smoother, T w) {
+__device__ __forceinline__ void tail_smem_cycle(const MGLevel<T> *__restrict__ Ls, int first,
+                                                int nl, int smoother, T w) {
   extern __shared__ __align__(16) unsigned char tail_raw[];
   __shared__ MGLevel<T> S[TAIL_MAX_LEVELS];
   __shared__ TailSeg seg[7 * TAIL_MAX_LEVELS + 1];
   __shared__ int nseg;
-  pdl_enter();
   const int nt = nl - first;
   if ((int)threadIdx.x < nt) S[threadIdx.x] = Ls[first + threadIdx.x];
   __syncthreads();
@@ -1059,6 +1101,43 @@ __global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
   tail_cycle<T, H>(S, 0, nt, smoother, w, S[0].t);
   T *xo = Ls[first].x;
   for (int c = threadIdx.x; c < (int)S[0].n; c += blockDim.x) xo[c] = S[0].x[c];
+}
+
+template <typename T, bool H>
+__global__ void __launch_bounds__(TAIL_THREADS) k_vcycle_tail_smem(
+    const MGLevel<T> *__restrict__ Ls, int first, int nl, int smoother, T w) {
+  pdl_enter();
+  tail_smem_cycle<T, H>(Ls, first, nl, smoother, w);
+}
+
+// Middle levels on one thread-block cluster: levels mid .. tail-1 hold tens
+// of thousands of cells, too few to fill the GPU but enough that one block
+// is slow on them.  The cluster's blocks walk their phases together in one
+// launch (barrier.cluster between phases, data in global memory / L2), and
+// block 0 alone runs the tail levels tail .. nl-1 in between, in shared
+// memory when tail_in_smem (as k_vcycle_tail_smem) or from global memory
+// (as k_vcycle_tail).  Same phases and per-cell arithmetic as the grid
+// kernels, so the V-cycle's result does not depend on where the levels run.
+template <typename T, bool H>
+__global__ void __launch_bounds__(TAIL_THREADS, 1) k_vcycle_mid(
+    const MGLevel<T> *__restrict__ Ls, int mid, int tail, int nl, int smoother, T w, T *tmp,
+    int tail_in_smem) {
+  pdl_enter();
+  for (int l = mid; l < tail; l++) {
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_down<T, H, ClusterTeam>(L, C, smoother, w, tmp);
+  }
+  if (cluster_rank() == 0) {
+    if (tail_in_smem)
+      tail_smem_cycle<T, H>(Ls, tail, nl, smoother, w);
+    else
+      tail_cycle<T, H, BlockTeam>(Ls, tail, nl, smoother, w, tmp);
+  }
+  ClusterTeam::sync();
+  for (int l = tail - 1; l >= mid; l--) {
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_up<T, H, ClusterTeam>(L, C, smoother, w, tmp);
+  }
 }
 
 template <typename T>
@@ -1258,9 +1337,17 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
   rb_sweep(L, x, b, 0, 0, st, f, h16);
   if (flip) *flip = g;
 }
-// opt the fused smoother and the shared-memory tails into their dynamic
-// shared memory (> 48 KB); called once per device before any launch or
-// graph capture
+template <typename K>
+static cudaError_t mid_prepare(K kern) {
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)TAIL_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
+// opt the fused smoother, the shared-memory tails and the cluster kernel into
+// their dynamic shared memory (> 48 KB) and cluster sizes above 8; called once
+// per device before any launch or graph capture
 cudaError_t mg_prepare_kernels() {
   cudaError_t e = rbr_fused_prepare<float>();
   if (e != cudaSuccess) return e;
@@ -1272,8 +1359,34 @@ cudaError_t mg_prepare_kernels() {
   e = cudaFuncSetAttribute(k_vcycle_tail_smem<float, true>,
                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
   if (e != cudaSuccess) return e;
-  return cudaFuncSetAttribute(k_vcycle_tail_smem<double, false>,
-                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
+  e = cudaFuncSetAttribute(k_vcycle_tail_smem<double, false>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TAIL_SMEM_MAX);
+  if (e != cudaSuccess) return e;
+  e = mid_prepare(k_vcycle_mid<float, false>);
+  if (e != cudaSuccess) return e;
+  e = mid_prepare(k_vcycle_mid<float, true>);
+  if (e != cudaSuccess) return e;
+  return mid_prepare(k_vcycle_mid<double, false>);
+}
+
+template <typename T>
+int vcycle_mid_cluster_size(bool h16, size_t smem) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(16);
+  cfg.blockDim = dim3(TAIL_THREADS);
+  cfg.dynamicSmemBytes = smem;
+  int cs = 0;
+  cudaError_t e;
+  if constexpr (kHasH16<T>)
+    e = h16 ? cudaOccupancyMaxPotentialClusterSize(&cs, k_vcycle_mid<T, true>, &cfg)
+            : cudaOccupancyMaxPotentialClusterSize(&cs, k_vcycle_mid<T, false>, &cfg);
+  else
+    e = cudaOccupancyMaxPotentialClusterSize(&cs, k_vcycle_mid<T, false>, &cfg);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return cs;
 }
 
 template <typename T>
@@ -1352,6 +1465,20 @@ void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smo
   else
     launch_pdl(k_vcycle_tail<T, false>, dim3(1), dim3(512), st, levels_dev, first, nl, smoother,
                (T)weight, tmp);
+}
+template <typename T>
+void launch_vcycle_mid(const MGLevel<T> *levels_dev, int mid, int tail, int nl, int smoother,
+                       double weight, T *tmp, size_t smem, int cs, cudaStream_t st, bool h16) {
+  const int in_smem = smem > 0 ? 1 : 0;
+  if constexpr (kHasH16<T>) {
+    if (h16) {
+      launch_pdl_cluster(k_vcycle_mid<T, true>, cs, dim3(TAIL_THREADS), smem, st, levels_dev,
+                         mid, tail, nl, smoother, (T)weight, tmp, in_smem);
+      return;
+    }
+  }
+  launch_pdl_cluster(k_vcycle_mid<T, false>, cs, dim3(TAIL_THREADS), smem, st, levels_dev, mid,
+                     tail, nl, smoother, (T)weight, tmp, in_smem);
 }
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st) {
@@ -1543,6 +1670,9 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
                                       cudaStream_t, int, bool);                               \
   template void launch_mg_prolong_add<T>(const MGLevel<T> &, const MGLevel<T> &, const T *,   \
                                          T *, cudaStream_t, int, bool);                       \
+  template void launch_vcycle_mid<T>(const MGLevel<T> *, int, int, int, int, double, T *,       \
+                                     size_t, int, cudaStream_t, bool);                         \
+  template int vcycle_mid_cluster_size<T>(bool, size_t);                                       \
   template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *, size_t, \
                                       cudaStream_t, bool);                                    \
   template size_t tail_smem_bytes<T>(const MGLevel<T> *, int, int, bool);                    \

@@ -45,6 +45,27 @@ inline void launch_pdl_smem(void (*kern)(KArgs...), dim3 grid, dim3 block, size_
   cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
 }
 
+// one thread-block cluster of cs blocks along x
+template <typename... KArgs, typename... Args>
+inline void launch_pdl_cluster(void (*kern)(KArgs...), int cs, dim3 block, size_t smem,
+                               cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs);
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[2];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = pdl_on() ? 1 : 0;
+  attr[1].id = cudaLaunchAttributeClusterDimension;
+  attr[1].val.clusterDim.x = cs;
+  attr[1].val.clusterDim.y = 1;
+  attr[1].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 2;
+  cudaLaunchKernelEx(&cfg, kern, static_cast<KArgs>(args)...);
+}
+
 template <typename... KArgs, typename... Args>
 inline void launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
                        Args... args) {

@@ -69,6 +69,8 @@ struct MG {
   std::vector<MGLevel<T>> L;
   MGLevel<T> *Ldev = nullptr;  // device copy of the level table (tail kernels)
   int tail = 0;                // first level run by the single-block tail kernels
+  int mid = 0;                 // first level run by the cluster kernel (== tail: none)
+  int mid_cs = 0;              // blocks in that kernel's cluster
   size_t tail_smem = 0;        // shared-memory bytes of the V-cycle tail (0: global)
   std::vector<char> waved;     // level smoothed by the wavefront kernel
   std::vector<WaveLevel> wave; // its control words
@@ -90,6 +92,12 @@ struct MG {
 //                     single-block tail kernels, as far as the tail fits in
 //                     shared memory (default 1024)
 //   PFGPU_TAIL_SMEM   0 runs the V-cycle tail from global memory
+//   PFGPU_MID_CELLS   grid levels at or below this many cells run, with the
+//                     tail, inside one thread-block-cluster kernel (default 0:
+//                     none; on B200 each of its phases waits about as long on
+//                     L2 as a grid launch does, so it is slower overall)
+//   PFGPU_MID_CLUSTER most blocks in that cluster (default 16, as many as the
+//                     device can co-schedule)
 //   PFGPU_FLIP        0 runs every V-cycle launch in forward block order
 //   PFGPU_SPLIT       0 keeps x and b of the grid levels in the natural
 //                     (interleaved-colour) layout; the TMA-fused and wavefront
@@ -396,14 +404,16 @@ static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
 
 // One V-cycle with zero initial guess on level-0 (b -> x)
 // (pfsimulator/parflow_lib/mg_semi.c:93-432 with MaxIter 1)
-// Levels below mg.tail use one grid-wide kernel per phase; levels mg.tail ..
-// nl-1 (a few thousand cells each) run inside one single-block kernel.
+// Levels below mg.mid use one grid-wide kernel per phase; levels mg.mid ..
+// mg.tail-1 (when there are any) run in one cluster kernel, which also runs
+// levels mg.tail .. nl-1 (a few thousand cells each) in one of its blocks;
+// otherwise those run inside one single-block kernel.
 template <typename T>
 static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
   const int sk = smoother == 1 ? 2 : 3;
-  const int first = mg.tail;
+  const int first = mg.mid;
   // block order of the next grid launch: with mg.flip every launch runs in
   // the opposite order of the one before it (the input conversion runs
   // forward), so it starts on the data still in L2
@@ -432,7 +442,11 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
     k += 2;
   }
   // levels first .. nl-1, coarse solve (RedBlackGSPoint, mg_semi.c:1276) included
-  launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st, mg.h16);
+  if (mg.mid < mg.tail)
+    launch_vcycle_mid<T>(mg.Ldev, mg.mid, mg.tail, nl, smoother, w, mg.wtmp, mg.tail_smem,
+                         mg.mid_cs, st, mg.h16);
+  else
+    launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st, mg.h16);
   k++;
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
@@ -971,16 +985,33 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
     mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
   }
   mg.flip = env_ll("PFGPU_FLIP", 1) != 0;
+  // middle levels: the grid levels at or below PFGPU_MID_CELLS cells just
+  // above the tail, when the device can co-schedule a cluster for them
+  mg.mid = mg.tail;
+  {
+    const long long mid_cells = env_ll("PFGPU_MID_CELLS", 0);
+    int l = mg.tail;
+    while (mid_cells > 0 && l > 1 && mg.L[l - 1].n <= mid_cells) l--;
+    if (l < mg.tail) {
+      int cs = vcycle_mid_cluster_size<T>(mg.h16, mg.tail_smem);
+      const int cap = (int)env_ll("PFGPU_MID_CLUSTER", 16);
+      if (cs > cap) cs = cap;
+      if (cs >= 2) {
+        mg.mid = l;
+        mg.mid_cs = cs;
+      }
+    }
+  }
   // colour-split x / b on the grid levels (red/black smoother); the tail
   // levels keep the natural layout
   const bool split = h->d.mg_smoother == PFGPU_SMOOTH_RBGS && env_ll("PFGPU_SPLIT", 1) != 0;
-  for (int l = 0; l < nl; l++) mg.L[l].split = split && l < mg.tail ? 1 : 0;
+  for (int l = 0; l < nl; l++) mg.L[l].split = split && l < mg.mid ? 1 : 0;
   // grid levels large enough for the fused smoother get an output buffer
   // distinct from the input iterate
   const long long fused_cells = env_ll("PFGPU_RBR_FUSED_CELLS", LLONG_MAX);
   mg.fused.assign(nl, 0);
   mg.maps.resize(nl);
-  for (int l = 0; l < mg.tail; l++) {
+  for (int l = 0; l < mg.mid; l++) {
     MGLevel<T> &L = mg.L[l];
     if (mg.h16 || L.split || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || L.n < fused_cells ||
         !rbr_fused_eligible(L))
@@ -1000,7 +1031,7 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   const int wave_chunk = (int)env_ll("PFGPU_WAVE_CHUNK", 2048);
   mg.waved.assign(nl, 0);
   mg.wave.resize(nl);
-  for (int l = 0; l < mg.tail; l++) {
+  for (int l = 0; l < mg.mid; l++) {
     if (mg.h16 || mg.L[l].split || h->d.mg_smoother != PFGPU_SMOOTH_RBGS || mg.fused[l] ||
         mg.L[l].n < wave_cells)
       continue;

@@ -196,6 +196,16 @@ size_t tail_smem_bytes(const MGLevel<T> *levels_host, int first, int nl, bool h1
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
                         double weight, T *tmp, size_t smem, cudaStream_t st, bool h16 = false);
+// levels mid .. tail-1 of a V-cycle on one thread-block cluster of cs blocks
+// (TAIL_THREADS threads each), block 0 of which runs the tail levels tail ..
+// nl-1 in between (from shared memory when smem > 0, as launch_vcycle_tail)
+template <typename T>
+void launch_vcycle_mid(const MGLevel<T> *levels_dev, int mid, int tail, int nl, int smoother,
+                       double weight, T *tmp, size_t smem, int cs, cudaStream_t st,
+                       bool h16 = false);
+// largest cluster the device co-schedules for that kernel (0 if none)
+template <typename T>
+int vcycle_mid_cluster_size(bool h16, size_t smem);
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
 // a natural-layout FP64 vector r into b of level 0 / x of level 0 back into a
