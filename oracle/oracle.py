@@ -31,7 +31,8 @@ class Problem(C.Structure):
                 ("sslope_x", _dp), ("sslope_y", _dp),
                 ("tslope_x", _dp), ("tslope_y", _dp),
                 ("mannings", _dp),
-                ("ov_epsilon", C.c_double)]
+                ("ov_epsilon", C.c_double),
+                ("ov_p_old", _dp)]
 
 
 class Settings(C.Structure):
@@ -72,6 +73,7 @@ def lib():
         L.pfo_mg_create.argtypes = [C.POINTER(Problem), C.POINTER(Settings)]
         L.pfo_mg_create.restype = C.c_void_p
         L.pfo_mg_setup.argtypes = [C.c_void_p, C.POINTER(_dp)]
+        L.pfo_mg_set_wghost.argtypes = [C.c_void_p, _dp]
         L.pfo_mg_apply.argtypes = [C.c_void_p, _dp, _dp]
         L.pfo_mg_num_levels.argtypes = [C.c_void_p]
         L.pfo_mg_level_info.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_int)] * 4
@@ -163,12 +165,21 @@ class Oracle:
         lib().pfo_relperm(C.byref(self.P), _ptr(p), _ptr(s), der)
         return s
 
-    def jacobian(self, p, dt, symm=0):
+    def jacobian(self, p, dt, symm=0, p_old=None):
+        """J(p) (7 arrays C W E S N L U) or its PFSymmetric PC form (symm=1:
+        C E N U; symm=2: also the (nz, ny) W entries of the i = 0 cells that
+        the symmetric storage keeps in a ghost column); p_old is the step's
+        old pressure, which only the diffusive overland terms read."""
         p = np.ascontiguousarray(p, dtype=np.float64)
         ns = 4 if symm else 7
         J = [np.empty_like(p) for _ in range(ns)]
-        arr = (_dp * ns)(*[_ptr(x) for x in J])
+        if symm == 2:
+            J.append(np.empty(p.shape[:2]))
+        arr = (_dp * len(J))(*[_ptr(x) for x in J])
+        po = np.ascontiguousarray(p if p_old is None else p_old, dtype=np.float64)
+        self.P.ov_p_old = _ptr(po)
         lib().pfo_jacobian(C.byref(self.P), dt, _ptr(p), symm, arr)
+        self.P.ov_p_old = None
         return J
 
     def matvec(self, J, x):
@@ -229,9 +240,12 @@ class MG:
         return out
 
     def setup(self, A4):
+        """A4 = C E N U, optionally followed by the i = 0 W plane (jacobian
+        with symm=2)."""
         A4 = [np.ascontiguousarray(a, dtype=np.float64) for a in A4]
         self._A = A4
-        arr = (_dp * 4)(*[_ptr(a) for a in A4])
+        lib().pfo_mg_set_wghost(self.h, _ptr(A4[4]) if len(A4) > 4 else None)
+        arr = (_dp * 4)(*[_ptr(a) for a in A4[:4]])
         lib().pfo_mg_setup(self.h, arr)
 
     def apply(self, b):

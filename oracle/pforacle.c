@@ -253,6 +253,213 @@ static void ovl_der(const pfo_problem *pb, const double *p, double *ke, double *
 }
 
 /* -------------------------------------------------------------------------
+ * Diffusive overland flow on the top layer (PL/overlandflow_eval_diffusive.c).
+ * The friction slope adds the ponded-depth gradient to the topographic slope;
+ * its magnitude comes from the old pressure.  Box conventions as for the
+ * kinematic form: top = nz-1 in every column, -1 in the ghost frame, and the
+ * (never positive) ghost pressure beyond the upper x / y edges enters as 0.
+ * ------------------------------------------------------------------------- */
+static double ptop0(const pfo_problem *pb, const double *p, int i, int j)
+{
+  if (i >= pb->nx || j >= pb->ny)
+    return 0.0;
+  return PFMAX(p[(long)pb->nx * pb->ny * (pb->nz - 1) + i + (long)pb->nx * j], 0.0);
+}
+
+/* CALCFCN (:125-250): q_x, q_y per column, then ke/kw/kn/ks gathered */
+static void ovd_fcn(const pfo_problem *pb, const double *p, const double *op, double *ke,
+                    double *kw, double *kn, double *ks)
+{
+  const int nx = pb->nx, ny = pb->ny, sy = nx + 2;
+  const long n2 = (long)(nx + 2) * (ny + 2);
+  const double dx = pb->dx, dy = pb->dy, eps = pb->ov_epsilon;
+  double *qx = (double*)calloc(n2, sizeof(double));
+  double *qy = (double*)calloc(n2, sizeof(double));
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      const double sxv = pb->tslope_x[i + nx * j], syv = pb->tslope_y[i + nx * j];
+      const double n_man = pb->mannings[i + nx * j];
+      double Pupx = ptop0(pb, p, i + 1, j), Pupy = ptop0(pb, p, i, j + 1);
+      double Pupox = ptop0(pb, op, i + 1, j), Pupoy = ptop0(pb, op, i, j + 1);
+      double Pdown = ptop0(pb, p, i, j), Pdowno = ptop0(pb, op, i, j);
+      double Sf_x = sxv + (Pupx - Pdown) / dx;
+      double Sf_y = syv + (Pupy - Pdown) / dy;
+      double Sf_xo = sxv + (Pupox - Pdowno) / dx;
+      double Sf_yo = syv + (Pupoy - Pdowno) / dy;
+      double Sf_mag = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+      if (Sf_mag < eps) Sf_mag = eps;
+      double Press_x = UPSTREAM(-Sf_x, 0.0, Pdown, Pupx);
+      double Press_y = UPSTREAM(-Sf_y, 0.0, Pdown, Pupy);
+      qx[io] = -(Sf_x / (pow(fabs(Sf_mag), 0.5) * n_man)) * pow(Press_x, (5.0 / 3.0));
+      qy[io] = -(Sf_y / (pow(fabs(Sf_mag), 0.5) * n_man)) * pow(Press_y, (5.0 / 3.0));
+      if (i == 0)   /* lower x boundary :179-195 */
+      {
+        Press_x = Pdown;
+        Sf_x = sxv + (Press_x - 0.0) / dx;
+        Pupox = Pdowno;
+        Sf_xo = sxv + (Pupox - 0.0) / dx;
+        double m = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+        if (m < eps) m = eps;
+        if (Sf_x > 0.0)
+          qx[io - 1] = -(Sf_x / (pow(fabs(m), 0.5) * n_man)) * pow(Press_x, (5.0 / 3.0));
+      }
+      if (j == 0)   /* lower y boundary :197-228 (its y differences divide by dx) */
+      {
+        Press_y = Pdown;
+        Sf_y = syv + (Press_y - 0.0) / dx;
+        Pupoy = Pdowno;
+        Sf_yo = syv + (Pupoy - 0.0) / dx;
+        double m = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+        if (m < eps) m = eps;
+        if (Sf_y > 0.0)
+          qy[io - sy] = -(Sf_y / (pow(fabs(m), 0.5) * n_man)) * pow(Press_y, (5.0 / 3.0));
+        if (i == 0 && Sf_x > 0.0)   /* corner: q_x again with this magnitude */
+          qx[io - 1] = -(Sf_x / (pow(fabs(m), 0.5) * n_man)) * pow(Press_x, (5.0 / 3.0));
+      }
+    }
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      ke[io] = qx[io];
+      kw[io] = qx[io - 1];
+      kn[io] = qy[io];
+      ks[io] = qy[io - sy];
+    }
+  free(qx);
+  free(qy);
+}
+
+/* CALCDER (:252-455): symmetric (ke kw kn ks) and non-symmetric (…ns)
+ * derivative terms, written into this and neighbouring columns' entries */
+static void ovd_der(const pfo_problem *pb, const double *p, const double *op, double *ke,
+                    double *kw, double *kn, double *ks, double *kens, double *kwns,
+                    double *knns, double *ksns)
+{
+  const int nx = pb->nx, ny = pb->ny, sy = nx + 2;
+  const double dx = pb->dx, dy = pb->dy, eps = pb->ov_epsilon;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      const double sxv = pb->tslope_x[i + nx * j], syv = pb->tslope_y[i + nx * j];
+      const double n_man = pb->mannings[i + nx * j];
+      double Pupx = ptop0(pb, p, i + 1, j), Pupy = ptop0(pb, p, i, j + 1);
+      double Pupox = ptop0(pb, op, i + 1, j), Pupoy = ptop0(pb, op, i, j + 1);
+      double Pdown = ptop0(pb, p, i, j), Pdowno = ptop0(pb, op, i, j);
+      double Sf_x = sxv + (Pupx - Pdown) / dx;
+      double Sf_y = syv + (Pupy - Pdown) / dy;
+      double Sf_xo = sxv + (Pupox - Pdowno) / dx;
+      double Sf_yo = syv + (Pupoy - Pdowno) / dy;
+      double Sf_mag = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+      if (Sf_mag < eps) Sf_mag = eps;
+      double sq = pow(fabs(Sf_mag), 0.5);
+      if (Sf_x < 0)
+      {
+        ke[io] = (5.0 / 3.0) * (-sxv - (Pupx / dx)) / (sq * n_man) * pow(Pdown, (2.0 / 3.0)) +
+                 (8.0 / 3.0) * pow(Pdown, (5.0 / 3.0)) / (sq * n_man * dx);
+        kw[io + 1] = -pow(Pdown, (5.0 / 3.0)) / (sq * n_man * dx);
+        kens[io] = kw[io + 1];
+        kwns[io + 1] = ke[io];
+      }
+      if (Sf_x >= 0)
+      {
+        ke[io] = pow(Pupx, (5.0 / 3.0)) / (sq * n_man * dx);
+        kw[io + 1] = (5.0 / 3.0) * (-sxv + (Pdown / dx)) / (sq * n_man) * pow(Pupx, (2.0 / 3.0)) -
+                     (8.0 / 3.0) * pow(Pupx, (5.0 / 3.0)) / (sq * n_man * dx);
+        kens[io] = kw[io + 1];
+        kwns[io + 1] = ke[io];
+      }
+      if (Sf_y < 0)
+      {
+        kn[io] = (5.0 / 3.0) * (-syv - (Pupy / dy)) / (sq * n_man) * pow(Pdown, (2.0 / 3.0)) +
+                 (8.0 / 3.0) * pow(Pdown, (5.0 / 3.0)) / (sq * n_man * dy);
+        ks[io + sy] = -pow(Pdown, (5.0 / 3.0)) / (sq * n_man * dy);
+        knns[io] = ks[io + sy];
+        ksns[io + sy] = kn[io];
+      }
+      if (Sf_y >= 0)
+      {
+        kn[io] = pow(Pupy, (5.0 / 3.0)) / (sq * n_man * dy);
+        ks[io + sy] = (5.0 / 3.0) * (-syv + (Pdown / dy)) / (sq * n_man) * pow(Pupy, (2.0 / 3.0)) -
+                      (8.0 / 3.0) * pow(Pupy, (5.0 / 3.0)) / (sq * n_man * dy);
+        knns[io] = ks[io + sy];
+        ksns[io + sy] = kn[io];
+      }
+      if (i == 0)   /* lower x boundary :343-372 */
+      {
+        Pupx = Pdown;
+        Sf_x = sxv + (Pupx - 0.0) / dx;
+        Pupox = Pdowno;
+        Sf_xo = sxv + (Pupox - 0.0) / dx;
+        double m = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+        if (m < eps) m = eps;
+        double sm = pow(fabs(m), 0.5);
+        if (Sf_x < 0)
+        {
+          ke[io - 1] = 0.0;
+          kw[io] = 0.0;
+          kwns[io] = 0.0;
+          kens[io - 1] = 0.0;
+        }
+        if (Sf_x >= 0)
+        {
+          ke[io - 1] = pow(Pupx, (5.0 / 3.0)) / (sm * n_man * dx);
+          kw[io] = (5.0 / 3.0) * (-sxv + 0.0) / (sm * n_man) * pow(Pupx, (2.0 / 3.0)) -
+                   (8.0 / 3.0) * pow(Pupx, (5.0 / 3.0)) / (sm * n_man * dx);
+          kens[io - 1] = kw[io];
+          kwns[io] = ke[io - 1];
+        }
+      }
+      if (j == 0)   /* lower y boundary :374-421 */
+      {
+        Pupy = Pdown;
+        Sf_y = syv + (Pupy - 0.0) / dy;
+        Pupoy = Pdowno;
+        Sf_yo = syv + (Pupoy - 0.0) / dy;
+        double m = pow(Sf_xo * Sf_xo + Sf_yo * Sf_yo, 0.5);
+        if (m < eps) m = eps;
+        double sm = pow(fabs(m), 0.5);
+        if (Sf_y < 0)
+        {
+          kn[io - sy] = 0.0;
+          ks[io] = 0.0;
+          ksns[io] = 0.0;
+          knns[io - sy] = 0.0;
+        }
+        if (Sf_y >= 0)
+        {
+          knns[io - sy] = pow(Pupy, (5.0 / 3.0)) / (sm * n_man * dy);
+          ks[io] = (5.0 / 3.0) * (-syv + 0.0) / (sm * n_man) * pow(Pupy, (2.0 / 3.0)) -
+                   (8.0 / 3.0) * pow(Pupy, (5.0 / 3.0)) / (sm * n_man * dy);
+          knns[io - sy] = ks[io];
+          ksns[io] = kn[io - sy];
+        }
+        if (i == 0)   /* corner (:404-420): the x terms again with this magnitude */
+        {
+          if (Sf_x < 0)
+          {
+            kn[io - sy] = 0.0;
+            ks[io] = 0.0;
+            ksns[io] = 0.0;
+            knns[io - sy] = 0.0;
+          }
+          if (Sf_x >= 0)
+          {
+            ke[io - 1] = pow(Pupx, (5.0 / 3.0)) / (sm * n_man * dx);
+            kw[io] = (5.0 / 3.0) * (-sxv + 0.0) / (sm * n_man) * pow(Pupx, (2.0 / 3.0)) -
+                     (8.0 / 3.0) * pow(Pupx, (5.0 / 3.0)) / (sm * n_man * dx);
+            kens[io - 1] = kw[io];
+            kwns[io] = ke[io - 1];
+          }
+        }
+      }
+    }
+}
+
+/* -------------------------------------------------------------------------
  * Residual  (PL/nl_function_eval.c:167-2323)
  * ------------------------------------------------------------------------- */
 void pfo_residual(const pfo_problem *pb, double dt, const double *p,
@@ -336,15 +543,19 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
   {
     const double *vals = pb->bc_val[face];
     int type = pb->bc_type[face];
-    if (type == PFO_BC_OVERLAND_KIN)
+    if (type == PFO_BC_OVERLAND_KIN || type == PFO_BC_OVERLAND_DIFF)
     {
-      /* OverlandKinematicBC :1786-2000, z_upper only */
+      /* OverlandKinematicBC :1786-2026 / OverlandDiffusiveBC :2028-2259,
+       * z_upper only; the two differ only in the face fluxes */
       long n2 = (long)(nx + 2) * (ny + 2);
       ke = (double*)calloc(n2, sizeof(double));
       kw = (double*)calloc(n2, sizeof(double));
       kn = (double*)calloc(n2, sizeof(double));
       ks = (double*)calloc(n2, sizeof(double));
-      ovl_fcn(pb, p, ke, kw, kn, ks);
+      if (type == PFO_BC_OVERLAND_KIN)
+        ovl_fcn(pb, p, ke, kw, kn, ks);
+      else
+        ovd_fcn(pb, p, p_old, ke, kw, kn, ks);
       for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++)
         {
@@ -428,7 +639,10 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
 
 /* -------------------------------------------------------------------------
  * Jacobian  (PL/richards_jacobian_eval.c:217-1420)
- *   J[0..6] = C W E S N L U (full) ; symm: J[0..3] = C E N U
+ *   J[0..6] = C W E S N L U (full) ; symm: J[0..3] = C E N U ; symm 2: also
+ *   J[4] (ny*nz) = the W entries of the i = 0 cells, which the symmetric
+ *   storage keeps in the x_lower ghost column of E (matrix.c:477-490) and
+ *   MGSemi's setup reads (mg_semi.c:563, 671-682)
  * ------------------------------------------------------------------------- */
 void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
                   double *const *J)
@@ -454,6 +668,9 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
 
   for (int s = 0; s < nst; s++)
     memset(J[s], 0, N * sizeof(double));
+  double *wghost = (symm == 2) ? J[4] : NULL;
+  if (wghost)
+    memset(wghost, 0, (size_t)ny * nz * sizeof(double));
   pfo_saturation(pb, p, sat, 0);
   pfo_saturation(pb, p, dsat, 1);
   pfo_relperm(pb, p, kr, 0);
@@ -671,6 +888,46 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
     free(kn);
     free(ks);
   }
+  /* diffusive overland terms on the top layer, MGSemi form (:1989-2026):
+   * off-diagonals from the non-symmetric derivative parts of this column */
+  if (pb->bc_type[5] == PFO_BC_OVERLAND_DIFF)
+  {
+    const int sy2 = nx + 2;
+    long n2 = (long)(nx + 2) * (ny + 2);
+    double *buf = (double*)calloc(8 * n2, sizeof(double));
+    double *ke = buf, *kw = buf + n2, *kn = buf + 2 * n2, *ks = buf + 3 * n2;
+    double *kens = buf + 4 * n2, *kwns = buf + 5 * n2, *knns = buf + 6 * n2, *ksns = buf + 7 * n2;
+    ovd_der(pb, p, pb->ov_p_old, ke, kw, kn, ks, kens, kwns, knns, ksns);
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        long io = (i + 1) + (long)sy2 * (j + 1);
+        if (p[c] > 0.0)
+          cp[c] += (vol / dz) + (vol / ffy) * dt * (ke[io] - kw[io])
+                   + (vol / ffx) * dt * (kn[io] - ks[io]);
+        double tw = (vol / ffy) * dt * (kwns[io]);
+        double te = (vol / ffy) * dt * (kens[io]);
+        double ts = (vol / ffx) * dt * (ksns[io]);
+        double tn = (vol / ffx) * dt * (knns[io]);
+        if (!symm)
+        {
+          wp[c] -= tw;
+          ep[c] += te;
+          sop[c] -= ts;
+          np[c] += tn;
+        }
+        else
+        {
+          if (i > 0) ep[c - 1] -= tw;
+          else if (wghost) wghost[j + (long)ny * (nz - 1)] -= tw;
+          ep[c] += te;
+          if (j > 0) np[c - sy] -= ts;
+          np[c] += tn;
+        }
+      }
+    free(buf);
+  }
   free(sat);
   free(dsat);
   free(kr);
@@ -713,6 +970,9 @@ typedef struct {
   double *x, *b, *t;  /* solution, rhs, temp */
   int dir;            /* coarsening direction to the next level */
   double *p1, *p2;    /* prolongation weights, fine-grid sized (used at odd points) */
+  double *wg;         /* (ny*nz) W entries of the i = 0 cells: the x_lower ghost column
+                       * of E in the symmetric storage; zero unless the finest
+                       * operator has one (diffusive overland terms) */
 } mg_level;
 
 struct pfo_mg {
@@ -733,6 +993,7 @@ static void lvl_alloc(mg_level *l, int nx, int ny, int nz)
   l->t = (double*)calloc(l->n, sizeof(double));
   l->p1 = (double*)calloc(l->n, sizeof(double));
   l->p2 = (double*)calloc(l->n, sizeof(double));
+  l->wg = (double*)calloc((size_t)ny * nz, sizeof(double));
 }
 
 /* coarsening directions: PL/mg_semi.c:858-923 */
@@ -793,7 +1054,7 @@ void pfo_mg_destroy(pfo_mg *mg)
   {
     mg_level *l = &mg->L[i];
     for (int s = 0; s < 4; s++) free(l->a[s]);
-    free(l->x); free(l->b); free(l->t); free(l->p1); free(l->p2);
+    free(l->x); free(l->b); free(l->t); free(l->p1); free(l->p2); free(l->wg);
   }
   free(mg->L);
   free(mg);
@@ -809,7 +1070,7 @@ static double coef(const mg_level *l, int s, int i, int j, int k)
   switch (s)
   {
     case 0: return l->a[0][IDX(i, j, k)];
-    case 1: return (i > 0) ? l->a[1][IDX(i - 1, j, k)] : 0.0;
+    case 1: return (i > 0) ? l->a[1][IDX(i - 1, j, k)] : l->wg[j + (long)ny * k];
     case 2: return l->a[1][IDX(i, j, k)];
     case 3: return (j > 0) ? l->a[2][IDX(i, j - 1, k)] : 0.0;
     case 4: return l->a[2][IDX(i, j, k)];
@@ -838,6 +1099,16 @@ static void snum_for(int dir, int s[7])
 }
 
 /* PL/mg_semi.c:437-760 */
+void pfo_mg_set_wghost(pfo_mg *mg, const double *wg)
+{
+  mg_level *L0 = &mg->L[0];
+  size_t n = (size_t)L0->ny * L0->nz;
+  if (wg)
+    memcpy(L0->wg, wg, n * sizeof(double));
+  else
+    memset(L0->wg, 0, n * sizeof(double));
+}
+
 void pfo_mg_setup(pfo_mg *mg, double *const *A4)
 {
   mg_level *L0 = &mg->L[0];
@@ -897,6 +1168,16 @@ void pfo_mg_setup(pfo_mg *mg, double *const *A4)
           ac[0][cc] = coef(F, s[0], i, j, k) + coef(F, s[3], i, j, k) + coef(F, s[4], i, j, k)
                       + coef(F, s[5], i, j, k) + coef(F, s[6], i, j, k)
                       + coef(F, s[1], i, j, k) * p2_1 + coef(F, s[2], i, j, k) * p1_2;
+          /* the coarse W entry of an i = 0 cell goes to the coarse ghost
+           * column (mg_semi.c:671-677 through the symmetric aliasing); along
+           * x it is W times the (zero) weight of the fine ghost point */
+          if (ic == 0)
+          {
+            double wc = 0.0;
+            for (int q = 1; q <= 6; q++)
+              if (s[q] == 1) wc = ac[q][cc];
+            Cl->wg[jc + (long)cny * kc] = wc;
+          }
         }
     /* symmetric storage of the coarse operator: an upper entry is last
      * written through its neighbour's lower entry when that neighbour exists */
@@ -1127,7 +1408,7 @@ typedef struct {
   const double *p_old, *s_old;
   long N;
   double *J[7];
-  double *PC[4];
+  double *PC[5];   /* C E N U, and the W ghost plane of the i = 0 column */
   pfo_mg *mg;
   pfo_stats *stats;
 } kctx;
@@ -1351,17 +1632,23 @@ done:
 }
 
 /* KINSol (KS/kinsol.c:363-910) with LineSearch globalization */
-void pfo_newton_solve(const pfo_problem *pb, const pfo_settings *st, double dt,
+void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double dt,
                       const double *p_old, const double *s_old, double *p,
                       pfo_stats *stats)
 {
   kctx kc;
+  /* the Jacobian of this step sees its old pressure (RichardsJacobianEval's
+   * old_pressure argument) */
+  pfo_problem pstep = *pb_in;
+  pstep.ov_p_old = p_old;
+  const pfo_problem *pb = &pstep;
   long N = (long)pb->nx * pb->ny * pb->nz;
   memset(stats, 0, sizeof(*stats));
   kc.pb = pb; kc.st = st; kc.dt = dt; kc.p_old = p_old; kc.s_old = s_old; kc.N = N;
   kc.stats = stats;
   for (int s = 0; s < 7; s++) kc.J[s] = (double*)malloc(N * sizeof(double));
   for (int s = 0; s < 4; s++) kc.PC[s] = (double*)malloc(N * sizeof(double));
+  kc.PC[4] = (double*)malloc((long)pb->ny * pb->nz * sizeof(double));
   kc.mg = pfo_mg_create(pb, st);
 
   double *uu = p;
@@ -1412,7 +1699,8 @@ void pfo_newton_solve(const pfo_problem *pb, const pfo_settings *st, double dt,
     double eps = (eta + uround) * fnorm;
     if (eps < epsmin) eps = epsmin;
     /* KINLinSolDrv: preconditioner setup every iteration (msbpre = 1) */
-    pfo_jacobian(pb, dt, uu, 1, kc.PC);
+    pfo_jacobian(pb, dt, uu, 2, kc.PC);
+    pfo_mg_set_wghost(kc.mg, kc.PC[4]);
     pfo_mg_setup(kc.mg, kc.PC);
     stats->npe++;
     for (long q = 0; q < N; q++) bb[q] = -fval[q];
@@ -1604,7 +1892,7 @@ void pfo_newton_solve(const pfo_problem *pb, const pfo_settings *st, double dt,
   stats->fnorm = fnorm;
 out:
   for (int s = 0; s < 7; s++) free(kc.J[s]);
-  for (int s = 0; s < 4; s++) free(kc.PC[s]);
+  for (int s = 0; s < 5; s++) free(kc.PC[s]);
   pfo_mg_destroy(kc.mg);
   free(fval); free(unew); free(pp); free(bb);
 }

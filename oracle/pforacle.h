@@ -16,7 +16,7 @@
 extern "C" {
 #endif
 
-enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2 };
+enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2, PFO_BC_OVERLAND_DIFF = 3 };
 
 typedef struct {
   int nx, ny, nz;
@@ -38,7 +38,11 @@ typedef struct {
   const double *sslope_x, *sslope_y;
   const double *tslope_x, *tslope_y;
   const double *mannings;
-  double ov_epsilon;               /* Solver.OverlandKinematic.Epsilon */
+  double ov_epsilon;               /* Solver.Overland{Kinematic,Diffusive}.Epsilon */
+  /* old pressure (interior layout) for the diffusive overland slope magnitude
+   * in the Jacobian (overlandflow_eval_diffusive.c CALCDER); the residual
+   * takes it as an argument */
+  const double *ov_p_old;
 } pfo_problem;
 
 typedef struct {
@@ -66,7 +70,8 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
                   const double *p_old, const double *s_old, double *f);
 
 /* Jacobian: full 7 arrays C,W,E,S,N,L,U (symm=0) or the symmetric PC part
- * stored as C,E,N,U (symm=1) (richards_jacobian_eval.c:217-1420) */
+ * stored as C,E,N,U (symm=1), plus J[4] = the (ny*nz) W entries of the
+ * i = 0 cells (symm=2) (richards_jacobian_eval.c:217-1420) */
 void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
                   double *const *J);
 
@@ -77,6 +82,9 @@ void pfo_matvec7(const pfo_problem *pb, double *const *J, const double *x, doubl
 typedef struct pfo_mg pfo_mg;
 pfo_mg *pfo_mg_create(const pfo_problem *pb, const pfo_settings *st);
 void pfo_mg_setup(pfo_mg *mg, double *const *A4);
+/* W entries (ny*nz) of the finest operator's i = 0 cells, or NULL for none;
+ * read by the next pfo_mg_setup */
+void pfo_mg_set_wghost(pfo_mg *mg, const double *wg);
 void pfo_mg_apply(pfo_mg *mg, const double *b, double *x);
 int pfo_mg_num_levels(const pfo_mg *mg);
 void pfo_mg_level_info(const pfo_mg *mg, int l, int *nx, int *ny, int *nz, int *dir);

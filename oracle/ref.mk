@@ -89,7 +89,8 @@ OMP_OBJ := $(addprefix $(OUT)/omp/pl_,$(addsuffix .o,$(CONST))) \
            $(addprefix $(OUT)/omp/am_,$(addsuffix .o,$(AMSRC))) \
            $(OUT)/omp/cjson.o $(OUT)/seq/dsign.o
 
-WRAPS := -Wl,--wrap=KINSolFunctionEval -Wl,--wrap=KINSolMatVec -Wl,--wrap=KinsolPC
+WRAPS := -Wl,--wrap=KINSolFunctionEval -Wl,--wrap=KINSolMatVec -Wl,--wrap=KinsolPC \
+         -Wl,--wrap=RichardsJacobianEval
 
 all: $(OUT)/bin/parflow $(OUT)/bin/parflow_omp $(OUT)/bin/parflow_hook
 

@@ -9,9 +9,13 @@
  *                 p (before the call), f, saturation, density, old pressure,
  *                 old saturation, dt, time
  *   mv_NNNNN.bin  KINSolMatVec (pfsimulator/parflow_lib/richards_jacobian_eval.c:165)
- *                 x, y = J x, pressure, recompute flag
+ *                 x, y = J x, pressure, old pressure, recompute flag
  *   pc_NNNNN.bin  KinsolPC (pfsimulator/parflow_lib/kinsol_pc.c:58)
  *                 rhs before, rhs after (= M^-1 rhs)
+ *   pj_NNNNN.bin  RichardsJacobianEval with symm_part set (the preconditioner
+ *                 matrix, pfsimulator/parflow_lib/richards_jacobian_eval.c:217)
+ *                 its stored coefficients C E N U (ghost frame included),
+ *                 pressure, old pressure
  *
  * PFREF_DUMP_MAX (default 64) bounds the number of files per kind.
  *
@@ -31,8 +35,12 @@ void __real_KINSolFunctionEval(int size, N_Vector pressure, N_Vector fval,
 int __real_KINSolMatVec(void *current_state, N_Vector x, N_Vector y,
                         int *recompute, N_Vector pressure);
 void __real_KinsolPC(Vector *rhs);
+void __real_RichardsJacobianEval(Vector *pressure, Vector *old_pressure, Matrix **ptr_to_J,
+                                 Matrix **ptr_to_JC, Vector *saturation, Vector *density,
+                                 ProblemData *problem_data, double dt, double time,
+                                 int symm_part);
 
-static int counters[3];
+static int counters[4];
 
 static FILE *open_dump(int kind, const char *prefix)
 {
@@ -147,10 +155,11 @@ int __wrap_KINSolMatVec(void *current_state, N_Vector x, N_Vector y,
     FILE *fp = open_dump(1, "mv");
     if (fp)
     {
-      put_header(fp, "MATVEC", 3, StateDt(st), StateTime(st), rc_in);
+      put_header(fp, "MATVEC", 4, StateDt(st), StateTime(st), rc_in);
       put_snapshot(fp, x, x_in, n);
       put_vector(fp, y);
       put_vector(fp, pressure);
+      put_vector(fp, StateOldPressure(st));
       fclose(fp);
     }
     free(x_in);
@@ -176,5 +185,46 @@ void __wrap_KinsolPC(Vector *rhs)
       fclose(fp);
     }
     free(r_in);
+  }
+}
+
+/* One stencil coefficient of a matrix's only submatrix, as a dump vector. */
+static void put_stencil(FILE *fp, Matrix *A, int s)
+{
+  Submatrix *sm = MatrixSubmatrix(A, 0);
+  int hdr[6];
+
+  hdr[0] = SubmatrixNX(sm);
+  hdr[1] = SubmatrixNY(sm);
+  hdr[2] = SubmatrixNZ(sm);
+  hdr[3] = SubmatrixIX(sm);
+  hdr[4] = SubmatrixIY(sm);
+  hdr[5] = SubmatrixIZ(sm);
+  fwrite(hdr, sizeof(int), 6, fp);
+  fwrite(SubmatrixStencilData(sm, s), sizeof(double),
+         (size_t)hdr[0] * hdr[1] * hdr[2], fp);
+}
+
+void __wrap_RichardsJacobianEval(Vector *pressure, Vector *old_pressure, Matrix **ptr_to_J,
+                                 Matrix **ptr_to_JC, Vector *saturation, Vector *density,
+                                 ProblemData *problem_data, double dt, double time,
+                                 int symm_part)
+{
+  __real_RichardsJacobianEval(pressure, old_pressure, ptr_to_J, ptr_to_JC, saturation,
+                              density, problem_data, dt, time, symm_part);
+  if (symm_part && getenv("PFREF_DUMP_DIR"))
+  {
+    FILE *fp = open_dump(3, "pj");
+    if (fp)
+    {
+      /* stencil order C W E S N L U; the stored (upper) ones are C E N U */
+      static const int stored[4] = { 0, 2, 4, 6 };
+      put_header(fp, "PCMAT", 6, dt, time, symm_part);
+      for (int s = 0; s < 4; s++)
+        put_stencil(fp, *ptr_to_J, stored[s]);
+      put_vector(fp, pressure);
+      put_vector(fp, old_pressure);
+      fclose(fp);
+    }
   }
 }

@@ -77,9 +77,10 @@ def hetero(nx=512, ny=512, nz=50, nsteps=20, dt=0.05, seed=2,
 
 def overland(nx=256, ny=256, nz=20, nsteps=16, dt=0.25, seed=1, wt_depth=1.0,
              mannings=5.5e-5, rain=-0.01, rain_steps=8, dry_steps=8,
-             solver: SolverSettings = None) -> RichardsProblem:
+             solver: SolverSettings = None, kind: int = BC_OVERLAND_KIN) -> RichardsProblem:
     """Config 1.  ``wt_depth`` is the water-table depth below the surface
-    (negative: ponded start)."""
+    (negative: ponded start); ``kind`` the overland routing of the top face
+    (kinematic, or BC_OVERLAND_DIFF for the diffusive wave)."""
     shape = (nz, ny, nx)
     top = np.arange(nz)[:, None, None] >= nz // 2
     perm = np.where(top, 0.1, 0.005) * np.ones(shape)
@@ -95,7 +96,7 @@ def overland(nx=256, ny=256, nz=20, nsteps=16, dt=0.25, seed=1, wt_depth=1.0,
     p.mannings = mannings
     p.bc = {face: BC(BC_FLUX, (0.0,)) for face in
             ("x_lower", "x_upper", "y_lower", "y_upper", "z_lower")}
-    p.bc["z_upper"] = BC(BC_OVERLAND_KIN, (rain, 0.0), lengths=(rain_steps, dry_steps))
+    p.bc["z_upper"] = BC(kind, (rain, 0.0), lengths=(rain_steps, dry_steps))
     p.ic = p.hydrostatic_ic(-wt_depth, "z_upper")
     return p
 

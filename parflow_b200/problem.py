@@ -40,9 +40,11 @@ FACES = ("x_lower", "x_upper", "y_lower", "y_upper", "z_lower", "z_upper")
 BC_FLUX = 0          # FluxConst (pfsimulator/parflow_lib/problem_bc_pressure.c:582)
 BC_DIRICHLET = 1     # DirEquilRefPatch (problem_bc_pressure.c:143)
 BC_OVERLAND_KIN = 2  # OverlandKinematic (bc_pressure_package.c:409)
+BC_OVERLAND_DIFF = 3  # OverlandDiffusive (bc_pressure_package.c:427)
 
 _PF_BC_NAME = {BC_FLUX: "FluxConst", BC_DIRICHLET: "DirEquilRefPatch",
-               BC_OVERLAND_KIN: "OverlandKinematic"}
+               BC_OVERLAND_KIN: "OverlandKinematic",
+               BC_OVERLAND_DIFF: "OverlandDiffusive"}
 
 
 def pfround(x: float) -> int:
@@ -473,4 +475,4 @@ class RichardsProblem:
 
 
 __all__ = ["RichardsProblem", "BC", "SolverSettings", "FACES",
-           "BC_FLUX", "BC_DIRICHLET", "BC_OVERLAND_KIN", "pfround"]
+           "BC_FLUX", "BC_DIRICHLET", "BC_OVERLAND_KIN", "BC_OVERLAND_DIFF", "pfround"]

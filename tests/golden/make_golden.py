@@ -77,6 +77,7 @@ def make(case_name: str, max_dumps: int = 6):
         out["mv_x"] = stack([inner(d["vectors"][0][1]) for d in mv])
         out["mv_y"] = stack([inner(d["vectors"][1][1]) for d in mv])
         out["mv_p"] = stack([inner(d["vectors"][2][1]) for d in mv])
+        out["mv_pold"] = stack([inner(d["vectors"][3][1]) for d in mv])
         out["mv_dt"] = np.array([d["dt"] for d in mv])
         out["mv_time"] = np.array([d["time"] for d in mv])
         out["pc_in"] = stack([inner(d["vectors"][0][1]) for d in pc])
