@@ -60,6 +60,9 @@ extern "C" {
 #define PFGPU_BC_DIRICHLET 1   /* DirEquilRefPatch: pressure head values on the face */
 #define PFGPU_BC_OVERLAND_KIN 2 /* OverlandKinematic (z_upper only): rain flux values as
                                   * FluxConst plus kinematic-wave ponding and routing */
+#define PFGPU_BC_OVERLAND_DIFF 3 /* OverlandDiffusive (z_upper only): the same with
+                                   * diffusive-wave routing, whose friction slope
+                                   * includes the ponded-depth gradient */
 
 /* faces, ParFlow box patch order */
 #define PFGPU_X_LOWER 0
@@ -197,8 +200,9 @@ int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path);
  * terrain_following (Solver.TerrainFollowingGrid, solver_richards.c:562-572)
  * puts the slopes into the subsurface x / y face gravity terms
  * (nl_function_eval.c:725-733, richards_jacobian_eval.c:620-660);
- * ov_epsilon is Solver.OverlandKinematic.Epsilon (1e-5 by default).  Needed
- * before a PFGPU_BC_OVERLAND_KIN face is set. */
+ * ov_epsilon is Solver.OverlandKinematic.Epsilon or
+ * Solver.OverlandDiffusive.Epsilon (1e-5 by default).  Needed before a
+ * PFGPU_BC_OVERLAND_KIN or PFGPU_BC_OVERLAND_DIFF face is set. */
 int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
                       const double *mannings, int terrain_following, double ov_epsilon);
 
@@ -208,7 +212,9 @@ int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slop
  * BCPressure (pfsimulator/parflow_lib/problem_bc_pressure.c:60).  An
  * OverlandKinematic face (z_upper) adds the kinematic-wave overland flow of
  * overlandflow_eval_Kin.c to the top layer (nl_function_eval.c:1786-2000,
- * richards_jacobian_eval.c:1863-1990). */
+ * richards_jacobian_eval.c:1863-1990); an OverlandDiffusive face the
+ * diffusive-wave flow of overlandflow_eval_diffusive.c
+ * (nl_function_eval.c:2028-2259, richards_jacobian_eval.c:1989-2026). */
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values);
 
 /* Residual F(p) of one implicit step (NlFunctionEval,
@@ -223,6 +229,13 @@ int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old
  * matvec.c:35).  Uses the handle's matvec precision. */
 int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt,
                           const double *x, double *y);
+
+/* Sets the old pressure (ParFlow layout) that the Jacobian of
+ * pfgpu_jacobian_matvec and pfgpu_pc_setup reads: the old_pressure argument
+ * of RichardsJacobianEval (richards_jacobian_eval.c:217), used only by the
+ * diffusive overland terms.  pfgpu_nl_function_eval and the solves set it
+ * too (their p_old). */
+int pfgpu_set_old_pressure(pfgpu_handle *h, const double *p_old);
 
 /* Assembles the preconditioner matrix (PCMatrixType PFSymmetric) at p and
  * builds the semicoarsening multigrid hierarchy
@@ -291,7 +304,10 @@ int pfgpu_ensemble_advance(pfgpu_handle *const *members, int n, const double *dt
  * interior indices i + nx*(j + ny*k)) and obs_values (nobs_steps x nobs,
  * step-major) are host arrays.  The boundary tables in effect are used for
  * every step (constant boundary conditions over the window).  Use an FP64
- * handle: the mixed form stores J in FP32. */
+ * handle: the mixed form stores J in FP32.  Not available with a diffusive
+ * overland face (PFGPU_ERR_STATE): its terms depend on the old pressure
+ * through the slope magnitude, a coupling between steps with no adjoint
+ * here. */
 int pfgpu_adjoint_record(pfgpu_handle *h, int max_steps);
 int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps, int nobs,
                            const long long *obs_cells, const double *obs_values, double tol,

@@ -18,6 +18,7 @@ struct LV {
   int nx, ny, nz;
   long long n;
   const T *a0, *ae, *an, *au;
+  const T *wg;                       // W of the i = 0 cells (MGLevel::wg)
   const __half *he, *hn, *hu, *hd;  // scaled FP16 operator (H mode)
   const int *hflag;                  // nonzero: read the scaled diagonal hd
 };
@@ -27,6 +28,7 @@ __device__ __forceinline__ LV<T> lv(const MGLevel<T> &L) {
   LV<T> v;
   v.nx = L.nx; v.ny = L.ny; v.nz = L.nz; v.n = L.n;
   v.a0 = L.a[0]; v.ae = L.a[1]; v.an = L.a[2]; v.au = L.a[3];
+  v.wg = L.wg;
   v.he = L.h[0]; v.hn = L.h[1]; v.hu = L.h[2]; v.hd = L.h[3];
   v.hflag = L.hflag;
   return v;
@@ -60,7 +62,11 @@ __device__ __forceinline__ T coef(const LV<T> &L, int s, int i, int j, int k) {
   long long c = i + (long long)L.nx * (j + (long long)L.ny * k);
   switch (s) {
     case 0: return diag<T, H>(L, c);
-    case 1: return i > 0 ? ld_off<T, H>(L.ae, L.he, c - 1) : T(0);
+    case 1:
+      if (i > 0) return ld_off<T, H>(L.ae, L.he, c - 1);
+      // the ghost column: read by the setup (plain operator) only
+      if constexpr (H) return T(0);
+      else return L.wg ? L.wg[j + L.ny * k] : T(0);
     case 2: return ld_off<T, H>(L.ae, L.he, c);
     case 3: return j > 0 ? ld_off<T, H>(L.an, L.hn, c - L.nx) : T(0);
     case 4: return ld_off<T, H>(L.an, L.hn, c);
@@ -211,6 +217,10 @@ __device__ __forceinline__ void coarse_op_core(const MGLevel<T> &F, const MGLeve
   C.a[2][cc] = N;
   C.a[3][cc] = U;
   C.a[0][cc] = ac[0] - (ac[3] + ac[4] + ac[5] + ac[6]);
+  // the coarse W of an i = 0 cell goes to the coarse ghost column: the
+  // transverse sum when coarsening along y or z, and along x the fine W
+  // times the zero weight of the fine ghost point
+  if (ic == 0 && C.wg) C.wg[jc + C.ny * kc] = d == 1 ? ac[3] : d == 2 ? ac[5] : T(0);
 }
 
 // coarse operator from stored weights (single-block setup tail)
@@ -307,7 +317,7 @@ __device__ __forceinline__ void gather7(const LV<T> &L, int i, int j, int k, T s
   const int sy = L.nx, sz = L.nx * L.ny;
   const int c = in ? i + sy * j + sz * k : 0;
   st[0] = in ? L.a0[c] : T(0);
-  st[1] = in && i > 0 ? L.ae[c - 1] : T(0);
+  st[1] = in && i > 0 ? L.ae[c - 1] : (in && L.wg ? L.wg[j + L.ny * k] : T(0));
   st[2] = in ? L.ae[c] : T(0);
   st[3] = in && j > 0 ? L.an[c - sy] : T(0);
   st[4] = in ? L.an[c] : T(0);
@@ -386,6 +396,8 @@ __global__ void __launch_bounds__(256) k_setup_level(MGLevel<T> F, MGLevel<T> C)
   C.a[3][cc] = U;
   const T cdiag = ac0 - (ac3 + ac4 + ac5 + ac6);
   C.a[0][cc] = cdiag;
+  // coarse ghost column (see coarse_op_core)
+  if (ic == 0 && C.wg) C.wg[jc + C.ny * kc] = D == 1 ? ac3 : D == 2 ? ac5 : T(0);
   if constexpr (H) {
     const int nx = F.nx, ny = F.ny, nz = F.nz;
     const int sy = nx, sz = nx * ny;

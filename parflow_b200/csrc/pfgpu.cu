@@ -337,13 +337,15 @@ static void assemble(pfgpu_handle *h, const double *u, double dt, bool want_J, b
   vg_state(h, u, reuse_vg);
   if (h->mixed) {
     PCOut<float> M{};
-    if (want_M) M = {h->mgf.L[0].a[0], h->mgf.L[0].a[1], h->mgf.L[0].a[2], h->mgf.L[0].a[3]};
+    if (want_M)
+      M = {h->mgf.L[0].a[0], h->mgf.L[0].a[1], h->mgf.L[0].a[2], h->mgf.L[0].a[3], h->mgf.L[0].wg};
     JacOut<float> J{};
     if (want_J) J = h->Jf;
     launch_jacobian<float, float>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
   } else {
     PCOut<double> M{};
-    if (want_M) M = {h->mgd.L[0].a[0], h->mgd.L[0].a[1], h->mgd.L[0].a[2], h->mgd.L[0].a[3]};
+    if (want_M)
+      M = {h->mgd.L[0].a[0], h->mgd.L[0].a[1], h->mgd.L[0].a[2], h->mgd.L[0].a[3], h->mgd.L[0].wg};
     JacOut<double> J{};
     if (want_J) J = h->Jd;
     launch_jacobian<double, double>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
@@ -946,6 +948,8 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
     // the shorter colour when nx is odd)
     const long long nxb = std::max(L.n, 2LL * L.hx * ny * nz);
     if (dalloc(&L.x, nxb) || dalloc(&L.b, nxb) || dalloc(&L.t, L.n)) return PFGPU_ERR_NOMEM;
+    if (dalloc(&L.wg, (long long)ny * nz)) return PFGPU_ERR_NOMEM;
+    CK(cudaMemset(L.wg, 0, (long long)ny * nz * sizeof(T)));
     if (l < nl - 1) {
       if (dalloc(&L.p1, L.n) || dalloc(&L.p2, L.n)) return PFGPU_ERR_NOMEM;
       CK(cudaMemset(L.p1, 0, L.n * sizeof(T)));
@@ -1053,7 +1057,7 @@ static void free_mg(MG<T> &mg) {
   for (auto &L : mg.L) {
     for (int s = 0; s < 4; s++) cudaFree(L.a[s]);
     cudaFree(L.x); cudaFree(L.b); cudaFree(L.t); cudaFree(L.p1); cudaFree(L.p2);
-    cudaFree(L.x2);
+    cudaFree(L.x2); cudaFree(L.wg);
     for (int s = 0; s < 4; s++) cudaFree(L.h[s]);
     cudaFree(L.q1); cudaFree(L.q2); cudaFree(L.sinv);
   }
@@ -1141,6 +1145,7 @@ static int create_impl(pfgpu_handle *h) {
   P.kx = h->kx; P.ky = h->ky; P.kz = h->kz;
   P.zmult = h->zmult;
   P.zface = h->zface;
+  P.ov_pold = h->p_old;
   P.inv_dx = 1.0 / d.dx;
   P.inv_dy = 1.0 / d.dy;
   P.inv_visc = 1.0 / d.viscosity;
@@ -1487,12 +1492,14 @@ int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slop
 
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values) {
   if (!h || !values || face < 0 || face > 5 ||
-      (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET && type != PFGPU_BC_OVERLAND_KIN)) {
+      (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET && type != PFGPU_BC_OVERLAND_KIN &&
+       type != PFGPU_BC_OVERLAND_DIFF)) {
     set_err("pfgpu_set_bc: bad argument");
     return PFGPU_ERR_ARG;
   }
-  if (type == PFGPU_BC_OVERLAND_KIN && (face != PFGPU_Z_UPPER || !h->P.ov_sx)) {
-    set_err("pfgpu_set_bc: OverlandKinematic needs face z_upper and pfgpu_set_surface first");
+  if ((type == PFGPU_BC_OVERLAND_KIN || type == PFGPU_BC_OVERLAND_DIFF) &&
+      (face != PFGPU_Z_UPPER || !h->P.ov_sx)) {
+    set_err("pfgpu_set_bc: overland flow needs face z_upper and pfgpu_set_surface first");
     return PFGPU_ERR_ARG;
   }
   CK(cudaSetDevice(h->device));
@@ -1575,9 +1582,9 @@ int pfgpu_set_bc_cycle(pfgpu_handle *h, int face, int nint, const int *types,
   int len = 0;
   for (int q = 0; q < nint; q++) {
     const int t = types[q];
-    if ((t != PFGPU_BC_FLUX && t != PFGPU_BC_DIRICHLET && t != PFGPU_BC_OVERLAND_KIN) ||
-        lengths[q] < 1 ||
-        (t == PFGPU_BC_OVERLAND_KIN && (face != PFGPU_Z_UPPER || !h->P.ov_sx))) {
+    const bool ovl = t == PFGPU_BC_OVERLAND_KIN || t == PFGPU_BC_OVERLAND_DIFF;
+    if ((t != PFGPU_BC_FLUX && t != PFGPU_BC_DIRICHLET && !ovl) || lengths[q] < 1 ||
+        (ovl && (face != PFGPU_Z_UPPER || !h->P.ov_sx))) {
       set_err("pfgpu_set_bc_cycle: bad type or length in interval %d", q);
       return PFGPU_ERR_ARG;
     }
@@ -1763,6 +1770,14 @@ int pfgpu_pc_setup(pfgpu_handle *h, const double *p, double dt) {
   return PFGPU_OK;
 }
 
+int pfgpu_set_old_pressure(pfgpu_handle *h, const double *p_old) {
+  if (!h || !p_old) { set_err("pfgpu_set_old_pressure: null argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (in_vec(h, p_old, h->p_old)) return PFGPU_ERR_CUDA;
+  CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
 int pfgpu_pc_apply(pfgpu_handle *h, const double *r, double *z) {
   if (!h || !r || !z) { set_err("pfgpu_pc_apply: null argument"); return PFGPU_ERR_ARG; }
   if (!h->pc_ready) { set_err("pfgpu_pc_apply: call pfgpu_pc_setup first"); return PFGPU_ERR_STATE; }
@@ -1944,6 +1959,12 @@ int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps
   }
   if (!h->recording || h->hist_len < 1) {
     set_err("pfgpu_adjoint_gradient: no recorded steps (pfgpu_adjoint_record, then pfgpu_advance)");
+    return PFGPU_ERR_STATE;
+  }
+  if (h->P.bc_type[5] == PFGPU_BC_OVERLAND_DIFF) {
+    // the diffusive terms depend on the old pressure through the slope
+    // magnitude; that coupling between steps has no adjoint here
+    set_err("pfgpu_adjoint_gradient: not available with a diffusive overland face");
     return PFGPU_ERR_STATE;
   }
   if (h->hist_overflow) {

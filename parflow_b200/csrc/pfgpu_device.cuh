@@ -33,10 +33,14 @@ struct DevProblem {
   // terrain-following grid: per column (ny*nx) g sin(atan S) and g cos(atan S)
   // of the subsurface slopes; null = flat (0 and g)
   const double *tfg_xs, *tfg_xc, *tfg_ys, *tfg_yc;
-  // kinematic overland flow on a z_upper patch of type 2: topographic slopes
-  // and Manning's n per column (ny*nx), Solver.OverlandKinematic.Epsilon
+  // kinematic (type 2) or diffusive (type 3) overland flow on the z_upper
+  // patch: topographic slopes and Manning's n per column (ny*nx),
+  // Solver.Overland{Kinematic,Diffusive}.Epsilon
   const double *ov_sx, *ov_sy, *ov_n;
   double ov_eps;
+  // old pressure of the step (dense interior), read by the diffusive terms'
+  // slope magnitude in the residual and the Jacobian
+  const double *ov_pold;
 };
 
 // Gravity terms of the x face between columns i and i+1 (and of the y face
@@ -259,6 +263,154 @@ __device__ __forceinline__ double ov_press_x(const DevProblem &P, const double *
 __device__ __forceinline__ double ov_press_y(const DevProblem &P, const double *p, int i, int j,
                                              const OvCell &o) {
   return upstream(-o.sfy, 0.0, pmax0(p_top(P, p, i, j)), pmax0(p_top(P, p, i, j + 1)));
+}
+
+// ---------------------------------------------------------------------------
+// Diffusive overland flow on the top layer (overlandflow_eval_diffusive.c):
+// the friction slope adds the gradient of the ponded depth to the
+// topographic slope, S_f = S_0 + (max(p_up, 0) - max(p, 0)) / dx, and its
+// magnitude comes from the old pressure.  Same box conventions as the
+// kinematic form.  Gather form: a column's terms are computed by every cell
+// that needs them (its own, and its +x / +y neighbours).
+// ---------------------------------------------------------------------------
+struct OvdCol {
+  double sx, sy, n;          // topographic slopes, Manning's n
+  double pd, pux, puy;       // max(p, 0) at (i,j), (i+1,j), (i,j+1)
+  double pdo;                // max(p_old, 0) at (i,j)
+  double sfx, sfy;           // friction slopes
+  double sfxo, sfyo;         // friction slopes of the old pressure
+  double sq;                 // |S_f,old|^(1/2), magnitude floored at eps
+};
+__device__ __forceinline__ OvdCol ovd_col(const DevProblem &P, const double *p, int i, int j) {
+  const long long a = i + (long long)P.nx * j;
+  OvdCol o;
+  o.sx = __ldg(P.ov_sx + a);
+  o.sy = __ldg(P.ov_sy + a);
+  o.n = __ldg(P.ov_n + a);
+  const double *po = P.ov_pold;
+  o.pd = pmax0(p_top(P, p, i, j));
+  o.pux = pmax0(p_top(P, p, i + 1, j));
+  o.puy = pmax0(p_top(P, p, i, j + 1));
+  o.pdo = pmax0(p_top(P, po, i, j));
+  const double puxo = pmax0(p_top(P, po, i + 1, j)), puyo = pmax0(p_top(P, po, i, j + 1));
+  o.sfx = o.sx + (o.pux - o.pd) / P.dx;
+  o.sfy = o.sy + (o.puy - o.pd) / P.dy;
+  o.sfxo = o.sx + (puxo - o.pdo) / P.dx;
+  o.sfyo = o.sy + (puyo - o.pdo) / P.dy;
+  double mag = pow(o.sfxo * o.sfxo + o.sfyo * o.sfyo, 0.5);
+  if (mag < P.ov_eps) mag = P.ov_eps;
+  o.sq = pow(fabs(mag), 0.5);
+  return o;
+}
+// |S_f|^(1/2) of two slope components, magnitude floored at eps
+__device__ __forceinline__ double ovd_sqrt_mag(const DevProblem &P, double a, double b) {
+  double m = pow(a * a + b * b, 0.5);
+  if (m < P.ov_eps) m = P.ov_eps;
+  return pow(fabs(m), 0.5);
+}
+// CALCFCN (:125-250): the face fluxes q_x (i | i+1), q_y (j | j+1) of a column
+__device__ __forceinline__ double ovd_qx(const OvdCol &o) {
+  return -(o.sfx / (o.sq * o.n)) * pow(upstream(-o.sfx, 0.0, o.pd, o.pux), (5.0 / 3.0));
+}
+__device__ __forceinline__ double ovd_qy(const OvdCol &o) {
+  return -(o.sfy / (o.sq * o.n)) * pow(upstream(-o.sfy, 0.0, o.pd, o.puy), (5.0 / 3.0));
+}
+// the edge fixes of CALCFCN for column (i, j): the flux through the lower x
+// edge when i = 0 (:179-195; recomputed with the magnitude of the lower y
+// fix when j = 0 too, :215-227) and through the lower y edge when j = 0
+// (:197-213, whose differences divide by dx, as the reference's do)
+__device__ __forceinline__ void ovd_q_edges(const DevProblem &P, const OvdCol &o, int i, int j,
+                                            double &qxw, double &qys) {
+  double sfxo = o.sfxo, sfx = 0.0;
+  qxw = 0.0;
+  qys = 0.0;
+  if (i == 0) {
+    sfx = o.sx + (o.pd - 0.0) / P.dx;
+    sfxo = o.sx + (o.pdo - 0.0) / P.dx;
+    const double sm = ovd_sqrt_mag(P, sfxo, o.sfyo);
+    if (sfx > 0.0) qxw = -(sfx / (sm * o.n)) * pow(o.pd, (5.0 / 3.0));
+  }
+  if (j == 0) {
+    const double sfy = o.sy + (o.pd - 0.0) / P.dx;
+    const double sfyo = o.sy + (o.pdo - 0.0) / P.dx;
+    const double sm = ovd_sqrt_mag(P, sfxo, sfyo);
+    if (sfy > 0.0) qys = -(sfy / (sm * o.n)) * pow(o.pd, (5.0 / 3.0));
+    if (i == 0 && sfx > 0.0) qxw = -(sfx / (sm * o.n)) * pow(o.pd, (5.0 / 3.0));
+  }
+}
+// CALCDER (:252-342): derivative terms of a column's x face (i | i+1):
+// a = ke(i) = kwns(i+1) (with respect to this column's depth) and
+// b = kw(i+1) = kens(i) (with respect to the +x column's depth); likewise y
+__device__ __forceinline__ void ovd_der_x(const DevProblem &P, const OvdCol &o, double &a,
+                                          double &b) {
+  const double dx = P.dx;
+  if (o.sfx < 0) {
+    a = (5.0 / 3.0) * (-o.sx - (o.pux / dx)) / (o.sq * o.n) * pow(o.pd, (2.0 / 3.0)) +
+        (8.0 / 3.0) * pow(o.pd, (5.0 / 3.0)) / (o.sq * o.n * dx);
+    b = -pow(o.pd, (5.0 / 3.0)) / (o.sq * o.n * dx);
+  } else {
+    a = pow(o.pux, (5.0 / 3.0)) / (o.sq * o.n * dx);
+    b = (5.0 / 3.0) * (-o.sx + (o.pd / dx)) / (o.sq * o.n) * pow(o.pux, (2.0 / 3.0)) -
+        (8.0 / 3.0) * pow(o.pux, (5.0 / 3.0)) / (o.sq * o.n * dx);
+  }
+}
+__device__ __forceinline__ void ovd_der_y(const DevProblem &P, const OvdCol &o, double &a,
+                                          double &b) {
+  const double dy = P.dy;
+  if (o.sfy < 0) {
+    a = (5.0 / 3.0) * (-o.sy - (o.puy / dy)) / (o.sq * o.n) * pow(o.pd, (2.0 / 3.0)) +
+        (8.0 / 3.0) * pow(o.pd, (5.0 / 3.0)) / (o.sq * o.n * dy);
+    b = -pow(o.pd, (5.0 / 3.0)) / (o.sq * o.n * dy);
+  } else {
+    a = pow(o.puy, (5.0 / 3.0)) / (o.sq * o.n * dy);
+    b = (5.0 / 3.0) * (-o.sy + (o.pd / dy)) / (o.sq * o.n) * pow(o.puy, (2.0 / 3.0)) -
+        (8.0 / 3.0) * pow(o.puy, (5.0 / 3.0)) / (o.sq * o.n * dy);
+  }
+}
+// the edge fixes of CALCDER for column (i, j) (:343-421): kw / kwns of the
+// lower x edge (i = 0) and ks / ksns of the lower y edge (j = 0); the
+// corner (i = j = 0) recomputes the x terms with the lower y fix's
+// magnitude and, when the x edge slope is negative, clears the y terms
+__device__ __forceinline__ void ovd_der_edges(const DevProblem &P, const OvdCol &o, int i, int j,
+                                              double &kw, double &kwns, double &ks,
+                                              double &ksns) {
+  const double dx = P.dx, dy = P.dy;
+  double sfxo = o.sfxo, sfx = 0.0;
+  const double pux = o.pd;  // the edge fixes take the column's own depth
+  if (i == 0) {
+    sfx = o.sx + (pux - 0.0) / dx;
+    sfxo = o.sx + (o.pdo - 0.0) / dx;
+    const double sm = ovd_sqrt_mag(P, sfxo, o.sfyo);
+    if (sfx < 0) {
+      kw = 0.0;
+      kwns = 0.0;
+    } else {
+      kwns = pow(pux, (5.0 / 3.0)) / (sm * o.n * dx);
+      kw = (5.0 / 3.0) * (-o.sx + 0.0) / (sm * o.n) * pow(pux, (2.0 / 3.0)) -
+           (8.0 / 3.0) * pow(pux, (5.0 / 3.0)) / (sm * o.n * dx);
+    }
+  }
+  if (j == 0) {
+    const double puy = o.pd;
+    const double sfy = o.sy + (puy - 0.0) / dy;
+    const double sfyo = o.sy + (o.pdo - 0.0) / dy;
+    const double sm = ovd_sqrt_mag(P, sfxo, sfyo);
+    ksns = 0.0;  // the ghost row's kn, never written
+    if (sfy < 0)
+      ks = 0.0;
+    else
+      ks = (5.0 / 3.0) * (-o.sy + 0.0) / (sm * o.n) * pow(puy, (2.0 / 3.0)) -
+           (8.0 / 3.0) * pow(puy, (5.0 / 3.0)) / (sm * o.n * dy);
+    if (i == 0) {
+      if (sfx < 0) {
+        ks = 0.0;
+      } else {
+        kwns = pow(pux, (5.0 / 3.0)) / (sm * o.n * dx);
+        kw = (5.0 / 3.0) * (-o.sx + 0.0) / (sm * o.n) * pow(pux, (2.0 / 3.0)) -
+             (8.0 / 3.0) * pow(pux, (5.0 / 3.0)) / (sm * o.n * dx);
+      }
+    }
+  }
 }
 
 // Index of a boundary cell in its face table.

@@ -23,9 +23,12 @@ struct JacIn {
 };
 // Symmetric operator: C and the upper entries E N U; W(i) = E(i-1),
 // S(i) = N(i-nx), L(i) = U(i-nx*ny) (pfsimulator/parflow_lib/matrix.c:258-310).
+// wg (ny*nz, optional): W of the i = 0 cells, i.e. the x_lower ghost column
+// of E, which only the diffusive overland terms make nonzero.
 template <typename T>
 struct PCOut {
   T *c, *e, *n, *u;
+  T *wg;
 };
 
 void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
@@ -52,6 +55,13 @@ struct MGLevel {
   T *x, *b, *t;
   T *x2;            // output of the fused post-smoother (levels it runs on)
   T *p1, *p2;       // prolongation weights (fine points of this level)
+  // (ny*nz) W entries of the i = 0 cells: the x_lower ghost column of E in
+  // the reference's symmetric storage, which its setup reads (transverse sums
+  // and coarse entries, mg_semi.c:563, 671-682) and which stays in the ghost
+  // column of the coarser levels until a coarsening along x; zero unless the
+  // finest operator has diffusive overland terms.  The smoothers and
+  // residuals multiply it by a zero ghost iterate, so only the setup reads it.
+  T *wg;
   // scaled FP16 operator (PFGPU_PREC_MIXED_H16): with S = sqrt(|C|) (1 where
   // C is 0 or not finite) the V-cycle runs on y = S x, b^ = b / S and
   // A^ = S^-1 A S^-1, whose off-diagonals A_ij / (S_i S_j) are h[0..2] =

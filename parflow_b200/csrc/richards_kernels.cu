@@ -143,6 +143,18 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
       fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
             dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
       u_new = ffz * value;
+    } else if (SURF && P.bc_type[face] == 3) {
+      // OverlandDiffusive top face (nl_function_eval.c:2028-2259): the same
+      // ponding and routing term with the diffusive-wave face fluxes
+      const OvdCol o = ovd_col(P, p, i, j);
+      double qxw, qys;
+      ovd_q_edges(P, o, i, j, qxw, qys);
+      const double ke = ovd_qx(o), kn = ovd_qy(o);
+      const double kw = i > 0 ? ovd_qx(ovd_col(P, p, i - 1, j)) : qxw;
+      const double ks = j > 0 ? ovd_qy(ovd_col(P, p, i, j - 1)) : qys;
+      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      u_new = ffz * value;
     } else {
       const VG v = vg_at(P, c);
       double krg = vg_kr(P, value, v.alpha, v.n);
@@ -450,6 +462,37 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
     ns += tn;
     if (j + 1 < P.ny) ns -= cy * (kn_d);  // the north neighbour's south term
   }
+  // diffusive overland terms of a top cell, MGSemi form
+  // (richards_jacobian_eval.c:1989-2026, CALCDER of
+  // overlandflow_eval_diffusive.c): off-diagonals from the non-symmetric
+  // derivative parts.  In the symmetric storage the west term of an i = 0
+  // cell lands in the x_lower ghost column of E, which MGSemi's setup reads:
+  // it is returned in wgv for the multigrid's ghost plane.
+  double wgv = 0.0;
+  if (SURF && k == P.nz - 1 && P.bc_type[5] == 3) {
+    const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
+    const OvdCol o = ovd_col(P, p, i, j);
+    double ke_d, kens, kn_d, knns;
+    ovd_der_x(P, o, ke_d, kens);
+    ovd_der_y(P, o, kn_d, knns);
+    double kw_d = 0.0, kwns = 0.0, ks_d = 0.0, ksns = 0.0;
+    ovd_der_edges(P, o, i, j, kw_d, kwns, ks_d, ksns);
+    if (i > 0) ovd_der_x(P, ovd_col(P, p, i - 1, j), kwns, kw_d);
+    if (j > 0) ovd_der_y(P, ovd_col(P, p, i, j - 1), ksns, ks_d);
+    if (pc > 0.0)
+      cp += (vol / P.dz) + cx * (ke_d - kw_d) + cy * (kn_d - ks_d);
+    const double tw = cx * (kwns), te = cx * (kens);
+    const double ts = cy * (ksns), tn = cy * (knns);
+    w -= tw;
+    e += te;
+    s -= ts;
+    nn += tn;
+    if (i == 0) wgv -= tw;
+    es += te;
+    if (i + 1 < P.nx) es -= cx * (ke_d);  // the east neighbour's west term
+    ns += tn;
+    if (j + 1 < P.ny) ns -= cy * (kn_d);  // the north neighbour's south term
+  }
   if (J.c) {
     J.c[c] = (TJ)cp;
     J.w[c] = (TJ)w;
@@ -464,6 +507,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
     M.e[c] = (TP)es;
     M.n[c] = (TP)ns;
     M.u[c] = (TP)us;
+    if (M.wg && i == 0) M.wg[j + (long long)P.ny * k] = (TP)wgv;
   }
 }
 
@@ -517,7 +561,7 @@ void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      double *f, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 256, g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2)
+  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3)
     launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
   else
     launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
@@ -529,7 +573,7 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
                      JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 128, g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2)
+  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3)
     launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J, M);
   else
     launch_pdl(k_jacobian<TJ, TP, false>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J,

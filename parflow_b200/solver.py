@@ -182,13 +182,22 @@ class RichardsGPU:
         L.check(self.lib.pfgpu_saturation(self.h, _ptr(self._io(p)), _ptr(s)), "saturation")
         return unpad(s)
 
-    def jacobian_matvec(self, p, dt, x):
+    def set_old_pressure(self, p_old):
+        """The step's old pressure, read by the Jacobian's diffusive overland
+        terms (RichardsJacobianEval's old_pressure argument)."""
+        L.check(self.lib.pfgpu_set_old_pressure(self.h, _ptr(self._io(p_old))), "set_old_pressure")
+
+    def jacobian_matvec(self, p, dt, x, p_old=None):
+        if p_old is not None:
+            self.set_old_pressure(p_old)
         y = np.zeros(tuple(n + 2 for n in self.prob.shape))
         L.check(self.lib.pfgpu_jacobian_matvec(self.h, _ptr(self._io(p)), dt, _ptr(self._io(x)),
                                                _ptr(y)), "jacobian_matvec")
         return unpad(y)
 
-    def pc_setup(self, p, dt):
+    def pc_setup(self, p, dt, p_old=None):
+        if p_old is not None:
+            self.set_old_pressure(p_old)
         L.check(self.lib.pfgpu_pc_setup(self.h, _ptr(self._io(p)), dt), "pc_setup")
 
     def pc_apply(self, r):

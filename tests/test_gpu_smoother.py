@@ -77,7 +77,7 @@ def test_fused_preconditioner_vs_reference(solver, monkeypatch, golden, name):
     s = solver.RichardsGPU(cases.get(name))
     for i in range(len(g["pc_in"])):
         s.set_time(g["mv_time"][i])
-        s.pc_setup(g["mv_p"][i], g["mv_dt"][i])
+        s.pc_setup(g["mv_p"][i], g["mv_dt"][i], g["mv_pold"][i] if "mv_pold" in g else None)
         z = s.pc_apply(g["pc_in"][i])
         err = np.linalg.norm(z - g["pc_out"][i]) / np.linalg.norm(g["pc_out"][i])
         assert err <= 1e-12, (name, i, err)
