@@ -63,6 +63,9 @@ extern "C" {
 #define PFGPU_BC_OVERLAND_DIFF 3 /* OverlandDiffusive (z_upper only): the same with
                                    * diffusive-wave routing, whose friction slope
                                    * includes the ponded-depth gradient */
+#define PFGPU_BC_OVERLAND 4      /* OverlandFlow (z_upper only): the same with each
+                                   * column's kinematic flux along its own slope,
+                                   * upwinded between columns (overlandflow_eval.c) */
 
 /* faces, ParFlow box patch order */
 #define PFGPU_X_LOWER 0
@@ -202,7 +205,8 @@ int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path);
  * (nl_function_eval.c:725-733, richards_jacobian_eval.c:620-660);
  * ov_epsilon is Solver.OverlandKinematic.Epsilon or
  * Solver.OverlandDiffusive.Epsilon (1e-5 by default).  Needed before a
- * PFGPU_BC_OVERLAND_KIN or PFGPU_BC_OVERLAND_DIFF face is set. */
+ * PFGPU_BC_OVERLAND_KIN, PFGPU_BC_OVERLAND_DIFF or PFGPU_BC_OVERLAND face is
+ * set. */
 int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
                       const double *mannings, int terrain_following, double ov_epsilon);
 
@@ -214,7 +218,9 @@ int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slop
  * overlandflow_eval_Kin.c to the top layer (nl_function_eval.c:1786-2000,
  * richards_jacobian_eval.c:1863-1990); an OverlandDiffusive face the
  * diffusive-wave flow of overlandflow_eval_diffusive.c
- * (nl_function_eval.c:2028-2259, richards_jacobian_eval.c:1989-2026). */
+ * (nl_function_eval.c:2028-2259, richards_jacobian_eval.c:1989-2026); an
+ * OverlandFlow face that of overlandflow_eval.c (nl_function_eval.c:1437-1690,
+ * richards_jacobian_eval.c:2028-2090). */
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values);
 
 /* Residual F(p) of one implicit step (NlFunctionEval,

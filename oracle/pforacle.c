@@ -253,6 +253,72 @@ static void ovl_der(const pfo_problem *pb, const double *p, double *ke, double *
 }
 
 /* -------------------------------------------------------------------------
+ * Overland flow of the OverlandFlow patch type (PL/overlandflow_eval.c):
+ * each column's kinematic flux q = dir(S) |S|^(1/2) / n max(p, 0)^(5/3)
+ * along the sign of its own slope, upwinded between neighbouring columns;
+ * columns outside the domain (top index -1) carry no flux.
+ * ------------------------------------------------------------------------- */
+static double ovf_dir(double s)
+{
+  return (s > 0.0) ? -1.0 : (s < 0.0) ? 1.0 : 0.0;
+}
+
+/* q of column (i, j) along x (ax = 1) or y (ax = 0); 0 outside the domain */
+static double ovf_q(const pfo_problem *pb, const double *p, int i, int j, int ax)
+{
+  if (i < 0 || j < 0 || i >= pb->nx || j >= pb->ny)
+    return 0.0;
+  const long a = i + (long)pb->nx * j;
+  const double s = ax ? pb->tslope_x[a] : pb->tslope_y[a];
+  const double pt = p[(long)pb->nx * pb->ny * (pb->nz - 1) + a];
+  return ovf_dir(s) * (pow(fabs(s), 0.5) / pb->mannings[a]) * pow(PFMAX(pt, 0.0), (5.0 / 3.0));
+}
+
+/* CALCFCN (:104-250): ke, kw, kn, ks of every top cell */
+static void ovf_fcn(const pfo_problem *pb, const double *p, double *ke, double *kw, double *kn,
+                    double *ks)
+{
+  const int nx = pb->nx, ny = pb->ny, sy = nx + 2;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      double q0 = ovf_q(pb, p, i - 1, j, 1), q1 = ovf_q(pb, p, i, j, 1),
+             q2 = ovf_q(pb, p, i + 1, j, 1);
+      kw[io] = PFMAX(q0, 0.0) - PFMAX(-q1, 0.0);
+      ke[io] = PFMAX(q1, 0.0) - PFMAX(-q2, 0.0);
+      q0 = ovf_q(pb, p, i, j - 1, 0);
+      q1 = ovf_q(pb, p, i, j, 0);
+      q2 = ovf_q(pb, p, i, j + 1, 0);
+      ks[io] = PFMAX(q0, 0.0) - PFMAX(-q1, 0.0);
+      kn[io] = PFMAX(q1, 0.0) - PFMAX(-q2, 0.0);
+    }
+}
+
+/* CALCDER (:251-330): derivative terms of each column's own flux */
+static void ovf_der(const pfo_problem *pb, const double *p, double *ke, double *kw, double *kn,
+                    double *ks)
+{
+  const int nx = pb->nx, ny = pb->ny, nz = pb->nz, sy = nx + 2;
+  for (int j = 0; j < ny; j++)
+    for (int i = 0; i < nx; i++)
+    {
+      long io = (i + 1) + (long)sy * (j + 1);
+      long a = i + (long)nx * j;
+      double pt = p[(long)nx * ny * (nz - 1) + a];
+      double sx = pb->tslope_x[a], syv = pb->tslope_y[a], n = pb->mannings[a];
+      double q_mid = ovf_dir(sx) * (5.0 / 3.0) * (pow(fabs(sx), 0.5) / n)
+                     * pow(PFMAX(pt, 0.0), (2.0 / 3.0));
+      kw[io] = -PFMAX(-q_mid, 0.0);
+      ke[io] = PFMAX(q_mid, 0.0);
+      q_mid = ovf_dir(syv) * (5.0 / 3.0) * (pow(fabs(syv), 0.5) / n)
+              * pow(PFMAX(pt, 0.0), (2.0 / 3.0));
+      ks[io] = -PFMAX(-q_mid, 0.0);
+      kn[io] = PFMAX(q_mid, 0.0);
+    }
+}
+
+/* -------------------------------------------------------------------------
  * Diffusive overland flow on the top layer (PL/overlandflow_eval_diffusive.c).
  * The friction slope adds the ponded-depth gradient to the topographic slope;
  * its magnitude comes from the old pressure.  Box conventions as for the
@@ -543,10 +609,12 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
   {
     const double *vals = pb->bc_val[face];
     int type = pb->bc_type[face];
-    if (type == PFO_BC_OVERLAND_KIN || type == PFO_BC_OVERLAND_DIFF)
+    if (type == PFO_BC_OVERLAND_KIN || type == PFO_BC_OVERLAND_DIFF || type == PFO_BC_OVERLAND)
     {
-      /* OverlandKinematicBC :1786-2026 / OverlandDiffusiveBC :2028-2259,
-       * z_upper only; the two differ only in the face fluxes */
+      /* OverlandBC :1437-1690 / OverlandKinematicBC :1786-2026 /
+       * OverlandDiffusiveBC :2028-2259, z_upper only; they differ in the
+       * face fluxes (and OverlandBC adds the spin-up damping term, zero
+       * with OverlandSpinupDampP1/P2 at their defaults of 0) */
       long n2 = (long)(nx + 2) * (ny + 2);
       ke = (double*)calloc(n2, sizeof(double));
       kw = (double*)calloc(n2, sizeof(double));
@@ -554,8 +622,10 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
       ks = (double*)calloc(n2, sizeof(double));
       if (type == PFO_BC_OVERLAND_KIN)
         ovl_fcn(pb, p, ke, kw, kn, ks);
-      else
+      else if (type == PFO_BC_OVERLAND_DIFF)
         ovd_fcn(pb, p, p_old, ke, kw, kn, ks);
+      else
+        ovf_fcn(pb, p, ke, kw, kn, ks);
       for (int j = 0; j < ny; j++)
         for (int i = 0; i < nx; i++)
         {
@@ -563,6 +633,9 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           long io = (i + 1) + (long)(nx + 2) * (j + 1);
           double q_overlnd = vol * (PFMAX(p[c], 0.0) - PFMAX(p_old[c], 0.0)) / dz +
                              dt * vol * ((ke[io] - kw[io]) / dx + (kn[io] - ks[io]) / dy) / dz;
+          if (type == PFO_BC_OVERLAND)   /* spin-up damping, P1 = P2 = 0 */
+            q_overlnd = q_overlnd
+                        + vol * dt / dz * (exp((p[c] < 0.0 ? p[c] : 0.0) * 0.0) * 0.0);
           f[c] += q_overlnd;
           f[c] += dt * 1.0 * (ffz * vals[i + nx * j]);
         }
@@ -887,6 +960,48 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
     free(kw);
     free(kn);
     free(ks);
+  }
+  /* OverlandFlow terms on the top layer, MGSemi form (:2028-2090): the
+   * derivative parts of each column's own flux; the spin-up damping term
+   * of a non-ponded cell is zero with its default parameters */
+  if (pb->bc_type[5] == PFO_BC_OVERLAND)
+  {
+    const int sy2 = nx + 2;
+    long n2 = (long)(nx + 2) * (ny + 2);
+    double *buf = (double*)calloc(4 * n2, sizeof(double));
+    double *ke = buf, *kw = buf + n2, *kn = buf + 2 * n2, *ks = buf + 3 * n2;
+    ovf_der(pb, p, ke, kw, kn, ks);
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        long io = (i + 1) + (long)sy2 * (j + 1);
+        if (p[c] > 0.0)
+          cp[c] += (vol / dz) + (vol / ffy) * dt * (ke[io] - kw[io])
+                   + (vol / ffx) * dt * (kn[io] - ks[io]);
+        else
+          cp[c] += 0.0 + dt * (vol / dz) * (0.0 * exp((p[c] < 0.0 ? p[c] : 0.0) * 0.0) * 0.0);
+        double tw = (vol / ffy) * dt * (ke[io - 1]);
+        double te = (vol / ffy) * dt * (kw[io + 1]);
+        double ts = (vol / ffx) * dt * (kn[io - sy2]);
+        double tn = (vol / ffx) * dt * (ks[io + sy2]);
+        if (!symm)
+        {
+          wp[c] -= tw;
+          ep[c] += te;
+          sop[c] -= ts;
+          np[c] += tn;
+        }
+        else
+        {
+          if (i > 0) ep[c - 1] -= tw;
+          else if (wghost) wghost[j + (long)ny * (nz - 1)] -= tw;
+          ep[c] += te;
+          if (j > 0) np[c - sy] -= ts;
+          np[c] += tn;
+        }
+      }
+    free(buf);
   }
   /* diffusive overland terms on the top layer, MGSemi form (:1989-2026):
    * off-diagonals from the non-symmetric derivative parts of this column */

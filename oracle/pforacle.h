@@ -16,7 +16,8 @@
 extern "C" {
 #endif
 
-enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2, PFO_BC_OVERLAND_DIFF = 3 };
+enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2, PFO_BC_OVERLAND_DIFF = 3,
+       PFO_BC_OVERLAND = 4 };
 
 typedef struct {
   int nx, ny, nz;

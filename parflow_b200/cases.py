@@ -7,7 +7,8 @@ reference CPU build and the oracle finish in seconds.
 from __future__ import annotations
 
 from . import configs
-from .problem import BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND_DIFF, RichardsProblem, SolverSettings
+from .problem import (BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND, BC_OVERLAND_DIFF, RichardsProblem,
+                      SolverSettings)
 
 
 def box_small() -> RichardsProblem:
@@ -59,6 +60,13 @@ def overland_diff_small() -> RichardsProblem:
                             kind=BC_OVERLAND_DIFF)
 
 
+def overland_flow_small() -> RichardsProblem:
+    """The overland case with the OverlandFlow patch type (overlandflow_eval.c:
+    each column's flux along its own slope, upwinded between columns)."""
+    return configs.overland(nx=12, ny=10, nz=6, nsteps=4, seed=13, wt_depth=-0.02,
+                            mannings=1e-3, rain_steps=2, dry_steps=2, kind=BC_OVERLAND)
+
+
 def tfg_small() -> RichardsProblem:
     """Terrain-following slopes in the subsurface fluxes without overland
     flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""
@@ -69,7 +77,8 @@ def tfg_small() -> RichardsProblem:
 
 
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
-          "overland_small", "tfg_small", "overland_diff_small"]
+          "overland_small", "tfg_small", "overland_diff_small",
+          "overland_flow_small"]
 
 
 def get(name: str) -> RichardsProblem:

@@ -79,8 +79,9 @@ def overland(nx=256, ny=256, nz=20, nsteps=16, dt=0.25, seed=1, wt_depth=1.0,
              mannings=5.5e-5, rain=-0.01, rain_steps=8, dry_steps=8,
              solver: SolverSettings = None, kind: int = BC_OVERLAND_KIN) -> RichardsProblem:
     """Config 1.  ``wt_depth`` is the water-table depth below the surface
-    (negative: ponded start); ``kind`` the overland routing of the top face
-    (kinematic, or BC_OVERLAND_DIFF for the diffusive wave)."""
+    (negative: ponded start); ``kind`` the overland routing of the top face:
+    BC_OVERLAND_KIN (OverlandKinematic), BC_OVERLAND (OverlandFlow) or
+    BC_OVERLAND_DIFF (OverlandDiffusive)."""
     shape = (nz, ny, nx)
     top = np.arange(nz)[:, None, None] >= nz // 2
     perm = np.where(top, 0.1, 0.005) * np.ones(shape)

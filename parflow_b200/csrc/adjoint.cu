@@ -104,7 +104,7 @@ __global__ void k_adj_rhs(DevProblem P, const double *__restrict__ p,
   const double rho = P.density, vol = P.dx * P.dy * P.dz, zm = __ldg(P.zmult + k);
   double b = rho * P.porosity * vol * zm * dsat[c] +
              P.sstorage * vol * zm * rho * (sat[c] + p[c] * dsat[c]);
-  if (k == P.nz - 1 && P.bc_type[5] == 2 && p[c] > 0.0) b += vol / P.dz;
+  if (k == P.nz - 1 && (P.bc_type[5] == 2 || P.bc_type[5] == 4) && p[c] > 0.0) b += vol / P.dz;
   rhs[c] = b * lam_next[c];
 }
 

@@ -266,6 +266,34 @@ __device__ __forceinline__ double ov_press_y(const DevProblem &P, const double *
 }
 
 // ---------------------------------------------------------------------------
+// Overland flow of the OverlandFlow patch type (overlandflow_eval.c): each
+// column's flux q = dir(S) |S|^(1/2) / n max(p, 0)^(5/3) along the sign of
+// its own slope (dir = -1 for S > 0, +1 for S < 0, 0 for S = 0), upwinded
+// between neighbouring columns; no flux outside the domain.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double ovf_dir(double s) {
+  return (s > 0.0) ? -1.0 : (s < 0.0) ? 1.0 : 0.0;
+}
+// q of column (i, j) along x (AX) or y; 0 outside the domain
+template <bool AX>
+__device__ __forceinline__ double ovf_q(const DevProblem &P, const double *p, int i, int j) {
+  if (i < 0 || j < 0 || i >= P.nx || j >= P.ny) return 0.0;
+  const long long a = i + (long long)P.nx * j;
+  const double s = AX ? __ldg(P.ov_sx + a) : __ldg(P.ov_sy + a);
+  return ovf_dir(s) * (pow(fabs(s), 0.5) / __ldg(P.ov_n + a)) *
+         pow(pmax0(p_top(P, p, i, j)), (5.0 / 3.0));
+}
+// CALCDER: derivative of a column's own flux, q' = dir 5/3 |S|^(1/2) / n
+// max(p, 0)^(2/3), along x (AX) or y
+template <bool AX>
+__device__ __forceinline__ double ovf_qder(const DevProblem &P, double ptop, int i, int j) {
+  const long long a = i + (long long)P.nx * j;
+  const double s = AX ? __ldg(P.ov_sx + a) : __ldg(P.ov_sy + a);
+  return ovf_dir(s) * (5.0 / 3.0) * (pow(fabs(s), 0.5) / __ldg(P.ov_n + a)) *
+         pow(pmax0(ptop), (2.0 / 3.0));
+}
+
+// ---------------------------------------------------------------------------
 // Diffusive overland flow on the top layer (overlandflow_eval_diffusive.c):
 // the friction slope adds the gradient of the ponded depth to the
 // topographic slope, S_f = S_0 + (max(p_up, 0) - max(p, 0)) / dx, and its

@@ -143,6 +143,19 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
       fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
             dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
       u_new = ffz * value;
+    } else if (SURF && P.bc_type[face] == 4) {
+      // OverlandFlow top face (nl_function_eval.c:1437-1690): each face flux
+      // is the upwind part of the two columns' own fluxes; the spin-up
+      // damping term is zero with its default parameters
+      const double qw = ovf_q<true>(P, p, i - 1, j), qc = ovf_q<true>(P, p, i, j),
+                   qe = ovf_q<true>(P, p, i + 1, j);
+      const double kw = pmax0(qw) - pmax0(-qc), ke = pmax0(qc) - pmax0(-qe);
+      const double qs = ovf_q<false>(P, p, i, j - 1), qm = ovf_q<false>(P, p, i, j),
+                   qn = ovf_q<false>(P, p, i, j + 1);
+      const double ks = pmax0(qs) - pmax0(-qm), kn = pmax0(qm) - pmax0(-qn);
+      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      u_new = ffz * value;
     } else if (SURF && P.bc_type[face] == 3) {
       // OverlandDiffusive top face (nl_function_eval.c:2028-2259): the same
       // ponding and routing term with the diffusive-wave face fluxes
@@ -462,6 +475,35 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
     ns += tn;
     if (j + 1 < P.ny) ns -= cy * (kn_d);  // the north neighbour's south term
   }
+  // OverlandFlow terms of a top cell, MGSemi form
+  // (richards_jacobian_eval.c:2028-2090, CALCDER of overlandflow_eval.c):
+  // the derivative parts of each column's own flux; neighbours' parts give
+  // the off-diagonals, and the east neighbour's west term lands in E(i)
+  if (SURF && k == P.nz - 1 && P.bc_type[5] == 4) {
+    const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
+    const double qx = ovf_qder<true>(P, pc, i, j), qy = ovf_qder<false>(P, pc, i, j);
+    const double ke_d = pmax0(qx), kw_d = -pmax0(-qx);
+    const double kn_d = pmax0(qy), ks_d = -pmax0(-qy);
+    // the neighbours' derivative parts: ke of i-1, kw of i+1, kn of j-1, ks of j+1
+    const double ke_w = i > 0 ? pmax0(ovf_qder<true>(P, p[c - 1], i - 1, j)) : 0.0;
+    const double kw_e = i + 1 < P.nx ? -pmax0(-ovf_qder<true>(P, p[c + 1], i + 1, j)) : 0.0;
+    const double kn_s = j > 0 ? pmax0(ovf_qder<false>(P, p[c - sy], i, j - 1)) : 0.0;
+    const double ks_n = j + 1 < P.ny ? -pmax0(-ovf_qder<false>(P, p[c + sy], i, j + 1)) : 0.0;
+    if (pc > 0.0)
+      cp += (vol / P.dz) + cx * (ke_d - kw_d) + cy * (kn_d - ks_d);
+    else
+      cp += 0.0 + dt * (vol / P.dz) * (0.0 * exp(fmin(pc, 0.0) * 0.0) * 0.0);
+    const double tw = cx * (ke_w), te = cx * (kw_e);
+    const double ts = cy * (kn_s), tn = cy * (ks_n);
+    w -= tw;
+    e += te;
+    s -= ts;
+    nn += tn;
+    es += te;
+    if (i + 1 < P.nx) es -= cx * (ke_d);  // the east neighbour's west term
+    ns += tn;
+    if (j + 1 < P.ny) ns -= cy * (kn_d);  // the north neighbour's south term
+  }
   // diffusive overland terms of a top cell, MGSemi form
   // (richards_jacobian_eval.c:1989-2026, CALCDER of
   // overlandflow_eval_diffusive.c): off-diagonals from the non-symmetric
@@ -561,7 +603,7 @@ void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      double *f, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 256, g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3)
+  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
     launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
   else
     launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
@@ -573,7 +615,7 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
                      JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
   dim3 g, b;
   shape(P.nx, P.ny, P.nz, 128, g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3)
+  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
     launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J, M);
   else
     launch_pdl(k_jacobian<TJ, TP, false>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J,

@@ -108,7 +108,7 @@ class RichardsGPU:
     # ---- setup ---------------------------------------------------------------
     def _upload_fields(self):
         p = self.prob
-        if p.terrain_following or any(bc.kind in (L.BC_OVERLAND_KIN, L.BC_OVERLAND_DIFF)
+        if p.terrain_following or any(bc.kind in (L.BC_OVERLAND_KIN, L.BC_OVERLAND_DIFF, L.BC_OVERLAND)
                                         for bc in p.bc.values()):
             self._upload_surface()
         L.check(self.lib.pfgpu_set_field(self.h, L.FIELD_PERM_X, _ptr(pad(p.field3d(p.perm)))),

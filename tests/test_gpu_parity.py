@@ -189,7 +189,7 @@ def test_device_pointers_match_host(gpu, golden):
     assert (out.cpu().numpy()[0] == 0).all()  # ghost frame written as zero
 
 
-@pytest.mark.parametrize("name", ["overland_small", "overland_diff_small"])
+@pytest.mark.parametrize("name", ["overland_small", "overland_diff_small", "overland_flow_small"])
 def test_preconditioner_grid_levels_vs_reference(name, golden, gpu, monkeypatch):
     """The grid-level setup and smoother kernels (the tail moved down to 16
     cells) against the reference's MGSemi output; with diffusive overland
@@ -206,16 +206,19 @@ def test_preconditioner_grid_levels_vs_reference(name, golden, gpu, monkeypatch)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed16"])
-def test_overland_diffusive_vs_oracle(gpu, precision):
-    """Diffusive-wave overland flow on a 40 x 36 x 10 hillslope (grid-level
-    multigrid kernels), three steps against the oracle: FP64 within 1e-9 with
-    identical Newton and GMRES counts, the mixed form within 1e-8."""
+@pytest.mark.parametrize("kind", ["OverlandDiffusive", "OverlandFlow"])
+def test_overland_types_vs_oracle(gpu, precision, kind):
+    """Diffusive-wave and OverlandFlow overland flow on a 40 x 36 x 10
+    hillslope (grid-level multigrid kernels), three steps against the oracle:
+    FP64 within 1e-9 with identical Newton and GMRES counts, the mixed form
+    within 1e-8."""
     from oracle.oracle import Oracle
     from parflow_b200 import configs
-    from parflow_b200.problem import BC_OVERLAND_DIFF
+    from parflow_b200.problem import BC_OVERLAND, BC_OVERLAND_DIFF
 
-    prob = configs.overland(nx=40, ny=36, nz=10, nsteps=3, seed=5, wt_depth=-0.02,
-                            mannings=1e-3, rain_steps=2, dry_steps=1, kind=BC_OVERLAND_DIFF)
+    k = {"OverlandDiffusive": BC_OVERLAND_DIFF, "OverlandFlow": BC_OVERLAND}[kind]
+    prob = configs.overland(nx=40, ny=36, nz=10, nsteps=3, seed=5, wt_depth=0.05,
+                            mannings=3e-4, rain_steps=2, dry_steps=1, kind=k)
     ps_o, st_o = Oracle(prob).run()
     ps_g, st_g = gpu.RichardsGPU(prob, precision=precision).run()
     for t in range(3):
