@@ -66,6 +66,9 @@ extern "C" {
 #define PFGPU_BC_OVERLAND 4      /* OverlandFlow (z_upper only): the same with each
                                    * column's kinematic flux along its own slope,
                                    * upwinded between columns (overlandflow_eval.c) */
+#define PFGPU_BC_SEEPAGE 5       /* SeepageFace: flux values as FluxConst; on z_upper
+                                   * the ponded water also drains, (vol/dz) dt max(p, 0)
+                                   * (nl_function_eval.c:1692-1784) */
 
 /* faces, ParFlow box patch order */
 #define PFGPU_X_LOWER 0

@@ -651,8 +651,12 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           double value = vals[face_index(pb, face, i, j, k)];
           double dir = (face & 1) ? 1.0 : -1.0;
           double u_new;
-          if (type == PFO_BC_FLUX)
+          if (type == PFO_BC_FLUX || type == PFO_BC_SEEPAGE)
           {
+            /* FluxConst, or SeepageFace (:1692-1784): a flux face whose top
+             * face also drains the ponded water, (vol / dz) dt max(p, 0) */
+            if (type == PFO_BC_SEEPAGE && face == 5)
+              f[c] += (vol / dz) * dt * (PFMAX(p[c], 0.0) - 0.0);
             double h = (face < 2) ? ffx * zm[k] : (face < 4) ? ffy * zm[k] : ffz;
             u_new = h * value;
           }
@@ -916,6 +920,19 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           cp[c] -= o_temp;
         }
   }
+
+  /* SeepageFace on the top face (:1319-1345), in patch order after the
+   * Dirichlet corrections of the other faces */
+  if (pb->bc_type[5] == PFO_BC_SEEPAGE)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        if (p[c] >= 0.0)
+          cp[c] += (vol / dz) * dt * (1.0 + 0.0);
+        else
+          cp[c] += 0.0;
+      }
 
   /* kinematic overland terms on the top layer, MGSemi form (:1863-1990),
    * after every other term.  In the symmetric storage a lower coefficient is

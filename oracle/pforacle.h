@@ -17,7 +17,7 @@ extern "C" {
 #endif
 
 enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2, PFO_BC_OVERLAND_DIFF = 3,
-       PFO_BC_OVERLAND = 4 };
+       PFO_BC_OVERLAND = 4, PFO_BC_SEEPAGE = 5 };
 
 typedef struct {
   int nx, ny, nz;

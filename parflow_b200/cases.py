@@ -7,7 +7,8 @@ reference CPU build and the oracle finish in seconds.
 from __future__ import annotations
 
 from . import configs
-from .problem import (BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND, BC_OVERLAND_DIFF, RichardsProblem,
+from .problem import (BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND, BC_OVERLAND_DIFF, BC_SEEPAGE,
+                      RichardsProblem,
                       SolverSettings)
 
 
@@ -67,6 +68,16 @@ def overland_flow_small() -> RichardsProblem:
                             mannings=1e-3, rain_steps=2, dry_steps=2, kind=BC_OVERLAND)
 
 
+def seepage_small() -> RichardsProblem:
+    """Config-0 box with SeepageFace patches: the top face (water table 0.3 m
+    above it, so the top layer is ponded and drains) and the x_upper face."""
+    p = configs.box(nx=12, ny=10, nz=8, nsteps=3, seed=19)
+    p.bc["z_upper"] = BC(BC_SEEPAGE, (-0.05,))
+    p.bc["x_upper"] = BC(BC_SEEPAGE, (0.0,))
+    p.ic = p.hydrostatic_ic(4.3, "z_lower")
+    return p
+
+
 def tfg_small() -> RichardsProblem:
     """Terrain-following slopes in the subsurface fluxes without overland
     flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""
@@ -78,7 +89,7 @@ def tfg_small() -> RichardsProblem:
 
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
-          "overland_flow_small"]
+          "overland_flow_small", "seepage_small"]
 
 
 def get(name: str) -> RichardsProblem:

@@ -1493,7 +1493,7 @@ int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slop
 int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values) {
   if (!h || !values || face < 0 || face > 5 ||
       (type != PFGPU_BC_FLUX && type != PFGPU_BC_DIRICHLET && type != PFGPU_BC_OVERLAND_KIN &&
-       type != PFGPU_BC_OVERLAND_DIFF && type != PFGPU_BC_OVERLAND)) {
+       type != PFGPU_BC_OVERLAND_DIFF && type != PFGPU_BC_OVERLAND && type != PFGPU_BC_SEEPAGE)) {
     set_err("pfgpu_set_bc: bad argument");
     return PFGPU_ERR_ARG;
   }
@@ -1585,7 +1585,8 @@ int pfgpu_set_bc_cycle(pfgpu_handle *h, int face, int nint, const int *types,
     const int t = types[q];
     const bool ovl =
         t == PFGPU_BC_OVERLAND_KIN || t == PFGPU_BC_OVERLAND_DIFF || t == PFGPU_BC_OVERLAND;
-    if ((t != PFGPU_BC_FLUX && t != PFGPU_BC_DIRICHLET && !ovl) || lengths[q] < 1 ||
+    if ((t != PFGPU_BC_FLUX && t != PFGPU_BC_DIRICHLET && t != PFGPU_BC_SEEPAGE && !ovl) ||
+        lengths[q] < 1 ||
         (ovl && (face != PFGPU_Z_UPPER || !h->P.ov_sx))) {
       set_err("pfgpu_set_bc_cycle: bad type or length in interval %d", q);
       return PFGPU_ERR_ARG;

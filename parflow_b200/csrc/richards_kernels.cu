@@ -118,7 +118,10 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
     const double value = __ldg(P.bc_val[face] + face_slot(P, face, i, j, k));
     const double dir = (face & 1) ? 1.0 : -1.0;
     double u_new;
-    if (P.bc_type[face] == 0) {
+    if (P.bc_type[face] == 0 || P.bc_type[face] == 5) {
+      // FluxConst, or SeepageFace (nl_function_eval.c:1692-1784): a flux
+      // face whose top face also drains the ponded water
+      if (P.bc_type[face] == 5 && face == 5) fc += (vol / P.dz) * dt * (pmax0(pc) - 0.0);
       double h = (face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz;
       u_new = h * value;
     } else if (SURF && P.bc_type[face] == 2) {
@@ -425,6 +428,10 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
     }
     cp -= o_temp;
   }
+
+  // SeepageFace on the top face (richards_jacobian_eval.c:1319-1345), in
+  // patch order after the Dirichlet corrections
+  if (k == P.nz - 1 && P.bc_type[5] == 5 && pc >= 0.0) cp += (vol / P.dz) * dt * (1.0 + 0.0);
 
   // kinematic overland terms of a top cell, MGSemi form
   // (richards_jacobian_eval.c:1863-1990, CALCDER of overlandflow_eval_Kin.c),

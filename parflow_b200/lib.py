@@ -14,7 +14,8 @@ LIB_PATH = os.path.join(HERE, "libpfgpu.so")
 
 ABI_VERSION = 1
 PREC_FP64, PREC_MIXED, PREC_MIXED_H16 = 0, 1, 2
-BC_FLUX, BC_DIRICHLET, BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND = 0, 1, 2, 3, 4
+BC_FLUX, BC_DIRICHLET, BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND, BC_SEEPAGE = \
+    0, 1, 2, 3, 4, 5
 FIELD_PERM_X, FIELD_PERM_Y, FIELD_PERM_Z = 0, 1, 2
 FIELD_VG_ALPHA, FIELD_VG_N, FIELD_S_RES, FIELD_S_SAT = 3, 4, 5, 6
 OK, NOT_CONVERGED = 0, 1

@@ -42,10 +42,12 @@ BC_DIRICHLET = 1     # DirEquilRefPatch (problem_bc_pressure.c:143)
 BC_OVERLAND_KIN = 2  # OverlandKinematic (bc_pressure_package.c:409)
 BC_OVERLAND_DIFF = 3  # OverlandDiffusive (bc_pressure_package.c:427)
 BC_OVERLAND = 4       # OverlandFlow (bc_pressure_package.c:354)
+BC_SEEPAGE = 5        # SeepageFace (bc_pressure_package.c:392)
 
 _PF_BC_NAME = {BC_FLUX: "FluxConst", BC_DIRICHLET: "DirEquilRefPatch",
                BC_OVERLAND_KIN: "OverlandKinematic",
-               BC_OVERLAND_DIFF: "OverlandDiffusive", BC_OVERLAND: "OverlandFlow"}
+               BC_OVERLAND_DIFF: "OverlandDiffusive", BC_OVERLAND: "OverlandFlow",
+               BC_SEEPAGE: "SeepageFace"}
 
 
 def pfround(x: float) -> int:
@@ -476,4 +478,4 @@ class RichardsProblem:
 
 
 __all__ = ["RichardsProblem", "BC", "SolverSettings", "FACES",
-           "BC_FLUX", "BC_DIRICHLET", "BC_OVERLAND_KIN", "BC_OVERLAND_DIFF", "BC_OVERLAND", "pfround"]
+           "BC_FLUX", "BC_DIRICHLET", "BC_OVERLAND_KIN", "BC_OVERLAND_DIFF", "BC_OVERLAND", "BC_SEEPAGE", "pfround"]
