@@ -435,8 +435,10 @@ def gpu_arm(args, rank, world, local_rank):
 # ---------------------------------------------------------------------------
 def ensemble_arm(args, rank, world, local_rank):
     """Member-timesteps/s of the 48-member ensemble, every member resident on
-    the GPU and all advanced concurrently (pfgpu_ensemble_advance), against the
-    same members advanced one after another through the same library."""
+    the GPU and all advanced concurrently (pfgpu_ensemble_advance) with the
+    stencil launches' block shapes picked by the autotuner (pfgpu_autotune,
+    untimed, once per member size), against the same members on the built-in
+    block-shape heuristic and advanced one after another."""
     import torch
 
     from parflow_b200 import configs
@@ -446,12 +448,16 @@ def ensemble_arm(args, rank, world, local_rank):
     probs = configs.ensemble(48, nsteps=10)
     cells = [p.ncells for p in probs]
 
-    def fresh():
+    shapes = {}
+
+    def fresh(tuned=True):
         ms = []
         for p in probs:
             g = RichardsGPU(p, precision=HEADLINE, device=local_rank)
             g.set_pressure(p.initial_pressure())
             g.set_time(p.start_time + p.dt)
+            if tuned:
+                shapes[p.shape] = g.autotune()
             ms.append(g)
         return ms
 
@@ -480,6 +486,11 @@ def ensemble_arm(args, rank, world, local_rank):
     t_conc, st_conc = timed(conc, nsteps, True)
     for g in conc:
         g.close()
+    heur = fresh(tuned=False)
+    ensemble_advance(heur, warm)
+    t_heur, _ = timed(heur, nsteps, True)
+    for g in heur:
+        g.close()
     seq = fresh()
     ensemble_advance(seq, warm)
     t_seq, st_seq = timed(seq, nsteps, False)
@@ -503,6 +514,9 @@ def ensemble_arm(args, rank, world, local_rank):
                        "cells": sum(cells), "dt_h": 0.1},
             "sequential_member_timesteps_per_s": member_steps / (t_seq * 1e-3),
             "concurrency_speedup": t_seq / t_conc,
+            "heuristic_shapes_member_timesteps_per_s": member_steps / (t_heur * 1e-3),
+            "autotune_speedup": t_heur / t_conc,
+            "tile_shapes": {"x".join(map(str, k[::-1])): v for k, v in sorted(shapes.items())},
             "newton_iters_total": newton,
             "cell_newton_updates_per_s": cell_updates * world / (t_conc * 1e-3),
         }), flush=True)

@@ -347,6 +347,20 @@ int pfgpu_mg_levels(pfgpu_handle *h, int *levels, int *dims, int max_levels);
 #define PFGPU_KERNEL_COLOUR_SWEEP 6
 int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double *bytes);
 
+/* Autotuner of the stencil launches (no counterpart in the reference):
+ * times candidate thread-block shapes (bx, by) of the residual, Jacobian
+ * and matvec kernels on this handle's grid, `reps` launches each on its
+ * current state, and keeps the fastest (the built-in heuristic unless a
+ * shape is clearly faster).  Choices are cached per grid size, precision
+ * and kernel variant for the life of the process, so later handles of the
+ * same size (ensemble members) take them without timing.  shapes (6 ints,
+ * may be NULL) receives bx, by of the residual, Jacobian and matvec; 0, 0
+ * means the heuristic.  Results are unchanged bit for bit (every cell's
+ * arithmetic is independent of the block shape).  The timing overwrites
+ * the assembled Jacobian and preconditioner, which the next solve or
+ * pfgpu_pc_setup rebuilds. */
+int pfgpu_autotune(pfgpu_handle *h, int reps, int *shapes);
+
 /* Residual F(p) without any device allocation, for callers that may not call
  * the CUDA allocator (a host framework with a fixed device-memory budget
  * reserved at start-up, or a latency-critical loop where cudaMalloc/cudaFree

@@ -14,6 +14,9 @@
 #include <algorithm>
 #include <array>
 #include <climits>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
@@ -367,10 +370,10 @@ static void matvec_impl(pfgpu_handle *h, const double *x, double *y) {
   }
   if (h->mixed) {
     JacIn<float> J{h->Jf.c, h->Jf.w, h->Jf.e, h->Jf.s, h->Jf.n, h->Jf.l, h->Jf.u};
-    launch_matvec7<float>(h->nx, h->ny, h->nz, J, x, y, h->st);
+    launch_matvec7<float>(h->nx, h->ny, h->nz, J, x, y, h->st, h->P.tile[2]);
   } else {
     JacIn<double> J{h->Jd.c, h->Jd.w, h->Jd.e, h->Jd.s, h->Jd.n, h->Jd.l, h->Jd.u};
-    launch_matvec7<double>(h->nx, h->ny, h->nz, J, x, y, h->st);
+    launch_matvec7<double>(h->nx, h->ny, h->nz, J, x, y, h->st, h->P.tile[2]);
   }
   h->launches++;
 }
@@ -2151,6 +2154,122 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
   h->jac_valid = 0;
   return PFGPU_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Autotuner of the stencil launches' thread-block shapes
+// ---------------------------------------------------------------------------
+// Candidate shapes (bx, by): bx a multiple of the warp width, bx * by within
+// the kernel's launch bound (256 threads for the residual and the matvec,
+// 128 for the Jacobian).  The choice depends on the grid (a block wider than
+// nx idles lanes, a narrow one multiplies the blocks) and is cached per grid
+// size, precision and kernel variant for the life of the process.
+namespace {
+struct TuneKey {
+  int nx, ny, nz, mixed, surf;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(nx, ny, nz, mixed, surf) < std::tie(o.nx, o.ny, o.nz, o.mixed, o.surf);
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, std::array<int, 6>> g_tune_cache;
+}  // namespace
+
+int pfgpu_autotune(pfgpu_handle *h, int reps, int *shapes) {
+  if (!h || reps < 1) { set_err("pfgpu_autotune: bad argument"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  const int surf = (h->P.tfg_xs || h->P.bc_type[5] >= 2) ? 1 : 0;
+  const TuneKey key{h->nx, h->ny, h->nz, h->mixed ? 1 : 0, surf};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      for (int q = 0; q < 3; q++) {
+        h->P.tile[q][0] = it->second[2 * q];
+        h->P.tile[q][1] = it->second[2 * q + 1];
+      }
+      if (shapes) std::copy(it->second.begin(), it->second.end(), shapes);
+      return PFGPU_OK;
+    }
+  }
+  static const int cand256[][2] = {{32, 8}, {64, 4}, {128, 2}, {256, 1}, {32, 4}, {64, 2},
+                                   {128, 1}};
+  static const int cand128[][2] = {{32, 4}, {64, 2}, {128, 1}, {32, 2}, {64, 1}, {32, 1}};
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  const double dt = 0.05;
+  vg_state(h, h->u, false);
+  auto run = [&](int kernel) {
+    if (kernel == 0) {
+      launch_residual(h->P, h->u, h->p_old, h->s_old, h->kr, h->sat, dt, h->fval, h->st);
+    } else if (kernel == 1) {
+      if (h->mixed) {
+        PCOut<float> M{h->mgf.L[0].a[0], h->mgf.L[0].a[1], h->mgf.L[0].a[2], h->mgf.L[0].a[3],
+                       h->mgf.L[0].wg};
+        launch_jacobian<float, float>(h->P, h->u, h->kr, h->dkr, h->sat, h->dsat, dt, h->Jf, M,
+                                      h->st);
+      } else {
+        PCOut<double> M{h->mgd.L[0].a[0], h->mgd.L[0].a[1], h->mgd.L[0].a[2], h->mgd.L[0].a[3],
+                        h->mgd.L[0].wg};
+        launch_jacobian<double, double>(h->P, h->u, h->kr, h->dkr, h->sat, h->dsat, dt, h->Jd,
+                                        M, h->st);
+      }
+    } else {
+      matvec_impl(h, h->u, h->bb);
+    }
+    h->launches++;
+  };
+  auto time_of = [&](int kernel) -> float {
+    run(kernel);  // warm-up
+    cudaEventRecord(e0, h->st);
+    for (int r = 0; r < reps; r++) run(kernel);
+    cudaEventRecord(e1, h->st);
+    cudaEventSynchronize(e1);
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    return ms;
+  };
+  // the Jacobian first: the matvec then reads the J it assembled
+  const int order[3] = {1, 0, 2};
+  for (int oi = 0; oi < 3; oi++) {
+    const int q = order[oi];
+    const int (*cand)[2] = q == 1 ? cand128 : cand256;
+    const int nc = q == 1 ? (int)(sizeof(cand128) / sizeof(cand128[0]))
+                          : (int)(sizeof(cand256) / sizeof(cand256[0]));
+    h->P.tile[q][0] = h->P.tile[q][1] = 0;
+    float best = time_of(q);
+    int bx = 0, by = 0;
+    for (int c = 0; c < nc; c++) {
+      if (cand[c][1] > 1 && cand[c][1] > h->ny) continue;  // rows beyond the grid
+      h->P.tile[q][0] = cand[c][0];
+      h->P.tile[q][1] = cand[c][1];
+      const float t = time_of(q);
+      // a shape replaces the heuristic only when it is clearly faster
+      if (t < (bx ? best : 0.97f * best)) {
+        best = t;
+        bx = cand[c][0];
+        by = cand[c][1];
+      }
+    }
+    h->P.tile[q][0] = bx;
+    h->P.tile[q][1] = by;
+  }
+  CK(cudaGetLastError());
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  // the timing runs overwrote J and the preconditioner matrix
+  h->jac_valid = 0;
+  h->pc_ready = false;
+  std::array<int, 6> out{h->P.tile[0][0], h->P.tile[0][1], h->P.tile[1][0],
+                         h->P.tile[1][1], h->P.tile[2][0], h->P.tile[2][1]};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune_cache[key] = out;
+  }
+  if (shapes) std::copy(out.begin(), out.end(), shapes);
+  return PFGPU_OK;
+}
+
 
 void *pfgpu_stream(pfgpu_handle *h) { return h ? (void *)h->st : nullptr; }
 

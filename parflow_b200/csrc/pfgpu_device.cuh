@@ -41,6 +41,10 @@ struct DevProblem {
   // old pressure of the step (dense interior), read by the diffusive terms'
   // slope magnitude in the residual and the Jacobian
   const double *ov_pold;
+  // thread-block shapes (bx, by) of the residual, Jacobian and matvec
+  // launches picked by pfgpu_autotune; (0, 0) = the default heuristic.
+  // Host-side launch configuration only: no kernel reads it.
+  int tile[3][2];
 };
 
 // Gravity terms of the x face between columns i and i+1 (and of the y face

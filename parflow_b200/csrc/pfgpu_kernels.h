@@ -41,9 +41,10 @@ template <typename TJ, typename TP>
 void launch_jacobian(const DevProblem &P, const double *p, const double *kr, const double *dkr,
                      const double *sat, const double *dsat, double dt, JacOut<TJ> J,
                      PCOut<TP> M, cudaStream_t st);
+// tile: a tuned thread-block shape (bx, by) or null for the heuristic
 template <typename TJ>
 void launch_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double *y,
-                    cudaStream_t st);
+                    cudaStream_t st, const int *tile = nullptr);
 
 // ---- multigrid (mg_kernels.cu) --------------------------------------------
 template <typename T>

@@ -595,6 +595,16 @@ static inline void shape(int nx, int ny, int nz, int threads, dim3 &grid, dim3 &
   block = dim3(bx, by, 1);
   grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, nz);
 }
+// the tuned shape (bx, by) when one is set, else the heuristic
+static inline void shape_tuned(int nx, int ny, int nz, int threads, const int tile[2],
+                               dim3 &grid, dim3 &block) {
+  if (!tile || tile[0] <= 0 || tile[1] <= 0) {
+    shape(nx, ny, nz, threads, grid, block);
+    return;
+  }
+  block = dim3(tile[0], tile[1], 1);
+  grid = dim3((nx + tile[0] - 1) / tile[0], (ny + tile[1] - 1) / tile[1], nz);
+}
 
 void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
                    double *dsat, cudaStream_t st) {
@@ -609,7 +619,7 @@ void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      const double *s_old, const double *kr, const double *sat, double dt,
                      double *f, cudaStream_t st) {
   dim3 g, b;
-  shape(P.nx, P.ny, P.nz, 256, g, b);
+  shape_tuned(P.nx, P.ny, P.nz, 256, P.tile[0], g, b);
   if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
     launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
   else
@@ -621,7 +631,7 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
                      const double *dkr, const double *sat, const double *dsat, double dt,
                      JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
   dim3 g, b;
-  shape(P.nx, P.ny, P.nz, 128, g, b);
+  shape_tuned(P.nx, P.ny, P.nz, 128, P.tile[1], g, b);
   if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
     launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J, M);
   else
@@ -631,9 +641,9 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
 
 template <typename TJ>
 void launch_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *x, double *y,
-                    cudaStream_t st) {
+                    cudaStream_t st, const int *tile) {
   dim3 g, b;
-  shape(nx, ny, nz, 256, g, b);
+  shape_tuned(nx, ny, nz, 256, tile, g, b);
   launch_pdl(k_matvec7<TJ>, dim3(g), dim3(b), st, nx, ny, nz, J, x, y);
 }
 
@@ -645,8 +655,8 @@ template void launch_jacobian<float, float>(const DevProblem &, const double *, 
                                             const double *, const double *, const double *,
                                             double, JacOut<float>, PCOut<float>, cudaStream_t);
 template void launch_matvec7<double>(int, int, int, JacIn<double>, const double *, double *,
-                                     cudaStream_t);
+                                     cudaStream_t, const int *);
 template void launch_matvec7<float>(int, int, int, JacIn<float>, const double *, double *,
-                                    cudaStream_t);
+                                    cudaStream_t, const int *);
 
 }  // namespace pfgpu

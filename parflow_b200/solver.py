@@ -354,6 +354,15 @@ class RichardsGPU:
                 "time_kernel")
         return ms.value, by.value
 
+    def autotune(self, reps: int = 10) -> dict:
+        """Pick the thread-block shapes of the residual, Jacobian and matvec
+        launches for this grid (pfgpu_autotune); returns them, (0, 0) being
+        the built-in heuristic."""
+        out = (C.c_int * 6)()
+        L.check(self.lib.pfgpu_autotune(self.h, reps, out), "autotune")
+        return {"residual": (out[0], out[1]), "jacobian": (out[2], out[3]),
+                "matvec": (out[4], out[5])}
+
     def kernel_launches(self) -> int:
         return int(self.lib.pfgpu_kernel_launches(self.h))
 
