@@ -239,6 +239,16 @@ int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old
 int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt,
                           const double *x, double *y);
 
+/* Solver.Nonlinear.UseJacobian and Solver.Nonlinear.DerivativeEpsilon
+ * (kinsol_nonlin_solver.c:860-885): use_jacobian = 1 (the default of this
+ * library) gives GMRES the analytic Jacobian; 0 the difference quotient
+ * J v = (F(u + sigma v) - F(u)) / sigma of KINSpgmrAtimesDQ
+ * (kinsol/kinspgmr.c:481-518) with sigma from sqrt(derivative_epsilon), one
+ * residual evaluation per product (counted in fevals); the preconditioner
+ * keeps the analytic symmetric part.  Not available with an overland face
+ * (the solves return PFGPU_ERR_STATE). */
+int pfgpu_set_jacobian_mode(pfgpu_handle *h, int use_jacobian, double derivative_epsilon);
+
 /* Sets the old pressure (ParFlow layout) that the Jacobian of
  * pfgpu_jacobian_matvec and pfgpu_pc_setup reads: the old_pressure argument
  * of RichardsJacobianEval (richards_jacobian_eval.c:217), used only by the

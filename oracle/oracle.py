@@ -41,7 +41,8 @@ class Settings(C.Structure):
                 ("eta_choice", C.c_int),
                 ("eta_value", C.c_double), ("eta_alpha", C.c_double), ("eta_gamma", C.c_double),
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
-                ("wjacobi_weight", C.c_double)]
+                ("wjacobi_weight", C.c_double),
+                ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double)]
 
 
 class Stats(C.Structure):
@@ -135,6 +136,8 @@ class Oracle:
         S.mg_max_levels = s.mg_max_levels
         S.mg_smoother = 0 if s.mg_smoother == "RedBlackGSPoint" else 1
         S.wjacobi_weight = 1.0
+        S.use_jacobian = 1 if s.use_jacobian else 0
+        S.derivative_epsilon = s.derivative_epsilon
         self.S = S
 
     def set_time(self, t: float):

@@ -1543,6 +1543,8 @@ typedef struct {
   double *PC[5];   /* C E N U, and the W ghost plane of the i = 0 column */
   pfo_mg *mg;
   pfo_stats *stats;
+  const double *fval;   /* F at the Newton iterate (difference quotients) */
+  double *dq_u, *dq_f;  /* difference-quotient point and its F */
 } kctx;
 
 static double dot(const double *a, const double *b, long n)
@@ -1550,6 +1552,14 @@ static double dot(const double *a, const double *b, long n)
   double s = 0.0;
   for (long i = 0; i < n; i++)
     s += a[i] * b[i];
+  return s;
+}
+
+static double l1norm(const double *a, long n)
+{
+  double s = 0.0;
+  for (long i = 0; i < n; i++)
+    s += fabs(a[i]);
   return s;
 }
 
@@ -1578,6 +1588,30 @@ static void precond(kctx *kc, double *z)
 }
 
 /* SpgmrSolve with x0 = 0, right preconditioning, MGS (KS/spgmr.c:168-450) */
+/* KINSpgmrAtimesDQ (KS/kinspgmr.c:481-518) with uscale = 1:
+ * J v ~ (F(u + sigma v) - F(u)) / sigma, sigma from Brown and Saad,
+ * sign(u.v) sqrt(DerivativeEpsilon) max(|u.v|, |v|_1) / (v.v) */
+static void atimes_dq(kctx *kc, const double *u, const double *v, double *z)
+{
+  long N = kc->N;
+  double sutsv = dot(u, v, N);
+  double vtv = dot(v, v, N);
+  double sq1norm = l1norm(v, N);
+  double sign = (sutsv >= 0.0) ? 1.0 : -1.0;
+  double sqrt_relfunc = sqrt(kc->st->derivative_epsilon > 0.0 ? kc->st->derivative_epsilon
+                                                              : DBL_EPSILON);
+  double sigma = sign * sqrt_relfunc * (fabs(sutsv) > sq1norm ? fabs(sutsv) : sq1norm) / vtv;
+  double sigma_inv = 1.0 / sigma;
+  /* N_VLinearSum(1, u, sigma, v): sigma v + u */
+  for (long q = 0; q < N; q++)
+    kc->dq_u[q] = sigma * v[q] + u[q];
+  feval(kc, kc->dq_u, kc->dq_f);
+  /* N_VLinearSum(sigma_inv, F(u + sigma v), -sigma_inv, F(u)): the a == -b
+   * case, sigma_inv (x - y) */
+  for (long q = 0; q < N; q++)
+    z[q] = sigma_inv * (kc->dq_f[q] - kc->fval[q]);
+}
+
 static int spgmr(kctx *kc, double *x, const double *b, double delta,
                  const double *u, int *jac_current, double *res_norm)
 {
@@ -1617,12 +1651,17 @@ static int spgmr(kctx *kc, double *x, const double *b, double delta,
       krydim = l + 1;
       memcpy(vtemp, V[l], N * sizeof(double));
       precond(kc, vtemp);
-      if (!*jac_current)
+      if (!kc->st->use_jacobian)
+        atimes_dq(kc, u, vtemp, V[l + 1]);
+      else
       {
-        pfo_jacobian(kc->pb, kc->dt, u, 0, kc->J);
-        *jac_current = 1;
+        if (!*jac_current)
+        {
+          pfo_jacobian(kc->pb, kc->dt, u, 0, kc->J);
+          *jac_current = 1;
+        }
+        pfo_matvec7(kc->pb, kc->J, vtemp, V[l + 1]);
       }
-      pfo_matvec7(kc->pb, kc->J, vtemp, V[l + 1]);
       /* ModifiedGS (KS/iterativ.c:30-86) */
       {
         int k = l + 1;
@@ -1788,6 +1827,9 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
   double *unew = (double*)malloc(N * sizeof(double));
   double *pp = (double*)malloc(N * sizeof(double));
   double *bb = (double*)malloc(N * sizeof(double));
+  kc.fval = fval;
+  kc.dq_u = (double*)malloc(N * sizeof(double));
+  kc.dq_f = (double*)malloc(N * sizeof(double));
   const double uround = DBL_EPSILON;
   double fnormtol = st->residual_tol, scsteptol = st->step_tol;
   int mxiter = st->max_iter;
@@ -1845,13 +1887,19 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
       ret = 8;
       break;
     }
-    if (!jac_current)
+    /* sJpnorm, sfdotJp (KS/kinspgmr.c:384-398): J p by KINSpgmrAtimes, the
+     * analytic matvec or the difference quotient */
+    if (!st->use_jacobian)
+      atimes_dq(&kc, uu, pp, bb);
+    else
     {
-      pfo_jacobian(pb, dt, uu, 0, kc.J);
-      jac_current = 1;
+      if (!jac_current)
+      {
+        pfo_jacobian(pb, dt, uu, 0, kc.J);
+        jac_current = 1;
+      }
+      pfo_matvec7(pb, kc.J, pp, bb);
     }
-    /* sJpnorm, sfdotJp (KS/kinspgmr.c:422-431) */
-    pfo_matvec7(pb, kc.J, pp, bb);
     sJpnorm = sqrt(dot(bb, bb, N));
     sfdotJp = dot(fval, bb, N);
 
@@ -2026,5 +2074,5 @@ out:
   for (int s = 0; s < 7; s++) free(kc.J[s]);
   for (int s = 0; s < 5; s++) free(kc.PC[s]);
   pfo_mg_destroy(kc.mg);
-  free(fval); free(unew); free(pp); free(bb);
+  free(fval); free(unew); free(pp); free(bb); free(kc.dq_u); free(kc.dq_f);
 }

@@ -54,6 +54,9 @@ typedef struct {
   int mg_max_levels;
   int mg_smoother;                 /* 0 = RBGS (symmetric), 1 = WJacobi */
   double wjacobi_weight;
+  int use_jacobian;                /* Solver.Nonlinear.UseJacobian: 1 analytic J v,
+                                    * 0 KINSOL's difference quotient */
+  double derivative_epsilon;       /* Solver.Nonlinear.DerivativeEpsilon */
 } pfo_settings;
 
 typedef struct {

@@ -78,6 +78,15 @@ def seepage_small() -> RichardsProblem:
     return p
 
 
+def dq_small() -> RichardsProblem:
+    """The reference's default Solver.Nonlinear.UseJacobian False: GMRES on
+    KINSOL's difference-quotient J v (the preconditioner keeps the analytic
+    symmetric part), config-0 physics with per-cell van Genuchten files."""
+    p = configs.hetero(nx=14, ny=12, nz=9, nsteps=2, seed=23,
+                       solver=SolverSettings(use_jacobian=False))
+    return p
+
+
 def tfg_small() -> RichardsProblem:
     """Terrain-following slopes in the subsurface fluxes without overland
     flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""
@@ -89,7 +98,7 @@ def tfg_small() -> RichardsProblem:
 
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
-          "overland_flow_small", "seepage_small"]
+          "overland_flow_small", "seepage_small", "dq_small"]
 
 
 def get(name: str) -> RichardsProblem:

@@ -277,6 +277,21 @@ struct OpInitNorms {
   }
 };
 
+// <u, v>, <v, v> and sum |v| of a difference-quotient product (KINSpgmrAtimesDQ)
+struct OpDQ {
+  static constexpr int K = 3;
+  const double *u, *v;
+  double *dst[K];
+  __device__ void setup() {}
+  __device__ void acc(long long i, double *s) const {
+    const double ui = u[i], vi = v[i];
+    s[0] = s[0] + ui * vi;
+    s[1] = s[1] + vi * vi;
+    s[2] = s[2] + fabs(vi);
+  }
+  __device__ static double comb(int, double x, double y) { return comb_sum(x, y); }
+};
+
 template <typename Op>
 static void reduce_multi(Op op, long long n, ReduceBuf rb, cudaStream_t st) {
   long long need = (n + RED_THREADS - 1) / RED_THREADS;
@@ -314,6 +329,56 @@ void launch_init_norms(const double *u, const double *f, long long n, double *d_
                        double *d_fmax, double *d_f2, ReduceBuf rb, cudaStream_t st) {
   OpInitNorms op{u, f, {d_u2, d_fmax, d_f2}};
   reduce_multi(op, n, rb, st);
+}
+
+// ---- difference-quotient J v (kinspgmr.c:481-518, uscale = 1) ---------------
+// d[0..2] = <u, v>, <v, v>, |v|_1 from OpDQ; writes sigma to d[3] and 1/sigma
+// to d[4]: sigma = sign(<u, v>) sqrt_relfunc max(|<u, v>|, |v|_1) / <v, v>
+__global__ void k_dq_sigma(double *d, double sqrt_relfunc) {
+  pdl_enter();
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    const double sutsv = d[0], vtv = d[1], sq1norm = d[2];
+    const double sign = (sutsv >= 0.0) ? 1.0 : -1.0;
+    const double a = fabs(sutsv);
+    const double sigma = sign * sqrt_relfunc * (a > sq1norm ? a : sq1norm) / vtv;
+    d[3] = sigma;
+    d[4] = 1.0 / sigma;
+  }
+}
+// w = sigma v + u
+__global__ void k_dq_point(double *__restrict__ w, const double *__restrict__ u,
+                           const double *__restrict__ v, const double *__restrict__ d,
+                           long long n) {
+  pdl_enter();
+  const double sigma = d[3];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    w[i] = sigma * v[i] + u[i];
+}
+// z = (1/sigma) (fw - f)
+__global__ void k_dq_finish(double *__restrict__ z, const double *__restrict__ fw,
+                            const double *__restrict__ f, const double *__restrict__ d,
+                            long long n) {
+  pdl_enter();
+  const double sigma_inv = d[4];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    z[i] = sigma_inv * (fw[i] - f[i]);
+}
+static inline int grid_for(long long n);
+void launch_dq_prepare(const double *u, const double *v, long long n, double *d,
+                       double sqrt_relfunc, ReduceBuf rb, cudaStream_t st) {
+  OpDQ op{u, v, {d, d + 1, d + 2}};
+  reduce_multi(op, n, rb, st);
+  launch_pdl(k_dq_sigma, dim3(1), dim3(32), st, d, sqrt_relfunc);
+}
+void launch_dq_point(double *w, const double *u, const double *v, const double *d, long long n,
+                     cudaStream_t st) {
+  launch_pdl(k_dq_point, dim3(grid_for(n)), dim3(256), st, w, u, v, d, n);
+}
+void launch_dq_finish(double *z, const double *fw, const double *f, const double *d,
+                      long long n, cudaStream_t st) {
+  launch_pdl(k_dq_finish, dim3(grid_for(n)), dim3(256), st, z, fw, f, d, n);
 }
 
 // ---- element-wise ---------------------------------------------------------

@@ -62,7 +62,8 @@ enum {
   D_JP2,         // <Jp, Jp>
   D_FJP,         // <f, Jp>
   D_U2,          // <u, u>
-  D_COUNT
+  D_COUNT,
+  D_DQ = 40      // five slots of the difference-quotient product (launch_dq_prepare)
 };
 
 struct Handle;
@@ -170,6 +171,11 @@ struct pfgpu_handle {
   bool pc_ready = false;
   long long launches = 0;
   int jac_valid = 0;
+  // Solver.Nonlinear.UseJacobian (1: analytic J v; 0: KINSOL's difference
+  // quotient with sqrt(DerivativeEpsilon)) and its two work vectors
+  int use_jacobian = 1;
+  double sqrt_relfunc = 0.0;
+  double *dq_w = nullptr, *dq_f = nullptr;
   int *kerr = nullptr;   // device error word of the pipelined kernels
   int *hkerr = nullptr;  // pinned host mirror
   // discrete adjoint: recorded trajectory p_0 .. p_len (dense, device) and
@@ -548,6 +554,28 @@ static void pc_setup_dense(pfgpu_handle *h, const double *u, double dt, bool als
 // reuses the norm of f from the line search) the start needs no reduction and
 // no host synchronisation; V0 = b / ||b|| is then formed in one pass.  The
 // solution x is written only on return, as M^{-1} (V y) (x0 = 0).
+// z = J(u) v: the analytic matvec (J assembled at u on first use), or the
+// difference quotient (F(u + sigma v) - F(u)) / sigma of KINSpgmrAtimesDQ
+// (kinsol/kinspgmr.c:481-518, uscale = 1) with F(u) in h->fval
+static void atimes(pfgpu_handle *h, const double *u, double dt, const double *v, double *z,
+                   pfgpu_stats *stats) {
+  if (h->use_jacobian) {
+    if (!h->jac_valid) {
+      assemble(h, u, dt, true, false, true);
+      h->jac_valid = 1;
+    }
+    matvec(h, v, z);
+    return;
+  }
+  launch_dq_prepare(u, v, h->N, h->dsc + D_DQ, h->sqrt_relfunc, h->rb, h->st);
+  launch_dq_point(h->dq_w, u, v, h->dsc + D_DQ, h->N, h->st);
+  h->launches += 3;
+  feval(h, h->dq_w, dt, h->dq_f);
+  stats->fevals++;
+  launch_dq_finish(z, h->dq_f, h->fval, h->dsc + D_DQ, h->N, h->st);
+  h->launches++;
+}
+
 static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
                  const double *bn2_dev, double bnorm, double delta, const double *u, double dt,
                  pfgpu_stats *stats, int *status) {
@@ -597,11 +625,7 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
       // vtemp = M^{-1} V[l] (the preconditioner reads V[l], writes vtemp)
       if (pc_apply_dense(h, h->V[l], h->vtemp)) return PFGPU_ERR_CUDA;
       stats->pc_solves++;
-      if (!h->jac_valid) {
-        assemble(h, u, dt, true, false, true);
-        h->jac_valid = 1;
-      }
-      matvec(h, h->vtemp, h->V[l + 1]);
+      atimes(h, u, dt, h->vtemp, h->V[l + 1], stats);
       // ModifiedGS (iterativ.c:30-86): <vk,vk> and h(0) in one pass, then each
       // projection vk -= h(i) v_i fused with the next dot (h(i+1), or the
       // new <vk,vk> after the last); same per-element arithmetic
@@ -730,7 +754,7 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
     if (eps < epsmin) eps = epsmin;
     // preconditioner setup every iteration (msbpre = 1); J at the same u
     h->jac_valid = 0;
-    pc_setup_dense(h, u, dt, true, true);
+    pc_setup_dense(h, u, dt, h->use_jacobian != 0, true);
     stats->pc_setups++;
     // b = -f; its norm is the fnorm of the last residual evaluation
     int sstat = 0;
@@ -741,12 +765,9 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
       ret = 8;
       break;
     }
-    if (!h->jac_valid) {
-      assemble(h, u, dt, true, false, true);
-      h->jac_valid = 1;
-    }
-    // sJpnorm, sfdotJp (kinspgmr.c:422-431) and line-search inputs
-    matvec(h, h->pp, h->bb);
+    // sJpnorm, sfdotJp (kinspgmr.c:384-398) and line-search inputs; J p by
+    // KINSpgmrAtimes, analytic or by difference quotient
+    atimes(h, u, dt, h->pp, h->bb, stats);
     launch_linesearch_inputs(h->bb, h->fval, h->pp, u, N, dsc + D_JP2, dsc + D_FJP, dsc + D_P2,
                              dsc + D_PLEN, h->rb, h->st);
     h->launches++;
@@ -906,6 +927,14 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   return (ret == 1 || ret == 2) ? PFGPU_OK : PFGPU_NOT_CONVERGED;
 }
 static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
+  const int ov = h->P.bc_type[5];
+  if (!h->use_jacobian && (ov == PFGPU_BC_OVERLAND_KIN || ov == PFGPU_BC_OVERLAND_DIFF ||
+                           ov == PFGPU_BC_OVERLAND)) {
+    // without the analytic Jacobian the reference builds the overland
+    // preconditioner terms in another form (richards_jacobian_eval.c:1244-1283)
+    set_err("difference-quotient J v (UseJacobian False) with an overland face is not available");
+    return PFGPU_ERR_STATE;
+  }
   const int m = ph_begin(h);
   const int rc = newton_impl(h, dt, stats);
   ph_end(h, m, PH_NEWTON);
@@ -1174,6 +1203,8 @@ static void destroy_impl(pfgpu_handle *h) {
               h->pacc[q], h->pcnt[q], h->pcnt[q] ? h->pacc[q] / h->pcnt[q] : 0.0);
   }
   for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
+  cudaFree(h->dq_w);
+  cudaFree(h->dq_f);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   cudaFree(h->hist);
   cudaFree(h->adj);
@@ -1773,6 +1804,23 @@ int pfgpu_pc_setup(pfgpu_handle *h, const double *p, double dt) {
   pc_setup_dense(h, h->unew, dt, false);
   h->jac_valid = 0;
   CK(cudaStreamSynchronize(h->st));
+  return PFGPU_OK;
+}
+
+int pfgpu_set_jacobian_mode(pfgpu_handle *h, int use_jacobian, double derivative_epsilon) {
+  if (!h || (use_jacobian != 0 && use_jacobian != 1) || derivative_epsilon < 0.0) {
+    set_err("pfgpu_set_jacobian_mode: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  if (!use_jacobian && (!h->dq_w || !h->dq_f)) {
+    if (dalloc(&h->dq_w, h->N) || dalloc(&h->dq_f, h->N)) return PFGPU_ERR_NOMEM;
+  }
+  h->use_jacobian = use_jacobian;
+  // sqrt_relfunc (kinsol.c:516-531): sqrt of DerivativeEpsilon, or of the
+  // unit roundoff when it is 0
+  h->sqrt_relfunc = sqrt(derivative_epsilon > 0.0 ? derivative_epsilon : DBL_EPSILON);
+  h->jac_valid = 0;
   return PFGPU_OK;
 }
 

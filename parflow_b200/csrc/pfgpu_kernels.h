@@ -281,6 +281,14 @@ void launch_axpy_dev(double *y, const double *x, const double *s, double sign, l
                      cudaStream_t st);
 // y = a*x + b*y (host scalars)
 void launch_axpby(double *y, const double *x, double a, double b, long long n, cudaStream_t st);
+// difference-quotient J v (KINSpgmrAtimesDQ): the sums and sigma into d[0..4],
+// the point u + sigma v, and (F(u + sigma v) - F(u)) / sigma
+void launch_dq_prepare(const double *u, const double *v, long long n, double *d,
+                       double sqrt_relfunc, ReduceBuf rb, cudaStream_t st);
+void launch_dq_point(double *w, const double *u, const double *v, const double *d, long long n,
+                     cudaStream_t st);
+void launch_dq_finish(double *z, const double *fw, const double *f, const double *d,
+                      long long n, cudaStream_t st);
 // z = x + a*y
 void launch_xpay(double *z, const double *x, double a, const double *y, long long n,
                  cudaStream_t st);

@@ -109,6 +109,7 @@ class SolverSettings:
     eta_gamma: float = 0.9
     globalization: str = "LineSearch"
     use_jacobian: bool = True
+    derivative_epsilon: float = 1e-7  # Solver.Nonlinear.DerivativeEpsilon (J v by differences)
     preconditioner: str = "MGSemi"
     pc_matrix_type: str = "PFSymmetric"
     mg_max_iter: int = 1
@@ -461,6 +462,7 @@ class RichardsProblem:
             k["Solver.Nonlinear.EtaAlpha"] = s.eta_alpha
             k["Solver.Nonlinear.EtaGamma"] = s.eta_gamma
         k["Solver.Nonlinear.UseJacobian"] = bool(s.use_jacobian)
+        k["Solver.Nonlinear.DerivativeEpsilon"] = float(s.derivative_epsilon)
         k["Solver.Nonlinear.Globalization"] = s.globalization
         k["Solver.Linear.KrylovDimension"] = s.krylov_dim
         k["Solver.Linear.MaxRestarts"] = s.max_restarts

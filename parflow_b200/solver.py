@@ -91,6 +91,9 @@ class RichardsGPU:
         self._vg_scalar = {L.FIELD_VG_ALPHA: d.vg_alpha, L.FIELD_VG_N: d.vg_n,
                            L.FIELD_S_RES: d.s_res, L.FIELD_S_SAT: d.s_sat}
         self._vg_cells = set()
+        if not s.use_jacobian:
+            L.check(self.lib.pfgpu_set_jacobian_mode(self.h, 0, s.derivative_epsilon),
+                    "set_jacobian_mode")
         self._upload_fields()
         self.set_time(prob.start_time + prob.dt)
 

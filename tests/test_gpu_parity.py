@@ -33,6 +33,13 @@ def gpu():
     return solver
 
 
+def _npc(g):
+    """Preconditioner dumps paired with a matvec dump (the preconditioner is
+    set up at the matvec's pressure); a run on difference quotients has no
+    matvec dumps."""
+    return min(len(g["pc_in"]), len(g["mv_p"]))
+
+
 def _pold(g, i):
     """Old pressure of matvec dump i (fixtures made after it was dumped)."""
     return g["mv_pold"][i] if "mv_pold" in g else None
@@ -83,7 +90,7 @@ def test_jacobian_matvec_vs_reference(name, golden, gpu):
 def test_preconditioner_vs_reference(name, golden, gpu):
     g = golden(name)
     s = gpu.RichardsGPU(cases.get(name))
-    for i in range(len(g["pc_in"])):
+    for i in range(_npc(g)):
         s.set_time(g["mv_time"][i])
         s.pc_setup(g["mv_p"][i], g["mv_dt"][i], _pold(g, i))
         z = s.pc_apply(g["pc_in"][i])
@@ -102,7 +109,7 @@ PC_TOL = {"mixed": 1e-4, "mixed16": 5e-3}
 def test_mixed_preconditioner_close(name, precision, golden, gpu):
     g = golden(name)
     s = gpu.RichardsGPU(cases.get(name), precision=precision)
-    for i in range(len(g["pc_in"])):
+    for i in range(_npc(g)):
         s.set_time(g["mv_time"][i])
         s.pc_setup(g["mv_p"][i], g["mv_dt"][i], _pold(g, i))
         z = s.pc_apply(g["pc_in"][i])
@@ -197,7 +204,7 @@ def test_preconditioner_grid_levels_vs_reference(name, golden, gpu, monkeypatch)
     monkeypatch.setenv("PFGPU_TAIL_CELLS", "16")
     g = golden(name)
     s = gpu.RichardsGPU(cases.get(name))
-    for i in range(len(g["pc_in"])):
+    for i in range(_npc(g)):
         s.set_time(g["mv_time"][i])
         s.pc_setup(g["mv_p"][i], g["mv_dt"][i], _pold(g, i))
         z = s.pc_apply(g["pc_in"][i])
@@ -228,3 +235,25 @@ def test_overland_types_vs_oracle(gpu, precision, kind):
             assert st_g[t].nonlin_iters == st_o[t].nni and st_g[t].lin_iters == st_o[t].nli
         else:
             assert err <= 1e-8, (t, err)
+
+
+def test_difference_quotient_counts_fevals(gpu, golden):
+    """UseJacobian False: every GMRES product (and the line search's J p) is
+    one more residual evaluation, as the reference counts them."""
+    g = golden("dq_small")
+    s = gpu.RichardsGPU(cases.get("dq_small"))
+    _, sts = s.run()
+    for t, st in enumerate(sts):
+        assert st.fevals == g["counts"][t, 2], (t, st.fevals, g["counts"][t, 2])
+        assert st.pc_solves == g["counts"][t, 4], (t, st.pc_solves)
+
+
+def test_difference_quotient_rejects_overland(gpu):
+    from parflow_b200 import lib as L
+    from parflow_b200.problem import SolverSettings
+
+    prob = cases.overland_small()
+    prob.solver = SolverSettings(use_jacobian=False)
+    s = gpu.RichardsGPU(prob)
+    with pytest.raises(L.PfgpuError):
+        s.run(1)
