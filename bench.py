@@ -113,6 +113,7 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 def _workloads():
     from parflow_b200 import configs
+    from parflow_b200.problem import BC_OVERLAND, BC_OVERLAND_DIFF
 
     return {
         # the bench line: heterogeneous box, 13.1M cells
@@ -126,6 +127,22 @@ def _workloads():
             "build": lambda nx, ny, nz, nsteps: configs.overland(nx=nx, ny=ny, nz=nz, nsteps=nsteps),
             "dims": (256, 256, 20), "sample": (64, 64, 20),
             "label": "overland hillslope 256x256x20 (1.31M cells), kinematic overland flow, "
+                     "terrain-following grid, rain 2 h on / 2 h off",
+            "config": {"dt_h": 0.25, "dx_m": 10.0, "dz_m": 0.2, "mannings": 5.5e-5}},
+        # config 1 with the OverlandFlow patch type (overlandflow_eval.c)
+        "overland_flow": {
+            "build": lambda nx, ny, nz, nsteps: configs.overland(nx=nx, ny=ny, nz=nz, nsteps=nsteps,
+                                                                kind=BC_OVERLAND),
+            "dims": (256, 256, 20), "sample": (64, 64, 20),
+            "label": "overland hillslope 256x256x20 (1.31M cells), OverlandFlow overland flow, "
+                     "terrain-following grid, rain 2 h on / 2 h off",
+            "config": {"dt_h": 0.25, "dx_m": 10.0, "dz_m": 0.2, "mannings": 5.5e-5}},
+        # config 1 with diffusive-wave routing (overlandflow_eval_diffusive.c)
+        "overland_diff": {
+            "build": lambda nx, ny, nz, nsteps: configs.overland(nx=nx, ny=ny, nz=nz, nsteps=nsteps,
+                                                                kind=BC_OVERLAND_DIFF),
+            "dims": (256, 256, 20), "sample": (64, 64, 20),
+            "label": "overland hillslope 256x256x20 (1.31M cells), diffusive-wave overland flow, "
                      "terrain-following grid, rain 2 h on / 2 h off",
             "config": {"dt_h": 0.25, "dx_m": 10.0, "dz_m": 0.2, "mannings": 5.5e-5}},
     }
@@ -653,9 +670,12 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--workload", default="hetero",
-                    choices=["hetero", "overland", "ensemble", "adjoint"],
-                    help="hetero: the 512x512x50 bench line; overland: the 256x256x20 "
-                         "overland hillslope; ensemble: the 48-member set")
+                    choices=["hetero", "overland", "overland_flow", "overland_diff", "ensemble",
+                             "adjoint"],
+                    help="hetero: the 512x512x50 bench line; overland / overland_flow / "
+                         "overland_diff: the 256x256x20 overland hillslope with "
+                         "OverlandKinematic / OverlandFlow / OverlandDiffusive routing; "
+                         "ensemble: the 48-member set; adjoint: the gradient workload")
     ap.add_argument("--profile", action="store_true",
                     help="mixed solve only, timed steps bracketed by cudaProfilerStart/Stop")
     ap.add_argument("--size", default=f"{NX},{NY},{NZ}",
