@@ -239,6 +239,20 @@ int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old
 int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt,
                           const double *x, double *y);
 
+/* Relative permeability from the reference's lookup table instead of the
+ * closed form (Geom.domain.RelPerm.NumSamplePoints / MinPressureHead /
+ * InterpolationMethod, problem_phase_rel_perm.c:1894-1916; VanGComputeTable
+ * :116-262): kr and its derivative at num_sample_points + 1 evenly spaced
+ * heads from 0 to |min_pressure_head|, interpolated by monotone cubic
+ * Hermite splines or linearly; zero beyond the table.  Needs uniform van
+ * Genuchten alpha and n (the descriptor scalars).  PFGPU_KRT_NONE restores
+ * the closed form.  The adjoint is not available with a table. */
+#define PFGPU_KRT_NONE 0
+#define PFGPU_KRT_SPLINE 1
+#define PFGPU_KRT_LINEAR 2
+int pfgpu_set_relperm_table(pfgpu_handle *h, int method, int num_sample_points,
+                            double min_pressure_head);
+
 /* Solver.Nonlinear.UseJacobian and Solver.Nonlinear.DerivativeEpsilon
  * (kinsol_nonlin_solver.c:860-885): use_jacobian = 1 (the default of this
  * library) gives GMRES the analytic Jacobian; 0 the difference quotient

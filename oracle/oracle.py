@@ -32,7 +32,8 @@ class Problem(C.Structure):
                 ("tslope_x", _dp), ("tslope_y", _dp),
                 ("mannings", _dp),
                 ("ov_epsilon", C.c_double),
-                ("ov_p_old", _dp)]
+                ("ov_p_old", _dp),
+                ("kr_table", C.c_void_p)]
 
 
 class Settings(C.Structure):
@@ -75,6 +76,9 @@ def lib():
         L.pfo_mg_create.restype = C.c_void_p
         L.pfo_mg_setup.argtypes = [C.c_void_p, C.POINTER(_dp)]
         L.pfo_mg_set_wghost.argtypes = [C.c_void_p, _dp]
+        L.pfo_vgtable_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
+        L.pfo_vgtable_create.restype = C.c_void_p
+        L.pfo_vgtable_destroy.argtypes = [C.c_void_p]
         L.pfo_mg_apply.argtypes = [C.c_void_p, _dp, _dp]
         L.pfo_mg_num_levels.argtypes = [C.c_void_p]
         L.pfo_mg_level_info.argtypes = [C.c_void_p, C.c_int] + [C.POINTER(C.c_int)] * 4
@@ -125,6 +129,13 @@ class Oracle:
         if prob.terrain_following:
             P.sslope_x, P.sslope_y = _ptr(sx), _ptr(sy)
         P.ov_epsilon = 1.0e-5
+        self._table = None
+        if prob.kr_table:
+            method = {"Spline": 0, "Linear": 1}[prob.kr_table[0]]
+            self._table = lib().pfo_vgtable_create(method, int(prob.kr_table[1]),
+                                                   float(prob.kr_table[2]),
+                                                   float(prob.vg_alpha), float(prob.vg_n))
+            P.kr_table = self._table
         self.P = P
         self.set_time(prob.start_time + prob.dt if t is None else t)
         s = prob.solver
@@ -139,6 +150,13 @@ class Oracle:
         S.use_jacobian = 1 if s.use_jacobian else 0
         S.derivative_epsilon = s.derivative_epsilon
         self.S = S
+
+    def __del__(self):
+        if getattr(self, "_table", None):
+            try:
+                lib().pfo_vgtable_destroy(self._table)
+            except Exception:
+                pass
 
     def set_time(self, t: float):
         self.t = t

@@ -83,12 +83,147 @@ void pfo_saturation(const pfo_problem *pb, const double *p, double *s, int der)
                         pb->s_res[c], pb->s_sat[c], pb->vg_from_file);
 }
 
+/* VanGComputeTable (problem_phase_rel_perm.c:116-262) */
+pfo_vgtable *pfo_vgtable_create(int method, int npts, double min_head, double alpha, double n)
+{
+  pfo_vgtable *t = (pfo_vgtable*)calloc(1, sizeof(pfo_vgtable));
+  t->method = method;
+  t->npts = npts;
+  t->min_head = min_head;
+  double **arr[] = { &t->x, &t->a, &t->d, &t->a_der, &t->d_der, &t->slope, &t->slope_der };
+  for (int q = 0; q < 7; q++)
+    *arr[q] = (double*)calloc(npts + 1, sizeof(double));
+  double *x = t->x, *a = t->a, *d = t->d, *a_der = t->a_der, *d_der = t->d_der;
+  double *del = (double*)calloc(npts + 1, sizeof(double));
+  double *del_der = (double*)calloc(npts + 1, sizeof(double));
+  double interval = min_head / (double)(npts - 1);
+  t->interval = fabs(interval);
+  double m = 1.0e0 - (1.0e0 / n);
+  for (int i = 0; i <= npts; i++)
+  {
+    x[i] = fabs(i * interval);
+    double opahn = 1.0 + pow(alpha * x[i], n);
+    double ahnm1 = pow(alpha * x[i], n - 1);
+    a[i] = pow(1.0 - ahnm1 / (pow(opahn, m)), 2) / pow(opahn, (m / 2));
+    double coeff = 1.0 - ahnm1 * pow(opahn, -m);
+    a_der[i] = 2.0 * (coeff / (pow(opahn, (m / 2))))
+               * ((n - 1) * pow(alpha * x[i], n - 2) * alpha * pow(opahn, -m)
+                  - ahnm1 * m * pow(opahn, -(m + 1)) * n * alpha * ahnm1)
+               + pow(coeff, 2) * (m / 2) * pow(opahn, (-(m + 2) / 2)) * n * alpha * ahnm1;
+    if ((n < 2) && (i == 0))
+      a_der[i] = 0;
+  }
+  if (method == 1)
+    for (int i = 0; i < npts; i++)
+    {
+      t->slope[i] = (a[i + 1] - a[i]) / t->interval;
+      t->slope_der[i] = (a_der[i + 1] - a_der[i]) / t->interval;
+    }
+  /* monotone cubic Hermite slopes (Fritsch and Carlson 1980) */
+  for (int i = 0; i < npts; i++)
+  {
+    double h = x[i + 1] - x[i];
+    del[i] = (a[i + 1] - a[i]) / h;
+    del_der[i] = (a_der[i + 1] - a_der[i]) / h;
+  }
+  d[0] = del[0];
+  d[npts] = del[npts - 1];
+  d_der[0] = del_der[0];
+  d_der[npts] = del_der[npts - 1];
+  for (int i = 1; i < npts; i++)
+  {
+    d[i] = (del[i - 1] + del[i]) / 2;
+    d_der[i] = (del_der[i - 1] + del_der[i]) / 2;
+  }
+  for (int i = 0; i < npts; i++)
+  {
+    if (del[i] == 0.0)
+    {
+      d[i] = 0;
+      d[i + 1] = 0;
+    }
+    else
+    {
+      double alph = d[i] / del[i], beta = d[i + 1] / del[i];
+      double magn = pow(alph, 2) + pow(beta, 2);
+      if (magn > 9.0)
+      {
+        d[i] = 3 * alph * del[i] / magn;
+        d[i + 1] = 3 * beta * del[i] / magn;
+      }
+    }
+    if (del_der[i] == 0.0)
+    {
+      d_der[i] = 0;
+      d_der[i + 1] = 0;
+    }
+    else
+    {
+      double alph = d_der[i] / del_der[i], beta = d_der[i + 1] / del_der[i];
+      double magn = pow(alph, 2) + pow(beta, 2);
+      if (magn > 9.0)
+      {
+        d_der[i] = 3 * alph * del_der[i] / magn;
+        d_der[i + 1] = 3 * beta * del_der[i] / magn;
+      }
+    }
+  }
+  free(del);
+  free(del_der);
+  return t;
+}
+
+void pfo_vgtable_destroy(pfo_vgtable *t)
+{
+  if (!t) return;
+  free(t->x); free(t->a); free(t->d); free(t->a_der); free(t->d_der);
+  free(t->slope); free(t->slope_der);
+  free(t);
+}
+
+/* VanGLookupSpline (:265-355) and the linear lookup (:357-400, and inline in
+ * PhaseRelPerm :718-758): kr (der = 0) or the table's derivative (der = 1)
+ * at a pressure head >= 0 */
+static double vgt_lookup(const pfo_vgtable *t, double head, int der)
+{
+  if (head >= fabs(t->min_head))
+    return 0.0;
+  int pt = (int)floor(head / t->interval);
+  if (t->method == 1)
+    return der ? t->a_der[pt] + t->slope_der[pt] * (head - t->x[pt])
+               : t->a[pt] + t->slope[pt] * (head - t->x[pt]);
+  int max = t->npts + 1;
+  if (pt > max)
+    pt = max - 1;
+  const double *A = der ? t->a_der : t->a, *D = der ? t->d_der : t->d;
+  double x = t->x[pt], x1 = t->x[pt + 1];
+  double tt = (head - x) / (x1 - x);
+  return (2.0 * pow(tt, 3) - 3.0 * pow(tt, 2) + 1.0) * A[pt]
+         + (pow(tt, 3) - 2.0 * pow(tt, 2) + tt) * (x1 - x) * D[pt]
+         + (-2.0 * pow(tt, 3) + 3.0 * pow(tt, 2)) * (A[pt + 1])
+         + (pow(tt, 3) - pow(tt, 2)) * (x1 - x) * (D[pt + 1]);
+}
+
+/* rel. perm. (der = 0) or its derivative (der = 1) at pressure p of a cell
+ * with VG parameters alpha, n: the table when one is set (:700-712,
+ * 1064-1080, 1170-1184), else the closed form */
+static double kr_at(const pfo_problem *pb, double p, double alpha, double n, int der)
+{
+  if (pb->kr_table)
+  {
+    if (p >= 0.0)
+      return der ? 0.0 : 1.0;
+    return vgt_lookup(pb->kr_table, fabs(p) / (pb->density * pb->gravity), der);
+  }
+  return der ? vg_dkr(p, pb->density, pb->gravity, alpha, n)
+             : vg_kr(p, pb->density, pb->gravity, alpha, n);
+}
+
 void pfo_relperm(const pfo_problem *pb, const double *p, double *kr, int der)
 {
   long N = (long)pb->nx * pb->ny * pb->nz;
   for (long c = 0; c < N; c++)
-    kr[c] = der ? vg_dkr(p[c], pb->density, pb->gravity, pb->alpha[c], pb->n[c])
-                : vg_kr(p[c], pb->density, pb->gravity, pb->alpha[c], pb->n[c]);
+    kr[c] = kr_at(pb, p[c], pb->alpha[c], pb->n[c], der);
 }
 
 /* -------------------------------------------------------------------------
@@ -664,7 +799,7 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           {
             /* ghost cell holds the Dirichlet value; its rel. perm. uses the
              * interior cell's VG parameters (GrGeomSurfLoop, :615) */
-            double krg = vg_kr(value, rho, g, pb->alpha[c], pb->n[c]);
+            double krg = kr_at(pb, value, pb->alpha[c], pb->n[c], 0);
             if (face < 4)
             {
               double h = (face < 2) ? ffx * zm[k] : ffy * zm[k];
@@ -865,7 +1000,7 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           double den_d = rho;
           double prod = kr[c] * rho;
           double prod_der = dkr[c] * rho + kr[c] * drho;
-          double prod_val = vg_kr(value, rho, g, pb->alpha[c], pb->n[c]) * den_d;
+          double prod_val = kr_at(pb, value, pb->alpha[c], pb->n[c], 0) * den_d;
           double o_temp, coeff, diff;
           double zu = (k + 1 < nz) ? zm[k + 1] : 0.0;
           switch (face)

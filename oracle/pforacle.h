@@ -19,6 +19,19 @@ extern "C" {
 enum { PFO_BC_FLUX = 0, PFO_BC_DIRICHLET = 1, PFO_BC_OVERLAND_KIN = 2, PFO_BC_OVERLAND_DIFF = 3,
        PFO_BC_OVERLAND = 4, PFO_BC_SEEPAGE = 5 };
 
+/* van Genuchten relative-permeability lookup table (VanGComputeTable,
+ * problem_phase_rel_perm.c:116-262): kr and dkr/dhead at npts + 1 evenly
+ * spaced heads 0 .. |min_head|, with monotone spline slopes (Fritsch and
+ * Carlson) or linear slopes */
+typedef struct {
+  int method;                      /* InterpolationMethod: 0 Spline, 1 Linear */
+  int npts;                        /* NumSamplePoints */
+  double min_head, interval;
+  double *x, *a, *d, *a_der, *d_der, *slope, *slope_der;
+} pfo_vgtable;
+pfo_vgtable *pfo_vgtable_create(int method, int npts, double min_head, double alpha, double n);
+void pfo_vgtable_destroy(pfo_vgtable *t);
+
 typedef struct {
   int nx, ny, nz;
   double dx, dy, dz;
@@ -44,6 +57,9 @@ typedef struct {
    * in the Jacobian (overlandflow_eval_diffusive.c CALCDER); the residual
    * takes it as an argument */
   const double *ov_p_old;
+  /* relative permeability from a lookup table instead of the closed form
+   * (Geom.domain.RelPerm.NumSamplePoints > 0), or NULL */
+  const pfo_vgtable *kr_table;
 } pfo_problem;
 
 typedef struct {

@@ -87,6 +87,21 @@ def dq_small() -> RichardsProblem:
     return p
 
 
+def krtable_spline_small() -> RichardsProblem:
+    """Config-0 box whose relative permeability comes from the reference's
+    lookup table, monotone spline (crater2D_vangtable_spline's keys)."""
+    p = configs.box(nx=12, ny=10, nz=8, nsteps=2, seed=29)
+    p.kr_table = ("Spline", 20000, -300.0)
+    return p
+
+
+def krtable_linear_small() -> RichardsProblem:
+    """The same with linear interpolation in the table."""
+    p = configs.box(nx=12, ny=10, nz=8, nsteps=2, seed=29)
+    p.kr_table = ("Linear", 20000, -300.0)
+    return p
+
+
 def tfg_small() -> RichardsProblem:
     """Terrain-following slopes in the subsurface fluxes without overland
     flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""
@@ -98,7 +113,8 @@ def tfg_small() -> RichardsProblem:
 
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
-          "overland_flow_small", "seepage_small", "dq_small"]
+          "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
+          "krtable_linear_small"]
 
 
 def get(name: str) -> RichardsProblem:

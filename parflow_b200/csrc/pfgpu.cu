@@ -176,6 +176,7 @@ struct pfgpu_handle {
   int use_jacobian = 1;
   double sqrt_relfunc = 0.0;
   double *dq_w = nullptr, *dq_f = nullptr;
+  double *krt = nullptr;  // relative-permeability lookup table (device)
   int *kerr = nullptr;   // device error word of the pipelined kernels
   int *hkerr = nullptr;  // pinned host mirror
   // discrete adjoint: recorded trajectory p_0 .. p_len (dense, device) and
@@ -1205,6 +1206,7 @@ static void destroy_impl(pfgpu_handle *h) {
   for (cudaEvent_t e : h->pev) cudaEventDestroy(e);
   cudaFree(h->dq_w);
   cudaFree(h->dq_f);
+  cudaFree(h->krt);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   cudaFree(h->hist);
   cudaFree(h->adj);
@@ -1807,6 +1809,104 @@ int pfgpu_pc_setup(pfgpu_handle *h, const double *p, double dt) {
   return PFGPU_OK;
 }
 
+// VanGComputeTable (problem_phase_rel_perm.c:116-262): kr and dkr/dhead at
+// npts + 1 heads 0, |min_head| / (npts - 1), ..., the linear slopes and the
+// monotone cubic Hermite slopes (Fritsch and Carlson 1980); t holds x a d
+// a_der d_der slope slope_der, npts + 1 values each
+static void vg_table(int linear, int npts, double min_head, double alpha, double n,
+                     std::vector<double> &t, double *interval_out) {
+  const int m1 = npts + 1;
+  t.assign(7 * (size_t)m1, 0.0);
+  double *x = t.data(), *a = x + m1, *d = x + 2 * m1, *a_der = x + 3 * m1, *d_der = x + 4 * m1,
+         *slope = x + 5 * m1, *slope_der = x + 6 * m1;
+  const double interval = min_head / (double)(npts - 1);
+  const double ival = fabs(interval);
+  *interval_out = ival;
+  const double m = 1.0e0 - (1.0e0 / n);
+  for (int i = 0; i <= npts; i++) {
+    x[i] = fabs(i * interval);
+    const double opahn = 1.0 + pow(alpha * x[i], n);
+    const double ahnm1 = pow(alpha * x[i], n - 1);
+    a[i] = pow(1.0 - ahnm1 / (pow(opahn, m)), 2) / pow(opahn, (m / 2));
+    const double coeff = 1.0 - ahnm1 * pow(opahn, -m);
+    a_der[i] = 2.0 * (coeff / (pow(opahn, (m / 2)))) *
+                   ((n - 1) * pow(alpha * x[i], n - 2) * alpha * pow(opahn, -m) -
+                    ahnm1 * m * pow(opahn, -(m + 1)) * n * alpha * ahnm1) +
+               pow(coeff, 2) * (m / 2) * pow(opahn, (-(m + 2) / 2)) * n * alpha * ahnm1;
+    if ((n < 2) && (i == 0)) a_der[i] = 0;
+  }
+  if (linear)
+    for (int i = 0; i < npts; i++) {
+      slope[i] = (a[i + 1] - a[i]) / ival;
+      slope_der[i] = (a_der[i + 1] - a_der[i]) / ival;
+    }
+  std::vector<double> del(m1, 0.0), del_der(m1, 0.0);
+  for (int i = 0; i < npts; i++) {
+    const double hh = x[i + 1] - x[i];
+    del[i] = (a[i + 1] - a[i]) / hh;
+    del_der[i] = (a_der[i + 1] - a_der[i]) / hh;
+  }
+  d[0] = del[0];
+  d[npts] = del[npts - 1];
+  d_der[0] = del_der[0];
+  d_der[npts] = del_der[npts - 1];
+  for (int i = 1; i < npts; i++) {
+    d[i] = (del[i - 1] + del[i]) / 2;
+    d_der[i] = (del_der[i - 1] + del_der[i]) / 2;
+  }
+  auto limit = [&](double *dd, const double *dl, int i) {
+    if (dl[i] == 0.0) {
+      dd[i] = 0;
+      dd[i + 1] = 0;
+    } else {
+      const double alph = dd[i] / dl[i], beta = dd[i + 1] / dl[i];
+      const double magn = pow(alph, 2) + pow(beta, 2);
+      if (magn > 9.0) {
+        dd[i] = 3 * alph * dl[i] / magn;
+        dd[i + 1] = 3 * beta * dl[i] / magn;
+      }
+    }
+  };
+  for (int i = 0; i < npts; i++) {
+    limit(d, del.data(), i);
+    limit(d_der, del_der.data(), i);
+  }
+}
+
+int pfgpu_set_relperm_table(pfgpu_handle *h, int method, int num_sample_points,
+                            double min_pressure_head) {
+  if (!h || method < PFGPU_KRT_NONE || method > PFGPU_KRT_LINEAR ||
+      (method != PFGPU_KRT_NONE && (num_sample_points < 2 || !(min_pressure_head < 0.0)))) {
+    set_err("pfgpu_set_relperm_table: bad argument");
+    return PFGPU_ERR_ARG;
+  }
+  CK(cudaSetDevice(h->device));
+  if (method == PFGPU_KRT_NONE) {
+    h->P.krt = nullptr;
+    h->vg_for = nullptr;
+    return PFGPU_OK;
+  }
+  if (h->d.vg_from_file || h->P.alpha || h->P.vgn) {
+    set_err("pfgpu_set_relperm_table: the table needs uniform van Genuchten alpha and n");
+    return PFGPU_ERR_STATE;
+  }
+  std::vector<double> t;
+  double interval = 0.0;
+  vg_table(method == PFGPU_KRT_LINEAR, num_sample_points, min_pressure_head, h->d.vg_alpha,
+           h->d.vg_n, t, &interval);
+  cudaFree(h->krt);
+  h->krt = nullptr;
+  if (dalloc(&h->krt, (long long)t.size())) return PFGPU_ERR_NOMEM;
+  CK(cudaMemcpy(h->krt, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice));
+  h->P.krt = h->krt;
+  h->P.krt_method = method == PFGPU_KRT_LINEAR ? 1 : 0;
+  h->P.krt_npts = num_sample_points;
+  h->P.krt_interval = interval;
+  h->P.krt_min = min_pressure_head;
+  h->vg_for = nullptr;  // cached van Genuchten state is stale
+  return PFGPU_OK;
+}
+
 int pfgpu_set_jacobian_mode(pfgpu_handle *h, int use_jacobian, double derivative_epsilon) {
   if (!h || (use_jacobian != 0 && use_jacobian != 1) || derivative_epsilon < 0.0) {
     set_err("pfgpu_set_jacobian_mode: bad argument");
@@ -2013,6 +2113,10 @@ int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps
   }
   if (!h->recording || h->hist_len < 1) {
     set_err("pfgpu_adjoint_gradient: no recorded steps (pfgpu_adjoint_record, then pfgpu_advance)");
+    return PFGPU_ERR_STATE;
+  }
+  if (h->P.krt) {
+    set_err("pfgpu_adjoint_gradient: not available with a relative-permeability table");
     return PFGPU_ERR_STATE;
   }
   if (h->P.bc_type[5] == PFGPU_BC_OVERLAND_DIFF) {

@@ -41,6 +41,12 @@ struct DevProblem {
   // old pressure of the step (dense interior), read by the diffusive terms'
   // slope magnitude in the residual and the Jacobian
   const double *ov_pold;
+  // relative-permeability lookup table (Geom.domain.RelPerm.NumSamplePoints
+  // > 0, problem_phase_rel_perm.c:116-262), or null: krt holds x a d a_der
+  // d_der slope slope_der, krt_npts + 1 values each
+  const double *krt;
+  int krt_method, krt_npts;  // method 0 spline, 1 linear
+  double krt_interval, krt_min;
   // thread-block shapes (bx, by) of the residual, Jacobian and matvec
   // launches picked by pfgpu_autotune; (0, 0) = the default heuristic.
   // Host-side launch configuration only: no kernel reads it.
@@ -121,8 +127,29 @@ __device__ __forceinline__ double vg_dsat(const DevProblem &P, double p, const V
 }
 
 // Relative permeability (pfsimulator/parflow_lib/problem_phase_rel_perm.c:788, :981)
+// table lookup at a pressure head >= 0: kr (der = 0) or the table's
+// derivative (der = 1) (VanGLookupSpline :265-355, linear :357-400, 718-758)
+__device__ __forceinline__ double krt_lookup(const DevProblem &P, double head, int der) {
+  if (head >= fabs(P.krt_min)) return 0.0;
+  const int m1 = P.krt_npts + 1;
+  const double *x = P.krt, *a = P.krt + m1, *d = P.krt + 2 * m1, *a_der = P.krt + 3 * m1,
+               *d_der = P.krt + 4 * m1, *slope = P.krt + 5 * m1, *slope_der = P.krt + 6 * m1;
+  int pt = (int)floor(head / P.krt_interval);
+  if (P.krt_method == 1)
+    return der ? a_der[pt] + slope_der[pt] * (head - x[pt]) : a[pt] + slope[pt] * (head - x[pt]);
+  if (pt > m1) pt = m1 - 1;
+  const double *A = der ? a_der : a, *Dd = der ? d_der : d;
+  const double x0 = x[pt], x1 = x[pt + 1];
+  const double t = (head - x0) / (x1 - x0);
+  return (2.0 * pow(t, 3) - 3.0 * pow(t, 2) + 1.0) * A[pt] +
+         (pow(t, 3) - 2.0 * pow(t, 2) + t) * (x1 - x0) * Dd[pt] +
+         (-2.0 * pow(t, 3) + 3.0 * pow(t, 2)) * (A[pt + 1]) +
+         (pow(t, 3) - pow(t, 2)) * (x1 - x0) * (Dd[pt + 1]);
+}
+
 __device__ __forceinline__ double vg_kr(const DevProblem &P, double p, double alpha, double n) {
   if (p >= 0.0) return 1.0;
+  if (P.krt) return krt_lookup(P, fabs(p) / (P.density * P.gravity), 0);
   double m = 1.0 - (1.0 / n);
   double head = fabs(p) / (P.density * P.gravity);
   double opahn = 1.0 + pow(alpha * head, n);

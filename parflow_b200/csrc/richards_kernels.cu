@@ -34,6 +34,17 @@ __global__ void __launch_bounds__(256, 5) k_vg_all(DevProblem P, const double *_
   long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (c >= P.n) return;
   VGAll v = vg_all(P, p[c], vg_at(P, c));
+  if (P.krt) {  // relative permeability from the lookup table
+    const double pc = p[c];
+    if (pc >= 0.0) {
+      v.kr = 1.0;
+      v.dkr = 0.0;
+    } else {
+      const double head = fabs(pc) / (P.density * P.gravity);
+      v.kr = krt_lookup(P, head, 0);
+      v.dkr = krt_lookup(P, head, 1);
+    }
+  }
   kr[c] = v.kr;
   dkr[c] = v.dkr;
   sat[c] = v.s;

@@ -150,6 +150,10 @@ class RichardsProblem:
     slope_x: object = 0.0                 # (ny, nx) or float
     slope_y: object = 0.0
     mannings: float = 5.5e-5
+    # relative permeability from a lookup table (Geom.domain.RelPerm.
+    # NumSamplePoints / MinPressureHead / InterpolationMethod): None or
+    # (method "Spline" | "Linear", sample points, min pressure head)
+    kr_table: Optional[tuple] = None
     solver: SolverSettings = field(default_factory=SolverSettings)
     name: str = "richards"
 
@@ -393,6 +397,10 @@ class RichardsProblem:
             k["Geom.domain.Saturation.SSat"] = float(self.s_sat)
         else:
             k["Geom.domain.RelPerm.Alpha"] = float(self.vg_alpha)
+            if self.kr_table:
+                k["Geom.domain.RelPerm.NumSamplePoints"] = int(self.kr_table[1])
+                k["Geom.domain.RelPerm.MinPressureHead"] = float(self.kr_table[2])
+                k["Geom.domain.RelPerm.InterpolationMethod"] = str(self.kr_table[0])
             k["Geom.domain.RelPerm.N"] = float(self.vg_n)
             k["Geom.domain.Saturation.Alpha"] = float(self.vg_alpha)
             k["Geom.domain.Saturation.N"] = float(self.vg_n)

@@ -94,6 +94,11 @@ class RichardsGPU:
         if not s.use_jacobian:
             L.check(self.lib.pfgpu_set_jacobian_mode(self.h, 0, s.derivative_epsilon),
                     "set_jacobian_mode")
+        if prob.kr_table:
+            method = {"Spline": 1, "Linear": 2}[prob.kr_table[0]]
+            L.check(self.lib.pfgpu_set_relperm_table(self.h, method, int(prob.kr_table[1]),
+                                                     float(prob.kr_table[2])),
+                    "set_relperm_table")
         self._upload_fields()
         self.set_time(prob.start_time + prob.dt)
 
