@@ -102,6 +102,32 @@ def krtable_linear_small() -> RichardsProblem:
     return p
 
 
+def default_richards() -> RichardsProblem:
+    """The reference's own regression case default_richards
+    (test/python/default_richards.py): 18x15x8 box at origin (-10, 10, 1),
+    K = 4, porosity 1, VG alpha 0.005, n 2, Sres 0.2, Ssat 0.99, hydrostatic
+    start (3.0 at the bottom), DirEquilRefPatch 5.0 / 3.0 on the x faces,
+    no-flow elsewhere, 50 steps of 0.001.  Its reference outputs were made
+    with PFMG; MGSemi stands in here, so the comparison is at the test's own
+    6 significant digits."""
+    s = SolverSettings(residual_tol=1e-9, max_iter=10, krylov_dim=10, eta_value=1e-5)
+    p = RichardsProblem(nx=18, ny=15, nz=8, dx=8.8888888888888893, dy=10.666666666666666,
+                        dz=1.0, perm=4.0, porosity=1.0, specific_storage=1.0e-4,
+                        vg_alpha=0.005, vg_n=2.0, s_res=0.2, s_sat=0.99, dt=0.001, nsteps=50,
+                        solver=s, name="default_richards")
+    p.x0, p.y0, p.z0 = -10.0, 10.0, 1.0
+    p.bc = {
+        "x_lower": BC(BC_DIRICHLET, (5.0,), ref_patch="z_lower"),
+        "x_upper": BC(BC_DIRICHLET, (3.0,), ref_patch="z_lower"),
+        "y_lower": BC(BC_FLUX, (0.0,)),
+        "y_upper": BC(BC_FLUX, (0.0,)),
+        "z_lower": BC(BC_FLUX, (0.0,)),
+        "z_upper": BC(BC_FLUX, (0.0,)),
+    }
+    p.ic = p.hydrostatic_ic(3.0, "z_lower")
+    return p
+
+
 def tfg_small() -> RichardsProblem:
     """Terrain-following slopes in the subsurface fluxes without overland
     flow: config-1 layers and slopes, no-flow top, Dirichlet bottom."""

@@ -1,0 +1,55 @@
+"""The reference's own regression test default_richards
+(test/python/default_richards.py, outputs in test/correct_output/, copied to
+tests/golden/default_richards_ref.npz by tests/golden/make_reference_outputs.py).
+
+The reference made those outputs with the hypre PFMG preconditioner, which is
+not available here; MGSemi stands in, so the check is the reference test's own
+criterion, 6 significant digits of pressure and saturation (taken here as
+max |x - x_ref| <= 1e-6 max |x_ref|), at steps 1, 10, 25 and 50.  The oracle
+runs on CPU; the GPU library in FP64 and in the headline mixed form.
+"""
+
+import numpy as np
+import pytest
+
+from parflow_b200 import cases
+
+TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def ref(golden):
+    return golden("default_richards_ref")
+
+
+def _check(ps, sats, ref):
+    for k, s in enumerate(ref["steps"]):
+        for got, want in ((ps[s - 1], ref["press"][k]), (sats[s - 1], ref["satur"][k])):
+            err = np.abs(got - want).max() / np.abs(want).max()
+            assert err <= TOL, (int(s), err)
+
+
+def test_oracle_matches_reference_regression(ref):
+    from oracle.oracle import Oracle
+
+    prob = cases.default_richards()
+    orc = Oracle(prob)
+    ps, st = orc.run()
+    assert all(x.status in (1, 2) for x in st)
+    _check(ps, [orc.saturation(p) for p in ps], ref)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed16"])
+def test_gpu_matches_reference_regression(ref, precision):
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.fail("CUDA device required for gpu tests")
+    from parflow_b200.solver import RichardsGPU
+
+    g = RichardsGPU(cases.default_richards(), precision=precision)
+    ps, st = g.run()
+    sats = [g.saturation(p) for p in ps]
+    g.close()
+    _check(ps, sats, ref)
