@@ -148,84 +148,80 @@ def _workloads():
     }
 
 
-def _ref_binary():
-    for name in ("parflow_omp", "parflow"):
-        p = os.path.join(ROOT, "oracle", "_ref", "bin", name)
-        if os.path.exists(p):
-            return p, name
-    return None, None
+def _config(wl: dict, world: int) -> dict:
+    """The workload's config as both arms print it (same keys, same values)."""
+    cells = int(np.prod(wl["dims"]))
+    return dict({"workload": wl["label"]}, **wl["config"],
+                solver="KINSOL line search, EtaConstant 1e-5, GMRES(25), MGSemi V(1,1)",
+                l2=f"inputs larger than L2 (every vector {cells * 8 / 1e6:.0f} MB, "
+                   "working set several GB)",
+                parallelism=f"replicas x{world}")
 
 
-def run_reference_cpu(nsteps: int, threads: int, workload: str = "hetero"):
-    """Time the unmodified reference (oracle/_ref) on a bounded sample of the
-    workload (same physics, fewer cells); returns (steps/s scaled by cells to
-    the full workload, info dict)."""
+def reference_steps(workload: str, first: int, count: int, exe: str = "parflow_omp",
+                    dump: bool = False):
+    """Run the unmodified reference build (oracle/_ref) on the full workload
+    for first + count timesteps from its initial condition and time steps
+    first+1 .. first+count (per-step ends from the reference's KINSOL log).
+    Returns (timesteps/s, the run's record)."""
+    from oracle import refrun
+
     wl = _workloads()[workload]
-    exe, name = _ref_binary()
-    sx, sy, sz = wl["sample"]
-    fx, fy, fz = wl["dims"]
-    prob = wl["build"](sx, sy, sz, nsteps)
-    if exe is None:
-        # the oracle port, one core
-        from oracle.oracle import Oracle
-
-        orc = Oracle(prob)
-        t0 = time.perf_counter()
-        orc.run(nsteps)
-        secs = time.perf_counter() - t0
-        kind, cores = "port", 1
-    else:
-        wd = tempfile.mkdtemp(prefix="pfref_")
-        run = prob.to_reference(wd, "bench", dump_interval=-1)
-        env = dict(os.environ, OMP_NUM_THREADS=str(threads))
-        t0 = time.perf_counter()
-        subprocess.run([exe, run], cwd=wd, env=env, check=True,
-                       stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
-        wall = time.perf_counter() - t0
-        secs = wall
-        try:
-            txt = open(os.path.join(wd, run + ".out.timing.csv")).read()
-            m = re.search(r"^KINSol,\s*([0-9.eE+-]+)", txt, re.M)
-            if m:
-                secs = float(m.group(1))
-        except OSError:
-            pass
-        shutil.rmtree(wd, ignore_errors=True)
-        kind, cores = "reference", threads if name == "parflow_omp" else 1
-    scale = (sx * sy * sz) / float(fx * fy * fz)
-    steps_per_s = nsteps / secs * scale
-    info = {"kind": kind, "cores": cores,
-            "sample": f"{sx}x{sy}x{sz} sample of the {workload} workload "
-                      f"(1/{int(round(1 / scale))} of its cells), {nsteps} steps, KINSol time "
-                      f"{secs:.2f} s, scaled by cell count to {fx}x{fy}x{fz}",
-            "binary": name or "oracle port"}
-    return steps_per_s, info
+    nx, ny, nz = wl["dims"]
+    prob = wl["build"](nx, ny, nz, first + count)
+    res = refrun.run(prob, first + count, exe=exe, dump=dump)
+    return refrun.steps_per_second(res, first, count), res
 
 
 def reference_arm(args, rank, world):
+    """The reference's own CPU implementation on the same workload, at full
+    size: the OpenMP build on every host thread runs warmup + steps
+    timesteps and the last `steps` are timed; then the sequential build on
+    one core times its second step.  Under torchrun only rank 0 runs."""
     if rank != 0:
         return
-    # the reference has no ensemble driver or adjoint: those fall back to the
-    # headline workload's sample
-    wl_name = args.workload if args.workload in ("hetero", "overland") else "hetero"
-    threads = os.cpu_count() or 1
-    total = 0.0
-    per = []
-    k = max(1, args.steps)
-    # each step: one bounded reference sample of 2 timesteps
-    for _ in range(k):
-        v, info = run_reference_cpu(2, threads, wl_name)
-        per.append(v)
-    value = float(np.median(per))
+    from oracle import refrun
+
+    # the reference has no ensemble driver or adjoint: those use the headline workload
+    wl_name = args.workload if args.workload in _workloads() else "hetero"
+    wl = _workloads()[wl_name]
+    nx, ny, nz = wl["dims"]
+    k, w = max(1, args.steps), max(0, args.warmup)
+    exe = "parflow_omp" if refrun.binary("parflow_omp") else "parflow"
+    if refrun.binary(exe) is None:
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "reference build missing under oracle/_ref (built by "
+                                         "oracle/ref.mk where the ParFlow sources are)"}),
+              flush=True)
+        return
+    value, res = reference_steps(wl_name, w, k, exe=exe)
+    counts = res["counts"]
+    timed = counts[w:w + k]
     out = {"impl": "reference", "metric": METRIC, "value": value, "unit": "timesteps/s",
-           "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-           "ms_per_step": 1e3 / value if value else None, "higher_is_better": True,
+           "n_gpus": args.gpus, "steps": k, "warmup": w,
+           "ms_per_step": 1e3 / value, "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-           "config": {"workload": _workloads()[wl_name]["label"] + ", sampled"},
-           "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": info["cores"],
-                            "kind": info["kind"], "sample": info["sample"]},
+           "config": _config(wl, world),
+           "cpu_baseline": {"value": value, "unit": "timesteps/s", "cores": res["threads"],
+                            "kind": "reference",
+                            "sample": f"the full workload ({nx}x{ny}x{nz}): {w + k} timesteps "
+                                      f"from the initial condition with the unmodified "
+                                      f"{exe} build, steps {w + 1}-{w + k} timed from the "
+                                      f"reference's per-step KINSOL log",
+                            "cpu": refrun.cpu_model()},
            "e2e": {"value": value, "unit": "timesteps/s", "h2d_bytes_per_step": 0,
-                   "d2h_bytes_per_step": 0}}
+                   "d2h_bytes_per_step": 0},
+           "wall_s": res["wall"], "kinsol_s": res["timing"].get("KINSol"),
+           "newton_iters_per_step": float(timed[:, 0].mean()),
+           "gmres_iters_per_step": float(timed[:, 1].mean()),
+           "cell_newton_updates_per_s": nx * ny * nz * float(timed[:, 0].sum()) /
+                                        (k / value)}
+    if args.ref_seq_steps > 0 and refrun.binary("parflow"):
+        sv, sres = reference_steps(wl_name, args.ref_seq_steps - 1, 1, exe="parflow")
+        out["seq_1core"] = {"value": sv, "unit": "timesteps/s", "cores": 1,
+                            "sample": f"step {args.ref_seq_steps} of the full workload from "
+                                      f"its initial condition, sequential build, one core",
+                            "wall_s": sres["wall"]}
     print(json.dumps(out), flush=True)
 
 
@@ -247,6 +243,36 @@ def max_over_ranks(ms: float, dist=None, device: str = "cuda") -> float:
 def job_throughput(steps: int, world: int, ms_max: float) -> float:
     """Whole-job timesteps/s: every rank's steps over the slowest rank's time."""
     return steps * world / (ms_max * 1e-3)
+
+
+def compare_with_reference(prob, plan, ic, res, device: int) -> dict:
+    """Max relative pressure difference (max |p - p_ref| / max |p_ref|) of
+    every GPU form against the reference's pressures after each of the
+    steps the reference run dumped, from the same initial condition, and
+    whether the per-step Newton and GMRES counts equal the reference's."""
+    from parflow_b200.solver import RichardsGPU
+
+    ref_p = res["press"]
+    out = {}
+    for precision in ("fp64", "mixed", HEADLINE):
+        g = RichardsGPU(prob, precision=precision, device=device)
+        g.set_pressure(ic)
+        errs, same = [], True
+        for n in range(ref_p.shape[0]):
+            t, dt = plan[n]
+            g.set_time(t)
+            st = g.advance(1, dt)[0]
+            p = g.get_pressure()
+            errs.append(float(np.abs(p - ref_p[n]).max() / np.abs(ref_p[n]).max()))
+            same = same and (st.nonlin_iters == int(res["counts"][n, 0]) and
+                             st.lin_iters == int(res["counts"][n, 1]))
+        g.close()
+        key = {"fp64": "fp64", "mixed": "mixed_fp32_mg", HEADLINE: "mixed"}[precision]
+        out[key + "_max_rel_pressure_err"] = max(errs)
+        out[key + "_per_step"] = errs
+        out[key + "_counts_equal"] = bool(same)
+    out["reference_counts"] = res["counts"][:, :2].tolist()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -388,12 +414,21 @@ def gpu_arm(args, rank, world, local_rank):
     d2h = 2 * nbytes   # p, s
     e2e_ms = max_over_ranks(e2e_ms, dist)
 
-    cpu = None
+    # the reference build on the full workload: the CPU baseline (its second
+    # timestep, timed from its KINSOL log) and the pressures after steps 1
+    # and 2, against which every GPU form is checked from the same initial
+    # condition (max relative difference, Newton and GMRES counts per step)
+    cpu, vs_ref = None, None
     if rank == 0 and world == 1 and not args.no_cpu:
         try:
-            v, info = run_reference_cpu(2, os.cpu_count() or 1, args.workload)
-            cpu = {"value": v, "unit": "timesteps/s", "cores": info["cores"],
-                   "kind": info["kind"], "sample": info["sample"]}
+            v, res = reference_steps(args.workload, 1, 1, dump=True)
+            cpu = {"value": v, "unit": "timesteps/s", "cores": res["threads"],
+                   "kind": "reference",
+                   "sample": f"the full workload ({nx}x{ny}x{nz}), unmodified {res['binary']} "
+                             "build: 2 timesteps from the initial condition with pressure "
+                             "output, step 2 timed from the reference's per-step KINSOL log",
+                   "cpu": __import__("oracle.refrun", fromlist=["cpu_model"]).cpu_model()}
+            vs_ref = compare_with_reference(prob, plan, ic, res, local_rank)
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "unit": "timesteps/s", "cores": 0, "kind": "reference",
                    "sample": f"failed: {e}"}
@@ -409,12 +444,8 @@ def gpu_arm(args, rank, world, local_rank):
             "dtype": "f64 Newton/Arnoldi; f32 multigrid arithmetic on a diagonal-scaled f16 "
                      "operator; f32 Jacobian storage",
             "data": "synthetic",
-            "config": dict({"workload": wl["label"] + " mixed precision (" + HEADLINE + ")"},
-                           **wl["config"],
-                           solver="KINSOL line search, EtaConstant 1e-5, GMRES(25), MGSemi V(1,1)",
-                           l2=f"inputs larger than L2 (every vector {cells * 8 / 1e6:.0f} MB, "
-                              "working set several GB)",
-                           parallelism=f"replicas x{world}"),
+            "precision": HEADLINE,
+            "config": _config(wl, world),
             "fp64_steps_per_s": steps_64,
             "mixed_speedup_vs_fp64": steps_mx / steps_64,
             "mixed_vs_fp64_max_rel_pressure_err": rel_err,
@@ -434,6 +465,7 @@ def gpu_arm(args, rank, world, local_rank):
                             "gbs": (v[1] / (v[0] * 1e-3) / 1e9) if v[1] else None}
                         for k, v in kern.items()},
             "cpu_baseline": cpu,
+            "vs_reference_steps_1_2": vs_ref,
             "e2e": {"value": world / (e2e_ms * 1e-3), "unit": "timesteps/s",
                     "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "api": "pfgpu_newton_solve_sat with pinned host buffers"},
@@ -668,7 +700,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-cpu", action="store_true",
+                    help="skip the reference CPU baseline and the check against its pressures")
+    ap.add_argument("--ref-seq-steps", type=int, default=2,
+                    help="reference arm: also time step N of the sequential one-core build "
+                         "(0: skip)")
     ap.add_argument("--workload", default="hetero",
                     choices=["hetero", "overland", "overland_flow", "overland_diff", "ensemble",
                              "adjoint"],

@@ -395,13 +395,19 @@ int pfgpu_autotune(pfgpu_handle *h, int reps, int *shapes);
  * c = i + nx*(j + ny*k)); perm is the one permeability array used for x, y
  * and z; vg_alpha, vg_n, s_res, s_sat are per-cell arrays or NULL for desc's
  * scalars; bc_type[6] lives on the host and bc_values[6] are device tables
- * laid out as for pfgpu_set_bc.  Runs on the current device and is ordered on
- * `stream` (a cudaStream_t, NULL = legacy default stream): f is ready when the
- * stream reaches this point.  The first call on a device resolves the scratch
- * address (cudaGetSymbolAddress) and should come before any stream capture.
- * Calls on one device share the scratch, so calls that may overlap on the GPU
- * race.  Same arithmetic as pfgpu_nl_function_eval (nl_function_eval.c:167).
- * No counterpart in the reference. */
+ * laid out as for pfgpu_set_bc; only FluxConst (PFGPU_BC_FLUX) and Dirichlet
+ * (PFGPU_BC_DIRICHLET) faces are accepted (no overland, seepage or terrain-
+ * following terms), others return PFGPU_ERR_ARG.  Every pointer must be
+ * memory of the current device (or managed memory).  Runs on the current
+ * device and is ordered on `stream` (a cudaStream_t, NULL = legacy default
+ * stream): f is ready when the stream reaches this point.  The first call on
+ * a device resolves the scratch address (cudaGetSymbolAddress) and should
+ * come before any stream capture; a cudaDeviceReset invalidates that address,
+ * so do not call this again on a device that was reset.  Calls on one device
+ * share the scratch, so calls that may overlap on the GPU race.  Host cost per
+ * call: up to 15 cudaPointerGetAttributes checks and one small kernel per 64
+ * layers (the layer constants) besides the two residual kernels.  Same
+ * arithmetic as pfgpu_nl_function_eval.  No counterpart in the reference. */
 int pfgpu_residual_noalloc(const pfgpu_desc *desc, const double *perm,
                            const double *vg_alpha, const double *vg_n,
                            const double *s_res, const double *s_sat,

@@ -18,7 +18,9 @@
 # (parflow_config.h, pfversion.h) are written by this recipe from the values
 # the CMake templates would substitute for a seq/no-hypre build.
 
-REF     ?= /root/reference
+ifeq ($(strip $(REF)),)
+$(error REF is not set: make -f oracle/ref.mk REF=<parflow source tree>)
+endif
 HERE    := $(dir $(lastword $(MAKEFILE_LIST)))
 OUT     := $(HERE)_ref
 PL      := $(REF)/pfsimulator/parflow_lib

@@ -48,12 +48,22 @@ def build(force: bool = False, verbose: bool = False) -> str:
                     "-I" + os.path.join(ROOT, "include"), "--expt-relaxed-constexpr"]
     if verbose:
         flags += ["-Xptxas", "-v"]
-    objs = []
+    headers = [d for d in deps() if not d.endswith(".cu")]
+    newest_header = max(os.path.getmtime(h) for h in headers)
+    jobs, objs = [], []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
-        cmd = [nvcc()] + flags + ["-c", src, "-o", obj]
-        subprocess.check_call(cmd)
+        if (force or not os.path.exists(obj) or os.path.getmtime(obj) < os.path.getmtime(src)
+                or os.path.getmtime(obj) < newest_header):
+            jobs.append([nvcc()] + flags + ["-c", src, "-o", obj])
+    # one nvcc per translation unit, in parallel
+    from concurrent.futures import ThreadPoolExecutor
+
+    with ThreadPoolExecutor(max_workers=min(8, os.cpu_count() or 1)) as ex:
+        for rc, cmd in zip(ex.map(lambda c: subprocess.call(c), jobs), jobs):
+            if rc != 0:
+                raise subprocess.CalledProcessError(rc, cmd)
     tmp = LIB + ".tmp"
     subprocess.check_call([nvcc()] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs)
     os.replace(tmp, LIB)

@@ -21,6 +21,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "../../include/pfgpu.h"
 #include "pfgpu_kernels.h"
@@ -37,7 +38,13 @@ constexpr long long kScratchDoubles = 4 * kMaxCells + 4LL * kMaxLayers;
 static __device__ __align__(256) double g_noalloc_scratch[kScratchDoubles];
 
 constexpr int kMaxDevices = 64;
+// device address of g_noalloc_scratch per device, resolved once under the
+// mutex (two host threads making their first call on one device at the same
+// time both see the one resolved address).  cudaDeviceReset destroys the
+// context the address belongs to: a process that resets a device must not
+// call pfgpu_residual_noalloc on it again.
 double *g_scratch_ptr[kMaxDevices] = {nullptr};
+std::mutex g_scratch_mu;
 
 // layer constants of up to kLayerChunk layers, passed by value to k_layers
 constexpr int kLayerChunk = 64;
@@ -67,14 +74,17 @@ int fail(int code, const char *fmt, ...) {
   return code;
 }
 
-bool on_device(const void *p) {
+// device memory of device `dev` (a buffer of another GPU is rejected: the
+// kernels would read it over the peer path or fault), or managed memory
+bool on_device(const void *p, int dev) {
   if (!p) return false;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace
@@ -98,35 +108,45 @@ extern "C" int pfgpu_residual_noalloc(const pfgpu_desc *desc, const double *perm
                 n, desc->nz, kMaxCells, kMaxLayers);
   if (!bc_type || !bc_values)
     return fail(PFGPU_ERR_ARG, "pfgpu_residual_noalloc: null boundary tables");
-  const void *dev_args[] = {perm, p, p_old, s_old, f};
-  for (const void *a : dev_args)
-    if (!on_device(a))
-      return fail(PFGPU_ERR_ARG, "pfgpu_residual_noalloc: inputs and output must be device memory");
-  for (int face = 0; face < 6; face++) {
-    if (bc_type[face] != PFGPU_BC_FLUX && bc_type[face] != PFGPU_BC_DIRICHLET)
-      return fail(PFGPU_ERR_ARG, "pfgpu_residual_noalloc: bad boundary type on face %d", face);
-    if (!on_device(bc_values[face]))
-      return fail(PFGPU_ERR_ARG, "pfgpu_residual_noalloc: face %d table must be device memory", face);
-  }
-  const double *vg[] = {vg_alpha, vg_n, s_res, s_sat};
-  for (const double *a : vg)
-    if (a && !on_device(a))
-      return fail(PFGPU_ERR_ARG, "pfgpu_residual_noalloc: per-cell fields must be device memory");
-
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices)
     return fail(PFGPU_ERR_CUDA, "pfgpu_residual_noalloc: no usable current device");
+  const void *dev_args[] = {perm, p, p_old, s_old, f};
+  for (const void *a : dev_args)
+    if (!on_device(a, dev))
+      return fail(PFGPU_ERR_ARG,
+                  "pfgpu_residual_noalloc: inputs and output must be memory of the current "
+                  "device %d", dev);
+  for (int face = 0; face < 6; face++) {
+    if (bc_type[face] != PFGPU_BC_FLUX && bc_type[face] != PFGPU_BC_DIRICHLET)
+      return fail(PFGPU_ERR_ARG,
+                  "pfgpu_residual_noalloc: face %d: only FluxConst and Dirichlet faces", face);
+    if (!on_device(bc_values[face], dev))
+      return fail(PFGPU_ERR_ARG,
+                  "pfgpu_residual_noalloc: face %d table must be memory of the current device",
+                  face);
+  }
+  const double *vg[] = {vg_alpha, vg_n, s_res, s_sat};
+  for (const double *a : vg)
+    if (a && !on_device(a, dev))
+      return fail(PFGPU_ERR_ARG,
+                  "pfgpu_residual_noalloc: per-cell fields must be memory of the current device");
+
   // set-up, once per device, with that device current: the device address of
   // the scratch array (its host-side name is only a stand-in)
-  if (!g_scratch_ptr[dev]) {
-    void *ptr = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
-    if (e != cudaSuccess || !ptr)
-      return fail(PFGPU_ERR_CUDA, "pfgpu_residual_noalloc: cudaGetSymbolAddress failed: %s",
-                  cudaGetErrorString(e));
-    g_scratch_ptr[dev] = static_cast<double *>(ptr);
+  double *scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+      void *ptr = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+      if (e != cudaSuccess || !ptr)
+        return fail(PFGPU_ERR_CUDA, "pfgpu_residual_noalloc: cudaGetSymbolAddress failed: %s",
+                    cudaGetErrorString(e));
+      g_scratch_ptr[dev] = static_cast<double *>(ptr);
+    }
+    scratch = g_scratch_ptr[dev];
   }
-  double *scratch = g_scratch_ptr[dev];
   double *kr = scratch, *dkr = scratch + kMaxCells, *sat = scratch + 2 * kMaxCells,
          *dsat = scratch + 3 * kMaxCells;
   double *zmult = scratch + 4 * kMaxCells, *zface = zmult + kMaxLayers;

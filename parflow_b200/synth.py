@@ -30,7 +30,7 @@ def _spectral_exponential(shape, corr, rng):
     amp = 1.0 / (1.0 + k2)
     noise = rng.standard_normal(pads)
     spec = np.fft.rfftn(noise) * amp
-    field = np.fft.irfftn(spec, s=pads)
+    field = np.fft.irfftn(spec, s=pads, axes=(0, 1, 2))
     return field[: shape[0], : shape[1], : shape[2]]
 
 

@@ -30,4 +30,8 @@ def main(src: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PARFLOW_REF_SRC")
+    if not src:
+        sys.exit("usage: make_reference_outputs.py <parflow source tree> "
+                 "(or set PARFLOW_REF_SRC)")
+    main(src)
