@@ -92,9 +92,12 @@ extern "C" {
 #define PFGPU_ETA_WALKER1 1
 #define PFGPU_ETA_WALKER2 2
 
-/* smoothers (pfsimulator/parflow_lib/mg_semi.c:1251) */
+/* smoothers (pfsimulator/parflow_lib/mg_semi.c:1251): RedBlackGSPoint with
+ * Smoother.Symmetric True (red, black, red) or False (red, black;
+ * rb_GS_point.c:452-470), WJacobi with Smoother.Weight (w_jacobi.c:392) */
 #define PFGPU_SMOOTH_RBGS 0
 #define PFGPU_SMOOTH_WJACOBI 1
+#define PFGPU_SMOOTH_RBGS_NONSYM 2
 
 typedef struct pfgpu_handle pfgpu_handle;
 

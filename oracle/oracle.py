@@ -145,8 +145,8 @@ class Oracle:
         S.eta_choice = ETA[s.eta_choice]
         S.eta_value, S.eta_alpha, S.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
         S.mg_max_levels = s.mg_max_levels
-        S.mg_smoother = 0 if s.mg_smoother == "RedBlackGSPoint" else 1
-        S.wjacobi_weight = 1.0
+        S.mg_smoother = s.smoother_code()
+        S.wjacobi_weight = float(s.wjacobi_weight)
         S.use_jacobian = 1 if s.use_jacobian else 0
         S.derivative_epsilon = s.derivative_epsilon
         self.S = S

@@ -1529,13 +1529,20 @@ static void rb_sweep(const mg_level *l, double *x, const double *b, int colour, 
       }
 }
 
-/* RedBlackGSPoint with MaxIter 1 and Symmetric True: red, black, red; with a
- * zero initial guess the first red sweep is x = b / a0 (PL/rb_GS_point.c:107-240) */
-static void rbgs(const mg_level *l, double *x, const double *b, int zero)
+/* RedBlackGSPoint with MaxIter 1: red, black, red with Symmetric True, red,
+ * black with Symmetric False (the sweep count runs from 1 or 2 up to
+ * 2 MaxIter + 1, PL/rb_GS_point.c:118-140, 221); with a zero initial guess
+ * the first red sweep is x = b / a0 (PL/rb_GS_point.c:128-215) */
+static void rbgs_sym(const mg_level *l, double *x, const double *b, int zero, int symmetric)
 {
   rb_sweep(l, x, b, 0, zero);
   rb_sweep(l, x, b, 1, 0);
-  rb_sweep(l, x, b, 0, 0);
+  if (symmetric)
+    rb_sweep(l, x, b, 0, 0);
+}
+static void rbgs(const mg_level *l, double *x, const double *b, int zero)
+{
+  rbgs_sym(l, x, b, zero, 1);
 }
 
 /* WJacobi with MaxIter 1 (PL/w_jacobi.c:120-290) */
@@ -1579,7 +1586,7 @@ static void smooth(const pfo_mg *mg, const mg_level *l, double *x, const double 
   if (mg->smoother == 1)
     wjacobi(l, x, b, zero, mg->weight);
   else
-    rbgs(l, x, b, zero);
+    rbgs_sym(l, x, b, zero, mg->smoother != 2);
 }
 
 /* r_c = r_f(c) + p2(f below) r_f(f below) + p1(f above) r_f(f above)

@@ -137,10 +137,25 @@ def tfg_small() -> RichardsProblem:
     return p
 
 
+def wjacobi_small() -> RichardsProblem:
+    """The multigrid with the weighted Jacobi smoother (MGSemi.Smoother
+    WJacobi, Smoother.Weight 0.8) on config-2 physics (per-cell van
+    Genuchten files)."""
+    return configs.hetero(nx=15, ny=13, nz=9, nsteps=2, seed=31,
+                          solver=SolverSettings(mg_smoother="WJacobi", wjacobi_weight=0.8))
+
+
+def rbgs_nonsym_small() -> RichardsProblem:
+    """Red/black Gauss-Seidel with Smoother.Symmetric False (red, black per
+    smoothing) on config-0 physics."""
+    return configs.box(nx=13, ny=11, nz=9, nsteps=2, seed=37,
+                       solver=SolverSettings(mg_smoother_symmetric=False))
+
+
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
-          "krtable_linear_small"]
+          "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small"]
 
 
 def get(name: str) -> RichardsProblem:

@@ -941,7 +941,8 @@ __device__ __forceinline__ void team_smooth(const MGLevel<T> &L, T *x, const T *
   const int hx = (L.nx + 1) / 2;
   const int half = hx * L.ny * L.nz;
   const FastDiv fx = fast_div(hx), fy = fast_div(L.ny);
-  for (int sweep = 0; sweep < 3; sweep++) {
+  const int nsweep = smoother == 2 ? 2 : 3;  // non-symmetric: red, black
+  for (int sweep = 0; sweep < nsweep; sweep++) {
     const int colour = sweep == 1 ? 1 : 0;
     const int init = (sweep == 0) ? zero : 0;
     for (int t = r0; t < half; t += rs) {
@@ -1319,8 +1320,10 @@ static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init
   }
   launch_pdl(k_rb_sweep<T, false>, dim3(g.grid), dim3(g.block), st, L, x, b, colour, init, flip);
 }
-// RedBlackGSPoint, MaxIter 1, Symmetric: red, black, red; a zero initial
-// guess turns the first red sweep into x = b / a0 (rb_GS_point.c:107-240)
+// RedBlackGSPoint, MaxIter 1: red, black, red (Symmetric True, smoother 0)
+// or red, black (Symmetric False, smoother 2); a zero initial guess turns the
+// first red sweep into x = b / a0 (rb_GS_point.c:107-240).  Smoother 9 is a
+// single red sweep (kernel timing).
 template <typename T>
 void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st, int *flip, bool h16) {
@@ -1340,8 +1343,14 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
                zero);
     return;
   }
-  if (smoother == 2) {  // a single red sweep (kernel timing)
+  if (smoother == 9) {  // a single red sweep (kernel timing)
     rb_sweep(L, x, b, 0, 0, st, 0, h16);
+    return;
+  }
+  if (smoother == 2) {
+    rb_sweep(L, x, b, 0, zero, st, f, h16);
+    rb_sweep(L, x, b, 1, 0, st, g, h16);
+    if (flip) *flip = f;
     return;
   }
   rb_sweep(L, x, b, 0, zero, st, f, h16);

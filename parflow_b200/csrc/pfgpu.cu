@@ -424,7 +424,7 @@ template <typename T>
 static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
-  const int sk = smoother == 1 ? 2 : 3;
+  const int sk = (smoother == 1 || smoother == 2) ? 2 : 3;
   const int first = mg.mid;
   // block order of the next grid launch: with mg.flip every launch runs in
   // the opposite order of the one before it (the input conversion runs
@@ -1041,7 +1041,9 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   }
   // colour-split x / b on the grid levels (red/black smoother); the tail
   // levels keep the natural layout
-  const bool split = h->d.mg_smoother == PFGPU_SMOOTH_RBGS && env_ll("PFGPU_SPLIT", 1) != 0;
+  const bool split = (h->d.mg_smoother == PFGPU_SMOOTH_RBGS ||
+                      h->d.mg_smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
+                     env_ll("PFGPU_SPLIT", 1) != 0;
   for (int l = 0; l < nl; l++) mg.L[l].split = split && l < mg.mid ? 1 : 0;
   // grid levels large enough for the fused smoother get an output buffer
   // distinct from the input iterate
@@ -1264,6 +1266,11 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
   }
   if (desc->max_restarts != 0) {
     set_err("pfgpu_create: only MaxRestarts 0 is supported");
+    return nullptr;
+  }
+  if (desc->mg_smoother != PFGPU_SMOOTH_RBGS && desc->mg_smoother != PFGPU_SMOOTH_WJACOBI &&
+      desc->mg_smoother != PFGPU_SMOOTH_RBGS_NONSYM) {
+    set_err("pfgpu_create: unknown multigrid smoother %d", desc->mg_smoother);
     return nullptr;
   }
   if (desc->precision != PFGPU_PREC_FP64 && desc->precision != PFGPU_PREC_MIXED &&
@@ -2279,10 +2286,10 @@ int pfgpu_time_kernel(pfgpu_handle *h, int kernel, int reps, double *ms, double 
       case PFGPU_KERNEL_COLOUR_SWEEP:  // one red sweep of the finest level
         if (h->mixed) {
           MGLevel<float> &L = h->mgf.L[0];
-          launch_mg_smooth<float>(L, L.x, L.b, 0, 2, 1.0, h->mgf.wtmp, h->st, nullptr, h->mgf.h16);
+          launch_mg_smooth<float>(L, L.x, L.b, 0, 9, 1.0, h->mgf.wtmp, h->st, nullptr, h->mgf.h16);
         } else {
           MGLevel<double> &L = h->mgd.L[0];
-          launch_mg_smooth<double>(L, L.x, L.b, 0, 2, 1.0, h->mgd.wtmp, h->st);
+          launch_mg_smooth<double>(L, L.x, L.b, 0, 9, 1.0, h->mgd.wtmp, h->st);
         }
         h->launches++;
         break;

@@ -115,6 +115,19 @@ class SolverSettings:
     mg_max_iter: int = 1
     mg_max_levels: int = 100
     mg_smoother: str = "RedBlackGSPoint"
+    # ...MGSemi.Smoother.Symmetric (RedBlackGSPoint: red, black, red when True,
+    # red, black when False) and ...MGSemi.Smoother.Weight (WJacobi)
+    mg_smoother_symmetric: bool = True
+    wjacobi_weight: float = 1.0
+
+    def smoother_code(self) -> int:
+        """PFGPU_SMOOTH_* of the smoother keys: 0 symmetric red/black
+        Gauss-Seidel, 1 weighted Jacobi, 2 non-symmetric red/black."""
+        if self.mg_smoother == "WJacobi":
+            return 1
+        if self.mg_smoother != "RedBlackGSPoint":
+            raise ValueError(f"unknown MGSemi smoother {self.mg_smoother}")
+        return 0 if self.mg_smoother_symmetric else 2
     max_convergence_failures: int = 3
 
 
@@ -479,6 +492,10 @@ class RichardsProblem:
         k["Solver.Linear.Preconditioner.MGSemi.MaxIter"] = s.mg_max_iter
         k["Solver.Linear.Preconditioner.MGSemi.MaxLevels"] = s.mg_max_levels
         k["Solver.Linear.Preconditioner.MGSemi.Smoother"] = s.mg_smoother
+        if s.mg_smoother == "RedBlackGSPoint" and not s.mg_smoother_symmetric:
+            k["Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric"] = "False"
+        if s.mg_smoother == "WJacobi" and s.wjacobi_weight != 1.0:
+            k["Solver.Linear.Preconditioner.MGSemi.Smoother.Weight"] = float(s.wjacobi_weight)
         k["Solver.PrintSubsurfData"] = False
         k["Solver.PrintPressure"] = True
         k["Solver.PrintSaturation"] = True

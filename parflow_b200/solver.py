@@ -78,8 +78,8 @@ class RichardsGPU:
         d.eta_choice = _ETA[s.eta_choice]
         d.eta_value, d.eta_alpha, d.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
         d.mg_max_levels = s.mg_max_levels
-        d.mg_smoother = 0 if s.mg_smoother == "RedBlackGSPoint" else 1
-        d.wjacobi_weight = 1.0
+        d.mg_smoother = s.smoother_code()
+        d.wjacobi_weight = float(s.wjacobi_weight)
         self.desc = d
         self.precision = precision
         h = self.lib.pfgpu_create(C.byref(d), device)
