@@ -235,6 +235,34 @@ int pfgpu_set_bc(pfgpu_handle *h, int face, int type, const double *values);
 int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old,
                            const double *s_old, double dt, double *f);
 
+/* Land-surface sink/source per cell [1/h], the evap_trans vector the
+ * residual subtracts as vol z_mult dt (source + evap_trans)
+ * (nl_function_eval.c:533-541; read from Solver.EvapTrans.FileName or set by
+ * CLM each step, solver_richards.c:1080-1090).  ParFlow layout, host or
+ * device; NULL clears it (zero).  Kept until replaced; the Jacobian does not
+ * depend on it.  The reference's ovrl_bc_flx argument is not read by the
+ * residual (nl_function_eval.c:178), so it has no setter. */
+int pfgpu_set_evap_trans(pfgpu_handle *h, const double *et);
+
+/* Face velocities [m/h] and overland fluxes of the residual evaluated at p:
+ * what NlFunctionEval writes into x_velocity, y_velocity, z_velocity (interior
+ * faces flux / area, nl_function_eval.c:845-848; boundary faces as the patch
+ * loops store them, :1227-1230, :1432, :1681-1687, :1775-1781) and
+ * q_overlnd_x / q_overlnd_y (ke, kn of each column on an overland z_upper
+ * face, :1648-1656; zero otherwise).  p = NULL takes the handle's pressure
+ * state (the solution of the last pfgpu_newton_solve / pfgpu_advance step);
+ * p_old / s_old = NULL keep the old pressure and saturation of the last
+ * solve or evaluation, so after a solve pfgpu_face_velocities(h, NULL, NULL,
+ * NULL, dt, ...) gives the velocities of the last residual evaluation of
+ * that step, as the reference's state holds after KINSol returns.  Outputs
+ * in ParFlow layout on the face grids (one cell wider along their axis, one
+ * ghost layer, ghosts written as 0): vx (nx+3)(ny+2)(nz+2), vy
+ * (nx+2)(ny+3)(nz+2), vz (nx+2)(ny+2)(nz+3), qx / qy on the 2-D grid
+ * (nx+2)(ny+2)*3; host or device; any may be NULL. */
+int pfgpu_face_velocities(pfgpu_handle *h, const double *p, const double *p_old,
+                          const double *s_old, double dt, double *vx, double *vy, double *vz,
+                          double *qx, double *qy);
+
 /* y = J(p) x with the analytic 7-point Jacobian assembled at p
  * (KINSolMatVec + RichardsJacobianEval with symm_part = 0,
  * pfsimulator/parflow_lib/richards_jacobian_eval.c:165, :217; Matvec,

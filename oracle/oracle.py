@@ -33,7 +33,12 @@ class Problem(C.Structure):
                 ("mannings", _dp),
                 ("ov_epsilon", C.c_double),
                 ("ov_p_old", _dp),
-                ("kr_table", C.c_void_p)]
+                ("kr_table", C.c_void_p),
+                ("evap_trans", _dp)]
+
+
+class FluxOut(C.Structure):
+    _fields_ = [("vx", _dp), ("vy", _dp), ("vz", _dp), ("qx", _dp), ("qy", _dp)]
 
 
 class Settings(C.Structure):
@@ -68,6 +73,8 @@ def lib():
         build()
         L = C.CDLL(LIB)
         L.pfo_residual.argtypes = [C.POINTER(Problem), C.c_double, _dp, _dp, _dp, _dp]
+        L.pfo_residual_out.argtypes = [C.POINTER(Problem), C.c_double, _dp, _dp, _dp, _dp,
+                                       C.POINTER(FluxOut)]
         L.pfo_jacobian.argtypes = [C.POINTER(Problem), C.c_double, _dp, C.c_int, C.POINTER(_dp)]
         L.pfo_matvec7.argtypes = [C.POINTER(Problem), C.POINTER(_dp), _dp, _dp]
         L.pfo_saturation.argtypes = [C.POINTER(Problem), _dp, _dp, C.c_int]
@@ -129,6 +136,10 @@ class Oracle:
         if prob.terrain_following:
             P.sslope_x, P.sslope_y = _ptr(sx), _ptr(sy)
         P.ov_epsilon = 1.0e-5
+        if prob.evap_trans is not None:
+            et = np.ascontiguousarray(prob.field3d(prob.evap_trans), dtype=np.float64)
+            self._keep.append(et)
+            P.evap_trans = _ptr(et)
         self._table = None
         if prob.kr_table:
             method = {"Spline": 0, "Linear": 1}[prob.kr_table[0]]
@@ -173,6 +184,23 @@ class Oracle:
         f = np.empty_like(p)
         lib().pfo_residual(C.byref(self.P), dt, _ptr(p), _ptr(p_old), _ptr(s_old), _ptr(f))
         return f
+
+    def residual_velocities(self, p, p_old, s_old, dt):
+        """F(p) with the face velocities and overland fluxes the evaluation
+        writes: (f, vx (nz, ny, nx+1), vy (nz, ny+1, nx), vz (nz+1, ny, nx),
+        qx, qy (ny, nx))."""
+        p, p_old, s_old = (np.ascontiguousarray(x, dtype=np.float64) for x in (p, p_old, s_old))
+        nz, ny, nx = p.shape
+        f = np.empty_like(p)
+        vx = np.zeros((nz, ny, nx + 1))
+        vy = np.zeros((nz, ny + 1, nx))
+        vz = np.zeros((nz + 1, ny, nx))
+        qx = np.zeros((ny, nx))
+        qy = np.zeros((ny, nx))
+        out = FluxOut(_ptr(vx), _ptr(vy), _ptr(vz), _ptr(qx), _ptr(qy))
+        lib().pfo_residual_out(C.byref(self.P), dt, _ptr(p), _ptr(p_old), _ptr(s_old), _ptr(f),
+                               C.byref(out))
+        return f, vx, vy, vz, qx, qy
 
     def saturation(self, p, der=0):
         p = np.ascontiguousarray(p, dtype=np.float64)

@@ -666,6 +666,16 @@ static void ovd_der(const pfo_problem *pb, const double *p, const double *op, do
 void pfo_residual(const pfo_problem *pb, double dt, const double *p,
                   const double *p_old, const double *s_old, double *f)
 {
+  pfo_residual_out(pb, dt, p, p_old, s_old, f, NULL);
+}
+
+void pfo_residual_out(const pfo_problem *pb, double dt, const double *p,
+                      const double *p_old, const double *s_old, double *f,
+                      const pfo_flux_out *out)
+{
+  static const pfo_flux_out none = {NULL, NULL, NULL, NULL, NULL};
+  if (!out)
+    out = &none;
   const int nx = pb->nx, ny = pb->ny, nz = pb->nz;
   const long N = (long)nx * ny * nz;
   const double dx = pb->dx, dy = pb->dy, dz = pb->dz;
@@ -688,7 +698,8 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
         f[c] = (sat[c] * rho - s_old[c] * rho) * pb->porosity * vol * 1.0 * 1.0 * zm[k];
         f[c] += pb->sstorage * vol * 1.0 * 1.0 * zm[k]
                 * (p[c] * sat[c] * rho - p_old[c] * s_old[c] * rho);
-        f[c] -= vol * 1.0 * 1.0 * zm[k] * dt * (0.0 + 0.0);
+        /* sources: PhaseSources (0 here) plus the evap_trans sink (:533-541) */
+        f[c] -= vol * 1.0 * 1.0 * zm[k] * dt * (0.0 + (pb->evap_trans ? pb->evap_trans[c] : 0.0));
       }
 
   /* interior faces :696-854, gravity terms from the subsurface slopes */
@@ -732,6 +743,14 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           u_upper = ffz * 1.0 * 1.0 * HARMONIC_DZ(pb->kz[c], pb->kz[u], zc, zu) * diff_l
                     * UPSTREAM(lower, upper, kr[c] * rho, kr[u] * rho) / visc;
         }
+        /* face velocities :845-848 (flow barriers 1); the boundary faces
+         * are written by the patch loops below */
+        if (out->vx && i + 1 < nx)
+          out->vx[(i + 1) + (long)(nx + 1) * (j + (long)ny * k)] = u_right / (ffx * zm[k] * 1.0);
+        if (out->vy && j + 1 < ny)
+          out->vy[i + (long)nx * ((j + 1) + (long)(ny + 1) * k)] = u_front / (ffy * zm[k] * 1.0);
+        if (out->vz && k + 1 < nz)
+          out->vz[c + (long)nx * ny] = u_upper / (ffz * 1.0 * 1.0);
         f[c] += dt * (u_right + u_front + u_upper);
         if (i + 1 < nx) f[c + 1] += -dt * u_right;
         if (j + 1 < ny) f[c + nx] += -dt * u_front;
@@ -772,7 +791,19 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
             q_overlnd = q_overlnd
                         + vol * dt / dz * (exp((p[c] < 0.0 ? p[c] : 0.0) * 0.0) * 0.0);
           f[c] += q_overlnd;
-          f[c] += dt * 1.0 * (ffz * vals[i + nx * j]);
+          double u_new = ffz * vals[i + nx * j];
+          f[c] += dt * 1.0 * u_new;
+          /* q_overlnd_x/y = ke, kn of the column; the top face velocity
+           * carries the ponding and routing term (:1648-1687) */
+          if (out->qx)
+            out->qx[i + (long)nx * j] = ke[io];
+          if (out->qy)
+            out->qy[i + (long)nx * j] = kn[io];
+          if (out->vz)
+          {
+            u_new += q_overlnd / dt;
+            out->vz[c + (long)nx * ny] = u_new / ffz;
+          }
         }
       continue;
     }
@@ -785,15 +816,32 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
           long c = IDX(i, j, k);
           double value = vals[face_index(pb, face, i, j, k)];
           double dir = (face & 1) ? 1.0 : -1.0;
-          double u_new;
+          double u_new, h_face = 0.0, vel;
+          /* this face's entry of vx / vy / vz (the patch loops' vel_idx) */
+          double *vslot = NULL;
+          if (face < 2 && out->vx)
+            vslot = out->vx + (i + (face & 1)) + (long)(nx + 1) * (j + (long)ny * k);
+          else if (face >= 2 && face < 4 && out->vy)
+            vslot = out->vy + i + (long)nx * ((j + (face & 1)) + (long)(ny + 1) * k);
+          else if (face >= 4 && out->vz)
+            vslot = out->vz + i + (long)nx * (j + (long)ny * (k + (face & 1)));
           if (type == PFO_BC_FLUX || type == PFO_BC_SEEPAGE)
           {
             /* FluxConst, or SeepageFace (:1692-1784): a flux face whose top
              * face also drains the ponded water, (vol / dz) dt max(p, 0) */
+            double q_overlnd = 0.0;
             if (type == PFO_BC_SEEPAGE && face == 5)
-              f[c] += (vol / dz) * dt * (PFMAX(p[c], 0.0) - 0.0);
+            {
+              q_overlnd = (vol / dz) * dt * (PFMAX(p[c], 0.0) - 0.0);
+              f[c] += q_overlnd;
+            }
             double h = (face < 2) ? ffx * zm[k] : (face < 4) ? ffy * zm[k] : ffz;
             u_new = h * value;
+            /* FluxBC stores the patch value itself (:1432); SeepageFaceBC
+             * (u_new + q_overlnd / dt) / h (:1775-1781) */
+            vel = (type == PFO_BC_FLUX) ? value : (u_new + q_overlnd / dt) / h;
+            if (vslot)
+              *vslot = vel;
           }
           else
           {
@@ -837,6 +885,10 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
               }
               u_new = u_new * h * (pb->kz[c] / visc) * 2.0 * (lower - upper);
             }
+            /* DirichletBC: u_new / h (:1227-1230) */
+            h_face = (face < 2) ? ffx * zm[k] : (face < 4) ? ffy * zm[k] : ffz;
+            if (vslot)
+              *vslot = u_new / h_face;
           }
           f[c] += dt * dir * u_new;
         }

@@ -60,6 +60,9 @@ typedef struct {
   /* relative permeability from a lookup table instead of the closed form
    * (Geom.domain.RelPerm.NumSamplePoints > 0), or NULL */
   const pfo_vgtable *kr_table;
+  /* land-surface sink/source per cell [1/h] (the evap_trans vector), or
+   * NULL = 0 (nl_function_eval.c:533-541) */
+  const double *evap_trans;
 } pfo_problem;
 
 typedef struct {
@@ -84,6 +87,18 @@ typedef struct {
 /* van Genuchten (problem_saturation.c:221-415, problem_phase_rel_perm.c:567-1361) */
 void pfo_saturation(const pfo_problem *pb, const double *p, double *s, int der);
 void pfo_relperm(const pfo_problem *pb, const double *p, double *kr, int der);
+
+/* face velocities and overland fluxes written by the residual evaluation
+ * (nl_function_eval.c:846-848 interior faces, the BC loops' vel_vec for the
+ * boundary faces, q_overlnd_x/y on an overland z_upper patch); dense, x
+ * fastest: vx (nz, ny, nx+1) with face i between cells i-1 and i, vy
+ * (nz, ny+1, nx), vz (nz+1, ny, nx), qx / qy (ny, nx).  Any may be NULL. */
+typedef struct {
+  double *vx, *vy, *vz, *qx, *qy;
+} pfo_flux_out;
+void pfo_residual_out(const pfo_problem *pb, double dt, const double *p,
+                      const double *p_old, const double *s_old, double *f,
+                      const pfo_flux_out *out);
 
 /* residual F(p) at (dt, time-fixed BC tables) (nl_function_eval.c:167-2323) */
 void pfo_residual(const pfo_problem *pb, double dt, const double *p,

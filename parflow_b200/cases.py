@@ -152,10 +152,35 @@ def rbgs_nonsym_small() -> RichardsProblem:
                        solver=SolverSettings(mg_smoother_symmetric=False))
 
 
+def vel_small() -> RichardsProblem:
+    """Face velocities written by the residual (Solver.PrintVelocities) on
+    config-2 physics with a Dirichlet x_lower face, a SeepageFace x_upper
+    face, a flux top and a seeded land-surface sink/source (evap_trans)."""
+    import numpy as np
+
+    p = configs.hetero(nx=12, ny=10, nz=8, nsteps=2, seed=41)
+    p.bc["x_lower"] = BC(BC_DIRICHLET, (1.8,), ref_patch="z_lower")
+    p.bc["x_upper"] = BC(BC_SEEPAGE, (0.0,))
+    rng = np.random.default_rng(41)
+    p.evap_trans = 0.02 * (rng.random(p.shape) - 0.5)
+    p.print_velocities = True
+    return p
+
+
+def vel_overland_small() -> RichardsProblem:
+    """Face velocities and the overland fluxes q_overlnd_x / y of the
+    ponded kinematic overland case (Solver.PrintQxOverland / PrintQyOverland)."""
+    p = overland_small()
+    p.nsteps = 3
+    p.print_velocities = True
+    return p
+
+
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
-          "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small"]
+          "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
+          "vel_overland_small"]
 
 
 def get(name: str) -> RichardsProblem:

@@ -177,6 +177,11 @@ struct pfgpu_handle {
   double sqrt_relfunc = 0.0;
   double *dq_w = nullptr, *dq_f = nullptr;
   double *krt = nullptr;  // relative-permeability lookup table (device)
+  double *et = nullptr;   // evap_trans sink/source per cell (dense, device)
+  // face velocities and overland fluxes (pfgpu_face_velocities): dense
+  // vx, vy, vz, qx, qy in one allocation, and a staging buffer of the
+  // largest ParFlow-layout face grid for host outputs
+  double *vel = nullptr, *vstage = nullptr;
   int *kerr = nullptr;   // device error word of the pipelined kernels
   int *hkerr = nullptr;  // pinned host mirror
   // discrete adjoint: recorded trajectory p_0 .. p_len (dense, device) and
@@ -1209,6 +1214,9 @@ static void destroy_impl(pfgpu_handle *h) {
   cudaFree(h->dq_w);
   cudaFree(h->dq_f);
   cudaFree(h->krt);
+  cudaFree(h->et);
+  cudaFree(h->vel);
+  cudaFree(h->vstage);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   cudaFree(h->hist);
   cudaFree(h->adj);
@@ -1793,6 +1801,80 @@ int pfgpu_nl_function_eval(pfgpu_handle *h, const double *p, const double *p_old
     return PFGPU_ERR_CUDA;
   feval(h, h->unew, dt, h->fval);
   return out_vec(h, h->fval, f);
+}
+
+int pfgpu_set_evap_trans(pfgpu_handle *h, const double *et) {
+  if (!h) { set_err("pfgpu_set_evap_trans: null handle"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  if (!et) {
+    h->P.et = nullptr;
+    return PFGPU_OK;
+  }
+  if (!h->et && dalloc(&h->et, h->N)) return PFGPU_ERR_NOMEM;
+  if (in_vec(h, et, h->et)) return PFGPU_ERR_CUDA;
+  h->P.et = h->et;
+  return PFGPU_OK;
+}
+
+int pfgpu_face_velocities(pfgpu_handle *h, const double *p, const double *p_old,
+                          const double *s_old, double dt, double *vx, double *vy, double *vz,
+                          double *qx, double *qy) {
+  if (!h) { set_err("pfgpu_face_velocities: null handle"); return PFGPU_ERR_ARG; }
+  if (!(dt > 0.0)) { set_err("pfgpu_face_velocities: dt must be positive"); return PFGPU_ERR_ARG; }
+  CK(cudaSetDevice(h->device));
+  const long long nx = h->nx, ny = h->ny, nz = h->nz;
+  const long long nvx = (nx + 1) * ny * nz, nvy = nx * (ny + 1) * nz, nvz = nx * ny * (nz + 1);
+  const long long nq = nx * ny;
+  if (!h->vel) {
+    const long long pad_max = std::max({(nx + 3) * (ny + 2) * (nz + 2),
+                                        (nx + 2) * (ny + 3) * (nz + 2),
+                                        (nx + 2) * (ny + 2) * (nz + 3)});
+    if (dalloc(&h->vel, nvx + nvy + nvz + 2 * nq) || dalloc(&h->vstage, pad_max))
+      return PFGPU_ERR_NOMEM;
+  }
+  VelOut V{h->vel, h->vel + nvx, h->vel + nvx + nvy, h->vel + nvx + nvy + nvz,
+           h->vel + nvx + nvy + nvz + nq};
+  // the overland fluxes exist only on an overland z_upper face: zero elsewhere
+  CK(cudaMemsetAsync(V.qx, 0, 2 * nq * sizeof(double), h->st));
+  const double *u = h->u;
+  if (p) {
+    if (in_vec(h, p, h->unew)) return PFGPU_ERR_CUDA;
+    u = h->unew;
+  }
+  if ((p_old && in_vec(h, p_old, h->p_old)) || (s_old && in_vec(h, s_old, h->s_old)))
+    return PFGPU_ERR_CUDA;
+  h->P.ov_pold = h->p_old;
+  vg_state(h, u, false);
+  launch_residual(h->P, u, h->p_old, h->s_old, h->kr, h->sat, dt, h->bb, h->st, &V);
+  h->launches++;
+  CK(cudaGetLastError());
+  // ParFlow layouts: the face grids grown by one along their axis, each with
+  // a one-cell ghost frame (x_grid / y_grid / z_grid vectors of
+  // solver_richards.c:5110-5160); q on the 2-D grid, one plane plus ghosts
+  struct Out {
+    const double *src;
+    double *dst;
+    int ax, ay, az;
+  } outs[5] = {{V.vx, vx, (int)nx + 1, (int)ny, (int)nz},
+               {V.vy, vy, (int)nx, (int)ny + 1, (int)nz},
+               {V.vz, vz, (int)nx, (int)ny, (int)nz + 1},
+               {V.qx, qx, (int)nx, (int)ny, 1},
+               {V.qy, qy, (int)nx, (int)ny, 1}};
+  for (const Out &o : outs) {
+    if (!o.dst) continue;
+    const long long np = (long long)(o.ax + 2) * (o.ay + 2) * (o.az + 2);
+    if (is_device_ptr(o.dst)) {
+      launch_pad(o.src, o.dst, o.ax, o.ay, o.az, h->st);
+      h->launches++;
+    } else {
+      launch_pad(o.src, h->vstage, o.ax, o.ay, o.az, h->st);
+      h->launches++;
+      CK(cudaMemcpyAsync(o.dst, h->vstage, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+      CK(cudaStreamSynchronize(h->st));
+    }
+  }
+  CK(cudaGetLastError());
+  return PFGPU_OK;
 }
 
 int pfgpu_jacobian_matvec(pfgpu_handle *h, const double *p, double dt, const double *x,

@@ -47,6 +47,9 @@ struct DevProblem {
   const double *krt;
   int krt_method, krt_npts;  // method 0 spline, 1 linear
   double krt_interval, krt_min;
+  // land-surface sink/source per cell [1/h] (the evap_trans vector,
+  // nl_function_eval.c:533-541), dense interior layout, or null = 0
+  const double *et;
   // thread-block shapes (bx, by) of the residual, Jacobian and matvec
   // launches picked by pfgpu_autotune; (0, 0) = the default heuristic.
   // Host-side launch configuration only: no kernel reads it.
@@ -471,6 +474,14 @@ __device__ __forceinline__ void ovd_der_edges(const DevProblem &P, const OvdCol 
     }
   }
 }
+
+// Face velocities and overland fluxes a residual evaluation writes (all
+// dense, x fastest; null pointers are skipped): vx (nz, ny, nx+1) with face i
+// between cells i-1 and i, vy (nz, ny+1, nx), vz (nz+1, ny, nx), qx / qy
+// (ny, nx) on the top layer of an overland z_upper face.
+struct VelOut {
+  double *vx, *vy, *vz, *qx, *qy;
+};
 
 // Index of a boundary cell in its face table.
 __device__ __forceinline__ int face_slot(const DevProblem &P, int face, int i, int j, int k) {

@@ -34,9 +34,10 @@ struct PCOut {
 void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
                    double *dsat, cudaStream_t st);
 void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStream_t st);
+// vel: also write the face velocities and overland fluxes (null: F only)
 void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      const double *s_old, const double *kr, const double *sat, double dt,
-                     double *f, cudaStream_t st);
+                     double *f, cudaStream_t st, const VelOut *vel = nullptr);
 template <typename TJ, typename TP>
 void launch_jacobian(const DevProblem &P, const double *p, const double *kr, const double *dkr,
                      const double *sat, const double *dsat, double dt, JacOut<TJ> J,

@@ -63,11 +63,15 @@ __global__ void k_saturation(DevProblem P, const double *__restrict__ p, double 
 // fluxes scattered from the k-1, j-1, i-1 neighbours, the cell's own three
 // upper faces, and finally the boundary patches in patch order.
 // SURF: slopes and/or overland flow present (false: flat box, the lean path)
-template <bool SURF>
+// VEL: also write the face velocities and overland fluxes (VelOut): interior
+// faces as flux / area (nl_function_eval.c:845-848), boundary faces as the
+// patch loops store them (vel_vec[vel_idx], :1227-1230, :1432, :1681-1687,
+// :1775-1781), q_overlnd_x / y = ke, kn of the column (:1648-1656)
+template <bool SURF, bool VEL = false>
 __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double *__restrict__ p,
                            const double *__restrict__ p_old, const double *__restrict__ s_old,
                            const double *__restrict__ kr, const double *__restrict__ satv,
-                           double dt, double *__restrict__ f) {
+                           double dt, double *__restrict__ f, VelOut V = VelOut{}) {
   pdl_enter();
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
@@ -81,7 +85,7 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
   const double so = s_old[c];
   double fc = (sat * rho - so * rho) * P.porosity * vol * 1.0 * 1.0 * zm;
   fc += P.sstorage * vol * 1.0 * 1.0 * zm * (pc * sat * rho - p_old[c] * so * rho);
-  fc -= vol * 1.0 * 1.0 * zm * dt * (0.0 + 0.0);
+  fc -= vol * 1.0 * 1.0 * zm * dt * (0.0 + (P.et ? __ldg(P.et + c) : 0.0));
 
   const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
   const double krc = kr[c];
@@ -119,6 +123,14 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
                      __ldg(P.zmult + k + 1), k);
   }
   fc += dt * (u_right + u_front + u_upper);
+  if (VEL) {
+    const long long fx1 = (long long)(P.nx + 1), cyz = (long long)P.nx * (P.ny + 1);
+    if (V.vx && i + 1 < P.nx)
+      V.vx[(i + 1) + fx1 * (j + (long long)P.ny * k)] = u_right / (P.dy * P.dz * zm * 1.0);
+    if (V.vy && j + 1 < P.ny)
+      V.vy[i + (long long)P.nx * (j + 1) + cyz * k] = u_front / (P.dx * P.dz * zm * 1.0);
+    if (V.vz && k + 1 < P.nz) V.vz[c + sz] = u_upper / (P.dx * P.dy * 1.0 * 1.0);
+  }
 
   // boundary patches (nl_function_eval.c:979-1435)
   const double ffx = P.dy * P.dz, ffy = P.dx * P.dz, ffz = P.dx * P.dy;
@@ -129,12 +141,18 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
     const double value = __ldg(P.bc_val[face] + face_slot(P, face, i, j, k));
     const double dir = (face & 1) ? 1.0 : -1.0;
     double u_new;
+    double vel = 0.0;  // this face's velocity (VEL)
     if (P.bc_type[face] == 0 || P.bc_type[face] == 5) {
       // FluxConst, or SeepageFace (nl_function_eval.c:1692-1784): a flux
       // face whose top face also drains the ponded water
-      if (P.bc_type[face] == 5 && face == 5) fc += (vol / P.dz) * dt * (pmax0(pc) - 0.0);
+      double q_ov = 0.0;
+      if (P.bc_type[face] == 5 && face == 5) {
+        q_ov = (vol / P.dz) * dt * (pmax0(pc) - 0.0);
+        fc += q_ov;
+      }
       double h = (face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz;
       u_new = h * value;
+      if (VEL) vel = (P.bc_type[face] == 0) ? value : (u_new + q_ov / dt) / h;
     } else if (SURF && P.bc_type[face] == 2) {
       // OverlandKinematic top face (nl_function_eval.c:1786-2000): ponding and
       // routing term, then the rain flux like FluxConst
@@ -154,9 +172,15 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
       } else if (o.sfy > 0.0) {  // outflow through the lower y edge
         ks = -(o.sfy / (o.sq * o.n)) * pow(pmax0(pc), (5.0 / 3.0));
       }
-      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
-            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      const double q_ov = vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+                          dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      fc += q_ov;
       u_new = ffz * value;
+      if (VEL) {
+        vel = (u_new + q_ov / dt) / ffz;
+        if (V.qx) V.qx[i + (long long)P.nx * j] = ke;
+        if (V.qy) V.qy[i + (long long)P.nx * j] = kn;
+      }
     } else if (SURF && P.bc_type[face] == 4) {
       // OverlandFlow top face (nl_function_eval.c:1437-1690): each face flux
       // is the upwind part of the two columns' own fluxes; the spin-up
@@ -167,9 +191,15 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
       const double qs = ovf_q<false>(P, p, i, j - 1), qm = ovf_q<false>(P, p, i, j),
                    qn = ovf_q<false>(P, p, i, j + 1);
       const double ks = pmax0(qs) - pmax0(-qm), kn = pmax0(qm) - pmax0(-qn);
-      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
-            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      const double q_ov = vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+                          dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      fc += q_ov;
       u_new = ffz * value;
+      if (VEL) {
+        vel = (u_new + q_ov / dt) / ffz;
+        if (V.qx) V.qx[i + (long long)P.nx * j] = ke;
+        if (V.qy) V.qy[i + (long long)P.nx * j] = kn;
+      }
     } else if (SURF && P.bc_type[face] == 3) {
       // OverlandDiffusive top face (nl_function_eval.c:2028-2259): the same
       // ponding and routing term with the diffusive-wave face fluxes
@@ -179,9 +209,15 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
       const double ke = ovd_qx(o), kn = ovd_qy(o);
       const double kw = i > 0 ? ovd_qx(ovd_col(P, p, i - 1, j)) : qxw;
       const double ks = j > 0 ? ovd_qy(ovd_col(P, p, i, j - 1)) : qys;
-      fc += vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
-            dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      const double q_ov = vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+                          dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      fc += q_ov;
       u_new = ffz * value;
+      if (VEL) {
+        vel = (u_new + q_ov / dt) / ffz;
+        if (V.qx) V.qx[i + (long long)P.nx * j] = ke;
+        if (V.qy) V.qy[i + (long long)P.nx * j] = kn;
+      }
     } else {
       const VG v = vg_at(P, c);
       double krg = vg_kr(P, value, v.alpha, v.n);
@@ -212,8 +248,19 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
         }
         u_new = u_new * ffz * (kzc * P.inv_visc) * 2.0 * (lower - upper);
       }
+      // DirichletBC: u_new / h (nl_function_eval.c:1227-1230)
+      if (VEL) vel = u_new / ((face < 2) ? ffx * zm : (face < 4) ? ffy * zm : ffz);
     }
     fc += dt * dir * u_new;
+    if (VEL) {
+      const int up = face & 1;
+      if (face < 2 && V.vx)
+        V.vx[(i + up) + (long long)(P.nx + 1) * (j + (long long)P.ny * k)] = vel;
+      else if (face >= 2 && face < 4 && V.vy)
+        V.vy[i + (long long)P.nx * (j + up) + (long long)P.nx * (P.ny + 1) * k] = vel;
+      else if (face >= 4 && V.vz)
+        V.vz[c + up * sz] = vel;
+    }
   }
   f[c] = fc;
 }
@@ -628,13 +675,25 @@ void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStre
 
 void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      const double *s_old, const double *kr, const double *sat, double dt,
-                     double *f, cudaStream_t st) {
+                     double *f, cudaStream_t st, const VelOut *vel) {
   dim3 g, b;
   shape_tuned(P.nx, P.ny, P.nz, 256, P.tile[0], g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
-    launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
+  const bool surf = P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4;
+  if (vel) {
+    if (surf)
+      launch_pdl(k_residual<true, true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
+                 *vel);
+    else
+      launch_pdl(k_residual<false, true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt,
+                 f, *vel);
+    return;
+  }
+  if (surf)
+    launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
+               VelOut{});
   else
-    launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f);
+    launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
+               VelOut{});
 }
 
 template <typename TJ, typename TP>

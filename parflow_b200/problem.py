@@ -167,6 +167,11 @@ class RichardsProblem:
     # NumSamplePoints / MinPressureHead / InterpolationMethod): None or
     # (method "Spline" | "Linear", sample points, min pressure head)
     kr_table: Optional[tuple] = None
+    # land-surface sink/source per cell [1/h] (Solver.EvapTransFile /
+    # Solver.EvapTrans.FileName): None, a float or an (nz, ny, nx) array
+    evap_trans: object = None
+    # reference output of the face velocities (Solver.PrintVelocities)
+    print_velocities: bool = False
     solver: SolverSettings = field(default_factory=SolverSettings)
     name: str = "richards"
 
@@ -496,6 +501,17 @@ class RichardsProblem:
             k["Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric"] = "False"
         if s.mg_smoother == "WJacobi" and s.wjacobi_weight != 1.0:
             k["Solver.Linear.Preconditioner.MGSemi.Smoother.Weight"] = float(s.wjacobi_weight)
+        if self.evap_trans is not None:
+            write_pfb(pj("evap_trans.pfb"), self.field3d(self.evap_trans), self.dx, self.dy,
+                      self.dz, dist=True)
+            k["Solver.EvapTransFile"] = True
+            k["Solver.EvapTrans.FileName"] = "evap_trans.pfb"
+        if self.print_velocities:
+            k["Solver.PrintVelocities"] = True
+            if any(bc.kind in (BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND)
+                   for bc in self.bc.values()):
+                k["Solver.PrintQxOverland"] = True
+                k["Solver.PrintQyOverland"] = True
         k["Solver.PrintSubsurfData"] = False
         k["Solver.PrintPressure"] = True
         k["Solver.PrintSaturation"] = True

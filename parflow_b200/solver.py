@@ -100,6 +100,8 @@ class RichardsGPU:
                                                      float(prob.kr_table[2])),
                     "set_relperm_table")
         self._upload_fields()
+        if prob.evap_trans is not None:
+            self.set_evap_trans(prob.field3d(prob.evap_trans))
         self.set_time(prob.start_time + prob.dt)
 
     def close(self):
@@ -177,6 +179,36 @@ class RichardsGPU:
     # ---- function-level operators (ParFlow layout in/out) -------------------
     def _io(self, a):
         return a if hasattr(a, "data_ptr") else pad(a)
+
+    def set_evap_trans(self, et):
+        """Per-cell land-surface sink/source [1/h] (interior (nz, ny, nx)), or
+        None to clear it."""
+        if et is None:
+            L.check(self.lib.pfgpu_set_evap_trans(self.h, None), "set_evap_trans")
+            return
+        a = pad(np.broadcast_to(np.asarray(et, dtype=np.float64), self.prob.shape))
+        L.check(self.lib.pfgpu_set_evap_trans(self.h, _ptr(a)), "set_evap_trans")
+
+    def face_velocities(self, dt, p=None, p_old=None, s_old=None):
+        """Face velocities and overland fluxes of the residual at p (None:
+        the handle's pressure state and the last step's old state), dense:
+        vx (nz, ny, nx+1), vy (nz, ny+1, nx), vz (nz+1, ny, nx), qx, qy
+        (ny, nx)."""
+        nz, ny, nx = self.prob.shape
+        vx = np.zeros((nz + 2, ny + 2, nx + 3))
+        vy = np.zeros((nz + 2, ny + 3, nx + 2))
+        vz = np.zeros((nz + 3, ny + 2, nx + 2))
+        qx = np.zeros((3, ny + 2, nx + 2))
+        qy = np.zeros((3, ny + 2, nx + 2))
+        bufs = []  # padded inputs, alive through the call
+        for a in (p, p_old, s_old):
+            bufs.append(None if a is None else pad(np.ascontiguousarray(a, dtype=np.float64)))
+        rc = self.lib.pfgpu_face_velocities(self.h, *[None if b is None else _ptr(b) for b in bufs],
+                                            float(dt), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(qx),
+                                            _ptr(qy))
+        L.check(rc, "face_velocities")
+        return (unpad(vx), unpad(vy), unpad(vz), np.ascontiguousarray(qx[1, 1:-1, 1:-1]),
+                np.ascontiguousarray(qy[1, 1:-1, 1:-1]))
 
     def nl_function_eval(self, p, p_old, s_old, dt):
         f = np.zeros(tuple(x + 2 for x in self.prob.shape))

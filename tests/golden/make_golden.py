@@ -62,7 +62,18 @@ def make(case_name: str, max_dumps: int = 6):
 
         def stack(arrs):
             return np.stack(arrs) if arrs else np.zeros((0,) + prob.shape)
-        out = {"press": press, "counts": counts,
+        # face velocities (and overland fluxes) after every step, where the
+        # case prints them (Solver.PrintVelocities / PrintQ{x,y}Overland)
+        extra = {}
+        for key, tag in (("velx", "velx"), ("vely", "vely"), ("velz", "velz"),
+                         ("qx_overland", "qx_overland"), ("qy_overland", "qy_overland")):
+            files = [os.path.join(wd, f"{run}.out.{tag}.{t:05d}.pfb")
+                     for t in range(1, prob.nsteps + 1)]
+            if all(os.path.exists(f) for f in files):
+                extra[key] = np.stack([read_pfb(f) for f in files])
+        if prob.evap_trans is not None:
+            extra["evap_trans"] = prob.field3d(prob.evap_trans)
+        out = {"press": press, "counts": counts, **extra,
                "perm": prob.field3d(prob.perm), "alpha": prob.field3d(prob.vg_alpha),
                "n": prob.field3d(prob.vg_n)}
         fe = [read_dump(f) for f in list_dumps(dump, "fe")]

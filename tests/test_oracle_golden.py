@@ -86,3 +86,28 @@ def test_mg_hierarchy_shape():
     assert lv[-1][:3] == (1, 1, 1) and lv[-1][3] == -1
     dirs = [d for *_, d in lv[:-1]]
     assert dirs[:4] == [2, 0, 1, 2]
+
+
+VEL_CASES = [n for n in CASES if n.startswith("vel_")]
+
+
+@pytest.mark.parametrize("name", VEL_CASES)
+def test_face_velocities_bitexact(name, golden):
+    """Face velocities (and overland fluxes) written by the residual at each
+    step's solution equal the reference's velx / vely / velz (qx_overland,
+    qy_overland) outputs bit for bit: interior faces, Dirichlet, flux and
+    seepage faces, the overland top face, with an evap_trans sink/source."""
+    g = golden(name)
+    prob = cases.get(name)
+    orc = Oracle(prob)
+    plan = prob.time_plan()
+    for n in range(1, prob.nsteps + 1):
+        t, dt = plan[n - 1]
+        orc.set_time(t)
+        p_old, p = g["press"][n - 1], g["press"][n]
+        _, vx, vy, vz, qx, qy = orc.residual_velocities(p, p_old, orc.saturation(p_old), dt)
+        for key, mine in (("velx", vx), ("vely", vy), ("velz", vz),
+                          ("qx_overland", qx), ("qy_overland", qy)):
+            if key in g:
+                ref = g[key][n - 1].reshape(mine.shape)
+                assert np.array_equal(mine, ref), (name, n, key, np.abs(mine - ref).max())
