@@ -14,6 +14,11 @@
 #   oracle/_ref/bin/parflow_hook   seq build linked with oracle/ref_hooks.c via
 #                                  ld --wrap: dumps F(p), J*v and PC(r) operands
 #                                  when PFREF_DUMP_DIR is set.
+#   oracle/_ref/bin/parflow_gpu    seq build with the GPU nonlinear-solver module
+#                                  (parflow_b200/pfmodule/, libpfgpu.so) linked
+#                                  in via ld --wrap; selected per run by
+#                                  Solver.Nonlinear.GPU True (target gpu, after
+#                                  libpfgpu.so is built).
 # Nothing is written outside oracle/_ref/.  The two generated headers
 # (parflow_config.h, pfversion.h) are written by this recipe from the values
 # the CMake templates would substitute for a seq/no-hypre build.
@@ -94,9 +99,16 @@ OMP_OBJ := $(addprefix $(OUT)/omp/pl_,$(addsuffix .o,$(CONST))) \
 WRAPS := -Wl,--wrap=KINSolFunctionEval -Wl,--wrap=KINSolMatVec -Wl,--wrap=KinsolPC \
          -Wl,--wrap=RichardsJacobianEval
 
-all: $(OUT)/bin/parflow $(OUT)/bin/parflow_omp $(OUT)/bin/parflow_hook
+GPU_LIBDIR := $(abspath $(HERE)../parflow_b200)
+GPU_WRAPS := $(foreach f,KinsolNonlinSolver KinsolNonlinSolverInitInstanceXtra \
+               KinsolNonlinSolverFreeInstanceXtra KinsolNonlinSolverNewPublicXtra \
+               KinsolNonlinSolverFreePublicXtra KinsolNonlinSolverSizeOfTempData,-Wl,--wrap=$(f))
+
+all: $(OUT)/bin/parflow $(OUT)/bin/parflow_omp $(OUT)/bin/parflow_hook $(OUT)/bin/parflow_gpu
 
 seq: $(OUT)/bin/parflow $(OUT)/bin/parflow_hook
+
+gpu: $(OUT)/bin/parflow_gpu
 
 HDRS := $(OUT)/include/parflow_config.h $(OUT)/include/pfversion.h
 
@@ -150,6 +162,19 @@ $(OUT)/bin/parflow_hook: $(SEQ_OBJ) $(OUT)/seq/main.o $(OUT)/seq/hooks.o
 	@mkdir -p $(dir $@)
 	$(CC) -o $@ $^ $(WRAPS) -lm
 
+# the GPU module against the reference's headers; libpfgpu.so is found next
+# to the package at run time (rpath relative to the binary)
+$(OUT)/seq/kinsol_gpu.o: $(HERE)../parflow_b200/pfmodule/kinsol_gpu_nonlin_solver.c \
+                         $(HERE)../include/pfgpu.h $(HDRS)
+	@mkdir -p $(dir $@)
+	$(CC) $(CFLAGS) -I$(HERE)../include -c $< -o $@
+
+$(OUT)/bin/parflow_gpu: $(SEQ_OBJ) $(OUT)/seq/main.o $(OUT)/seq/kinsol_gpu.o \
+                        $(GPU_LIBDIR)/libpfgpu.so
+	@mkdir -p $(dir $@)
+	$(CC) -o $@ $(SEQ_OBJ) $(OUT)/seq/main.o $(OUT)/seq/kinsol_gpu.o $(GPU_WRAPS) \
+	  -L$(GPU_LIBDIR) -lpfgpu -Wl,-rpath,'$$ORIGIN/../../../parflow_b200' -lstdc++ -lm
+
 # ---- OpenMP -----------------------------------------------------------------
 OMPDEF := -DPARFLOW_HAVE_OMP -fopenmp
 $(OUT)/omp/pl_%.o: $(PL)/%.c $(HDRS)
@@ -181,4 +206,4 @@ $(OUT)/bin/parflow_omp: $(OMP_OBJ) $(OUT)/omp/main.o
 	@mkdir -p $(dir $@)
 	$(OMPCXX) -fopenmp -o $@ $^ -lm
 
-.PHONY: all seq
+.PHONY: all seq gpu

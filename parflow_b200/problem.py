@@ -323,8 +323,10 @@ class RichardsProblem:
 
     # ------------------------------------------------------------------ reference
     def to_reference(self, workdir: str, run: Optional[str] = None,
-                     dump_interval: int = 1) -> str:
-        """Write ``<run>.pfidb`` and its PFB inputs into ``workdir``."""
+                     dump_interval: int = 1, gpu: Optional[str] = None) -> str:
+        """Write ``<run>.pfidb`` and its PFB inputs into ``workdir``.  gpu
+        ("FP64", "Mixed", "Mixed16") selects the GPU nonlinear-solver module
+        of a ParFlow build that links it (Solver.Nonlinear.GPU)."""
         run = run or self.name
         os.makedirs(workdir, exist_ok=True)
         pj = lambda f: os.path.join(workdir, f)
@@ -516,6 +518,9 @@ class RichardsProblem:
         k["Solver.PrintPressure"] = True
         k["Solver.PrintSaturation"] = True
         k["Solver.PrintMask"] = False
+        if gpu:
+            k["Solver.Nonlinear.GPU"] = True
+            k["Solver.Nonlinear.GPU.Precision"] = gpu
         write_pfidb(k, pj(run + ".pfidb"))
         return run
 
