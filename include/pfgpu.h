@@ -255,10 +255,11 @@ int pfgpu_set_evap_trans(pfgpu_handle *h, const double *et);
  * solve or evaluation, so after a solve pfgpu_face_velocities(h, NULL, NULL,
  * NULL, dt, ...) gives the velocities of the last residual evaluation of
  * that step, as the reference's state holds after KINSol returns.  Outputs
- * in ParFlow layout on the face grids (one cell wider along their axis, one
- * ghost layer, ghosts written as 0): vx (nx+3)(ny+2)(nz+2), vy
- * (nx+2)(ny+3)(nz+2), vz (nx+2)(ny+2)(nz+3), qx / qy on the 2-D grid
- * (nx+2)(ny+2)*3; host or device; any may be NULL. */
+ * in the layouts of ParFlow's state vectors on the face grids (one cell
+ * wider along their axis; solver_richards.c:1035-1045, 5110-5160), ghosts
+ * written as 0: vx (nx+3)(ny+2)(nz+2) and vy (nx+2)(ny+3)(nz+2) with one
+ * ghost layer, vz (nx+4)(ny+4)(nz+5) with two, qx / qy on the 2-D grid
+ * (nx+2)(ny+2)*3 with one; host or device; any may be NULL. */
 int pfgpu_face_velocities(pfgpu_handle *h, const double *p, const double *p_old,
                           const double *s_old, double dt, double *vx, double *vy, double *vz,
                           double *qx, double *qy);

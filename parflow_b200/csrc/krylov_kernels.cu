@@ -659,6 +659,26 @@ __global__ void k_pad(const double *__restrict__ dense, double *__restrict__ pad
     pad[c] = in ? dense[i + (long long)nx * (j + (long long)ny * k)] : 0.0;
   }
 }
+// dense -> a frame of g ghost layers on every side (ghosts written as 0)
+__global__ void k_pad_ghost(const double *__restrict__ dense, double *__restrict__ pad, int nx,
+                            int ny, int nz, int g) {
+  pdl_enter();
+  const int px = nx + 2 * g, py = ny + 2 * g;
+  long long n = (long long)px * py * (nz + 2 * g);
+  for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n;
+       c += (long long)gridDim.x * blockDim.x) {
+    int i = (int)(c % px) - g;
+    long long r = c / px;
+    int j = (int)(r % py) - g, k = (int)(r / py) - g;
+    bool in = i >= 0 && j >= 0 && k >= 0 && i < nx && j < ny && k < nz;
+    pad[c] = in ? dense[i + (long long)nx * (j + (long long)ny * k)] : 0.0;
+  }
+}
+void launch_pad_ghost(const double *dense, double *pad, int nx, int ny, int nz, int g,
+                      cudaStream_t st) {
+  const long long n = (long long)(nx + 2 * g) * (ny + 2 * g) * (nz + 2 * g);
+  launch_pdl(k_pad_ghost, dim3(grid_for(n)), dim3(256), st, dense, pad, nx, ny, nz, g);
+}
 void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st) {
   launch_pdl(k_unpad, dim3(grid_for((long long)nx * ny * nz)), dim3(256), st, pad, dense, nx, ny, nz);
 }

@@ -1828,7 +1828,7 @@ int pfgpu_face_velocities(pfgpu_handle *h, const double *p, const double *p_old,
   if (!h->vel) {
     const long long pad_max = std::max({(nx + 3) * (ny + 2) * (nz + 2),
                                         (nx + 2) * (ny + 3) * (nz + 2),
-                                        (nx + 2) * (ny + 2) * (nz + 3)});
+                                        (nx + 4) * (ny + 4) * (nz + 5)});
     if (dalloc(&h->vel, nvx + nvy + nvz + 2 * nq) || dalloc(&h->vstage, pad_max))
       return PFGPU_ERR_NOMEM;
   }
@@ -1848,26 +1848,28 @@ int pfgpu_face_velocities(pfgpu_handle *h, const double *p, const double *p_old,
   launch_residual(h->P, u, h->p_old, h->s_old, h->kr, h->sat, dt, h->bb, h->st, &V);
   h->launches++;
   CK(cudaGetLastError());
-  // ParFlow layouts: the face grids grown by one along their axis, each with
-  // a one-cell ghost frame (x_grid / y_grid / z_grid vectors of
-  // solver_richards.c:5110-5160); q on the 2-D grid, one plane plus ghosts
+  // ParFlow layouts: the face grids grown by one along their axis
+  // (x_grid / y_grid / z_grid, solver_richards.c:5110-5160) with the ghost
+  // widths of the state vectors (one for x and y, two for z,
+  // solver_richards.c:1035-1045); q on the 2-D grid, one plane, one ghost
   struct Out {
     const double *src;
     double *dst;
-    int ax, ay, az;
-  } outs[5] = {{V.vx, vx, (int)nx + 1, (int)ny, (int)nz},
-               {V.vy, vy, (int)nx, (int)ny + 1, (int)nz},
-               {V.vz, vz, (int)nx, (int)ny, (int)nz + 1},
-               {V.qx, qx, (int)nx, (int)ny, 1},
-               {V.qy, qy, (int)nx, (int)ny, 1}};
+    int ax, ay, az, g;
+  } outs[5] = {{V.vx, vx, (int)nx + 1, (int)ny, (int)nz, 1},
+               {V.vy, vy, (int)nx, (int)ny + 1, (int)nz, 1},
+               {V.vz, vz, (int)nx, (int)ny, (int)nz + 1, 2},
+               {V.qx, qx, (int)nx, (int)ny, 1, 1},
+               {V.qy, qy, (int)nx, (int)ny, 1, 1}};
   for (const Out &o : outs) {
     if (!o.dst) continue;
-    const long long np = (long long)(o.ax + 2) * (o.ay + 2) * (o.az + 2);
+    const long long np =
+        (long long)(o.ax + 2 * o.g) * (o.ay + 2 * o.g) * (o.az + 2 * o.g);
     if (is_device_ptr(o.dst)) {
-      launch_pad(o.src, o.dst, o.ax, o.ay, o.az, h->st);
+      launch_pad_ghost(o.src, o.dst, o.ax, o.ay, o.az, o.g, h->st);
       h->launches++;
     } else {
-      launch_pad(o.src, h->vstage, o.ax, o.ay, o.az, h->st);
+      launch_pad_ghost(o.src, h->vstage, o.ax, o.ay, o.az, o.g, h->st);
       h->launches++;
       CK(cudaMemcpyAsync(o.dst, h->vstage, np * sizeof(double), cudaMemcpyDeviceToHost, h->st));
       CK(cudaStreamSynchronize(h->st));

@@ -317,6 +317,9 @@ void launch_axpy_gated(double *y, const double *x, const double *coef, const dou
 // ParFlow layout (ghost frame 1) <-> dense interior
 void launch_unpad(const double *pad, double *dense, int nx, int ny, int nz, cudaStream_t st);
 void launch_pad(const double *dense, double *pad, int nx, int ny, int nz, cudaStream_t st);
+// dense (nx, ny, nz) -> a frame of g ghost layers (ghosts 0)
+void launch_pad_ghost(const double *dense, double *pad, int nx, int ny, int nz, int g,
+                      cudaStream_t st);
 
 // ---- discrete adjoint (adjoint.cu) ------------------------------------------
 template <typename TJ>

@@ -197,7 +197,7 @@ class RichardsGPU:
         nz, ny, nx = self.prob.shape
         vx = np.zeros((nz + 2, ny + 2, nx + 3))
         vy = np.zeros((nz + 2, ny + 3, nx + 2))
-        vz = np.zeros((nz + 3, ny + 2, nx + 2))
+        vz = np.zeros((nz + 5, ny + 4, nx + 4))  # two ghost layers, as ParFlow's z_velocity
         qx = np.zeros((3, ny + 2, nx + 2))
         qy = np.zeros((3, ny + 2, nx + 2))
         bufs = []  # padded inputs, alive through the call
@@ -207,7 +207,8 @@ class RichardsGPU:
                                             float(dt), _ptr(vx), _ptr(vy), _ptr(vz), _ptr(qx),
                                             _ptr(qy))
         L.check(rc, "face_velocities")
-        return (unpad(vx), unpad(vy), unpad(vz), np.ascontiguousarray(qx[1, 1:-1, 1:-1]),
+        return (unpad(vx), unpad(vy), np.ascontiguousarray(vz[2:-2, 2:-2, 2:-2]),
+                np.ascontiguousarray(qx[1, 1:-1, 1:-1]),
                 np.ascontiguousarray(qy[1, 1:-1, 1:-1]))
 
     def nl_function_eval(self, p, p_old, s_old, dt):
