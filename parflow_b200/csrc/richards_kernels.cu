@@ -67,16 +67,24 @@ __global__ void k_saturation(DevProblem P, const double *__restrict__ p, double 
 // faces as flux / area (nl_function_eval.c:845-848), boundary faces as the
 // patch loops store them (vel_vec[vel_idx], :1227-1230, :1432, :1681-1687,
 // :1775-1781), q_overlnd_x / y = ke, kn of the column (:1648-1656)
-template <bool SURF, bool VEL = false>
-__global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double *__restrict__ p,
-                           const double *__restrict__ p_old, const double *__restrict__ s_old,
-                           const double *__restrict__ kr, const double *__restrict__ satv,
-                           double dt, double *__restrict__ f, VelOut V = VelOut{}) {
-  pdl_enter();
-  int i, j, k;
-  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
-  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
-  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+//
+// residual_cell is everything of one cell's F but the interior face fluxes,
+// which the caller supplies: the lower z / y / x faces (fl_z, fl_y, fl_x,
+// used where k, j, i > 0) and the cell's own right / front / upper faces
+// (0 on the domain's upper faces).  Both launch forms below pass the values
+// of the same flux functions with the same operands, so their F is equal
+// bit for bit.
+template <bool SURF, bool VEL>
+__device__ __forceinline__ void residual_cell(const DevProblem &P, int i, int j, int k,
+                                              long long c, const double *__restrict__ p,
+                                              const double *__restrict__ p_old,
+                                              const double *__restrict__ s_old,
+                                              const double *__restrict__ kr,
+                                              const double *__restrict__ satv, double dt,
+                                              double *__restrict__ f, const VelOut &V,
+                                              double fl_z, double fl_y, double fl_x,
+                                              double u_right, double u_front, double u_upper) {
+  const long long sz = (long long)P.nx * P.ny;
   const double rho = P.density, g = P.gravity;
   const double vol = P.dx * P.dy * P.dz;
   const double zm = __ldg(P.zmult + k);
@@ -86,42 +94,12 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
   double fc = (sat * rho - so * rho) * P.porosity * vol * 1.0 * 1.0 * zm;
   fc += P.sstorage * vol * 1.0 * 1.0 * zm * (pc * sat * rho - p_old[c] * so * rho);
   fc -= vol * 1.0 * 1.0 * zm * dt * (0.0 + (P.et ? __ldg(P.et + c) : 0.0));
-
   const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
   const double krc = kr[c];
   // neighbours' scatter (reference loop order: plane k-1, row j-1, cell i-1)
-  if (k > 0) {
-    long long l = c - sz;
-    double zl = __ldg(P.zmult + k - 1);
-    fc += -dt * flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
-  }
-  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
-  if (j > 0) {
-    long long s = c - sy;
-    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
-    fc += -dt * flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm, gs, gc);
-  }
-  if (i > 0) {
-    long long w = c - 1;
-    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
-    fc += -dt * flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm, gs, gc);
-  }
-  double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
-  if (i + 1 < P.nx) {
-    long long e = c + 1;
-    if (SURF) tfg_face_x(P, i, j, gs, gc);
-    u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm, gs, gc);
-  }
-  if (j + 1 < P.ny) {
-    long long nn = c + sy;
-    if (SURF) tfg_face_y(P, i, j, gs, gc);
-    u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm, gs, gc);
-  }
-  if (k + 1 < P.nz) {
-    long long u = c + sz;
-    u_upper = flux_z(P, pc, p[u], kzc, __ldg(P.kz + u), krc, kr[u], zm,
-                     __ldg(P.zmult + k + 1), k);
-  }
+  if (k > 0) fc += -dt * fl_z;
+  if (j > 0) fc += -dt * fl_y;
+  if (i > 0) fc += -dt * fl_x;
   fc += dt * (u_right + u_front + u_upper);
   if (VEL) {
     const long long fx1 = (long long)(P.nx + 1), cyz = (long long)P.nx * (P.ny + 1);
@@ -265,6 +243,135 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
   f[c] = fc;
 }
 
+// Gather form: every cell evaluates all six of its face fluxes (a face shared
+// by two cells is evaluated by both, with the same operands in the same
+// order).  Used by the allocation-free residual and selectable with
+// PFGPU_RESIDUAL_GATHER=1.
+template <bool SURF, bool VEL = false>
+__global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ p_old, const double *__restrict__ s_old,
+                           const double *__restrict__ kr, const double *__restrict__ satv,
+                           double dt, double *__restrict__ f, VelOut V = VelOut{}) {
+  pdl_enter();
+  int i, j, k;
+  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
+  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double g = P.gravity;
+  const double zm = __ldg(P.zmult + k);
+  const double pc = p[c];
+  const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+  const double krc = kr[c];
+  double fl_z = 0.0, fl_y = 0.0, fl_x = 0.0;
+  if (k > 0) {
+    long long l = c - sz;
+    double zl = __ldg(P.zmult + k - 1);
+    fl_z = flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
+  }
+  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
+  if (j > 0) {
+    long long s = c - sy;
+    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
+    fl_y = flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm, gs, gc);
+  }
+  if (i > 0) {
+    long long w = c - 1;
+    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
+    fl_x = flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm, gs, gc);
+  }
+  double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
+  if (i + 1 < P.nx) {
+    long long e = c + 1;
+    if (SURF) tfg_face_x(P, i, j, gs, gc);
+    u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm, gs, gc);
+  }
+  if (j + 1 < P.ny) {
+    long long nn = c + sy;
+    if (SURF) tfg_face_y(P, i, j, gs, gc);
+    u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm, gs, gc);
+  }
+  if (k + 1 < P.nz) {
+    long long u = c + sz;
+    u_upper = flux_z(P, pc, p[u], kzc, __ldg(P.kz + u), krc, kr[u], zm,
+                     __ldg(P.zmult + k + 1), k);
+  }
+  residual_cell<SURF, VEL>(P, i, j, k, c, p, p_old, s_old, kr, satv, dt, f, V, fl_z, fl_y, fl_x,
+                           u_right, u_front, u_upper);
+}
+
+// Face-once form: a block owns a (blockDim.x x blockDim.y) column tile of
+// planes k0 .. k0+kchunk-1 and walks up through them.  Each cell evaluates
+// only its right, front and upper faces; the right / front fluxes go to shared
+// memory for the neighbour in the tile, the upper flux stays in a register as
+// the lower flux of the next plane.  The tile's west / south edge faces and
+// the chunk's first lower faces are evaluated by the cells on those edges.
+// Every flux is the same function of the same operands as in the gather form.
+// Shared memory: blockDim.y x (blockDim.x + 1) right fluxes and
+// (blockDim.y + 1) x blockDim.x front fluxes.
+template <bool SURF, bool VEL = false>
+__global__ void __launch_bounds__(256) k_residual_zm(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ p_old, const double *__restrict__ s_old,
+                           const double *__restrict__ kr, const double *__restrict__ satv,
+                           double dt, double *__restrict__ f, VelOut V, int kchunk) {
+  extern __shared__ double zm_smem[];
+  const int bx = blockDim.x, by = blockDim.y, tx = threadIdx.x, ty = threadIdx.y;
+  double *sE = zm_smem;                    // [by][bx + 1]: sE[ty][tx + 1] = right face of (tx, ty)
+  double *sN = zm_smem + by * (bx + 1);    // [by + 1][bx]: sN[ty + 1][tx] = front face
+  pdl_enter();
+  const int i = blockIdx.x * bx + tx, j = blockIdx.y * by + ty;
+  const int k0 = blockIdx.z * kchunk, k1 = min(P.nz, k0 + kchunk);
+  const bool in = i < P.nx && j < P.ny;
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double g = P.gravity;
+  // gravity terms of this column's faces (constant through the planes)
+  double gsw = 0.5 * (g * 0.0 + g * 0.0), gcw = 0.5 * (g * 1.0 + g * 1.0);
+  double gss = gsw, gcs = gcw, gse = gsw, gce = gcw, gsn = gsw, gcn = gcw;
+  if (SURF && in) {
+    if (i > 0) tfg_face_x(P, i - 1, j, gsw, gcw);
+    if (j > 0) tfg_face_y(P, i, j - 1, gss, gcs);
+    if (i + 1 < P.nx) tfg_face_x(P, i, j, gse, gce);
+    if (j + 1 < P.ny) tfg_face_y(P, i, j, gsn, gcn);
+  }
+  long long c = i + (long long)P.nx * (j + (long long)P.ny * k0);
+  double fl_z = 0.0;
+  if (in && k0 > 0 && k0 < k1)
+    fl_z = flux_z(P, p[c - sz], p[c], __ldg(P.kz + c - sz), __ldg(P.kz + c), kr[c - sz], kr[c],
+                  __ldg(P.zmult + k0 - 1), __ldg(P.zmult + k0), k0 - 1);
+  for (int k = k0; k < k1; k++, c += sz) {
+    double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
+    if (in) {
+      const double zm = __ldg(P.zmult + k);
+      const double pc = p[c];
+      const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+      const double krc = kr[c];
+      if (i + 1 < P.nx)
+        u_right = flux_x(P, pc, p[c + 1], kxc, __ldg(P.kx + c + 1), krc, kr[c + 1], zm, gse, gce);
+      if (j + 1 < P.ny)
+        u_front = flux_y(P, pc, p[c + sy], kyc, __ldg(P.ky + c + sy), krc, kr[c + sy], zm, gsn,
+                         gcn);
+      if (k + 1 < P.nz)
+        u_upper = flux_z(P, pc, p[c + sz], kzc, __ldg(P.kz + c + sz), krc, kr[c + sz], zm,
+                         __ldg(P.zmult + k + 1), k);
+      // the tile's west and south edge faces
+      if (tx == 0 && i > 0)
+        sE[ty * (bx + 1)] = flux_x(P, p[c - 1], pc, __ldg(P.kx + c - 1), kxc, kr[c - 1], krc, zm,
+                                   gsw, gcw);
+      if (ty == 0 && j > 0)
+        sN[tx] = flux_y(P, p[c - sy], pc, __ldg(P.ky + c - sy), kyc, kr[c - sy], krc, zm, gss,
+                        gcs);
+    }
+    sE[ty * (bx + 1) + tx + 1] = u_right;
+    sN[(ty + 1) * bx + tx] = u_front;
+    __syncthreads();
+    if (in)
+      residual_cell<SURF, VEL>(P, i, j, k, c, p, p_old, s_old, kr, satv, dt, f, V, fl_z,
+                               sN[ty * bx + tx], sE[ty * (bx + 1) + tx], u_right, u_front,
+                               u_upper);
+    fl_z = u_upper;
+    __syncthreads();
+  }
+}
+
 // Flux derivatives of one x (or y) face between a (left) and b (right)
 // (richards_jacobian_eval.c:618-660): returns west/east and symmetric parts.
 // TA is the arithmetic of the face terms: double for the FP64 Jacobian; for
@@ -347,17 +454,30 @@ __device__ __forceinline__ FaceDer<TA> face_der_z(const DevProblem &P, double dt
 // 7-point J (C W E S N L U, FP64 or FP32) and the symmetric preconditioner
 // matrix (C E N U: full diagonal, symmetric off-diagonal parts; PCMatrixType
 // PFSymmetric), in the preconditioner's precision.
+//
+// jacobian_cell is everything of one cell's row but the interior face
+// derivatives, which the caller supplies: the lower z / y / x faces' (lo, hi)
+// parts (used where k, j, i > 0) and the cell's own upper faces (zero on the
+// domain's upper faces).  Both launch forms below pass the values of the
+// same face functions with the same operands, so their J and PC matrix are
+// equal bit for bit.
+template <typename TA>
+struct FaceLH {
+  TA lo, hi;
+};
+
 template <typename TJ, typename TP, bool SURF>
-__global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double *__restrict__ p,
-                           const double *__restrict__ kr, const double *__restrict__ dkr,
-                           const double *__restrict__ satv, const double *__restrict__ dsatv,
-                           double dt, JacOut<TJ> J, PCOut<TP> M) {
-  pdl_enter();
-  using TA = TJ;  // arithmetic of the face terms (see face_der_xy)
-  int i, j, k;
-  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
-  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
-  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+__device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j, int k,
+                                              long long c, const double *__restrict__ p,
+                                              const double *__restrict__ kr,
+                                              const double *__restrict__ dkr,
+                                              const double *__restrict__ satv,
+                                              const double *__restrict__ dsatv, double dt,
+                                              const JacOut<TJ> &J, const PCOut<TP> &M,
+                                              FaceLH<TJ> dl_z, FaceLH<TJ> dl_y, FaceLH<TJ> dl_x,
+                                              const FaceDer<TJ> &de, const FaceDer<TJ> &dn,
+                                              const FaceDer<TJ> &du) {
+  const long long sy = P.nx;
   const double rho = P.density, g = P.gravity, drho = 0.0;
   const double vol = P.dx * P.dy * P.dz;
   const double ffx = P.dy * P.dz, ffy = P.dx * P.dz, ffz = P.dx * P.dy;
@@ -366,6 +486,8 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   const double sat = satv[c], dsat = dsatv[c];
   const double prod = kr[c] * rho, prod_der = dkr[c] * rho + kr[c] * drho;
   const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+  (void)g;
+  (void)kzc;
 
   double vol2 = vol * zm;
   double cp = 0.0;
@@ -375,56 +497,32 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   double w = 0.0, s = 0.0, l = 0.0, e = 0.0, nn = 0.0, u = 0.0;
   double es = 0.0, ns = 0.0, us = 0.0;
   if (k > 0) {
-    long long q = c - sz;
-    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
-                           dkr[q] * rho + kr[q] * drho, prod, prod_der, __ldg(P.zmult + k - 1),
-                           zm, k - 1);
-    cp += -d.hi;
-    l = d.lo;
+    cp += -dl_z.hi;
+    l = dl_z.lo;
   }
-  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
   if (j > 0) {
-    long long q = c - sy;
-    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
-    cp += -d.hi;
-    s = d.lo;
+    cp += -dl_y.hi;
+    s = dl_y.lo;
   }
   if (i > 0) {
-    long long q = c - 1;
-    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
-    cp += -d.hi;
-    w = d.lo;
+    cp += -dl_x.hi;
+    w = dl_x.lo;
   }
   double west_t = 0.0, south_t = 0.0, lower_t = 0.0;
   if (i + 1 < P.nx) {
-    long long q = c + 1;
-    if (SURF) tfg_face_x(P, i, j, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
-    west_t = d.lo;
-    e = d.hi;
-    es = d.sym;
+    west_t = de.lo;
+    e = de.hi;
+    es = de.sym;
   }
   if (j + 1 < P.ny) {
-    long long q = c + sy;
-    if (SURF) tfg_face_y(P, i, j, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
-    south_t = d.lo;
-    nn = d.hi;
-    ns = d.sym;
+    south_t = dn.lo;
+    nn = dn.hi;
+    ns = dn.sym;
   }
   if (k + 1 < P.nz) {
-    long long q = c + sz;
-    FaceDer<TA> d = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
-                           dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
-    lower_t = d.lo;
-    u = d.hi;
-    us = d.sym;
+    lower_t = du.lo;
+    u = du.hi;
+    us = du.sym;
   }
   cp += -(west_t + south_t + lower_t);
 
@@ -618,6 +716,158 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   }
 }
 
+// Gather form: every cell evaluates the derivative parts of all six of its
+// faces.  Selectable with PFGPU_RESIDUAL_GATHER=1 (with the residual).
+template <typename TJ, typename TP, bool SURF>
+__global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ kr, const double *__restrict__ dkr,
+                           const double *__restrict__ satv, const double *__restrict__ dsatv,
+                           double dt, JacOut<TJ> J, PCOut<TP> M) {
+  pdl_enter();
+  using TA = TJ;  // arithmetic of the face terms (see face_der_xy)
+  int i, j, k;
+  if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
+  const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double rho = P.density, g = P.gravity, drho = 0.0;
+  const double ffx = P.dy * P.dz, ffy = P.dx * P.dz;
+  const double zm = __ldg(P.zmult + k);
+  const double pc = p[c];
+  const double prod = kr[c] * rho, prod_der = dkr[c] * rho + kr[c] * drho;
+  const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+  FaceLH<TA> dl_z{}, dl_y{}, dl_x{};
+  FaceDer<TA> de{}, dn{}, du{};
+  if (k > 0) {
+    long long q = c - sz;
+    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
+                           dkr[q] * rho + kr[q] * drho, prod, prod_der, __ldg(P.zmult + k - 1),
+                           zm, k - 1);
+    dl_z = {d.lo, d.hi};
+  }
+  double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
+  if (j > 0) {
+    long long q = c - sy;
+    if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
+    dl_y = {d.lo, d.hi};
+  }
+  if (i > 0) {
+    long long q = c - 1;
+    if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
+                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
+    dl_x = {d.lo, d.hi};
+  }
+  if (i + 1 < P.nx) {
+    long long q = c + 1;
+    if (SURF) tfg_face_x(P, i, j, gs, gc);
+    de = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
+  }
+  if (j + 1 < P.ny) {
+    long long q = c + sy;
+    if (SURF) tfg_face_y(P, i, j, gs, gc);
+    dn = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
+  }
+  if (k + 1 < P.nz) {
+    long long q = c + sz;
+    du = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
+                           dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
+  }
+  jacobian_cell<TJ, TP, SURF>(P, i, j, k, c, p, kr, dkr, satv, dsatv, dt, J, M, dl_z, dl_y,
+                              dl_x, de, dn, du);
+}
+
+// Face-once form (as k_residual_zm): each cell evaluates the derivative
+// parts of its right, front and upper faces; the (lo, hi) parts the
+// neighbour needs go through shared memory (x, y) or a register (z).
+// Shared memory: blockDim.y x (blockDim.x + 1) and (blockDim.y + 1) x
+// blockDim.x pairs of TJ.
+template <typename TJ, typename TP, bool SURF>
+__global__ void __launch_bounds__(256, 3) k_jacobian_zm(DevProblem P, const double *__restrict__ p,
+                           const double *__restrict__ kr, const double *__restrict__ dkr,
+                           const double *__restrict__ satv, const double *__restrict__ dsatv,
+                           double dt, JacOut<TJ> J, PCOut<TP> M, int kchunk) {
+  using TA = TJ;
+  extern __shared__ __align__(16) unsigned char jz_smem[];
+  const int bx = blockDim.x, by = blockDim.y, tx = threadIdx.x, ty = threadIdx.y;
+  FaceLH<TA> *sE = reinterpret_cast<FaceLH<TA> *>(jz_smem);  // [by][bx + 1]
+  FaceLH<TA> *sN = sE + by * (bx + 1);                         // [by + 1][bx]
+  pdl_enter();
+  const int i = blockIdx.x * bx + tx, j = blockIdx.y * by + ty;
+  const int k0 = blockIdx.z * kchunk, k1 = min(P.nz, k0 + kchunk);
+  const bool in = i < P.nx && j < P.ny;
+  const long long sy = P.nx, sz = (long long)P.nx * P.ny;
+  const double rho = P.density, g = P.gravity, drho = 0.0;
+  const double ffx = P.dy * P.dz, ffy = P.dx * P.dz;
+  double gsw = 0.5 * (g * 0.0 + g * 0.0), gcw = 0.5 * (g * 1.0 + g * 1.0);
+  double gss = gsw, gcs = gcw, gse = gsw, gce = gcw, gsn = gsw, gcn = gcw;
+  if (SURF && in) {
+    if (i > 0) tfg_face_x(P, i - 1, j, gsw, gcw);
+    if (j > 0) tfg_face_y(P, i, j - 1, gss, gcs);
+    if (i + 1 < P.nx) tfg_face_x(P, i, j, gse, gce);
+    if (j + 1 < P.ny) tfg_face_y(P, i, j, gsn, gcn);
+  }
+  long long c = i + (long long)P.nx * (j + (long long)P.ny * k0);
+  FaceLH<TA> dl_z{};
+  if (in && k0 > 0 && k0 < k1) {
+    const long long q = c - sz;
+    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], p[c], __ldg(P.kz + q), __ldg(P.kz + c),
+                                   kr[q] * rho, dkr[q] * rho + kr[q] * drho, kr[c] * rho,
+                                   dkr[c] * rho + kr[c] * drho, __ldg(P.zmult + k0 - 1),
+                                   __ldg(P.zmult + k0), k0 - 1);
+    dl_z = {d.lo, d.hi};
+  }
+  for (int k = k0; k < k1; k++, c += sz) {
+    FaceDer<TA> de{}, dn{}, du{};
+    if (in) {
+      const double zm = __ldg(P.zmult + k);
+      const double pc = p[c];
+      const double prod = kr[c] * rho, prod_der = dkr[c] * rho + kr[c] * drho;
+      const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
+      if (i + 1 < P.nx) {
+        const long long q = c + 1;
+        de = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod,
+                             prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gse, gce);
+      }
+      if (j + 1 < P.ny) {
+        const long long q = c + sy;
+        dn = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod,
+                             prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gsn, gcn);
+      }
+      if (k + 1 < P.nz) {
+        const long long q = c + sz;
+        du = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
+                            dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
+      }
+      if (tx == 0 && i > 0) {
+        const long long q = c - 1;
+        FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q),
+                                        kxc, kr[q] * rho, dkr[q] * rho + kr[q] * drho, prod,
+                                        prod_der, zm, gsw, gcw);
+        sE[ty * (bx + 1)] = {d.lo, d.hi};
+      }
+      if (ty == 0 && j > 0) {
+        const long long q = c - sy;
+        FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q),
+                                        kyc, kr[q] * rho, dkr[q] * rho + kr[q] * drho, prod,
+                                        prod_der, zm, gss, gcs);
+        sN[tx] = {d.lo, d.hi};
+      }
+    }
+    sE[ty * (bx + 1) + tx + 1] = {de.lo, de.hi};
+    sN[(ty + 1) * bx + tx] = {dn.lo, dn.hi};
+    __syncthreads();
+    if (in)
+      jacobian_cell<TJ, TP, SURF>(P, i, j, k, c, p, kr, dkr, satv, dsatv, dt, J, M, dl_z,
+                                  sN[ty * bx + tx], sE[ty * (bx + 1) + tx], de, dn, du);
+    dl_z = {du.lo, du.hi};
+    __syncthreads();
+  }
+}
+
 // y = J x (matvec.c:35-330 order: y = 0, then C W E S N L U), FP64 accumulate
 template <typename TJ>
 __global__ void k_matvec7(int nx, int ny, int nz, JacIn<TJ> J, const double *__restrict__ x,
@@ -673,27 +923,70 @@ void launch_saturation(const DevProblem &P, const double *p, double *s, cudaStre
   launch_pdl(k_saturation, dim3(blocks_for(P.n, 256)), dim3(256), st, P, p, s);
 }
 
+static bool residual_gather() {
+  static const bool on = [] {
+    const char *v = getenv("PFGPU_RESIDUAL_GATHER");
+    return v && *v == '1';
+  }();
+  return on;
+}
+
+// planes per block of the face-once kernels: enough blocks for about eight
+// per SM while each block walks as many planes as that allows
+static inline int zm_chunk(const dim3 &g2, int nz) {
+  const long long tiles = (long long)g2.x * g2.y;
+  long long chunks = (8LL * 148 + tiles - 1) / tiles;
+  if (chunks < 1) chunks = 1;
+  if (chunks > nz) chunks = nz;
+  return (int)((nz + chunks - 1) / chunks);
+}
+
+// tile of the face-once kernels: a tuned shape when one is set, else 32 x 8
+// (one extra x face per 32 cells and one extra y face per 8)
+static inline void zm_shape(int nx, int ny, const int tile[2], dim3 &grid, dim3 &block) {
+  int bx = 32, by = 8;
+  if (tile && tile[0] > 0 && tile[1] > 0 && tile[0] * tile[1] <= 256) {
+    bx = tile[0];
+    by = tile[1];
+  }
+  block = dim3(bx, by, 1);
+  grid = dim3((nx + bx - 1) / bx, (ny + by - 1) / by, 1);
+}
+
+template <bool SURF, bool VEL>
+static void launch_residual_t(const DevProblem &P, const double *p, const double *p_old,
+                              const double *s_old, const double *kr, const double *sat,
+                              double dt, double *f, cudaStream_t st, const VelOut &vel) {
+  dim3 g, b;
+  if (residual_gather()) {
+    shape_tuned(P.nx, P.ny, P.nz, 256, P.tile[0], g, b);
+    launch_pdl(k_residual<SURF, VEL>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
+               vel);
+    return;
+  }
+  zm_shape(P.nx, P.ny, P.tile[0], g, b);
+  const int kchunk = zm_chunk(g, P.nz);
+  const dim3 gz(g.x, g.y, (P.nz + kchunk - 1) / kchunk);
+  const size_t smem = sizeof(double) * ((size_t)b.y * (b.x + 1) + (size_t)(b.y + 1) * b.x);
+  launch_pdl_smem(k_residual_zm<SURF, VEL>, gz, b, smem, st, P, p, p_old, s_old, kr, sat, dt, f,
+                  vel, kchunk);
+}
+
 void launch_residual(const DevProblem &P, const double *p, const double *p_old,
                      const double *s_old, const double *kr, const double *sat, double dt,
                      double *f, cudaStream_t st, const VelOut *vel) {
-  dim3 g, b;
-  shape_tuned(P.nx, P.ny, P.nz, 256, P.tile[0], g, b);
   const bool surf = P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4;
   if (vel) {
     if (surf)
-      launch_pdl(k_residual<true, true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
-                 *vel);
+      launch_residual_t<true, true>(P, p, p_old, s_old, kr, sat, dt, f, st, *vel);
     else
-      launch_pdl(k_residual<false, true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt,
-                 f, *vel);
+      launch_residual_t<false, true>(P, p, p_old, s_old, kr, sat, dt, f, st, *vel);
     return;
   }
   if (surf)
-    launch_pdl(k_residual<true>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
-               VelOut{});
+    launch_residual_t<true, false>(P, p, p_old, s_old, kr, sat, dt, f, st, VelOut{});
   else
-    launch_pdl(k_residual<false>, dim3(g), dim3(b), st, P, p, p_old, s_old, kr, sat, dt, f,
-               VelOut{});
+    launch_residual_t<false, false>(P, p, p_old, s_old, kr, sat, dt, f, st, VelOut{});
 }
 
 template <typename TJ, typename TP>
@@ -701,12 +994,27 @@ void launch_jacobian(const DevProblem &P, const double *p, const double *kr,
                      const double *dkr, const double *sat, const double *dsat, double dt,
                      JacOut<TJ> J, PCOut<TP> M, cudaStream_t st) {
   dim3 g, b;
-  shape_tuned(P.nx, P.ny, P.nz, 128, P.tile[1], g, b);
-  if (P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4)
-    launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J, M);
+  const bool surf = P.tfg_xs || P.bc_type[5] == 2 || P.bc_type[5] == 3 || P.bc_type[5] == 4;
+  if (residual_gather()) {
+    shape_tuned(P.nx, P.ny, P.nz, 128, P.tile[1], g, b);
+    if (surf)
+      launch_pdl(k_jacobian<TJ, TP, true>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J,
+                 M);
+    else
+      launch_pdl(k_jacobian<TJ, TP, false>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt,
+                 J, M);
+    return;
+  }
+  zm_shape(P.nx, P.ny, P.tile[1], g, b);
+  const int kchunk = zm_chunk(g, P.nz);
+  const dim3 gz(g.x, g.y, (P.nz + kchunk - 1) / kchunk);
+  const size_t smem = sizeof(FaceLH<TJ>) * ((size_t)b.y * (b.x + 1) + (size_t)(b.y + 1) * b.x);
+  if (surf)
+    launch_pdl_smem(k_jacobian_zm<TJ, TP, true>, gz, b, smem, st, P, p, kr, dkr, sat, dsat, dt,
+                    J, M, kchunk);
   else
-    launch_pdl(k_jacobian<TJ, TP, false>, dim3(g), dim3(b), st, P, p, kr, dkr, sat, dsat, dt, J,
-               M);
+    launch_pdl_smem(k_jacobian_zm<TJ, TP, false>, gz, b, smem, st, P, p, kr, dkr, sat, dsat, dt,
+                    J, M, kchunk);
 }
 
 template <typename TJ>
