@@ -922,6 +922,60 @@ struct ClusterTeam {
   }
 };
 
+// GridTeam is every block of a cooperative launch (all blocks resident at
+// once): its barrier is a counter and a generation word in global memory.
+// The last block to arrive resets the counter and advances the generation;
+// the others poll the generation.  Every wait is bounded (GRID_WAIT_NS by
+// the global timer): a block that gives up writes 3 into the error word and
+// later barriers of the launch no longer wait, so the kernel always ends;
+// the host reports the error after the solve (its results are then invalid).
+// A fence on both sides of the barrier orders one phase's global writes
+// before the next phase's plain loads on every SM.
+constexpr unsigned long long GRID_WAIT_NS = 1000000000ull;  // 1 s
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ __forceinline__ GridCtl &grid_ctl() {
+  __shared__ GridCtl ctl;
+  return ctl;
+}
+__device__ __forceinline__ void grid_barrier(const GridCtl &g) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile int *err = g.err;
+    if (*err == 0) {
+      volatile unsigned *gen = g.gen;
+      const unsigned gen0 = *gen;
+      __threadfence();
+      const unsigned arrived = atomicAdd(g.count, 1u) + 1u;
+      if (arrived == gridDim.x) {
+        atomicExch(g.count, 0u);
+        __threadfence();
+        atomicAdd(g.gen, 1u);
+      } else {
+        const unsigned long long t0 = global_ns();
+        while (*gen == gen0) {
+          if (*err != 0) break;
+          if (global_ns() - t0 > GRID_WAIT_NS) {
+            atomicCAS(g.err, 0, 3);
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+  }
+  __syncthreads();
+}
+struct GridTeam {
+  __device__ static int rank() { return blockIdx.x * blockDim.x + threadIdx.x; }
+  __device__ static int size() { return gridDim.x * blockDim.x; }
+  __device__ static void sync() { grid_barrier(grid_ctl()); }
+};
+
 template <typename T, bool H, class Team>
 __device__ __forceinline__ void team_smooth(const MGLevel<T> &L, T *x, const T *b, int zero,
                                             int smoother, T w, T *tmp) {
@@ -1150,6 +1204,36 @@ __global__ void __launch_bounds__(TAIL_THREADS, 1) k_vcycle_mid(
   for (int l = tail - 1; l >= mid; l--) {
     const MGLevel<T> L = Ls[l], C = Ls[l + 1];
     team_up<T, H, ClusterTeam>(L, C, smoother, w, tmp);
+  }
+}
+
+// Levels mid .. tail-1 of a V-cycle on a grid team (cooperative launch):
+// the down leg (pre-smooth, residual, restriction per level) in one launch,
+// the up leg (prolongation and correction, post-smooth per level) in
+// another, the tail levels in between in their own single-block kernel.
+// Same phases and per-cell arithmetic as the per-phase grid kernels, so the
+// V-cycle's result does not depend on where the levels run.  A launch whose
+// barrier gave up (error word set) stops after the phase it was in.
+template <typename T, bool H>
+__global__ void __launch_bounds__(GRID_THREADS) k_vcycle_grid_down(
+    const MGLevel<T> *__restrict__ Ls, int mid, int tail, int smoother, T w, T *tmp, GridCtl ctl) {
+  if (threadIdx.x == 0) grid_ctl() = ctl;
+  __syncthreads();
+  for (int l = mid; l < tail; l++) {
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_down<T, H, GridTeam>(L, C, smoother, w, tmp);
+    if (*(volatile int *)ctl.err) return;
+  }
+}
+template <typename T, bool H>
+__global__ void __launch_bounds__(GRID_THREADS) k_vcycle_grid_up(
+    const MGLevel<T> *__restrict__ Ls, int mid, int tail, int smoother, T w, T *tmp, GridCtl ctl) {
+  if (threadIdx.x == 0) grid_ctl() = ctl;
+  __syncthreads();
+  for (int l = tail - 1; l >= mid; l--) {
+    const MGLevel<T> L = Ls[l], C = Ls[l + 1];
+    team_up<T, H, GridTeam>(L, C, smoother, w, tmp);
+    if (*(volatile int *)ctl.err) return;
   }
 }
 
@@ -1501,6 +1585,86 @@ void launch_vcycle_mid(const MGLevel<T> *levels_dev, int mid, int tail, int nl, 
   launch_pdl_cluster(k_vcycle_mid<T, false>, cs, dim3(TAIL_THREADS), smem, st, levels_dev, mid,
                      tail, nl, smoother, (T)weight, tmp, in_smem);
 }
+// blocks of the cooperative V-cycle kernels: as many as the device keeps
+// resident at once, at most per_sm per SM (cooperative-launch limit)
+template <typename T>
+int vcycle_grid_blocks(bool h16, int per_sm) {
+  int dev = 0, sms = 0, occ = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 0;
+  cudaError_t e;
+  if constexpr (kHasH16<T>) {
+    if (h16)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vcycle_grid_down<T, true>,
+                                                        GRID_THREADS, 0);
+    else
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vcycle_grid_down<T, false>,
+                                                        GRID_THREADS, 0);
+  } else {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_vcycle_grid_down<T, false>,
+                                                      GRID_THREADS, 0);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  int up = 0;
+  if constexpr (kHasH16<T>) {
+    if (h16)
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, k_vcycle_grid_up<T, true>,
+                                                        GRID_THREADS, 0);
+    else
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, k_vcycle_grid_up<T, false>,
+                                                        GRID_THREADS, 0);
+  } else {
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&up, k_vcycle_grid_up<T, false>,
+                                                      GRID_THREADS, 0);
+  }
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  occ = occ < up ? occ : up;
+  if (occ > per_sm) occ = per_sm;
+  return occ * sms;
+}
+
+template <typename K, typename... Args>
+static cudaError_t launch_coop(K kern, int blocks, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(blocks);
+  cfg.blockDim = dim3(GRID_THREADS);
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+template <typename T>
+cudaError_t launch_vcycle_grid(const MGLevel<T> *levels_dev, int mid, int tail, int up,
+                               int smoother, double weight, T *tmp, int blocks, GridCtl ctl,
+                               cudaStream_t st, bool h16) {
+  // a counter left by a launch whose barrier gave up starts from zero again
+  cudaError_t e = cudaMemsetAsync(ctl.count, 0, sizeof(unsigned), st);
+  if (e != cudaSuccess) return e;
+  const T w = (T)weight;
+  if constexpr (kHasH16<T>) {
+    if (h16)
+      return up ? launch_coop(k_vcycle_grid_up<T, true>, blocks, st, levels_dev, mid, tail,
+                              smoother, w, tmp, ctl)
+                : launch_coop(k_vcycle_grid_down<T, true>, blocks, st, levels_dev, mid, tail,
+                              smoother, w, tmp, ctl);
+  }
+  return up ? launch_coop(k_vcycle_grid_up<T, false>, blocks, st, levels_dev, mid, tail,
+                          smoother, w, tmp, ctl)
+            : launch_coop(k_vcycle_grid_down<T, false>, blocks, st, levels_dev, mid, tail,
+                          smoother, w, tmp, ctl);
+}
+
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st) {
   launch_pdl(k_setup_tail<T>, dim3(1), dim3(512), st, levels_dev, first, nl);
@@ -1694,6 +1858,9 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
   template void launch_vcycle_mid<T>(const MGLevel<T> *, int, int, int, int, double, T *,       \
                                      size_t, int, cudaStream_t, bool);                         \
   template int vcycle_mid_cluster_size<T>(bool, size_t);                                       \
+  template int vcycle_grid_blocks<T>(bool, int);                                               \
+  template cudaError_t launch_vcycle_grid<T>(const MGLevel<T> *, int, int, int, int, double, T *, \
+                                             int, GridCtl, cudaStream_t, bool);                \
   template void launch_vcycle_tail<T>(const MGLevel<T> *, int, int, int, double, T *, size_t, \
                                       cudaStream_t, bool);                                    \
   template size_t tail_smem_bytes<T>(const MGLevel<T> *, int, int, bool);                    \

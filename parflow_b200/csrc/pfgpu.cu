@@ -75,6 +75,8 @@ struct MG {
   int tail = 0;                // first level run by the single-block tail kernels
   int mid = 0;                 // first level run by the cluster kernel (== tail: none)
   int mid_cs = 0;              // blocks in that kernel's cluster
+  int grid_blocks = 0;         // levels mid .. tail-1 on cooperative grid kernels instead
+  unsigned *gbar = nullptr;    // their barrier: counter, generation
   size_t tail_smem = 0;        // shared-memory bytes of the V-cycle tail (0: global)
   std::vector<char> waved;     // level smoothed by the wavefront kernel
   std::vector<WaveLevel> wave; // its control words
@@ -102,6 +104,11 @@ struct MG {
 //                     L2 as a grid launch does, so it is slower overall)
 //   PFGPU_MID_CLUSTER most blocks in that cluster (default 16, as many as the
 //                     device can co-schedule)
+//   PFGPU_GRID_CELLS  grid levels at or below this many cells run, per V-cycle
+//                     leg, inside one cooperative kernel over the whole GPU
+//                     (barriers between phases instead of one launch per
+//                     phase); 0 turns it off (see alloc_mg for the default)
+//   PFGPU_GRID_PER_SM resident blocks per SM of those kernels (default 1)
 //   PFGPU_FLIP        0 runs every V-cycle launch in forward block order
 //   PFGPU_SPLIT       0 keeps x and b of the grid levels in the natural
 //                     (interleaved-colour) layout; the TMA-fused and wavefront
@@ -226,8 +233,9 @@ static int check_kernel_error(pfgpu_handle *h) {
     const int code = *h->hkerr;
     *h->hkerr = 0;
     CK(cudaMemsetAsync(h->kerr, 0, sizeof(int), h->st));
-    set_err(code == 2 ? "the wavefront smoother gave up waiting for a neighbouring plane"
-                      : "a pipelined smoother kernel gave up waiting for its TMA copies");
+    set_err(code == 3 ? "a cooperative multigrid kernel gave up waiting at a grid barrier"
+            : code == 2 ? "the wavefront smoother gave up waiting for a neighbouring plane"
+                        : "a pipelined smoother kernel gave up waiting for its TMA copies");
     return PFGPU_ERR_CUDA;
   }
   return 0;
@@ -459,12 +467,22 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
     k += 2;
   }
   // levels first .. nl-1, coarse solve (RedBlackGSPoint, mg_semi.c:1276) included
-  if (mg.mid < mg.tail)
+  if (mg.mid < mg.tail && mg.grid_blocks > 0) {
+    const GridCtl ctl{mg.gbar, mg.gbar + 1, mg.kerr};
+    launch_vcycle_grid<T>(mg.Ldev, mg.mid, mg.tail, 0, smoother, w, mg.wtmp, mg.grid_blocks, ctl,
+                          st, mg.h16);
+    launch_vcycle_tail<T>(mg.Ldev, mg.tail, nl, smoother, w, mg.wtmp, mg.tail_smem, st, mg.h16);
+    launch_vcycle_grid<T>(mg.Ldev, mg.mid, mg.tail, 1, smoother, w, mg.wtmp, mg.grid_blocks, ctl,
+                          st, mg.h16);
+    k += 3;
+  } else if (mg.mid < mg.tail) {
     launch_vcycle_mid<T>(mg.Ldev, mg.mid, mg.tail, nl, smoother, w, mg.wtmp, mg.tail_smem,
                          mg.mid_cs, st, mg.h16);
-  else
+    k++;
+  } else {
     launch_vcycle_tail<T>(mg.Ldev, first, nl, smoother, w, mg.wtmp, mg.tail_smem, st, mg.h16);
-  k++;
+    k++;
+  }
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
     const MGLevel<T> &C = mg.L[l + 1];
@@ -1044,6 +1062,23 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
       }
     }
   }
+  // else the grid levels at or below PFGPU_GRID_CELLS cells just above the
+  // tail, on cooperative kernels over the whole GPU (one launch per V-cycle
+  // leg instead of one per phase: these levels are bound by launch latency)
+  if (mg.mid == mg.tail) {
+    const long long grid_cells = env_ll("PFGPU_GRID_CELLS", 1LL << 20);
+    int l = mg.tail;
+    while (grid_cells > 0 && l > 1 && mg.L[l - 1].n <= grid_cells) l--;
+    if (l < mg.tail) {
+      const int blocks = vcycle_grid_blocks<T>(mg.h16, (int)env_ll("PFGPU_GRID_PER_SM", 1));
+      if (blocks > 0) {
+        CK(cudaMalloc((void **)&mg.gbar, 2 * sizeof(unsigned)));
+        CK(cudaMemset(mg.gbar, 0, 2 * sizeof(unsigned)));
+        mg.mid = l;
+        mg.grid_blocks = blocks;
+      }
+    }
+  }
   // colour-split x / b on the grid levels (red/black smoother); the tail
   // levels keep the natural layout
   const bool split = (h->d.mg_smoother == PFGPU_SMOOTH_RBGS ||
@@ -1106,6 +1141,8 @@ static void free_mg(MG<T> &mg) {
   for (auto &w : mg.wave) wave_free(&w);
   cudaFree(mg.hflag);
   mg.hflag = nullptr;
+  cudaFree(mg.gbar);
+  mg.gbar = nullptr;
   mg.wave.clear();
   mg.L.clear();
 }

@@ -218,6 +218,25 @@ void launch_vcycle_mid(const MGLevel<T> *levels_dev, int mid, int tail, int nl, 
 // largest cluster the device co-schedules for that kernel (0 if none)
 template <typename T>
 int vcycle_mid_cluster_size(bool h16, size_t smem);
+// levels mid .. tail-1 of a V-cycle on every block of a cooperative launch
+// (blocks of GRID_THREADS threads, all resident at once): the down leg
+// (up = 0) or the up leg (up = 1); the tail levels run in between in their
+// own kernel.  ctl: the barrier's counter and generation words (device
+// memory, the counter is cleared by this call) and the error word a barrier
+// that gave up after one second sets to 3.
+constexpr int GRID_THREADS = 512;
+struct GridCtl {
+  unsigned *count, *gen;
+  int *err;
+};
+template <typename T>
+cudaError_t launch_vcycle_grid(const MGLevel<T> *levels_dev, int mid, int tail, int up,
+                               int smoother, double weight, T *tmp, int blocks, GridCtl ctl,
+                               cudaStream_t st, bool h16 = false);
+// blocks of those launches the device keeps resident at once, at most per_sm
+// per SM (0 if the kernels cannot be launched cooperatively)
+template <typename T>
+int vcycle_grid_blocks(bool h16, int per_sm);
 template <typename T>
 void launch_setup_tail(const MGLevel<T> *levels_dev, int first, int nl, cudaStream_t st);
 // a natural-layout FP64 vector r into b of level 0 / x of level 0 back into a

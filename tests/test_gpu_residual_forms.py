@@ -1,9 +1,10 @@
 """The two launch forms of the residual kernel give the same F bit for bit:
-the face-once form (default: each interior face flux evaluated once, shared
-through shared memory within a tile and through a register between planes)
-and the gather form (PFGPU_RESIDUAL_GATHER=1: every cell evaluates all six of
-its faces).  The form is chosen once per process, so the gather side runs in
-a child process."""
+the gather form (the default: every cell evaluates all six of its faces) and
+the face-once form (PFGPU_RESIDUAL_FACE_ONCE=1: each interior face flux
+evaluated once, shared through shared memory within a tile and through a
+register between planes).  The form is chosen once per process, so each side
+runs in a child process.  The Jacobian launches follow the same switch: the
+test compares J x and the preconditioner output M^-1 r too."""
 
 import json
 import os
@@ -37,7 +38,11 @@ for name in json.loads(sys.argv[2]):
     p = p_old + 0.03 * np.random.default_rng(3).standard_normal(p_old.shape)
     f = g.nl_function_eval(p, p_old, g.saturation(p_old), dt)
     v = g.face_velocities(dt, p=p, p_old=p_old, s_old=g.saturation(p_old))
-    out[name] = [f.tobytes().hex()] + [a.tobytes().hex() for a in v]
+    x = np.random.default_rng(4).standard_normal(p.shape)
+    y = g.jacobian_matvec(p, dt, x, p_old=p_old)
+    g.pc_setup(p, dt, p_old=p_old)
+    z = g.pc_apply(x)
+    out[name] = [a.tobytes().hex() for a in (f,) + tuple(v) + (y, z)]
     g.close()
 json.dump(out, open(sys.argv[3], "w"))
 """
@@ -47,9 +52,9 @@ def _run(tmp_path, gather):
     path = str(tmp_path / ("gather.json" if gather else "once.json"))
     env = dict(os.environ)
     if gather:
-        env["PFGPU_RESIDUAL_GATHER"] = "1"
+        env.pop("PFGPU_RESIDUAL_FACE_ONCE", None)
     else:
-        env.pop("PFGPU_RESIDUAL_GATHER", None)
+        env["PFGPU_RESIDUAL_FACE_ONCE"] = "1"
     subprocess.run([sys.executable, "-c", CHILD, ROOT, json.dumps(NAMES), path], env=env,
                    check=True, timeout=600)
     return json.load(open(path))
