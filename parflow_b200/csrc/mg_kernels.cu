@@ -941,31 +941,45 @@ __device__ __forceinline__ GridCtl &grid_ctl() {
   __shared__ GridCtl ctl;
   return ctl;
 }
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned *p, unsigned v) {
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v)
+               : "memory");
+  return old;
+}
 __device__ __forceinline__ void grid_barrier(const GridCtl &g) {
   __syncthreads();
   if (threadIdx.x == 0) {
     volatile int *err = g.err;
     if (*err == 0) {
-      volatile unsigned *gen = g.gen;
-      const unsigned gen0 = *gen;
-      __threadfence();
-      const unsigned arrived = atomicAdd(g.count, 1u) + 1u;
+      const unsigned gen0 = ld_acquire_gpu(g.gen);
+      // arrive (release this block's writes of the phase)
+      const unsigned arrived = atom_add_acq_rel_gpu(g.count, 1u) + 1u;
       if (arrived == gridDim.x) {
         atomicExch(g.count, 0u);
-        __threadfence();
-        atomicAdd(g.gen, 1u);
+        atom_add_acq_rel_gpu(g.gen, 1u);
       } else {
-        const unsigned long long t0 = global_ns();
-        while (*gen == gen0) {
-          if (*err != 0) break;
-          if (global_ns() - t0 > GRID_WAIT_NS) {
-            atomicCAS(g.err, 0, 3);
-            break;
+        // wait (acquire the other blocks' writes); the timer is read only
+        // every 256 polls
+        unsigned long long t0 = 0;
+        for (unsigned it = 0; ld_acquire_gpu(g.gen) == gen0; it++) {
+          if ((it & 255u) == 0) {
+            if (*err != 0) break;
+            const unsigned long long t = global_ns();
+            if (it == 0) {
+              t0 = t;
+            } else if (t - t0 > GRID_WAIT_NS) {
+              atomicCAS(g.err, 0, 3);
+              break;
+            }
           }
-          __nanosleep(32);
         }
       }
-      __threadfence();
     }
   }
   __syncthreads();

@@ -106,8 +106,8 @@ struct MG {
 //                     device can co-schedule)
 //   PFGPU_GRID_CELLS  grid levels at or below this many cells run, per V-cycle
 //                     leg, inside one cooperative kernel over the whole GPU
-//                     (barriers between phases instead of one launch per
-//                     phase); 0 turns it off (see alloc_mg for the default)
+//                     (grid barriers between phases instead of one launch
+//                     per phase; default 0: off, slower on B200)
 //   PFGPU_GRID_PER_SM resident blocks per SM of those kernels (default 1)
 //   PFGPU_FLIP        0 runs every V-cycle launch in forward block order
 //   PFGPU_SPLIT       0 keeps x and b of the grid levels in the natural
@@ -1066,7 +1066,7 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   // tail, on cooperative kernels over the whole GPU (one launch per V-cycle
   // leg instead of one per phase: these levels are bound by launch latency)
   if (mg.mid == mg.tail) {
-    const long long grid_cells = env_ll("PFGPU_GRID_CELLS", 1LL << 20);
+    const long long grid_cells = env_ll("PFGPU_GRID_CELLS", 0);
     int l = mg.tail;
     while (grid_cells > 0 && l > 1 && mg.L[l - 1].n <= grid_cells) l--;
     if (l < mg.tail) {

@@ -1,12 +1,15 @@
-"""The thread-block-cluster kernel for the middle multigrid levels.
+"""The kernels that run the middle multigrid levels as one team.
 
 PFGPU_MID_CELLS hands the grid levels at or below that many cells (above the
 single-block tail) to one cluster kernel, which walks their phases with
-cluster barriers between them and runs the tail in its first block.  Every
-per-cell operation is the one the per-level grid kernels perform, in the same
-order, so the preconditioner output must be bitwise identical to the
-default configuration, with fewer launches, for both smoothers, every
-precision, the shared-memory and global-memory tails and any cluster size.
+cluster barriers between them and runs the tail in its first block;
+PFGPU_GRID_CELLS hands them to two cooperative kernels over the whole GPU
+(down leg, up leg) with grid barriers between the phases, the tail running in
+its own kernel in between.  Every per-cell operation is the one the per-level
+grid kernels perform, in the same order, so the preconditioner output must be
+bitwise identical to the default configuration, with fewer launches, for both
+smoothers, every precision, the shared-memory and global-memory tails and any
+cluster size.
 """
 
 import numpy as np
@@ -17,7 +20,8 @@ from parflow_b200.problem import SolverSettings
 
 pytestmark = pytest.mark.gpu
 
-ENV = ("PFGPU_MID_CELLS", "PFGPU_MID_CLUSTER", "PFGPU_TAIL_SMEM", "PFGPU_TAIL_CELLS")
+ENV = ("PFGPU_MID_CELLS", "PFGPU_MID_CLUSTER", "PFGPU_TAIL_SMEM", "PFGPU_TAIL_CELLS",
+       "PFGPU_GRID_CELLS", "PFGPU_GRID_PER_SM")
 
 
 @pytest.fixture(scope="module")
@@ -68,20 +72,25 @@ def test_mid_levels_bitwise_equal(solver, monkeypatch, name, precision):
                 {"PFGPU_MID_CELLS": "1000000000"},
                 {"PFGPU_MID_CELLS": "1000000000", "PFGPU_TAIL_SMEM": "0"},
                 {"PFGPU_MID_CELLS": "1000000000", "PFGPU_MID_CLUSTER": "2"},
-                {"PFGPU_MID_CELLS": "1000000000", "PFGPU_TAIL_CELLS": "1"}):
+                {"PFGPU_MID_CELLS": "1000000000", "PFGPU_TAIL_CELLS": "1"},
+                {"PFGPU_GRID_CELLS": "20000"},
+                {"PFGPU_GRID_CELLS": "1000000000"},
+                {"PFGPU_GRID_CELLS": "1000000000", "PFGPU_GRID_PER_SM": "2"},
+                {"PFGPU_GRID_CELLS": "1000000000", "PFGPU_TAIL_SMEM": "0"}):
         z, n = _pc(solver, prob, precision, monkeypatch, env)
         assert np.array_equal(z, z_ref), env
-        assert n < n_ref, ("the cluster kernel did not run", env)
+        assert n < n_ref, ("the team kernel did not run", env)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_mid_levels_weighted_jacobi(solver, monkeypatch, precision):
     prob = _problems("WJacobi")["hetero_96"]
     z_ref, n_ref = _pc(solver, prob, precision, monkeypatch, {})
-    z, n = _pc(solver, prob, precision, monkeypatch, {"PFGPU_MID_CELLS": "1000000000"})
     assert np.isfinite(z_ref).all()
-    assert np.array_equal(z, z_ref)
-    assert n < n_ref
+    for env in ({"PFGPU_MID_CELLS": "1000000000"}, {"PFGPU_GRID_CELLS": "1000000000"}):
+        z, n = _pc(solver, prob, precision, monkeypatch, env)
+        assert np.array_equal(z, z_ref), env
+        assert n < n_ref, env
 
 
 def test_mid_levels_newton_solve_identical(solver, monkeypatch):
@@ -89,7 +98,7 @@ def test_mid_levels_newton_solve_identical(solver, monkeypatch):
     counts with and without the cluster kernel."""
     prob = configs.hetero(nx=96, ny=80, nz=20, nsteps=2)
     out = []
-    for env in ({}, {"PFGPU_MID_CELLS": "100000"}):
+    for env in ({}, {"PFGPU_MID_CELLS": "100000"}, {"PFGPU_GRID_CELLS": "100000"}):
         for k in ENV:
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
@@ -99,5 +108,6 @@ def test_mid_levels_newton_solve_identical(solver, monkeypatch):
         st = s.advance(2, prob.dt)
         out.append((s.get_pressure(), [(x.nonlin_iters, x.lin_iters) for x in st]))
         s.close()
-    assert np.array_equal(out[0][0], out[1][0])
-    assert out[0][1] == out[1][1]
+    for o in out[1:]:
+        assert np.array_equal(out[0][0], o[0])
+        assert out[0][1] == o[1]
