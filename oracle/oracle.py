@@ -249,6 +249,80 @@ class Oracle:
                                _ptr(p), C.byref(st))
         return p, st
 
+    def run_time_loop(self, dump_interval: float = 0.0):
+        """AdvanceRichards's time loop (solver_richards.c:2075-2090,
+        2965-3410, 3700-3720): one SelectTimeStep before the loop, then per
+        step SelectTimeStep on the running dt (constant, or growth of it,
+        select_time_step.c:58-155, cut to the next cycle transition), the
+        dump-time snap and the stop-time cut on every attempt, and on a
+        failed solve t and the state put back and dt halved, at most
+        Solver.MaxConvergenceFailures attempts.  Returns (pressure per step,
+        times, dts, stats per step)."""
+        prob = self.prob
+        eps = float(np.finfo(np.float32).eps) * 10.0
+        g = prob.growth
+        stop = prob.stop_time()
+
+        def select(t, dt):
+            if g is None:
+                dt = float(prob.dt)
+            elif dt == 0.0:
+                dt = float(g[0])
+            else:
+                dt = min(max(dt * float(g[1]), float(g[2])), float(g[3]))
+            bc_dt = prob.next_transition(t)
+            if bc_dt > 0.0 and dt > bc_dt:
+                dt = bc_dt
+            return dt
+
+        t = float(prob.start_time)
+        dump_index = 1.0
+        p = prob.initial_pressure().copy()
+        dt = select(t, 0.0)
+        out_p, times, dts, stats = [], [], [], []
+        while t < stop:
+            converged, failures = True, 0
+            p_old = s_old = None
+            while True:
+                if converged:
+                    dt = select(t, dt)
+                    p_old = p.copy()
+                    s_old = self.saturation(p_old)
+                else:
+                    t -= dt
+                    half = 0.5 * dt
+                    if not (t + half) - t > eps:
+                        raise RuntimeError("time increment too small")
+                    dt = half
+                dump_files = False
+                if dump_interval > 0:
+                    print_dt = prob.start_time + dump_index * dump_interval - t
+                    if dt + eps > print_dt:
+                        if abs(dt - print_dt) > eps:
+                            dt = print_dt
+                        dump_files = True
+                if t + dt >= stop:
+                    last = stop - t
+                    if (t + last) - t > eps:
+                        dt = last
+                t += dt
+                self.set_time(t)
+                p_new, st = self.newton_solve(p_old, p_old, s_old, dt)
+                converged = st.status in (1, 2)
+                if converged:
+                    p = p_new
+                    break
+                failures += 1
+                if failures >= prob.solver.max_convergence_failures:
+                    raise RuntimeError(f"time step at t = {t} failed {failures} times")
+            if dump_files:
+                dump_index += 1.0
+            out_p.append(p.copy())
+            times.append(t)
+            dts.append(dt)
+            stats.append(st)
+        return out_p, times, dts, stats
+
     def run(self, nsteps=None, callback=None):
         """Advance the problem ``nsteps`` timesteps (AdvanceRichards semantics
         without dt halving).  Returns (pressures per step, stats per step)."""

@@ -107,7 +107,7 @@ def run(prob, nsteps: int, exe: str = "parflow_omp", threads: Optional[int] = No
     prob.nsteps = nsteps
     wd = workdir or tempfile.mkdtemp(prefix="pfref_")
     try:
-        name = prob.to_reference(wd, "ref", dump_interval=1 if dump else -1)
+        name = prob.to_reference(wd, "ref", dump_interval=1 if dump else 0)
         threads = threads or (os.cpu_count() or 1)
         env = dict(os.environ, OMP_NUM_THREADS=str(threads))
         log = os.path.join(wd, name + ".out.kinsol.log")

@@ -176,15 +176,42 @@ def vel_overland_small() -> RichardsProblem:
     return p
 
 
+def growth_small() -> RichardsProblem:
+    """The time loop with TimeStep.Type Growth (initial 0.04, factor 1.7,
+    min 0.01, max 0.15) on a box whose top flux cycles between rain (2 base
+    units of 0.1) and none (3 units): steps grow, are cut at the cycle's
+    transitions and at the stop time; pressures written every step."""
+    p = configs.box(nx=14, ny=12, nz=9, nsteps=7, dt=0.1, seed=47)
+    p.bc["z_upper"] = BC(BC_FLUX, (-0.05, 0.0), lengths=(2, 3), repeat=-1)
+    p.growth = (0.04, 1.7, 0.01, 0.15)
+    return p
+
+
+def halving_small() -> RichardsProblem:
+    """The dt-halving retry of AdvanceRichards: steps of 1.0 with
+    Solver.Nonlinear.MaxIter 4, too few for the first steps, so KINSol fails
+    and the step is retried at dt / 2 and dt / 4 from the old state
+    (Solver.MaxConvergenceFailures 3); dump times every 1.0 snap the
+    following steps."""
+    return configs.box(nx=12, ny=10, nz=8, nsteps=2, dt=1.0, seed=43,
+                       solver=SolverSettings(max_iter=4))
+
+
+# pressure output of the golden runs (to_reference's dump_interval):
+# every step for the growth case, every 1.0 (one base dt) otherwise
+DUMP = {"growth_small": -1}
+
 GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic",
           "overland_small", "tfg_small", "overland_diff_small",
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
-          "vel_overland_small"]
+          "vel_overland_small", "growth_small", "halving_small"]
+# cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
+TIME_LOOP = ["growth_small", "halving_small"]
 
 
 def get(name: str) -> RichardsProblem:
     return globals()[name]()
 
 
-__all__ = ["get", "GOLDEN"] + GOLDEN
+__all__ = ["get", "GOLDEN", "TIME_LOOP", "DUMP"] + GOLDEN

@@ -212,7 +212,7 @@ struct pfgpu_handle {
     double base_unit = 1.0, start_time = 0.0;
   } cyc[6];
   int ts_type = 0;  // 0 constant, 1 growth (select_time_step.c:42-51)
-  double ts_step = 0.0, ts_factor = 1.0, ts_min = 0.0, ts_max = 0.0, ts_dt = 0.0;
+  double ts_step = 0.0, ts_factor = 1.0, ts_min = 0.0, ts_max = 0.0;
   int max_failures = 3;
   bool ptime = false;
   std::vector<cudaEvent_t> pev;                  // event pool
@@ -1713,7 +1713,6 @@ int pfgpu_set_time_step(pfgpu_handle *h, int type, double step, double factor,
   h->ts_factor = factor;
   h->ts_min = min_step;
   h->ts_max = max_step;
-  h->ts_dt = 0.0;
   h->max_failures = max_failures;
   return PFGPU_OK;
 }
@@ -1729,16 +1728,17 @@ static void bc_cycles_at(pfgpu_handle *h, double t) {
   }
 }
 
-// SelectTimeStep (select_time_step.c:58-155): the step rule, then the next
-// boundary-cycle transition
-static double select_time_step(pfgpu_handle *h, double t) {
-  double dt;
+// SelectTimeStep (select_time_step.c:58-155) on the running dt: constant
+// steps, or growth of the previous dt (dt == 0, only before the loop: the
+// initial step) clamped to [min, max]; then cut to the next boundary-cycle
+// transition
+static double select_time_step(pfgpu_handle *h, double t, double dt) {
   if (h->ts_type == 0) {
     dt = h->ts_step;
-  } else if (h->ts_dt == 0.0) {
+  } else if (dt == 0.0) {
     dt = h->ts_step;
   } else {
-    dt = h->ts_dt * h->ts_factor;
+    dt = dt * h->ts_factor;
     if (dt < h->ts_min) dt = h->ts_min;
     if (dt > h->ts_max) dt = h->ts_max;
   }
@@ -1747,8 +1747,14 @@ static double select_time_step(pfgpu_handle *h, double t) {
   return dt;
 }
 
-// AdvanceRichards's time loop on the device state (solver_richards.c:2965-3406
-// and the dump/stop adjustments of :3139-3230)
+// AdvanceRichards's time loop on the device state, with its control flow
+// (solver_richards.c:2075-2090 before the loop, 2965-3410 per step, 3700-3720
+// after a step): one time-step selection before the loop (the initial step),
+// then per step a selection on the running dt (so growth first multiplies
+// the initial step, and multiplies the dt that cuts, halvings and dump
+// snapping left), the dump-time snap and the stop-time cut on every attempt,
+// the solve, and on failure t and the state put back and dt halved; the dump
+// index advances once per converged step that dumped.
 int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval, int max_steps,
               double *times, double *dts, pfgpu_stats *stats, int *nsteps) {
   if (!h || !(stop_time > t) || max_steps < 1 || !nsteps || !(h->ts_step > 0)) {
@@ -1760,23 +1766,15 @@ int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval,
   double dump_index = 1.0;
   int n = 0;
   *nsteps = 0;
+  double dt = select_time_step(h, t, 0.0);
   while (t < stop_time && n < max_steps) {
-    bool converged = true;
+    bool converged = true, dump_files = false;
     int failures = 0;
-    double dt = 0.0;
     pfgpu_stats st{};
     int rc = PFGPU_NOT_CONVERGED;
     do {
       if (converged) {
-        dt = select_time_step(h, t);
-        if (dump_interval > 0) {
-          const double print_dt = start + dump_index * dump_interval - t;
-          if ((dt + kTimeEpsilon) > print_dt) {
-            if (fabs(dt - print_dt) > kTimeEpsilon) dt = print_dt;
-            dump_index += 1.0;
-          }
-        }
-        if (t + dt >= stop_time) dt = stop_time - t;
+        dt = select_time_step(h, t, dt);
         CK(cudaMemcpyAsync(h->p_old, h->u, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
                            h->st));
         launch_saturation(h->P, h->u, h->s_old, h->st);
@@ -1794,6 +1792,18 @@ int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval,
                            h->st));
         h->vg_for = nullptr;
       }
+      dump_files = false;
+      if (dump_interval > 0) {
+        const double print_dt = start + dump_index * dump_interval - t;
+        if ((dt + kTimeEpsilon) > print_dt) {
+          if (fabs(dt - print_dt) > kTimeEpsilon) dt = print_dt;
+          dump_files = true;
+        }
+      }
+      if (t + dt >= stop_time) {
+        const double last = stop_time - t;
+        if ((t + last) - t > kTimeEpsilon) dt = last;
+      }
       t += dt;
       bc_cycles_at(h, t);
       rc = newton(h, dt, &st);
@@ -1807,7 +1817,7 @@ int pfgpu_run(pfgpu_handle *h, double t, double stop_time, double dump_interval,
       *nsteps = n;
       return PFGPU_NOT_CONVERGED;
     }
-    h->ts_dt = dt;
+    if (dump_files) dump_index += 1.0;
     if (times) times[n] = t;
     if (dts) dts[n] = dt;
     if (stats) stats[n] = st;

@@ -172,6 +172,9 @@ class RichardsProblem:
     evap_trans: object = None
     # reference output of the face velocities (Solver.PrintVelocities)
     print_velocities: bool = False
+    # TimeStep.Type Growth: (initial step, growth factor, min step, max
+    # step); None = constant dt.  The time-cycle base unit stays dt.
+    growth: Optional[tuple] = None
     solver: SolverSettings = field(default_factory=SolverSettings)
     name: str = "richards"
 
@@ -290,6 +293,41 @@ class RichardsProblem:
     def stop_time(self) -> float:
         return float(self.start_time + self.nsteps * self.dt)
 
+    def next_transition(self, t: float) -> float:
+        """Time from t to the next interval transition of any face's cycle,
+        or -1 (TimeCycleDataComputeNextTransition, time_cycle_data.c:206-297,
+        over the BCPressure cycles)."""
+        base = self.base_unit if self.base_unit is not None else self.dt
+        sub = 1000
+        time_eps = float(np.finfo(np.float32).eps) * 10.0
+        best = None
+        for face in FACES:
+            bc = self.bc.get(face, BC(BC_FLUX, (0.0,)))
+            lengths = [int(v) for v in bc.lengths]
+            if len(lengths) <= 1:
+                continue
+            clen = sum(lengths)
+            stop_defined = bc.repeat * clen * base if bc.repeat > 0 else 1e300
+            if not t < stop_defined:
+                continue
+            dtime = pfround(t / (base / sub)) // sub
+            dstart = pfround(self.start_time / (base / sub)) // sub
+            n = int((dtime - dstart) / clen)
+            done = int(np.fmod(dtime - dstart - 1, clen))
+            q, total = 0, lengths[0]
+            while done >= total and q + 1 < len(lengths):
+                q += 1
+                total += lengths[q]
+            if (q + 1) % len(lengths) == 0:
+                tt = self.start_time + float((n + 1) * clen) * base
+            else:
+                tt = self.start_time + float(n * clen + total) * base
+            if tt < stop_defined:
+                best = tt - t if best is None else min(best, tt - t)
+        if best is None or not (t + best) - t > time_eps:
+            return -1.0
+        return best
+
     def time_plan(self, dump_interval: int = 1):
         """[(t_new, dt)] per timestep, as AdvanceRichards chooses them
         (pfsimulator/parflow_lib/solver_richards.c:3139-3230): constant dt,
@@ -324,9 +362,14 @@ class RichardsProblem:
     # ------------------------------------------------------------------ reference
     def to_reference(self, workdir: str, run: Optional[str] = None,
                      dump_interval: int = 1, gpu: Optional[str] = None) -> str:
-        """Write ``<run>.pfidb`` and its PFB inputs into ``workdir``.  gpu
-        ("FP64", "Mixed", "Mixed16") selects the GPU nonlinear-solver module
-        of a ParFlow build that links it (Solver.Nonlinear.GPU)."""
+        """Write ``<run>.pfidb`` and its PFB inputs into ``workdir``.
+        dump_interval: > 0 writes pressure and saturation every
+        dump_interval * dt of simulated time (TimingInfo.DumpInterval, with
+        the dt snapping to dump times that goes with it), < 0 every
+        |dump_interval| steps (ParFlow's negative convention,
+        solver_richards.c:3165-3170), 0 never.  gpu ("FP64", "Mixed",
+        "Mixed16") selects the GPU nonlinear-solver module of a ParFlow build
+        that links it (Solver.Nonlinear.GPU)."""
         run = run or self.name
         os.makedirs(workdir, exist_ok=True)
         pj = lambda f: os.path.join(workdir, f)
@@ -383,9 +426,21 @@ class RichardsProblem:
         k["TimingInfo.StartCount"] = 0
         k["TimingInfo.StartTime"] = float(self.start_time)
         k["TimingInfo.StopTime"] = self.stop_time()
-        k["TimingInfo.DumpInterval"] = -1 if dump_interval < 0 else float(dump_interval * self.dt)
-        k["TimeStep.Type"] = "Constant"
-        k["TimeStep.Value"] = float(self.dt)
+        if dump_interval > 0:
+            k["TimingInfo.DumpInterval"] = float(dump_interval * self.dt)
+        else:
+            k["TimingInfo.DumpInterval"] = int(dump_interval) if dump_interval < 0 else -1
+        if self.growth is None:
+            k["TimeStep.Type"] = "Constant"
+            k["TimeStep.Value"] = float(self.dt)
+        else:
+            # SelectTimeStep growth (select_time_step.c:206-240)
+            init, factor, lo, hi = (float(v) for v in self.growth)
+            k["TimeStep.Type"] = "Growth"
+            k["TimeStep.InitialStep"] = init
+            k["TimeStep.GrowthFactor"] = factor
+            k["TimeStep.MinStep"] = lo
+            k["TimeStep.MaxStep"] = hi
         k["Geom.Porosity.GeomNames"] = "domain"
         k["Geom.domain.Porosity.Type"] = "Constant"
         k["Geom.domain.Porosity.Value"] = float(self.porosity)
@@ -515,8 +570,8 @@ class RichardsProblem:
                 k["Solver.PrintQxOverland"] = True
                 k["Solver.PrintQyOverland"] = True
         k["Solver.PrintSubsurfData"] = False
-        k["Solver.PrintPressure"] = True
-        k["Solver.PrintSaturation"] = True
+        k["Solver.PrintPressure"] = dump_interval != 0
+        k["Solver.PrintSaturation"] = dump_interval != 0
         k["Solver.PrintMask"] = False
         if gpu:
             k["Solver.Nonlinear.GPU"] = True

@@ -46,18 +46,29 @@ def kinsol_counts(log: str):
     return np.array(rows, dtype=np.int64)
 
 
+def attempt_times(log: str):
+    """Target time of every nonlinear solve in a kinsol.log, in order (a
+    solve that failed is followed by a retry at an earlier time)."""
+    return np.array([float(x) for x in re.findall(r"KINSOL starting step for time ([-+0-9.eE]+)",
+                                                  log)])
+
+
 def make(case_name: str, max_dumps: int = 6):
     prob = cases.get(case_name)
     with tempfile.TemporaryDirectory() as wd:
-        run = prob.to_reference(wd, "golden")
+        run = prob.to_reference(wd, "golden", dump_interval=cases.DUMP.get(case_name, 1))
         dump = os.path.join(wd, "dump")
         os.makedirs(dump)
         env = dict(os.environ, PFREF_DUMP_DIR=dump, PFREF_DUMP_MAX=str(max_dumps))
         subprocess.run([HOOK, run], cwd=wd, env=env, check=True,
                        stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        nfiles = 0
+        while os.path.exists(os.path.join(wd, f"{run}.out.press.{nfiles:05d}.pfb")):
+            nfiles += 1
         press = np.stack([read_pfb(os.path.join(wd, f"{run}.out.press.{t:05d}.pfb"))
-                          for t in range(prob.nsteps + 1)])
-        counts = kinsol_counts(open(os.path.join(wd, f"{run}.out.kinsol.log")).read())
+                          for t in range(nfiles)])
+        log = open(os.path.join(wd, f"{run}.out.kinsol.log")).read()
+        counts = kinsol_counts(log)
         inner = lambda a: np.ascontiguousarray(a[1:-1, 1:-1, 1:-1])
 
         def stack(arrs):
@@ -68,12 +79,12 @@ def make(case_name: str, max_dumps: int = 6):
         for key, tag in (("velx", "velx"), ("vely", "vely"), ("velz", "velz"),
                          ("qx_overland", "qx_overland"), ("qy_overland", "qy_overland")):
             files = [os.path.join(wd, f"{run}.out.{tag}.{t:05d}.pfb")
-                     for t in range(1, prob.nsteps + 1)]
+                     for t in range(1, nfiles)]
             if all(os.path.exists(f) for f in files):
                 extra[key] = np.stack([read_pfb(f) for f in files])
         if prob.evap_trans is not None:
             extra["evap_trans"] = prob.field3d(prob.evap_trans)
-        out = {"press": press, "counts": counts, **extra,
+        out = {"press": press, "counts": counts, "attempt_times": attempt_times(log), **extra,
                "perm": prob.field3d(prob.perm), "alpha": prob.field3d(prob.vg_alpha),
                "n": prob.field3d(prob.vg_n)}
         fe = [read_dump(f) for f in list_dumps(dump, "fe")]

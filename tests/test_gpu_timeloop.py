@@ -1,19 +1,21 @@
-"""The native time loop (pfgpu_run) against the per-step host loop.
+"""The native time loop (pfgpu_run) against the reference and the host loop.
 
 pfgpu_run keeps every boundary time cycle on the device (pfgpu_set_bc_cycle),
-selects dt as SelectTimeStep does (constant, or growth clamped to [min, max],
-cut to the next cycle transition), snaps dt to dump times and cuts it to the
-stop time, as AdvanceRichards does.  On the reference's fixtures it must take
-the steps of the host loop (RichardsGPU.run, which follows time_plan) and end
-on the same pressure bitwise; with growth steps it must follow a host
-restatement of the same rules.
+selects dt as SelectTimeStep does (constant, or growth of the running dt
+clamped to [min, max], cut to the next cycle transition), snaps dt to dump
+times, cuts it to the stop time and halves it on a failed solve, as
+AdvanceRichards does.  On the reference's time-loop fixtures (growth with
+cycle transitions; a forced dt-halving retry with dump snapping) it must take
+the reference's steps with its counts and end on its pressures; on the other
+fixtures it must take the steps of the host loop (RichardsGPU.run, which
+follows time_plan) and end on the same pressure bitwise.
 """
 
 import numpy as np
 import pytest
 
 from parflow_b200 import cases, configs
-from parflow_b200.problem import BC, BC_FLUX, pfround
+from parflow_b200.problem import BC, BC_FLUX
 
 pytestmark = pytest.mark.gpu
 
@@ -29,7 +31,23 @@ def solver():
     return s
 
 
-@pytest.mark.parametrize("name", cases.GOLDEN)
+@pytest.mark.parametrize("name", cases.TIME_LOOP)
+def test_run_device_vs_reference_time_loop(solver, golden, name):
+    g = golden(name)
+    prob = cases.get(name)
+    dump = prob.dt * cases.DUMP.get(name, 1) if cases.DUMP.get(name, 1) > 0 else 0.0
+    s = solver.RichardsGPU(prob)
+    p, times, dts, st = s.run_device(dump_interval=dump, growth=prob.growth)
+    s.close()
+    at = g["attempt_times"]
+    ok = [i for i in range(len(at)) if i == len(at) - 1 or at[i + 1] > at[i]]
+    assert np.allclose(times, at[ok], rtol=0, atol=5e-7), (times, at[ok])
+    assert [(x.nonlin_iters, x.lin_iters) for x in st] == [tuple(r) for r in g["counts"][ok, :2]]
+    ref = g["press"][-1]
+    assert np.abs(p - ref).max() / np.abs(ref).max() <= 1e-9
+
+
+@pytest.mark.parametrize("name", [c for c in cases.GOLDEN if c not in cases.TIME_LOOP])
 def test_run_device_equals_host_loop(solver, name):
     prob = cases.get(name)
     s = solver.RichardsGPU(prob)
@@ -44,45 +62,27 @@ def test_run_device_equals_host_loop(solver, name):
     assert np.array_equal(p, ps[-1])
 
 
-def _next_transition(bc, t, base, start):
-    """TimeCycleDataComputeNextTransition (time_cycle_data.c:206-297) for one
-    face cycle repeating for ever."""
-    lengths = list(bc.lengths)
-    if len(lengths) <= 1:
-        return -1.0
-    clen = sum(lengths)
-    sub = 1000
-    dtime = pfround(t / (base / sub)) // sub
-    dstart = pfround(start / (base / sub)) // sub
-    n = (dtime - dstart) // clen
-    done = int(np.fmod(dtime - dstart - 1, clen))
-    q, total = 0, lengths[0]
-    while done >= total:
-        q += 1
-        total += lengths[q]
-    if (q + 1) % len(lengths) == 0:
-        tt = start + (n + 1) * clen * base
-    else:
-        tt = start + (n * clen + total) * base
-    return tt - t
-
-
 def test_growth_steps_and_cycle_transitions(solver):
+    """Growth steps cut at cycle transitions on a larger box: pfgpu_run
+    against the host stepping the same steps one by one (the step rule is
+    pinned to the reference by the time-loop fixtures above)."""
     prob = configs.box(nx=24, ny=20, nz=10, nsteps=6, dt=0.1, seed=7)
     prob.bc["z_upper"] = BC(BC_FLUX, (-0.05, 0.0), lengths=(2, 3), repeat=-1)
-    growth = (0.04, 1.7, 0.01, 0.15)
+    prob.growth = (0.04, 1.7, 0.01, 0.15)
     s = solver.RichardsGPU(prob)
-    p_dev, times, dts, _ = s.run_device(dump_interval=0.0, growth=growth)
+    p_dev, times, dts, _ = s.run_device(dump_interval=0.0, growth=prob.growth)
     s.close()
-    # host restatement: SelectTimeStep growth, transition cut, stop cut
-    init, factor, lo, hi = growth
-    base, start, stop = prob.dt, prob.start_time, prob.stop_time()
+    # host restatement of SelectTimeStep growth on the running dt
+    # (select_time_step.c:97-115; the initial step before the loop), the
+    # transition cut and the stop cut
+    init, factor, lo, hi = prob.growth
+    stop = prob.stop_time()
     s = solver.RichardsGPU(prob)
     s.set_pressure(prob.initial_pressure())
-    t, last, want_t, want_dt = start, 0.0, [], []
+    t, dt, want_t, want_dt = prob.start_time, init, [], []
     while t < stop:
-        dt = init if last == 0.0 else min(max(last * factor, lo), hi)
-        bc_dt = _next_transition(prob.bc["z_upper"], t, base, start)
+        dt = min(max(dt * factor, lo), hi)
+        bc_dt = prob.next_transition(t)
         if bc_dt > 0 and dt > bc_dt:
             dt = bc_dt
         if t + dt >= stop:
@@ -90,7 +90,6 @@ def test_growth_steps_and_cycle_transitions(solver):
         t += dt
         s.set_time(t)
         s.advance(1, dt)
-        last = dt
         want_t.append(t)
         want_dt.append(dt)
     p_host = s.get_pressure()

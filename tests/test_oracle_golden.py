@@ -53,7 +53,32 @@ def test_jacobian_and_pc_bitexact(name, golden):
         assert np.array_equal(z, g["pc_out"][i]), (name, i)
 
 
-@pytest.mark.parametrize("name", CASES)
+def successful_attempts(times):
+    """Indices of the solves that succeeded in a kinsol.log's sequence of
+    target times: a failed solve is retried at an earlier time."""
+    return [i for i in range(len(times)) if i == len(times) - 1 or times[i + 1] > times[i]]
+
+
+@pytest.mark.parametrize("name", cases.TIME_LOOP)
+def test_time_loop_bitexact(name, golden):
+    """AdvanceRichards's step selection (growth from the running dt, cuts
+    at cycle transitions, dump snapping, stop cut) and dt-halving retry:
+    the oracle's loop takes the reference's steps, with its counts and
+    pressures bit for bit."""
+    g = golden(name)
+    prob = cases.get(name)
+    dump = prob.dt * cases.DUMP.get(name, 1) if cases.DUMP.get(name, 1) > 0 else 0.0
+    ps, times, dts, sts = Oracle(prob).run_time_loop(dump_interval=dump)
+    ok = successful_attempts(g["attempt_times"])
+    assert np.allclose(times, g["attempt_times"][ok], rtol=0, atol=5e-7)
+    assert [(s.nni, s.nli) for s in sts] == [tuple(r) for r in g["counts"][ok, :2]]
+    if cases.DUMP.get(name, 1) < 0:  # every step written
+        for n, p in enumerate(ps):
+            assert np.array_equal(p, g["press"][n + 1]), (name, n)
+    assert np.array_equal(ps[-1], g["press"][-1])
+
+
+@pytest.mark.parametrize("name", [c for c in CASES if c not in cases.TIME_LOOP])
 def test_timesteps_bitexact(name, golden):
     g = golden(name)
     prob = cases.get(name)
