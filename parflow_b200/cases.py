@@ -197,6 +197,15 @@ def halving_small() -> RichardsProblem:
                        solver=SolverSettings(max_iter=4))
 
 
+def restart_small() -> RichardsProblem:
+    """Restarted GMRES: Solver.Linear.KrylovDimension 2 with
+    Solver.Linear.MaxRestarts 5 and a two-level multigrid on config-2 physics
+    with steps of 5 h, so that most linear solves need several cycles
+    (spgmr.c:390-409)."""
+    return configs.hetero(nx=15, ny=13, nz=9, nsteps=2, dt=5.0, seed=53,
+                          solver=SolverSettings(krylov_dim=2, max_restarts=5, mg_max_levels=2))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -205,7 +214,7 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "overland_small", "tfg_small", "overland_diff_small",
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
-          "vel_overland_small", "growth_small", "halving_small"]
+          "vel_overland_small", "growth_small", "halving_small", "restart_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

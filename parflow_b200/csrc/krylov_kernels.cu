@@ -428,14 +428,30 @@ struct VecList {
   const double *v[32];
 };
 // xcor = yg[0] V0 + 0, then xcor = yg[k] Vk + xcor (sequential N_VLinearSum order)
+// xcor = sum_k yg[k] V_k, accumulated in k order onto 0 (accumulate = 0) or
+// onto xcor itself (accumulate = 1: a GMRES restart cycle adds to the
+// correction of the earlier cycles, spgmr.c:357-358)
 __global__ void k_combine(double *__restrict__ xcor, VecList V, const double *__restrict__ yg,
-                          int kdim, long long n) {
+                          int kdim, long long n, int accumulate) {
   pdl_enter();
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
        i += (long long)gridDim.x * blockDim.x) {
-    double acc = 0.0;
+    double acc = accumulate ? xcor[i] : 0.0;
     for (int k = 0; k < kdim; k++) acc = yg[k] * V.v[k][i] + 1.0 * acc;
     xcor[i] = acc;
+  }
+}
+
+// restart direction V_0 = yg[0] V_0 + sum_{k=1..kdim} yg[k] V_k, in place
+// (spgmr.c:405-409): every element reads only its own index
+__global__ void k_restart_v0(double *v0, VecList V, const double *__restrict__ yg, int kdim,
+                             long long n) {
+  pdl_enter();
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = yg[0] * v0[i];
+    for (int k = 1; k <= kdim; k++) acc = yg[k] * V.v[k][i] + 1.0 * acc;
+    v0[i] = acc;
   }
 }
 
@@ -465,10 +481,16 @@ void launch_fill(double *x, double v, long long n, cudaStream_t st) {
   launch_pdl(k_fill, dim3(grid_for(n)), dim3(256), st, x, v, n);
 }
 void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
-                    cudaStream_t st) {
+                    cudaStream_t st, int accumulate) {
   VecList L;
   for (int k = 0; k < kdim && k < 32; k++) L.v[k] = V[k];
-  launch_pdl(k_combine, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, n);
+  launch_pdl(k_combine, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, n, accumulate);
+}
+void launch_restart_v0(double *const *V, const double *yg, int kdim, long long n,
+                       cudaStream_t st) {
+  VecList L;
+  for (int k = 0; k <= kdim && k < 32; k++) L.v[k] = V[k];
+  launch_pdl(k_restart_v0, dim3(grid_for(n)), dim3(256), st, V[0], L, yg, kdim, n);
 }
 
 // ---- GMRES scalars ----------------------------------------------------------
@@ -577,6 +599,25 @@ __global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
         g.yg[k] /= g.h(k, k);
         for (int i = 0; i < k; i++) g.yg[i] -= g.yg[k] * g.h(i, k);
       }
+      break;
+    }
+    case 6: {  // restart (spgmr.c:390-404), krydim = l: the residual direction's
+               // coefficients yg and the new r_norm
+      int kd = l;
+      double s_product = 1.0;
+      for (int i = kd; i > 0; i--) {
+        g.yg[i] = s_product * g.giv[2 * i - 2];
+        s_product *= g.giv[2 * i - 1];
+      }
+      g.yg[0] = s_product;
+      double r_norm = sc[SC_RNORM] * s_product;
+      for (int i = 0; i <= kd; i++) g.yg[i] *= r_norm;
+      sc[SC_RNORM] = fabs(r_norm);
+      break;
+    }
+    case 7: {  // next restart cycle: Hessenberg cleared, rotation product 1
+      sc[SC_ROT] = 1.0;
+      for (int i = 0; i < (lmax + 1) * lmax; i++) g.H[i] = 0.0;
       break;
     }
     case 5: {  // finish reorthogonalisation: corrected new norm (iterativ.c:79-84)

@@ -635,12 +635,13 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
   }
 
   for (int ntries = 0; ntries <= h->d.max_restarts; ntries++) {
-    if (ntries > 0) {
-      launch_gmres_scalar(GM_START, S, 0, lmax, h->st);  // re-zero H, keep r_norm squared?
-      h->launches++;
+    if (ntries == 0) {
+      // V0 = b / r_norm = src * (bsign / r_norm)
+      launch_axpby(h->V[0], src, bsign * (1.0 / r_norm), 0.0, N, h->st);
+    } else {
+      // the restart direction (built below) scaled by 1 / r_norm
+      launch_scale_inv_dev(h->V[0], sc + SCI_RNORM, N, h->st);
     }
-    // V0 = b / r_norm = src * (bsign / r_norm)
-    launch_axpby(h->V[0], src, bsign * (1.0 / r_norm), 0.0, N, h->st);
     h->launches++;
     int l;
     for (l = 0; l < lmax; l++) {
@@ -684,9 +685,10 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
       launch_scale_inv_dev(h->V[l + 1], Hp(l + 1, l), N, h->st);
       h->launches++;
     }
-    // QRsol and xcor = V y
+    // QRsol and xcor (+)= V y
     launch_gmres_scalar(GM_QRSOL, S, krydim, lmax, h->st);
-    launch_combine(h->xcor, h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st);
+    launch_combine(h->xcor, h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st,
+                   ntries > 0 ? 1 : 0);
     h->launches += 2;
     CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_QRFAIL, sizeof(double),
                        cudaMemcpyDeviceToHost, h->st));
@@ -704,9 +706,12 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
       return 0;
     }
     if (ntries == h->d.max_restarts) break;
-    // restart: not used by the configurations here (MaxRestarts 0)
-    set_err("GMRES restarts are not supported by this build");
-    return PFGPU_ERR_ARG;
+    // restart (spgmr.c:390-409): the new residual direction from the
+    // Givens rotations and the current basis, then a fresh cycle
+    launch_gmres_scalar(GM_RESTART, S, krydim, lmax, h->st);
+    launch_restart_v0(h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st);
+    launch_gmres_scalar(GM_RESTART_INIT, S, 0, lmax, h->st);
+    h->launches += 3;
   }
   if (rho < beta) {
     if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;
@@ -1309,8 +1314,8 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
     set_err("pfgpu_create: krylov_dim must be in [1, 30]");
     return nullptr;
   }
-  if (desc->max_restarts != 0) {
-    set_err("pfgpu_create: only MaxRestarts 0 is supported");
+  if (desc->max_restarts < 0) {
+    set_err("pfgpu_create: max_restarts must not be negative");
     return nullptr;
   }
   if (desc->mg_smoother != PFGPU_SMOOTH_RBGS && desc->mg_smoother != PFGPU_SMOOTH_WJACOBI &&

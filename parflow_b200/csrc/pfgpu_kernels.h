@@ -317,12 +317,17 @@ void launch_scale_inv_dev(double *x, const double *s, long long n, cudaStream_t 
 // x *= a
 void launch_scale(double *x, double a, long long n, cudaStream_t st);
 // xcor = sum_k yg[k] * V[k] (sequential axpy order)
+// xcor = sum_k yg[k] V_k (onto xcor when accumulate)
 void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
-                    cudaStream_t st);
+                    cudaStream_t st, int accumulate = 0);
+// V_0 = yg[0] V_0 + sum_{k=1..kdim} yg[k] V_k (GMRES restart direction)
+void launch_restart_v0(double *const *V, const double *yg, int kdim, long long n,
+                       cudaStream_t st);
 void launch_fill(double *x, double v, long long n, cudaStream_t st);
 
 // GMRES scalar kernels (single thread); S layout and ops in krylov_kernels.cu
-enum { GM_START = 0, GM_AFTER_GS = 1, GM_QR = 3, GM_QRSOL = 4, GM_REORTH_DONE = 5 };
+enum { GM_START = 0, GM_AFTER_GS = 1, GM_QR = 3, GM_QRSOL = 4, GM_REORTH_DONE = 5,
+       GM_RESTART = 6, GM_RESTART_INIT = 7 };
 enum { SCI_RNORM = 0, SCI_ROT, SCI_RHO, SCI_VKNORM2, SCI_NEWNORM2, SCI_FLAG, SCI_NN2, SCI_NP,
        SCI_GATE, SCI_COEF, SCI_HLL, SCI_BETA, SCI_QRFAIL, SCI_COUNT };
 inline long long gs_size(int lmax) { return (long long)(lmax + 1) * lmax + 2 * lmax + lmax + 1 + SCI_COUNT; }
