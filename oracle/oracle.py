@@ -157,7 +157,7 @@ class Oracle:
         S.eta_value, S.eta_alpha, S.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
         S.mg_max_levels = s.mg_max_levels
         S.mg_smoother = s.smoother_code()
-        S.wjacobi_weight = float(s.wjacobi_weight)
+        S.wjacobi_weight = s.smoother_weight()
         S.use_jacobian = 1 if s.use_jacobian else 0
         S.derivative_epsilon = s.derivative_epsilon
         self.S = S

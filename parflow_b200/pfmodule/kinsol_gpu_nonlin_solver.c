@@ -23,7 +23,8 @@
  *     pfgpu_set_bc;
  *   - uploads evap_trans (nl_function_eval.c:533-541);
  *   - solves with pfgpu_newton_solve (KINSol with line search, SPGMR and the
- *     MGSemi preconditioner on the GPU): pressure in as the initial guess,
+ *     semicoarsening multigrid preconditioner on the GPU, keyed MGSemi or
+ *     PFMG): pressure in as the initial guess,
  *     out as the solution; old_pressure and old_saturation in;
  *   - writes the face velocities and q_overlnd_x / q_overlnd_y of the last
  *     residual evaluation (pfgpu_face_velocities) into the state vectors;
@@ -183,37 +184,67 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
   NA_FreeNameArray(na);
   na = NA_NewNameArray("NoPC MGSemi SMG PFMG PFMGOctree");
   name = GetStringDefault("Solver.Linear.Preconditioner", "MGSemi");
-  if (NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner") != 1)
-    gpu_fail("only Solver.Linear.Preconditioner MGSemi is available");
+  const int pc = NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner");
   NA_FreeNameArray(na);
+  if (pc != 1 && pc != 3)
+    gpu_fail("only Solver.Linear.Preconditioner MGSemi or PFMG is available");
   /* KinsolPC's matrix type (kinsol_pc.c:215-246) and MGSemi's keys
    * (mg_semi.c:1230-1310, rb_GS_point.c:440-470, w_jacobi.c:385-395) */
+  /* PFSymmetric, SymmetricPart and Picard give the same matrix: the
+   * Jacobian evaluation tests its symm_part argument only for zero
+   * (richards_jacobian_eval.c:760, 781, 2246) */
   na = NA_NewNameArray("FullJacobian PFSymmetric SymmetricPart Picard");
   name = GetStringDefault("Solver.Linear.Preconditioner.PCMatrixType", "PFSymmetric");
-  if (NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.PCMatrixType") != 1)
-    gpu_fail("only PCMatrixType PFSymmetric is available");
+  if (NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.PCMatrixType") == 0)
+    gpu_fail("PCMatrixType FullJacobian is not available");
   NA_FreeNameArray(na);
-  if (GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxIter", 1) != 1)
-    gpu_fail("only MGSemi.MaxIter 1 is available");
-  d->mg_max_levels = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxLevels", 100);
-  na = NA_NewNameArray("RedBlackGSPoint WJacobi");
-  name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother", "RedBlackGSPoint");
-  int smoother = NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.MGSemi.Smoother");
-  NA_FreeNameArray(na);
-  if (smoother == 0)
+  if (pc == 3)
   {
-    na = NA_NewNameArray("True False");
-    name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric", "True");
-    int sym = NA_NameToIndexExitOnError(na, name,
-                                        "Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric");
+    /* PFMG (pf_pfmg.c:285-330) on the semicoarsening multigrid: one pre-
+     * and one post-relaxation of its smoother */
+    if (GetIntDefault("Solver.Linear.Preconditioner.PFMG.MaxIter", 1) != 1 ||
+        GetIntDefault("Solver.Linear.Preconditioner.PFMG.NumPreRelax", 1) != 1 ||
+        GetIntDefault("Solver.Linear.Preconditioner.PFMG.NumPostRelax", 1) != 1)
+      gpu_fail("PFMG with MaxIter, NumPreRelax and NumPostRelax 1 only");
+    na = NA_NewNameArray("Jacobi WJacobi RBGaussSeidelSymmetric RBGaussSeidelNonSymmetric");
+    name = GetStringDefault("Solver.Linear.Preconditioner.PFMG.Smoother",
+                            "RBGaussSeidelNonSymmetric");
+    const int sm = NA_NameToIndexExitOnError(na, name,
+                                             "Solver.Linear.Preconditioner.PFMG.Smoother");
     NA_FreeNameArray(na);
-    d->mg_smoother = sym == 0 ? PFGPU_SMOOTH_RBGS : PFGPU_SMOOTH_RBGS_NONSYM;
+    if (sm == 1)
+      gpu_fail("PFMG smoother WJacobi is not available");
+    d->mg_smoother = sm == 0 ? PFGPU_SMOOTH_WJACOBI : sm == 2 ? PFGPU_SMOOTH_RBGS
+                     : PFGPU_SMOOTH_RBGS_NONSYM;
+    d->wjacobi_weight = 1.0;
+    d->mg_max_levels = 100;
   }
   else
   {
-    d->mg_smoother = PFGPU_SMOOTH_WJACOBI;
+    if (GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxIter", 1) != 1)
+      gpu_fail("only MGSemi.MaxIter 1 is available");
+    d->mg_max_levels = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxLevels", 100);
+    na = NA_NewNameArray("RedBlackGSPoint WJacobi");
+    name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother", "RedBlackGSPoint");
+    const int smoother =
+        NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.MGSemi.Smoother");
+    NA_FreeNameArray(na);
+    if (smoother == 0)
+    {
+      na = NA_NewNameArray("True False");
+      name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric", "True");
+      const int sym = NA_NameToIndexExitOnError(
+          na, name, "Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric");
+      NA_FreeNameArray(na);
+      d->mg_smoother = sym == 0 ? PFGPU_SMOOTH_RBGS : PFGPU_SMOOTH_RBGS_NONSYM;
+    }
+    else
+    {
+      d->mg_smoother = PFGPU_SMOOTH_WJACOBI;
+    }
+    d->wjacobi_weight =
+        GetDoubleDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.Weight", 1.0);
   }
-  d->wjacobi_weight = GetDoubleDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.Weight", 1.0);
   na = NA_NewNameArray("FP64 Mixed Mixed16");
   name = GetStringDefault("Solver.Nonlinear.GPU.Precision", "FP64");
   int prec = NA_NameToIndexExitOnError(na, name, "Solver.Nonlinear.GPU.Precision");

@@ -119,15 +119,36 @@ class SolverSettings:
     # red, black when False) and ...MGSemi.Smoother.Weight (WJacobi)
     mg_smoother_symmetric: bool = True
     wjacobi_weight: float = 1.0
+    # Solver.Linear.Preconditioner.PFMG.Smoother (pf_pfmg.c:300-305); the
+    # other PFMG keys keep their defaults (MaxIter 1, NumPreRelax 1,
+    # NumPostRelax 1, RAPType NonGalerkin)
+    pfmg_smoother: str = "RBGaussSeidelNonSymmetric"
 
     def smoother_code(self) -> int:
         """PFGPU_SMOOTH_* of the smoother keys: 0 symmetric red/black
-        Gauss-Seidel, 1 weighted Jacobi, 2 non-symmetric red/black."""
+        Gauss-Seidel, 1 weighted Jacobi, 2 non-symmetric red/black.  The
+        PFMG preconditioner runs on the same semicoarsening multigrid with
+        one pre- and one post-relaxation of its smoother (PFMG's defaults):
+        RBGaussSeidelNonSymmetric is one red and one black sweep,
+        RBGaussSeidelSymmetric red, black, red, Jacobi a weight-1 Jacobi
+        sweep."""
+        if self.preconditioner == "PFMG":
+            table = {"RBGaussSeidelNonSymmetric": 2, "RBGaussSeidelSymmetric": 0, "Jacobi": 1}
+            if self.pfmg_smoother not in table:
+                raise ValueError(f"PFMG smoother {self.pfmg_smoother} is not available")
+            return table[self.pfmg_smoother]
+        if self.preconditioner != "MGSemi":
+            raise ValueError(f"preconditioner {self.preconditioner} is not available")
         if self.mg_smoother == "WJacobi":
             return 1
         if self.mg_smoother != "RedBlackGSPoint":
             raise ValueError(f"unknown MGSemi smoother {self.mg_smoother}")
         return 0 if self.mg_smoother_symmetric else 2
+
+    def smoother_weight(self) -> float:
+        if self.preconditioner == "PFMG":
+            return 1.0
+        return float(self.wjacobi_weight)
     max_convergence_failures: int = 3
 
 
@@ -553,6 +574,8 @@ class RichardsProblem:
         k["Solver.Linear.Preconditioner.PCMatrixType"] = s.pc_matrix_type
         k["Solver.Linear.Preconditioner.MGSemi.MaxIter"] = s.mg_max_iter
         k["Solver.Linear.Preconditioner.MGSemi.MaxLevels"] = s.mg_max_levels
+        if s.preconditioner == "PFMG":
+            k["Solver.Linear.Preconditioner.PFMG.Smoother"] = s.pfmg_smoother
         k["Solver.Linear.Preconditioner.MGSemi.Smoother"] = s.mg_smoother
         if s.mg_smoother == "RedBlackGSPoint" and not s.mg_smoother_symmetric:
             k["Solver.Linear.Preconditioner.MGSemi.Smoother.Symmetric"] = "False"

@@ -79,7 +79,7 @@ class RichardsGPU:
         d.eta_value, d.eta_alpha, d.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
         d.mg_max_levels = s.mg_max_levels
         d.mg_smoother = s.smoother_code()
-        d.wjacobi_weight = float(s.wjacobi_weight)
+        d.wjacobi_weight = s.smoother_weight()
         self.desc = d
         self.precision = precision
         h = self.lib.pfgpu_create(C.byref(d), device)
