@@ -206,6 +206,13 @@ def restart_small() -> RichardsProblem:
                           solver=SolverSettings(krylov_dim=2, max_restarts=5, mg_max_levels=2))
 
 
+def picard_small() -> RichardsProblem:
+    """PCMatrixType Picard (the reference builds the same symmetric
+    preconditioner matrix as for PFSymmetric) on config-2 physics."""
+    return configs.hetero(nx=13, ny=11, nz=8, nsteps=2, seed=59,
+                          solver=SolverSettings(pc_matrix_type="Picard"))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -214,7 +221,8 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "overland_small", "tfg_small", "overland_diff_small",
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
-          "vel_overland_small", "growth_small", "halving_small", "restart_small"]
+          "vel_overland_small", "growth_small", "halving_small", "restart_small",
+          "picard_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

@@ -132,6 +132,12 @@ class SolverSettings:
         RBGaussSeidelNonSymmetric is one red and one black sweep,
         RBGaussSeidelSymmetric red, black, red, Jacobi a weight-1 Jacobi
         sweep."""
+        # KinsolPC's PCMatrixType (kinsol_pc.c:215-246) reaches the Jacobian
+        # evaluation as symm_part, which is only tested for zero
+        # (richards_jacobian_eval.c:760, 781, 2246): PFSymmetric,
+        # SymmetricPart and Picard build the same preconditioner matrix
+        if self.pc_matrix_type not in ("PFSymmetric", "SymmetricPart", "Picard"):
+            raise ValueError(f"PCMatrixType {self.pc_matrix_type} is not available")
         if self.preconditioner == "PFMG":
             table = {"RBGaussSeidelNonSymmetric": 2, "RBGaussSeidelSymmetric": 0, "Jacobi": 1}
             if self.pfmg_smoother not in table:
