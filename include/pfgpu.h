@@ -332,6 +332,20 @@ int pfgpu_newton_solve(pfgpu_handle *h, const double *p_old, const double *s_old
 int pfgpu_newton_solve_sat(pfgpu_handle *h, const double *p_old, const double *s_old,
                            double dt, double *p, double *s, pfgpu_stats *stats);
 
+/* How every Newton solve of the handle runs.  mode 1 (the default; the
+ * environment variable PFGPU_SOLVE_GRAPH=0 makes 0 the default): the whole
+ * solve is one CUDA graph launch, captured at the first solve and again
+ * whenever the problem's boundary tables, fields or Jacobian mode change;
+ * control kernels on the device take KINSOL's and SPGMR's decisions and the
+ * host reads the counters once per solve.  mode 0: the host drives the
+ * iteration (one small device-to-host read per GMRES iteration and per
+ * line-search evaluation).  Both take the same steps with the same
+ * arithmetic.  mode -1 returns 1 if the handle's last solve ran as a graph,
+ * 0 if it ran host-driven (phase timing on, or the graph could not be built:
+ * pfgpu_last_error then says why).  No counterpart in the reference (its
+ * KINSOL loop is host code). */
+int pfgpu_solve_graph(pfgpu_handle *h, int mode);
+
 /* Device-resident time stepping: advances the handle's own pressure state by
  * nsteps steps of dt with the boundary tables already set, keeping every
  * vector on the GPU (the step body of AdvanceRichards,

@@ -13,6 +13,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIB = os.path.join(HERE, "libpfgpu.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# the device-side Newton control restates host arithmetic: no contracted
+# multiply-adds there
+NO_FMAD_SOURCES = {"nk_control.cu"}
+NO_FMAD = ["-fmad=false"]
 
 
 def nvcc() -> str:
@@ -56,7 +60,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs.append(obj)
         if (force or not os.path.exists(obj) or os.path.getmtime(obj) < os.path.getmtime(src)
                 or os.path.getmtime(obj) < newest_header):
-            jobs.append([nvcc()] + flags + ["-c", src, "-o", obj])
+            extra = NO_FMAD if os.path.basename(src) in NO_FMAD_SOURCES else []
+            jobs.append([nvcc()] + flags + extra + ["-c", src, "-o", obj])
     # one nvcc per translation unit, in parallel
     from concurrent.futures import ThreadPoolExecutor
 

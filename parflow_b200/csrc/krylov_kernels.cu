@@ -8,6 +8,7 @@
 // pfsimulator/kinsol/iterativ.c:30-286 and spgmr.c:168-450.
 #include "pdl.cuh"
 #include "pfgpu_kernels.h"
+#include "nk_control.h"
 
 namespace pfgpu {
 
@@ -493,6 +494,121 @@ void launch_restart_v0(double *const *V, const double *yg, int kdim, long long n
   launch_pdl(k_restart_v0, dim3(grid_for(n)), dim3(256), st, V[0], L, yg, kdim, n);
 }
 
+// ---- the same steps with their scalars on the device (graph solve) ---------
+// V0 of a GMRES cycle: b / ||b|| = src * (bsign / r_norm) on the first cycle
+// (as launch_axpby with b = 0), the restart direction / its norm after
+__global__ void k_v0_init(double *__restrict__ v0, const double *__restrict__ src,
+                          const NkState *S, const double *__restrict__ sc, long long n) {
+  pdl_enter();
+  const bool first = S->ntries == 0;
+  const double a = first ? S->k.bsign * (1.0 / S->r_norm) : 1.0 / sc[SCI_RNORM];
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    if (first)
+      v0[i] = a * src[i];
+    else
+      v0[i] *= a;
+  }
+}
+__global__ void k_combine_dev(double *__restrict__ xcor, VecList V, const double *__restrict__ yg,
+                              const int *kdim_p, const int *acc_p, long long n) {
+  pdl_enter();
+  const int kdim = *kdim_p, accumulate = *acc_p;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = accumulate ? xcor[i] : 0.0;
+    for (int k = 0; k < kdim; k++) acc = yg[k] * V.v[k][i] + 1.0 * acc;
+    xcor[i] = acc;
+  }
+}
+__global__ void k_restart_v0_dev(double *v0, VecList V, const double *__restrict__ yg,
+                                 const int *kdim_p, long long n) {
+  pdl_enter();
+  const int kdim = *kdim_p;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    double acc = yg[0] * v0[i];
+    for (int k = 1; k <= kdim; k++) acc = yg[k] * V.v[k][i] + 1.0 * acc;
+    v0[i] = acc;
+  }
+}
+__global__ void k_scale_inv_dev_unless(double *__restrict__ x, const double *__restrict__ s,
+                                       const int *skip, long long n) {
+  pdl_enter();
+  if (*skip) return;
+  double a = 1.0 / (*s);
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void k_fill_if(double *__restrict__ x, double v, const int *flag, long long n) {
+  pdl_enter();
+  if (!*flag) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+// a trial step: z = x + lam y, or z = x when lam == 0 (the copy of KINSOL's
+// N_VScale(ONE, uu, unew))
+__global__ void k_xpay_lam(double *__restrict__ z, const double *__restrict__ x,
+                           const double *lam, const double *__restrict__ y, long long n) {
+  pdl_enter();
+  const double a = *lam;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    z[i] = (a == 0.0) ? x[i] : x[i] + a * y[i];
+}
+__global__ void k_scale_by(double *__restrict__ x, const double *a_p, long long n) {
+  pdl_enter();
+  const double a = *a_p;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    x[i] *= a;
+}
+__global__ void k_copy_if(double *__restrict__ dst, const double *__restrict__ src,
+                          const int *flag, long long n) {
+  pdl_enter();
+  if (!*flag) return;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x)
+    dst[i] = src[i];
+}
+
+void launch_v0_init(double *v0, const double *src, const NkState *S, const double *sc,
+                    long long n, cudaStream_t st) {
+  launch_pdl(k_v0_init, dim3(grid_for(n)), dim3(256), st, v0, src, S, sc, n);
+}
+void launch_combine_dev(double *xcor, double *const *V, int nv, const double *yg, const int *kdim,
+                        const int *accumulate, long long n, cudaStream_t st) {
+  VecList L{};
+  for (int k = 0; k < nv && k < 32; k++) L.v[k] = V[k];
+  launch_pdl(k_combine_dev, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, accumulate, n);
+}
+void launch_restart_v0_dev(double *const *V, int nv, const double *yg, const int *kdim,
+                           long long n, cudaStream_t st) {
+  VecList L{};
+  for (int k = 0; k < nv && k < 32; k++) L.v[k] = V[k];
+  launch_pdl(k_restart_v0_dev, dim3(grid_for(n)), dim3(256), st, V[0], L, yg, kdim, n);
+}
+void launch_scale_inv_dev_unless(double *x, const double *s, const int *skip, long long n,
+                                 cudaStream_t st) {
+  launch_pdl(k_scale_inv_dev_unless, dim3(grid_for(n)), dim3(256), st, x, s, skip, n);
+}
+void launch_fill_if(double *x, double v, const int *flag, long long n, cudaStream_t st) {
+  launch_pdl(k_fill_if, dim3(grid_for(n)), dim3(256), st, x, v, flag, n);
+}
+void launch_xpay_lam(double *z, const double *x, const double *lam, const double *y, long long n,
+                     cudaStream_t st) {
+  launch_pdl(k_xpay_lam, dim3(grid_for(n)), dim3(256), st, z, x, lam, y, n);
+}
+void launch_scale_by(double *x, const double *a, long long n, cudaStream_t st) {
+  launch_pdl(k_scale_by, dim3(grid_for(n)), dim3(256), st, x, a, n);
+}
+void launch_copy_if(double *dst, const double *src, const int *flag, long long n,
+                    cudaStream_t st) {
+  launch_pdl(k_copy_if, dim3(grid_for(n)), dim3(256), st, dst, src, flag, n);
+}
+
 // ---- GMRES scalars ----------------------------------------------------------
 // S layout: [0, (lmax+1)*lmax) Hessenberg H(i,j) at i*lmax+j; then givens
 // (2*lmax), yg (lmax+1), then named scalars.
@@ -529,8 +645,7 @@ __device__ void givens(double t1, double t2, double &c, double &s) {
   }
 }
 
-__global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
-  pdl_enter();
+__device__ __forceinline__ void gmres_scalar_op(int op, double *S, int l, int lmax) {
   GS g = gs_view(S, lmax);
   double *sc = g.sc;
   switch (op) {
@@ -632,6 +747,15 @@ __global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
     }
   }
 }
+__global__ void k_gmres_scalar(int op, double *S, int l, int lmax) {
+  pdl_enter();
+  gmres_scalar_op(op, S, l, lmax);
+}
+// the same step with its column / Krylov dimension read from the device
+__global__ void k_gmres_scalar_dev(int op, double *S, const int *l, int lmax) {
+  pdl_enter();
+  gmres_scalar_op(op, S, *l, lmax);
+}
 
 // Reorthogonalisation decision for basis vector i against V_k
 // (iterativ.c:68-77): dot result in SC_NP; sets SC_GATE (apply?) and SC_COEF.
@@ -665,6 +789,9 @@ __global__ void k_axpy_gated(double *__restrict__ y, const double *__restrict__ 
 
 void launch_gmres_scalar(int op, double *S, int l, int lmax, cudaStream_t st) {
   launch_pdl(k_gmres_scalar, dim3(1), dim3(1), st, op, S, l, lmax);
+}
+void launch_gmres_scalar_dev(int op, double *S, const int *l, int lmax, cudaStream_t st) {
+  launch_pdl(k_gmres_scalar_dev, dim3(1), dim3(1), st, op, S, l, lmax);
 }
 void launch_reorth_decide(double *S, int i, int l, int lmax, cudaStream_t st) {
   launch_pdl(k_reorth_decide, dim3(1), dim3(1), st, S, i, l, lmax);

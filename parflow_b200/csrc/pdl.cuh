@@ -21,12 +21,18 @@ __device__ __forceinline__ void pdl_enter() {
 #endif
 }
 
+// set while capturing a graph whose driver refused programmatic edges
+inline bool &pdl_capture_off() {
+  static thread_local bool off = false;
+  return off;
+}
+
 inline bool pdl_on() {
   static const bool on = [] {
     const char *v = getenv("PFGPU_PDL");
     return !(v && *v == '0');
   }();
-  return on;
+  return on && !pdl_capture_off();
 }
 
 template <typename... KArgs, typename... Args>

@@ -3,13 +3,18 @@
 //
 // Control flow mirrors the embedded KINSOL of ParFlow (pfsimulator/kinsol/
 // kinsol.c:690-910, kinspgmr.c:344-440, spgmr.c:168-450, iterativ.c:30-286)
-// with every vector and every GMRES scalar in device memory; the host reads
-// back only the few scalars that steer control flow (one small copy per
-// GMRES iteration and per line-search evaluation).  The multigrid V-cycle is
-// a fixed kernel sequence and is replayed from a CUDA graph.
+// with every vector and every GMRES scalar in device memory.  By default a
+// whole Newton solve is one CUDA graph launch: control kernels on the device
+// take the decisions and steer the graph's conditional nodes, and the host
+// reads the solve's counters once at its end.  The host-driven form (one
+// small read per GMRES iteration and per line-search evaluation) remains for
+// phase timing and as the reference the graph solve is tested against.  The
+// multigrid V-cycle is a fixed kernel sequence and is replayed from a CUDA
+// graph.
 #include <cuda_runtime.h>
 
 #include <cfloat>
+#include <chrono>
 #include <cmath>
 #include <algorithm>
 #include <array>
@@ -25,6 +30,8 @@
 #include <vector>
 
 #include "../../include/pfgpu.h"
+#include "nk_control.h"
+#include "pdl.cuh"
 #include "pfgpu_kernels.h"
 
 using namespace pfgpu;
@@ -51,20 +58,6 @@ void pfgpu::record_error(const char *msg) { set_err("%s", msg); }
   } while (0)
 
 namespace {
-
-// device scalar slots
-enum {
-  D_F2 = 0,      // <f, f>
-  D_FMAX,        // max |f|
-  D_STEP,        // max |unew - u| / (1 + |unew|)
-  D_P2,          // <p, p>
-  D_PLEN,        // max |p| / (1 + |u|)
-  D_JP2,         // <Jp, Jp>
-  D_FJP,         // <f, Jp>
-  D_U2,          // <u, u>
-  D_COUNT,
-  D_DQ = 40      // five slots of the difference-quotient product (launch_dq_prepare)
-};
 
 struct Handle;
 
@@ -219,6 +212,27 @@ struct pfgpu_handle {
   std::vector<std::array<int, 3>> pmark;        // (phase, start event, end event)
   double pacc[8] = {};
   long long pcnt[8] = {};
+  // the Newton solve captured as one CUDA graph (device-side control)
+  struct NkGraph {
+    bool enabled = true;   // pfgpu_solve_graph / PFGPU_SOLVE_GRAPH
+    bool failed = false;   // capture or instantiation failed: host-driven solves
+    bool used_last = false;
+    bool capturing = false;
+    cudaGraphExec_t exec = nullptr;
+    NkState *S = nullptr;   // device control state
+    NkState *hS = nullptr;  // pinned host copy
+    double *dt = nullptr, *hdt = nullptr;
+    cudaStream_t cs[6] = {};  // capture streams, one per nesting depth
+    long long kernels[NKB_COUNT] = {};
+    std::vector<std::array<long long, 3>> stack;  // (body, launches at entry, nested)
+    // what the graph was captured for
+    unsigned char key_P[sizeof(DevProblem)] = {};
+    unsigned char key_d[sizeof(pfgpu_desc)] = {};
+    const double *key_u = nullptr, *key_unew = nullptr;
+    int key_usejac = -1;
+    double key_relfunc = 0.0;
+    bool valid = false;
+  } nk;
 };
 
 // ---------------------------------------------------------------------------
@@ -533,7 +547,12 @@ static int pc_apply_dense_impl(pfgpu_handle *h, const double *r, double *z) {
   else
     k += launch_level_in<double>(h->mgd.L[0], r, nullptr, h->st);
   CK(cudaGetLastError());
-  CK(cudaGraphLaunch(h->vgraph, h->st));
+  if (h->nk.capturing) {
+    k += (int)vcycle_launch(h);  // inline in the solve's graph
+  } else {
+    CK(cudaGraphLaunch(h->vgraph, h->st));
+    h->launches += h->graph_nodes;
+  }
   if (h->mixed)
     k += launch_level_out<float>(h->mgf.L[0], vcycle_out(h->mgf, h->d.mg_smoother), z,
                                  h->h16 ? h->mgf.L[0].sinv : nullptr, h->mgf.flip_out, h->st);
@@ -541,7 +560,7 @@ static int pc_apply_dense_impl(pfgpu_handle *h, const double *r, double *z) {
     k += launch_level_out<double>(h->mgd.L[0], vcycle_out(h->mgd, h->d.mg_smoother), z, nullptr,
                                   h->mgd.flip_out, h->st);
   CK(cudaGetLastError());
-  h->launches += h->graph_nodes + k;
+  h->launches += k;
   return 0;
 }
 static int pc_apply_dense(pfgpu_handle *h, const double *r, double *z) {
@@ -955,6 +974,470 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   stats->fnorm = fnorm;
   return (ret == 1 || ret == 2) ? PFGPU_OK : PFGPU_NOT_CONVERGED;
 }
+// ---------------------------------------------------------------------------
+// The Newton solve as one CUDA graph.  The same launches as newton_impl and
+// spgmr, captured once per handle; the decisions the host makes there between
+// launches are made on the device by the control kernels of nk_control.cu,
+// which steer conditional nodes:
+//
+//   F(u), norms, init
+//   WHILE newton:
+//     iter; J and preconditioner setup; SPGMR start
+//     WHILE restart:                        (one GMRES cycle)
+//       cycle_begin; V0
+//       iteration 0, IF iteration 1, ..., IF iteration lmax-1
+//       QR solve; x (+)= V y; cycle_end
+//       IF restart: restart direction
+//     after_gmres; IF post: x = M^{-1} V y; x = 0 when SPGMR gave none
+//     IF ok:
+//       J p, line-search inputs; ls_init; IF scale: scale p
+//       WHILE backtrack: trial; ls1
+//       WHILE refine: trial; ls2
+//       IF rllo: trial; ls3
+//       newton_end; u <- unew
+//     tail
+//   final
+//
+// The vectors and the iterate keep their buffers (u <- unew is a copy where
+// the host-driven loop swaps pointers); dt is read from device memory, so one
+// graph serves every timestep until the problem's device description, the
+// iterate buffers or the Jacobian mode change.
+// ---------------------------------------------------------------------------
+static void nk_begin(pfgpu_handle *h, int body) {
+  h->nk.stack.push_back({(long long)body, h->launches, 0});
+}
+static void nk_end(pfgpu_handle *h) {
+  const std::array<long long, 3> t = h->nk.stack.back();
+  h->nk.stack.pop_back();
+  const long long total = h->launches - t[1];
+  h->nk.kernels[t[0]] += total - t[2];
+  if (!h->nk.stack.empty()) h->nk.stack.back()[2] += total;
+}
+
+// a conditional handle of the graph being captured on stream s
+static int nk_handle(cudaStream_t s, cudaGraphConditionalHandle *hd) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr));
+  CK(cudaGraphConditionalHandleCreate(hd, g, 0, 0));
+  return 0;
+}
+
+// appends a conditional node at the capture point of stream s; returns its body
+static int nk_cond(cudaStream_t s, cudaGraphConditionalHandle hd,
+                   cudaGraphConditionalNodeType type, cudaGraph_t *body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t g = nullptr;
+  const cudaGraphNode_t *deps = nullptr;
+  size_t nd = 0;
+  CK(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+  cudaGraphNodeParams p = {};
+  p.type = cudaGraphNodeTypeConditional;
+  p.conditional.handle = hd;
+  p.conditional.type = type;
+  p.conditional.size = 1;
+  cudaGraphNode_t node;
+  CK(cudaGraphAddNode(&node, g, deps, nd, &p));
+  CK(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+  *body = p.conditional.phGraph_out[0];
+  return 0;
+}
+
+// captures fn's launches into a conditional node's body on the capture
+// stream of nesting depth `depth`, attributing them to body `count`
+template <typename F>
+static int nk_body(pfgpu_handle *h, cudaGraphConditionalHandle hd,
+                   cudaGraphConditionalNodeType type, int depth, int count, F fn) {
+  cudaGraph_t body = nullptr;
+  if (nk_cond(h->st, hd, type, &body)) return PFGPU_ERR_CUDA;
+  cudaStream_t s = h->nk.cs[depth];
+  CK(cudaStreamBeginCaptureToGraph(s, body, nullptr, nullptr, 0,
+                                   cudaStreamCaptureModeThreadLocal));
+  cudaStream_t saved = h->st;
+  h->st = s;
+  nk_begin(h, count);
+  int rc = fn();
+  if (!rc && cudaPeekAtLastError() != cudaSuccess) {
+    set_err("launch failed while capturing the solve graph: %s",
+            cudaGetErrorString(cudaGetLastError()));
+    rc = PFGPU_ERR_CUDA;
+  }
+  nk_end(h);
+  h->st = saved;
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s, &out);
+  if (rc) return rc;
+  CK(e);
+  return 0;
+}
+
+static void nk_try_step(pfgpu_handle *h, double dt) {
+  const long long N = h->N;
+  double *dsc = h->dsc;
+  launch_xpay_lam(h->unew, h->u, &h->nk.S->lam, h->pp, N, h->st);
+  feval(h, h->unew, dt, h->fval);
+  launch_step_norms(h->fval, h->unew, h->u, N, dsc + D_F2, dsc + D_FMAX, dsc + D_STEP, h->rb,
+                    h->st);
+  h->launches += 2;
+}
+
+// one GMRES iteration l of a cycle (as the body of spgmr's inner loop)
+static int nk_gmres_iter(pfgpu_handle *h, int l, double dt, NkConds &C) {
+  const long long N = h->N;
+  const int lmax = h->d.krylov_dim;
+  double *S = h->gs;
+  double *sc = S + gs_sc_offset(lmax);
+  auto Hp = [&](int i, int j) { return S + (long long)i * lmax + j; };
+  pfgpu_stats dummy{};
+  if (pc_apply_dense_impl(h, h->V[l], h->vtemp)) return PFGPU_ERR_CUDA;
+  atimes(h, h->u, dt, h->vtemp, h->V[l + 1], &dummy);
+  const int k = l + 1;
+  launch_mgs_first(h->V[k], h->V[0], N, sc + SCI_VKNORM2, Hp(0, k - 1), h->rb, h->st);
+  h->launches++;
+  for (int i = 0; i < k; i++) {
+    const bool more = i + 1 < k;
+    launch_axpy_dot(h->V[k], h->V[i], Hp(i, k - 1), -1.0, more ? h->V[i + 1] : nullptr, N,
+                    more ? Hp(i + 1, k - 1) : sc + SCI_NEWNORM2, h->rb, h->st);
+    h->launches++;
+  }
+  launch_gmres_scalar(GM_AFTER_GS, S, l, lmax, h->st);
+  h->launches++;
+  for (int i = 0; i < k; i++) {
+    launch_dot_gated(h->V[i], h->V[k], N, sc + SCI_NP, sc + SCI_FLAG, h->rb, h->st);
+    launch_reorth_decide(S, i, l, lmax, h->st);
+    launch_axpy_gated(h->V[k], h->V[i], sc + SCI_COEF, sc + SCI_GATE, N, h->st);
+    h->launches += 3;
+  }
+  launch_gmres_scalar(GM_REORTH_DONE, S, l, lmax, h->st);
+  launch_gmres_scalar(GM_QR, S, l, lmax, h->st);
+  launch_nk_gm_iter(h->nk.S, sc, l, C, h->st);
+  launch_scale_inv_dev_unless(h->V[l + 1], Hp(l + 1, l), &h->nk.S->converged, N, h->st);
+  h->launches += 4;
+  return 0;
+}
+
+// one GMRES cycle (the body of spgmr's restart loop)
+static int nk_gmres_cycle(pfgpu_handle *h, double dt, NkConds &C) {
+  const long long N = h->N;
+  const int lmax = h->d.krylov_dim;
+  double *S = h->gs;
+  double *sc = S + gs_sc_offset(lmax);
+  NkState *St = h->nk.S;
+  for (int l = 1; l < lmax; l++)
+    if (nk_handle(h->st, &C.iter[l])) return PFGPU_ERR_CUDA;
+  if (nk_handle(h->st, &C.do_restart)) return PFGPU_ERR_CUDA;
+  launch_nk_cycle_begin(St, C, h->st);
+  launch_v0_init(h->V[0], h->fval, St, sc, N, h->st);
+  h->launches += 2;
+  nk_begin(h, NKB_GM0);
+  int rc = nk_gmres_iter(h, 0, dt, C);
+  nk_end(h);
+  if (rc) return rc;
+  for (int l = 1; l < lmax; l++) {
+    rc = nk_body(h, C.iter[l], cudaGraphCondTypeIf, 3, NKB_GM0 + l,
+                 [&]() { return nk_gmres_iter(h, l, dt, C); });
+    if (rc) return rc;
+  }
+  launch_gmres_scalar_dev(GM_QRSOL, S, &St->krydim, lmax, h->st);
+  launch_combine_dev(h->xcor, h->V.data(), lmax + 1, S + gs_yg_offset(lmax), &St->krydim,
+                     &St->accumulate, N, h->st);
+  launch_nk_cycle_end(St, sc, C, h->st);
+  h->launches += 3;
+  return nk_body(h, C.do_restart, cudaGraphCondTypeIf, 3, NKB_RESTART, [&]() {
+    launch_gmres_scalar_dev(GM_RESTART, S, &St->krydim, lmax, h->st);
+    launch_restart_v0_dev(h->V.data(), lmax + 1, S + gs_yg_offset(lmax), &St->krydim, N, h->st);
+    launch_gmres_scalar(GM_RESTART_INIT, S, 0, lmax, h->st);
+    launch_nk_count(St, NKB_RESTART, 0, h->st);
+    h->launches += 4;
+    return 0;
+  });
+}
+
+// the line search after a successful linear solve (kinsol.c:1228-1420)
+static int nk_line_search(pfgpu_handle *h, double dt, NkConds &C) {
+  const long long N = h->N;
+  double *dsc = h->dsc;
+  NkState *St = h->nk.S;
+  pfgpu_stats dummy{};
+  if (nk_handle(h->st, &C.scale) || nk_handle(h->st, &C.ls1) || nk_handle(h->st, &C.ls2) ||
+      nk_handle(h->st, &C.ls3))
+    return PFGPU_ERR_CUDA;
+  atimes(h, h->u, dt, h->pp, h->bb, &dummy);
+  launch_linesearch_inputs(h->bb, h->fval, h->pp, h->u, N, dsc + D_JP2, dsc + D_FJP, dsc + D_P2,
+                           dsc + D_PLEN, h->rb, h->st);
+  launch_nk_ls_init(St, dsc, C, h->st);
+  h->launches += 2;
+  int rc = nk_body(h, C.scale, cudaGraphCondTypeIf, 3, NKB_SCALE, [&]() {
+    launch_scale_by(h->pp, &St->ratio, N, h->st);
+    launch_steplen(h->pp, h->u, N, dsc + D_PLEN, h->rb, h->st);
+    launch_nk_count(St, NKB_SCALE, 0, h->st);
+    h->launches += 3;
+    return 0;
+  });
+  if (rc) return rc;
+  launch_nk_ls_setup(St, dsc, C, h->st);
+  h->launches++;
+  rc = nk_body(h, C.ls1, cudaGraphCondTypeWhile, 3, NKB_LS1, [&]() {
+    nk_try_step(h, dt);
+    launch_nk_ls1(St, dsc, C, h->st);
+    h->launches++;
+    return 0;
+  });
+  if (rc) return rc;
+  launch_nk_ls2_init(St, C, h->st);
+  h->launches++;
+  rc = nk_body(h, C.ls2, cudaGraphCondTypeWhile, 3, NKB_LS2, [&]() {
+    nk_try_step(h, dt);
+    launch_nk_ls2(St, dsc, C, h->st);
+    h->launches++;
+    return 0;
+  });
+  if (rc) return rc;
+  launch_nk_ls3_decide(St, C, h->st);
+  h->launches++;
+  rc = nk_body(h, C.ls3, cudaGraphCondTypeIf, 3, NKB_LS3, [&]() {
+    nk_try_step(h, dt);
+    launch_nk_ls3(St, dsc, h->st);
+    h->launches++;
+    return 0;
+  });
+  if (rc) return rc;
+  launch_nk_newton_end(St, h->st);
+  launch_copy_if(h->u, h->unew, &St->do_copy, N, h->st);
+  h->launches += 2;
+  return 0;
+}
+
+// one Newton iteration (the body of newton_impl's loop)
+static int nk_newton_iter(pfgpu_handle *h, double dt, NkConds &C) {
+  const long long N = h->N;
+  const int lmax = h->d.krylov_dim;
+  double *S = h->gs;
+  double *sc = S + gs_sc_offset(lmax);
+  NkState *St = h->nk.S;
+  if (nk_handle(h->st, &C.ok) || nk_handle(h->st, &C.restart) || nk_handle(h->st, &C.post))
+    return PFGPU_ERR_CUDA;
+  launch_nk_iter(St, C, h->st);
+  h->launches++;
+  h->jac_valid = 0;
+  pc_setup_dense_impl(h, h->u, dt, h->use_jacobian != 0, true);
+  CK(cudaMemcpyAsync(sc + SCI_RNORM, h->dsc + D_F2, sizeof(double), cudaMemcpyDeviceToDevice,
+                     h->st));
+  launch_gmres_scalar(GM_START, S, 0, lmax, h->st);
+  h->launches++;
+  int rc = nk_body(h, C.restart, cudaGraphCondTypeWhile, 2, NKB_CYCLE,
+                   [&]() { return nk_gmres_cycle(h, dt, C); });
+  if (rc) return rc;
+  launch_nk_after_gmres(St, C, h->st);
+  h->launches++;
+  rc = nk_body(h, C.post, cudaGraphCondTypeIf, 2, NKB_POST, [&]() {
+    if (pc_apply_dense_impl(h, h->xcor, h->pp)) return (int)PFGPU_ERR_CUDA;
+    launch_nk_count(St, NKB_POST, 1, h->st);
+    h->launches++;
+    return 0;
+  });
+  if (rc) return rc;
+  launch_fill_if(h->pp, 0.0, &St->zero_x, N, h->st);
+  h->launches++;
+  rc = nk_body(h, C.ok, cudaGraphCondTypeIf, 2, NKB_OK,
+               [&]() { return nk_line_search(h, dt, C); });
+  if (rc) return rc;
+  launch_nk_tail(St, C, h->st);
+  h->launches++;
+  return 0;
+}
+
+static void nk_key(pfgpu_handle *h, bool store, bool *same) {
+  pfgpu_handle::NkGraph &G = h->nk;
+  DevProblem P;
+  memcpy(&P, &h->P, sizeof(P));
+  P.dtp = nullptr;
+  if (store) {
+    memcpy(G.key_P, &P, sizeof(P));
+    memcpy(G.key_d, &h->d, sizeof(h->d));
+    G.key_u = h->u;
+    G.key_unew = h->unew;
+    G.key_usejac = h->use_jacobian;
+    G.key_relfunc = h->sqrt_relfunc;
+    return;
+  }
+  *same = memcmp(G.key_P, &P, sizeof(P)) == 0 && memcmp(G.key_d, &h->d, sizeof(h->d)) == 0 &&
+          G.key_u == h->u && G.key_unew == h->unew && G.key_usejac == h->use_jacobian &&
+          G.key_relfunc == h->sqrt_relfunc;
+}
+
+static int nk_capture(pfgpu_handle *h, cudaGraph_t *graph) {
+  pfgpu_handle::NkGraph &G = h->nk;
+  const long long N = h->N;
+  double *dsc = h->dsc;
+  NkConds C{};
+  for (auto &k : G.kernels) k = 0;
+  G.stack.clear();
+  cudaStream_t s0 = G.cs[0];
+  CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  cudaStream_t saved = h->st;
+  h->st = s0;
+  int rc = nk_handle(s0, &C.newton);
+  if (!rc) {
+    nk_begin(h, NKB_TOP);
+    h->vg_for = nullptr;
+    const double dt = 0.0;  // the kernels read dt from G.dt (P.dtp)
+    feval(h, h->u, dt, h->fval);
+    launch_init_norms(h->u, h->fval, N, dsc + D_U2, dsc + D_FMAX, dsc + D_F2, h->rb, h->st);
+    launch_nk_init(G.S, dsc, C, h->st);
+    h->launches += 2;
+    rc = nk_body(h, C.newton, cudaGraphCondTypeWhile, 1, NKB_NEWTON,
+                 [&]() { return nk_newton_iter(h, dt, C); });
+    launch_nk_final(G.S, h->st);
+    h->launches++;
+    nk_end(h);
+  }
+  h->st = saved;
+  *graph = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s0, graph);
+  if (rc) {
+    if (*graph) cudaGraphDestroy(*graph);
+    *graph = nullptr;
+    return rc;
+  }
+  CK(e);
+  return 0;
+}
+
+// (re)builds the solve graph when what it was captured for has changed
+static int nk_prepare(pfgpu_handle *h) {
+  pfgpu_handle::NkGraph &G = h->nk;
+  if (G.valid) {
+    bool same = false;
+    nk_key(h, false, &same);
+    if (same) return 0;
+    CK(cudaGraphExecDestroy(G.exec));
+    G.exec = nullptr;
+    G.valid = false;
+  }
+  if (!G.S) {
+    if (dalloc(&G.S, 1) || dalloc(&G.dt, 1)) return PFGPU_ERR_CUDA;
+    CK(cudaMallocHost(&G.hS, sizeof(NkState)));
+    CK(cudaMallocHost(&G.hdt, sizeof(double)));
+    for (auto &s : G.cs) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  }
+  // constants of the solve (newton_impl's set-up)
+  const pfgpu_desc &d = h->d;
+  const double uround = DBL_EPSILON;
+  NkConst k{};
+  k.fnormtol = d.residual_tol;
+  k.scsteptol = d.step_tol;
+  if (k.scsteptol <= 0.0) k.scsteptol = pow(uround, 2.0 / 3.0);
+  if (k.fnormtol <= 0.0) k.fnormtol = pow(uround, 1.0 / 3.0);
+  k.mxiter = d.max_iter > 0 ? d.max_iter : 200;
+  k.etaflag = d.eta_choice;
+  if (k.etaflag == 1) k.ealpha = (1.0 + sqrt(5.0)) / 2.0;
+  if (k.etaflag == 2) {
+    k.ealpha = d.eta_alpha;
+    k.egamma = d.eta_gamma;
+    if (k.ealpha <= 1.0 || k.ealpha > 2.0) k.ealpha = 2.0;
+    if (k.egamma <= 0.0 || k.egamma > 1.0) k.egamma = 0.9;
+  }
+  k.eta0 = (k.etaflag == 0) ? d.eta_value : 0.5;
+  if (k.eta0 <= 0.0 || k.eta0 > 1.0) k.eta0 = 0.1;
+  k.epsmin = 0.01 * k.fnormtol;
+  k.bsign = -1.0;
+  k.lmax = d.krylov_dim;
+  k.max_restarts = d.max_restarts;
+  k.use_dq = h->use_jacobian ? 0 : 1;
+  CK(cudaMemcpy(&G.S->k, &k, sizeof(k), cudaMemcpyHostToDevice));
+
+  const DevProblem P0 = h->P;
+  const long long launches0 = h->launches;
+  const int jac0 = h->jac_valid;
+  h->P.dtp = G.dt;
+  G.capturing = true;
+  cudaGraph_t graph = nullptr;
+  int rc = nk_capture(h, &graph);
+  cudaGraphExec_t exec = nullptr;
+  if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    // programmatic launches inside conditional bodies are what a driver may
+    // refuse: capture again without them
+    cudaGetLastError();
+    cudaGraphDestroy(graph);
+    graph = nullptr;
+    exec = nullptr;
+    pdl_capture_off() = true;
+    rc = nk_capture(h, &graph);
+    pdl_capture_off() = false;
+    if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+      set_err("solve graph: instantiation failed: %s", cudaGetErrorString(cudaGetLastError()));
+      exec = nullptr;
+      rc = PFGPU_ERR_CUDA;
+    }
+  }
+  if (graph) cudaGraphDestroy(graph);
+  G.capturing = false;
+  h->P = P0;
+  h->launches = launches0;
+  h->jac_valid = jac0;
+  h->vg_for = nullptr;
+  if (rc) return rc;
+  CK(cudaGraphUpload(exec, h->st));
+  G.exec = exec;
+  G.valid = true;
+  nk_key(h, true, nullptr);
+  return 0;
+}
+
+static bool nk_usable(pfgpu_handle *h) {
+  const pfgpu_handle::NkGraph &G = h->nk;
+  if (!G.enabled || G.failed || h->ptime) return false;
+  // cooperative launches stay out of captured graphs
+  return (h->mixed ? h->mgf.grid_blocks : h->mgd.grid_blocks) == 0;
+}
+
+static int newton_graph(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
+  pfgpu_handle::NkGraph &G = h->nk;
+  *G.hdt = dt;
+  CK(cudaMemcpyAsync(G.dt, G.hdt, sizeof(double), cudaMemcpyHostToDevice, h->st));
+  CK(cudaGraphLaunch(G.exec, h->st));
+  CK(cudaMemcpyAsync(G.hS, G.S, sizeof(NkState), cudaMemcpyDeviceToHost, h->st));
+  // every loop of the graph is bounded by its control kernels; the host
+  // still waits at most PFGPU_SOLVE_TIMEOUT_S seconds (default 600)
+  {
+    static const double limit = (double)env_ll("PFGPU_SOLVE_TIMEOUT_S", 600);
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      const cudaError_t q = cudaStreamQuery(h->st);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) CK(q);
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
+        set_err("solve graph did not finish within %.0f s", limit);
+        return PFGPU_ERR_STATE;
+      }
+    }
+  }
+  const NkState &S = *G.hS;
+  long long k = 0;
+  for (int b = 0; b < NKB_COUNT; b++) k += G.kernels[b] * (long long)S.execs[b];
+  h->launches += k;
+  h->vg_for = nullptr;
+  h->jac_valid = 0;
+  memset(stats, 0, sizeof(*stats));
+  stats->nonlin_iters = S.nonlin_iters;
+  stats->lin_iters = S.lin_iters;
+  stats->fevals = S.fevals;
+  stats->pc_setups = S.pc_setups;
+  stats->pc_solves = S.pc_solves;
+  stats->lin_conv_fails = S.lin_conv_fails;
+  stats->beta_cond_fails = S.beta_cond_fails;
+  stats->backtracks = S.backtracks;
+  stats->kinsol_status = S.kinsol_status;
+  stats->fnorm = S.fnorm;
+  if (S.err) {
+    set_err("line search exceeded its iteration bound");
+    return PFGPU_ERR_STATE;
+  }
+  const int ret = S.kinsol_status;
+  return (ret == 1 || ret == 2) ? PFGPU_OK : PFGPU_NOT_CONVERGED;
+}
+
 static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
   const int ov = h->P.bc_type[5];
   if (!h->use_jacobian && (ov == PFGPU_BC_OVERLAND_KIN || ov == PFGPU_BC_OVERLAND_DIFF ||
@@ -963,6 +1446,17 @@ static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
     // preconditioner terms in another form (richards_jacobian_eval.c:1244-1283)
     set_err("difference-quotient J v (UseJacobian False) with an overland face is not available");
     return PFGPU_ERR_STATE;
+  }
+  h->nk.used_last = false;
+  if (nk_usable(h)) {
+    const int rc = nk_prepare(h);
+    if (rc == PFGPU_OK) {
+      h->nk.used_last = true;
+      return newton_graph(h, dt, stats);
+    }
+    // the solve runs host-driven from now on; the reason stays readable
+    // through pfgpu_last_error until the next failing call
+    h->nk.failed = true;
   }
   const int m = ph_begin(h);
   const int rc = newton_impl(h, dt, stats);
@@ -1260,6 +1754,13 @@ static void destroy_impl(pfgpu_handle *h) {
   cudaFree(h->vel);
   cudaFree(h->vstage);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
+  if (h->nk.exec) cudaGraphExecDestroy(h->nk.exec);
+  cudaFree(h->nk.S);
+  cudaFree(h->nk.dt);
+  if (h->nk.hS) cudaFreeHost(h->nk.hS);
+  if (h->nk.hdt) cudaFreeHost(h->nk.hdt);
+  for (cudaStream_t s : h->nk.cs)
+    if (s) cudaStreamDestroy(s);
   cudaFree(h->hist);
   cudaFree(h->adj);
   double *vecs[] = {h->u, h->unew, h->fval, h->pp, h->bb, h->p_old, h->s_old, h->kr,
@@ -1343,6 +1844,7 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
   h->mixed = desc->precision == PFGPU_PREC_MIXED || desc->precision == PFGPU_PREC_MIXED_H16;
   h->h16 = desc->precision == PFGPU_PREC_MIXED_H16;
   h->ptime = env_ll("PFGPU_PHASE_TIMES", 0) != 0;
+  h->nk.enabled = env_ll("PFGPU_SOLVE_GRAPH", 0) != 0;
   if (create_impl(h) != 0) {
     destroy_impl(h);
     delete h;
@@ -2129,6 +2631,21 @@ int pfgpu_newton_solve_sat(pfgpu_handle *h, const double *p_old, const double *s
   int rc2 = out_vec(h, h->u, p);
   if (!rc2) rc2 = out_vec(h, h->fval, s);
   return rc2 ? rc2 : rc;
+}
+
+int pfgpu_solve_graph(pfgpu_handle *h, int mode) {
+  if (!h) {
+    set_err("pfgpu_solve_graph: null handle");
+    return PFGPU_ERR_ARG;
+  }
+  if (mode == 0 || mode == 1) {
+    h->nk.enabled = mode == 1;
+    h->nk.failed = false;
+    return PFGPU_OK;
+  }
+  if (mode == -1) return h->nk.used_last ? 1 : 0;
+  set_err("pfgpu_solve_graph: mode must be 0, 1 or -1");
+  return PFGPU_ERR_ARG;
 }
 
 int pfgpu_set_pressure(pfgpu_handle *h, const double *p) {

@@ -50,6 +50,9 @@ struct DevProblem {
   // land-surface sink/source per cell [1/h] (the evap_trans vector,
   // nl_function_eval.c:533-541), dense interior layout, or null = 0
   const double *et;
+  // timestep read from device memory by the residual and Jacobian kernels
+  // (a graph captured once serves every dt), or null: the launch's dt
+  const double *dtp;
   // thread-block shapes (bx, by) of the residual, Jacobian and matvec
   // launches picked by pfgpu_autotune; (0, 0) = the default heuristic.
   // Host-side launch configuration only: no kernel reads it.

@@ -252,6 +252,7 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
                            const double *__restrict__ kr, const double *__restrict__ satv,
                            double dt, double *__restrict__ f, VelOut V = VelOut{}) {
   pdl_enter();
+  if (P.dtp) dt = *P.dtp;
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
   const long long c = i + (long long)P.nx * (j + (long long)P.ny * k);
@@ -317,6 +318,7 @@ __global__ void __launch_bounds__(256) k_residual_zm(DevProblem P, const double 
   double *sE = zm_smem;                    // [by][bx + 1]: sE[ty][tx + 1] = right face of (tx, ty)
   double *sN = zm_smem + by * (bx + 1);    // [by + 1][bx]: sN[ty + 1][tx] = front face
   pdl_enter();
+  if (P.dtp) dt = *P.dtp;
   const int i = blockIdx.x * bx + tx, j = blockIdx.y * by + ty;
   const int k0 = blockIdx.z * kchunk, k1 = min(P.nz, k0 + kchunk);
   const bool in = i < P.nx && j < P.ny;
@@ -723,6 +725,7 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
                            const double *__restrict__ satv, const double *__restrict__ dsatv,
                            double dt, JacOut<TJ> J, PCOut<TP> M) {
   pdl_enter();
+  if (P.dtp) dt = *P.dtp;
   using TA = TJ;  // arithmetic of the face terms (see face_der_xy)
   int i, j, k;
   if (!launch_ijk(P.nx, P.ny, P.nz, i, j, k)) return;
@@ -795,6 +798,7 @@ __global__ void __launch_bounds__(256, 3) k_jacobian_zm(DevProblem P, const doub
   FaceLH<TA> *sE = reinterpret_cast<FaceLH<TA> *>(jz_smem);  // [by][bx + 1]
   FaceLH<TA> *sN = sE + by * (bx + 1);                         // [by + 1][bx]
   pdl_enter();
+  if (P.dtp) dt = *P.dtp;
   const int i = blockIdx.x * bx + tx, j = blockIdx.y * by + ty;
   const int k0 = blockIdx.z * kchunk, k1 = min(P.nz, k0 + kchunk);
   const bool in = i < P.nx && j < P.ny;

@@ -180,6 +180,15 @@ class RichardsGPU:
     def _io(self, a):
         return a if hasattr(a, "data_ptr") else pad(a)
 
+    def solve_graph(self, mode: int = -1) -> int:
+        """Newton solves as one CUDA graph launch (mode 1, the default) or
+        host-driven (0); mode -1 returns 1 if the last solve ran as a graph."""
+        r = self.lib.pfgpu_solve_graph(self.h, int(mode))
+        if mode == -1:
+            return int(r)
+        L.check(r, "solve_graph")
+        return 0
+
     def set_evap_trans(self, et):
         """Per-cell land-surface sink/source [1/h] (interior (nz, ny, nx)), or
         None to clear it."""
