@@ -356,9 +356,14 @@ int pfgpu_get_pressure(pfgpu_handle *h, double *p);
 int pfgpu_advance(pfgpu_handle *h, double dt, int nsteps, pfgpu_stats *stats);
 
 /* Ensemble stepping: advances n independent problems (one handle each, same
- * semantics as pfgpu_advance, members[m] by dt[m]) concurrently, their
- * kernels overlapping on the GPU through the handles' own streams, driven by
- * nthreads host threads (0 = one per member).  stats (may be NULL) receives
+ * semantics as pfgpu_advance, members[m] by dt[m]) concurrently.  By default
+ * each timestep of all members is one CUDA graph launch holding every
+ * member's whole Newton solve with its own device-side control (members
+ * converge independently; a failed solve is retried with the halved dt for
+ * that member alone).  Where that does not apply (PFGPU_ENSEMBLE_GRAPH=0,
+ * host-driven solves, trajectory recording, members on several devices) the
+ * members run on their own streams, driven by nthreads host threads (0 = one
+ * per member).  stats (may be NULL) receives
  * n * nsteps entries, member-major; status[m] receives each member's
  * pfgpu_advance result.  Returns PFGPU_OK when every member succeeded,
  * otherwise the first error (or PFGPU_NOT_CONVERGED).  The members must be

@@ -1,16 +1,20 @@
 // Ensemble stepping: many independent Richards problems advanced at once.
 //
-// Each member is its own handle with its own non-blocking stream, its own
-// CUDA graph and its own device state, so the members' kernels are free to
-// overlap on the GPU: while one member's host loop waits on a Krylov scalar
-// or runs the launch-bound coarse multigrid levels, the others stream their
-// large-level kernels.  A pool of host threads drives the members' Newton
-// loops (KINSOL's control flow is host-driven, one thread per member at a
-// time); members are taken from a shared counter so uneven grids balance.
+// By default every timestep of all members is one CUDA graph launch: each
+// member's whole Newton solve, with its own device-side KINSOL/SPGMR control
+// (the member's convergence steers its own conditional nodes), is one root
+// branch of the graph, so the members' kernels overlap on the GPU and the
+// host waits once per timestep (ensemble_graph_advance in pfgpu.cu).  A
+// member whose solve fails is retried with the halved dt on its own.
 //
-// This is the ensemble configuration of the survey (48 members of uneven
-// size); the reference runs the members as separate processes one after
-// another.  No counterpart in the reference API.
+// Otherwise (PFGPU_ENSEMBLE_GRAPH=0, host-driven solves, trajectory
+// recording, members on several devices) a pool of host threads drives the
+// members' steps, each member on its own non-blocking stream; members are
+// taken from a shared counter so uneven grids balance.
+//
+// The workload is an ensemble of independent realisations (48 members of
+// uneven size); the reference runs such members as separate processes one
+// after another.  No counterpart in the reference API.
 #include <atomic>
 #include <string>
 #include <thread>
@@ -18,6 +22,16 @@
 
 #include "../../include/pfgpu.h"
 #include "pfgpu_kernels.h"
+
+namespace pfgpu {
+// Advances the ensemble members as pfgpu_ensemble_advance does, every
+// timestep of all members as one CUDA graph launch, when every member can
+// run its solve as a graph (same device, distinct handles, no trajectory
+// recording); *handled is false when it did nothing (the caller's
+// per-member path then runs).
+int ensemble_graph_advance(pfgpu_handle *const *members, int n, const double *dt, int nsteps,
+                           pfgpu_stats *stats, int *status, bool *handled);
+}  // namespace pfgpu
 
 extern "C" int pfgpu_ensemble_advance(pfgpu_handle *const *members, int n, const double *dt,
                                       int nsteps, int nthreads, pfgpu_stats *stats,
@@ -31,6 +45,10 @@ extern "C" int pfgpu_ensemble_advance(pfgpu_handle *const *members, int n, const
       pfgpu::record_error("pfgpu_ensemble_advance: null member or non-positive dt");
       return PFGPU_ERR_ARG;
     }
+  bool handled = false;
+  const int grc =
+      pfgpu::ensemble_graph_advance(members, n, dt, nsteps, stats, status, &handled);
+  if (handled) return grc;
   if (nthreads <= 0 || nthreads > n) nthreads = n;
   std::atomic<int> next{0};
   std::vector<std::string> msg(n);  // a failing member's message (thread-local there)

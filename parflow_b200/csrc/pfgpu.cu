@@ -18,6 +18,7 @@
 #include <cmath>
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <climits>
 #include <map>
 #include <mutex>
@@ -26,6 +27,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <type_traits>
 #include <vector>
 
@@ -152,6 +154,13 @@ struct pfgpu_handle {
   double *zface = nullptr;
   double *xcor = nullptr, *vtemp = nullptr;
   std::vector<double *> V;
+  // Mixed forms keep the preconditioned basis Z[l] = M^{-1} V[l] and form the
+  // correction as Z y: one V-cycle less per linear solve than M^{-1} (V y).
+  // Equal in exact arithmetic; the reduced-precision V-cycle is not exactly
+  // linear, so the two differ by its rounding.  The FP64 form follows SPGMR
+  // (M^{-1} (V y), spgmr.c:364-388) as the reference does.
+  bool zbasis = false;
+  std::vector<double *> Z;
   double *gs = nullptr;   // GMRES scalars
   double *dsc = nullptr;  // named device scalars
   double *hsc = nullptr;  // pinned host mirror of dsc / rho
@@ -222,17 +231,13 @@ struct pfgpu_handle {
     NkState *S = nullptr;   // device control state
     NkState *hS = nullptr;  // pinned host copy
     double *dt = nullptr, *hdt = nullptr;
-    cudaStream_t cs[6] = {};  // capture streams, one per nesting depth
+    std::vector<cudaStream_t> cs;  // capture streams, one per nesting depth
     long long kernels[NKB_COUNT] = {};
     std::vector<std::array<long long, 3>> stack;  // (body, launches at entry, nested)
-    // what the graph was captured for
-    unsigned char key_P[sizeof(DevProblem)] = {};
-    unsigned char key_d[sizeof(pfgpu_desc)] = {};
-    const double *key_u = nullptr, *key_unew = nullptr;
-    int key_usejac = -1;
-    double key_relfunc = 0.0;
+    std::vector<unsigned char> key;  // what the graph was captured for (nk_key)
     bool valid = false;
   } nk;
+  unsigned long long uid = 0;  // never reused: names the handle in ensemble graphs
 };
 
 // ---------------------------------------------------------------------------
@@ -666,10 +671,12 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
     for (l = 0; l < lmax; l++) {
       stats->lin_iters++;
       krydim = l + 1;
-      // vtemp = M^{-1} V[l] (the preconditioner reads V[l], writes vtemp)
-      if (pc_apply_dense(h, h->V[l], h->vtemp)) return PFGPU_ERR_CUDA;
+      // z = M^{-1} V[l] (the preconditioner reads V[l], writes z: vtemp, or
+      // the kept preconditioned basis vector Z[l])
+      double *z = h->zbasis ? h->Z[l] : h->vtemp;
+      if (pc_apply_dense(h, h->V[l], z)) return PFGPU_ERR_CUDA;
       stats->pc_solves++;
-      atimes(h, u, dt, h->vtemp, h->V[l + 1], stats);
+      atimes(h, u, dt, z, h->V[l + 1], stats);
       // ModifiedGS (iterativ.c:30-86): <vk,vk> and h(0) in one pass, then each
       // projection vk -= h(i) v_i fused with the next dot (h(i+1), or the
       // new <vk,vk> after the last); same per-element arithmetic
@@ -704,10 +711,14 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
       launch_scale_inv_dev(h->V[l + 1], Hp(l + 1, l), N, h->st);
       h->launches++;
     }
-    // QRsol and xcor (+)= V y
+    // QRsol and xcor (+)= V y; with the kept basis x (+)= Z y directly
     launch_gmres_scalar(GM_QRSOL, S, krydim, lmax, h->st);
-    launch_combine(h->xcor, h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st,
-                   ntries > 0 ? 1 : 0);
+    if (h->zbasis)
+      launch_combine(x, h->Z.data(), S + gs_yg_offset(lmax), krydim, N, h->st,
+                     ntries > 0 ? 1 : 0);
+    else
+      launch_combine(h->xcor, h->V.data(), S + gs_yg_offset(lmax), krydim, N, h->st,
+                     ntries > 0 ? 1 : 0);
     h->launches += 2;
     CK(cudaMemcpyAsync(h->hsc + D_COUNT, sc + SCI_QRFAIL, sizeof(double),
                        cudaMemcpyDeviceToHost, h->st));
@@ -719,8 +730,10 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
       return 0;
     }
     if (converged) {
-      if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;  // x = 0 + M^{-1} V y
-      stats->pc_solves++;
+      if (!h->zbasis) {
+        if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;  // x = 0 + M^{-1} V y
+        stats->pc_solves++;
+      }
       *status = 0;
       return 0;
     }
@@ -733,8 +746,10 @@ static int spgmr(pfgpu_handle *h, double *x, const double *src, double bsign,
     h->launches += 3;
   }
   if (rho < beta) {
-    if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;
-    stats->pc_solves++;
+    if (!h->zbasis) {
+      if (pc_apply_dense(h, h->xcor, x)) return PFGPU_ERR_CUDA;
+      stats->pc_solves++;
+    }
     *status = 1;
   } else {
     *status = 2;
@@ -1089,8 +1104,9 @@ static int nk_gmres_iter(pfgpu_handle *h, int l, double dt, NkConds &C) {
   double *sc = S + gs_sc_offset(lmax);
   auto Hp = [&](int i, int j) { return S + (long long)i * lmax + j; };
   pfgpu_stats dummy{};
-  if (pc_apply_dense_impl(h, h->V[l], h->vtemp)) return PFGPU_ERR_CUDA;
-  atimes(h, h->u, dt, h->vtemp, h->V[l + 1], &dummy);
+  double *z = h->zbasis ? h->Z[l] : h->vtemp;
+  if (pc_apply_dense_impl(h, h->V[l], z)) return PFGPU_ERR_CUDA;
+  atimes(h, h->u, dt, z, h->V[l + 1], &dummy);
   const int k = l + 1;
   launch_mgs_first(h->V[k], h->V[0], N, sc + SCI_VKNORM2, Hp(0, k - 1), h->rb, h->st);
   h->launches++;
@@ -1129,18 +1145,25 @@ static int nk_gmres_cycle(pfgpu_handle *h, double dt, NkConds &C) {
   launch_nk_cycle_begin(St, C, h->st);
   launch_v0_init(h->V[0], h->fval, St, sc, N, h->st);
   h->launches += 2;
+  // iteration l + 1 nests inside iteration l's body: once GMRES stops, no
+  // further conditional node is evaluated
+  std::function<int(int)> iteration = [&](int l) -> int {
+    const int rc = nk_gmres_iter(h, l, dt, C);
+    if (rc || l + 1 >= lmax) return rc;
+    return nk_body(h, C.iter[l + 1], cudaGraphCondTypeIf, 4 + l, NKB_GM0 + l + 1,
+                   [&]() { return iteration(l + 1); });
+  };
   nk_begin(h, NKB_GM0);
-  int rc = nk_gmres_iter(h, 0, dt, C);
+  int rc = iteration(0);
   nk_end(h);
   if (rc) return rc;
-  for (int l = 1; l < lmax; l++) {
-    rc = nk_body(h, C.iter[l], cudaGraphCondTypeIf, 3, NKB_GM0 + l,
-                 [&]() { return nk_gmres_iter(h, l, dt, C); });
-    if (rc) return rc;
-  }
   launch_gmres_scalar_dev(GM_QRSOL, S, &St->krydim, lmax, h->st);
-  launch_combine_dev(h->xcor, h->V.data(), lmax + 1, S + gs_yg_offset(lmax), &St->krydim,
-                     &St->accumulate, N, h->st);
+  if (h->zbasis)
+    launch_combine_dev(h->pp, h->Z.data(), lmax, S + gs_yg_offset(lmax), &St->krydim,
+                       &St->accumulate, N, h->st);
+  else
+    launch_combine_dev(h->xcor, h->V.data(), lmax + 1, S + gs_yg_offset(lmax), &St->krydim,
+                       &St->accumulate, N, h->st);
   launch_nk_cycle_end(St, sc, C, h->st);
   h->launches += 3;
   return nk_body(h, C.do_restart, cudaGraphCondTypeIf, 3, NKB_RESTART, [&]() {
@@ -1231,8 +1254,12 @@ static int nk_newton_iter(pfgpu_handle *h, double dt, NkConds &C) {
   launch_nk_after_gmres(St, C, h->st);
   h->launches++;
   rc = nk_body(h, C.post, cudaGraphCondTypeIf, 2, NKB_POST, [&]() {
-    if (pc_apply_dense_impl(h, h->xcor, h->pp)) return (int)PFGPU_ERR_CUDA;
-    launch_nk_count(St, NKB_POST, 1, h->st);
+    if (h->zbasis) {  // x = Z y is already formed
+      launch_nk_count(St, NKB_POST, 0, h->st);
+    } else {
+      if (pc_apply_dense_impl(h, h->xcor, h->pp)) return (int)PFGPU_ERR_CUDA;
+      launch_nk_count(St, NKB_POST, 1, h->st);
+    }
     h->launches++;
     return 0;
   });
@@ -1247,26 +1274,34 @@ static int nk_newton_iter(pfgpu_handle *h, double dt, NkConds &C) {
   return 0;
 }
 
-static void nk_key(pfgpu_handle *h, bool store, bool *same) {
-  pfgpu_handle::NkGraph &G = h->nk;
+// everything a captured solve bakes in: the problem's device description
+// (its dt pointer aside), the solver settings, the iterate buffers and the
+// Jacobian mode.  Copied bytewise: a spurious difference only costs a capture.
+static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   DevProblem P;
   memcpy(&P, &h->P, sizeof(P));
   P.dtp = nullptr;
-  if (store) {
-    memcpy(G.key_P, &P, sizeof(P));
-    memcpy(G.key_d, &h->d, sizeof(h->d));
-    G.key_u = h->u;
-    G.key_unew = h->unew;
-    G.key_usejac = h->use_jacobian;
-    G.key_relfunc = h->sqrt_relfunc;
-    return;
-  }
-  *same = memcmp(G.key_P, &P, sizeof(P)) == 0 && memcmp(G.key_d, &h->d, sizeof(h->d)) == 0 &&
-          G.key_u == h->u && G.key_unew == h->unew && G.key_usejac == h->use_jacobian &&
-          G.key_relfunc == h->sqrt_relfunc;
+  const double *ptrs[2] = {h->u, h->unew};
+  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + sizeof(int) +
+                               sizeof(double));
+  unsigned char *q = k.data();
+  memcpy(q, &P, sizeof(P));
+  q += sizeof(P);
+  memcpy(q, &h->d, sizeof(h->d));
+  q += sizeof(h->d);
+  memcpy(q, ptrs, sizeof(ptrs));
+  q += sizeof(ptrs);
+  memcpy(q, &h->use_jacobian, sizeof(int));
+  q += sizeof(int);
+  memcpy(q, &h->sqrt_relfunc, sizeof(double));
+  return k;
 }
 
-static int nk_capture(pfgpu_handle *h, cudaGraph_t *graph) {
+// Captures the solve into a new graph, or (target given) as one more root
+// branch of the ensemble graph `target`: there the branch also takes the
+// step's start (dt in, p_old = u, s_old = S(u)) and ends with the control
+// state and the error word copied to pinned host memory.
+static int nk_capture(pfgpu_handle *h, cudaGraph_t *graph, cudaGraph_t target) {
   pfgpu_handle::NkGraph &G = h->nk;
   const long long N = h->N;
   double *dsc = h->dsc;
@@ -1274,10 +1309,24 @@ static int nk_capture(pfgpu_handle *h, cudaGraph_t *graph) {
   for (auto &k : G.kernels) k = 0;
   G.stack.clear();
   cudaStream_t s0 = G.cs[0];
-  CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
+  if (target)
+    CK(cudaStreamBeginCaptureToGraph(s0, target, nullptr, nullptr, 0,
+                                     cudaStreamCaptureModeThreadLocal));
+  else
+    CK(cudaStreamBeginCapture(s0, cudaStreamCaptureModeThreadLocal));
   cudaStream_t saved = h->st;
   h->st = s0;
   int rc = nk_handle(s0, &C.newton);
+  if (!rc && target) {
+    if (cudaMemcpyAsync(G.dt, G.hdt, sizeof(double), cudaMemcpyHostToDevice, s0) !=
+            cudaSuccess ||
+        cudaMemcpyAsync(h->p_old, h->u, N * sizeof(double), cudaMemcpyDeviceToDevice, s0) !=
+            cudaSuccess) {
+      set_err("solve graph: copy capture failed: %s", cudaGetErrorString(cudaGetLastError()));
+      rc = PFGPU_ERR_CUDA;
+    }
+    launch_saturation(h->P, h->u, h->s_old, s0);
+  }
   if (!rc) {
     nk_begin(h, NKB_TOP);
     h->vg_for = nullptr;
@@ -1292,33 +1341,36 @@ static int nk_capture(pfgpu_handle *h, cudaGraph_t *graph) {
     h->launches++;
     nk_end(h);
   }
+  if (!rc && target &&
+      (cudaMemcpyAsync(G.hS, G.S, sizeof(NkState), cudaMemcpyDeviceToHost, s0) != cudaSuccess ||
+       cudaMemcpyAsync(h->hkerr, h->kerr, sizeof(int), cudaMemcpyDeviceToHost, s0) !=
+           cudaSuccess)) {
+    set_err("solve graph: copy capture failed: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = PFGPU_ERR_CUDA;
+  }
   h->st = saved;
-  *graph = nullptr;
-  const cudaError_t e = cudaStreamEndCapture(s0, graph);
+  cudaGraph_t out = nullptr;
+  const cudaError_t e = cudaStreamEndCapture(s0, &out);
+  if (graph) *graph = target ? nullptr : out;
   if (rc) {
-    if (*graph) cudaGraphDestroy(*graph);
-    *graph = nullptr;
+    if (out && !target) cudaGraphDestroy(out);
+    if (graph) *graph = nullptr;
     return rc;
   }
   CK(e);
   return 0;
 }
 
-// (re)builds the solve graph when what it was captured for has changed
-static int nk_prepare(pfgpu_handle *h) {
+// the solver constants on the device and the capture streams (once per handle)
+static int nk_setup(pfgpu_handle *h) {
   pfgpu_handle::NkGraph &G = h->nk;
-  if (G.valid) {
-    bool same = false;
-    nk_key(h, false, &same);
-    if (same) return 0;
-    CK(cudaGraphExecDestroy(G.exec));
-    G.exec = nullptr;
-    G.valid = false;
-  }
   if (!G.S) {
     if (dalloc(&G.S, 1) || dalloc(&G.dt, 1)) return PFGPU_ERR_CUDA;
     CK(cudaMallocHost(&G.hS, sizeof(NkState)));
     CK(cudaMallocHost(&G.hdt, sizeof(double)));
+    // depths: top, Newton body, GMRES cycle / line search, their bodies, and
+    // the nested GMRES iterations
+    G.cs.assign(h->d.krylov_dim + 6, nullptr);
     for (auto &s : G.cs) CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   }
   // constants of the solve (newton_impl's set-up)
@@ -1346,14 +1398,40 @@ static int nk_prepare(pfgpu_handle *h) {
   k.max_restarts = d.max_restarts;
   k.use_dq = h->use_jacobian ? 0 : 1;
   CK(cudaMemcpy(&G.S->k, &k, sizeof(k), cudaMemcpyHostToDevice));
+  return 0;
+}
 
+// nk_capture with the handle switched to capture mode (device dt, inline
+// V-cycles) and its host-side state restored afterwards
+static int nk_capture_guarded(pfgpu_handle *h, cudaGraph_t *graph, cudaGraph_t target) {
+  pfgpu_handle::NkGraph &G = h->nk;
   const DevProblem P0 = h->P;
   const long long launches0 = h->launches;
   const int jac0 = h->jac_valid;
   h->P.dtp = G.dt;
   G.capturing = true;
+  const int rc = nk_capture(h, graph, target);
+  G.capturing = false;
+  h->P = P0;
+  h->launches = launches0;
+  h->jac_valid = jac0;
+  h->vg_for = nullptr;
+  return rc;
+}
+
+// (re)builds the solve graph when what it was captured for has changed
+static int nk_prepare(pfgpu_handle *h) {
+  pfgpu_handle::NkGraph &G = h->nk;
+  if (G.valid) {
+    if (nk_key(h) == G.key) return 0;
+    CK(cudaGraphExecDestroy(G.exec));
+    G.exec = nullptr;
+    G.valid = false;
+  }
+  if (nk_setup(h)) return PFGPU_ERR_CUDA;
   cudaGraph_t graph = nullptr;
-  int rc = nk_capture(h, &graph);
+  bool pdl_used = pdl_on();
+  int rc = nk_capture_guarded(h, &graph, nullptr);
   cudaGraphExec_t exec = nullptr;
   if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
     // programmatic launches inside conditional bodies are what a driver may
@@ -1363,7 +1441,8 @@ static int nk_prepare(pfgpu_handle *h) {
     graph = nullptr;
     exec = nullptr;
     pdl_capture_off() = true;
-    rc = nk_capture(h, &graph);
+    pdl_used = false;
+    rc = nk_capture_guarded(h, &graph, nullptr);
     pdl_capture_off() = false;
     if (!rc && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
       set_err("solve graph: instantiation failed: %s", cudaGetErrorString(cudaGetLastError()));
@@ -1372,16 +1451,17 @@ static int nk_prepare(pfgpu_handle *h) {
     }
   }
   if (graph) cudaGraphDestroy(graph);
-  G.capturing = false;
-  h->P = P0;
-  h->launches = launches0;
-  h->jac_valid = jac0;
-  h->vg_for = nullptr;
   if (rc) return rc;
   CK(cudaGraphUpload(exec, h->st));
   G.exec = exec;
   G.valid = true;
-  nk_key(h, true, nullptr);
+  G.key = nk_key(h);
+  if (env_ll("PFGPU_GRAPH_INFO", 0)) {
+    long long nk = 0;
+    for (long long c : G.kernels) nk += c;
+    fprintf(stderr, "pfgpu solve graph (%dx%dx%d): %lld kernel nodes, programmatic launches %s\n",
+            h->nx, h->ny, h->nz, nk, pdl_used ? "on" : "off");
+  }
   return 0;
 }
 
@@ -1682,6 +1762,11 @@ static int create_impl(pfgpu_handle *h) {
   h->V.resize(d.krylov_dim + 1);
   for (auto &v : h->V)
     if (dalloc(&v, N)) return PFGPU_ERR_NOMEM;
+  if (h->zbasis) {
+    h->Z.resize(d.krylov_dim);
+    for (auto &v : h->Z)
+      if (dalloc(&v, N)) return PFGPU_ERR_NOMEM;
+  }
   if (dalloc(&h->gs, gs_size(d.krylov_dim)) || dalloc(&h->dsc, 64) ||
       dalloc(&h->stage, h->NP) || dalloc(&h->rb.partial, reduce_partials()))
     return PFGPU_ERR_NOMEM;
@@ -1734,9 +1819,228 @@ static int create_impl(pfgpu_handle *h) {
   return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Ensemble timesteps as one graph launch.  Every member's step (dt in, old
+// state, the whole Newton solve with its own device-side control, the control
+// state back to pinned memory) is a root branch of one graph, so one launch
+// advances all members and each converges on its own.  A member whose solve
+// fails is retried host-side with the halved dt, as pfgpu_advance does.
+// Graphs are kept per member set (named by the handles' uids) and rebuilt
+// when a member's captured solve no longer matches it.
+// ---------------------------------------------------------------------------
+namespace {
+struct EnsembleGraph {
+  std::vector<unsigned long long> uids;
+  std::vector<std::vector<unsigned char>> keys;
+  cudaGraphExec_t exec = nullptr;
+  cudaStream_t st = nullptr;
+  int device = 0;
+};
+std::mutex g_ens_mu;
+std::vector<EnsembleGraph *> g_ens;
+std::atomic<unsigned long long> g_uid{1};
+
+void ens_free(EnsembleGraph *E) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  cudaSetDevice(E->device);
+  if (E->exec) cudaGraphExecDestroy(E->exec);
+  if (E->st) cudaStreamDestroy(E->st);
+  cudaSetDevice(cur);
+  delete E;
+}
+}  // namespace
+
+// drops every ensemble graph that holds the handle
+static void ens_forget(unsigned long long uid) {
+  std::lock_guard<std::mutex> lk(g_ens_mu);
+  for (size_t i = 0; i < g_ens.size();) {
+    const auto &u = g_ens[i]->uids;
+    if (std::find(u.begin(), u.end(), uid) != u.end()) {
+      ens_free(g_ens[i]);
+      g_ens.erase(g_ens.begin() + (long)i);
+    } else {
+      i++;
+    }
+  }
+}
+
+static int ens_build(pfgpu_handle *const *members, int n, EnsembleGraph *E) {
+  for (int attempt = 0; attempt < 2; attempt++) {
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    pdl_capture_off() = attempt == 1;
+    int rc = 0;
+    for (int m = 0; m < n && !rc; m++) rc = nk_capture_guarded(members[m], nullptr, g);
+    pdl_capture_off() = false;
+    if (!rc && cudaGraphInstantiate(&E->exec, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      E->exec = nullptr;
+      rc = PFGPU_ERR_CUDA;
+      set_err("ensemble graph: instantiation failed");
+    }
+    cudaGraphDestroy(g);
+    if (!rc) {
+      CK(cudaGraphUpload(E->exec, E->st));
+      return 0;
+    }
+    if (attempt == 1) return rc;
+  }
+  return PFGPU_ERR_CUDA;
+}
+
+namespace pfgpu {
+int ensemble_graph_advance(pfgpu_handle *const *members, int n, const double *dt, int nsteps,
+                           pfgpu_stats *stats, int *status, bool *handled);
+}
+int pfgpu::ensemble_graph_advance(pfgpu_handle *const *members, int n, const double *dt,
+                                  int nsteps, pfgpu_stats *stats, int *status, bool *handled) {
+  *handled = false;
+  static const bool on = env_ll("PFGPU_ENSEMBLE_GRAPH", 1) != 0;
+  if (!on || n < 1) return PFGPU_OK;
+  const int dev = members[0]->device;
+  for (int m = 0; m < n; m++) {
+    pfgpu_handle *h = members[m];
+    if (!nk_usable(h) || h->recording || h->device != dev) return PFGPU_OK;
+    for (int q = 0; q < m; q++)
+      if (members[q] == h) return PFGPU_OK;
+  }
+  CK(cudaSetDevice(dev));
+  for (int m = 0; m < n; m++)
+    if (nk_prepare(members[m]) != PFGPU_OK) return PFGPU_OK;  // the per-member path decides
+  std::vector<unsigned long long> uids(n);
+  std::vector<std::vector<unsigned char>> keys(n);
+  for (int m = 0; m < n; m++) {
+    uids[m] = members[m]->uid;
+    keys[m] = nk_key(members[m]);
+  }
+  EnsembleGraph *E = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_ens_mu);
+    for (size_t i = 0; i < g_ens.size(); i++)
+      if (g_ens[i]->uids == uids) {
+        E = g_ens[i];
+        g_ens.erase(g_ens.begin() + (long)i);
+        break;
+      }
+  }
+  if (E && E->keys != keys) {
+    ens_free(E);
+    E = nullptr;
+  }
+  if (!E) {
+    E = new EnsembleGraph();
+    E->uids = uids;
+    E->keys = keys;
+    E->device = dev;
+    if (cudaStreamCreateWithFlags(&E->st, cudaStreamNonBlocking) != cudaSuccess ||
+        ens_build(members, n, E) != 0) {
+      cudaGetLastError();
+      ens_free(E);
+      return PFGPU_OK;  // not handled: the per-member path runs
+    }
+  }
+  {
+    std::lock_guard<std::mutex> lk(g_ens_mu);
+    g_ens.push_back(E);
+  }
+  *handled = true;
+  for (int m = 0; m < n; m++) status[m] = PFGPU_OK;
+  static const double limit = (double)env_ll("PFGPU_SOLVE_TIMEOUT_S", 600);
+  std::vector<char> done(n, 0);  // member stopped (failed step or error)
+  bool all = true;               // every member still in the graph
+  for (int s = 0; s < nsteps; s++) {
+    if (!all) {
+      // a member stopped: the rest finish on the per-member path
+      for (int m = 0; m < n; m++) {
+        if (done[m]) continue;
+        pfgpu_stats st{};
+        const int rc = pfgpu_advance(members[m], dt[m], 1, &st);
+        if (stats) stats[(size_t)m * nsteps + s] = st;
+        if (rc != PFGPU_OK) {
+          status[m] = rc;
+          done[m] = 1;
+        }
+      }
+      continue;
+    }
+    for (int m = 0; m < n; m++) {
+      *members[m]->nk.hdt = dt[m];
+      CK(cudaStreamSynchronize(members[m]->st));  // the member's earlier work
+    }
+    CK(cudaGraphLaunch(E->exec, E->st));
+    const auto t0 = std::chrono::steady_clock::now();
+    for (;;) {
+      const cudaError_t q = cudaStreamQuery(E->st);
+      if (q == cudaSuccess) break;
+      if (q != cudaErrorNotReady) CK(q);
+      if (std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count() > limit) {
+        set_err("ensemble graph did not finish within %.0f s", limit);
+        return PFGPU_ERR_STATE;
+      }
+    }
+    for (int m = 0; m < n; m++) {
+      pfgpu_handle *h = members[m];
+      const NkState &S = *h->nk.hS;
+      long long k = 1;  // the saturation of the step's start
+      for (int b = 0; b < NKB_COUNT; b++) k += h->nk.kernels[b] * (long long)S.execs[b];
+      h->launches += k;
+      h->vg_for = nullptr;
+      h->jac_valid = 0;
+      h->nk.used_last = true;
+      pfgpu_stats st{};
+      st.nonlin_iters = S.nonlin_iters;
+      st.lin_iters = S.lin_iters;
+      st.fevals = S.fevals;
+      st.pc_setups = S.pc_setups;
+      st.pc_solves = S.pc_solves;
+      st.lin_conv_fails = S.lin_conv_fails;
+      st.beta_cond_fails = S.beta_cond_fails;
+      st.backtracks = S.backtracks;
+      st.kinsol_status = S.kinsol_status;
+      st.fnorm = S.fnorm;
+      int rc = S.err ? PFGPU_ERR_STATE
+                     : (S.kinsol_status == 1 || S.kinsol_status == 2) ? PFGPU_OK
+                                                                      : PFGPU_NOT_CONVERGED;
+      if (S.err) set_err("line search exceeded its iteration bound");
+      if (rc >= 0 && *h->hkerr) rc = check_kernel_error(h) ? PFGPU_ERR_CUDA : rc;
+      // failed solves: the retries of pfgpu_advance (u back to p_old, dt halved)
+      // as pfgpu_advance: after every failed attempt u goes back to p_old
+      // and dt is halved; at most three attempts
+      double dts = dt[m];
+      for (int fail = 1; rc == PFGPU_NOT_CONVERGED; fail++) {
+        CK(cudaMemcpyAsync(h->u, h->p_old, h->N * sizeof(double), cudaMemcpyDeviceToDevice,
+                           h->st));
+        h->vg_for = nullptr;
+        dts *= 0.5;
+        if (fail == 3) break;
+        rc = newton(h, dts, &st);
+        if (rc >= 0 && check_kernel_error(h)) rc = PFGPU_ERR_CUDA;
+      }
+      if (stats) stats[(size_t)m * nsteps + s] = st;
+      if (rc == PFGPU_NOT_CONVERGED)
+        set_err("pfgpu_advance: time step %d failed after 3 convergence failures", s);
+      if (rc != PFGPU_OK) {
+        status[m] = rc;
+        done[m] = 1;
+        all = false;
+      }
+    }
+  }
+  for (int m = 0; m < n; m++) CK(cudaStreamSynchronize(members[m]->st));
+  int rc = PFGPU_OK;
+  for (int m = 0; m < n; m++) {
+    if (status[m] == PFGPU_OK) continue;
+    if (status[m] < 0 && rc >= 0) rc = status[m];
+    else if (rc == PFGPU_OK) rc = PFGPU_NOT_CONVERGED;
+  }
+  return rc;
+}
+
 static void destroy_impl(pfgpu_handle *h) {
   if (!h) return;
   cudaSetDevice(h->device);
+  ens_forget(h->uid);
   if (h->st) cudaStreamSynchronize(h->st);
   if (h->ptime && h->pcnt[PH_NEWTON] > 0) {
     fprintf(stderr, "pfgpu phase times (%lldx%lldx%lld, %s): device ms summed over %lld solves\n",
@@ -1774,6 +2078,7 @@ static void destroy_impl(pfgpu_handle *h) {
   for (int f = 0; f < 6; f++) cudaFree(h->bcv[f]);
   for (int f = 0; f < 6; f++) cudaFree(h->cyc[f].table);
   for (auto v : h->V) cudaFree(v);
+  for (auto v : h->Z) cudaFree(v);
   cudaFree(h->rb.ticket);
   cudaFree(h->kerr);
   if (h->hkerr) cudaFreeHost(h->hkerr);
@@ -1835,6 +2140,7 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
     return nullptr;
   }
   pfgpu_handle *h = new pfgpu_handle();
+  h->uid = g_uid.fetch_add(1);
   h->d = *desc;
   h->d.z_mult = nullptr;
   h->device = device;
@@ -1844,7 +2150,13 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
   h->mixed = desc->precision == PFGPU_PREC_MIXED || desc->precision == PFGPU_PREC_MIXED_H16;
   h->h16 = desc->precision == PFGPU_PREC_MIXED_H16;
   h->ptime = env_ll("PFGPU_PHASE_TIMES", 0) != 0;
-  h->nk.enabled = env_ll("PFGPU_SOLVE_GRAPH", 0) != 0;
+  h->nk.enabled = env_ll("PFGPU_SOLVE_GRAPH", 1) != 0;
+  {
+    // PFGPU_PC_BASIS: 0 never keeps the preconditioned basis, 1 (default) in
+    // the mixed forms, 2 in every form
+    const long long zb = env_ll("PFGPU_PC_BASIS", 1);
+    h->zbasis = zb >= 2 || (zb == 1 && h->mixed);
+  }
   if (create_impl(h) != 0) {
     destroy_impl(h);
     delete h;

@@ -361,4 +361,5 @@ void launch_adj_grad(const DevProblem &P, const double *p, const double *p_prev,
 // sets the message pfgpu_last_error returns on this thread
 void record_error(const char *msg);
 
+
 }  // namespace pfgpu
