@@ -355,6 +355,13 @@ def gpu_arm(args, rank, world, local_rank):
     s64.close()
     s32, ms32, _, _, _, p32 = timed_run("mixed")
     s32.close()
+    # the FP64 form with the mixed forms' kept preconditioned basis (x = Z y
+    # instead of M^{-1} (V y)): separates that saving from the precision's
+    os.environ["PFGPU_PC_BASIS"] = "2"
+    s64z, ms64z, st64z, _, _, p64z = timed_run("fp64")
+    s64z.close()
+    del os.environ["PFGPU_PC_BASIS"]
+    rel_err64z = float(np.abs(p64z - p64).max() / np.abs(p64).max())
     smx, msmx, stmx, launches, clocks, pmx = timed_run(HEADLINE)
     rel_err = float(np.abs(pmx - p64).max() / np.abs(p64).max())
     rel_err32 = float(np.abs(p32 - p64).max() / np.abs(p64).max())
@@ -451,6 +458,10 @@ def gpu_arm(args, rank, world, local_rank):
             "mixed_vs_fp64_max_rel_pressure_err": rel_err,
             "mixed_fp32_mg_steps_per_s": job_throughput(args.steps, world, ms32),
             "mixed_fp32_mg_vs_fp64_max_rel_pressure_err": rel_err32,
+            "fp64_kept_basis_steps_per_s": job_throughput(args.steps, world, ms64z),
+            "fp64_kept_basis_vs_fp64_max_rel_pressure_err": rel_err64z,
+            "solve": "one CUDA graph launch per Newton solve (device-side KINSOL/SPGMR "
+                     "control); mixed forms keep the preconditioned Krylov basis (x = Z y)",
             "newton_iters_per_step": newton / max(1, len(stmx)),
             "gmres_iters_per_step": sum(x.lin_iters for x in stmx) / max(1, len(stmx)),
             "cell_newton_updates_per_s": cells * newton * world / (msmx * 1e-3),
@@ -561,6 +572,10 @@ def ensemble_arm(args, rank, world, local_rank):
             "config": {"workload": "ensemble of 48 boxes, nx=ny in {64,96,128,192}, "
                                    "nz in {16,24,32,40}, 24.3M cells total",
                        "cells": sum(cells), "dt_h": 0.1},
+            "mode": ("one CUDA graph launch per ensemble timestep (every member's Newton solve "
+                     "with its own device-side control)"
+                     if os.environ.get("PFGPU_ENSEMBLE_GRAPH", "1") != "0" else
+                     "host thread per member"),
             "sequential_member_timesteps_per_s": member_steps / (t_seq * 1e-3),
             "concurrency_speedup": t_seq / t_conc,
             "heuristic_shapes_member_timesteps_per_s": member_steps / (t_heur * 1e-3),
