@@ -236,6 +236,14 @@ struct pfgpu_handle {
     std::vector<std::array<long long, 3>> stack;  // (body, launches at entry, nested)
     std::vector<unsigned char> key;  // what the graph was captured for (nk_key)
     bool valid = false;
+    // earlier graphs of the handle (a time cycle switches between a few
+    // boundary tables): most recent last
+    struct Kept {
+      std::vector<unsigned char> key;
+      cudaGraphExec_t exec;
+      std::array<long long, NKB_COUNT> kernels;
+    };
+    std::vector<Kept> kept;
   } nk;
   unsigned long long uid = 0;  // never reused: names the handle in ensemble graphs
 };
@@ -1422,11 +1430,28 @@ static int nk_capture_guarded(pfgpu_handle *h, cudaGraph_t *graph, cudaGraph_t t
 // (re)builds the solve graph when what it was captured for has changed
 static int nk_prepare(pfgpu_handle *h) {
   pfgpu_handle::NkGraph &G = h->nk;
+  std::vector<unsigned char> key = nk_key(h);
   if (G.valid) {
-    if (nk_key(h) == G.key) return 0;
-    CK(cudaGraphExecDestroy(G.exec));
+    if (key == G.key) return 0;
+    pfgpu_handle::NkGraph::Kept old{std::move(G.key), G.exec, {}};
+    std::copy(std::begin(G.kernels), std::end(G.kernels), old.kernels.begin());
+    G.kept.push_back(std::move(old));
     G.exec = nullptr;
     G.valid = false;
+    for (size_t i = 0; i < G.kept.size(); i++)
+      if (G.kept[i].key == key) {
+        G.exec = G.kept[i].exec;
+        G.key = std::move(G.kept[i].key);
+        std::copy(G.kept[i].kernels.begin(), G.kept[i].kernels.end(), std::begin(G.kernels));
+        G.kept.erase(G.kept.begin() + (long)i);
+        G.valid = true;
+        return 0;
+      }
+    constexpr size_t KEEP = 4;
+    while (G.kept.size() > KEEP) {
+      cudaGraphExecDestroy(G.kept.front().exec);
+      G.kept.erase(G.kept.begin());
+    }
   }
   if (nk_setup(h)) return PFGPU_ERR_CUDA;
   cudaGraph_t graph = nullptr;
@@ -2059,6 +2084,7 @@ static void destroy_impl(pfgpu_handle *h) {
   cudaFree(h->vstage);
   if (h->vgraph) cudaGraphExecDestroy(h->vgraph);
   if (h->nk.exec) cudaGraphExecDestroy(h->nk.exec);
+  for (auto &kv : h->nk.kept) cudaGraphExecDestroy(kv.exec);
   cudaFree(h->nk.S);
   cudaFree(h->nk.dt);
   if (h->nk.hS) cudaFreeHost(h->nk.hS);
