@@ -367,9 +367,10 @@ def gpu_arm(args, rank, world, local_rank):
     rel_err32 = float(np.abs(p32 - p64).max() / np.abs(p64).max())
 
     # roofline of the dominant kernel: k_rb_sweep, one red/black colour sweep
-    # (35% of a timestep's GPU time in the launch list); timed on the finest
-    # level, 13.1M cells, 18 algorithmic bytes per cell (FP16 scaled operator
-    # 6 B, b 4 B, x read and written 4 + 4 B)
+    # (27% of a timestep's GPU time in the launch list); timed on the finest
+    # level, 13.1M cells, 12 algorithmic bytes per cell of the level (the
+    # FP16 scaled operator 6 B; this colour's b 2 B, the other colour's x
+    # read 2 B and this colour's x written 2 B: FP32 values of half the cells)
     kern = {}
     for name in ("colour_sweep", "rb_smooth", "matvec", "residual", "jacobian", "vcycle",
                  "mg_setup"):
