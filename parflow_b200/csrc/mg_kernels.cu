@@ -851,7 +851,7 @@ __device__ __forceinline__ void prolong_add_cell(const MGLevel<T> &F, const MGLe
 template <typename T, bool H, int D>
 __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
                                                      const T *__restrict__ ec,
-                                                     T *__restrict__ xf, int flip) {
+                                                     T *__restrict__ xf, int flip, int skip_red) {
   pdl_enter();
   const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -859,6 +859,9 @@ __global__ void __launch_bounds__(256) k_prolong_add(MGLevel<T> F, MGLevel<T> C,
   const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
   const int nx = F.nx, ny = F.ny;
   if (i >= nx || j >= ny) return;
+  // a red/black post-smoother starts with a red sweep, which overwrites the
+  // red cells without reading them: only the black cells need the correction
+  if (skip_red && ((i + j + k) & 1)) return;
   const int c = i + nx * (j + ny * k);
   const int cd = D == 0 ? i : D == 1 ? j : k;
   const int nd = D == 0 ? nx : D == 1 ? ny : F.nz;
@@ -1533,14 +1536,17 @@ static void restrict_d(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T 
 }
 template <typename T, bool H>
 static void prolong_d(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
-                      cudaStream_t st, int flip) {
+                      cudaStream_t st, int flip, int skip_red) {
   Shape3 g = shape3(F.nx, F.ny, F.nz);
   if (F.dir == 0)
-    launch_pdl(k_prolong_add<T, H, 0>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+    launch_pdl(k_prolong_add<T, H, 0>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip,
+               skip_red);
   else if (F.dir == 1)
-    launch_pdl(k_prolong_add<T, H, 1>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+    launch_pdl(k_prolong_add<T, H, 1>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip,
+               skip_red);
   else
-    launch_pdl(k_prolong_add<T, H, 2>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip);
+    launch_pdl(k_prolong_add<T, H, 2>, dim3(g.grid), dim3(g.block), st, F, C, ec, xf, flip,
+               skip_red);
 }
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
@@ -1555,14 +1561,14 @@ void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T
 }
 template <typename T>
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
-                           cudaStream_t st, int flip, bool h16) {
+                           cudaStream_t st, int flip, bool h16, int skip_red) {
   if constexpr (kHasH16<T>) {
     if (h16) {
-      prolong_d<T, true>(F, C, ec, xf, st, flip);
+      prolong_d<T, true>(F, C, ec, xf, st, flip, skip_red);
       return;
     }
   }
-  prolong_d<T, false>(F, C, ec, xf, st, flip);
+  prolong_d<T, false>(F, C, ec, xf, st, flip, skip_red);
 }
 template <typename T>
 void launch_vcycle_tail(const MGLevel<T> *levels_dev, int first, int nl, int smoother,
@@ -1868,7 +1874,7 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
   template void launch_mg_restrict<T>(const MGLevel<T> &, const MGLevel<T> &, const T *, T *, \
                                       cudaStream_t, int, bool);                               \
   template void launch_mg_prolong_add<T>(const MGLevel<T> &, const MGLevel<T> &, const T *,   \
-                                         T *, cudaStream_t, int, bool);                       \
+                                         T *, cudaStream_t, int, bool, int);                  \
   template void launch_vcycle_mid<T>(const MGLevel<T> *, int, int, int, int, double, T *,       \
                                      size_t, int, cudaStream_t, bool);                         \
   template int vcycle_mid_cluster_size<T>(bool, size_t);                                       \

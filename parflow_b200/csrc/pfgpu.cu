@@ -513,7 +513,10 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   for (int l = first - 1; l >= 0; l--) {
     MGLevel<T> &Ll = mg.L[l];
     const MGLevel<T> &C = mg.L[l + 1];
-    launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st, next(), mg.h16);
+    // the plain red/black post-smoothers begin with a red sweep
+    const int skip_red = (smoother == PFGPU_SMOOTH_RBGS || smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
+                         !mg.fused[l] && !mg.waved[l];
+    launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st, next(), mg.h16, skip_red);
     if (mg.fused[l]) {
       launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x2, 0, mg.kerr, st);
       k += 2;

@@ -188,8 +188,9 @@ template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
                         cudaStream_t st, int flip = 0, bool h16 = false);
 template <typename T>
+// xf += P ec; skip_red: only the black cells (the next sweep is a red one)
 void launch_mg_prolong_add(const MGLevel<T> &F, const MGLevel<T> &C, const T *ec, T *xf,
-                           cudaStream_t st, int flip = 0, bool h16 = false);
+                           cudaStream_t st, int flip = 0, bool h16 = false, int skip_red = 0);
 // scaled FP16 operator of level F from its FP32 operator and the diagonal of
 // the next coarser level C (null on the coarsest); sets *F.hflag when a
 // scaled diagonal is not +1 (the flag is cleared before the first level)
