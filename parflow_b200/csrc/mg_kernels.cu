@@ -707,17 +707,11 @@ __device__ __forceinline__ void mg_residual_cell(const MGLevel<T> &Lv, const T *
 }
 
 // grid form of mg_residual_cell (same operation order, lean indices)
+// r = b - A x of one cell (the grid residual kernels' shared arithmetic)
 template <typename T, bool H>
-__global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__restrict__ x,
-                                                     const T *__restrict__ b,
-                                                     T *__restrict__ r, int flip) {
-  pdl_enter();
-  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = by * blockDim.y + threadIdx.y;
-  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+__device__ __forceinline__ T mg_residual_cell(const MGLevel<T> &L, const T *__restrict__ x,
+                                              const T *__restrict__ b, int i, int j, int k) {
   const int nx = L.nx, ny = L.ny, nz = L.nz;
-  if (i >= nx || j >= ny) return;
   const int sy = nx, sz = nx * ny;
   const int c = i + sy * j + sz * k;
   const bool hw = i > 0, he = i + 1 < nx, hs = j > 0, hn = j + 1 < ny, hl = k > 0,
@@ -758,7 +752,45 @@ __global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__re
   y += cn * (hn ? ldro(x + xn) : T(0));
   y += cl * (hl ? ldro(x + xl) : T(0));
   y += cu * (hu ? ldro(x + xu) : T(0));
-  r[c] = -y;
+  return -y;
+}
+
+template <typename T, bool H>
+__global__ void __launch_bounds__(256) k_mg_residual(MGLevel<T> L, const T *__restrict__ x,
+                                                     const T *__restrict__ b,
+                                                     T *__restrict__ r, int flip) {
+  pdl_enter();
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  if (i >= L.nx || j >= L.ny) return;
+  r[i + L.nx * (j + L.ny * k)] = mg_residual_cell<T, H>(L, x, b, i, j, k);
+}
+
+// The residual right after a red/black sweep of colour zc: the cells of that
+// colour were just solved against their current neighbours, so their
+// residual is zero up to rounding and is written as zero; one thread per
+// pair of cells (i, i+1) of a row, one of each colour, computes the other
+// cell's residual as k_mg_residual does.
+template <typename T, bool H>
+__global__ void __launch_bounds__(256) k_mg_residual_pair(MGLevel<T> L, const T *__restrict__ x,
+                                                          const T *__restrict__ b,
+                                                          T *__restrict__ r, int flip, int zc) {
+  pdl_enter();
+  const int by = flip ? gridDim.y - 1 - blockIdx.y : blockIdx.y;
+  const int i0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
+  const int j = by * blockDim.y + threadIdx.y;
+  const int k = flip ? gridDim.z - 1 - blockIdx.z : blockIdx.z;
+  const int nx = L.nx;
+  if (i0 >= nx || j >= L.ny) return;
+  // colour 0 (red) is parity 1 of i + j + k
+  const int zpar = zc == 0 ? 1 : 0;
+  const int iz = ((i0 + j + k) & 1) == zpar ? i0 : i0 + 1;  // the zero-residual cell
+  const int ic = iz == i0 ? i0 + 1 : i0;                     // the computed cell
+  const int row = nx * (j + L.ny * k);
+  if (iz < nx) r[iz + row] = T(0);
+  if (ic < nx) r[ic + row] = mg_residual_cell<T, H>(L, x, b, ic, j, k);
 }
 
 // r_c = r_f(c) + (p2(f-1) r_f(f-1) + p1(f+1) r_f(f+1)) (mg_semi_restrict.c:161-169)
@@ -1035,7 +1067,11 @@ __device__ __forceinline__ void team_down(const MGLevel<T> &L, const MGLevel<T> 
   for (int t = r0; t < (int)L.n; t += rs) {
     int i, j, k;
     split_ijk(t, fx, fy, i, j, k);
-    mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
+    // the colour swept last (red: (i+j+k) odd) has a zero residual
+    if (L.zc >= 0 && (((i + j + k) & 1) == (L.zc == 0 ? 1 : 0)))
+      L.t[t] = T(0);
+    else
+      mg_residual_cell<T, H>(L, (const T *)L.x, (const T *)L.b, L.t, i, j, k);
   }
   Team::sync();
   const FastDiv cx = fast_div(C.nx), cy = fast_div(C.ny);
@@ -1513,7 +1549,20 @@ int vcycle_mid_cluster_size(bool h16, size_t smem) {
 
 template <typename T>
 void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st,
-                        int flip, bool h16) {
+                        int flip, bool h16, int zero_colour) {
+  if (zero_colour >= 0) {
+    Shape3 g = shape3((L.nx + 1) / 2, L.ny, L.nz);
+    if constexpr (kHasH16<T>) {
+      if (h16) {
+        launch_pdl(k_mg_residual_pair<T, true>, dim3(g.grid), dim3(g.block), st, L, x, b, r,
+                   flip, zero_colour);
+        return;
+      }
+    }
+    launch_pdl(k_mg_residual_pair<T, false>, dim3(g.grid), dim3(g.block), st, L, x, b, r, flip,
+               zero_colour);
+    return;
+  }
   Shape3 g = shape3(L.nx, L.ny, L.nz);
   if constexpr (kHasH16<T>) {
     if (h16) {
@@ -1870,7 +1919,7 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
   template void launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *, \
                                     cudaStream_t, int *, bool);                               \
   template void launch_mg_residual<T>(const MGLevel<T> &, const T *, const T *, T *,          \
-                                      cudaStream_t, int, bool);                               \
+                                      cudaStream_t, int, bool, int);                          \
   template void launch_mg_restrict<T>(const MGLevel<T> &, const MGLevel<T> &, const T *, T *, \
                                       cudaStream_t, int, bool);                               \
   template void launch_mg_prolong_add<T>(const MGLevel<T> &, const MGLevel<T> &, const T *,   \

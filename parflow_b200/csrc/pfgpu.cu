@@ -489,7 +489,9 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
       launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st, fp, mg.h16);
       k += sk;
     }
-    launch_mg_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st, next(), mg.h16);
+    // after the plain red/black pre-smoother the colour swept last (red, or
+    // black for the non-symmetric order) has a zero residual up to rounding
+    launch_mg_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st, next(), mg.h16, Ll.zc);
     launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st, next(), mg.h16);
     k += 2;
   }
@@ -1726,6 +1728,18 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
       return PFGPU_ERR_CUDA;
     }
     mg.waved[l] = 1;
+  }
+  // the residual after the pre-smoother: the colour swept last is solved
+  // against its current neighbours, its residual zero up to rounding
+  // (PFGPU_PAIR_RESIDUAL=0 computes it anyway)
+  const bool pair = env_ll("PFGPU_PAIR_RESIDUAL", 1) != 0;
+  for (int l = 0; l < nl; l++) {
+    const int sm = h->d.mg_smoother;
+    // (the fused and wavefront smoothers run the same red/black/red sweeps)
+    mg.L[l].zc = !pair                           ? -1
+                 : sm == PFGPU_SMOOTH_RBGS        ? 0
+                 : sm == PFGPU_SMOOTH_RBGS_NONSYM ? 1
+                                                  : -1;
   }
   mg.kerr = h->kerr;
   CK(cudaMalloc((void **)&mg.Ldev, nl * sizeof(MGLevel<T>)));

@@ -83,6 +83,10 @@ struct MGLevel {
   // colour sweep reads and writes whole lines of one colour only
   int split;
   int hx;
+  // colour whose residual is written as zero right after the pre-smoother
+  // (the colour it swept last: 0 red for red/black/red, 1 black for
+  // red/black), or -1: every cell's residual is computed
+  int zc;
 };
 
 // storage index of cell (i,j,k) in a level's x / b arrays
@@ -182,8 +186,10 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
 cudaError_t mg_prepare_kernels();
 // h16: the level's scaled FP16 operator and weights (float levels only)
 template <typename T>
+// r = b - A x; zero_colour >= 0: right after a sweep of that colour, whose
+// cells' residual is written as zero
 void launch_mg_residual(const MGLevel<T> &L, const T *x, const T *b, T *r, cudaStream_t st,
-                        int flip = 0, bool h16 = false);
+                        int flip = 0, bool h16 = false, int zero_colour = -1);
 template <typename T>
 void launch_mg_restrict(const MGLevel<T> &F, const MGLevel<T> &C, const T *rf, T *rc,
                         cudaStream_t st, int flip = 0, bool h16 = false);
