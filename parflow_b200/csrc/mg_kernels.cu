@@ -271,6 +271,16 @@ static bool getenv_flag_one_cell() {
   return v;
 }
 
+// PFGPU_SKIP_ZERO_SWEEP=0: launch the zero-guess red sweep of the
+// pre-smoother even where the black sweep can read its values from b (A/B)
+static bool skip_zero_sweep() {
+  static const bool v = [] {
+    const char *e = getenv("PFGPU_SKIP_ZERO_SWEEP");
+    return !(e && *e == '0');
+  }();
+  return v;
+}
+
 // H-mode kernels exist for float storage only
 template <typename T>
 constexpr bool kHasH16 = std::is_same<T, float>::value;
@@ -560,7 +570,10 @@ __global__ void __launch_bounds__(256) k_rb_sweep(MGLevel<T> L, T *__restrict__ 
 // block) share the row's index arithmetic, the predicates, the diagonal flag
 // and the other-colour cell between them.  Same per-cell arithmetic, in the
 // same order, as k_rb_sweep.
-template <typename T, bool H>
+// from_b: the sweep that follows a zero-guess red sweep reads the red values
+// that sweep would have written, b / a0, straight from b (and the diagonal),
+// so the zero-guess sweep itself is not launched
+template <typename T, bool H, bool FROM_B = false>
 __global__ void __launch_bounds__(256) k_rb_sweep2(MGLevel<T> L, T *__restrict__ x,
                                                    const T *__restrict__ b, int colour,
                                                    int init, int flip) {
@@ -607,17 +620,29 @@ __global__ void __launch_bounds__(256) k_rb_sweep2(MGLevel<T> L, T *__restrict__
       return ldro(L.a[s + 1] + c);
   };
   const T *xr = x;  // the other colour: not written by this launch
-  const T xm = he0 ? ldro(xr + ob + r) : T(0);  // between the two cells
+  // the other colour's value at split index q (natural index cn)
+  auto xv = [&](int q, int cn) -> T {
+    if constexpr (!FROM_B) {
+      return ldro(xr + q);
+    } else {
+      const T bv = ldro(b + q);
+      if constexpr (H)
+        return unit ? bv : bv / (T)ldro_h(L.h[3] + cn);
+      else
+        return bv / ldro(L.a[0] + cn);
+    }
+  };
+  const T xm = he0 ? xv(ob + r, c0 + 1) : T(0);  // between the two cells
   {
     const T cw = hw ? coef(0, c0 - 1) : T(0), ce = coef(0, c0);
     const T cs = hsj ? coef(1, c0 - sy) : T(0), cn = coef(1, c0);
     const T cl = hl ? coef(2, c0 - sz) : T(0), cu = coef(2, c0);
-    T acc = cw * (hw ? ldro(xr + ob - 1 + r) : T(0));
+    T acc = cw * (hw ? xv(ob - 1 + r, c0 - 1) : T(0));
     acc = fma(ce, xm, acc);
-    acc = fma(cs, hsj ? ldro(xr + ob - hx) : T(0), acc);
-    acc = fma(cn, hn ? ldro(xr + ob + hx) : T(0), acc);
-    acc = fma(cl, hl ? ldro(xr + ob - hs) : T(0), acc);
-    acc = fma(cu, hu ? ldro(xr + ob + hs) : T(0), acc);
+    acc = fma(cs, hsj ? xv(ob - hx, c0 - sy) : T(0), acc);
+    acc = fma(cn, hn ? xv(ob + hx, c0 + sy) : T(0), acc);
+    acc = fma(cl, hl ? xv(ob - hs, c0 - sz) : T(0), acc);
+    acc = fma(cu, hu ? xv(ob + hs, c0 + sz) : T(0), acc);
     const T bc = ldro(b + xo);
     x[xo] = unit ? bc - acc : (bc - acc) / d0;
   }
@@ -627,11 +652,11 @@ __global__ void __launch_bounds__(256) k_rb_sweep2(MGLevel<T> L, T *__restrict__
     const T cs = hsj ? coef(1, c1 - sy) : T(0), cn = coef(1, c1);
     const T cl = hl ? coef(2, c1 - sz) : T(0), cu = coef(2, c1);
     T acc = cw * xm;
-    acc = fma(ce, he1 ? ldro(xr + o1 + r) : T(0), acc);
-    acc = fma(cs, hsj ? ldro(xr + o1 - hx) : T(0), acc);
-    acc = fma(cn, hn ? ldro(xr + o1 + hx) : T(0), acc);
-    acc = fma(cl, hl ? ldro(xr + o1 - hs) : T(0), acc);
-    acc = fma(cu, hu ? ldro(xr + o1 + hs) : T(0), acc);
+    acc = fma(ce, he1 ? xv(o1 + r, c1 + 1) : T(0), acc);
+    acc = fma(cs, hsj ? xv(o1 - hx, c1 - sy) : T(0), acc);
+    acc = fma(cn, hn ? xv(o1 + hx, c1 + sy) : T(0), acc);
+    acc = fma(cl, hl ? xv(o1 - hs, c1 - sz) : T(0), acc);
+    acc = fma(cu, hu ? xv(o1 + hs, c1 + sz) : T(0), acc);
     const T bc = ldro(b + xo + 1);
     x[xo + 1] = unit ? bc - acc : (bc - acc) / d1;
   }
@@ -1433,17 +1458,29 @@ void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_
   }
   setup_level_d<T, false>(F, C, st);
 }
+// the two-cells-per-thread sweep serves this level
+template <typename T>
+static bool rb_sweep_pairs(const MGLevel<T> &L, bool h16) {
+  if constexpr (kHasH16<T>)
+    return h16 && L.split && !getenv_flag_one_cell();
+  else
+    return false;
+}
 template <typename T>
 static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init,
-                     cudaStream_t st, int flip, bool h16) {
+                     cudaStream_t st, int flip, bool h16, int from_b = 0) {
   // two cells per thread on colour-split levels of the FP16 operator (it is
   // bound by instruction issue there; the FP32 and FP64 sweeps, bound by
   // memory, are as fast or faster with one cell per thread and more threads)
   if constexpr (kHasH16<T>) {
-    if (h16 && L.split && !getenv_flag_one_cell()) {
+    if (rb_sweep_pairs(L, h16)) {
       Shape3 g2 = shape3((L.hx + 1) / 2, L.ny, L.nz);
-      launch_pdl(k_rb_sweep2<T, true>, dim3(g2.grid), dim3(g2.block), st, L, x, b, colour,
-                 init, flip);
+      if (from_b)
+        launch_pdl(k_rb_sweep2<T, true, true>, dim3(g2.grid), dim3(g2.block), st, L, x, b,
+                   colour, init, flip);
+      else
+        launch_pdl(k_rb_sweep2<T, true>, dim3(g2.grid), dim3(g2.block), st, L, x, b, colour,
+                   init, flip);
       return;
     }
   }
@@ -1462,7 +1499,7 @@ static void rb_sweep(const MGLevel<T> &L, T *x, const T *b, int colour, int init
 // first red sweep into x = b / a0 (rb_GS_point.c:107-240).  Smoother 9 is a
 // single red sweep (kernel timing).
 template <typename T>
-void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
+int launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st, int *flip, bool h16) {
   const int f = flip ? *flip : 0, g = flip ? f ^ 1 : 0;
   if (smoother == 1) {
@@ -1478,22 +1515,31 @@ void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoot
       launch_pdl(k_wjacobi<T, false>, dim3(sh.grid), dim3(sh.block), st, L, x, b, tmp, zero);
     launch_pdl(k_wjacobi_update<T>, dim3(nb(L.n, 256)), dim3(256), st, x, tmp, L.n, (T)weight,
                zero);
-    return;
+    return 2;
   }
   if (smoother == 9) {  // a single red sweep (kernel timing)
     rb_sweep(L, x, b, 0, 0, st, 0, h16);
-    return;
+    return 1;
   }
   if (smoother == 2) {
     rb_sweep(L, x, b, 0, zero, st, f, h16);
     rb_sweep(L, x, b, 1, 0, st, g, h16);
     if (flip) *flip = f;
-    return;
+    return 2;
+  }
+  if (zero && rb_sweep_pairs(L, h16) && skip_zero_sweep()) {
+    // the black sweep reads the zero-guess red values from b; the last red
+    // sweep writes x of the red cells
+    rb_sweep(L, x, b, 1, 0, st, g, h16, 1);
+    rb_sweep(L, x, b, 0, 0, st, f, h16);
+    if (flip) *flip = g;
+    return 2;
   }
   rb_sweep(L, x, b, 0, zero, st, f, h16);
   rb_sweep(L, x, b, 1, 0, st, g, h16);
   rb_sweep(L, x, b, 0, 0, st, f, h16);
   if (flip) *flip = g;
+  return 3;
 }
 template <typename K>
 static cudaError_t mid_prepare(K kern) {
@@ -1916,7 +1962,7 @@ void launch_convert(const TI *in, TO *out, long long n, cudaStream_t st, int fli
   template void launch_mg_coarse_op<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t); \
   template void launch_mg_setup_level<T>(const MGLevel<T> &, const MGLevel<T> &, cudaStream_t, \
                                          bool);                                               \
-  template void launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *, \
+  template int launch_mg_smooth<T>(const MGLevel<T> &, T *, const T *, int, int, double, T *,  \
                                     cudaStream_t, int *, bool);                               \
   template void launch_mg_residual<T>(const MGLevel<T> &, const T *, const T *, T *,          \
                                       cudaStream_t, int, bool, int);                          \

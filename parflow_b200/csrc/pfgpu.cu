@@ -464,7 +464,6 @@ template <typename T>
 static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
-  const int sk = (smoother == 1 || smoother == 2) ? 2 : 3;
   const int first = mg.mid;
   // block order of the next grid launch: with mg.flip every launch runs in
   // the opposite order of the one before it (the input conversion runs
@@ -486,8 +485,7 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
       f = mg.flip ? 1 : 0;  // the wave ends on the top planes
       k++;
     } else {
-      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st, fp, mg.h16);
-      k += sk;
+      k += launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st, fp, mg.h16);
     }
     // after the plain red/black pre-smoother the colour swept last (red, or
     // black for the non-symmetric order) has a zero residual up to rounding
@@ -527,8 +525,7 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
       f = mg.flip ? 1 : 0;
       k += 2;
     } else {
-      launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st, fp, mg.h16);
-      k += 1 + sk;
+      k += 1 + launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st, fp, mg.h16);
     }
   }
   mg.flip_out = f;

@@ -178,9 +178,10 @@ template <typename T>
 void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_t st,
                            bool h16 = false);
 // flip (optional): block order of the first sweep (0 forward, 1 reversed);
-// sweeps alternate and *flip returns the order the next launch should use
+// sweeps alternate and *flip returns the order the next launch should use;
+// returns the number of kernels launched
 template <typename T>
-void launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
+int launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st, int *flip = nullptr,
                       bool h16 = false);
 cudaError_t mg_prepare_kernels();
