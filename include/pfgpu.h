@@ -346,6 +346,14 @@ int pfgpu_newton_solve_sat(pfgpu_handle *h, const double *p_old, const double *s
  * KINSOL loop is host code). */
 int pfgpu_solve_graph(pfgpu_handle *h, int mode);
 
+/* Solver.Nonlinear.Globalization (kinsol_nonlin_solver.c:887-905):
+ * PFGPU_GLOBAL_LINE_SEARCH (the default, KINLineSearch, kinsol.c:1228-1420)
+ * or PFGPU_GLOBAL_INEXACT_NEWTON (KINInexactNewton, kinsol.c:1152-1208: the
+ * full Newton step, shortened to the maximum step, no backtracking). */
+#define PFGPU_GLOBAL_LINE_SEARCH 0
+#define PFGPU_GLOBAL_INEXACT_NEWTON 1
+int pfgpu_set_globalization(pfgpu_handle *h, int strategy);
+
 /* Device-resident time stepping: advances the handle's own pressure state by
  * nsteps steps of dt with the boundary tables already set, keeping every
  * vector on the GPU (the step body of AdvanceRichards,

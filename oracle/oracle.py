@@ -48,7 +48,8 @@ class Settings(C.Structure):
                 ("eta_value", C.c_double), ("eta_alpha", C.c_double), ("eta_gamma", C.c_double),
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
                 ("wjacobi_weight", C.c_double),
-                ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double)]
+                ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double),
+                ("globalization", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -160,6 +161,7 @@ class Oracle:
         S.wjacobi_weight = s.smoother_weight()
         S.use_jacobian = 1 if s.use_jacobian else 0
         S.derivative_epsilon = s.derivative_epsilon
+        S.globalization = s.globalization_code()
         self.S = S
 
     def __del__(self):

@@ -1996,7 +1996,8 @@ done:
   return ret;
 }
 
-/* KINSol (KS/kinsol.c:363-910) with LineSearch globalization */
+/* KINSol (KS/kinsol.c:363-910) with LineSearch or InexactNewton
+ * globalization */
 void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double dt,
                       const double *p_old, const double *s_old, double *p,
                       pfo_stats *stats)
@@ -2097,9 +2098,30 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
     sJpnorm = sqrt(dot(bb, bb, N));
     sfdotJp = dot(fval, bb, N);
 
-    /* KINLineSearch (KS/kinsol.c:1228-1420) */
     int globalret = 0, maxStepTaken = 0;
     double fnormp, f1normp;
+    if (st->globalization == 1)
+    {
+      /* KINInexactNewton (KS/kinsol.c:1152-1208): the full step, shortened
+       * to mxnewtstep; no constraints are set */
+      double pnorm = sqrt(dot(pp, pp, N));
+      double ratio = 1.0;
+      if (pnorm > mxnewtstep)
+      {
+        ratio = mxnewtstep / pnorm;
+        for (long q = 0; q < N; q++) pp[q] *= ratio;
+        pnorm = mxnewtstep;
+      }
+      sfdotJp = sfdotJp * ratio;
+      sJpnorm = sJpnorm * ratio;
+      for (long q = 0; q < N; q++) unew[q] = uu[q] + pp[q];
+      feval(&kc, unew, fval);
+      fnormp = sqrt(dot(fval, fval, N));
+      f1normp = 0.5 * fnormp * fnormp;
+      if (pnorm > 0.99 * mxnewtstep) maxStepTaken = 1;
+      goto ls_done;
+    }
+    /* KINLineSearch (KS/kinsol.c:1228-1420) */
     {
       double pnorm = sqrt(dot(pp, pp, N));
       double ratio = 1.0, alpha = 0.0001, beta = 0.9;

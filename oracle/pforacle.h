@@ -76,6 +76,8 @@ typedef struct {
   int use_jacobian;                /* Solver.Nonlinear.UseJacobian: 1 analytic J v,
                                     * 0 KINSOL's difference quotient */
   double derivative_epsilon;       /* Solver.Nonlinear.DerivativeEpsilon */
+  int globalization;               /* Solver.Nonlinear.Globalization: 0 LineSearch,
+                                    * 1 InexactNewton */
 } pfo_settings;
 
 typedef struct {

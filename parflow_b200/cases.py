@@ -213,6 +213,15 @@ def picard_small() -> RichardsProblem:
                           solver=SolverSettings(pc_matrix_type="Picard"))
 
 
+def inexact_small() -> RichardsProblem:
+    """Solver.Nonlinear.Globalization InexactNewton: the full Newton step,
+    no line search (kinsol.c:1152-1208), on config-2 physics with steps of
+    20 h, where the line search would backtrack (8 Newton iterations and 35
+    residual evaluations in the first step against 5 and 6 here)."""
+    return configs.hetero(nx=13, ny=12, nz=8, nsteps=3, dt=20.0, seed=61,
+                          solver=SolverSettings(globalization="InexactNewton"))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -222,7 +231,7 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
-          "picard_small"]
+          "picard_small", "inexact_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

@@ -218,6 +218,10 @@ __global__ void k_nk_ls1(NkState *S, const double *dsc, NkConds c) {
   pdl_enter();
   S->execs[NKB_LS1]++;
   take_trial(S, dsc);
+  if (S->k.inexact) {  // KINInexactNewton takes the full step (kinsol.c:1152-1208)
+    setc(c.ls1, false);
+    return;
+  }
   if (S->ls_phase == 1) {  // the step was too small: u itself was re-evaluated
     S->backtracks = S->fevals - S->nfesav - 1;
     S->globalret = 1;
@@ -253,7 +257,7 @@ __global__ void k_nk_ls1(NkState *S, const double *dsc, NkConds c) {
 __global__ void k_nk_ls2_init(NkState *S, NkConds c) {
   pdl_enter();
   bool run = false;
-  if (S->globalret != 1 && !S->err) {
+  if (S->globalret != 1 && !S->err && !S->k.inexact) {
     S->beta_cond = S->f1norm + LS_BETA * S->slpi * S->rl;
     if (S->f1normp < S->beta_cond) {
       // (rl == 1 && pnorm < stepl) never holds without constraints

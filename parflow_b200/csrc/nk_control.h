@@ -51,6 +51,7 @@ enum {
 struct NkConst {
   double fnormtol, scsteptol, epsmin, ealpha, egamma, eta0, bsign;
   int etaflag, mxiter, lmax, max_restarts, use_dq;
+  int inexact;  // KINInexactNewton: the first trial step is taken, no backtracking
 };
 
 struct NkState {

@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <functional>
+#include <thread>
 #include <type_traits>
 #include <vector>
 
@@ -183,6 +184,7 @@ struct pfgpu_handle {
   // Solver.Nonlinear.UseJacobian (1: analytic J v; 0: KINSOL's difference
   // quotient with sqrt(DerivativeEpsilon)) and its two work vectors
   int use_jacobian = 1;
+  int globalization = PFGPU_GLOBAL_LINE_SEARCH;  // Solver.Nonlinear.Globalization
   double sqrt_relfunc = 0.0;
   double *dq_w = nullptr, *dq_f = nullptr;
   double *krt = nullptr;  // relative-permeability lookup table (device)
@@ -888,56 +890,63 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
       steplen_new = hsc[D_STEP];
       return 0;
     };
-    for (int it = 0;; it++) {
-      if (it > 1000) {
-        set_err("line search exceeded its iteration bound");
-        return PFGPU_ERR_STATE;
-      }
+    if (h->globalization == PFGPU_GLOBAL_INEXACT_NEWTON) {
+      // KINInexactNewton (kinsol.c:1152-1208): the full (possibly shortened)
+      // step; the common tail below scales sfdotJp and sJpnorm by ratio
+      // (rl = 1) and takes maxStepTaken from pnorm
       if (try_step(rl)) return PFGPU_ERR_CUDA;
-      alpha_cond = f1norm + alpha * slpi * rl;
-      if (f1normp <= alpha_cond) break;
-      if (rl < rlmin) {
-        // unew = u, re-evaluate and return 1
-        if (try_step(0.0)) return PFGPU_ERR_CUDA;
-        stats->backtracks = stats->fevals - nfesav - 1;
-        globalret = 1;
-        goto ls_done;
+    } else {
+      for (int it = 0;; it++) {
+        if (it > 1000) {
+          set_err("line search exceeded its iteration bound");
+          return PFGPU_ERR_STATE;
+        }
+        if (try_step(rl)) return PFGPU_ERR_CUDA;
+        alpha_cond = f1norm + alpha * slpi * rl;
+        if (f1normp <= alpha_cond) break;
+        if (rl < rlmin) {
+          // unew = u, re-evaluate and return 1
+          if (try_step(0.0)) return PFGPU_ERR_CUDA;
+          stats->backtracks = stats->fevals - nfesav - 1;
+          globalret = 1;
+          goto ls_done;
+        }
+        {
+          double rltmp = -slpi / (2.0 * (f1normp - f1norm - slpi));
+          if (rltmp > 0.5 * rl) rltmp = 0.5 * rl;
+          rlprev = rl;
+          double pt1trl = 0.1 * rl;
+          rl = (pt1trl > rltmp) ? pt1trl : rltmp;
+        }
       }
-      {
-        double rltmp = -slpi / (2.0 * (f1normp - f1norm - slpi));
-        if (rltmp > 0.5 * rl) rltmp = 0.5 * rl;
-        rlprev = rl;
-        double pt1trl = 0.1 * rl;
-        rl = (pt1trl > rltmp) ? pt1trl : rltmp;
-      }
-    }
-    beta_cond = f1norm + beta * slpi * rl;
-    if (f1normp < beta_cond) {
-      // (rl == 1 && pnorm < stepl) never holds without constraints
-      if (rl < 1.0 || ((rl > 1.0) && (f1normp > alpha_cond))) {
-        double rllo = (rl < rlprev) ? rl : rlprev;
-        double rldiff = fabs(rlprev - rl);
-        int it = 0;
-        do {
-          if (++it > 1000) {
-            set_err("line search refinement exceeded its iteration bound");
-            return PFGPU_ERR_STATE;
+      beta_cond = f1norm + beta * slpi * rl;
+      if (f1normp < beta_cond) {
+        // (rl == 1 && pnorm < stepl) never holds without constraints
+        if (rl < 1.0 || ((rl > 1.0) && (f1normp > alpha_cond))) {
+          double rllo = (rl < rlprev) ? rl : rlprev;
+          double rldiff = fabs(rlprev - rl);
+          int it = 0;
+          do {
+            if (++it > 1000) {
+              set_err("line search refinement exceeded its iteration bound");
+              return PFGPU_ERR_STATE;
+            }
+            double rlincr = 0.5 * rldiff;
+            rl = rllo + rlincr;
+            if (try_step(rl)) return PFGPU_ERR_CUDA;
+            alpha_cond = f1norm + alpha * slpi * rl;
+            beta_cond = f1norm + beta * slpi * rl;
+            if (f1normp > alpha_cond)
+              rldiff = rlincr;
+            else if (f1normp < beta_cond) {
+              rllo = rl;
+              rldiff = rldiff - rlincr;
+            }
+          } while (f1normp > alpha_cond || ((f1normp < beta_cond) && (rldiff > rlmin)));
+          if (f1normp < beta_cond) {
+            if (try_step(rllo)) return PFGPU_ERR_CUDA;
+            stats->beta_cond_fails++;
           }
-          double rlincr = 0.5 * rldiff;
-          rl = rllo + rlincr;
-          if (try_step(rl)) return PFGPU_ERR_CUDA;
-          alpha_cond = f1norm + alpha * slpi * rl;
-          beta_cond = f1norm + beta * slpi * rl;
-          if (f1normp > alpha_cond)
-            rldiff = rlincr;
-          else if (f1normp < beta_cond) {
-            rllo = rl;
-            rldiff = rldiff - rlincr;
-          }
-        } while (f1normp > alpha_cond || ((f1normp < beta_cond) && (rldiff > rlmin)));
-        if (f1normp < beta_cond) {
-          if (try_step(rllo)) return PFGPU_ERR_CUDA;
-          stats->beta_cond_fails++;
         }
       }
     }
@@ -1292,7 +1301,7 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(&P, &h->P, sizeof(P));
   P.dtp = nullptr;
   const double *ptrs[2] = {h->u, h->unew};
-  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + sizeof(int) +
+  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + 2 * sizeof(int) +
                                sizeof(double));
   unsigned char *q = k.data();
   memcpy(q, &P, sizeof(P));
@@ -1304,6 +1313,8 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(q, &h->use_jacobian, sizeof(int));
   q += sizeof(int);
   memcpy(q, &h->sqrt_relfunc, sizeof(double));
+  q += sizeof(double);
+  memcpy(q, &h->globalization, sizeof(int));
   return k;
 }
 
@@ -1407,6 +1418,7 @@ static int nk_setup(pfgpu_handle *h) {
   k.lmax = d.krylov_dim;
   k.max_restarts = d.max_restarts;
   k.use_dq = h->use_jacobian ? 0 : 1;
+  k.inexact = h->globalization == PFGPU_GLOBAL_INEXACT_NEWTON ? 1 : 0;
   CK(cudaMemcpy(&G.S->k, &k, sizeof(k), cudaMemcpyHostToDevice));
   return 0;
 }
@@ -1518,6 +1530,7 @@ static int newton_graph(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
         set_err("solve graph did not finish within %.0f s", limit);
         return PFGPU_ERR_STATE;
       }
+      std::this_thread::yield();
     }
   }
   const NkState &S = *G.hS;
@@ -1905,6 +1918,15 @@ static void ens_forget(unsigned long long uid) {
 }
 
 static int ens_build(pfgpu_handle *const *members, int n, EnsembleGraph *E) {
+  // the members' own graphs keep their launch counts whatever happens here
+  std::vector<std::array<long long, NKB_COUNT>> counts(n);
+  for (int m = 0; m < n; m++)
+    std::copy(std::begin(members[m]->nk.kernels), std::end(members[m]->nk.kernels),
+              counts[m].begin());
+  auto restore = [&]() {
+    for (int m = 0; m < n; m++)
+      std::copy(counts[m].begin(), counts[m].end(), std::begin(members[m]->nk.kernels));
+  };
   for (int attempt = 0; attempt < 2; attempt++) {
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
@@ -1920,11 +1942,16 @@ static int ens_build(pfgpu_handle *const *members, int n, EnsembleGraph *E) {
     }
     cudaGraphDestroy(g);
     if (!rc) {
+      restore();
       CK(cudaGraphUpload(E->exec, E->st));
       return 0;
     }
-    if (attempt == 1) return rc;
+    if (attempt == 1) {
+      restore();
+      return rc;
+    }
   }
+  restore();
   return PFGPU_ERR_CUDA;
 }
 
@@ -2017,6 +2044,7 @@ int pfgpu::ensemble_graph_advance(pfgpu_handle *const *members, int n, const dou
         set_err("ensemble graph did not finish within %.0f s", limit);
         return PFGPU_ERR_STATE;
       }
+      std::this_thread::yield();
     }
     for (int m = 0; m < n; m++) {
       pfgpu_handle *h = members[m];
@@ -2998,6 +3026,16 @@ int pfgpu_solve_graph(pfgpu_handle *h, int mode) {
   if (mode == -1) return h->nk.used_last ? 1 : 0;
   set_err("pfgpu_solve_graph: mode must be 0, 1 or -1");
   return PFGPU_ERR_ARG;
+}
+
+int pfgpu_set_globalization(pfgpu_handle *h, int strategy) {
+  if (!h || (strategy != PFGPU_GLOBAL_LINE_SEARCH && strategy != PFGPU_GLOBAL_INEXACT_NEWTON)) {
+    set_err("pfgpu_set_globalization: strategy must be PFGPU_GLOBAL_LINE_SEARCH or "
+            "PFGPU_GLOBAL_INEXACT_NEWTON");
+    return PFGPU_ERR_ARG;
+  }
+  h->globalization = strategy;
+  return PFGPU_OK;
 }
 
 int pfgpu_set_pressure(pfgpu_handle *h, const double *p) {

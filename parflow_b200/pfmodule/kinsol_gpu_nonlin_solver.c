@@ -66,6 +66,7 @@ typedef struct {
   pfgpu_desc desc; /* solver keys */
   int use_jacobian;
   double derivative_epsilon;
+  int globalization; /* PFGPU_GLOBAL_* */
 } GpuPublicXtra;
 
 typedef struct {
@@ -179,8 +180,10 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
   px->derivative_epsilon = GetDoubleDefault("Solver.Nonlinear.DerivativeEpsilon", 1e-7);
   na = NA_NewNameArray("InexactNewton LineSearch");
   name = GetStringDefault("Solver.Nonlinear.Globalization", "LineSearch");
-  if (NA_NameToIndexExitOnError(na, name, "Solver.Nonlinear.Globalization") != 1)
-    gpu_fail("only Solver.Nonlinear.Globalization LineSearch is available");
+  px->globalization =
+      NA_NameToIndexExitOnError(na, name, "Solver.Nonlinear.Globalization") == 0
+          ? PFGPU_GLOBAL_INEXACT_NEWTON
+          : PFGPU_GLOBAL_LINE_SEARCH;
   NA_FreeNameArray(na);
   na = NA_NewNameArray("NoPC MGSemi SMG PFMG PFMGOctree");
   name = GetStringDefault("Solver.Linear.Preconditioner", "MGSemi");
@@ -403,6 +406,8 @@ static void create_handle(GpuInstanceXtra *ix, GpuPublicXtra *px, Vector *pressu
     gpu_fail(pfgpu_last_error());
   if (!px->use_jacobian &&
       pfgpu_set_jacobian_mode(ix->h, 0, px->derivative_epsilon) != PFGPU_OK)
+    gpu_fail(pfgpu_last_error());
+  if (pfgpu_set_globalization(ix->h, px->globalization) != PFGPU_OK)
     gpu_fail(pfgpu_last_error());
 
   /* permeability: x, and y / z where they differ from x */

@@ -151,6 +151,14 @@ class SolverSettings:
             raise ValueError(f"unknown MGSemi smoother {self.mg_smoother}")
         return 0 if self.mg_smoother_symmetric else 2
 
+    def globalization_code(self) -> int:
+        """Solver.Nonlinear.Globalization (kinsol_nonlin_solver.c:887-905):
+        0 LineSearch, 1 InexactNewton."""
+        table = {"LineSearch": 0, "InexactNewton": 1}
+        if self.globalization not in table:
+            raise ValueError(f"Solver.Nonlinear.Globalization {self.globalization} is not available")
+        return table[self.globalization]
+
     def smoother_weight(self) -> float:
         if self.preconditioner == "PFMG":
             return 1.0

@@ -94,6 +94,9 @@ class RichardsGPU:
         if not s.use_jacobian:
             L.check(self.lib.pfgpu_set_jacobian_mode(self.h, 0, s.derivative_epsilon),
                     "set_jacobian_mode")
+        if s.globalization_code() != 0:
+            L.check(self.lib.pfgpu_set_globalization(self.h, s.globalization_code()),
+                    "set_globalization")
         if prob.kr_table:
             method = {"Spline": 1, "Linear": 2}[prob.kr_table[0]]
             L.check(self.lib.pfgpu_set_relperm_table(self.h, method, int(prob.kr_table[1]),
