@@ -86,6 +86,15 @@ extern "C" {
 #define PFGPU_FIELD_VG_N 4
 #define PFGPU_FIELD_S_RES 5
 #define PFGPU_FIELD_S_SAT 6
+/* flow-barrier multipliers of the faces between a cell and its +x / +y / +z
+ * neighbour (Solver.Nonlinear.FlowBarrierX/Y/Z, problem_FBx.c:60-120;
+ * nl_function_eval.c:841-843, richards_jacobian_eval.c:662-728); NULL values
+ * restore 1 everywhere.  The multipliers of the last cell along each
+ * direction (the boundary faces) are not used: the boundary patches set
+ * those fluxes. */
+#define PFGPU_FIELD_FB_X 7
+#define PFGPU_FIELD_FB_Y 8
+#define PFGPU_FIELD_FB_Z 9
 
 /* eta choice (pfsimulator/parflow_lib/kinsol_nonlin_solver.c:804-850) */
 #define PFGPU_ETA_CONSTANT 0
@@ -147,9 +156,10 @@ const char *pfgpu_last_error(void);
 /* Uploads a spatially varying cell field (ParFlow layout).  Replaces the
  * ProblemData fields read by the modules: permeability (subsrf_sim.c:684-810),
  * per-cell van Genuchten parameters (problem_saturation.c:943-950,
- * problem_phase_rel_perm.c:1930-1932).  values == NULL on a van Genuchten
- * field (PFGPU_FIELD_VG_ALPHA .. S_SAT) drops its per-cell array, so that the
- * descriptor's scalar serves every cell again; permeability needs values. */
+ * problem_phase_rel_perm.c:1930-1932), flow barriers (problem_FBx.c).
+ * values == NULL on a van Genuchten field (PFGPU_FIELD_VG_ALPHA .. S_SAT)
+ * drops its per-cell array, so that the descriptor's scalar serves every cell
+ * again, and on a flow-barrier field restores 1; permeability needs values. */
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values);
 
 /* Time-cycled boundary data (TimeCycleData, time_cycle_data.c, and the

@@ -34,7 +34,7 @@ class Problem(C.Structure):
                 ("ov_epsilon", C.c_double),
                 ("ov_p_old", _dp),
                 ("kr_table", C.c_void_p),
-                ("evap_trans", _dp)]
+                ("evap_trans", _dp), ("fbx", _dp), ("fby", _dp), ("fbz", _dp)]
 
 
 class FluxOut(C.Structure):
@@ -49,7 +49,7 @@ class Settings(C.Structure):
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
                 ("wjacobi_weight", C.c_double),
                 ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double),
-                ("globalization", C.c_int)]
+                ("globalization", C.c_int), ("pc_full", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -77,12 +77,15 @@ def lib():
         L.pfo_residual_out.argtypes = [C.POINTER(Problem), C.c_double, _dp, _dp, _dp, _dp,
                                        C.POINTER(FluxOut)]
         L.pfo_jacobian.argtypes = [C.POINTER(Problem), C.c_double, _dp, C.c_int, C.POINTER(_dp)]
+        L.pfo_jacobian_fd.argtypes = [C.POINTER(Problem), C.c_double, _dp, C.c_int, C.c_int,
+                                      C.POINTER(_dp)]
         L.pfo_matvec7.argtypes = [C.POINTER(Problem), C.POINTER(_dp), _dp, _dp]
         L.pfo_saturation.argtypes = [C.POINTER(Problem), _dp, _dp, C.c_int]
         L.pfo_relperm.argtypes = [C.POINTER(Problem), _dp, _dp, C.c_int]
         L.pfo_mg_create.argtypes = [C.POINTER(Problem), C.POINTER(Settings)]
         L.pfo_mg_create.restype = C.c_void_p
         L.pfo_mg_setup.argtypes = [C.c_void_p, C.POINTER(_dp)]
+        L.pfo_mg_setup_full.argtypes = [C.c_void_p, C.POINTER(_dp)]
         L.pfo_mg_set_wghost.argtypes = [C.c_void_p, _dp]
         L.pfo_vgtable_create.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double, C.c_double]
         L.pfo_vgtable_create.restype = C.c_void_p
@@ -141,6 +144,12 @@ class Oracle:
             et = np.ascontiguousarray(prob.field3d(prob.evap_trans), dtype=np.float64)
             self._keep.append(et)
             P.evap_trans = _ptr(et)
+        for name in ("fbx", "fby", "fbz"):
+            v = getattr(prob, name)
+            if v is not None:
+                a = np.ascontiguousarray(prob.field3d(v), dtype=np.float64)
+                self._keep.append(a)
+                setattr(P, name, _ptr(a))
         self._table = None
         if prob.kr_table:
             method = {"Spline": 0, "Linear": 1}[prob.kr_table[0]]
@@ -162,6 +171,7 @@ class Oracle:
         S.use_jacobian = 1 if s.use_jacobian else 0
         S.derivative_epsilon = s.derivative_epsilon
         S.globalization = s.globalization_code()
+        S.pc_full = s.pc_matrix_code()
         self.S = S
 
     def __del__(self):
@@ -216,11 +226,13 @@ class Oracle:
         lib().pfo_relperm(C.byref(self.P), _ptr(p), _ptr(s), der)
         return s
 
-    def jacobian(self, p, dt, symm=0, p_old=None):
+    def jacobian(self, p, dt, symm=0, p_old=None, fd=False):
         """J(p) (7 arrays C W E S N L U) or its PFSymmetric PC form (symm=1:
         C E N U; symm=2: also the (nz, ny) W entries of the i = 0 cells that
         the symmetric storage keeps in a ghost column); p_old is the step's
-        old pressure, which only the diffusive overland terms read."""
+        old pressure, which only the diffusive overland terms read; fd: the
+        matrix the reference builds with Solver.Nonlinear.UseJacobian False
+        (no overland surface terms)."""
         p = np.ascontiguousarray(p, dtype=np.float64)
         ns = 4 if symm else 7
         J = [np.empty_like(p) for _ in range(ns)]
@@ -229,7 +241,7 @@ class Oracle:
         arr = (_dp * len(J))(*[_ptr(x) for x in J])
         po = np.ascontiguousarray(p if p_old is None else p_old, dtype=np.float64)
         self.P.ov_p_old = _ptr(po)
-        lib().pfo_jacobian(C.byref(self.P), dt, _ptr(p), symm, arr)
+        lib().pfo_jacobian_fd(C.byref(self.P), dt, _ptr(p), symm, 1 if fd else 0, arr)
         self.P.ov_p_old = None
         return J
 
@@ -372,6 +384,13 @@ class MG:
         lib().pfo_mg_set_wghost(self.h, _ptr(A4[4]) if len(A4) > 4 else None)
         arr = (_dp * 4)(*[_ptr(a) for a in A4[:4]])
         lib().pfo_mg_setup(self.h, arr)
+
+    def setup_full(self, A7):
+        """A7 = the full Jacobian C W E S N L U (PCMatrixType FullJacobian)."""
+        A7 = [np.ascontiguousarray(a, dtype=np.float64) for a in A7]
+        self._A = A7
+        arr = (_dp * 7)(*[_ptr(a) for a in A7])
+        lib().pfo_mg_setup_full(self.h, arr)
 
     def apply(self, b):
         b = np.ascontiguousarray(b, dtype=np.float64)

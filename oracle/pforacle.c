@@ -743,8 +743,11 @@ void pfo_residual_out(const pfo_problem *pb, double dt, const double *p,
           u_upper = ffz * 1.0 * 1.0 * HARMONIC_DZ(pb->kz[c], pb->kz[u], zc, zu) * diff_l
                     * UPSTREAM(lower, upper, kr[c] * rho, kr[u] * rho) / visc;
         }
-        /* face velocities :845-848 (flow barriers 1); the boundary faces
-         * are written by the patch loops below */
+        /* flow barriers :841-843, then the face velocities :845-848; the
+         * boundary faces are written by the patch loops below */
+        if (pb->fbx) u_right = u_right * pb->fbx[c];
+        if (pb->fby) u_front = u_front * pb->fby[c];
+        if (pb->fbz) u_upper = u_upper * pb->fbz[c];
         if (out->vx && i + 1 < nx)
           out->vx[(i + 1) + (long)(nx + 1) * (j + (long)ny * k)] = u_right / (ffx * zm[k] * 1.0);
         if (out->vy && j + 1 < ny)
@@ -908,8 +911,23 @@ void pfo_residual_out(const pfo_problem *pb, double dt, const double *p,
  *   storage keeps in the x_lower ghost column of E (matrix.c:477-490) and
  *   MGSemi's setup reads (mg_semi.c:563, 671-682)
  * ------------------------------------------------------------------------- */
+void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm, int fd,
+                     double *const *J);
+
 void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
                   double *const *J)
+{
+  pfo_jacobian_fd(pb, dt, p, symm, 0, J);
+}
+
+/* fd = 1: the matrix the reference builds under Solver.Nonlinear.UseJacobian
+ * False, where the Jacobian module's type is no_nonlinear_jacobian
+ * (richards_jacobian_eval.c:2476-2484): the overland surface terms are left
+ * out (they are added only with using_MGSemi, which that key clears, :1863),
+ * and an OverlandFlow top cell with p > 0 gets the diagonal term of the
+ * "simple" case it falls through to (:1241-1254) */
+void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm, int fd,
+                     double *const *J)
 {
   const int nx = pb->nx, ny = pb->ny, nz = pb->nz;
   const long N = (long)nx * ny * nz;
@@ -970,7 +988,8 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           double prod_rt_der = dkr[e] * rho + kr[e] * drho;
           double diff = p[c] - p[e];
           double updir = (diff / dx) * x_dir_g_c - x_dir_g;
-          double x_coeff = 1.0 * dt * ffx * (1.0 / dx) * zm[k] * HARMONIC(pb->kx[c], pb->kx[e]) / visc;
+          double x_coeff = (pb->fbx ? pb->fbx[c] : 1.0) * dt * ffx * (1.0 / dx) * zm[k] *
+                           HARMONIC(pb->kx[c], pb->kx[e]) / visc;
           double sym_west_temp = (-x_coeff * UPSTREAM(updir, 0.0, prod, prod_rt)) * x_dir_g_c;
           west_temp = (-x_coeff * diff * UPSTREAM(updir, 0.0, prod_der, 0.0)) * x_dir_g_c + sym_west_temp;
           west_temp += (x_coeff * dx * UPSTREAM(updir, 0.0, prod_der, 0.0)) * x_dir_g;
@@ -985,7 +1004,8 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           double prod_no_der = dkr[n] * rho + kr[n] * drho;
           double diff = p[c] - p[n];
           double updir = (diff / dy) * y_dir_g_c - y_dir_g;
-          double y_coeff = 1.0 * dt * ffy * (1.0 / dy) * zm[k] * HARMONIC(pb->ky[c], pb->ky[n]) / visc;
+          double y_coeff = (pb->fby ? pb->fby[c] : 1.0) * dt * ffy * (1.0 / dy) * zm[k] *
+                           HARMONIC(pb->ky[c], pb->ky[n]) / visc;
           double sym_south_temp = -y_coeff * UPSTREAM(updir, 0.0, prod, prod_no) * y_dir_g_c;
           south_temp = -y_coeff * diff * UPSTREAM(updir, 0.0, prod_der, 0.0) * y_dir_g_c + sym_south_temp;
           south_temp += (y_coeff * dy * UPSTREAM(updir, 0.0, prod_der, 0.0)) * y_dir_g;
@@ -1003,7 +1023,8 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           double lower_cond = p[c] / sep - (zc / (zc + zu)) * rho * g;
           double upper_cond = p[u] / sep + (zu / (zc + zu)) * rho * g;
           double diff = lower_cond - upper_cond;
-          double z_coeff = 1.0 * dt * ffz * HARMONIC_DZ(pb->kz[c], pb->kz[u], zc, zu) / visc;
+          double z_coeff = (pb->fbz ? pb->fbz[c] : 1.0) * dt * ffz *
+                           HARMONIC_DZ(pb->kz[c], pb->kz[u], zc, zu) / visc;
           double sym_lower_temp = -z_coeff * (1.0 / (dz * AMEAN(zc, zu)))
                                   * UPSTREAM(lower_cond, upper_cond, prod, prod_up);
           lower_temp = -z_coeff * (diff * UPSTREAM(lower_cond, upper_cond, prod_der, 0.0)
@@ -1121,10 +1142,22 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
           cp[c] += 0.0;
       }
 
+  /* the "simple" diagonal term of an OverlandFlow patch in the
+   * difference-quotient mode; the z_mult ghost above the top layer keeps
+   * the 1 it was initialised with (problem_dz_scale.c:92) */
+  if (fd && pb->bc_type[5] == PFO_BC_OVERLAND)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        if (p[c] > 0.0)
+          cp[c] += (vol * zm[nz - 1]) / (dz * AMEAN(zm[nz - 1], 1.0)) * (dt + 1);
+      }
+
   /* kinematic overland terms on the top layer, MGSemi form (:1863-1990),
    * after every other term.  In the symmetric storage a lower coefficient is
    * the neighbour's upper one (matrix.c:484-490): W(i) = E(i-1), S(j) = N(j-1). */
-  if (pb->bc_type[5] == PFO_BC_OVERLAND_KIN)
+  if (!fd && pb->bc_type[5] == PFO_BC_OVERLAND_KIN)
   {
     const int sy2 = nx + 2;
     long n2 = (long)(nx + 2) * (ny + 2);
@@ -1168,7 +1201,7 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
   /* OverlandFlow terms on the top layer, MGSemi form (:2028-2090): the
    * derivative parts of each column's own flux; the spin-up damping term
    * of a non-ponded cell is zero with its default parameters */
-  if (pb->bc_type[5] == PFO_BC_OVERLAND)
+  if (!fd && pb->bc_type[5] == PFO_BC_OVERLAND)
   {
     const int sy2 = nx + 2;
     long n2 = (long)(nx + 2) * (ny + 2);
@@ -1209,7 +1242,7 @@ void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
   }
   /* diffusive overland terms on the top layer, MGSemi form (:1989-2026):
    * off-diagonals from the non-symmetric derivative parts of this column */
-  if (pb->bc_type[5] == PFO_BC_OVERLAND_DIFF)
+  if (!fd && pb->bc_type[5] == PFO_BC_OVERLAND_DIFF)
   {
     const int sy2 = nx + 2;
     long n2 = (long)(nx + 2) * (ny + 2);
@@ -1280,7 +1313,10 @@ void pfo_matvec7(const pfo_problem *pb, double *const *J, const double *x, doubl
  * MGSemi  (PL/mg_semi.c, mg_semi_restrict.c, mg_semi_prolong.c, rb_GS_point.c)
  * Every level stores a symmetric 7-point operator as C E N U; the lower
  * entries are the upper entries of the neighbour (PL/matrix.c:258-310,
- * 477-490).  Boundary-face coefficients are zero.
+ * 477-490).  Boundary-face coefficients are zero.  With PCMatrixType
+ * FullJacobian the finest operator is the non-symmetric Jacobian, whose
+ * lower entries W S L are stored apart (richards_jacobian_eval.c:2246-2258);
+ * the coarse operators are symmetric all the same (mg_semi.c:1071-1072).
  * ------------------------------------------------------------------------- */
 typedef struct {
   int nx, ny, nz;
@@ -1292,6 +1328,11 @@ typedef struct {
   double *wg;         /* (ny*nz) W entries of the i = 0 cells: the x_lower ghost column
                        * of E in the symmetric storage; zero unless the finest
                        * operator has one (diffusive overland terms) */
+  double *sg, *lg;    /* (nx*nz) S entries of the j = 0 cells and (nx*ny) L entries
+                       * of the k = 0 cells: the y_lower / z_lower ghost planes of
+                       * N and U, which the setup of a coarse operator writes */
+  double *lo[3];      /* W S L of a non-symmetric operator (finest level with
+                       * FullJacobian), else NULL */
 } mg_level;
 
 struct pfo_mg {
@@ -1313,6 +1354,10 @@ static void lvl_alloc(mg_level *l, int nx, int ny, int nz)
   l->p1 = (double*)calloc(l->n, sizeof(double));
   l->p2 = (double*)calloc(l->n, sizeof(double));
   l->wg = (double*)calloc((size_t)ny * nz, sizeof(double));
+  l->sg = (double*)calloc((size_t)nx * nz, sizeof(double));
+  l->lg = (double*)calloc((size_t)nx * ny, sizeof(double));
+  for (int s = 0; s < 3; s++)
+    l->lo[s] = NULL;
 }
 
 /* coarsening directions: PL/mg_semi.c:858-923 */
@@ -1374,26 +1419,32 @@ void pfo_mg_destroy(pfo_mg *mg)
     mg_level *l = &mg->L[i];
     for (int s = 0; s < 4; s++) free(l->a[s]);
     free(l->x); free(l->b); free(l->t); free(l->p1); free(l->p2); free(l->wg);
+    free(l->sg); free(l->lg);
+    for (int s = 0; s < 3; s++) free(l->lo[s]);
   }
   free(mg->L);
   free(mg);
 }
 
 /* Full 7-point coefficient s (0..6 = C W E S N L U) at (i,j,k) of a level,
- * from the symmetric C E N U storage; zero outside the level. */
+ * from the symmetric C E N U storage (the lower entries of the first
+ * row / column / plane from the ghost arrays) or from the W S L arrays of a
+ * non-symmetric level; zero outside the level. */
 static double coef(const mg_level *l, int s, int i, int j, int k)
 {
   int nx = l->nx, ny = l->ny, nz = l->nz;
   if (i < 0 || j < 0 || k < 0 || i >= nx || j >= ny || k >= nz)
     return 0.0;
+  if (l->lo[0] && (s == 1 || s == 3 || s == 5))
+    return l->lo[(s - 1) / 2][IDX(i, j, k)];
   switch (s)
   {
     case 0: return l->a[0][IDX(i, j, k)];
     case 1: return (i > 0) ? l->a[1][IDX(i - 1, j, k)] : l->wg[j + (long)ny * k];
     case 2: return l->a[1][IDX(i, j, k)];
-    case 3: return (j > 0) ? l->a[2][IDX(i, j - 1, k)] : 0.0;
+    case 3: return (j > 0) ? l->a[2][IDX(i, j - 1, k)] : l->sg[i + (long)nx * k];
     case 4: return l->a[2][IDX(i, j, k)];
-    case 5: return (k > 0) ? l->a[3][IDX(i, j, k - 1)] : 0.0;
+    case 5: return (k > 0) ? l->a[3][IDX(i, j, k - 1)] : l->lg[i + (long)nx * j];
     default: return l->a[3][IDX(i, j, k)];
   }
 }
@@ -1428,11 +1479,41 @@ void pfo_mg_set_wghost(pfo_mg *mg, const double *wg)
     memset(L0->wg, 0, n * sizeof(double));
 }
 
+static void mg_setup_levels(pfo_mg *mg);
+
 void pfo_mg_setup(pfo_mg *mg, double *const *A4)
 {
   mg_level *L0 = &mg->L[0];
   for (int s = 0; s < 4; s++)
     memcpy(L0->a[s], A4[s], L0->n * sizeof(double));
+  for (int s = 0; s < 3; s++)
+  {
+    free(L0->lo[s]);
+    L0->lo[s] = NULL;
+  }
+  mg_setup_levels(mg);
+}
+
+/* PCMatrixType FullJacobian: the finest operator is the full Jacobian
+ * C W E S N L U (kinsol_pc.c:215-246 -> richards_jacobian_eval.c with
+ * symm_part 0) */
+void pfo_mg_setup_full(pfo_mg *mg, double *const *A7)
+{
+  mg_level *L0 = &mg->L[0];
+  static const int up[4] = { 0, 2, 4, 6 }, dn[3] = { 1, 3, 5 };
+  for (int s = 0; s < 4; s++)
+    memcpy(L0->a[s], A7[up[s]], L0->n * sizeof(double));
+  for (int s = 0; s < 3; s++)
+  {
+    if (!L0->lo[s])
+      L0->lo[s] = (double*)malloc(L0->n * sizeof(double));
+    memcpy(L0->lo[s], A7[dn[s]], L0->n * sizeof(double));
+  }
+  mg_setup_levels(mg);
+}
+
+static void mg_setup_levels(pfo_mg *mg)
+{
   for (int li = 0; li + 1 < mg->nlev; li++)
   {
     mg_level *F = &mg->L[li], *Cl = &mg->L[li + 1];
@@ -1487,35 +1568,29 @@ void pfo_mg_setup(pfo_mg *mg, double *const *A4)
           ac[0][cc] = coef(F, s[0], i, j, k) + coef(F, s[3], i, j, k) + coef(F, s[4], i, j, k)
                       + coef(F, s[5], i, j, k) + coef(F, s[6], i, j, k)
                       + coef(F, s[1], i, j, k) * p2_1 + coef(F, s[2], i, j, k) * p1_2;
-          /* the coarse W entry of an i = 0 cell goes to the coarse ghost
-           * column (mg_semi.c:671-677 through the symmetric aliasing); along
-           * x it is W times the (zero) weight of the fine ghost point */
-          if (ic == 0)
-          {
-            double wc = 0.0;
-            for (int q = 1; q <= 6; q++)
-              if (s[q] == 1) wc = ac[q][cc];
-            Cl->wg[jc + (long)cny * kc] = wc;
-          }
         }
-    /* symmetric storage of the coarse operator: an upper entry is last
-     * written through its neighbour's lower entry when that neighbour exists */
-    long dstep = dir == 0 ? 1 : dir == 1 ? cnx : (long)cnx * cny;
+    /* symmetric storage of the coarse operator (the loop of mg_semi.c:667-687
+     * runs over the coarse cells in order): a lower entry written by a cell
+     * lands in the upper entry of its lower neighbour, so an upper entry is
+     * the one its upper neighbour wrote as a lower entry when that neighbour
+     * exists, and the lower entries of the first row / column / plane stay
+     * in the ghost arrays.  For a symmetric fine operator both writes carry
+     * the same value. */
+    int q_of[7];
+    for (int q = 0; q < 7; q++)
+      q_of[s[q]] = q;
+    const long csy = cnx, csz = (long)cnx * cny;
     for (int kc = 0; kc < Cl->nz; kc++)
       for (int jc = 0; jc < Cl->ny; jc++)
         for (int ic = 0; ic < Cl->nx; ic++)
         {
-          long cc = ic + (long)cnx * (jc + (long)cny * kc);
-          int last = dir == 0 ? (ic + 1 >= Cl->nx) : dir == 1 ? (jc + 1 >= Cl->ny) : (kc + 1 >= Cl->nz);
-          double along_up = last ? ac[2][cc] : ac[1][cc + dstep];
-          /* map reordered entries back to C E N U */
-          double E, Nn, U;
-          if (dir == 0) { E = along_up; Nn = ac[4][cc]; U = ac[6][cc]; }
-          else if (dir == 1) { E = ac[4][cc]; Nn = along_up; U = ac[6][cc]; }
-          else { E = ac[6][cc]; Nn = ac[4][cc]; U = along_up; }
-          Cl->a[1][cc] = E;
-          Cl->a[2][cc] = Nn;
-          Cl->a[3][cc] = U;
+          long cc = ic + csy * jc + csz * kc;
+          Cl->a[1][cc] = ic + 1 < cnx ? ac[q_of[1]][cc + 1] : ac[q_of[2]][cc];
+          Cl->a[2][cc] = jc + 1 < cny ? ac[q_of[3]][cc + csy] : ac[q_of[4]][cc];
+          Cl->a[3][cc] = kc + 1 < Cl->nz ? ac[q_of[5]][cc + csz] : ac[q_of[6]][cc];
+          if (ic == 0) Cl->wg[jc + (long)cny * kc] = ac[q_of[1]][cc];
+          if (jc == 0) Cl->sg[ic + (long)cnx * kc] = ac[q_of[3]][cc];
+          if (kc == 0) Cl->lg[ic + (long)cnx * jc] = ac[q_of[5]][cc];
         }
     /* centre: ac0 -= (ac3 + ac4 + ac5 + ac6), the transverse entries as stored */
     for (int kc = 0; kc < Cl->nz; kc++)
@@ -1735,6 +1810,7 @@ typedef struct {
   long N;
   double *J[7];
   double *PC[5];   /* C E N U, and the W ghost plane of the i = 0 column */
+  double *PC7[7];  /* the full preconditioner matrix (PCMatrixType FullJacobian) */
   pfo_mg *mg;
   pfo_stats *stats;
   const double *fval;   /* F at the Newton iterate (difference quotients) */
@@ -2015,6 +2091,8 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
   for (int s = 0; s < 7; s++) kc.J[s] = (double*)malloc(N * sizeof(double));
   for (int s = 0; s < 4; s++) kc.PC[s] = (double*)malloc(N * sizeof(double));
   kc.PC[4] = (double*)malloc((long)pb->ny * pb->nz * sizeof(double));
+  for (int s = 0; s < 7; s++)
+    kc.PC7[s] = st->pc_full ? (double*)malloc(N * sizeof(double)) : NULL;
   kc.mg = pfo_mg_create(pb, st);
 
   double *uu = p;
@@ -2068,9 +2146,17 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
     double eps = (eta + uround) * fnorm;
     if (eps < epsmin) eps = epsmin;
     /* KINLinSolDrv: preconditioner setup every iteration (msbpre = 1) */
-    pfo_jacobian(pb, dt, uu, 2, kc.PC);
-    pfo_mg_set_wghost(kc.mg, kc.PC[4]);
-    pfo_mg_setup(kc.mg, kc.PC);
+    if (st->pc_full)
+    {
+      pfo_jacobian_fd(pb, dt, uu, 0, !st->use_jacobian, kc.PC7);
+      pfo_mg_setup_full(kc.mg, kc.PC7);
+    }
+    else
+    {
+      pfo_jacobian_fd(pb, dt, uu, 2, !st->use_jacobian, kc.PC);
+      pfo_mg_set_wghost(kc.mg, kc.PC[4]);
+      pfo_mg_setup(kc.mg, kc.PC);
+    }
     stats->npe++;
     for (long q = 0; q < N; q++) bb[q] = -fval[q];
     int jac_current = 0;
@@ -2259,10 +2345,15 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
       sret2 = 1;
     else
     {
+      /* KS/kinsol.c:1540-1541 form the step in vtemp1 and pass it to
+       * KINScSteplength (:1490-1498), which first overwrites vtemp1 with
+       * 1/uscale + |unew| and then divides vtemp1 by itself: every component
+       * is 1, and so is the scaled step length */
       double rlength = 0.0;
       for (long q = 0; q < N; q++)
       {
-        double v = (unew[q] - uu[q]) / (1.0 / 1.0 + fabs(unew[q]));
+        double w = 1.0 / 1.0 + fabs(unew[q]);
+        double v = w / w;
         if (fabs(v) > rlength) rlength = fabs(v);
       }
       if (rlength <= scsteptol)
@@ -2289,6 +2380,7 @@ void pfo_newton_solve(const pfo_problem *pb_in, const pfo_settings *st, double d
 out:
   for (int s = 0; s < 7; s++) free(kc.J[s]);
   for (int s = 0; s < 5; s++) free(kc.PC[s]);
+  for (int s = 0; s < 7; s++) free(kc.PC7[s]);
   pfo_mg_destroy(kc.mg);
   free(fval); free(unew); free(pp); free(bb); free(kc.dq_u); free(kc.dq_f);
 }

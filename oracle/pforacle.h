@@ -63,6 +63,10 @@ typedef struct {
   /* land-surface sink/source per cell [1/h] (the evap_trans vector), or
    * NULL = 0 (nl_function_eval.c:533-541) */
   const double *evap_trans;
+  /* flow-barrier multipliers of the faces between cell (i,j,k) and its +x /
+   * +y / +z neighbour (Solver.Nonlinear.FlowBarrierX/Y/Z, problem_FBx.c), or
+   * NULL = 1; nl_function_eval.c:841-843, richards_jacobian_eval.c:662-728 */
+  const double *fbx, *fby, *fbz;
 } pfo_problem;
 
 typedef struct {
@@ -78,6 +82,9 @@ typedef struct {
   double derivative_epsilon;       /* Solver.Nonlinear.DerivativeEpsilon */
   int globalization;               /* Solver.Nonlinear.Globalization: 0 LineSearch,
                                     * 1 InexactNewton */
+  int pc_full;                     /* Solver.Linear.Preconditioner.PCMatrixType:
+                                    * 1 FullJacobian, 0 the symmetric part
+                                    * (PFSymmetric, SymmetricPart, Picard) */
 } pfo_settings;
 
 typedef struct {
@@ -111,6 +118,11 @@ void pfo_residual(const pfo_problem *pb, double dt, const double *p,
  * i = 0 cells (symm=2) (richards_jacobian_eval.c:217-1420) */
 void pfo_jacobian(const pfo_problem *pb, double dt, const double *p, int symm,
                   double *const *J);
+/* the same; fd = 1 builds the matrix of Solver.Nonlinear.UseJacobian False
+ * (no overland surface terms; richards_jacobian_eval.c:1241-1254, 1863,
+ * 2476-2484) */
+void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm, int fd,
+                     double *const *J);
 
 /* y = J x for a full 7-array stencil matrix (matvec.c:35-330) */
 void pfo_matvec7(const pfo_problem *pb, double *const *J, const double *x, double *y);
@@ -119,6 +131,9 @@ void pfo_matvec7(const pfo_problem *pb, double *const *J, const double *x, doubl
 typedef struct pfo_mg pfo_mg;
 pfo_mg *pfo_mg_create(const pfo_problem *pb, const pfo_settings *st);
 void pfo_mg_setup(pfo_mg *mg, double *const *A4);
+/* the same on the full non-symmetric C,W,E,S,N,L,U level-0 matrix
+ * (PCMatrixType FullJacobian) */
+void pfo_mg_setup_full(pfo_mg *mg, double *const *A7);
 /* W entries (ny*nz) of the finest operator's i = 0 cells, or NULL for none;
  * read by the next pfo_mg_setup */
 void pfo_mg_set_wghost(pfo_mg *mg, const double *wg);

@@ -6,6 +6,8 @@ reference CPU build and the oracle finish in seconds.
 
 from __future__ import annotations
 
+import numpy as np
+
 from . import configs
 from .problem import (BC, BC_DIRICHLET, BC_FLUX, BC_OVERLAND, BC_OVERLAND_DIFF, BC_SEEPAGE,
                       RichardsProblem,
@@ -222,6 +224,59 @@ def inexact_small() -> RichardsProblem:
                           solver=SolverSettings(globalization="InexactNewton"))
 
 
+def flow_barrier_small() -> RichardsProblem:
+    """Flow barriers (Solver.Nonlinear.FlowBarrierX/Y/Z with PFB fields, as
+    the reference's richards_FBx / FBy tests): a near-closed x barrier
+    between columns 5 and 6, a partial y barrier and a z barrier layer, all
+    on interior faces, on config-2 physics."""
+    prob = configs.hetero(nx=12, ny=11, nz=9, nsteps=2, seed=67)
+    fbx = np.ones(prob.shape)
+    fbx[:, :, 5] = 0.001
+    fby = np.ones(prob.shape)
+    fby[:, 4, 2:9] = 0.1
+    fbz = np.ones(prob.shape)
+    fbz[3, :, :] = 0.5
+    prob.fbx, prob.fby, prob.fbz = fbx, fby, fbz
+    return prob
+
+
+def fulljac_small() -> RichardsProblem:
+    """PCMatrixType FullJacobian: the multigrid's finest operator is the full
+    non-symmetric Jacobian, the coarse operators symmetric
+    (mg_semi.c:1071-1072), on config-2 physics."""
+    return configs.hetero(nx=13, ny=11, nz=8, nsteps=2, seed=71,
+                          solver=SolverSettings(pc_matrix_type="FullJacobian"))
+
+
+def fulljac_overland_small() -> RichardsProblem:
+    """PCMatrixType FullJacobian with kinematic overland flow and
+    KINSOL's difference-quotient J v, the combination of the reference's
+    overland_tiltedV_MGSemiTest: the finest multigrid operator carries the
+    surface terms' non-symmetric entries."""
+    return configs.overland(nx=12, ny=10, nz=6, nsteps=3, seed=73, wt_depth=-0.02,
+                            mannings=1e-3, rain_steps=2, dry_steps=1,
+                            solver=SolverSettings(pc_matrix_type="FullJacobian",
+                                                  use_jacobian=False))
+
+
+def fulljac_diff_small() -> RichardsProblem:
+    """PCMatrixType FullJacobian with diffusive-wave overland routing, whose
+    surface terms reach the W entries of the first column."""
+    return configs.overland(nx=12, ny=10, nz=6, nsteps=3, dt=0.05, seed=79, wt_depth=-0.02,
+                            mannings=1e-3, rain_steps=2, dry_steps=1, kind=BC_OVERLAND_DIFF,
+                            solver=SolverSettings(pc_matrix_type="FullJacobian"))
+
+
+def dq_overland_flow_small() -> RichardsProblem:
+    """The OverlandFlow patch with KINSOL's difference-quotient J v: the
+    reference then builds the preconditioner without the surface terms and
+    with the diagonal term of its "simple" case on ponded top cells
+    (richards_jacobian_eval.c:1241-1254, 2476-2484)."""
+    return configs.overland(nx=12, ny=10, nz=6, nsteps=3, seed=83, wt_depth=-0.02,
+                            mannings=1e-3, rain_steps=2, dry_steps=1, kind=BC_OVERLAND,
+                            solver=SolverSettings(use_jacobian=False))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -231,7 +286,8 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "overland_flow_small", "seepage_small", "dq_small", "krtable_spline_small",
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
-          "picard_small", "inexact_small"]
+          "picard_small", "inexact_small", "flow_barrier_small", "fulljac_small",
+          "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

@@ -247,15 +247,14 @@ struct OpLineSearchIn {
 };
 // after a trial step: <f, f>, max |f| and max |unew - u| / (1 + |unew|)
 struct OpStepNorms {
-  static constexpr int K = 3;
-  const double *f, *unew, *u;
+  static constexpr int K = 2;
+  const double *f;
   double *dst[K];
   __device__ void setup() {}
   __device__ void acc(long long i, double *v) const {
-    const double fi = f[i], a = unew[i];
+    const double fi = f[i];
     v[0] = v[0] + fi * fi;
     v[1] = comb_max(v[1], fabs(fi));
-    v[2] = comb_max(v[2], fabs((a - u[i]) / (1.0 / 1.0 + fabs(a))));
   }
   __device__ static double comb(int q, double x, double y) {
     return q == 0 ? comb_sum(x, y) : comb_max(x, y);
@@ -320,10 +319,9 @@ void launch_linesearch_inputs(const double *jp, const double *f, const double *p
   OpLineSearchIn op{jp, f, p, u, {d_jp2, d_fjp, d_p2, d_plen}};
   reduce_multi(op, n, rb, st);
 }
-void launch_step_norms(const double *f, const double *unew, const double *u, long long n,
-                       double *d_f2, double *d_fmax, double *d_step, ReduceBuf rb,
+void launch_step_norms(const double *f, long long n, double *d_f2, double *d_fmax, ReduceBuf rb,
                        cudaStream_t st) {
-  OpStepNorms op{f, unew, u, {d_f2, d_fmax, d_step}};
+  OpStepNorms op{f, {d_f2, d_fmax}};
   reduce_multi(op, n, rb, st);
 }
 void launch_init_norms(const double *u, const double *f, long long n, double *d_u2,

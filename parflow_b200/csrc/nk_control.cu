@@ -28,13 +28,17 @@ constexpr int NEWTON_GUARD = 100000;
 __device__ __forceinline__ void setc(cudaGraphConditionalHandle h, bool v) {
   cudaGraphSetConditional(h, v ? 1u : 0u);
 }
+// KINStop's scaled step length (kinsol.c:1540-1541): the step is formed in
+// vtemp1, which KINScSteplength (kinsol.c:1490-1498) then overwrites with
+// 1/uscale + |unew| before dividing the step by it, so every component is
+// (1 + |unew|) / (1 + |unew|) and the length is 1
+__device__ __forceinline__ double kinstop_steplength() { return 1.0; }
 // the trial step's norms (launch_step_norms)
 __device__ __forceinline__ void take_trial(NkState *S, const double *dsc) {
   S->fevals++;
   S->fnormp = sqrt(dsc[D_F2]);
   S->f1normp = 0.5 * S->fnormp * S->fnormp;
   S->fmax = dsc[D_FMAX];
-  S->steplen_new = dsc[D_STEP];
 }
 }  // namespace
 
@@ -361,7 +365,7 @@ __global__ void k_nk_newton_end(NkState *S) {
     sret = 3;
   else if (S->fmax <= S->k.fnormtol)
     sret = 1;
-  else if (S->steplen_new <= S->k.scsteptol)
+  else if (kinstop_steplength() <= S->k.scsteptol)
     sret = 2;
   else if (S->nonlin_iters >= S->k.mxiter)
     sret = 4;

@@ -19,7 +19,7 @@ namespace pfgpu {
 enum {
   D_F2 = 0,  // <f, f>
   D_FMAX,    // max |f|
-  D_STEP,    // max |unew - u| / (1 + |unew|)
+  D_FREE,    // unused
   D_P2,      // <p, p>
   D_PLEN,    // max |p| / (1 + |u|)
   D_JP2,     // <Jp, Jp>
@@ -60,7 +60,7 @@ struct NkState {
   double fnorm, f1norm, eta, eps, mxnewtstep;
   // line search
   double sJpnorm, sfdotJp, pnorm, ratio, slpi, rlength, rlmin, rl, rlprev, rllo, rldiff, rlincr;
-  double alpha_cond, beta_cond, fnormp, f1normp, fmax, steplen_new, lam;
+  double alpha_cond, beta_cond, fnormp, f1normp, fmax, lam;
   int ncscmx, ret, globalret, maxStepTaken, nfesav, ls_it, ls_phase, scaled, refined, do_copy,
       cont;
   // GMRES

@@ -145,6 +145,7 @@ struct pfgpu_handle {
   // surface: 7 column arrays of ny*nx (TFG g sin / g cos of x and y slopes,
   // overland slopes x / y, Manning's n) in one allocation
   double *surf = nullptr;
+  double *fb[3] = {nullptr, nullptr, nullptr};  // flow barriers x, y, z (or none)
   double *bcv[6] = {nullptr};
   // state and work vectors (dense interior layout)
   double *u = nullptr;      // current iterate / handle pressure state
@@ -852,7 +853,11 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
 
     // KINLineSearch (kinsol.c:1228-1420)
     int globalret = 0, maxStepTaken = 0;
-    double fnormp = 0.0, f1normp = 0.0, fmax = 0.0, steplen_new = 0.0;
+    double fnormp = 0.0, f1normp = 0.0, fmax = 0.0;
+    // KINStop's scaled step length is 1 whatever the step (kinsol.c:1540-1541
+    // pass the step in the work vector that KINScSteplength, :1490-1498,
+    // overwrites with 1/uscale + |unew| before dividing by it)
+    const double steplen_new = 1.0;
     double pnorm = sqrt(hsc[D_P2]);
     double ratio = 1.0;
     const double alpha = 0.0001, beta = 0.9;
@@ -880,14 +885,12 @@ static int newton_impl(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
       }
       feval(h, unew, dt, h->fval);
       stats->fevals++;
-      launch_step_norms(h->fval, unew, u, N, dsc + D_F2, dsc + D_FMAX, dsc + D_STEP, h->rb,
-                        h->st);
+      launch_step_norms(h->fval, N, dsc + D_F2, dsc + D_FMAX, h->rb, h->st);
       h->launches += 2;
-      if (read_scalars(h, 0, 3)) return PFGPU_ERR_CUDA;
+      if (read_scalars(h, 0, 2)) return PFGPU_ERR_CUDA;
       fnormp = sqrt(hsc[D_F2]);
       f1normp = 0.5 * fnormp * fnormp;
       fmax = hsc[D_FMAX];
-      steplen_new = hsc[D_STEP];
       return 0;
     };
     if (h->globalization == PFGPU_GLOBAL_INEXACT_NEWTON) {
@@ -1110,8 +1113,7 @@ static void nk_try_step(pfgpu_handle *h, double dt) {
   double *dsc = h->dsc;
   launch_xpay_lam(h->unew, h->u, &h->nk.S->lam, h->pp, N, h->st);
   feval(h, h->unew, dt, h->fval);
-  launch_step_norms(h->fval, h->unew, h->u, N, dsc + D_F2, dsc + D_FMAX, dsc + D_STEP, h->rb,
-                    h->st);
+  launch_step_norms(h->fval, N, dsc + D_F2, dsc + D_FMAX, h->rb, h->st);
   h->launches += 2;
 }
 
@@ -2144,6 +2146,7 @@ static void destroy_impl(pfgpu_handle *h) {
   if (h->ky && h->ky != h->kx) cudaFree(h->ky);
   if (h->kz && h->kz != h->kx && h->kz != h->ky) cudaFree(h->kz);
   for (int f = 0; f < 6; f++) cudaFree(h->bcv[f]);
+  for (double *f : h->fb) cudaFree(f);
   for (int f = 0; f < 6; f++) cudaFree(h->cyc[f].table);
   for (auto v : h->V) cudaFree(v);
   for (auto v : h->Z) cudaFree(v);
@@ -2241,6 +2244,22 @@ void pfgpu_destroy(pfgpu_handle *h) {
 int pfgpu_set_field(pfgpu_handle *h, int field, const double *values) {
   if (!h) { set_err("pfgpu_set_field: null handle"); return PFGPU_ERR_ARG; }
   CK(cudaSetDevice(h->device));
+  if (field >= PFGPU_FIELD_FB_X && field <= PFGPU_FIELD_FB_Z) {
+    double *&fb = h->fb[field - PFGPU_FIELD_FB_X];
+    if (!values) {
+      CK(cudaStreamSynchronize(h->st));
+      cudaFree(fb);
+      fb = nullptr;
+    } else {
+      if (!fb && dalloc(&fb, h->N)) return PFGPU_ERR_NOMEM;
+      if (in_vec(h, values, fb)) return PFGPU_ERR_CUDA;
+      CK(cudaStreamSynchronize(h->st));
+    }
+    h->P.fbx = h->fb[0];
+    h->P.fby = h->fb[1];
+    h->P.fbz = h->fb[2];
+    return PFGPU_OK;
+  }
   if (!values) {
     // drop a per-cell van Genuchten array: the descriptor scalar serves again
     double **vg = field == PFGPU_FIELD_VG_ALPHA ? &h->alpha
@@ -2362,7 +2381,7 @@ int pfgpu_write_pfb(pfgpu_handle *h, int what, const char *path, double x0, doub
 
 int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path) {
   if (!h || !path) { set_err("pfgpu_read_pfb: null argument"); return PFGPU_ERR_ARG; }
-  if (what != PFGPU_PFB_PRESSURE && (what < PFGPU_FIELD_PERM_X || what > PFGPU_FIELD_S_SAT)) {
+  if (what != PFGPU_PFB_PRESSURE && (what < PFGPU_FIELD_PERM_X || what > PFGPU_FIELD_FB_Z)) {
     set_err("pfgpu_read_pfb: unknown field %d", what);
     return PFGPU_ERR_ARG;
   }
@@ -3167,6 +3186,10 @@ int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps
   }
   if (h->P.krt) {
     set_err("pfgpu_adjoint_gradient: not available with a relative-permeability table");
+    return PFGPU_ERR_STATE;
+  }
+  if (h->P.fbx || h->P.fby || h->P.fbz) {
+    set_err("pfgpu_adjoint_gradient: not available with flow barriers");
     return PFGPU_ERR_STATE;
   }
   if (h->P.bc_type[5] == PFGPU_BC_OVERLAND_DIFF) {

@@ -24,6 +24,9 @@ struct DevProblem {
   double alpha0, vgn0, sres0, ssat0;
   int vg_from_file;
   const double *kx, *ky, *kz;   // per cell
+  // flow-barrier multipliers of the faces to the +x / +y / +z neighbour, or
+  // null (1 everywhere)
+  const double *fbx, *fby, *fbz;
   const double *zmult;          // per layer
   // per z face between layers k and k+1: 1/sep, z_k/(z_k+z_k+1), z_k+1/(z_k+z_k+1)
   const double *zface;          // 3*nz
@@ -224,6 +227,18 @@ __device__ __forceinline__ VGAll vg_all(const DevProblem &P, double p, const VG 
 // gravity terms x_dir_g / x_dir_g_c (tfg_face_x).
 // a = lower/left cell, b = upper/right cell.
 // ---------------------------------------------------------------------------
+// flow-barrier multiplier of the face between cell c and its +x / +y / +z
+// neighbour (nl_function_eval.c:841-843)
+__device__ __forceinline__ double fb_x(const DevProblem &P, long long c) {
+  return P.fbx ? __ldg(P.fbx + c) : 1.0;
+}
+__device__ __forceinline__ double fb_y(const DevProblem &P, long long c) {
+  return P.fby ? __ldg(P.fby + c) : 1.0;
+}
+__device__ __forceinline__ double fb_z(const DevProblem &P, long long c) {
+  return P.fbz ? __ldg(P.fbz + c) : 1.0;
+}
+
 __device__ __forceinline__ double flux_x(const DevProblem &P, double pa, double pb, double ka,
                                          double kb, double kra, double krb, double zm,
                                          double x_dir_g, double x_dir_g_c) {

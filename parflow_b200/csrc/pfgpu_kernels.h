@@ -299,8 +299,7 @@ void launch_axpy_dot(double *y, const double *x, const double *s, double sign, c
 void launch_linesearch_inputs(const double *jp, const double *f, const double *p,
                               const double *u, long long n, double *d_jp2, double *d_fjp,
                               double *d_p2, double *d_plen, ReduceBuf rb, cudaStream_t st);
-void launch_step_norms(const double *f, const double *unew, const double *u, long long n,
-                       double *d_f2, double *d_fmax, double *d_step, ReduceBuf rb,
+void launch_step_norms(const double *f, long long n, double *d_f2, double *d_fmax, ReduceBuf rb,
                        cudaStream_t st);
 void launch_init_norms(const double *u, const double *f, long long n, double *d_u2,
                        double *d_fmax, double *d_f2, ReduceBuf rb, cudaStream_t st);

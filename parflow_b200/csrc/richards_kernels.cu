@@ -267,33 +267,39 @@ __global__ void __launch_bounds__(256, 5) k_residual(DevProblem P, const double 
     long long l = c - sz;
     double zl = __ldg(P.zmult + k - 1);
     fl_z = flux_z(P, p[l], pc, __ldg(P.kz + l), kzc, kr[l], krc, zl, zm, k - 1);
+    if (P.fbz) fl_z = fl_z * fb_z(P, l);
   }
   double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
   if (j > 0) {
     long long s = c - sy;
     if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
     fl_y = flux_y(P, p[s], pc, __ldg(P.ky + s), kyc, kr[s], krc, zm, gs, gc);
+    if (P.fby) fl_y = fl_y * fb_y(P, s);
   }
   if (i > 0) {
     long long w = c - 1;
     if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
     fl_x = flux_x(P, p[w], pc, __ldg(P.kx + w), kxc, kr[w], krc, zm, gs, gc);
+    if (P.fbx) fl_x = fl_x * fb_x(P, w);
   }
   double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
   if (i + 1 < P.nx) {
     long long e = c + 1;
     if (SURF) tfg_face_x(P, i, j, gs, gc);
     u_right = flux_x(P, pc, p[e], kxc, __ldg(P.kx + e), krc, kr[e], zm, gs, gc);
+    if (P.fbx) u_right = u_right * fb_x(P, c);
   }
   if (j + 1 < P.ny) {
     long long nn = c + sy;
     if (SURF) tfg_face_y(P, i, j, gs, gc);
     u_front = flux_y(P, pc, p[nn], kyc, __ldg(P.ky + nn), krc, kr[nn], zm, gs, gc);
+    if (P.fby) u_front = u_front * fb_y(P, c);
   }
   if (k + 1 < P.nz) {
     long long u = c + sz;
     u_upper = flux_z(P, pc, p[u], kzc, __ldg(P.kz + u), krc, kr[u], zm,
                      __ldg(P.zmult + k + 1), k);
+    if (P.fbz) u_upper = u_upper * fb_z(P, c);
   }
   residual_cell<SURF, VEL>(P, i, j, k, c, p, p_old, s_old, kr, satv, dt, f, V, fl_z, fl_y, fl_x,
                            u_right, u_front, u_upper);
@@ -337,7 +343,8 @@ __global__ void __launch_bounds__(256) k_residual_zm(DevProblem P, const double 
   double fl_z = 0.0;
   if (in && k0 > 0 && k0 < k1)
     fl_z = flux_z(P, p[c - sz], p[c], __ldg(P.kz + c - sz), __ldg(P.kz + c), kr[c - sz], kr[c],
-                  __ldg(P.zmult + k0 - 1), __ldg(P.zmult + k0), k0 - 1);
+                  __ldg(P.zmult + k0 - 1), __ldg(P.zmult + k0), k0 - 1) *
+           fb_z(P, c - sz);
   for (int k = k0; k < k1; k++, c += sz) {
     double u_right = 0.0, u_front = 0.0, u_upper = 0.0;
     if (in) {
@@ -346,20 +353,26 @@ __global__ void __launch_bounds__(256) k_residual_zm(DevProblem P, const double 
       const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
       const double krc = kr[c];
       if (i + 1 < P.nx)
-        u_right = flux_x(P, pc, p[c + 1], kxc, __ldg(P.kx + c + 1), krc, kr[c + 1], zm, gse, gce);
+        u_right = flux_x(P, pc, p[c + 1], kxc, __ldg(P.kx + c + 1), krc, kr[c + 1], zm, gse,
+                         gce) *
+                  fb_x(P, c);
       if (j + 1 < P.ny)
         u_front = flux_y(P, pc, p[c + sy], kyc, __ldg(P.ky + c + sy), krc, kr[c + sy], zm, gsn,
-                         gcn);
+                         gcn) *
+                  fb_y(P, c);
       if (k + 1 < P.nz)
         u_upper = flux_z(P, pc, p[c + sz], kzc, __ldg(P.kz + c + sz), krc, kr[c + sz], zm,
-                         __ldg(P.zmult + k + 1), k);
+                         __ldg(P.zmult + k + 1), k) *
+                  fb_z(P, c);
       // the tile's west and south edge faces
       if (tx == 0 && i > 0)
         sE[ty * (bx + 1)] = flux_x(P, p[c - 1], pc, __ldg(P.kx + c - 1), kxc, kr[c - 1], krc, zm,
-                                   gsw, gcw);
+                                   gsw, gcw) *
+                            fb_x(P, c - 1);
       if (ty == 0 && j > 0)
         sN[tx] = flux_y(P, p[c - sy], pc, __ldg(P.ky + c - sy), kyc, kr[c - sy], krc, zm, gss,
-                        gcs);
+                        gcs) *
+                 fb_y(P, c - sy);
     }
     sE[ty * (bx + 1) + tx + 1] = u_right;
     sN[(ty + 1) * bx + tx] = u_front;
@@ -400,7 +413,8 @@ __device__ __forceinline__ TA pick(double a, double b, TA c, TA d) {
 }
 
 template <typename TA>
-__device__ __forceinline__ FaceDer<TA> face_der_xy(const DevProblem &P, double dt, double h_ff,
+__device__ __forceinline__ FaceDer<TA> face_der_xy(const DevProblem &P, double dt, double fb,
+                                                   double h_ff,
                                                    double dd, double inv_dd, double pa,
                                                    double pb, double ka, double kb, double prod,
                                                    double prod_der, double prod_rt,
@@ -409,7 +423,8 @@ __device__ __forceinline__ FaceDer<TA> face_der_xy(const DevProblem &P, double d
   const double diff64 = pa - pb;
   const double updir = (diff64 * inv_dd) * dir_g_c - dir_g;
   const TA diff = (TA)diff64;
-  const TA coeff = TA(1.0) * (TA)dt * (TA)h_ff * (TA)inv_dd * (TA)zm *
+  // x_coeff / y_coeff (richards_jacobian_eval.c:662, 692): FB * dt * ...
+  const TA coeff = (TA)fb * (TA)dt * (TA)h_ff * (TA)inv_dd * (TA)zm *
                    harmonic_t<TA>((TA)ka, (TA)kb) * (TA)P.inv_visc;
   const TA dgc = (TA)dir_g_c, dg = (TA)dir_g, tdd = (TA)dd;
   FaceDer<TA> r;
@@ -424,7 +439,8 @@ __device__ __forceinline__ FaceDer<TA> face_der_xy(const DevProblem &P, double d
 
 // z face between a (lower) and b (upper) (richards_jacobian_eval.c:697-745)
 template <typename TA>
-__device__ __forceinline__ FaceDer<TA> face_der_z(const DevProblem &P, double dt, double pa,
+__device__ __forceinline__ FaceDer<TA> face_der_z(const DevProblem &P, double dt, double fb,
+                                                  double pa,
                                                   double pb, double ka, double kb, double prod,
                                                   double prod_der, double prod_up,
                                                   double prod_up_der, double za, double zb,
@@ -435,7 +451,7 @@ __device__ __forceinline__ FaceDer<TA> face_der_z(const DevProblem &P, double dt
   double lower_cond = pa * inv_sep - __ldg(P.zface + 3 * k + 1) * rho * g;
   double upper_cond = pb * inv_sep + __ldg(P.zface + 3 * k + 2) * rho * g;
   const TA diff = (TA)(lower_cond - upper_cond);
-  const TA z_coeff = TA(1.0) * (TA)dt * ((TA)P.dx * (TA)P.dy) *
+  const TA z_coeff = (TA)fb * (TA)dt * ((TA)P.dx * (TA)P.dy) *
                      harmonic_dz_t<TA>((TA)ka, (TA)kb, (TA)za, (TA)zb) * (TA)P.inv_visc;
   const TA up = pick<TA>(lower_cond, upper_cond, (TA)prod, (TA)prod_up);
   const TA grav = (TA)(-g * 0.5 * dz * (amean(za, zb)) * drho);
@@ -741,42 +757,44 @@ __global__ void __launch_bounds__(128, 8) k_jacobian(DevProblem P, const double 
   FaceDer<TA> de{}, dn{}, du{};
   if (k > 0) {
     long long q = c - sz;
-    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], pc, __ldg(P.kz + q), kzc, kr[q] * rho,
-                           dkr[q] * rho + kr[q] * drho, prod, prod_der, __ldg(P.zmult + k - 1),
-                           zm, k - 1);
+    FaceDer<TA> d = face_der_z<TA>(P, dt, fb_z(P, q), p[q], pc, __ldg(P.kz + q), kzc,
+                                   kr[q] * rho, dkr[q] * rho + kr[q] * drho, prod, prod_der,
+                                   __ldg(P.zmult + k - 1), zm, k - 1);
     dl_z = {d.lo, d.hi};
   }
   double gs = 0.5 * (g * 0.0 + g * 0.0), gc = 0.5 * (g * 1.0 + g * 1.0);
   if (j > 0) {
     long long q = c - sy;
     if (SURF) tfg_face_y(P, i, j - 1, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q), kyc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, fb_y(P, q), ffy, P.dy, P.inv_dy, p[q], pc,
+                                    __ldg(P.ky + q), kyc, kr[q] * rho,
+                                    dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     dl_y = {d.lo, d.hi};
   }
   if (i > 0) {
     long long q = c - 1;
     if (SURF) tfg_face_x(P, i - 1, j, gs, gc);
-    FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q), kxc, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
+    FaceDer<TA> d = face_der_xy<TA>(P, dt, fb_x(P, q), ffx, P.dx, P.inv_dx, p[q], pc,
+                                    __ldg(P.kx + q), kxc, kr[q] * rho,
+                                    dkr[q] * rho + kr[q] * drho, prod, prod_der, zm, gs, gc);
     dl_x = {d.lo, d.hi};
   }
   if (i + 1 < P.nx) {
     long long q = c + 1;
     if (SURF) tfg_face_x(P, i, j, gs, gc);
-    de = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
+    de = face_der_xy<TA>(P, dt, fb_x(P, c), ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q),
+                         prod, prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
   }
   if (j + 1 < P.ny) {
     long long q = c + sy;
     if (SURF) tfg_face_y(P, i, j, gs, gc);
-    dn = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod, prod_der,
-                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
+    dn = face_der_xy<TA>(P, dt, fb_y(P, c), ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q),
+                         prod, prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gs, gc);
   }
   if (k + 1 < P.nz) {
     long long q = c + sz;
-    du = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
-                           dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
+    du = face_der_z<TA>(P, dt, fb_z(P, c), pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der,
+                        kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
   }
   jacobian_cell<TJ, TP, SURF>(P, i, j, k, c, p, kr, dkr, satv, dsatv, dt, J, M, dl_z, dl_y,
                               dl_x, de, dn, du);
@@ -817,7 +835,7 @@ __global__ void __launch_bounds__(256, 3) k_jacobian_zm(DevProblem P, const doub
   FaceLH<TA> dl_z{};
   if (in && k0 > 0 && k0 < k1) {
     const long long q = c - sz;
-    FaceDer<TA> d = face_der_z<TA>(P, dt, p[q], p[c], __ldg(P.kz + q), __ldg(P.kz + c),
+    FaceDer<TA> d = face_der_z<TA>(P, dt, fb_z(P, q), p[q], p[c], __ldg(P.kz + q), __ldg(P.kz + c),
                                    kr[q] * rho, dkr[q] * rho + kr[q] * drho, kr[c] * rho,
                                    dkr[c] * rho + kr[c] * drho, __ldg(P.zmult + k0 - 1),
                                    __ldg(P.zmult + k0), k0 - 1);
@@ -832,30 +850,35 @@ __global__ void __launch_bounds__(256, 3) k_jacobian_zm(DevProblem P, const doub
       const double kxc = __ldg(P.kx + c), kyc = __ldg(P.ky + c), kzc = __ldg(P.kz + c);
       if (i + 1 < P.nx) {
         const long long q = c + 1;
-        de = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, pc, p[q], kxc, __ldg(P.kx + q), prod,
-                             prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gse, gce);
+        de = face_der_xy<TA>(P, dt, fb_x(P, c), ffx, P.dx, P.inv_dx, pc, p[q], kxc,
+                             __ldg(P.kx + q), prod, prod_der, kr[q] * rho,
+                             dkr[q] * rho + kr[q] * drho, zm, gse, gce);
       }
       if (j + 1 < P.ny) {
         const long long q = c + sy;
-        dn = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, pc, p[q], kyc, __ldg(P.ky + q), prod,
-                             prod_der, kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm, gsn, gcn);
+        dn = face_der_xy<TA>(P, dt, fb_y(P, c), ffy, P.dy, P.inv_dy, pc, p[q], kyc,
+                             __ldg(P.ky + q), prod, prod_der, kr[q] * rho,
+                             dkr[q] * rho + kr[q] * drho, zm, gsn, gcn);
       }
       if (k + 1 < P.nz) {
         const long long q = c + sz;
-        du = face_der_z<TA>(P, dt, pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der, kr[q] * rho,
-                            dkr[q] * rho + kr[q] * drho, zm, __ldg(P.zmult + k + 1), k);
+        du = face_der_z<TA>(P, dt, fb_z(P, c), pc, p[q], kzc, __ldg(P.kz + q), prod, prod_der,
+                            kr[q] * rho, dkr[q] * rho + kr[q] * drho, zm,
+                            __ldg(P.zmult + k + 1), k);
       }
       if (tx == 0 && i > 0) {
         const long long q = c - 1;
-        FaceDer<TA> d = face_der_xy<TA>(P, dt, ffx, P.dx, P.inv_dx, p[q], pc, __ldg(P.kx + q),
-                                        kxc, kr[q] * rho, dkr[q] * rho + kr[q] * drho, prod,
+        FaceDer<TA> d = face_der_xy<TA>(P, dt, fb_x(P, q), ffx, P.dx, P.inv_dx, p[q], pc,
+                                        __ldg(P.kx + q), kxc, kr[q] * rho,
+                                        dkr[q] * rho + kr[q] * drho, prod,
                                         prod_der, zm, gsw, gcw);
         sE[ty * (bx + 1)] = {d.lo, d.hi};
       }
       if (ty == 0 && j > 0) {
         const long long q = c - sy;
-        FaceDer<TA> d = face_der_xy<TA>(P, dt, ffy, P.dy, P.inv_dy, p[q], pc, __ldg(P.ky + q),
-                                        kyc, kr[q] * rho, dkr[q] * rho + kr[q] * drho, prod,
+        FaceDer<TA> d = face_der_xy<TA>(P, dt, fb_y(P, q), ffy, P.dy, P.inv_dy, p[q], pc,
+                                        __ldg(P.ky + q), kyc, kr[q] * rho,
+                                        dkr[q] * rho + kr[q] * drho, prod,
                                         prod_der, zm, gss, gcs);
         sN[tx] = {d.lo, d.hi};
       }

@@ -18,6 +18,7 @@ BC_FLUX, BC_DIRICHLET, BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND, BC_SEEPAG
     0, 1, 2, 3, 4, 5
 FIELD_PERM_X, FIELD_PERM_Y, FIELD_PERM_Z = 0, 1, 2
 FIELD_VG_ALPHA, FIELD_VG_N, FIELD_S_RES, FIELD_S_SAT = 3, 4, 5, 6
+FIELD_FB_X, FIELD_FB_Y, FIELD_FB_Z = 7, 8, 9
 OK, NOT_CONVERGED = 0, 1
 
 _dp = C.POINTER(C.c_double)

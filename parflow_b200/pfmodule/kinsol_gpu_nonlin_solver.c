@@ -422,6 +422,23 @@ static void create_handle(GpuInstanceXtra *ix, GpuPublicXtra *px, Vector *pressu
       pfgpu_set_field(ix->h, PFGPU_FIELD_PERM_Z, SubvectorData(VectorSubvector(kz, 0))))
     gpu_fail(pfgpu_last_error());
 
+  /* flow barriers (problem_FBx.c etc.: 1 everywhere unless the key is on) */
+  {
+    static const char *const fkey[3] = {"Solver.Nonlinear.FlowBarrierX",
+                                        "Solver.Nonlinear.FlowBarrierY",
+                                        "Solver.Nonlinear.FlowBarrierZ"};
+    Vector *fb[3] = {ProblemDataFBx(pd), ProblemDataFBy(pd), ProblemDataFBz(pd)};
+    for (int q = 0; q < 3; q++)
+    {
+      NameArray fna = NA_NewNameArray("False True");
+      const int on = NA_NameToIndexExitOnError(fna, GetStringDefault(fkey[q], "False"), fkey[q]);
+      NA_FreeNameArray(fna);
+      if (on && pfgpu_set_field(ix->h, PFGPU_FIELD_FB_X + q,
+                                SubvectorData(VectorSubvector(fb[q], 0))) != PFGPU_OK)
+        gpu_fail(pfgpu_last_error());
+    }
+  }
+
   /* per-cell van Genuchten files */
   if (s_file)
   {

@@ -132,12 +132,7 @@ class SolverSettings:
         RBGaussSeidelNonSymmetric is one red and one black sweep,
         RBGaussSeidelSymmetric red, black, red, Jacobi a weight-1 Jacobi
         sweep."""
-        # KinsolPC's PCMatrixType (kinsol_pc.c:215-246) reaches the Jacobian
-        # evaluation as symm_part, which is only tested for zero
-        # (richards_jacobian_eval.c:760, 781, 2246): PFSymmetric,
-        # SymmetricPart and Picard build the same preconditioner matrix
-        if self.pc_matrix_type not in ("PFSymmetric", "SymmetricPart", "Picard"):
-            raise ValueError(f"PCMatrixType {self.pc_matrix_type} is not available")
+        self.pc_matrix_code()
         if self.preconditioner == "PFMG":
             table = {"RBGaussSeidelNonSymmetric": 2, "RBGaussSeidelSymmetric": 0, "Jacobi": 1}
             if self.pfmg_smoother not in table:
@@ -150,6 +145,17 @@ class SolverSettings:
         if self.mg_smoother != "RedBlackGSPoint":
             raise ValueError(f"unknown MGSemi smoother {self.mg_smoother}")
         return 0 if self.mg_smoother_symmetric else 2
+
+    def pc_matrix_code(self) -> int:
+        """Solver.Linear.Preconditioner.PCMatrixType (kinsol_pc.c:215-246):
+        1 FullJacobian, 0 the symmetric part.  The type reaches the Jacobian
+        evaluation as symm_part, which is only tested for zero
+        (richards_jacobian_eval.c:760, 781, 2246): PFSymmetric, SymmetricPart
+        and Picard build the same preconditioner matrix."""
+        table = {"FullJacobian": 1, "PFSymmetric": 0, "SymmetricPart": 0, "Picard": 0}
+        if self.pc_matrix_type not in table:
+            raise ValueError(f"PCMatrixType {self.pc_matrix_type} is not available")
+        return table[self.pc_matrix_type]
 
     def globalization_code(self) -> int:
         """Solver.Nonlinear.Globalization (kinsol_nonlin_solver.c:887-905):
@@ -205,6 +211,12 @@ class RichardsProblem:
     # land-surface sink/source per cell [1/h] (Solver.EvapTransFile /
     # Solver.EvapTrans.FileName): None, a float or an (nz, ny, nx) array
     evap_trans: object = None
+    # flow-barrier multipliers of the faces between a cell and its +x / +y /
+    # +z neighbour (Solver.Nonlinear.FlowBarrierX/Y/Z, FBx/FBy/FBz.Type
+    # PFBFile): None (1 everywhere) or an (nz, ny, nx) array
+    fbx: object = None
+    fby: object = None
+    fbz: object = None
     # reference output of the face velocities (Solver.PrintVelocities)
     print_velocities: bool = False
     # TimeStep.Type Growth: (initial step, growth factor, min step, max
@@ -600,6 +612,13 @@ class RichardsProblem:
                       self.dz, dist=True)
             k["Solver.EvapTransFile"] = True
             k["Solver.EvapTrans.FileName"] = "evap_trans.pfb"
+        for d, v in (("X", self.fbx), ("Y", self.fby), ("Z", self.fbz)):
+            if v is not None:
+                fn = f"fb{d.lower()}.pfb"
+                write_pfb(pj(fn), self.field3d(v), self.dx, self.dy, self.dz, dist=True)
+                k[f"Solver.Nonlinear.FlowBarrier{d}"] = True
+                k[f"FB{d.lower()}.Type"] = "PFBFile"
+                k[f"Geom.domain.FB{d.lower()}.FileName"] = fn
         if self.print_velocities:
             k["Solver.PrintVelocities"] = True
             if any(bc.kind in (BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND)

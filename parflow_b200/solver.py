@@ -105,6 +105,10 @@ class RichardsGPU:
         self._upload_fields()
         if prob.evap_trans is not None:
             self.set_evap_trans(prob.field3d(prob.evap_trans))
+        for fid, v in ((L.FIELD_FB_X, prob.fbx), (L.FIELD_FB_Y, prob.fby), (L.FIELD_FB_Z, prob.fbz)):
+            if v is not None:
+                L.check(self.lib.pfgpu_set_field(self.h, fid, _ptr(pad(prob.field3d(v)))),
+                        "set_field (flow barrier)")
         self.set_time(prob.start_time + prob.dt)
 
     def close(self):
