@@ -364,6 +364,21 @@ int pfgpu_solve_graph(pfgpu_handle *h, int mode);
 #define PFGPU_GLOBAL_INEXACT_NEWTON 1
 int pfgpu_set_globalization(pfgpu_handle *h, int strategy);
 
+/* Solver.Linear.Preconditioner.PCMatrixType (KinsolPCNewPublicXtra,
+ * kinsol_pc.c:215-246): PFGPU_PCM_SYMMETRIC for PFSymmetric, SymmetricPart
+ * and Picard (the reference builds the same symmetric matrix for the three:
+ * richards_jacobian_eval.c:760, 781), PFGPU_PCM_FULL for FullJacobian, where
+ * the multigrid's finest operator is the full non-symmetric Jacobian and its
+ * coarse operators are symmetric (mg_semi.c:1071-1072).  FullJacobian needs
+ * a red/black Gauss-Seidel smoother, at least two multigrid levels and the
+ * FP64 or FP32 multigrid (not PFGPU_PREC_MIXED_H16).  With
+ * pfgpu_set_jacobian_mode(h, 0, ...) the matrix is built as the reference
+ * builds it under UseJacobian False: without the overland surface terms
+ * (richards_jacobian_eval.c:1241-1254, 1863, 2476-2484). */
+#define PFGPU_PCM_SYMMETRIC 0
+#define PFGPU_PCM_FULL 1
+int pfgpu_set_pc_matrix(pfgpu_handle *h, int type);
+
 /* Device-resident time stepping: advances the handle's own pressure state by
  * nsteps steps of dt with the boundary tables already set, keeping every
  * vector on the GPU (the step body of AdvanceRichards,

@@ -1075,7 +1075,9 @@ void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm
           double prod_der = dkr[c] * rho + kr[c] * drho;
           double prod_val = kr_at(pb, value, pb->alpha[c], pb->n[c], 0) * den_d;
           double o_temp, coeff, diff;
-          double zu = (k + 1 < nz) ? zm[k + 1] : 0.0;
+          /* the z_mult ghost above the top layer keeps the 1 it was
+           * initialised with (problem_dz_scale.c:92) */
+          double zu = (k + 1 < nz) ? zm[k + 1] : 1.0;
           switch (face)
           {
             case 0:

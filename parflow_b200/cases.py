@@ -277,6 +277,16 @@ def dq_overland_flow_small() -> RichardsProblem:
                             solver=SolverSettings(use_jacobian=False))
 
 
+def dirichlet_top_small() -> RichardsProblem:
+    """A Dirichlet (constant head) top face: its Jacobian coefficient takes
+    the mean of the top layer's z multiplier and the ghost one above, which
+    keeps the 1 it was initialised with (richards_jacobian_eval.c:1168-1170,
+    problem_dz_scale.c:92)."""
+    p = configs.box(nx=10, ny=8, nz=6, nsteps=2, seed=5)
+    p.bc["z_upper"] = BC(BC_DIRICHLET, (-0.3,))
+    return p
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -287,7 +297,8 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "krtable_linear_small", "wjacobi_small", "rbgs_nonsym_small", "vel_small",
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
           "picard_small", "inexact_small", "flow_barrier_small", "fulljac_small",
-          "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small"]
+          "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small",
+          "dirichlet_top_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

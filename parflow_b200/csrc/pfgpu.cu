@@ -186,6 +186,7 @@ struct pfgpu_handle {
   // quotient with sqrt(DerivativeEpsilon)) and its two work vectors
   int use_jacobian = 1;
   int globalization = PFGPU_GLOBAL_LINE_SEARCH;  // Solver.Nonlinear.Globalization
+  int pc_matrix = PFGPU_PCM_SYMMETRIC;  // Solver.Linear.Preconditioner.PCMatrixType
   double sqrt_relfunc = 0.0;
   double *dq_w = nullptr, *dq_f = nullptr;
   double *krt = nullptr;  // relative-permeability lookup table (device)
@@ -383,27 +384,61 @@ static void feval(pfgpu_handle *h, const double *u, double dt, double *f) {
   ph_end(h, m, PH_FEVAL);
 }
 
+// the multigrid's finest operator as a full 7-array matrix (FullJacobian)
+template <typename T>
+static JacOut<T> level0_full(MG<T> &mg) {
+  MGLevel<T> &L = mg.L[0];
+  return JacOut<T>{L.a[0], L.lo[0], L.a[1], L.lo[1], L.a[2], L.lo[2], L.a[3]};
+}
+
+template <typename T>
+static void assemble_T(pfgpu_handle *h, MG<T> &mg, JacOut<T> &Jh, const double *u, double dt,
+                       bool want_J, bool want_M) {
+  // Solver.Nonlinear.UseJacobian False: the preconditioner matrix without
+  // the overland surface terms (PCOut::fd); J for a matvec keeps them
+  const int fd = want_M && !h->use_jacobian;
+  if (want_M && h->pc_matrix == PFGPU_PCM_FULL) {
+    // FullJacobian: the Jacobian itself is the finest multigrid operator
+    PCOut<T> M{};
+    M.fd = fd;
+    JacOut<T> L0 = level0_full(mg);
+    launch_jacobian<T, T>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, L0, M, h->st);
+    h->launches++;
+    if (want_J && !fd) {
+      T *const src[7] = {L0.c, L0.w, L0.e, L0.s, L0.n, L0.l, L0.u};
+      T *const dst[7] = {Jh.c, Jh.w, Jh.e, Jh.s, Jh.n, Jh.l, Jh.u};
+      for (int q = 0; q < 7; q++)
+        cudaMemcpyAsync(dst[q], src[q], h->N * sizeof(T), cudaMemcpyDeviceToDevice, h->st);
+      return;
+    }
+    if (!want_J) return;
+    want_M = false;
+  }
+  PCOut<T> M{};
+  if (want_M) M = {mg.L[0].a[0], mg.L[0].a[1], mg.L[0].a[2], mg.L[0].a[3], mg.L[0].wg, 0};
+  JacOut<T> J{};
+  if (want_J) J = Jh;
+  if (fd && want_M && want_J) {
+    // J with the surface terms, then the preconditioner without them
+    PCOut<T> none{};
+    launch_jacobian<T, T>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, none, h->st);
+    h->launches++;
+    J = JacOut<T>{};
+  }
+  M.fd = want_M ? fd : 0;
+  launch_jacobian<T, T>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
+  h->launches++;
+}
+
 // assemble J (full) and the preconditioner matrix at u (one pass); the VG
 // state of the last residual evaluation is reused when it was taken at u
 static void assemble(pfgpu_handle *h, const double *u, double dt, bool want_J, bool want_M,
                      bool reuse_vg = false) {
   vg_state(h, u, reuse_vg);
-  if (h->mixed) {
-    PCOut<float> M{};
-    if (want_M)
-      M = {h->mgf.L[0].a[0], h->mgf.L[0].a[1], h->mgf.L[0].a[2], h->mgf.L[0].a[3], h->mgf.L[0].wg};
-    JacOut<float> J{};
-    if (want_J) J = h->Jf;
-    launch_jacobian<float, float>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
-  } else {
-    PCOut<double> M{};
-    if (want_M)
-      M = {h->mgd.L[0].a[0], h->mgd.L[0].a[1], h->mgd.L[0].a[2], h->mgd.L[0].a[3], h->mgd.L[0].wg};
-    JacOut<double> J{};
-    if (want_J) J = h->Jd;
-    launch_jacobian<double, double>(h->P, u, h->kr, h->dkr, h->sat, h->dsat, dt, J, M, h->st);
-  }
-  h->launches++;
+  if (h->mixed)
+    assemble_T<float>(h, h->mgf, h->Jf, u, dt, want_J, want_M);
+  else
+    assemble_T<double>(h, h->mgd, h->Jd, u, dt, want_J, want_M);
 }
 
 static void matvec_impl(pfgpu_handle *h, const double *x, double *y) {
@@ -437,6 +472,8 @@ template <typename T>
 static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
   long long k = 0;
   const int nl = (int)mg.L.size();
+  // FullJacobian: every level from the generic setup (mg_full.cu)
+  if (mg.L[0].lo[0]) return launch_mg_full_setup<T>(mg.L.data(), nl, st);
   if (mg.h16) cudaMemsetAsync(mg.hflag, 0, sizeof(int), st);
   for (int l = 0; l < mg.tail && l + 1 < nl; l++) {
     launch_mg_setup_level<T>(mg.L[l], mg.L[l + 1], st, mg.h16);
@@ -480,6 +517,14 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
   };
   for (int l = 0; l < first; l++) {
     MGLevel<T> &Ll = mg.L[l];
+    if (Ll.lo[0]) {
+      // the non-symmetric finest operator of FullJacobian (mg_full.cu)
+      k += launch_mg_full_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother != PFGPU_SMOOTH_RBGS_NONSYM, st);
+      launch_mg_full_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st);
+      launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st, next(), mg.h16);
+      k += 2;
+      continue;
+    }
     if (mg.fused[l]) {
       launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x, 1, mg.kerr, st);  // zero guess: x not read
       k++;
@@ -520,7 +565,10 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
     const int skip_red = (smoother == PFGPU_SMOOTH_RBGS || smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
                          !mg.fused[l] && !mg.waved[l];
     launch_mg_prolong_add<T>(Ll, C, mg.res(l + 1), Ll.x, st, next(), mg.h16, skip_red);
-    if (mg.fused[l]) {
+    if (Ll.lo[0]) {
+      k += 1 + launch_mg_full_smooth<T>(Ll, Ll.x, Ll.b, 0,
+                                        smoother != PFGPU_SMOOTH_RBGS_NONSYM, st);
+    } else if (mg.fused[l]) {
       launch_rbr_fused<T>(Ll, mg.maps[l], Ll.x2, 0, mg.kerr, st);
       k += 2;
     } else if (mg.waved[l]) {
@@ -1303,7 +1351,7 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(&P, &h->P, sizeof(P));
   P.dtp = nullptr;
   const double *ptrs[2] = {h->u, h->unew};
-  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + 2 * sizeof(int) +
+  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + 3 * sizeof(int) +
                                sizeof(double));
   unsigned char *q = k.data();
   memcpy(q, &P, sizeof(P));
@@ -1317,6 +1365,8 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(q, &h->sqrt_relfunc, sizeof(double));
   q += sizeof(double);
   memcpy(q, &h->globalization, sizeof(int));
+  q += sizeof(int);
+  memcpy(q, &h->pc_matrix, sizeof(int));
   return k;
 }
 
@@ -1561,14 +1611,6 @@ static int newton_graph(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
 }
 
 static int newton(pfgpu_handle *h, double dt, pfgpu_stats *stats) {
-  const int ov = h->P.bc_type[5];
-  if (!h->use_jacobian && (ov == PFGPU_BC_OVERLAND_KIN || ov == PFGPU_BC_OVERLAND_DIFF ||
-                           ov == PFGPU_BC_OVERLAND)) {
-    // without the analytic Jacobian the reference builds the overland
-    // preconditioner terms in another form (richards_jacobian_eval.c:1244-1283)
-    set_err("difference-quotient J v (UseJacobian False) with an overland face is not available");
-    return PFGPU_ERR_STATE;
-  }
   h->nk.used_last = false;
   if (nk_usable(h)) {
     const int rc = nk_prepare(h);
@@ -1760,12 +1802,60 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   return 0;
 }
 
+// FullJacobian storage for a hierarchy: W S L on level 0, the S / L ghost
+// planes on every level, level 0 taken out of the fused / wavefront smoothers
+// and the single-block kernels (their kernels assume a symmetric operator)
+template <typename T>
+static int mg_enable_full(pfgpu_handle *h, MG<T> &mg) {
+  const int nl = (int)mg.L.size();
+  MGLevel<T> &L0 = mg.L[0];
+  if (!L0.lo[0])
+    for (int s = 0; s < 3; s++)
+      if (dalloc(&L0.lo[s], L0.n)) return PFGPU_ERR_NOMEM;
+  for (int l = 0; l < nl; l++) {
+    MGLevel<T> &L = mg.L[l];
+    if (!L.sg && (dalloc(&L.sg, (long long)L.nx * L.nz) || dalloc(&L.lg, (long long)L.nx * L.ny)))
+      return PFGPU_ERR_NOMEM;
+    CK(cudaMemset(L.sg, 0, (long long)L.nx * L.nz * sizeof(T)));
+    CK(cudaMemset(L.lg, 0, (long long)L.nx * L.ny * sizeof(T)));
+  }
+  if (nl > 1) {
+    if (mg.tail < 1) {
+      mg.tail = 1;
+      const size_t b = tail_smem_bytes<T>(mg.L.data(), 1, nl, mg.h16);
+      mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
+    }
+    if (mg.mid < 1) mg.mid = 1;
+  }
+  mg.fused[0] = 0;
+  mg.waved[0] = 0;
+  L0.split = (h->d.mg_smoother == PFGPU_SMOOTH_RBGS ||
+              h->d.mg_smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
+             env_ll("PFGPU_SPLIT", 1) != 0 && nl > 1;
+  L0.zc = -1;
+  CK(cudaMemcpy(mg.Ldev, mg.L.data(), nl * sizeof(MGLevel<T>), cudaMemcpyHostToDevice));
+  return PFGPU_OK;
+}
+template <typename T>
+static int mg_disable_full(MG<T> &mg) {
+  MGLevel<T> &L0 = mg.L[0];
+  for (int s = 0; s < 3; s++) {
+    cudaFree(L0.lo[s]);
+    L0.lo[s] = nullptr;
+  }
+  CK(cudaMemcpy(mg.Ldev, mg.L.data(), mg.L.size() * sizeof(MGLevel<T>),
+                cudaMemcpyHostToDevice));
+  return PFGPU_OK;
+}
+
 template <typename T>
 static void free_mg(MG<T> &mg) {
   for (auto &L : mg.L) {
     for (int s = 0; s < 4; s++) cudaFree(L.a[s]);
     cudaFree(L.x); cudaFree(L.b); cudaFree(L.t); cudaFree(L.p1); cudaFree(L.p2);
     cudaFree(L.x2); cudaFree(L.wg);
+    for (int s = 0; s < 3; s++) cudaFree(L.lo[s]);
+    cudaFree(L.sg); cudaFree(L.lg);
     for (int s = 0; s < 4; s++) cudaFree(L.h[s]);
     cudaFree(L.q1); cudaFree(L.q2); cudaFree(L.sinv);
   }
@@ -3045,6 +3135,46 @@ int pfgpu_solve_graph(pfgpu_handle *h, int mode) {
   if (mode == -1) return h->nk.used_last ? 1 : 0;
   set_err("pfgpu_solve_graph: mode must be 0, 1 or -1");
   return PFGPU_ERR_ARG;
+}
+
+int pfgpu_set_pc_matrix(pfgpu_handle *h, int type) {
+  if (!h || (type != PFGPU_PCM_SYMMETRIC && type != PFGPU_PCM_FULL)) {
+    set_err("pfgpu_set_pc_matrix: type must be PFGPU_PCM_SYMMETRIC or PFGPU_PCM_FULL");
+    return PFGPU_ERR_ARG;
+  }
+  if (type == h->pc_matrix) return PFGPU_OK;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->st));
+  int rc;
+  if (type == PFGPU_PCM_FULL) {
+    if (h->mixed && h->mgf.h16) {
+      set_err("PCMatrixType FullJacobian: not available with the scaled FP16 multigrid "
+              "(PFGPU_PREC_MIXED_H16)");
+      return PFGPU_ERR_ARG;
+    }
+    if (h->d.mg_smoother == PFGPU_SMOOTH_WJACOBI) {
+      set_err("PCMatrixType FullJacobian: not available with the WJacobi smoother");
+      return PFGPU_ERR_ARG;
+    }
+    if (h->nlev < 2) {
+      set_err("PCMatrixType FullJacobian: needs at least two multigrid levels");
+      return PFGPU_ERR_ARG;
+    }
+    rc = h->mixed ? mg_enable_full<float>(h, h->mgf) : mg_enable_full<double>(h, h->mgd);
+  } else {
+    rc = h->mixed ? mg_disable_full<float>(h->mgf) : mg_disable_full<double>(h->mgd);
+  }
+  if (rc != PFGPU_OK) return rc;
+  // the host-driven V-cycle graph holds the old level-0 path
+  if (h->vgraph) {
+    CK(cudaGraphExecDestroy(h->vgraph));
+    h->vgraph = nullptr;
+  }
+  if (build_vgraph(h)) return PFGPU_ERR_CUDA;
+  h->pc_matrix = type;
+  h->pc_ready = false;
+  h->jac_valid = 0;
+  return PFGPU_OK;
 }
 
 int pfgpu_set_globalization(pfgpu_handle *h, int strategy) {

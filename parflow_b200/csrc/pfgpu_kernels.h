@@ -25,10 +25,16 @@ struct JacIn {
 // S(i) = N(i-nx), L(i) = U(i-nx*ny) (pfsimulator/parflow_lib/matrix.c:258-310).
 // wg (ny*nz, optional): W of the i = 0 cells, i.e. the x_lower ghost column
 // of E, which only the diffusive overland terms make nonzero.
+// fd: the launch builds the preconditioner of Solver.Nonlinear.UseJacobian
+// False (into M, or into J for PCMatrixType FullJacobian), which the
+// reference assembles without the overland surface terms and with the
+// diagonal term of its "simple" case on ponded OverlandFlow cells
+// (richards_jacobian_eval.c:1241-1254, 1863, 2476-2484)
 template <typename T>
 struct PCOut {
   T *c, *e, *n, *u;
   T *wg;
+  int fd;
 };
 
 void launch_vg_all(const DevProblem &P, const double *p, double *kr, double *dkr, double *sat,
@@ -87,6 +93,13 @@ struct MGLevel {
   // (the colour it swept last: 0 red for red/black/red, 1 black for
   // red/black), or -1: every cell's residual is computed
   int zc;
+  // PCMatrixType FullJacobian (mg_full.cu): W S L of the non-symmetric
+  // finest operator (level 0 only, else null), and on every level the S of
+  // the j = 0 cells (nx*nz) and the L of the k = 0 cells (nx*ny), the
+  // y_lower / z_lower ghost planes of N and U that the setup of a coarse
+  // operator writes (the companions of wg); null in the symmetric mode
+  T *lo[3];
+  T *sg, *lg;
 };
 
 // storage index of cell (i,j,k) in a level's x / b arrays
@@ -180,6 +193,19 @@ void launch_mg_setup_level(const MGLevel<T> &F, const MGLevel<T> &C, cudaStream_
 // flip (optional): block order of the first sweep (0 forward, 1 reversed);
 // sweeps alternate and *flip returns the order the next launch should use;
 // returns the number of kernels launched
+// PCMatrixType FullJacobian (mg_full.cu): prolongation weights and coarse
+// operators of all levels from a non-symmetric level 0; red/black sweeps
+// (red, black and, when symmetric, red again; zero: zero initial guess) and
+// the residual on the non-symmetric level 0.  Each returns its launches.
+template <typename T>
+int launch_mg_full_setup(const MGLevel<T> *L, int nl, cudaStream_t st);
+template <typename T>
+int launch_mg_full_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int symmetric,
+                          cudaStream_t st);
+template <typename T>
+void launch_mg_full_residual(const MGLevel<T> &L, const T *x, const T *b, T *r,
+                             cudaStream_t st);
+
 template <typename T>
 int launch_mg_smooth(const MGLevel<T> &L, T *x, const T *b, int zero, int smoother,
                       double weight, T *tmp, cudaStream_t st, int *flip = nullptr,

@@ -553,7 +553,9 @@ __device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j,
     const double den_d = rho;
     const VG v = vg_at(P, c);
     const double prod_val = vg_kr(P, value, v.alpha, v.n) * den_d;
-    const double zu = (k + 1 < P.nz) ? __ldg(P.zmult + k + 1) : 0.0;
+    // above the top layer the z_mult ghost keeps the 1 it was initialised
+    // with (problem_dz_scale.c:92)
+    const double zu = (k + 1 < P.nz) ? __ldg(P.zmult + k + 1) : 1.0;
     double coeff, diff, o_temp;
     switch (face) {
       case 0:
@@ -612,7 +614,12 @@ __device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j,
   // terms belong to the neighbour's E / N entry (lower coefficient aliasing,
   // matrix.c:484-490): E(i) gets this cell's east term, then the east
   // neighbour's west term, in the reference's loop order.
-  if (SURF && k == P.nz - 1 && P.bc_type[5] == 2) {
+  // difference-quotient mode: an OverlandFlow top cell with p > 0 gets
+  // vol zm / (dz mean(zm, 1)) (dt + 1), the z_mult ghost above the top layer
+  // keeping its initial 1 (problem_dz_scale.c:92), and no surface terms
+  if (M.fd && k == P.nz - 1 && P.bc_type[5] == 4 && pc > 0.0)
+    cp += (vol * zm) / (P.dz * (0.5 * (zm + 1.0))) * (dt + 1);
+  if (SURF && !M.fd && k == P.nz - 1 && P.bc_type[5] == 2) {
     const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
     const double two3 = 2.0 / 3.0;
     const OvCell o = ov_cell(P, i, j);
@@ -659,7 +666,7 @@ __device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j,
   // (richards_jacobian_eval.c:2028-2090, CALCDER of overlandflow_eval.c):
   // the derivative parts of each column's own flux; neighbours' parts give
   // the off-diagonals, and the east neighbour's west term lands in E(i)
-  if (SURF && k == P.nz - 1 && P.bc_type[5] == 4) {
+  if (SURF && !M.fd && k == P.nz - 1 && P.bc_type[5] == 4) {
     const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
     const double qx = ovf_qder<true>(P, pc, i, j), qy = ovf_qder<false>(P, pc, i, j);
     const double ke_d = pmax0(qx), kw_d = -pmax0(-qx);
@@ -691,7 +698,7 @@ __device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j,
   // cell lands in the x_lower ghost column of E, which MGSemi's setup reads:
   // it is returned in wgv for the multigrid's ghost plane.
   double wgv = 0.0;
-  if (SURF && k == P.nz - 1 && P.bc_type[5] == 3) {
+  if (SURF && !M.fd && k == P.nz - 1 && P.bc_type[5] == 3) {
     const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
     const OvdCol o = ovd_col(P, p, i, j);
     double ke_d, kens, kn_d, knns;

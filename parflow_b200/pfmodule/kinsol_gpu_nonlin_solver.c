@@ -67,6 +67,7 @@ typedef struct {
   int use_jacobian;
   double derivative_epsilon;
   int globalization; /* PFGPU_GLOBAL_* */
+  int pc_matrix;     /* PFGPU_PCM_* */
 } GpuPublicXtra;
 
 typedef struct {
@@ -198,8 +199,9 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
    * (richards_jacobian_eval.c:760, 781, 2246) */
   na = NA_NewNameArray("FullJacobian PFSymmetric SymmetricPart Picard");
   name = GetStringDefault("Solver.Linear.Preconditioner.PCMatrixType", "PFSymmetric");
-  if (NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.PCMatrixType") == 0)
-    gpu_fail("PCMatrixType FullJacobian is not available");
+  px->pc_matrix =
+    NA_NameToIndexExitOnError(na, name, "Solver.Linear.Preconditioner.PCMatrixType") == 0
+    ? PFGPU_PCM_FULL : PFGPU_PCM_SYMMETRIC;
   NA_FreeNameArray(na);
   if (pc == 3)
   {
@@ -408,6 +410,8 @@ static void create_handle(GpuInstanceXtra *ix, GpuPublicXtra *px, Vector *pressu
       pfgpu_set_jacobian_mode(ix->h, 0, px->derivative_epsilon) != PFGPU_OK)
     gpu_fail(pfgpu_last_error());
   if (pfgpu_set_globalization(ix->h, px->globalization) != PFGPU_OK)
+    gpu_fail(pfgpu_last_error());
+  if (pfgpu_set_pc_matrix(ix->h, px->pc_matrix) != PFGPU_OK)
     gpu_fail(pfgpu_last_error());
 
   /* permeability: x, and y / z where they differ from x */

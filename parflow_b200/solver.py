@@ -97,6 +97,8 @@ class RichardsGPU:
         if s.globalization_code() != 0:
             L.check(self.lib.pfgpu_set_globalization(self.h, s.globalization_code()),
                     "set_globalization")
+        if s.pc_matrix_code():
+            L.check(self.lib.pfgpu_set_pc_matrix(self.h, s.pc_matrix_code()), "set_pc_matrix")
         if prob.kr_table:
             method = {"Spline": 1, "Linear": 2}[prob.kr_table[0]]
             L.check(self.lib.pfgpu_set_relperm_table(self.h, method, int(prob.kr_table[1]),

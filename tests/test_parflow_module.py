@@ -68,7 +68,8 @@ def test_wrapped_build_without_gpu_is_the_reference(name, golden):
 GPU_CASES = ["box_small", "box_odd", "hetero_small", "walker2_small", "seepage_small",
              "overland_small", "tfg_small", "vel_small", "vel_overland_small", "wjacobi_small",
              "krtable_spline_small", "growth_small", "halving_small", "restart_small",
-             "inexact_small", "rbgs_nonsym_small", "flow_barrier_small"]
+             "inexact_small", "rbgs_nonsym_small", "flow_barrier_small", "fulljac_small",
+             "fulljac_overland_small", "dq_overland_flow_small", "dirichlet_top_small"]
 
 
 @pytest.mark.gpu
