@@ -125,7 +125,7 @@ typedef struct {
   int precision;                    /* PFGPU_PREC_* */
   /* Solver.Nonlinear.* / Solver.Linear.* keys */
   double residual_tol, step_tol;
-  int max_iter, krylov_dim, max_restarts;
+  int max_iter, krylov_dim, max_restarts;  /* krylov_dim: 1 .. 64 */
   int eta_choice;
   double eta_value, eta_alpha, eta_gamma;
   int mg_max_levels, mg_smoother;

@@ -424,7 +424,7 @@ __global__ void k_fill(double *__restrict__ x, double v, long long n) {
     x[i] = v;
 }
 struct VecList {
-  const double *v[32];
+  const double *v[NK_MAX_KRYLOV + 1];
 };
 // xcor = yg[0] V0 + 0, then xcor = yg[k] Vk + xcor (sequential N_VLinearSum order)
 // xcor = sum_k yg[k] V_k, accumulated in k order onto 0 (accumulate = 0) or
@@ -482,13 +482,13 @@ void launch_fill(double *x, double v, long long n, cudaStream_t st) {
 void launch_combine(double *xcor, double *const *V, const double *yg, int kdim, long long n,
                     cudaStream_t st, int accumulate) {
   VecList L;
-  for (int k = 0; k < kdim && k < 32; k++) L.v[k] = V[k];
+  for (int k = 0; k < kdim && k <= NK_MAX_KRYLOV; k++) L.v[k] = V[k];
   launch_pdl(k_combine, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, n, accumulate);
 }
 void launch_restart_v0(double *const *V, const double *yg, int kdim, long long n,
                        cudaStream_t st) {
   VecList L;
-  for (int k = 0; k <= kdim && k < 32; k++) L.v[k] = V[k];
+  for (int k = 0; k <= kdim && k <= NK_MAX_KRYLOV; k++) L.v[k] = V[k];
   launch_pdl(k_restart_v0, dim3(grid_for(n)), dim3(256), st, V[0], L, yg, kdim, n);
 }
 
@@ -579,13 +579,13 @@ void launch_v0_init(double *v0, const double *src, const NkState *S, const doubl
 void launch_combine_dev(double *xcor, double *const *V, int nv, const double *yg, const int *kdim,
                         const int *accumulate, long long n, cudaStream_t st) {
   VecList L{};
-  for (int k = 0; k < nv && k < 32; k++) L.v[k] = V[k];
+  for (int k = 0; k < nv && k <= NK_MAX_KRYLOV; k++) L.v[k] = V[k];
   launch_pdl(k_combine_dev, dim3(grid_for(n)), dim3(256), st, xcor, L, yg, kdim, accumulate, n);
 }
 void launch_restart_v0_dev(double *const *V, int nv, const double *yg, const int *kdim,
                            long long n, cudaStream_t st) {
   VecList L{};
-  for (int k = 0; k < nv && k < 32; k++) L.v[k] = V[k];
+  for (int k = 0; k < nv && k <= NK_MAX_KRYLOV; k++) L.v[k] = V[k];
   launch_pdl(k_restart_v0_dev, dim3(grid_for(n)), dim3(256), st, V[0], L, yg, kdim, n);
 }
 void launch_scale_inv_dev_unless(double *x, const double *s, const int *skip, long long n,

@@ -29,7 +29,8 @@ enum {
   D_DQ = 40  // five slots of the difference-quotient product (launch_dq_prepare)
 };
 
-constexpr int NK_MAX_L = 32;  // more than the largest Krylov dimension (30)
+constexpr int NK_MAX_KRYLOV = 64;  // largest Krylov dimension (KrylovDimension)
+constexpr int NK_MAX_L = NK_MAX_KRYLOV + 2;
 
 // graph bodies whose executions are counted (launches = sum over bodies of
 // kernels per body x executions)

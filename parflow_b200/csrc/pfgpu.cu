@@ -2277,8 +2277,8 @@ pfgpu_handle *pfgpu_create(const pfgpu_desc *desc, int device) {
     set_err("pfgpu_create: grid must hold fewer than 2^31 cells");
     return nullptr;
   }
-  if (desc->krylov_dim < 1 || desc->krylov_dim > 30) {
-    set_err("pfgpu_create: krylov_dim must be in [1, 30]");
+  if (desc->krylov_dim < 1 || desc->krylov_dim > NK_MAX_KRYLOV) {
+    set_err("pfgpu_create: krylov_dim must be in [1, %d]", NK_MAX_KRYLOV);
     return nullptr;
   }
   if (desc->max_restarts < 0) {

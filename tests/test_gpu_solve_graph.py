@@ -117,3 +117,25 @@ def test_graph_recaptured_when_the_problem_changes(gpu):
         assert np.array_equal(a, b)
     for a, b in zip(res[0][2], res[1][2]):
         _same_stats(a, b, "dq")
+
+
+def test_graph_solve_large_krylov_dimension(gpu):
+    """Krylov dimension 50 (the reference's tilted-V tests) with a one-level
+    multigrid, so that GMRES cycles run past 30 iterations (27 on average in
+    the second step): the graph's nested GMRES iteration bodies are 50 deep.
+    Graph and host-driven solves bitwise equal, counts equal the oracle's."""
+    from oracle.oracle import Oracle
+    from parflow_b200 import configs
+    from parflow_b200.problem import SolverSettings
+
+    prob = configs.hetero(nx=16, ny=14, nz=10, nsteps=2, dt=5.0, seed=29,
+                          solver=SolverSettings(krylov_dim=50, eta_value=1e-10,
+                                                mg_max_levels=1))
+    pg, sg = _run(gpu, prob, "fp64", 1)
+    ph, sh = _run(gpu, prob, "fp64", 0)
+    _, so = Oracle(prob).run()
+    for t, (a, b) in enumerate(zip(pg, ph)):
+        assert np.array_equal(a, b), (t, np.abs(a - b).max())
+    for t, (a, b) in enumerate(zip(sg, sh)):
+        _same_stats(a, b, ("krylov50", t))
+    assert [(x.nonlin_iters, x.lin_iters) for x in sg] == [(x.nni, x.nli) for x in so]
