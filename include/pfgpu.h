@@ -379,6 +379,14 @@ int pfgpu_set_globalization(pfgpu_handle *h, int strategy);
 #define PFGPU_PCM_FULL 1
 int pfgpu_set_pc_matrix(pfgpu_handle *h, int type);
 
+/* Solver.Linear.Preconditioner.MGSemi.MaxIter (MGSemiNewPublicXtra,
+ * mg_semi.c:1312-1313; default 1): V-cycles per preconditioner application,
+ * KinsolPC's tolerance 0 skipping every convergence test (kinsol_pc.c:65-72,
+ * mg_semi.c:198-365).  0 makes the preconditioner the identity; a cycle
+ * after the first begins with a smoothing of the finest level's current
+ * iterate. */
+int pfgpu_set_mg_max_iter(pfgpu_handle *h, int max_iter);
+
 /* Device-resident time stepping: advances the handle's own pressure state by
  * nsteps steps of dt with the boundary tables already set, keeping every
  * vector on the GPU (the step body of AdvanceRichards,

@@ -49,7 +49,7 @@ class Settings(C.Structure):
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
                 ("wjacobi_weight", C.c_double),
                 ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double),
-                ("globalization", C.c_int), ("pc_full", C.c_int)]
+                ("globalization", C.c_int), ("mg_max_iter", C.c_int), ("pc_full", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -172,6 +172,7 @@ class Oracle:
         S.derivative_epsilon = s.derivative_epsilon
         S.globalization = s.globalization_code()
         S.pc_full = s.pc_matrix_code()
+        S.mg_max_iter = s.mg_max_iter
         self.S = S
 
     def __del__(self):

@@ -1342,6 +1342,7 @@ struct pfo_mg {
   mg_level *L;
   int smoother;
   double weight;
+  int max_iter;       /* Solver.Linear.Preconditioner.MGSemi.MaxIter */
 };
 
 static void lvl_alloc(mg_level *l, int nx, int ny, int nz)
@@ -1389,6 +1390,7 @@ pfo_mg *pfo_mg_create(const pfo_problem *pb, const pfo_settings *st)
   mg->nlev = l + 1;
   mg->L = (mg_level*)calloc(mg->nlev, sizeof(mg_level));
   mg->smoother = st->mg_smoother;
+  mg->max_iter = st->mg_max_iter;
   mg->weight = st->wjacobi_weight > 0 ? st->wjacobi_weight : 1.0;
   int nx = pb->nx, ny = pb->ny, nz = pb->nz;
   for (int i = 0; i < mg->nlev; i++)
@@ -1766,38 +1768,52 @@ static void prolong_lvl(const mg_level *F, const mg_level *Cl, const double *ec,
 }
 
 /* One V-cycle with zero initial guess (PL/mg_semi.c:93-432, MaxIter 1) */
+/* MaxIter V-cycles, KinsolPC's tolerance 0 skipping every convergence test
+ * (PL/mg_semi.c:198-365, kinsol_pc.c:65-72): MaxIter 0 returns x = b; each
+ * cycle after the first starts with a smoothing of the current x */
 void pfo_mg_apply(pfo_mg *mg, const double *b, double *x)
 {
   int nl = mg->nlev;
   mg_level *L = mg->L;
+  if (mg->max_iter < 1)
+  {
+    memcpy(x, b, L[0].n * sizeof(double));
+    return;
+  }
   if (nl == 1)
   {
     smooth(mg, &L[0], x, b, 1);
     return;
   }
   smooth(mg, &L[0], x, b, 1);
-  lvl_residual(&L[0], x, b, L[0].t);
-  restrict_lvl(&L[0], &L[1], L[0].t, L[1].b);
-  int l;
-  for (l = 1; l <= nl - 2; l++)
+  for (int it = 1;; it++)
   {
-    smooth(mg, &L[l], L[l].x, L[l].b, 1);
-    lvl_residual(&L[l], L[l].x, L[l].b, L[l].t);
-    restrict_lvl(&L[l], &L[l + 1], L[l].t, L[l + 1].b);
+    lvl_residual(&L[0], x, b, L[0].t);
+    restrict_lvl(&L[0], &L[1], L[0].t, L[1].b);
+    int l;
+    for (l = 1; l <= nl - 2; l++)
+    {
+      smooth(mg, &L[l], L[l].x, L[l].b, 1);
+      lvl_residual(&L[l], L[l].x, L[l].b, L[l].t);
+      restrict_lvl(&L[l], &L[l + 1], L[l].t, L[l + 1].b);
+    }
+    /* coarse solve: RedBlackGSPoint, 1 iteration */
+    rbgs(&L[l], L[l].x, L[l].b, 1);
+    for (l = nl - 2; l >= 1; l--)
+    {
+      prolong_lvl(&L[l], &L[l + 1], L[l + 1].x, L[l].t);
+      for (long c = 0; c < L[l].n; c++)
+        L[l].x[c] += L[l].t[c];
+      smooth(mg, &L[l], L[l].x, L[l].b, 0);
+    }
+    prolong_lvl(&L[0], &L[1], L[1].x, L[0].t);
+    for (long c = 0; c < L[0].n; c++)
+      x[c] += L[0].t[c];
+    smooth(mg, &L[0], x, b, 0);
+    if (it + 1 > mg->max_iter)
+      break;
+    smooth(mg, &L[0], x, b, 0);
   }
-  /* coarse solve: RedBlackGSPoint, 1 iteration */
-  rbgs(&L[l], L[l].x, L[l].b, 1);
-  for (l = nl - 2; l >= 1; l--)
-  {
-    prolong_lvl(&L[l], &L[l + 1], L[l + 1].x, L[l].t);
-    for (long c = 0; c < L[l].n; c++)
-      L[l].x[c] += L[l].t[c];
-    smooth(mg, &L[l], L[l].x, L[l].b, 0);
-  }
-  prolong_lvl(&L[0], &L[1], L[1].x, L[0].t);
-  for (long c = 0; c < L[0].n; c++)
-    x[c] += L[0].t[c];
-  smooth(mg, &L[0], x, b, 0);
 }
 
 /* -------------------------------------------------------------------------

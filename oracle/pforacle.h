@@ -82,6 +82,7 @@ typedef struct {
   double derivative_epsilon;       /* Solver.Nonlinear.DerivativeEpsilon */
   int globalization;               /* Solver.Nonlinear.Globalization: 0 LineSearch,
                                     * 1 InexactNewton */
+  int mg_max_iter;                 /* Solver.Linear.Preconditioner.MGSemi.MaxIter */
   int pc_full;                     /* Solver.Linear.Preconditioner.PCMatrixType:
                                     * 1 FullJacobian, 0 the symmetric part
                                     * (PFSymmetric, SymmetricPart, Picard) */

@@ -287,6 +287,14 @@ def dirichlet_top_small() -> RichardsProblem:
     return p
 
 
+def mg_maxiter_small() -> RichardsProblem:
+    """MGSemi.MaxIter 2: two V-cycles per preconditioner application, the
+    second starting with a smoothing of the first's result (mg_semi.c:
+    198-365), on config-2 physics."""
+    return configs.hetero(nx=13, ny=11, nz=8, nsteps=2, seed=89,
+                          solver=SolverSettings(mg_max_iter=2))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -298,7 +306,7 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
           "picard_small", "inexact_small", "flow_barrier_small", "fulljac_small",
           "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small",
-          "dirichlet_top_small"]
+          "dirichlet_top_small", "mg_maxiter_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

@@ -187,6 +187,7 @@ struct pfgpu_handle {
   int use_jacobian = 1;
   int globalization = PFGPU_GLOBAL_LINE_SEARCH;  // Solver.Nonlinear.Globalization
   int pc_matrix = PFGPU_PCM_SYMMETRIC;  // Solver.Linear.Preconditioner.PCMatrixType
+  int mg_max_iter = 1;                  // Solver.Linear.Preconditioner.MGSemi.MaxIter
   double sqrt_relfunc = 0.0;
   double *dq_w = nullptr, *dq_f = nullptr;
   double *krt = nullptr;  // relative-permeability lookup table (device)
@@ -501,7 +502,8 @@ static long long mg_setup_T(MG<T> &mg, cudaStream_t st) {
 // levels mg.tail .. nl-1 (a few thousand cells each) in one of its blocks;
 // otherwise those run inside one single-block kernel.
 template <typename T>
-static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
+static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st,
+                          int max_iter = 1) {
   long long k = 0;
   const int nl = (int)mg.L.size();
   const int first = mg.mid;
@@ -515,11 +517,19 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
     if (mg.flip) f ^= 1;
     return r;
   };
+  // MGSemi.MaxIter cycles (mg_semi.c:198-365 with KinsolPC's tolerance 0):
+  // a cycle after the first begins with a smoothing of the finest level's
+  // current iterate (the level runs on the grid kernels then, on the plain
+  // colour sweeps); the coarse levels start from zero in every cycle
+  for (int cyc = 0; cyc < max_iter; cyc++) {
+  const int zero0 = cyc == 0 ? 1 : 0;
   for (int l = 0; l < first; l++) {
     MGLevel<T> &Ll = mg.L[l];
+    const int zero = l == 0 ? zero0 : 1;
     if (Ll.lo[0]) {
       // the non-symmetric finest operator of FullJacobian (mg_full.cu)
-      k += launch_mg_full_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother != PFGPU_SMOOTH_RBGS_NONSYM, st);
+      k += launch_mg_full_smooth<T>(Ll, Ll.x, Ll.b, zero, smoother != PFGPU_SMOOTH_RBGS_NONSYM,
+                                    st);
       launch_mg_full_residual<T>(Ll, Ll.x, Ll.b, Ll.t, st);
       launch_mg_restrict<T>(Ll, mg.L[l + 1], Ll.t, mg.L[l + 1].b, st, next(), mg.h16);
       k += 2;
@@ -533,7 +543,7 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
       f = mg.flip ? 1 : 0;  // the wave ends on the top planes
       k++;
     } else {
-      k += launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 1, smoother, w, mg.wtmp, st, fp, mg.h16);
+      k += launch_mg_smooth<T>(Ll, Ll.x, Ll.b, zero, smoother, w, mg.wtmp, st, fp, mg.h16);
     }
     // after the plain red/black pre-smoother the colour swept last (red, or
     // black for the non-symmetric order) has a zero residual up to rounding
@@ -579,6 +589,7 @@ static long long vcycle_T(MG<T> &mg, int smoother, double w, cudaStream_t st) {
       k += 1 + launch_mg_smooth<T>(Ll, Ll.x, Ll.b, 0, smoother, w, mg.wtmp, st, fp, mg.h16);
     }
   }
+  }
   mg.flip_out = f;
   return k;
 }
@@ -590,8 +601,9 @@ static T *vcycle_out(MG<T> &mg, int) {
 }
 
 static long long vcycle_launch(pfgpu_handle *h) {
-  if (h->mixed) return vcycle_T<float>(h->mgf, h->d.mg_smoother, h->d.wjacobi_weight, h->st);
-  return vcycle_T<double>(h->mgd, h->d.mg_smoother, h->d.wjacobi_weight, h->st);
+  if (h->mixed)
+    return vcycle_T<float>(h->mgf, h->d.mg_smoother, h->d.wjacobi_weight, h->st, h->mg_max_iter);
+  return vcycle_T<double>(h->mgd, h->d.mg_smoother, h->d.wjacobi_weight, h->st, h->mg_max_iter);
 }
 
 static int build_vgraph(pfgpu_handle *h) {
@@ -608,6 +620,12 @@ static int build_vgraph(pfgpu_handle *h) {
 // z = M^{-1} r (dense FP64 device vectors; r and z may alias)
 static int pc_apply_dense_impl(pfgpu_handle *h, const double *r, double *z) {
   int k = 0;
+  if (h->mg_max_iter == 0) {
+    // MGSemi.MaxIter 0: x = b (mg_semi.c:198-203)
+    if (z != r)
+      CK(cudaMemcpyAsync(z, r, h->N * sizeof(double), cudaMemcpyDeviceToDevice, h->st));
+    return 0;
+  }
   if (h->mixed)
     k += launch_level_in<float>(h->mgf.L[0], r, h->h16 ? h->mgf.L[0].sinv : nullptr, h->st);
   else
@@ -1351,7 +1369,7 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(&P, &h->P, sizeof(P));
   P.dtp = nullptr;
   const double *ptrs[2] = {h->u, h->unew};
-  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + 3 * sizeof(int) +
+  std::vector<unsigned char> k(sizeof(P) + sizeof(h->d) + sizeof(ptrs) + 4 * sizeof(int) +
                                sizeof(double));
   unsigned char *q = k.data();
   memcpy(q, &P, sizeof(P));
@@ -1367,6 +1385,8 @@ static std::vector<unsigned char> nk_key(pfgpu_handle *h) {
   memcpy(q, &h->globalization, sizeof(int));
   q += sizeof(int);
   memcpy(q, &h->pc_matrix, sizeof(int));
+  q += sizeof(int);
+  memcpy(q, &h->mg_max_iter, sizeof(int));
   return k;
 }
 
@@ -1802,6 +1822,31 @@ static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   return 0;
 }
 
+// The finest level on the per-phase grid kernels with the plain colour
+// sweeps: out of the single-block tail and cluster kernels and of the fused /
+// wavefront smoothers (FullJacobian's non-symmetric operator; MGSemi.MaxIter
+// cycles after the first, whose pre-smoothing reads the current iterate)
+template <typename T>
+static int mg_level0_on_grid(pfgpu_handle *h, MG<T> &mg) {
+  const int nl = (int)mg.L.size();
+  MGLevel<T> &L0 = mg.L[0];
+  if (nl > 1) {
+    if (mg.tail < 1) {
+      mg.tail = 1;
+      const size_t b = tail_smem_bytes<T>(mg.L.data(), 1, nl, mg.h16);
+      mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
+    }
+    if (mg.mid < 1) mg.mid = 1;
+  }
+  mg.fused[0] = 0;
+  mg.waved[0] = 0;
+  L0.split = (h->d.mg_smoother == PFGPU_SMOOTH_RBGS ||
+              h->d.mg_smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
+             env_ll("PFGPU_SPLIT", 1) != 0 && nl > 1;
+  CK(cudaMemcpy(mg.Ldev, mg.L.data(), nl * sizeof(MGLevel<T>), cudaMemcpyHostToDevice));
+  return PFGPU_OK;
+}
+
 // FullJacobian storage for a hierarchy: W S L on level 0, the S / L ghost
 // planes on every level, level 0 taken out of the fused / wavefront smoothers
 // and the single-block kernels (their kernels assume a symmetric operator)
@@ -1819,22 +1864,8 @@ static int mg_enable_full(pfgpu_handle *h, MG<T> &mg) {
     CK(cudaMemset(L.sg, 0, (long long)L.nx * L.nz * sizeof(T)));
     CK(cudaMemset(L.lg, 0, (long long)L.nx * L.ny * sizeof(T)));
   }
-  if (nl > 1) {
-    if (mg.tail < 1) {
-      mg.tail = 1;
-      const size_t b = tail_smem_bytes<T>(mg.L.data(), 1, nl, mg.h16);
-      mg.tail_smem = b <= TAIL_SMEM_MAX && env_ll("PFGPU_TAIL_SMEM", 1) ? b : 0;
-    }
-    if (mg.mid < 1) mg.mid = 1;
-  }
-  mg.fused[0] = 0;
-  mg.waved[0] = 0;
-  L0.split = (h->d.mg_smoother == PFGPU_SMOOTH_RBGS ||
-              h->d.mg_smoother == PFGPU_SMOOTH_RBGS_NONSYM) &&
-             env_ll("PFGPU_SPLIT", 1) != 0 && nl > 1;
   L0.zc = -1;
-  CK(cudaMemcpy(mg.Ldev, mg.L.data(), nl * sizeof(MGLevel<T>), cudaMemcpyHostToDevice));
-  return PFGPU_OK;
+  return mg_level0_on_grid(h, mg);
 }
 template <typename T>
 static int mg_disable_full(MG<T> &mg) {
@@ -3135,6 +3166,27 @@ int pfgpu_solve_graph(pfgpu_handle *h, int mode) {
   if (mode == -1) return h->nk.used_last ? 1 : 0;
   set_err("pfgpu_solve_graph: mode must be 0, 1 or -1");
   return PFGPU_ERR_ARG;
+}
+
+int pfgpu_set_mg_max_iter(pfgpu_handle *h, int max_iter) {
+  if (!h || max_iter < 0 || max_iter > 1000) {
+    set_err("pfgpu_set_mg_max_iter: max_iter must be in [0, 1000]");
+    return PFGPU_ERR_ARG;
+  }
+  if (max_iter == h->mg_max_iter) return PFGPU_OK;
+  CK(cudaSetDevice(h->device));
+  CK(cudaStreamSynchronize(h->st));
+  if (max_iter > 1) {
+    const int rc = h->mixed ? mg_level0_on_grid<float>(h, h->mgf) : mg_level0_on_grid<double>(h, h->mgd);
+    if (rc != PFGPU_OK) return rc;
+  }
+  h->mg_max_iter = max_iter;
+  if (h->vgraph) {
+    CK(cudaGraphExecDestroy(h->vgraph));
+    h->vgraph = nullptr;
+  }
+  if (build_vgraph(h)) return PFGPU_ERR_CUDA;
+  return PFGPU_OK;
 }
 
 int pfgpu_set_pc_matrix(pfgpu_handle *h, int type) {

@@ -68,6 +68,7 @@ typedef struct {
   double derivative_epsilon;
   int globalization; /* PFGPU_GLOBAL_* */
   int pc_matrix;     /* PFGPU_PCM_* */
+  int mg_max_iter;   /* MGSemi.MaxIter */
 } GpuPublicXtra;
 
 typedef struct {
@@ -156,6 +157,7 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
     return __real_KinsolNonlinSolverNewPublicXtra();
   PFModule *this_module = ThisPFModule;
   GpuPublicXtra *px = ctalloc(GpuPublicXtra, 1);
+  px->mg_max_iter = 1;
   pfgpu_desc *d = &px->desc;
   NameArray na;
   char *name;
@@ -226,8 +228,7 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
   }
   else
   {
-    if (GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxIter", 1) != 1)
-      gpu_fail("only MGSemi.MaxIter 1 is available");
+    px->mg_max_iter = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxIter", 1);
     d->mg_max_levels = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxLevels", 100);
     na = NA_NewNameArray("RedBlackGSPoint WJacobi");
     name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother", "RedBlackGSPoint");
@@ -412,6 +413,8 @@ static void create_handle(GpuInstanceXtra *ix, GpuPublicXtra *px, Vector *pressu
   if (pfgpu_set_globalization(ix->h, px->globalization) != PFGPU_OK)
     gpu_fail(pfgpu_last_error());
   if (pfgpu_set_pc_matrix(ix->h, px->pc_matrix) != PFGPU_OK)
+    gpu_fail(pfgpu_last_error());
+  if (pfgpu_set_mg_max_iter(ix->h, px->mg_max_iter) != PFGPU_OK)
     gpu_fail(pfgpu_last_error());
 
   /* permeability: x, and y / z where they differ from x */

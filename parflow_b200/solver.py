@@ -99,6 +99,8 @@ class RichardsGPU:
                     "set_globalization")
         if s.pc_matrix_code():
             L.check(self.lib.pfgpu_set_pc_matrix(self.h, s.pc_matrix_code()), "set_pc_matrix")
+        if s.mg_max_iter != 1:
+            L.check(self.lib.pfgpu_set_mg_max_iter(self.h, s.mg_max_iter), "set_mg_max_iter")
         if prob.kr_table:
             method = {"Spline": 1, "Linear": 2}[prob.kr_table[0]]
             L.check(self.lib.pfgpu_set_relperm_table(self.h, method, int(prob.kr_table[1]),

@@ -69,7 +69,8 @@ GPU_CASES = ["box_small", "box_odd", "hetero_small", "walker2_small", "seepage_s
              "overland_small", "tfg_small", "vel_small", "vel_overland_small", "wjacobi_small",
              "krtable_spline_small", "growth_small", "halving_small", "restart_small",
              "inexact_small", "rbgs_nonsym_small", "flow_barrier_small", "fulljac_small",
-             "fulljac_overland_small", "dq_overland_flow_small", "dirichlet_top_small"]
+             "fulljac_overland_small", "dq_overland_flow_small", "dirichlet_top_small",
+             "mg_maxiter_small"]
 
 
 @pytest.mark.gpu
