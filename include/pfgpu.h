@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define PFGPU_ABI_VERSION 1
+#define PFGPU_ABI_VERSION 2
 
 /* status codes */
 #define PFGPU_OK 0
@@ -130,6 +130,10 @@ typedef struct {
   double eta_value, eta_alpha, eta_gamma;
   int mg_max_levels, mg_smoother;
   double wjacobi_weight;
+  /* MGSemi.MaxMinNX / NY / NZ (mg_semi.c:1318-1325, default 1): a direction
+   * is coarsened only while it has at least max(2 n - 1, 2) cells
+   * (mg_semi.c:869-872); 0 counts as 1 */
+  int mg_max_min_n[3];
 } pfgpu_desc;
 
 /* Counters of one nonlinear solve (the kinsol.log fields,

@@ -49,7 +49,8 @@ class Settings(C.Structure):
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
                 ("wjacobi_weight", C.c_double),
                 ("use_jacobian", C.c_int), ("derivative_epsilon", C.c_double),
-                ("globalization", C.c_int), ("mg_max_iter", C.c_int), ("pc_full", C.c_int)]
+                ("globalization", C.c_int), ("mg_max_iter", C.c_int),
+                ("mg_max_min_n", C.c_int * 3), ("pc_full", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -173,6 +174,8 @@ class Oracle:
         S.globalization = s.globalization_code()
         S.pc_full = s.pc_matrix_code()
         S.mg_max_iter = s.mg_max_iter
+        for q in range(3):
+            S.mg_max_min_n[q] = s.mg_max_min_n[q]
         self.S = S
 
     def __del__(self):

@@ -1369,16 +1369,22 @@ pfo_mg *pfo_mg_create(const pfo_problem *pb, const pfo_settings *st)
   int max_levels = st->mg_max_levels > 0 ? st->mg_max_levels : 100;
   double DX = pb->dx, DY = pb->dy, DZ = pb->dz;
   int NX = pb->nx, NY = pb->ny, NZ = pb->nz;
-  int minN = 2;  /* max(2*MaxMinN - 1, 2) with MaxMinN = 1 */
+  /* max(2 MaxMinN - 1, 2) per direction (PL/mg_semi.c:869-872) */
+  int minN[3];
+  for (int q = 0; q < 3; q++)
+  {
+    int m = st->mg_max_min_n[q] > 1 ? st->mg_max_min_n[q] : 1;
+    minN[q] = 2 * m - 1 > 2 ? 2 * m - 1 : 2;
+  }
   int dirs[128];
   int l;
   for (l = 0; l < max_levels - 1 && l < 127; l++)
   {
     double min_spacing = DX + DY + DZ;
     int d = -1;
-    if ((NX >= minN) && (DX < min_spacing)) { min_spacing = DX; d = 0; }
-    if ((NY >= minN) && (DY < min_spacing)) { min_spacing = DY; d = 1; }
-    if ((NZ >= minN) && (DZ < min_spacing)) { min_spacing = DZ; d = 2; }
+    if ((NX >= minN[0]) && (DX < min_spacing)) { min_spacing = DX; d = 0; }
+    if ((NY >= minN[1]) && (DY < min_spacing)) { min_spacing = DY; d = 1; }
+    if ((NZ >= minN[2]) && (DZ < min_spacing)) { min_spacing = DZ; d = 2; }
     if (d == -1)
       break;
     if (d == 0) { DX *= 2; NX = (NX + 1) / 2; }

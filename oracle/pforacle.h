@@ -83,6 +83,7 @@ typedef struct {
   int globalization;               /* Solver.Nonlinear.Globalization: 0 LineSearch,
                                     * 1 InexactNewton */
   int mg_max_iter;                 /* Solver.Linear.Preconditioner.MGSemi.MaxIter */
+  int mg_max_min_n[3];             /* ...MGSemi.MaxMinNX / NY / NZ (0 counts as 1) */
   int pc_full;                     /* Solver.Linear.Preconditioner.PCMatrixType:
                                     * 1 FullJacobian, 0 the symmetric part
                                     * (PFSymmetric, SymmetricPart, Picard) */

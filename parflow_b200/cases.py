@@ -295,6 +295,14 @@ def mg_maxiter_small() -> RichardsProblem:
                           solver=SolverSettings(mg_max_iter=2))
 
 
+def mg_minn_small() -> RichardsProblem:
+    """MGSemi.MaxMinNX 3 and MaxMinNZ 3: x and z are coarsened only while
+    they have at least 5 cells (mg_semi.c:869-872), which changes the
+    hierarchy's coarsening directions and depth, on config-2 physics."""
+    return configs.hetero(nx=13, ny=11, nz=8, nsteps=2, seed=97,
+                          solver=SolverSettings(mg_max_min_n=(3, 1, 3)))
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -306,7 +314,7 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
           "picard_small", "inexact_small", "flow_barrier_small", "fulljac_small",
           "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small",
-          "dirichlet_top_small", "mg_maxiter_small"]
+          "dirichlet_top_small", "mg_maxiter_small", "mg_minn_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

@@ -1656,16 +1656,19 @@ template <typename T>
 static int alloc_mg(pfgpu_handle *h, MG<T> &mg) {
   double DX = h->d.dx, DY = h->d.dy, DZ = h->d.dz;
   int NX = h->nx, NY = h->ny, NZ = h->nz;
-  const int minN = 2;
+  // smallest size that is coarsened per direction (mg_semi.c:869-872)
+  int minN[3];
+  for (int q = 0; q < 3; q++)
+    minN[q] = std::max(2 * std::max(h->d.mg_max_min_n[q], 1) - 1, 2);
   int max_levels = h->d.mg_max_levels > 0 ? h->d.mg_max_levels : 100;
   std::vector<int> dirs;
   // coarsening directions (mg_semi.c:858-923)
   for (int l = 0; l < max_levels - 1; l++) {
     double ms = DX + DY + DZ;
     int dd = -1;
-    if ((NX >= minN) && (DX < ms)) { ms = DX; dd = 0; }
-    if ((NY >= minN) && (DY < ms)) { ms = DY; dd = 1; }
-    if ((NZ >= minN) && (DZ < ms)) { ms = DZ; dd = 2; }
+    if ((NX >= minN[0]) && (DX < ms)) { ms = DX; dd = 0; }
+    if ((NY >= minN[1]) && (DY < ms)) { ms = DY; dd = 1; }
+    if ((NZ >= minN[2]) && (DZ < ms)) { ms = DZ; dd = 2; }
     if (dd == -1) break;
     if (dd == 0) { DX *= 2; NX = (NX + 1) / 2; }
     if (dd == 1) { DY *= 2; NY = (NY + 1) / 2; }

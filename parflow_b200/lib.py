@@ -12,7 +12,7 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpfgpu.so")
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 PREC_FP64, PREC_MIXED, PREC_MIXED_H16 = 0, 1, 2
 BC_FLUX, BC_DIRICHLET, BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND, BC_SEEPAGE = \
     0, 1, 2, 3, 4, 5
@@ -40,7 +40,8 @@ class Desc(C.Structure):
                 ("eta_choice", C.c_int),
                 ("eta_value", C.c_double), ("eta_alpha", C.c_double), ("eta_gamma", C.c_double),
                 ("mg_max_levels", C.c_int), ("mg_smoother", C.c_int),
-                ("wjacobi_weight", C.c_double)]
+                ("wjacobi_weight", C.c_double),
+                ("mg_max_min_n", C.c_int * 3)]
 
 
 class Stats(C.Structure):

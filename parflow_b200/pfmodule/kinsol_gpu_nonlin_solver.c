@@ -230,6 +230,9 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
   {
     px->mg_max_iter = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxIter", 1);
     d->mg_max_levels = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxLevels", 100);
+    d->mg_max_min_n[0] = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxMinNX", 1);
+    d->mg_max_min_n[1] = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxMinNY", 1);
+    d->mg_max_min_n[2] = GetIntDefault("Solver.Linear.Preconditioner.MGSemi.MaxMinNZ", 1);
     na = NA_NewNameArray("RedBlackGSPoint WJacobi");
     name = GetStringDefault("Solver.Linear.Preconditioner.MGSemi.Smoother", "RedBlackGSPoint");
     const int smoother =

@@ -114,6 +114,9 @@ class SolverSettings:
     pc_matrix_type: str = "PFSymmetric"
     mg_max_iter: int = 1
     mg_max_levels: int = 100
+    # MGSemi.MaxMinNX / NY / NZ: a direction is coarsened only while it has
+    # at least max(2 n - 1, 2) cells
+    mg_max_min_n: tuple = (1, 1, 1)
     mg_smoother: str = "RedBlackGSPoint"
     # ...MGSemi.Smoother.Symmetric (RedBlackGSPoint: red, black, red when True,
     # red, black when False) and ...MGSemi.Smoother.Weight (WJacobi)
@@ -600,6 +603,9 @@ class RichardsProblem:
         k["Solver.Linear.Preconditioner.PCMatrixType"] = s.pc_matrix_type
         k["Solver.Linear.Preconditioner.MGSemi.MaxIter"] = s.mg_max_iter
         k["Solver.Linear.Preconditioner.MGSemi.MaxLevels"] = s.mg_max_levels
+        for axis, n in zip("XYZ", s.mg_max_min_n):
+            if n != 1:
+                k[f"Solver.Linear.Preconditioner.MGSemi.MaxMinN{axis}"] = n
         if s.preconditioner == "PFMG":
             k["Solver.Linear.Preconditioner.PFMG.Smoother"] = s.pfmg_smoother
         k["Solver.Linear.Preconditioner.MGSemi.Smoother"] = s.mg_smoother

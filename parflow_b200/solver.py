@@ -78,6 +78,8 @@ class RichardsGPU:
         d.eta_choice = _ETA[s.eta_choice]
         d.eta_value, d.eta_alpha, d.eta_gamma = s.eta_value, s.eta_alpha, s.eta_gamma
         d.mg_max_levels = s.mg_max_levels
+        for q in range(3):
+            d.mg_max_min_n[q] = s.mg_max_min_n[q]
         d.mg_smoother = s.smoother_code()
         d.wjacobi_weight = s.smoother_weight()
         self.desc = d
