@@ -253,6 +253,18 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
     }
     d->wjacobi_weight =
         GetDoubleDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.Weight", 1.0);
+    /* one smoothing iteration and the default coarse solve, one symmetric
+     * red/black Gauss-Seidel iteration (rb_GS_point.c:449-470,
+     * mg_semi.c:1281-1310) */
+    if (GetIntDefault("Solver.Linear.Preconditioner.MGSemi.Smoother.MaxIter", 1) != 1)
+      gpu_fail("only MGSemi.Smoother.MaxIter 1 is available");
+    if (strcmp(GetStringDefault("Solver.Linear.Preconditioner.MGSemi.CoarseSolve",
+                                "RedBlackGSPoint"), "RedBlackGSPoint") != 0 ||
+        GetIntDefault("Solver.Linear.Preconditioner.MGSemi.CoarseSolve.MaxIter", 1) != 1 ||
+        strcmp(GetStringDefault("Solver.Linear.Preconditioner.MGSemi.CoarseSolve.Symmetric",
+                                "True"), "True") != 0)
+      gpu_fail("only the default MGSemi.CoarseSolve (RedBlackGSPoint, MaxIter 1, "
+               "Symmetric True) is available");
   }
   na = NA_NewNameArray("FP64 Mixed Mixed16");
   name = GetStringDefault("Solver.Nonlinear.GPU.Precision", "FP64");
