@@ -506,7 +506,11 @@ def ensemble_arm(args, rank, world, local_rank):
     from parflow_b200.solver import RichardsGPU, ensemble_advance
 
     torch.cuda.set_device(local_rank)
-    probs = configs.ensemble(48, nsteps=10)
+    # the configuration's 10 timed timesteps per member (fewer with a smaller
+    # --steps) after the warm-up steps, which the members' plans also hold
+    warm = min(max(args.warmup, 1), 3)
+    nsteps = max(1, min(args.steps, 10))
+    probs = configs.ensemble(48, nsteps=warm + nsteps)
     cells = [p.ncells for p in probs]
 
     shapes = {}
@@ -540,8 +544,6 @@ def ensemble_arm(args, rank, world, local_rank):
         ms_total = max(t0.elapsed_time(e) for e in ends)
         return ms_total, stats
 
-    warm = 1
-    nsteps = max(1, min(args.steps, 10 - warm))
     conc = fresh()
     ensemble_advance(conc, warm)
     t_conc, st_conc = timed(conc, nsteps, True)
