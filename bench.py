@@ -506,11 +506,12 @@ def ensemble_arm(args, rank, world, local_rank):
     from parflow_b200.solver import RichardsGPU, ensemble_advance
 
     torch.cuda.set_device(local_rank)
-    # the configuration's 10 timed timesteps per member (fewer with a smaller
-    # --steps) after the warm-up steps, which the members' plans also hold
+    # the configuration's 10 timesteps per member (fewer with a smaller
+    # --steps), timed from the initial state again after the warm-up steps
+    # (graph capture, autotuning)
     warm = min(max(args.warmup, 1), 3)
     nsteps = max(1, min(args.steps, 10))
-    probs = configs.ensemble(48, nsteps=warm + nsteps)
+    probs = configs.ensemble(48, nsteps=10)
     cells = [p.ncells for p in probs]
 
     shapes = {}
@@ -525,6 +526,11 @@ def ensemble_arm(args, rank, world, local_rank):
                 shapes[p.shape] = g.autotune()
             ms.append(g)
         return ms
+
+    def restart(ms):
+        for g, p in zip(ms, probs):
+            g.set_pressure(p.initial_pressure())
+            g.set_time(p.start_time + p.dt)
 
     def timed(ms, nsteps, concurrent):
         streams = [torch.cuda.ExternalStream(g.stream()) for g in ms]
@@ -546,16 +552,19 @@ def ensemble_arm(args, rank, world, local_rank):
 
     conc = fresh()
     ensemble_advance(conc, warm)
+    restart(conc)
     t_conc, st_conc = timed(conc, nsteps, True)
     for g in conc:
         g.close()
     heur = fresh(tuned=False)
     ensemble_advance(heur, warm)
+    restart(heur)
     t_heur, _ = timed(heur, nsteps, True)
     for g in heur:
         g.close()
     seq = fresh()
     ensemble_advance(seq, warm)
+    restart(seq)
     t_seq, st_seq = timed(seq, nsteps, False)
     for g in seq:
         g.close()
