@@ -208,11 +208,12 @@ PFModule *__wrap_KinsolNonlinSolverNewPublicXtra(void)
   if (pc == 3)
   {
     /* PFMG (pf_pfmg.c:285-330) on the semicoarsening multigrid: one pre-
-     * and one post-relaxation of its smoother */
-    if (GetIntDefault("Solver.Linear.Preconditioner.PFMG.MaxIter", 1) != 1 ||
-        GetIntDefault("Solver.Linear.Preconditioner.PFMG.NumPreRelax", 1) != 1 ||
+     * and one post-relaxation of its smoother per cycle, MaxIter cycles
+     * (KinsolPC's tolerance 0 stops hypre on the count alone) */
+    px->mg_max_iter = GetIntDefault("Solver.Linear.Preconditioner.PFMG.MaxIter", 1);
+    if (GetIntDefault("Solver.Linear.Preconditioner.PFMG.NumPreRelax", 1) != 1 ||
         GetIntDefault("Solver.Linear.Preconditioner.PFMG.NumPostRelax", 1) != 1)
-      gpu_fail("PFMG with MaxIter, NumPreRelax and NumPostRelax 1 only");
+      gpu_fail("PFMG with NumPreRelax and NumPostRelax 1 only");
     na = NA_NewNameArray("Jacobi WJacobi RBGaussSeidelSymmetric RBGaussSeidelNonSymmetric");
     name = GetStringDefault("Solver.Linear.Preconditioner.PFMG.Smoother",
                             "RBGaussSeidelNonSymmetric");
