@@ -230,6 +230,15 @@ int pfgpu_read_pfb(pfgpu_handle *h, int what, const char *path);
 int pfgpu_set_surface(pfgpu_handle *h, const double *slope_x, const double *slope_y,
                       const double *mannings, int terrain_following, double ov_epsilon);
 
+/* OverlandFlowSpinUp (0 or 1) and OverlandSpinupDampP1 / P2 (0 by default)
+ * of a PFGPU_BC_OVERLAND face (NlFunctionEval, nl_function_eval.c:1659-1673;
+ * RichardsJacobianEval, richards_jacobian_eval.c:1258-1287, 2044-2057):
+ * with spin-up the ponded head drains at (vol/dz) dt max(p, 0) in place of
+ * the ponding and routing term; the damping term (vol/dz) dt
+ * exp(min(p, 0) P1) P2 joins either.  The Jacobian keeps the reference's
+ * terms as they are.  Not available with pfgpu_adjoint_gradient. */
+int pfgpu_set_overland_spinup(pfgpu_handle *h, int spinup, double damp_p1, double damp_p2);
+
 /* Sets the boundary condition of one face at the current time: `values`
  * holds one value per boundary cell, x faces (nz, ny), y faces (nz, nx),
  * z faces (ny, nx), first index slowest.  Replaces the BCStruct built by

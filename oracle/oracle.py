@@ -34,7 +34,8 @@ class Problem(C.Structure):
                 ("ov_epsilon", C.c_double),
                 ("ov_p_old", _dp),
                 ("kr_table", C.c_void_p),
-                ("evap_trans", _dp), ("fbx", _dp), ("fby", _dp), ("fbz", _dp)]
+                ("evap_trans", _dp), ("fbx", _dp), ("fby", _dp), ("fbz", _dp),
+                ("ov_spinup", C.c_int), ("ov_damp_p1", C.c_double), ("ov_damp_p2", C.c_double)]
 
 
 class FluxOut(C.Structure):
@@ -151,6 +152,8 @@ class Oracle:
                 a = np.ascontiguousarray(prob.field3d(v), dtype=np.float64)
                 self._keep.append(a)
                 setattr(P, name, _ptr(a))
+        P.ov_spinup = int(prob.overland_spinup)
+        P.ov_damp_p1, P.ov_damp_p2 = (float(v) for v in prob.spinup_damp)
         self._table = None
         if prob.kr_table:
             method = {"Spline": 0, "Linear": 1}[prob.kr_table[0]]

@@ -790,9 +790,17 @@ void pfo_residual_out(const pfo_problem *pb, double dt, const double *p,
           long io = (i + 1) + (long)(nx + 2) * (j + 1);
           double q_overlnd = vol * (PFMAX(p[c], 0.0) - PFMAX(p_old[c], 0.0)) / dz +
                              dt * vol * ((ke[io] - kw[io]) / dx + (kn[io] - ks[io]) / dy) / dz;
-          if (type == PFO_BC_OVERLAND)   /* spin-up damping, P1 = P2 = 0 */
-            q_overlnd = q_overlnd
-                        + vol * dt / dz * (exp((p[c] < 0.0 ? p[c] : 0.0) * 0.0) * 0.0);
+          if (type == PFO_BC_OVERLAND)
+          {
+            /* spin-up damping (OverlandSpinupDampP1 / P2), and with
+             * OverlandFlowSpinUp the ponded head drained in place of the
+             * ponding and routing term (:1659-1673) */
+            const double pm = p[c] < 0.0 ? p[c] : 0.0;
+            q_overlnd = q_overlnd + vol * dt / dz * (exp(pm * pb->ov_damp_p1) * pb->ov_damp_p2);
+            if (pb->ov_spinup == 1)
+              q_overlnd = (vol / dz) * dt
+                          * ((PFMAX(p[c], 0.0) - 0.0) + exp(pm * pb->ov_damp_p1) * pb->ov_damp_p2);
+          }
           f[c] += q_overlnd;
           double u_new = ffz * vals[i + nx * j];
           f[c] += dt * 1.0 * u_new;
@@ -1200,16 +1208,29 @@ void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm
     free(kn);
     free(ks);
   }
+  /* OverlandFlowSpinUp: the OverlandFlow patch's own diagonal term of a
+   * top cell with p >= 0 (:1258-1268), in patch order */
+  if (!fd && pb->bc_type[5] == PFO_BC_OVERLAND && pb->ov_spinup == 1)
+    for (int j = 0; j < ny; j++)
+      for (int i = 0; i < nx; i++)
+      {
+        long c = IDX(i, j, nz - 1);
+        if (p[c] >= 0.0)
+          cp[c] += (vol / dz) * dt * (1.0 + 0.0);
+      }
+
   /* OverlandFlow terms on the top layer, MGSemi form (:2028-2090): the
-   * derivative parts of each column's own flux; the spin-up damping term
-   * of a non-ponded cell is zero with its default parameters */
+   * derivative parts of each column's own flux (zero with
+   * OverlandFlowSpinUp, which skips their evaluation, :1287) and the
+   * derivative of the spin-up damping term of a non-ponded cell */
   if (!fd && pb->bc_type[5] == PFO_BC_OVERLAND)
   {
     const int sy2 = nx + 2;
     long n2 = (long)(nx + 2) * (ny + 2);
     double *buf = (double*)calloc(4 * n2, sizeof(double));
     double *ke = buf, *kw = buf + n2, *kn = buf + 2 * n2, *ks = buf + 3 * n2;
-    ovf_der(pb, p, ke, kw, kn, ks);
+    if (pb->ov_spinup != 1)
+      ovf_der(pb, p, ke, kw, kn, ks);
     for (int j = 0; j < ny; j++)
       for (int i = 0; i < nx; i++)
       {
@@ -1219,7 +1240,9 @@ void pfo_jacobian_fd(const pfo_problem *pb, double dt, const double *p, int symm
           cp[c] += (vol / dz) + (vol / ffy) * dt * (ke[io] - kw[io])
                    + (vol / ffx) * dt * (kn[io] - ks[io]);
         else
-          cp[c] += 0.0 + dt * (vol / dz) * (0.0 * exp((p[c] < 0.0 ? p[c] : 0.0) * 0.0) * 0.0);
+          cp[c] += 0.0 + dt * (vol / dz)
+                         * (pb->ov_damp_p1 * exp((p[c] < 0.0 ? p[c] : 0.0) * pb->ov_damp_p1)
+                            * pb->ov_damp_p2);
         double tw = (vol / ffy) * dt * (ke[io - 1]);
         double te = (vol / ffy) * dt * (kw[io + 1]);
         double ts = (vol / ffx) * dt * (kn[io - sy2]);

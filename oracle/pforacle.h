@@ -67,6 +67,11 @@ typedef struct {
    * +y / +z neighbour (Solver.Nonlinear.FlowBarrierX/Y/Z, problem_FBx.c), or
    * NULL = 1; nl_function_eval.c:841-843, richards_jacobian_eval.c:662-728 */
   const double *fbx, *fby, *fbz;
+  /* OverlandFlowSpinUp (0 / 1) and OverlandSpinupDampP1 / P2 of an
+   * OverlandFlow top patch (nl_function_eval.c:1659-1673,
+   * richards_jacobian_eval.c:1258-1287, 2044-2057) */
+  int ov_spinup;
+  double ov_damp_p1, ov_damp_p2;
 } pfo_problem;
 
 typedef struct {

@@ -303,6 +303,29 @@ def mg_minn_small() -> RichardsProblem:
                           solver=SolverSettings(mg_max_min_n=(3, 1, 3)))
 
 
+def spinup_small() -> RichardsProblem:
+    """OverlandFlowSpinUp 1 with OverlandSpinupDampP1 / P2 on the OverlandFlow
+    case: the ponded head drains in place of the routing, and the damping
+    term acts on non-ponded top cells (nl_function_eval.c:1659-1673)."""
+    p = configs.overland(nx=12, ny=10, nz=6, nsteps=3, dt=1.0, seed=101, wt_depth=0.02,
+                         mannings=1e-3, rain_steps=2, dry_steps=1, kind=BC_OVERLAND,
+                         solver=SolverSettings(max_iter=60))
+    p.overland_spinup = 1
+    p.spinup_damp = (10.0, 1e-4)
+    return p
+
+
+def spinup_damp_small() -> RichardsProblem:
+    """OverlandSpinupDampP1 / P2 without spin-up: the damping term joins the
+    ponding and routing term of the OverlandFlow patch (two rain steps; the
+    dry step after them needs 74 GMRES iterations in 4 Newton iterations,
+    where rounding alone moves the count by one)."""
+    p = configs.overland(nx=12, ny=10, nz=6, nsteps=2, seed=103, wt_depth=0.02,
+                         mannings=1e-3, rain_steps=2, dry_steps=0, kind=BC_OVERLAND)
+    p.spinup_damp = (10.0, 1e-4)
+    return p
+
+
 # pressure output of the golden runs (to_reference's dump_interval):
 # every step for the growth case, every 1.0 (one base dt) otherwise
 DUMP = {"growth_small": -1}
@@ -314,7 +337,8 @@ GOLDEN = ["box_small", "box_odd", "hetero_small", "walker2_small", "hydrostatic"
           "vel_overland_small", "growth_small", "halving_small", "restart_small",
           "picard_small", "inexact_small", "flow_barrier_small", "fulljac_small",
           "fulljac_overland_small", "fulljac_diff_small", "dq_overland_flow_small",
-          "dirichlet_top_small", "mg_maxiter_small", "mg_minn_small"]
+          "dirichlet_top_small", "mg_maxiter_small", "mg_minn_small",
+          "spinup_small", "spinup_damp_small"]
 # cases whose steps are not the constant-dt plan of RichardsProblem.time_plan
 TIME_LOOP = ["growth_small", "halving_small"]
 

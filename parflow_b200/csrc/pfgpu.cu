@@ -3232,6 +3232,17 @@ int pfgpu_set_pc_matrix(pfgpu_handle *h, int type) {
   return PFGPU_OK;
 }
 
+int pfgpu_set_overland_spinup(pfgpu_handle *h, int spinup, double damp_p1, double damp_p2) {
+  if (!h || (spinup != 0 && spinup != 1) || !std::isfinite(damp_p1) || !std::isfinite(damp_p2)) {
+    set_err("pfgpu_set_overland_spinup: spinup must be 0 or 1 and the damping finite");
+    return PFGPU_ERR_ARG;
+  }
+  h->P.ov_spinup = spinup;
+  h->P.ov_p1 = damp_p1;
+  h->P.ov_p2 = damp_p2;
+  return PFGPU_OK;
+}
+
 int pfgpu_set_globalization(pfgpu_handle *h, int strategy) {
   if (!h || (strategy != PFGPU_GLOBAL_LINE_SEARCH && strategy != PFGPU_GLOBAL_INEXACT_NEWTON)) {
     set_err("pfgpu_set_globalization: strategy must be PFGPU_GLOBAL_LINE_SEARCH or "
@@ -3375,6 +3386,10 @@ int pfgpu_adjoint_gradient(pfgpu_handle *h, int nobs_steps, const int *obs_steps
   }
   if (h->P.fbx || h->P.fby || h->P.fbz) {
     set_err("pfgpu_adjoint_gradient: not available with flow barriers");
+    return PFGPU_ERR_STATE;
+  }
+  if (h->P.ov_spinup || h->P.ov_p2 != 0.0) {
+    set_err("pfgpu_adjoint_gradient: not available with overland spin-up or its damping");
     return PFGPU_ERR_STATE;
   }
   if (h->P.bc_type[5] == PFGPU_BC_OVERLAND_DIFF) {

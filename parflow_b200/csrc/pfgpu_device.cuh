@@ -27,6 +27,11 @@ struct DevProblem {
   // flow-barrier multipliers of the faces to the +x / +y / +z neighbour, or
   // null (1 everywhere)
   const double *fbx, *fby, *fbz;
+  // OverlandFlowSpinUp and OverlandSpinupDampP1 / P2 of an OverlandFlow top
+  // patch (nl_function_eval.c:1659-1673, richards_jacobian_eval.c:1258-1287,
+  // 2044-2057)
+  int ov_spinup;
+  double ov_p1, ov_p2;
   const double *zmult;          // per layer
   // per z face between layers k and k+1: 1/sep, z_k/(z_k+z_k+1), z_k+1/(z_k+z_k+1)
   const double *zface;          // 3*nz

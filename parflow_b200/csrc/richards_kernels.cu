@@ -161,16 +161,22 @@ __device__ __forceinline__ void residual_cell(const DevProblem &P, int i, int j,
       }
     } else if (SURF && P.bc_type[face] == 4) {
       // OverlandFlow top face (nl_function_eval.c:1437-1690): each face flux
-      // is the upwind part of the two columns' own fluxes; the spin-up
-      // damping term is zero with its default parameters
+      // is the upwind part of the two columns' own fluxes, plus the spin-up
+      // damping term; with OverlandFlowSpinUp the ponded head drains in
+      // place of the ponding and routing term (:1659-1673)
       const double qw = ovf_q<true>(P, p, i - 1, j), qc = ovf_q<true>(P, p, i, j),
                    qe = ovf_q<true>(P, p, i + 1, j);
       const double kw = pmax0(qw) - pmax0(-qc), ke = pmax0(qc) - pmax0(-qe);
       const double qs = ovf_q<false>(P, p, i, j - 1), qm = ovf_q<false>(P, p, i, j),
                    qn = ovf_q<false>(P, p, i, j + 1);
       const double ks = pmax0(qs) - pmax0(-qm), kn = pmax0(qm) - pmax0(-qn);
-      const double q_ov = vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
-                          dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      double q_ov = vol * (pmax0(pc) - pmax0(p_old[c])) / P.dz +
+                    dt * vol * ((ke - kw) / P.dx + (kn - ks) / P.dy) / P.dz;
+      if (P.ov_p2 != 0.0 || P.ov_spinup == 1) {
+        const double damp = exp(fmin(pc, 0.0) * P.ov_p1) * P.ov_p2;
+        q_ov = q_ov + vol * dt / P.dz * damp;
+        if (P.ov_spinup == 1) q_ov = (vol / P.dz) * dt * ((pmax0(pc) - 0.0) + damp);
+      }
       fc += q_ov;
       u_new = ffz * value;
       if (VEL) {
@@ -666,20 +672,29 @@ __device__ __forceinline__ void jacobian_cell(const DevProblem &P, int i, int j,
   // (richards_jacobian_eval.c:2028-2090, CALCDER of overlandflow_eval.c):
   // the derivative parts of each column's own flux; neighbours' parts give
   // the off-diagonals, and the east neighbour's west term lands in E(i)
+  // With OverlandFlowSpinUp the patch's own diagonal term of a cell with
+  // p >= 0 comes first (richards_jacobian_eval.c:1258-1268) and the
+  // derivative parts are zero (their evaluation is skipped, :1287); a
+  // non-ponded cell gets the derivative of the spin-up damping term.
   if (SURF && !M.fd && k == P.nz - 1 && P.bc_type[5] == 4) {
+    const bool spin = P.ov_spinup == 1;
+    if (spin && pc >= 0.0) cp += (vol / P.dz) * dt * (1.0 + 0.0);
     const double cx = (vol / ffy) * dt, cy = (vol / ffx) * dt;
-    const double qx = ovf_qder<true>(P, pc, i, j), qy = ovf_qder<false>(P, pc, i, j);
+    const double qx = spin ? 0.0 : ovf_qder<true>(P, pc, i, j);
+    const double qy = spin ? 0.0 : ovf_qder<false>(P, pc, i, j);
     const double ke_d = pmax0(qx), kw_d = -pmax0(-qx);
     const double kn_d = pmax0(qy), ks_d = -pmax0(-qy);
     // the neighbours' derivative parts: ke of i-1, kw of i+1, kn of j-1, ks of j+1
-    const double ke_w = i > 0 ? pmax0(ovf_qder<true>(P, p[c - 1], i - 1, j)) : 0.0;
-    const double kw_e = i + 1 < P.nx ? -pmax0(-ovf_qder<true>(P, p[c + 1], i + 1, j)) : 0.0;
-    const double kn_s = j > 0 ? pmax0(ovf_qder<false>(P, p[c - sy], i, j - 1)) : 0.0;
-    const double ks_n = j + 1 < P.ny ? -pmax0(-ovf_qder<false>(P, p[c + sy], i, j + 1)) : 0.0;
+    const double ke_w = i > 0 && !spin ? pmax0(ovf_qder<true>(P, p[c - 1], i - 1, j)) : 0.0;
+    const double kw_e =
+        i + 1 < P.nx && !spin ? -pmax0(-ovf_qder<true>(P, p[c + 1], i + 1, j)) : 0.0;
+    const double kn_s = j > 0 && !spin ? pmax0(ovf_qder<false>(P, p[c - sy], i, j - 1)) : 0.0;
+    const double ks_n =
+        j + 1 < P.ny && !spin ? -pmax0(-ovf_qder<false>(P, p[c + sy], i, j + 1)) : 0.0;
     if (pc > 0.0)
       cp += (vol / P.dz) + cx * (ke_d - kw_d) + cy * (kn_d - ks_d);
     else
-      cp += 0.0 + dt * (vol / P.dz) * (0.0 * exp(fmin(pc, 0.0) * 0.0) * 0.0);
+      cp += 0.0 + dt * (vol / P.dz) * (P.ov_p1 * exp(fmin(pc, 0.0) * P.ov_p1) * P.ov_p2);
     const double tw = cx * (ke_w), te = cx * (kw_e);
     const double ts = cy * (kn_s), tn = cy * (ks_n);
     w -= tw;

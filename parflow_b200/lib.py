@@ -67,7 +67,8 @@ EXPORTS = ["pfgpu_create", "pfgpu_destroy", "pfgpu_last_error", "pfgpu_set_field
            "pfgpu_newton_solve_sat", "pfgpu_set_old_pressure", "pfgpu_autotune",
            "pfgpu_set_jacobian_mode", "pfgpu_set_relperm_table", "pfgpu_set_evap_trans",
            "pfgpu_face_velocities", "pfgpu_solve_graph", "pfgpu_set_globalization",
-           "pfgpu_set_pc_matrix", "pfgpu_set_mg_max_iter"]
+           "pfgpu_set_pc_matrix", "pfgpu_set_mg_max_iter",
+           "pfgpu_set_overland_spinup"]
 PFB_PRESSURE, PFB_SATURATION = 100, 101
 KERNELS = {"residual": 0, "jacobian": 1, "matvec": 2, "rb_smooth": 3, "vcycle": 4, "mg_setup": 5,
            "colour_sweep": 6}
@@ -120,6 +121,7 @@ def load(path: str = LIB_PATH):
     L.pfgpu_set_globalization.argtypes = [vp, C.c_int]
     L.pfgpu_set_pc_matrix.argtypes = [vp, C.c_int]
     L.pfgpu_set_mg_max_iter.argtypes = [vp, C.c_int]
+    L.pfgpu_set_overland_spinup.argtypes = [vp, C.c_int, C.c_double, C.c_double]
     L.pfgpu_face_velocities.argtypes = [vp, C.c_void_p, C.c_void_p, C.c_void_p, C.c_double] + \
         [C.c_void_p] * 5
     L.pfgpu_saturation.argtypes = [vp, C.c_void_p, C.c_void_p]

@@ -527,6 +527,11 @@ static void create_handle(GpuInstanceXtra *ix, GpuPublicXtra *px, Vector *pressu
     if (pfgpu_set_surface(ix->h, sx, sy, mn, tfg, eps) != PFGPU_OK)
       gpu_fail(pfgpu_last_error());
   }
+  /* OverlandFlowSpinUp and its damping (nl_function_eval.c:313, 2474-2477) */
+  if (pfgpu_set_overland_spinup(ix->h, GetIntDefault("OverlandFlowSpinUp", 0),
+                                GetDoubleDefault("OverlandSpinupDampP1", 0.0),
+                                GetDoubleDefault("OverlandSpinupDampP2", 0.0)) != PFGPU_OK)
+    gpu_fail(pfgpu_last_error());
   ix->face[0] = ctalloc(double, (long)d.nz * d.ny);
   ix->face[1] = ctalloc(double, (long)d.nz * d.ny);
   ix->face[2] = ctalloc(double, (long)d.nz * d.nx);

@@ -220,6 +220,10 @@ class RichardsProblem:
     fbx: object = None
     fby: object = None
     fbz: object = None
+    # OverlandFlowSpinUp (an OverlandFlow top patch drains its ponded head
+    # instead of routing it) and OverlandSpinupDampP1 / P2
+    overland_spinup: int = 0
+    spinup_damp: tuple = (0.0, 0.0)
     # reference output of the face velocities (Solver.PrintVelocities)
     print_velocities: bool = False
     # TimeStep.Type Growth: (initial step, growth factor, min step, max
@@ -625,6 +629,11 @@ class RichardsProblem:
                 k[f"Solver.Nonlinear.FlowBarrier{d}"] = True
                 k[f"FB{d.lower()}.Type"] = "PFBFile"
                 k[f"Geom.domain.FB{d.lower()}.FileName"] = fn
+        if self.overland_spinup:
+            k["OverlandFlowSpinUp"] = int(self.overland_spinup)
+        if self.spinup_damp != (0.0, 0.0):
+            k["OverlandSpinupDampP1"] = float(self.spinup_damp[0])
+            k["OverlandSpinupDampP2"] = float(self.spinup_damp[1])
         if self.print_velocities:
             k["Solver.PrintVelocities"] = True
             if any(bc.kind in (BC_OVERLAND_KIN, BC_OVERLAND_DIFF, BC_OVERLAND)

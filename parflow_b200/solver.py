@@ -101,6 +101,11 @@ class RichardsGPU:
                     "set_globalization")
         if s.pc_matrix_code():
             L.check(self.lib.pfgpu_set_pc_matrix(self.h, s.pc_matrix_code()), "set_pc_matrix")
+        if prob.overland_spinup or prob.spinup_damp != (0.0, 0.0):
+            L.check(self.lib.pfgpu_set_overland_spinup(self.h, int(prob.overland_spinup),
+                                                       float(prob.spinup_damp[0]),
+                                                       float(prob.spinup_damp[1])),
+                    "set_overland_spinup")
         if s.mg_max_iter != 1:
             L.check(self.lib.pfgpu_set_mg_max_iter(self.h, s.mg_max_iter), "set_mg_max_iter")
         if prob.kr_table:

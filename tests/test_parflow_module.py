@@ -70,7 +70,7 @@ GPU_CASES = ["box_small", "box_odd", "hetero_small", "walker2_small", "seepage_s
              "krtable_spline_small", "growth_small", "halving_small", "restart_small",
              "inexact_small", "rbgs_nonsym_small", "flow_barrier_small", "fulljac_small",
              "fulljac_overland_small", "dq_overland_flow_small", "dirichlet_top_small",
-             "mg_maxiter_small", "mg_minn_small"]
+             "mg_maxiter_small", "mg_minn_small", "spinup_small", "spinup_damp_small"]
 
 
 @pytest.mark.gpu
