@@ -321,7 +321,7 @@ def spinup_damp_small() -> RichardsProblem:
     dry step after them needs 74 GMRES iterations in 4 Newton iterations,
     where rounding alone moves the count by one)."""
     p = configs.overland(nx=12, ny=10, nz=6, nsteps=2, seed=103, wt_depth=0.02,
-                         mannings=1e-3, rain_steps=2, dry_steps=0, kind=BC_OVERLAND)
+                         mannings=1e-3, rain_steps=2, dry_steps=1, kind=BC_OVERLAND)
     p.spinup_damp = (10.0, 1e-4)
     return p
 
